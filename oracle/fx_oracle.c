@@ -1,0 +1,956 @@
+/*
+ * fx_oracle.c -- CPU oracle (test infrastructure) for the Flash-X unsplit
+ * hydro block update.  See fx_oracle.h for the role and parity status.
+ *
+ * This file restates, in FP64 C with the reference's operation order, the
+ * pure-hydro (FLASH_UHD_HYDRO), gamma-law (FLASH_EOS_GAMMA) branch of
+ *   FX = Flash-X/source, UHD = FX/physics/Hydro/HydroMain/unsplit
+ *   UHD/hy_computeFluxes.F90:87-417        per-block driver
+ *   UHD/hy_getRiemannState.F90:79-1487     cell loop, face-state storage, 3-D CTU
+ *   UHD/hy_dataReconstOneStep.F90:93-1222  per-direction dispatch, transverse terms
+ *   UHD/hy_DataReconstructNormalDir_PPM.F90:84-969
+ *   UHD/hy_DataReconstructNormalDir_WENO.F90:85-919
+ *   UHD/hy_eigenParameters.F90:53-299, hy_eigenValue.F90:44-75,
+ *   UHD/OnlyHydro/hy_eigenVector.F90:57-281
+ *   UHD/hy_TVDslope.F90:65-276, hy_slopeLimiters.F90
+ *   UHD/hy_upwindTransverseFlux.F90:54-222
+ *   UHD/hy_getFaceFlux.F90:64-1286, hy_HLLC.F90:64-335, hy_HLL.F90:64-182,
+ *   UHD/hy_prim2con.F90:34-67, hy_prim2flx.F90:36-151
+ *   UHD/hy_unsplitUpdate.F90:84-1306, hy_energyFix.F90:76-480
+ *   UHD/Hydro_computeDt.F90:151-291
+ *   FX/physics/Eos/EosMain/{Eos_getData,Eos_putData}.F90, Gamma/Eos.F90:227-250
+ *   FX/Grid/GridMain/UG/Grid_fillGuardCells.F90:260-306,
+ *   FX/Grid/GridBoundaryConditions/Grid_bcApplyToRegion.F90:458-531
+ *
+ * Build with -ffp-contract=off: no fused multiply-adds, every operation
+ * rounded as written, so results are reproducible bit for bit.
+ */
+#include "fx_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* Primitive slots of UHD.h:373-388 (0-based): HY_DENS..HY_EINT, HY_GRAV. */
+enum { H_D = 0, H_VX, H_VY, H_VZ, H_P, H_GC, H_GE, H_EI, H_GR, H_NV };
+/* Flux slots UHD.h:399-406 (0-based). */
+enum { F_D = 0, F_MX, F_MY, F_MZ, F_E, F_P, F_EI, F_VOL, F_NF };
+
+/* ---- Fortran intrinsics with gfortran semantics ------------------------ */
+/* MIN(a1,a2): mvar = a1; if (a2 < mvar) mvar = a2.  MAX likewise. */
+static inline double fmin2(double a, double b) { return (b < a) ? b : a; }
+static inline double fmax2(double a, double b) { return (b > a) ? b : a; }
+static inline double fmin3(double a, double b, double c) { return fmin2(fmin2(a, b), c); }
+static inline double fsign1(double b) { return copysign(1.0, b); }
+
+/* ---- limiters: hy_slopeLimiters.F90 ------------------------------------ */
+static inline double lim_minmod(double a, double b)
+{ return .5 * (fsign1(a) + fsign1(b)) * fmin2(fabs(a), fabs(b)); }
+static inline double lim_mc(double a, double b)
+{ return (fsign1(a) + fsign1(b)) * fmin3(fabs(a), .25 * fabs(a + b), fabs(b)); }
+static inline double lim_vanleer(double a, double b)
+{ if (a * b <= 0.) return 0.; return 2. * a * b / (a + b); }
+
+/* Per-block geometry shared by all routines. */
+typedef struct {
+    const fxo_params *p;
+    int ng, nig, njg, nkg, k2, k3;
+    int i0, imax, j0, jmax, k0, kmax;
+    double dx, dy, dz;
+    long ncell;                  /* nig*njg*nkg */
+} blk_t;
+
+static inline long cidx(const blk_t *b, int i, int j, int k)
+{ return ((long)k * b->njg + j) * b->nig + i; }
+
+static int n_end_vars(const fxo_params *p) { return p->use_gravity ? 9 : 8; }  /* HY_END_VARS */
+
+/* Load the primitive vector V(HY_DENS:HY_GRAV) of one cell. */
+static void load_v(const fxo_params *p, const double *u, double grav_dir, double V[H_NV])
+{
+    V[H_D] = u[FXO_DENS]; V[H_VX] = u[FXO_VELX]; V[H_VY] = u[FXO_VELY]; V[H_VZ] = u[FXO_VELZ];
+    V[H_P] = u[FXO_PRES]; V[H_GC] = u[FXO_GAMC]; V[H_GE] = u[FXO_GAME]; V[H_EI] = u[FXO_EINT];
+    V[H_GR] = p->use_gravity ? grav_dir : 0.;
+}
+
+/* ---- eigensystem (pure hydro, primitive form) --------------------------- */
+/* hy_eigenParameters.F90:84-100, hy_eigenValue.F90:58-62,
+ * OnlyHydro/hy_eigenVector.F90:87-167.  L[var][wave], R[var][wave]. */
+static int eigen(const double *V, int dir, double lam[5], double L[5][5], double R[5][5])
+{
+    double uN = V[H_VX + dir];
+    double a2 = V[H_GC] * V[H_P] / V[H_D];
+    if (a2 <= 0.) return 1;
+    double cf = sqrt(a2);
+    lam[0] = uN - cf; lam[1] = uN; lam[2] = uN; lam[3] = uN; lam[4] = uN + cf;
+    int v1 = H_VX + dir;
+    int v2 = (dir == 0) ? H_VY : (dir == 1) ? H_VZ : H_VX;
+    int v3 = (dir == 0) ? H_VZ : (dir == 1) ? H_VX : H_VY;
+    memset(L, 0, sizeof(double) * 25);
+    memset(R, 0, sizeof(double) * 25);
+    double dinv = 1. / V[H_D];
+    double aa2 = cf * cf;
+    double a2inv = 1. / aa2;
+    double ahinv = 0.5 / cf;
+    double Na = 0.5 * a2inv;
+    L[v1][0] = -ahinv;  L[H_P][0] = dinv * Na;
+    L[v2][1] = 1.;
+    L[H_D][2] = 1.;     L[H_P][2] = -a2inv;
+    L[v3][3] = 1.;
+    L[v1][4] = ahinv;   L[H_P][4] = L[H_P][0];
+    R[H_D][0] = V[H_D]; R[v1][0] = -cf; R[H_P][0] = V[H_D] * aa2;
+    R[v2][1] = 1.;
+    R[H_D][2] = 1.;
+    R[v3][3] = 1.;
+    R[H_D][4] = V[H_D]; R[v1][4] = cf;  R[H_P][4] = R[H_P][0];
+    return 0;
+}
+
+/* Fortran dot_product over HY_DENS:HY_PRES with a zero-initialised sum. */
+static inline double dot5(double L[5][5], int w, const double *x)
+{
+    double s = 0.;
+    for (int v = 0; v < 5; v++) s = s + L[v][w] * x[v];
+    return s;
+}
+
+/* ---- hy_TVDslope.F90:65-276 -------------------------------------------- */
+static void tvd_slope(const fxo_params *p, const double *VL, const double *V0, const double *VR,
+                      double L[5][5], double delbar[H_NV])
+{
+    double dL[H_NV], dR[H_NV];
+    int nend = n_end_vars(p);
+    for (int k = 0; k < H_NV; k++) { delbar[k] = 0.; dL[k] = V0[k] - VL[k]; dR[k] = VR[k] - V0[k]; }
+    int lim = p->limiter;
+    if (lim == FXO_MINMOD || lim == FXO_MC || lim == FXO_VANLEER) {
+        double (*f)(double, double) = (lim == FXO_MINMOD) ? lim_minmod : (lim == FXO_MC) ? lim_mc : lim_vanleer;
+        if (p->char_limiting) {
+            for (int w = 0; w < 5; w++) delbar[w] = f(dot5(L, w, dL), dot5(L, w, dR));
+            for (int k = H_GC; k < nend; k++) delbar[k] = f(dL[k], dR[k]);
+        } else {
+            for (int k = 0; k < nend; k++) delbar[k] = f(dL[k], dR[k]);
+        }
+    } else if (lim == FXO_HYBRID) {
+        if (p->char_limiting) {
+            delbar[0] = lim_minmod(dot5(L, 0, dL), dot5(L, 0, dR));
+            delbar[1] = lim_minmod(dot5(L, 1, dL), dot5(L, 1, dR));
+            delbar[2] = lim_mc(dot5(L, 2, dL), dot5(L, 2, dR));
+            delbar[3] = lim_minmod(dot5(L, 3, dL), dot5(L, 3, dR));
+            delbar[4] = lim_minmod(dot5(L, 4, dL), dot5(L, 4, dR));
+            for (int k = H_GC; k < nend; k++) delbar[k] = lim_mc(dL[k], dR[k]);
+        } else {
+            for (int k = 0; k < nend; k++) {
+                if (k == H_D || k == H_GC || k == H_GE || k == H_GR) delbar[k] = lim_mc(dL[k], dR[k]);
+                else if (k >= H_VX && k <= H_P) delbar[k] = lim_minmod(dL[k], dR[k]);
+            }
+        }
+    } else { /* LIMITED */
+        double beta = p->limited_beta;
+        int nw = p->char_limiting ? 5 : 0;
+        for (int k = 0; k < nend; k++) {
+            double d1, d2;
+            if (k < nw) { d1 = dot5(L, k, dL); d2 = dot5(L, k, dR); }
+            else if (p->char_limiting && k < H_GC) continue;
+            else { d1 = dL[k]; d2 = dR[k]; }
+            if (d2 > 0.) delbar[k] = fmax2(fmax2(0., fmin2(beta * d1, d2)), fmin2(d1, beta * d2));
+            else         delbar[k] = fmin2(fmin2(0., fmax2(beta * d1, d2)), fmax2(d1, beta * d2));
+        }
+    }
+}
+
+/* ---- hy_upwindTransverseFlux.F90:54-222 (hydro variables) -------------- */
+static void upwind_trans(const fxo_params *p, const double *vm1, const double *vc0, const double *vp1,
+                         const double lam[5], double L[5][5], double R[5][5], int sig_size, double *sig)
+{
+    double TF[H_NV];
+    for (int k = 0; k < sig_size; k++) sig[k] = 0.;
+    for (int n = 0; n < 5; n++) {
+        if (lam[n] > 0.) { for (int v = 0; v < 5; v++) TF[v] = vc0[v] - vm1[v]; }
+        else             { for (int v = 0; v < 5; v++) TF[v] = vp1[v] - vc0[v]; }
+        double d = dot5(L, n, TF);
+        for (int v = 0; v < 5; v++) { TF[v] = lam[n] * R[v][n] * d; sig[v] = sig[v] + TF[v]; }
+    }
+    if (p->use_aux_eint) {          /* hyBeg = hyVarEnd = HY_EINT */
+        double t = (lam[2] > 0.) ? (vc0[H_EI] - vm1[H_EI]) : (vp1[H_EI] - vc0[H_EI]);
+        sig[H_EI] = lam[2] * t;
+        if (p->use_gravity && H_GR < sig_size) sig[H_GR] = 0.;
+    }
+}
+
+/* ---- hy_DataReconstructNormalDir_PPM.F90:84-969 ------------------------ */
+/* S[0..4] = Vmm, Vm, Vc, Vp, Vpp (Vmm/Vpp unused when trans_only). */
+static int recon_ppm(const fxo_params *p, int dir, double dt, double delta,
+                     const double *S[5], int trans_only,
+                     double lam0[5], double L0[5][5], double R0[5][5],
+                     double Wp[H_NV], double Wm[H_NV], double sig[H_NV])
+{
+    const int nend = p->use_gravity ? 9 : (p->use_aux_eint ? 8 : 5);   /* hyEndVar */
+    const int npr = 5;                                                   /* hyEndPrimVar */
+    const double *Vm = S[1], *Vc = S[2], *Vp = S[3];
+    double dtn = dt / delta, hdtn = 0.5 * dtn;
+    for (int k = 0; k < H_NV; k++) { Wp[k] = 0.; Wm[k] = 0.; }
+    if (eigen(Vc, dir, lam0, L0, R0)) return 1;
+    if (p->ndim > 1) upwind_trans(p, Vm, Vc, Vp, lam0, L0, R0, n_end_vars(p), sig);
+    if (trans_only) return 0;
+
+    double lamP[5], LP[5][5], RP[5][5], lamN[5], LN[5][5], RN[5][5];
+    if (eigen(Vp, dir, lamP, LP, RP)) return 1;
+    if (eigen(Vm, dir, lamN, LN, RN)) return 1;
+    double dbN[H_NV], db0[H_NV], dbP[H_NV];
+    tvd_slope(p, S[0], Vm, Vc, LN, dbN);
+    tvd_slope(p, Vm, Vc, Vp, L0, db0);
+    tvd_slope(p, Vc, Vp, S[4], LP, dbP);
+    if (p->char_limiting) {
+        double t0[5], tP[5], tN[5];
+        for (int v = 0; v < 5; v++) {
+            t0[v] = R0[v][0] * db0[0] + R0[v][1] * db0[1] + R0[v][2] * db0[2] + R0[v][3] * db0[3] + R0[v][4] * db0[4];
+            tP[v] = RP[v][0] * dbP[0] + RP[v][1] * dbP[1] + RP[v][2] * dbP[2] + RP[v][3] * dbP[3] + RP[v][4] * dbP[4];
+            tN[v] = RN[v][0] * dbN[0] + RN[v][1] * dbN[1] + RN[v][2] * dbN[2] + RN[v][3] * dbN[3] + RN[v][4] * dbN[4];
+        }
+        for (int v = 0; v < 5; v++) { db0[v] = t0[v]; dbP[v] = tP[v]; dbN[v] = tN[v]; }
+    }
+    double vecL[H_NV], vecR[H_NV], delW[H_NV], W6[H_NV];
+    for (int k = 0; k < H_NV; k++) { vecL[k] = 0.; vecR[k] = 0.; }
+    for (int n = 0; n < nend; n++) {
+        vecL[n] = 0.5 * (Vc[n] + Vm[n]) - (db0[n] - dbN[n]) / 6.;
+        vecR[n] = 0.5 * (Vc[n] + Vp[n]) - (dbP[n] - db0[n]) / 6.;
+    }
+    /* monotonicity, CW84 eq. 1.10 */
+    for (int n = 0; n < nend; n++) {
+        if ((vecR[n] - Vc[n]) * (Vc[n] - vecL[n]) <= 0.) { vecL[n] = Vc[n]; vecR[n] = Vc[n]; }
+        if (6. * (vecR[n] - vecL[n]) * (Vc[n] - 0.5 * (vecL[n] + vecR[n])) > (vecR[n] - vecL[n]) * (vecR[n] - vecL[n]))
+            vecL[n] = 3. * Vc[n] - 2. * vecR[n];
+        if (6. * (vecR[n] - vecL[n]) * (Vc[n] - 0.5 * (vecL[n] + vecR[n])) < -((vecR[n] - vecL[n]) * (vecR[n] - vecL[n])))
+            vecR[n] = 3. * Vc[n] - 2. * vecL[n];
+    }
+    for (int n = 0; n < nend; n++) {
+        delW[n] = vecR[n] - vecL[n];
+        W6[n] = 6. * (Vc[n] - 0.5 * (vecR[n] + vecL[n]));
+    }
+    /* [7] initial guesses: only the secondary variables survive [10] */
+    double lmax = fmax2(lam0[2], 0.);
+    for (int n = npr; n < nend; n++)
+        Wp[n] = vecR[n] - lmax * hdtn * (delW[n] - (1.0 - lmax * hdtn * 4. / 3.) * W6[n]);
+    double lmin = -fmin2(lam0[2], 0.);
+    for (int n = npr; n < nend; n++)
+        Wm[n] = vecL[n] + lmin * hdtn * (delW[n] + (1.0 - lmin * hdtn * 4. / 3.) * W6[n]);
+    Wp[H_GC] = Vc[H_GC]; Wp[H_GE] = Vc[H_GE];   /* FLASH_EOS_GAMMA */
+    Wm[H_GC] = Vc[H_GC]; Wm[H_GE] = Vc[H_GE];
+    if (p->use_gravity) { Wp[H_GR] = vecR[H_GR]; Wm[H_GR] = vecL[H_GR]; }
+    /* [8] characteristic tracing, HLL-type branch */
+    double sigL[5] = {0., 0., 0., 0., 0.}, sigR[5] = {0., 0., 0., 0., 0.};
+    double mW6[5];
+    for (int v = 0; v < 5; v++) mW6[v] = -W6[v];
+    for (int n = 0; n < 5; n++) {
+        double cA = dot5(L0, n, delW);
+        double cB = dot5(L0, n, mW6);
+        double lt = dtn * lam0[n];
+        double aL = .5 * (-1. - dtn * lam0[n]);
+        double bL = .25 * (1. + 2. * dtn * lam0[n] + 4. / 3. * (lt * lt));
+        double aR = .5 * (1. - dtn * lam0[n]);
+        double bR = .25 * (1. - 2. * dtn * lam0[n] + 4. / 3. * (lt * lt));
+        for (int v = 0; v < 5; v++) {
+            sigL[v] = sigL[v] + (aL * R0[v][n] * cA + bL * R0[v][n] * cB);
+            sigR[v] = sigR[v] + (aR * R0[v][n] * cA + bR * R0[v][n] * cB);
+        }
+    }
+    for (int v = 0; v < npr; v++) {
+        Wm[v] = Vc[v] + W6[v] / 12. + sigL[v];
+        Wp[v] = Vc[v] + W6[v] / 12. + sigR[v];
+    }
+    return 0;
+}
+
+/* ---- WENO5 / WENO-Z reconstruction: see recon_weno below --------------- */
+static int recon_weno(const fxo_params *p, int dir, double dt, double delta,
+                      const double *S[5], int trans_only,
+                      double lam0[5], double L0[5][5], double R0[5][5],
+                      double Wp[H_NV], double Wm[H_NV], double sig[H_NV]);
+
+/* ---- Riemann solvers ---------------------------------------------------- */
+/* hy_prim2con.F90:34-67 */
+static void prim2con(const double *V, double U[5])
+{
+    double u2 = 0.; u2 = u2 + V[H_VX] * V[H_VX]; u2 = u2 + V[H_VY] * V[H_VY]; u2 = u2 + V[H_VZ] * V[H_VZ];
+    U[0] = V[H_D];
+    U[1] = V[H_D] * V[H_VX]; U[2] = V[H_D] * V[H_VY]; U[3] = V[H_D] * V[H_VZ];
+    U[4] = 0.5 * V[H_D] * u2 + V[H_P] / (V[H_GE] - 1.) + 0.5 * 0.;
+}
+/* hy_prim2flx.F90:36-151 (hydro) */
+static void prim2flx(const fxo_params *p, int dir, const double *V, double F[6])
+{
+    double u2 = 0.; u2 = u2 + V[H_VX] * V[H_VX]; u2 = u2 + V[H_VY] * V[H_VY]; u2 = u2 + V[H_VZ] * V[H_VZ];
+    double E = 0.5 * V[H_D] * u2 + V[H_P] / (V[H_GE] - 1.);
+    double fP = p->fpres;
+    F[F_P] = V[H_P];
+    double vn = V[H_VX + dir];
+    F[F_D] = V[H_D] * vn;
+    F[F_MX] = F[F_D] * V[H_VX];
+    F[F_MY] = F[F_D] * V[H_VY];
+    F[F_MZ] = F[F_D] * V[H_VZ];
+    F[F_MX + dir] = F[F_D] * V[H_VX + dir] + fP * V[H_P];
+    F[F_E] = (E + V[H_P]) * vn;
+}
+
+/* hy_HLLC.F90:64-335 (hydro).  Returns ierr. */
+static int riemann_hllc(const fxo_params *p, int dir, const double *Vm, const double *Vp, double Fs[6], double *speed)
+{
+    double velNL = Vm[H_VX + dir], velNR = Vp[H_VX + dir];
+    double aL2 = Vm[H_GC] * Vm[H_P] / Vm[H_D];
+    double aR2 = Vp[H_GC] * Vp[H_P] / Vp[H_D];
+    double tiny = p->tiny;
+    if ((Vm[H_D] < tiny && Vm[H_D] > 0.) || (Vp[H_D] < tiny && Vp[H_D] > 0.) ||
+        (Vm[H_P] < tiny && Vm[H_P] > 0.) || (Vp[H_P] < tiny && Vp[H_P] > 0.)) {
+        for (int k = 0; k < 6; k++) Fs[k] = 0.;
+        *speed = 0.;
+        return 0;
+    } else if (aL2 < 0. || aR2 < 0.) {
+        return 1;
+    }
+    double cfL = sqrt(aL2), cfR = sqrt(aR2);
+    double SL = fmin2(velNL - cfL, velNR - cfR);
+    double SR = fmax2(velNL + cfL, velNR + cfR);
+    *speed = fmax2(fabs(SL), fabs(SR));
+    double pL = Vm[H_P], pR = Vp[H_P];
+    double UL[5], UR[5], FL[6], FR[6];
+    prim2con(Vm, UL); prim2con(Vp, UR);
+    prim2flx(p, dir, Vm, FL); prim2flx(p, dir, Vp, FR);
+    /* (the HLL average state Uhll of :155-168 only feeds the MHD branch) */
+    double qStar = (Vp[H_D] * velNR * (SR - velNR) - Vm[H_D] * velNL * (SL - velNL) + pL - pR - 0. * 0. + 0. * 0.);
+    qStar = qStar / (Vp[H_D] * (SR - velNR) - Vm[H_D] * (SL - velNL));
+    double numerL = SL - velNL, denomL = SL - qStar;
+    double numerR = SR - velNR, denomR = SR - qStar;
+    double pStar = Vm[H_D] * numerL * (qStar - velNL) + pL;
+    double dStarL = UL[0] * numerL / denomL;
+    double dStarR = UR[0] * numerR / denomR;
+    double UCL[5], UCR[5];
+    UCL[0] = dStarL;
+    UCL[4] = UL[4] * numerL / denomL + ((pStar * qStar - pL * velNL)) / denomL;
+    UCR[0] = dStarR;
+    UCR[4] = UR[4] * numerR / denomR + ((pStar * qStar - pR * velNR)) / denomR;
+    for (int d = 0; d < 3; d++) {
+        if (d == dir) { UCL[1 + d] = dStarL * qStar; UCR[1 + d] = dStarR * qStar; }
+        else { UCL[1 + d] = UL[1 + d] * numerL / denomL; UCR[1 + d] = UR[1 + d] * numerR / denomR; }
+    }
+    if (SL >= 0.) {
+        for (int k = 0; k < 6; k++) Fs[k] = FL[k];
+    } else if (SL < 0. && qStar >= 0.) {
+        for (int k = 0; k < 5; k++) Fs[k] = FL[k] + SL * (UCL[k] - UL[k]);
+        Fs[F_P] = FL[F_P];
+    } else if (qStar < 0. && SR >= 0.) {
+        for (int k = 0; k < 5; k++) Fs[k] = FR[k] + SR * (UCR[k] - UR[k]);
+        Fs[F_P] = FR[F_P];
+    } else {
+        for (int k = 0; k < 6; k++) Fs[k] = FR[k];
+    }
+    return 0;
+}
+
+/* hy_HLL.F90:64-182 (hydro).  Note the solver's own tiny = 1e-32. */
+static int riemann_hll(const fxo_params *p, int dir, const double *Vm, const double *Vp, double Fs[6], double *speed)
+{
+    (void)p;
+    const double tiny = 1.e-32;
+    double velNL = Vm[H_VX + dir], velNR = Vp[H_VX + dir];
+    double aL2 = Vm[H_GC] * Vm[H_P] / Vm[H_D];
+    double aR2 = Vp[H_GC] * Vp[H_P] / Vp[H_D];
+    if ((Vm[H_D] < tiny && Vm[H_D] > 0.) || (Vp[H_D] < tiny && Vp[H_D] > 0.) ||
+        (Vm[H_P] < tiny && Vm[H_P] > 0.) || (Vp[H_P] < tiny && Vp[H_P] > 0.)) {
+        for (int k = 0; k < 6; k++) Fs[k] = 0.;
+        *speed = 0.;
+        return 0;
+    } else if (aL2 < 0. || aR2 < 0.) {
+        return 1;
+    }
+    double cfL = sqrt(aL2), cfR = sqrt(aR2);
+    double SL = fmin2(velNL - cfL, velNR - cfR);
+    double SR = fmax2(velNL + cfL, velNR + cfR);
+    *speed = fmax2(fabs(SL), fabs(SR));
+    double UL[6], UR[6], FL[6], FR[6];
+    prim2con(Vm, UL); prim2con(Vp, UR);
+    UL[5] = 0.; UR[5] = 0.;
+    prim2flx(p, dir, Vm, FL); prim2flx(p, dir, Vp, FR);
+    if (SL > 0.) {
+        for (int k = 0; k < 6; k++) Fs[k] = FL[k];
+    } else if (SR < 0.) {
+        for (int k = 0; k < 6; k++) Fs[k] = FR[k];
+    } else {
+        for (int k = 0; k < 6; k++)
+            Fs[k] = (SR * FL[k] - SL * FR[k] + SR * SL * (UR[k] - UL[k])) / (SR - SL);
+    }
+    return 0;
+}
+
+/* ======================================================================= */
+/* Per-block hy_computeFluxes with in-place update (Uout => Uin).          */
+/* ======================================================================= */
+typedef struct {
+    double *scr[3];     /* scrchFace{X,Y,Z}: [cell][16]: P01..P08 then N01..N08 */
+    double *flx[3];     /* fluxes: [cell][8] at face (i-1/2) etc. */
+    double *sig;        /* [cell][3][9] */
+    double *lam;        /* [cell][3][5] */
+    double *leig;       /* [cell][3][5][5] */
+    double *reig;       /* [cell][3][5][5] */
+    double *pav;        /* VAR1 averaged pressure [cell] */
+} scratch_t;
+
+static void scratch_alloc(scratch_t *s, long ncell)
+{
+    for (int d = 0; d < 3; d++) {
+        s->scr[d] = (double *)calloc((size_t)ncell * 16, sizeof(double));
+        s->flx[d] = (double *)calloc((size_t)ncell * 8, sizeof(double));
+    }
+    s->sig = (double *)calloc((size_t)ncell * 27, sizeof(double));
+    s->lam = (double *)calloc((size_t)ncell * 15, sizeof(double));
+    s->leig = (double *)calloc((size_t)ncell * 75, sizeof(double));
+    s->reig = (double *)calloc((size_t)ncell * 75, sizeof(double));
+    s->pav = (double *)calloc((size_t)ncell, sizeof(double));
+}
+static void scratch_free(scratch_t *s)
+{
+    for (int d = 0; d < 3; d++) { free(s->scr[d]); free(s->flx[d]); }
+    free(s->sig); free(s->lam); free(s->leig); free(s->reig); free(s->pav);
+}
+
+static void blk_init(blk_t *b, const fxo_params *p)
+{
+    b->p = p;
+    b->ng = p->nguard;
+    b->k2 = p->ndim >= 2; b->k3 = p->ndim == 3;
+    b->nig = p->nxb + 2 * b->ng;
+    b->njg = b->k2 ? p->nyb + 2 * b->ng : 1;
+    b->nkg = b->k3 ? p->nzb + 2 * b->ng : 1;
+    b->i0 = b->ng; b->imax = b->ng + p->nxb - 1;
+    b->j0 = b->k2 ? b->ng : 0; b->jmax = b->k2 ? b->ng + p->nyb - 1 : 0;
+    b->k0 = b->k3 ? b->ng : 0; b->kmax = b->k3 ? b->ng + p->nzb - 1 : 0;
+    b->dx = (p->xmax - p->xmin) / (double)(p->nxb * p->nblockx);
+    b->dy = b->k2 ? (p->ymax - p->ymin) / (double)(p->nyb * p->nblocky) : 1.;
+    b->dz = b->k3 ? (p->zmax - p->zmin) / (double)(p->nzb * p->nblockz) : 1.;
+    b->ncell = (long)b->nig * b->njg * b->nkg;
+}
+
+/* hy_getRiemannState.F90:482-912 and 963-1338 for one block. */
+static int riemann_states(const blk_t *b, const double *U, double dt, scratch_t *s)
+{
+    const fxo_params *p = b->p;
+    const int ndim = p->ndim;
+    const double del[3] = {b->dx, b->dy, b->dz};
+    const double hdt = 0.5 * dt;
+    const double hdtx = 0.5 * dt / b->dx, hdty = 0.5 * dt / b->dy, hdtz = 0.5 * dt / b->dz;
+    const int nev = n_end_vars(p);
+    const int klo = b->k3 ? b->k0 - 1 : 0, khi = b->k3 ? b->kmax + 1 : 0;
+    const int jlo = b->k2 ? b->j0 - 1 : 0, jhi = b->k2 ? b->jmax + 1 : 0;
+    for (int k = klo; k <= khi; k++)
+    for (int j = jlo; j <= jhi; j++)
+    for (int i = b->i0 - 1; i <= b->imax + 1; i++) {
+        long c = cidx(b, i, j, k);
+        int tr[3] = {0, 0, 0};
+        if (i > b->imax + 1 || i < b->i0 - 1) tr[0] = 1;
+        if (i > b->imax || i < b->i0) { tr[1] = 1; tr[2] = 1; }
+        if (ndim > 1) {
+            if (j > b->jmax + 1 || j < b->j0 - 1) tr[1] = 1;
+            if (j > b->jmax || j < b->j0) { tr[0] = 1; tr[2] = 1; }
+            if (ndim > 2) {
+                if (k > b->kmax + 1 || k < b->k0 - 1) tr[2] = 1;
+                if (k > b->kmax || k < b->k0) { tr[0] = 1; tr[1] = 1; }
+            }
+        }
+        double Wp[3][H_NV], Wn[3][H_NV];
+        double *sig = s->sig + c * 27;
+        double *lam = s->lam + c * 15;
+        double (*leig)[5][5] = (double (*)[5][5])(s->leig + c * 75);
+        double (*reig)[5][5] = (double (*)[5][5])(s->reig + c * 75);
+        /* hy_dataReconstOneStep: per-direction reconstruction */
+        for (int d = 0; d < ndim; d++) {
+            int ko = tr[d] ? 1 : 2;
+            double V[5][H_NV];
+            const double *S[5] = {NULL, NULL, NULL, NULL, NULL};
+            for (int o = -ko; o <= ko; o++) {
+                int ii = i + (d == 0 ? o : 0), jj = j + (d == 1 ? o : 0), kk = k + (d == 2 ? o : 0);
+                load_v(p, U + cidx(b, ii, jj, kk) * FXO_NUNK, p->grav[d], V[o + 2]);
+                S[o + 2] = V[o + 2];
+            }
+            int err = (p->order == 5)
+                ? recon_weno(p, d, dt, del[d], S, tr[d], lam + 5 * d, leig[d], reig[d], Wp[d], Wn[d], sig + 9 * d)
+                : recon_ppm(p, d, dt, del[d], S, tr[d], lam + 5 * d, leig[d], reig[d], Wp[d], Wn[d], sig + 9 * d);
+            if (err) return 1;
+        }
+        /* transverse contributions, hy_dataReconstOneStep.F90:931-962 */
+        if (ndim > 1) {
+            for (int v = 0; v < nev; v++) {
+                Wn[0][v] = Wn[0][v] - hdty * sig[9 + v];
+                Wp[0][v] = Wp[0][v] - hdty * sig[9 + v];
+                Wn[1][v] = Wn[1][v] - hdtx * sig[v];
+                Wp[1][v] = Wp[1][v] - hdtx * sig[v];
+            }
+            if (ndim > 2) {
+                for (int v = 0; v < nev; v++) {
+                    Wn[0][v] = Wn[0][v] - hdtz * sig[18 + v];
+                    Wp[0][v] = Wp[0][v] - hdtz * sig[18 + v];
+                    Wn[1][v] = Wn[1][v] - hdtz * sig[18 + v];
+                    Wp[1][v] = Wp[1][v] - hdtz * sig[18 + v];
+                    Wn[2][v] = Wn[2][v] - hdtx * sig[v] - hdty * sig[9 + v];
+                    Wp[2][v] = Wp[2][v] - hdtx * sig[v] - hdty * sig[9 + v];
+                }
+            }
+        }
+        /* last negativity check, hy_dataReconstOneStep.F90:1131-1165 */
+        for (int d = 0; d < ndim; d++) {
+            if (Wn[d][H_D] < 0. || Wp[d][H_D] < 0. || Wn[d][H_P] < 0. || Wp[d][H_P] < 0.) {
+                double Vc[H_NV];
+                load_v(p, U + c * FXO_NUNK, p->grav[d], Vc);
+                for (int v = 0; v < H_GR; v++) { Wn[d][v] = Vc[v]; Wp[d][v] = Vc[v]; }
+            }
+        }
+        /* gravity half update and storage, hy_getRiemannState.F90:843-891 */
+        for (int d = 0; d < ndim; d++) {
+            if (p->use_gravity) {
+                for (int e = 0; e < 3; e++) {
+                    double gp = (e == d) ? Wp[d][H_GR] : p->grav[e];
+                    double gn = (e == d) ? Wn[d][H_GR] : p->grav[e];
+                    Wp[d][H_VX + e] = Wp[d][H_VX + e] + hdt * gp;
+                    Wn[d][H_VX + e] = Wn[d][H_VX + e] + hdt * gn;
+                }
+            }
+            if (!tr[d]) {
+                double *sc = s->scr[d] + c * 16;
+                for (int v = 0; v < 8; v++) { sc[v] = Wp[d][v]; sc[8 + v] = Wn[d][v]; }
+            }
+        }
+    }
+
+    /* 3-D full CTU corner coupling, hy_getRiemannState.F90:963-1338 */
+    if (ndim == 3 && p->use_3d_full_ctu) {
+        const double dt2dxdy6 = dt * dt / (6. * b->dx * b->dy);
+        const double dt2dydz6 = dt * dt / (6. * b->dy * b->dz);
+        const double dt2dzdx6 = dt * dt / (6. * b->dz * b->dx);
+        for (int k = b->k0 - 2; k <= b->kmax + 2; k++)
+        for (int j = b->j0 - 2; j <= b->jmax + 2; j++)
+        for (int i = b->i0 - 2; i <= b->imax + 2; i++) {
+            long c = cidx(b, i, j, k);
+            double Vc[H_NV];
+            load_v(p, U + c * FXO_NUNK, 0., Vc);
+            /* pairs: (face dir, first transverse dir a with sig of dir sa, second b with sig sb) */
+            for (int fd = 0; fd < 3; fd++) {
+                int ii[3] = {i, j, k}, lo[3] = {b->i0, b->j0, b->k0}, hi[3] = {b->imax, b->jmax, b->kmax};
+                int ok = 1;
+                for (int e = 0; e < 3; e++) {
+                    if (e == fd) { if (ii[e] < lo[e] - 1 || ii[e] > hi[e] + 1) ok = 0; }
+                    else if (ii[e] < lo[e] || ii[e] > hi[e]) ok = 0;
+                }
+                if (!ok) continue;
+                /* X: TransFluxYZ (sig Z along y, eig Y) + TransFluxZY (sig Y along z, eig Z), factor dt2dydz6
+                 * Y: TransFluxZX (sig X along z, eig Z) + TransFluxXZ (sig Z along x, eig X), factor dt2dzdx6
+                 * Z: TransFluxXY (sig Y along x, eig X) + TransFluxYX (sig X along y, eig Y), factor dt2dxdy6 */
+                int e1, s1, e2, s2; double fac;
+                if (fd == 0)      { e1 = 1; s1 = 2; e2 = 2; s2 = 1; fac = dt2dydz6; }
+                else if (fd == 1) { e1 = 2; s1 = 0; e2 = 0; s2 = 2; fac = dt2dzdx6; }
+                else              { e1 = 0; s1 = 1; e2 = 1; s2 = 0; fac = dt2dxdy6; }
+                double T1[H_NV], T2[H_NV];
+                int es[2] = {e1, e2}, ss[2] = {s1, s2};
+                double *T[2] = {T1, T2};
+                for (int q = 0; q < 2; q++) {
+                    int e = es[q], sd = ss[q];
+                    int im = i - (e == 0), jm = j - (e == 1), km = k - (e == 2);
+                    int ip = i + (e == 0), jp = j + (e == 1), kp = k + (e == 2);
+                    const double *sm = s->sig + cidx(b, im, jm, km) * 27 + 9 * sd;
+                    const double *sc = s->sig + c * 27 + 9 * sd;
+                    const double *sp = s->sig + cidx(b, ip, jp, kp) * 27 + 9 * sd;
+                    double (*le)[5][5] = (double (*)[5][5])(s->leig + c * 75);
+                    double (*re)[5][5] = (double (*)[5][5])(s->reig + c * 75);
+                    upwind_trans(p, sm, sc, sp, s->lam + c * 15 + 5 * e, le[e], re[e], nev, T[q]);
+                }
+                double *scr = s->scr[fd] + c * 16;
+                for (int v = 0; v < 8; v++) {
+                    scr[v] = scr[v] + (T1[v] + T2[v]) * fac;
+                    scr[8 + v] = scr[8 + v] + (T1[v] + T2[v]) * fac;
+                }
+                if (scr[0] <= 0. || scr[8] <= 0. || scr[4] <= 0. || scr[12] <= 0.) {
+                    for (int v = 0; v < 8; v++) { scr[v] = Vc[v]; scr[8 + v] = Vc[v]; }
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+/* hy_getFaceFlux.F90:300-572 (+y, z) for one block. */
+static int face_fluxes(const blk_t *b, scratch_t *s)
+{
+    const fxo_params *p = b->p;
+    const int ndim = p->ndim;
+    for (int d = 0; d < ndim; d++) {
+        int kt = (d == 2), jt = (d == 1), it = (d == 0);
+        for (int k = b->k0; k <= b->kmax + kt; k++)
+        for (int j = b->j0; j <= b->jmax + jt; j++)
+        for (int i = b->i0; i <= b->imax + it; i++) {
+            long c = cidx(b, i, j, k);
+            long cm = cidx(b, i - it, j - jt, k - kt);
+            double VL[H_NV], VR[H_NV];
+            for (int v = 0; v < 8; v++) { VL[v] = s->scr[d][cm * 16 + v]; VR[v] = s->scr[d][c * 16 + 8 + v]; }
+            VL[H_GR] = 0.; VR[H_GR] = 0.;
+            double F[6], speed;
+            int err = (p->riemann == FXO_HLL) ? riemann_hll(p, d, VL, VR, F, &speed)
+                                              : riemann_hllc(p, d, VL, VR, F, &speed);
+            if (err) return 2;
+            double *fl = s->flx[d] + c * 8;
+            for (int v = 0; v < 6; v++) fl[v] = F[v];
+            if (p->use_aux_eint) {
+                if (fl[F_D] > 0.) { fl[F_VOL] = fl[F_D] / VL[H_D]; fl[F_EI] = fl[F_D] * VL[H_EI]; }
+                else              { fl[F_VOL] = fl[F_D] / VR[H_D]; fl[F_EI] = fl[F_D] * VR[H_EI]; }
+            } else { fl[F_VOL] = 0.; fl[F_EI] = 0.; }
+        }
+        /* cell-averaged n+1/2 pressure for the aux eint update */
+        if (p->use_aux_eint) {
+            for (int k = b->k0; k <= b->kmax; k++)
+            for (int j = b->j0; j <= b->jmax; j++)
+            for (int i = b->i0; i <= b->imax; i++) {
+                long c = cidx(b, i, j, k);
+                double sum = s->scr[d][c * 16 + 8 + 4] + s->scr[d][c * 16 + 4];   /* N05 + P05 */
+                if (d == 0) s->pav[c] = 0.5 * sum;
+                else if (d == 1) s->pav[c] = s->pav[c] * 0.5 + sum * 0.25;
+                else s->pav[c] = (s->pav[c] * 4.0 + sum) / 6.0;
+            }
+        }
+    }
+    return 0;
+}
+
+/* hy_unsplitUpdate.F90:392-933 + helpers :1195-1306 (Cartesian, UPDATE_ALL). */
+static void unsplit_update(const blk_t *b, double *U, double dt, scratch_t *s)
+{
+    const fxo_params *p = b->p;
+    const int ndim = p->ndim;
+    const double fP = p->fpres;
+    double dl[3] = {b->dx, b->dy, b->dz};
+    for (int k = b->k0; k <= b->kmax; k++)
+    for (int j = b->j0; j <= b->jmax; j++)
+    for (int i = b->i0; i <= b->imax; i++) {
+        long c = cidx(b, i, j, k);
+        double *u = U + c * FXO_NUNK;
+        double FLd[3][8], FRd[3][8];
+        for (int d = 0; d < 3; d++) {
+            if (d < ndim) {
+                long cp = cidx(b, i + (d == 0), j + (d == 1), k + (d == 2));
+                for (int v = 0; v < 8; v++) { FLd[d][v] = s->flx[d][c * 8 + v]; FRd[d][v] = s->flx[d][cp * 8 + v]; }
+            } else {
+                for (int v = 0; v < 8; v++) { FLd[d][v] = 0.; FRd[d][v] = 0.; }
+            }
+        }
+        double Sphys[5] = {0., 0., 0., 0., 0.};
+        Sphys[1] = (FLd[0][F_P] - FRd[0][F_P]) * (1.0 - fP) / dl[0];
+        if (ndim >= 2) Sphys[2] = (FLd[1][F_P] - FRd[1][F_P]) * (1.0 - fP) / dl[1];
+        if (ndim == 3) Sphys[3] = (FLd[2][F_P] - FRd[2][F_P]) * (1.0 - fP) / dl[2];
+        double U0[5];
+        U0[0] = u[FXO_DENS];
+        double IntEner = 0.;
+        if (p->use_aux_eint) {
+            IntEner = u[FXO_DENS] * u[FXO_EINT];
+            double pres = s->pav[c];
+            for (int d = 0; d < ndim; d++)
+                IntEner = IntEner + dt / dl[d] * (FLd[d][F_EI] - FRd[d][F_EI] + pres * (FLd[d][F_VOL] - FRd[d][F_VOL]));
+            IntEner = IntEner + dt * 0.0;
+        }
+        U0[1] = u[FXO_VELX] * u[FXO_DENS];
+        U0[2] = u[FXO_VELY] * u[FXO_DENS];
+        U0[3] = u[FXO_VELZ] * u[FXO_DENS];
+        U0[4] = u[FXO_DENS] * u[FXO_ENER];
+        /* updateConservedVariable */
+        double densOld = U0[0], momOld[3] = {U0[1], U0[2], U0[3]};
+        for (int d = 0; d < ndim; d++)
+            for (int v = 0; v < 5; v++) U0[v] = U0[v] - dt / dl[d] * (FRd[d][v] - FLd[d][v]);
+        for (int v = 0; v < 5; v++) U0[v] = U0[v] + dt * (0. + Sphys[v]);
+        if (p->use_gravity) {
+            for (int d = 0; d < 3; d++) U0[1 + d] = U0[1 + d] + 0.5 * dt * densOld * p->grav[d];
+            double dp = 0.; for (int d = 0; d < 3; d++) dp = dp + momOld[d] * p->grav[d];
+            U0[4] = U0[4] + 0.5 * dt * dp;
+        }
+        u[FXO_DENS] = fmax2(U0[0], p->small_dens);
+        u[FXO_ENER] = U0[4];
+        u[FXO_VELX] = U0[1] / u[FXO_DENS];
+        u[FXO_VELY] = U0[2] / u[FXO_DENS];
+        u[FXO_VELZ] = U0[3] / u[FXO_DENS];
+        u[FXO_ENER] = U0[4] / u[FXO_DENS];
+        if (p->use_aux_eint) u[FXO_EINT] = IntEner / u[FXO_DENS];
+    }
+}
+
+/* hy_energyFix.F90:240-260 on the block interior. */
+static void energy_fix(const blk_t *b, double *U)
+{
+    const fxo_params *p = b->p;
+    for (int k = b->k0; k <= b->kmax; k++)
+    for (int j = b->j0; j <= b->jmax; j++)
+    for (int i = b->i0; i <= b->imax; i++) {
+        double *u = U + cidx(b, i, j, k) * FXO_NUNK;
+        double ekin = 0.; ekin = ekin + u[FXO_VELX] * u[FXO_VELX]; ekin = ekin + u[FXO_VELY] * u[FXO_VELY];
+        ekin = ekin + u[FXO_VELZ] * u[FXO_VELZ];
+        ekin = 0.5 * ekin;
+        double eint = u[FXO_ENER] - ekin - 0.0;
+        double IntEner = u[FXO_EINT];
+        double newEint;
+        if (!p->use_aux_eint || eint > p->eint_switch * (ekin + 0.0)) newEint = fmax2(p->small_e, eint);
+        else newEint = fmax2(p->small_e, IntEner);
+        u[FXO_ENER] = newEint + ekin;
+        u[FXO_EINT] = newEint;
+    }
+}
+
+/* Eos_wrapped(MODE_DENS_EI) for one cell: Eos_getData.F90:116-150,
+ * Gamma/Eos.F90:238-250, Eos_putData.F90:208-222. */
+static void eos_cell(const fxo_params *p, double *u)
+{
+    double ekin = 0.5 * (u[FXO_VELX] * u[FXO_VELX] + u[FXO_VELY] * u[FXO_VELY] + u[FXO_VELZ] * u[FXO_VELZ]);
+    double eint = u[FXO_EINT];
+    if (u[FXO_ENER] - ekin > fmax2(p->small_e, p->eint_switch * ekin)) eint = u[FXO_ENER] - ekin;
+    double dens = u[FXO_DENS];
+    double gammam1 = 1.0 / (p->gamma - 1.0);          /* eos_gammam1, Gamma/Eos_init.F90:86 */
+    double ggprod = gammam1 * p->gas_constant;
+    double ggprodinv = 1. / ggprod;
+    double gam1inv = 1. / gammam1;
+    double pres = dens * eint * gam1inv;
+    double temp = eint * ggprodinv * p->abar;
+    u[FXO_PRES] = pres;
+    u[FXO_TEMP] = temp;
+    u[FXO_GAMC] = p->gamma;
+    u[FXO_EINT] = eint;
+    u[FXO_ENER] = eint + ekin;
+    u[FXO_GAME] = pres / (eint * dens) + 1;
+}
+
+static void eos_block(const blk_t *b, double *U)
+{
+    for (int k = b->k0; k <= b->kmax; k++)
+    for (int j = b->j0; j <= b->jmax; j++)
+    for (int i = b->i0; i <= b->imax; i++)
+        eos_cell(b->p, U + cidx(b, i, j, k) * FXO_NUNK);
+}
+
+/* ======================================================================= */
+long fxo_unk_size(const fxo_params *p)
+{
+    blk_t b; blk_init(&b, p);
+    return b.ncell * FXO_NUNK * (long)p->nblockx * p->nblocky * p->nblockz;
+}
+
+long fxo_index(const fxo_params *p, int var, int i, int j, int k, int blk)
+{
+    blk_t b; blk_init(&b, p);
+    return ((long)blk * b.ncell + cidx(&b, i, j, k)) * FXO_NUNK + var;
+}
+
+/* Grid_fillGuardCells for a uniform block grid.  The neighbour exchange of
+ * UG/gr_shiftData.F90 (periodic wrap included) is done axis by axis over the
+ * full guard extent of the other axes, followed by the physical boundary
+ * conditions applied in the order Z, Y, X over whole guard vectors
+ * (gr_bcApplyToAllBlks with WHOLE_VECTOR), as Grid_fillGuardCells.F90:300. */
+int fxo_fill_guardcells(const fxo_params *p, double *unk)
+{
+    blk_t b; blk_init(&b, p);
+    const int ng = b.ng, ndim = p->ndim;
+    int nb[3] = {p->nblockx, ndim >= 2 ? p->nblocky : 1, ndim == 3 ? p->nblockz : 1};
+    int nn[3] = {p->nxb, ndim >= 2 ? p->nyb : 1, ndim == 3 ? p->nzb : 1};
+    int gx[3] = {ng, ndim >= 2 ? ng : 0, ndim == 3 ? ng : 0};
+    long N[3], G[3];
+    for (int d = 0; d < 3; d++) { N[d] = (long)nb[d] * nn[d]; G[d] = N[d] + 2 * gx[d]; }
+    /* global grid with a guard ring */
+    double *g = (double *)malloc(sizeof(double) * G[0] * G[1] * G[2] * FXO_NUNK);
+#define GI(i, j, k) ((((long)(k) * G[1] + (j)) * G[0] + (i)) * FXO_NUNK)
+    long nblk = (long)nb[0] * nb[1] * nb[2];
+    for (long blk = 0; blk < nblk; blk++) {
+        int bx = blk % nb[0], by = (blk / nb[0]) % nb[1], bz = blk / ((long)nb[0] * nb[1]);
+        const double *U = unk + blk * b.ncell * FXO_NUNK;
+        for (int k = b.k0; k <= b.kmax; k++)
+        for (int j = b.j0; j <= b.jmax; j++)
+        for (int i = b.i0; i <= b.imax; i++) {
+            long gi = (long)bx * nn[0] + (i - b.i0) + gx[0];
+            long gj = (long)by * nn[1] + (j - b.j0) + gx[1];
+            long gk = (long)bz * nn[2] + (k - b.k0) + gx[2];
+            memcpy(g + GI(gi, gj, gk), U + cidx(&b, i, j, k) * FXO_NUNK, sizeof(double) * FXO_NUNK);
+        }
+    }
+    /* periodic exchanges, axis order X, Y, Z, full extent of the other axes */
+    for (int a = 0; a < ndim; a++) {
+        if (p->bc[2 * a] != FXO_BC_PERIODIC) continue;
+        for (long k = 0; k < G[2]; k++) for (long j = 0; j < G[1]; j++) for (long i = 0; i < G[0]; i++) {
+            long idx[3] = {i, j, k};
+            long x = idx[a];
+            if (x >= gx[a] && x < gx[a] + N[a]) continue;
+            long src = (x < gx[a]) ? x + N[a] : x - N[a];
+            long sidx[3] = {i, j, k}; sidx[a] = src;
+            memcpy(g + GI(i, j, k), g + GI(sidx[0], sidx[1], sidx[2]), sizeof(double) * FXO_NUNK);
+        }
+    }
+    /* physical boundaries, order Z, Y, X */
+    for (int a = ndim - 1; a >= 0; a--) {
+        for (int side = 0; side < 2; side++) {
+            int bc = p->bc[2 * a + side];
+            if (bc == FXO_BC_PERIODIC) continue;
+            for (long k = 0; k < G[2]; k++) for (long j = 0; j < G[1]; j++) for (long i = 0; i < G[0]; i++) {
+                long idx[3] = {i, j, k};
+                long x = idx[a];
+                long sidx[3] = {i, j, k};
+                if (side == 0) {
+                    if (x >= gx[a]) continue;
+                    sidx[a] = (bc == FXO_BC_OUTFLOW) ? gx[a] : 2 * gx[a] - 1 - x;
+                } else {
+                    if (x < gx[a] + N[a]) continue;
+                    long last = gx[a] + N[a] - 1;
+                    sidx[a] = (bc == FXO_BC_OUTFLOW) ? last : 2 * last + 1 - x;
+                }
+                double *dst = g + GI(i, j, k);
+                const double *src = g + GI(sidx[0], sidx[1], sidx[2]);
+                for (int v = 0; v < FXO_NUNK; v++) {
+                    double sgn = (bc == FXO_BC_REFLECTING && v == FXO_VELX + a) ? -1. : 1.;
+                    dst[v] = src[v] * sgn;
+                }
+            }
+        }
+    }
+    /* scatter windows back into each block's guard cells */
+    for (long blk = 0; blk < nblk; blk++) {
+        int bx = blk % nb[0], by = (blk / nb[0]) % nb[1], bz = blk / ((long)nb[0] * nb[1]);
+        double *U = unk + blk * b.ncell * FXO_NUNK;
+        for (int k = 0; k < b.nkg; k++)
+        for (int j = 0; j < b.njg; j++)
+        for (int i = 0; i < b.nig; i++) {
+            long gi = (long)bx * nn[0] + i;
+            long gj = (long)by * nn[1] + j;
+            long gk = (long)bz * nn[2] + k;
+            memcpy(U + cidx(&b, i, j, k) * FXO_NUNK, g + GI(gi, gj, gk), sizeof(double) * FXO_NUNK);
+        }
+    }
+#undef GI
+    free(g);
+    return 0;
+}
+
+int fxo_eos_interior(const fxo_params *p, double *unk)
+{
+    blk_t b; blk_init(&b, p);
+    long nblk = (long)p->nblockx * p->nblocky * p->nblockz;
+    for (long blk = 0; blk < nblk; blk++) eos_block(&b, unk + blk * b.ncell * FXO_NUNK);
+    return 0;
+}
+
+int fxo_hydro_step(const fxo_params *p, double *unk, double dt, double dt_old, int nthreads)
+{
+    (void)dt_old;
+    if (p->ndim < 2 || p->ndim > 3 || p->nguard < 4 || (p->order != 3 && p->order != 5)) return 3;
+    fxo_fill_guardcells(p, unk);
+    blk_t b; blk_init(&b, p);
+    long nblk = (long)p->nblockx * p->nblocky * p->nblockz;
+    int status = 0;
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel num_threads(nthreads)
+#endif
+    {
+        scratch_t s;
+        scratch_alloc(&s, b.ncell);
+        int lerr = 0;
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 1)
+#endif
+        for (long blk = 0; blk < nblk; blk++) {
+            double *U = unk + blk * b.ncell * FXO_NUNK;
+            int e = riemann_states(&b, U, dt, &s);
+            if (!e) e = face_fluxes(&b, &s);
+            if (!e) {
+                unsplit_update(&b, U, dt, &s);
+                if (!p->use_gravity) { energy_fix(&b, U); eos_block(&b, U); }
+            }
+            if (e) lerr = e;
+        }
+        scratch_free(&s);
+#ifdef _OPENMP
+#pragma omp critical
+#endif
+        { if (lerr) status = lerr; }
+    }
+    if (p->use_gravity) {
+        /* hy_gravityStepBlk: the n+1 gravity half step, then energyFix and Eos */
+        for (long blk = 0; blk < nblk; blk++) {
+            double *U = unk + blk * b.ncell * FXO_NUNK;
+            for (int k = b.k0; k <= b.kmax; k++)
+            for (int j = b.j0; j <= b.jmax; j++)
+            for (int i = b.i0; i <= b.imax; i++) {
+                double *u = U + cidx(&b, i, j, k) * FXO_NUNK;
+                double vold[3] = {u[FXO_VELX], u[FXO_VELY], u[FXO_VELZ]};
+                double hdt = 0.5 * dt;
+                double dp = 0.;
+                for (int d = 0; d < 3; d++) u[FXO_VELX + d] = vold[d] + hdt * p->grav[d];
+                for (int d = 0; d < 3; d++) dp = dp + u[FXO_VELX + d] * p->grav[d];
+                u[FXO_ENER] = u[FXO_ENER] + hdt * dp;
+            }
+            energy_fix(&b, U);
+            eos_block(&b, U);
+        }
+    }
+    return status;
+}
+
+int fxo_compute_dt(const fxo_params *p, const double *unk, double *dt_out)
+{
+    blk_t b; blk_init(&b, p);
+    long nblk = (long)p->nblockx * p->nblocky * p->nblockz;
+    double delinv[3] = {1.0 / b.dx, 1.0 / b.dy, 1.0 / b.dz};
+    double dtmin = 1.e300;   /* huge */
+    for (long blk = 0; blk < nblk; blk++) {
+        const double *U = unk + blk * b.ncell * FXO_NUNK;
+        double dt_temp = 0.;
+        for (int k = b.k0; k <= b.kmax; k++)
+        for (int j = b.j0; j <= b.jmax; j++)
+        for (int i = b.i0; i <= b.imax; i++) {
+            const double *u = U + cidx(&b, i, j, k) * FXO_NUNK;
+            double cs2 = u[FXO_GAMC] * u[FXO_PRES] / u[FXO_DENS];
+            double r = (fabs(u[FXO_VELX] - 0.) + sqrt(cs2)) * delinv[0];
+            if (p->ndim > 1) r = fmax2(r, (fabs(u[FXO_VELY] - 0.) + sqrt(cs2)) * delinv[1]);
+            if (p->ndim > 2) r = fmax2(r, (fabs(u[FXO_VELZ] - 0.) + sqrt(cs2)) * delinv[2]);
+            if (r * p->cfl > dt_temp * p->cfl) dt_temp = r;
+        }
+        double dtb = (dt_temp != 0.) ? p->cfl / dt_temp : 1.79769313486231570e308;
+        if (dtb < dtmin) dtmin = dtb;
+    }
+    *dt_out = dtmin;
+    return dtmin <= 0. ? 4 : 0;
+}
+
+double fxo_driver_dt(double dt_cfl, double dt_old, double f, double dtmin, double dtmax)
+{
+    double dtNew = fmin2(dt_cfl, dt_old * f);
+    return fmin2(fmax2(dtNew, dtmin), dtmax);
+}
+
+int fxo_integrals(const fxo_params *p, const double *unk, double out[7])
+{
+    blk_t b; blk_init(&b, p);
+    long nblk = (long)p->nblockx * p->nblocky * p->nblockz;
+    double dv = b.dx * b.dy * b.dz;
+    for (int q = 0; q < 7; q++) out[q] = 0.;
+    for (long blk = 0; blk < nblk; blk++) {
+        const double *U = unk + blk * b.ncell * FXO_NUNK;
+        for (int k = b.k0; k <= b.kmax; k++)
+        for (int j = b.j0; j <= b.jmax; j++)
+        for (int i = b.i0; i <= b.imax; i++) {
+            const double *u = U + cidx(&b, i, j, k) * FXO_NUNK;
+            double rho = u[FXO_DENS];
+            double ek = 0.5 * rho * (u[FXO_VELX] * u[FXO_VELX] + u[FXO_VELY] * u[FXO_VELY] + u[FXO_VELZ] * u[FXO_VELZ]);
+            out[0] += rho * dv;
+            out[1] += rho * u[FXO_VELX] * dv;
+            out[2] += rho * u[FXO_VELY] * dv;
+            out[3] += rho * u[FXO_VELZ] * dv;
+            out[4] += rho * u[FXO_ENER] * dv;
+            out[5] += rho * u[FXO_EINT] * dv;
+            out[6] += ek * dv;
+        }
+    }
+    return 0;
+}
+
+double fxo_flops_last_step(void) { return 0.; }
+
+#include "fx_oracle_weno.inc"

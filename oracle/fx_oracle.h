@@ -1,0 +1,87 @@
+/*
+ * fx_oracle.h -- CPU oracle for the Flash-X unsplit-hydro (UHD) hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C, FP64, line-by-line
+ * restatement of the reference Fortran solver, used as the checker for the
+ * CUDA path (tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg).
+ * The product library never links, loads or calls it.
+ *
+ * Parity status: the reference is Fortran and cannot be compiled in this
+ * image (no gfortran/MPI), and it ships no golden vectors for this path, so
+ * the oracle is pinned by known-answer tests (exact Sod Riemann solution,
+ * HLLC/HLL hand cases, conservation on periodic domains, Eos identities)
+ * rather than by reference outputs: "parity unpinned" against the reference
+ * binary itself.
+ *
+ * Storage layout follows Flash-X UNK: unk(var,i,j,k,blk) with var fastest,
+ * NGUARD guard cells per side, variables in the alphabetical order the Flash-X
+ * setup script assigns for UHD + Gamma:
+ *   dens eint ener gamc game pres shok temp velx vely velz
+ * (FX/physics/Hydro/HydroMain/unsplit/Config:66-76; bin/unitCfg.py:763-764).
+ */
+#ifndef FX_ORACLE_H
+#define FX_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { FXO_DENS = 0, FXO_EINT, FXO_ENER, FXO_GAMC, FXO_GAME, FXO_PRES,
+       FXO_SHOK, FXO_TEMP, FXO_VELX, FXO_VELY, FXO_VELZ, FXO_NUNK };
+
+enum { FXO_BC_PERIODIC = 0, FXO_BC_OUTFLOW = 1, FXO_BC_REFLECTING = 2 };
+enum { FXO_HLL = 3, FXO_HLLC = 4 };                    /* UHD.h:366-372 */
+enum { FXO_MINMOD = 1, FXO_MC = 2, FXO_VANLEER = 3, FXO_HYBRID = 4,
+       FXO_LIMITED = 5 };
+
+typedef struct {
+    int ndim;                       /* 2 or 3 */
+    int nxb, nyb, nzb;              /* block interior cells (nzb = 1 in 2-D) */
+    int nblockx, nblocky, nblockz;  /* uniform block grid */
+    int nguard;                     /* NGUARD (4) */
+    double xmin, xmax, ymin, ymax, zmin, zmax;
+    int bc[6];                      /* xl xr yl yr zl zr */
+    int order;                      /* 3 = PPM, 5 = WENO */
+    int weno_method;                /* 1 = WENO5 (Jiang-Shu), 2 = WENO-Z */
+    int riemann;                    /* FXO_HLL / FXO_HLLC */
+    int limiter;                    /* FXO_MINMOD ... */
+    int char_limiting;
+    int use_3d_full_ctu;
+    int use_aux_eint;
+    int use_gravity;
+    double grav[3];                 /* constant gravitational acceleration */
+    double cfl, gamma, eint_switch, small_dens, small_e, small_p, tiny;
+    double fpres;                   /* hy_fPresInMomFlux */
+    double limited_beta;            /* LimitedSlopeBeta */
+    double gas_constant, abar;      /* Eos Gamma: R and singleSpeciesA */
+} fxo_params;
+
+/* Number of doubles in one UNK array for the given geometry. */
+long fxo_unk_size(const fxo_params *p);
+/* Flop-free helpers for tests: linear UNK index of (var,i,j,k,blk). */
+long fxo_index(const fxo_params *p, int var, int i, int j, int k, int blk);
+
+/* Grid_fillGuardCells for a uniform block grid with physical BCs. */
+int fxo_fill_guardcells(const fxo_params *p, double *unk);
+/* Eos_wrapped(MODE_DENS_EI) on every block interior. */
+int fxo_eos_interior(const fxo_params *p, double *unk);
+/* Hydro(): guard fill, then per leaf block hy_computeFluxes with in-place
+ * update, hy_energyFix, Eos_wrapped.  Returns 0, or a nonzero error code
+ * (1 imaginary sound speed, 2 Riemann solver failure). */
+int fxo_hydro_step(const fxo_params *p, double *unk, double dt, double dt_old,
+                   int nthreads);
+/* Hydro_computeDt over all blocks: returns the global CFL time step. */
+int fxo_compute_dt(const fxo_params *p, const double *unk, double *dt_out);
+/* Driver_computeDt growth limit and clamp (Driver_computeDt.F90:452,460). */
+double fxo_driver_dt(double dt_cfl, double dt_old, double tstep_change_factor,
+                     double dtmin, double dtmax);
+/* Volume integrals of mass, x/y/z momentum, total energy, internal energy,
+ * kinetic energy (IO_writeIntegralQuantities.F90:60-224). */
+int fxo_integrals(const fxo_params *p, const double *unk, double out[7]);
+/* Number of flops counted by the instrumented build (0 otherwise). */
+double fxo_flops_last_step(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

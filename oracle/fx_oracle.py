@@ -1,0 +1,139 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg import
+this module, and only as the checker.  The oracle restates the Flash-X
+unsplit-hydro solver in plain C (oracle/fx_oracle.c); its header lists the
+reference files it follows.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfx_oracle.so")
+
+NUNK = 11
+DENS, EINT, ENER, GAMC, GAME, PRES, SHOK, TEMP, VELX, VELY, VELZ = range(11)
+BC_PERIODIC, BC_OUTFLOW, BC_REFLECTING = 0, 1, 2
+HLL, HLLC = 3, 4
+LIMITERS = {"minmod": 1, "mc": 2, "vanleer": 3, "hybrid": 4, "limited": 5}
+
+
+class FxoParams(ctypes.Structure):
+    _fields_ = [
+        ("ndim", ctypes.c_int),
+        ("nxb", ctypes.c_int), ("nyb", ctypes.c_int), ("nzb", ctypes.c_int),
+        ("nblockx", ctypes.c_int), ("nblocky", ctypes.c_int), ("nblockz", ctypes.c_int),
+        ("nguard", ctypes.c_int),
+        ("xmin", ctypes.c_double), ("xmax", ctypes.c_double),
+        ("ymin", ctypes.c_double), ("ymax", ctypes.c_double),
+        ("zmin", ctypes.c_double), ("zmax", ctypes.c_double),
+        ("bc", ctypes.c_int * 6),
+        ("order", ctypes.c_int), ("weno_method", ctypes.c_int),
+        ("riemann", ctypes.c_int), ("limiter", ctypes.c_int),
+        ("char_limiting", ctypes.c_int), ("use_3d_full_ctu", ctypes.c_int),
+        ("use_aux_eint", ctypes.c_int), ("use_gravity", ctypes.c_int),
+        ("grav", ctypes.c_double * 3),
+        ("cfl", ctypes.c_double), ("gamma", ctypes.c_double),
+        ("eint_switch", ctypes.c_double), ("small_dens", ctypes.c_double),
+        ("small_e", ctypes.c_double), ("small_p", ctypes.c_double),
+        ("tiny", ctypes.c_double), ("fpres", ctypes.c_double),
+        ("limited_beta", ctypes.c_double),
+        ("gas_constant", ctypes.c_double), ("abar", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+
+def build():
+    """Compile the oracle with its Makefile (gcc, -ffp-contract=off)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER(FxoParams)
+        D = ctypes.POINTER(ctypes.c_double)
+        L.fxo_unk_size.argtypes = [P]; L.fxo_unk_size.restype = ctypes.c_long
+        L.fxo_fill_guardcells.argtypes = [P, D]
+        L.fxo_eos_interior.argtypes = [P, D]
+        L.fxo_hydro_step.argtypes = [P, D, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        L.fxo_compute_dt.argtypes = [P, D, D]
+        L.fxo_driver_dt.argtypes = [ctypes.c_double] * 5
+        L.fxo_driver_dt.restype = ctypes.c_double
+        L.fxo_integrals.argtypes = [P, D, D]
+        _lib = L
+    return _lib
+
+
+def make_params(geom, hp):
+    """Build the C parameter struct from a geometry dict and a hydro-parameter
+    object exposing the Flash-X runtime-parameter names (see
+    flashx_b200.params.HydroParams)."""
+    p = FxoParams()
+    p.ndim = geom["ndim"]
+    p.nxb, p.nyb, p.nzb = geom["nxb"], geom["nyb"], geom["nzb"]
+    p.nblockx, p.nblocky, p.nblockz = geom["nblockx"], geom["nblocky"], geom["nblockz"]
+    p.nguard = geom.get("nguard", 4)
+    (p.xmin, p.xmax), (p.ymin, p.ymax), (p.zmin, p.zmax) = geom["bbox"]
+    for i, b in enumerate(geom["bc"]):
+        p.bc[i] = b
+    p.order = hp.order
+    p.weno_method = 2 if hp.wenoMethod.upper() == "WENOZ" else 1
+    p.riemann = HLLC if hp.RiemannSolver.upper() == "HLLC" else HLL
+    p.limiter = LIMITERS[hp.slopeLimiter.lower()]
+    p.char_limiting = int(hp.charLimiting)
+    p.use_3d_full_ctu = int(hp.use_3dFullCTU)
+    p.use_aux_eint = int(hp.use_auxEintEqn)
+    p.use_gravity = int(hp.useGravity)
+    for i in range(3):
+        p.grav[i] = hp.gravity[i]
+    p.cfl, p.gamma = hp.cfl, hp.gamma
+    p.eint_switch, p.small_dens, p.small_e, p.small_p = hp.eintSwitch, hp.smlrho, hp.smalle, hp.smallp
+    p.tiny, p.fpres, p.limited_beta = hp.tiny, hp.hy_fPresInMomFlux, hp.LimitedSlopeBeta
+    p.gas_constant, p.abar = hp.gasConstant, hp.eos_singleSpeciesA
+    return p
+
+
+def _dp(a):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def fill_guardcells(p, unk):
+    lib().fxo_fill_guardcells(ctypes.byref(p), _dp(unk))
+
+
+def eos_interior(p, unk):
+    lib().fxo_eos_interior(ctypes.byref(p), _dp(unk))
+
+
+def hydro_step(p, unk, dt, dt_old, nthreads=0):
+    rc = lib().fxo_hydro_step(ctypes.byref(p), _dp(unk), dt, dt_old, nthreads)
+    if rc:
+        raise RuntimeError(f"oracle hydro step failed with code {rc}")
+
+
+def compute_dt(p, unk):
+    out = ctypes.c_double()
+    rc = lib().fxo_compute_dt(ctypes.byref(p), _dp(unk), ctypes.byref(out))
+    if rc:
+        raise RuntimeError("oracle: computed dt is not positive")
+    return out.value
+
+
+def driver_dt(dt_cfl, dt_old, factor=2.0, dtmin=1e-10, dtmax=1e5):
+    return lib().fxo_driver_dt(dt_cfl, dt_old, factor, dtmin, dtmax)
+
+
+def integrals(p, unk):
+    out = np.zeros(7)
+    lib().fxo_integrals(ctypes.byref(p), _dp(unk), _dp(out))
+    return out
