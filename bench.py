@@ -1,0 +1,338 @@
+#!/usr/bin/env python
+"""Benchmark: zone-updates/s of the unsplit hydro step on B200.
+
+Workload (N=1 per GPU): 2-D Kelvin-Helmholtz, 2048^2 cells as 128x128 blocks
+of 16^2, periodic, PPM + HLLC, CFL 0.8 (the benchmark's second configuration;
+seeded synthetic initial state from flashx_b200.simulations).  A step is one
+Hydro() call over the whole grid plus Driver_computeDt: guard resolution,
+reconstruction, Riemann solve, conserved update, energyFix, Eos and the CFL
+reduction.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` is the plain FP64 path (bit-identical
+to the oracle); the FP32-reconstruction/FP64-update path is reported under
+`mixed` with its L1 density error against the FP64 result.  State arrays
+(2 x 10 x 4.2M FP64 = 671 MB) exceed the 126 MB L2, so no flush is needed.
+"""
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "flash-x_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "zone-updates/s FP64 vs FP32+FP64-update at stated L1 err; % HBM roofline"
+UNIT = "zone-updates/s"
+BYTES_PER_ZONE = 152   # 9 FP64 reads + 10 FP64 writes per zone-update (algorithmic)
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "hydro2d_kh2048_traffic.json")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="kh2d")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            m = json.load(f)
+        return m.get("hbm_gbs", 6650.0), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.tmp = None
+
+    def start(self):
+        try:
+            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.tmp.flush()
+        self.tmp.seek(0)
+        rows = [r for r in csv.reader(io.StringIO(self.tmp.read())) if len(r) >= 9]
+        os.unlink(self.tmp.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args, backend):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+        return dist, world, rank, local
+    return None, 1, 0, local
+
+
+def cpu_baseline_run(name, seconds=10.0, scale=1 / 4):
+    """The oracle (OpenMP over blocks, all host cores) on a bounded sample of
+    the workload: the same problem at reduced resolution, as many steps as fit
+    in `seconds`."""
+    from flashx_b200 import simulations as S
+    from oracle import fx_oracle as O
+    geom, hp, init = S.config(name, scale=scale)
+    unk = init(geom, hp)
+    p = O.make_params(geom.as_dict(), hp)
+    dt = 0.5 * O.compute_dt(p, unk)
+    O.hydro_step(p, unk, dt, dt)          # warm-up (thread pool, page-in)
+    n, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        O.hydro_step(p, unk, dt, dt)
+        dt = O.driver_dt(O.compute_dt(p, unk), dt)
+        n += 1
+    el = time.perf_counter() - t0
+    cores = os.cpu_count()
+    nx = geom.nxb * geom.nblockx
+    return {"value": geom.ncells * n / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{name} {nx}^{geom.ndim} ({geom.ncells} zones), {n} steps in {el:.1f} s, "
+                      f"OpenMP over blocks on {cores} threads"}
+
+
+def run_reference(args):
+    dist, world, rank, _ = dist_setup(args, "gloo")
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    from flashx_b200 import simulations as S
+    from oracle import fx_oracle as O
+    geom, hp, init = S.config(args.config, scale=1 / 2)
+    unk = init(geom, hp)
+    p = O.make_params(geom.as_dict(), hp)
+    dt = 0.5 * O.compute_dt(p, unk)
+    for _ in range(args.warmup):
+        O.hydro_step(p, unk, dt, dt)
+        dt = O.driver_dt(O.compute_dt(p, unk), dt)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.hydro_step(p, unk, dt, dt)
+        dt = O.driver_dt(O.compute_dt(p, unk), dt)
+    el = time.perf_counter() - t0
+    v = geom.ncells * args.steps / el
+    nx = geom.nxb * geom.nblockx
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "kh2d 2048^2 PPM+HLLC, sampled at %d^2 per step" % nx},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                             "sample": f"oracle restatement of the Flash-X unsplit solver (the Fortran reference "
+                                       f"cannot be built here), {nx}^2 KH per step, OpenMP on {os.cpu_count()} threads"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_ours(args):
+    import torch
+    dist, world, rank, local = dist_setup(args, "nccl")
+    torch.cuda.set_device(local)
+    from flashx_b200 import simulations as S
+    from flashx_b200.hydro import HydroDevice, driver_dt
+
+    geom, hp, init = S.config(args.config)
+    unk0 = init(geom, hp)
+    ncell = geom.ncells
+    K, W = args.steps, args.warmup
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def global_min(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        return float(t.item())
+
+    def timed_run(precision):
+        dev = HydroDevice(geom, hp, precision)
+        dev.attach_unk(unk0.copy())
+        dt = global_min(0.5 * dev.Hydro_computeDt())
+        ext = torch.cuda.ExternalStream(dev.lib.fxb_stream())
+        if world == 1:
+            dt, dt_old = dev.advance(W, dt, dt)
+            barrier()
+            clk = Clocks(local); clk.start()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            dt, dt_old = dev.advance(K, dt, dt_old)
+            e1.record(ext)
+            barrier()
+            clocks = clk.stop()
+            ms = e0.elapsed_time(e1)
+            launches = 2 * K
+        else:
+            dt_old = dt
+            for _ in range(W):
+                dev.Hydro(0.0, dt, dt_old)
+                dt_old, dt = dt, driver_dt(global_min(dev.Hydro_computeDt()), dt, hp)
+            barrier()
+            clk = Clocks(local); clk.start()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            for _ in range(K):
+                dev.Hydro(0.0, dt, dt_old)
+                dt_old, dt = dt, driver_dt(global_min(dev.Hydro_computeDt()), dt, hp)
+            e1.record(ext)
+            barrier()
+            clocks = clk.stop()
+            ms = e0.elapsed_time(e1)
+            launches = K
+        ms = max_over_ranks(ms)
+        return dev, ms, launches, clocks
+
+    # ---- FP64 (headline)
+    dev, ms, launches, clocks = timed_run("fp64")
+    value = world * ncell * K / (ms / 1e3)
+    # kernel-only timing of the fused hydro kernel for the roofline
+    kms = []
+    dt = 0.5 * dev.Hydro_computeDt()
+    for _ in range(min(K, 10)):
+        dev.Hydro(0.0, dt, dt)
+        kms.append(dev.last_timing()[0])
+    dev.Hydro_computeDt()
+    kernel_ms = statistics.mean(kms)
+    fp64_state = np.zeros(geom.unk_shape)
+    # e2e: host-driven loop through the C ABI, dt crossing PCIe every step
+    dev.attach_unk(unk0.copy())
+    dt = dt_old = 0.5 * dev.Hydro_computeDt()
+    barrier()
+    t0 = time.perf_counter()
+    t_sim = 0.0
+    for _ in range(K):
+        dev.Hydro(t_sim + dt, dt, dt_old)
+        t_sim += dt
+        dt_old, dt = dt, driver_dt(global_min(dev.Hydro_computeDt()), dt, hp)
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = world * ncell * K / e2e_s
+    dev.sync_to_host(fp64_state)
+    ref_after = S.gather_global(geom, fp64_state)
+
+    peak, peak_kind = measured_peaks()
+    achieved = BYTES_PER_ZONE * ncell / (kernel_ms / 1e3) / 1e9
+    traffic = None
+    try:
+        with open(TRAFFIC_FILE) as f:
+            traffic = json.load(f).get("bytes_per_launch")
+    except Exception:
+        pass
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded Philox4x32-10 KH initial state)",
+            "config": {"workload": "kh2d: 2-D Kelvin-Helmholtz 2048^2 (128x128 blocks of 16^2), periodic, "
+                                   "PPM+HLLC, mc/char limiting, CFL 0.8, gamma 1.4",
+                       "zones_per_gpu": ncell, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (671 MB state vs 126 MB L2)",
+                       "timing": "CUDA events on the library stream, device dt loop (CUDA graph)"},
+            "clocks": clocks,
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "hydro2d_kernel<double>", "kernel_ms": kernel_ms,
+                         "algorithmic_bytes_per_zone": BYTES_PER_ZONE},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24, "d2h_bytes_per_step": 8,
+                    "note": "host loop via fxb_hydro_step/fxb_compute_dt: (t, dt, dtOld) in, dt out per step; "
+                            "UNK stays resident on the device"}}
+    dev.close()
+
+    # ---- mixed precision
+    if not args.no_mixed:
+        mdev, mms, mlaunch, mclk = timed_run("mixed")
+        mstate = np.zeros(geom.unk_shape)
+        # same steps as the FP64 e2e run for the error estimate
+        mdev.attach_unk(unk0.copy())
+        dt = dt_old = 0.5 * mdev.Hydro_computeDt()
+        for _ in range(K):
+            mdev.Hydro(0.0, dt, dt_old)
+            dt_old, dt = dt, driver_dt(global_min(mdev.Hydro_computeDt()), dt, hp)
+        mdev.sync_to_host(mstate)
+        m_after = S.gather_global(geom, mstate)
+        mdev.close()
+        l1 = {v: float(np.mean(np.abs(m_after[..., i] - ref_after[..., i])) / max(np.mean(np.abs(ref_after[..., i])), 1e-300))
+              for v, i in (("dens", 0), ("pres", 5), ("velx", 8), ("vely", 9))}
+        line["mixed"] = {"value": world * ncell * K / (mms / 1e3), "ms_per_step": mms / K,
+                         "speedup_vs_fp64": ms / mms, "l1_rel_vs_fp64_after_steps": l1,
+                         "dtype": "f32 reconstruction/Riemann + f64 update", "clocks": mclk}
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_run(args.config)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

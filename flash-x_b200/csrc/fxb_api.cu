@@ -1,0 +1,590 @@
+// fxb_api.cu -- extern "C" entry points of libflashx_b200.so (see
+// include/flashx_b200.h for the contract and the reference interfaces each
+// one replaces).  Host code only orchestrates: device memory, the library
+// stream, kernel launches, CUDA graphs and error reporting.
+#include "../../include/flashx_b200.h"
+#include "fxb_launch.h"
+
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+#include <math.h>
+
+using namespace fxb;
+
+namespace {
+
+struct Lib {
+    bool inited = false;
+    fxb_params prm{};
+    fxb_domain dom{};
+    DevParams dprm{};
+    int dmap[NV_DEV];              // device variable -> UNK slot
+    int nunk = 0;
+    int nx = 0, ny = 1, nz = 1;
+    long ncell = 0, vstride = 0;
+    long unk_doubles = 0;
+    double *buf[2] = {nullptr, nullptr};
+    int cur = 0;
+    double *unk_dev = nullptr;     // UNK staging mirror (blocks with guard cells)
+    int *bcoord = nullptr;         // 3 ints per block
+    int *dmap_dev = nullptr;
+    int nblk = 0;
+    double *dtv = nullptr;         // [dt, dtOld]
+    unsigned long long *rate_max = nullptr;
+    int *err = nullptr;
+    double *partials = nullptr;
+    int npartials = 0;
+    bool rate_valid = false;
+    bool attached = false;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int last_launches = 0;
+    bool timing_valid = false;
+    cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};   // two steps starting from buffer 0 / 1
+    double gam1inv = 0., ggprodinv = 0.;
+    fxb_error lasterr{};
+};
+Lib L;
+
+int fail(int code, const char *msg)
+{
+    L.lasterr.code = code;
+    snprintf(L.lasterr.message, sizeof(L.lasterr.message), "%s", msg);
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *where)
+{
+    char buf[256];
+    snprintf(buf, sizeof(buf), "%s: %s", where, cudaGetErrorString(e));
+    return fail(FXB_ECUDA, buf);
+}
+
+#define CK(call)                                                    \
+    do {                                                            \
+        cudaError_t _e = (call);                                    \
+        if (_e != cudaSuccess) return cuda_fail(_e, #call);         \
+    } while (0)
+
+// device variable order -> fxb_var
+const int kDevToVar[NV_DEV] = {FXB_DENS, FXB_VELX, FXB_VELY, FXB_VELZ, FXB_PRES,
+                               FXB_GAMC, FXB_GAME, FXB_EINT, FXB_ENER, FXB_TEMP};
+
+// ------------------------------------------------------------------ kernels
+struct UnkGeom {
+    int ndim, nxb, nyb, nzb, ng, nig, njg, nkg, nunk;
+    int nx, ny, nz;
+    int bc[6];
+    long vstride;
+};
+
+__global__ void unk_to_state_kernel(const double *__restrict__ unk, double *__restrict__ st, UnkGeom g,
+                                    const int *__restrict__ bcoord, const int *__restrict__ dmap, int nblk)
+{
+    long n = (long)nblk * g.nxb * g.nyb * g.nzb;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
+        long per = (long)g.nxb * g.nyb * g.nzb;
+        int blk = (int)(idx / per);
+        long r = idx - blk * per;
+        int k = (int)(r / ((long)g.nxb * g.nyb)); r -= (long)k * g.nxb * g.nyb;
+        int j = (int)(r / g.nxb), i = (int)(r - (long)j * g.nxb);
+        int gj = g.ndim >= 2 ? g.ng : 0, gk = g.ndim == 3 ? g.ng : 0;
+        long u = ((((long)blk * g.nkg + k + gk) * g.njg + j + gj) * g.nig + i + g.ng) * g.nunk;
+        long gx = (long)bcoord[3 * blk] * g.nxb + i;
+        long gy = (long)bcoord[3 * blk + 1] * g.nyb + j;
+        long gz = (long)bcoord[3 * blk + 2] * g.nzb + k;
+        long c = (gz * g.ny + gy) * g.nx + gx;
+        for (int v = 0; v < NV_DEV; v++) st[v * g.vstride + c] = unk[u + dmap[v]];
+    }
+}
+
+__global__ void state_to_unk_kernel(const double *__restrict__ st, double *__restrict__ unk, UnkGeom g,
+                                    const int *__restrict__ bcoord, const int *__restrict__ dmap, int nblk)
+{
+    long per = (long)g.nig * g.njg * g.nkg;
+    long n = (long)nblk * per;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
+        int blk = (int)(idx / per);
+        long r = idx - blk * per;
+        int k = (int)(r / ((long)g.nig * g.njg)); r -= (long)k * g.nig * g.njg;
+        int j = (int)(r / g.nig), i = (int)(r - (long)j * g.nig);
+        int gj = g.ndim >= 2 ? g.ng : 0, gk = g.ndim == 3 ? g.ng : 0;
+        double sx = 1.0, sy = 1.0, sz = 1.0;
+        int mx = map_axis(bcoord[3 * blk] * g.nxb + i - g.ng, g.nx, g.bc[0], g.bc[1], &sx);
+        int my = g.ndim >= 2 ? map_axis(bcoord[3 * blk + 1] * g.nyb + j - gj, g.ny, g.bc[2], g.bc[3], &sy) : 0;
+        int mz = g.ndim == 3 ? map_axis(bcoord[3 * blk + 2] * g.nzb + k - gk, g.nz, g.bc[4], g.bc[5], &sz) : 0;
+        long c = ((long)mz * g.ny + my) * g.nx + mx;
+        long u = idx * g.nunk;
+        for (int v = 0; v < NV_DEV; v++) {
+            double val = st[v * g.vstride + c];
+            if (v == VX) val = val * sx;
+            if (v == VY) val = val * sy;
+            if (v == VZ) val = val * sz;
+            unk[u + dmap[v]] = val;
+        }
+    }
+}
+
+// Eos_wrapped(MODE_DENS_EI) on every interior cell of the device mirror
+__global__ void eos_kernel(double *st, long vstride, long ncell, DevParams prm, double gam1inv, double ggprodinv)
+{
+    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < ncell; c += (long)gridDim.x * blockDim.x) {
+        double dens = st[D * vstride + c];
+        double vx = st[VX * vstride + c], vy = st[VY * vstride + c], vz = st[VZ * vstride + c];
+        double ener = st[DV_ENER * vstride + c], eint = st[EI * vstride + c];
+        double ekin = 0.5 * (vx * vx + vy * vy + vz * vz);
+        if (ener - ekin > fmax2(prm.small_e, prm.eint_switch * ekin)) eint = ener - ekin;
+        double pres = dens * eint * gam1inv;
+        st[P * vstride + c] = pres;
+        st[DV_TEMP * vstride + c] = eint * ggprodinv * prm.abar;
+        st[GC * vstride + c] = prm.gamma;
+        st[EI * vstride + c] = eint;
+        st[DV_ENER * vstride + c] = eint + ekin;
+        st[GE * vstride + c] = pres / (eint * dens) + 1;
+    }
+}
+
+// Hydro_computeDt rate over a state (used when no fused step produced it)
+__global__ void rate_kernel(const double *st, long vstride, int nx, int ny, int nz, int ndim,
+                            double dx, double dy, double dz, unsigned long long *rate_max)
+{
+    long ncell = (long)nx * ny * nz;
+    double r = 0.;
+    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < ncell; c += (long)gridDim.x * blockDim.x) {
+        double dens = st[D * vstride + c], pres = st[P * vstride + c], gamc = st[GC * vstride + c];
+        double cs = sqrt(gamc * pres / dens);
+        double t = (fabs(st[VX * vstride + c] - 0.) + cs) * (1.0 / dx);
+        if (ndim > 1) t = fmax2(t, (fabs(st[VY * vstride + c] - 0.) + cs) * (1.0 / dy));
+        if (ndim > 2) t = fmax2(t, (fabs(st[VZ * vstride + c] - 0.) + cs) * (1.0 / dz));
+        r = fmax2(r, t);
+    }
+    for (int off = 16; off > 0; off >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, off));
+    if ((threadIdx.x & 31) == 0) atomicMax(rate_max, (unsigned long long)__double_as_longlong(r));
+}
+
+// Driver_computeDt on the device: dtNew = min(cfl/rate, f*dtOld), clamp.
+__global__ void dt_finalize_kernel(double *dtv, unsigned long long *rate_max, double cfl, double f,
+                                   double dtmin, double dtmax, int *err)
+{
+    double r = __longlong_as_double((long long)*rate_max);
+    double dtcfl = (r != 0.) ? cfl / r : 1.79769313486231570e308;
+    if (!(dtcfl > 0.)) atomicOr(err, 8);
+    double dtold = dtv[0];
+    double dtnew = fmin2(dtcfl, dtold * f);
+    dtnew = fmin2(fmax2(dtnew, dtmin), dtmax);
+    dtv[1] = dtold;
+    dtv[0] = dtnew;
+    *rate_max = 0ull;
+}
+
+// volume integrals: per-CTA partial sums in a fixed order (deterministic)
+__global__ void integrals_kernel(const double *st, long vstride, long ncell, double dv, double *partials)
+{
+    double s[7] = {0., 0., 0., 0., 0., 0., 0.};
+    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < ncell; c += (long)gridDim.x * blockDim.x) {
+        double rho = st[D * vstride + c];
+        double vx = st[VX * vstride + c], vy = st[VY * vstride + c], vz = st[VZ * vstride + c];
+        s[0] += rho * dv; s[1] += rho * vx * dv; s[2] += rho * vy * dv; s[3] += rho * vz * dv;
+        s[4] += rho * st[DV_ENER * vstride + c] * dv; s[5] += rho * st[EI * vstride + c] * dv;
+        s[6] += 0.5 * rho * (vx * vx + vy * vy + vz * vz) * dv;
+    }
+    __shared__ double sh[7][256];
+    for (int q = 0; q < 7; q++) sh[q][threadIdx.x] = s[q];
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int q = 0; q < 7; q++) sh[q][threadIdx.x] += sh[q][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 7; q++) partials[blockIdx.x * 7 + q] = sh[q][0];
+}
+
+__global__ void integrals_final_kernel(const double *partials, int n, double *out)
+{
+    if (threadIdx.x < 7) {
+        double t = 0.;
+        for (int b = 0; b < n; b++) t += partials[b * 7 + threadIdx.x];
+        out[threadIdx.x] = t;
+    }
+}
+
+UnkGeom unk_geom()
+{
+    UnkGeom g;
+    g.ndim = L.dom.ndim; g.nxb = L.dom.nxb; g.nyb = L.dom.nyb; g.nzb = L.dom.nzb; g.ng = L.dom.nguard;
+    g.nig = g.nxb + 2 * g.ng;
+    g.njg = g.ndim >= 2 ? g.nyb + 2 * g.ng : 1;
+    g.nkg = g.ndim == 3 ? g.nzb + 2 * g.ng : 1;
+    g.nunk = L.nunk;
+    g.nx = L.nx; g.ny = L.ny; g.nz = L.nz;
+    for (int i = 0; i < 6; i++) g.bc[i] = L.dom.bc[i];
+    g.vstride = L.vstride;
+    return g;
+}
+
+double cell_dx(int a)
+{
+    int n = a == 0 ? L.nx : (a == 1 ? L.ny : L.nz);
+    if (a >= L.dom.ndim) return 1.0;
+    return (L.dom.bbox[a][1] - L.dom.bbox[a][0]) / (double)n;
+}
+
+
+// launch one fused hydro step reading buffer `src`, writing 1-src
+int launch_hydro(int src, const double *dtv, double dt)
+{
+    if (L.dom.ndim == 2) {
+        Args2D a;
+        a.in = L.buf[src]; a.out = L.buf[1 - src]; a.vstride = L.vstride;
+        a.nx = L.nx; a.ny = L.ny;
+        for (int i = 0; i < 4; i++) a.bc[i] = L.dom.bc[i];
+        a.dx = cell_dx(0); a.dy = cell_dx(1);
+        a.dt_arg = dt; a.dtv = dtv;
+        a.gam1inv = L.gam1inv; a.ggprodinv = L.ggprodinv;
+        a.prm = L.dprm; a.rate_max = L.rate_max; a.err = L.err;
+        dim3 grid(L.nx / T2, L.ny / T2);
+        if (L.prm.precision == FXB_MIXED) launch_hydro2d_mixed(a, grid, L.stream);
+        else launch_hydro2d_fp64(a, grid, L.stream);
+    } else {
+        Args3D a;
+        a.in = L.buf[src]; a.out = L.buf[1 - src]; a.vstride = L.vstride;
+        a.nx = L.nx; a.ny = L.ny; a.nz = L.nz;
+        for (int i = 0; i < 6; i++) a.bc[i] = L.dom.bc[i];
+        a.dx = cell_dx(0); a.dy = cell_dx(1); a.dz = cell_dx(2);
+        a.dt_arg = dt; a.dtv = dtv;
+        a.gam1inv = L.gam1inv; a.ggprodinv = L.ggprodinv;
+        a.prm = L.dprm; a.rate_max = L.rate_max; a.err = L.err;
+        if (L.prm.precision == FXB_MIXED) launch_hydro3d_mixed(a, L.stream);
+        else launch_hydro3d_fp64(a, L.stream);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "hydro kernel launch");
+    return FXB_OK;
+}
+
+int check_err_word()
+{
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, L.err, sizeof(int), cudaMemcpyDeviceToHost, L.stream));
+    CK(cudaStreamSynchronize(L.stream));
+    if (h) {
+        CK(cudaMemsetAsync(L.err, 0, sizeof(int), L.stream));
+        if (h & ERR_SOUND)
+            return fail(FXB_ESOUND, "[hy_eigenParameters]: Zero or imaginary sound speed has obtained!");
+        if (h & ERR_RIEMANN) return fail(FXB_ERIEMANN, "[hy_getFaceFlux]: Riemann solver returned ierr /= 0");
+        if (h & 8) return fail(FXB_EDT, "[Hydro]: Computed dt is not positive! Aborting!");
+        return fail(FXB_ECUDA, "device error word set");
+    }
+    return FXB_OK;
+}
+
+void free_all()
+{
+    for (int i = 0; i < 2; i++) {
+        if (L.graph_exec[i]) cudaGraphExecDestroy(L.graph_exec[i]);
+        L.graph_exec[i] = nullptr;
+        if (L.buf[i]) cudaFree(L.buf[i]);
+        L.buf[i] = nullptr;
+    }
+    if (L.unk_dev) cudaFree(L.unk_dev);
+    if (L.bcoord) cudaFree(L.bcoord);
+    if (L.dmap_dev) cudaFree(L.dmap_dev);
+    if (L.dtv) cudaFree(L.dtv);
+    if (L.rate_max) cudaFree(L.rate_max);
+    if (L.err) cudaFree(L.err);
+    if (L.partials) cudaFree(L.partials);
+    if (L.ev0) cudaEventDestroy(L.ev0);
+    if (L.ev1) cudaEventDestroy(L.ev1);
+    if (L.stream) cudaStreamDestroy(L.stream);
+    fxb_error keep = L.lasterr;
+    L = Lib();
+    L.lasterr = keep;
+}
+
+} // namespace
+
+// ====================================================================== ABI
+extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, const int32_t *var_map, int nunk)
+{
+    if (!params || !domain || !var_map) return fail(FXB_EARG, "fxb_init: null argument");
+    if (L.inited) free_all();
+    const fxb_domain &d = *domain;
+    const fxb_params &p = *params;
+    if (d.ndim != 2 && d.ndim != 3) return fail(FXB_EUNSUPPORTED, "fxb_init: ndim must be 2 or 3");
+    if (d.nguard < 4) return fail(FXB_EARG, "fxb_init: NGUARD must be at least 4");
+    if (p.order != 3 && p.order != 5) return fail(FXB_EUNSUPPORTED, "fxb_init: order must be 3 (PPM) or 5 (WENO)");
+    if (p.riemann != 3 && p.riemann != 4) return fail(FXB_EUNSUPPORTED, "fxb_init: RiemannSolver must be HLL or HLLC");
+    if (p.limiter < 1 || p.limiter > 5) return fail(FXB_EARG, "fxb_init: unknown slope limiter");
+    if (p.precision != FXB_FP64 && p.precision != FXB_MIXED) return fail(FXB_EARG, "fxb_init: unknown precision");
+    if (d.ndim == 2 && p.use_gravity) return fail(FXB_EUNSUPPORTED, "fxb_init: gravity is implemented for 3-D only");
+    for (int i = 0; i < 2 * d.ndim; i++)
+        if (d.bc[i] < 0 || d.bc[i] > 2) return fail(FXB_EARG, "fxb_init: unknown boundary condition");
+    for (int a = 0; a < d.ndim; a++) {
+        bool per_lo = d.bc[2 * a] == FXB_BC_PERIODIC, per_hi = d.bc[2 * a + 1] == FXB_BC_PERIODIC;
+        if (per_lo != per_hi) return fail(FXB_EARG, "fxb_init: periodic boundaries must be paired");
+    }
+    if (nunk < FXB_NVAR) return fail(FXB_EARG, "fxb_init: nunk too small");
+    for (int v = 0; v < FXB_NVAR; v++)
+        if (var_map[v] < 0 || var_map[v] >= nunk) return fail(FXB_EARG, "fxb_init: var_map out of range");
+    L.prm = p;
+    L.dom = d;
+    L.nunk = nunk;
+    for (int v = 0; v < NV_DEV; v++) L.dmap[v] = var_map[kDevToVar[v]];
+    L.nx = d.nxb * d.nblockx;
+    L.ny = d.ndim >= 2 ? d.nyb * d.nblocky : 1;
+    L.nz = d.ndim == 3 ? d.nzb * d.nblockz : 1;
+    if (d.ndim == 2 && (L.nx % T2 || L.ny % T2))
+        return fail(FXB_EUNSUPPORTED, "fxb_init: 2-D grid extents must be multiples of 16");
+    if (d.ndim == 3 && (L.nx % T3X || L.ny % T3Y || L.nz % T3Z))
+        return fail(FXB_EUNSUPPORTED, "fxb_init: 3-D grid extents must be multiples of the 3-D tile");
+    L.ncell = (long)L.nx * L.ny * L.nz;
+    L.vstride = (L.ncell + 31) / 32 * 32;
+    L.nblk = d.nblockx * (d.ndim >= 2 ? d.nblocky : 1) * (d.ndim == 3 ? d.nblockz : 1);
+    long per = (long)(d.nxb + 2 * d.nguard) * (d.ndim >= 2 ? d.nyb + 2 * d.nguard : 1) *
+               (d.ndim == 3 ? d.nzb + 2 * d.nguard : 1);
+    L.unk_doubles = per * L.nblk * nunk;
+    DevParams &q = L.dprm;
+    q.order = p.order; q.weno_method = p.weno_method; q.riemann = p.riemann; q.limiter = p.limiter;
+    q.char_limiting = p.char_limiting; q.use_3d_full_ctu = p.use_3d_full_ctu; q.use_aux_eint = p.use_aux_eint;
+    q.use_gravity = p.use_gravity;
+    for (int i = 0; i < 3; i++) q.grav[i] = p.grav[i];
+    q.cfl = p.cfl; q.gamma = p.gamma; q.eint_switch = p.eint_switch; q.small_dens = p.small_dens;
+    q.small_e = p.small_e; q.small_p = p.small_p; q.tiny = p.tiny; q.fpres = p.fpres;
+    q.limited_beta = p.limited_beta; q.gas_constant = p.gas_constant; q.abar = p.abar;
+    // Gamma/Eos_init.F90:86 and Gamma/Eos.F90:177,240-241
+    double gammam1 = 1.0 / (p.gamma - 1.0);
+    L.gam1inv = 1. / gammam1;
+    L.ggprodinv = 1. / (gammam1 * p.gas_constant);
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(FXB_ECUDA, "fxb_init: no CUDA device visible");
+    }
+    CK(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&L.ev0));
+    CK(cudaEventCreate(&L.ev1));
+    for (int i = 0; i < 2; i++) {
+        CK(cudaMalloc(&L.buf[i], sizeof(double) * L.vstride * NV_DEV));
+        CK(cudaMemsetAsync(L.buf[i], 0, sizeof(double) * L.vstride * NV_DEV, L.stream));
+    }
+    CK(cudaMalloc(&L.unk_dev, sizeof(double) * L.unk_doubles));
+    CK(cudaMalloc(&L.dmap_dev, sizeof(int) * NV_DEV));
+    CK(cudaMemcpyAsync(L.dmap_dev, L.dmap, sizeof(int) * NV_DEV, cudaMemcpyHostToDevice, L.stream));
+    CK(cudaMalloc(&L.dtv, 2 * sizeof(double)));
+    CK(cudaMalloc(&L.rate_max, sizeof(unsigned long long)));
+    CK(cudaMalloc(&L.err, sizeof(int)));
+    CK(cudaMemsetAsync(L.err, 0, sizeof(int), L.stream));
+    CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
+    L.npartials = 1024;
+    CK(cudaMalloc(&L.partials, sizeof(double) * (L.npartials * 7 + 8)));
+    if (d.ndim == 2) {
+        CK(setup_hydro2d_fp64());
+        CK(setup_hydro2d_mixed());
+    } else {
+        CK(setup_hydro3d_fp64());
+        CK(setup_hydro3d_mixed());
+    }
+    CK(cudaStreamSynchronize(L.stream));
+    L.inited = true;
+    return FXB_OK;
+}
+
+extern "C" int fxb_register_blocks(const fxb_block_desc *blocks, int nblk)
+{
+    if (!L.inited) return fail(FXB_EARG, "fxb_register_blocks: call fxb_init first");
+    if (!blocks || nblk != L.nblk) return fail(FXB_EARG, "fxb_register_blocks: the block list must cover the grid");
+    int nb[3] = {L.dom.nblockx, L.dom.ndim >= 2 ? L.dom.nblocky : 1, L.dom.ndim == 3 ? L.dom.nblockz : 1};
+    int *h = new int[3 * nblk];
+    char *seen = new char[nblk]();
+    for (int b = 0; b < nblk; b++) {
+        for (int a = 0; a < 3; a++) {
+            int c = blocks[b].bcoord[a];
+            if (a >= L.dom.ndim) c = 0;
+            if (c < 0 || c >= nb[a]) { delete[] h; delete[] seen; return fail(FXB_EARG, "fxb_register_blocks: block coordinate out of range"); }
+            h[3 * b + a] = c;
+        }
+        long lin = ((long)h[3 * b + 2] * nb[1] + h[3 * b + 1]) * nb[0] + h[3 * b];
+        if (seen[lin]) { delete[] h; delete[] seen; return fail(FXB_EARG, "fxb_register_blocks: duplicate block"); }
+        seen[lin] = 1;
+        if (blocks[b].level != 1) { delete[] h; delete[] seen; return fail(FXB_EUNSUPPORTED, "fxb_register_blocks: only level-1 (uniform) block lists"); }
+    }
+    delete[] seen;
+    if (!L.bcoord) {
+        cudaError_t e = cudaMalloc(&L.bcoord, sizeof(int) * 3 * nblk);
+        if (e != cudaSuccess) { delete[] h; return cuda_fail(e, "cudaMalloc bcoord"); }
+    }
+    cudaError_t e = cudaMemcpy(L.bcoord, h, sizeof(int) * 3 * nblk, cudaMemcpyHostToDevice);
+    delete[] h;
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy bcoord");
+    return FXB_OK;
+}
+
+extern "C" int fxb_attach_unk(const double *unk_host)
+{
+    if (!L.inited || !L.bcoord) return fail(FXB_EARG, "fxb_attach_unk: call fxb_init and fxb_register_blocks first");
+    if (!unk_host) return fail(FXB_EARG, "fxb_attach_unk: null UNK");
+    CK(cudaMemcpyAsync(L.unk_dev, unk_host, sizeof(double) * L.unk_doubles, cudaMemcpyHostToDevice, L.stream));
+    UnkGeom g = unk_geom();
+    unk_to_state_kernel<<<1184, 256, 0, L.stream>>>(L.unk_dev, L.buf[L.cur], g, L.bcoord, L.dmap_dev, L.nblk);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(L.stream));
+    L.attached = true;
+    L.rate_valid = false;
+    return FXB_OK;
+}
+
+extern "C" int fxb_sync_from_host(const double *unk_host) { return fxb_attach_unk(unk_host); }
+
+extern "C" int fxb_sync_to_host(double *unk_host)
+{
+    if (!L.attached) return fail(FXB_EARG, "fxb_sync_to_host: no UNK attached");
+    if (!unk_host) return fail(FXB_EARG, "fxb_sync_to_host: null UNK");
+    UnkGeom g = unk_geom();
+    state_to_unk_kernel<<<1184, 256, 0, L.stream>>>(L.buf[L.cur], L.unk_dev, g, L.bcoord, L.dmap_dev, L.nblk);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(unk_host, L.unk_dev, sizeof(double) * L.unk_doubles, cudaMemcpyDeviceToHost, L.stream));
+    CK(cudaStreamSynchronize(L.stream));
+    return check_err_word();
+}
+
+extern "C" int fxb_fill_guardcells(double *unk_host) { return fxb_sync_to_host(unk_host); }
+
+extern "C" int fxb_eos(void)
+{
+    if (!L.attached) return fail(FXB_EARG, "fxb_eos: no UNK attached");
+    eos_kernel<<<1184, 256, 0, L.stream>>>(L.buf[L.cur], L.vstride, L.ncell, L.dprm, L.gam1inv, L.ggprodinv);
+    CK(cudaGetLastError());
+    L.rate_valid = false;
+    return FXB_OK;
+}
+
+extern "C" int fxb_hydro_step(double sim_time, double dt, double dt_old)
+{
+    (void)sim_time; (void)dt_old;
+    if (!L.attached) return fail(FXB_EARG, "fxb_hydro_step: no UNK attached");
+    if (!(dt > 0.)) return fail(FXB_EARG, "fxb_hydro_step: dt must be positive");
+    CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
+    CK(cudaEventRecord(L.ev0, L.stream));
+    int rc = launch_hydro(L.cur, nullptr, dt);
+    if (rc) return rc;
+    CK(cudaEventRecord(L.ev1, L.stream));
+    L.cur = 1 - L.cur;
+    L.rate_valid = true;
+    L.last_launches = 1;
+    L.timing_valid = true;
+    return FXB_OK;
+}
+
+extern "C" int fxb_compute_dt(double *dt_out, int32_t loc[5])
+{
+    if (!L.attached) return fail(FXB_EARG, "fxb_compute_dt: no UNK attached");
+    if (!dt_out) return fail(FXB_EARG, "fxb_compute_dt: null output");
+    if (!L.rate_valid) {
+        CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
+        rate_kernel<<<1184, 256, 0, L.stream>>>(L.buf[L.cur], L.vstride, L.nx, L.ny, L.nz, L.dom.ndim,
+                                                cell_dx(0), cell_dx(1), cell_dx(2), L.rate_max);
+        CK(cudaGetLastError());
+        L.rate_valid = true;
+    }
+    unsigned long long bits = 0;
+    CK(cudaMemcpyAsync(&bits, L.rate_max, sizeof(bits), cudaMemcpyDeviceToHost, L.stream));
+    CK(cudaStreamSynchronize(L.stream));
+    int rc = check_err_word();
+    if (rc) return rc;
+    double r;
+    memcpy(&r, &bits, sizeof(r));
+    double dt = (r != 0.) ? L.prm.cfl / r : 1.79769313486231570e308;
+    if (loc) { loc[0] = 0; loc[1] = 0; loc[2] = 0; loc[3] = 1; loc[4] = 0; }
+    *dt_out = dt;
+    if (!(dt > 0.)) return fail(FXB_EDT, "[Hydro]: Computed dt is not positive! Aborting!");
+    return FXB_OK;
+}
+
+extern "C" int fxb_advance(int nsteps, double *dt, double *dt_old, double f, double dtmin, double dtmax)
+{
+    if (!L.attached) return fail(FXB_EARG, "fxb_advance: no UNK attached");
+    if (!dt || !dt_old || nsteps < 0) return fail(FXB_EARG, "fxb_advance: bad argument");
+    double h[2] = {*dt, *dt_old};
+    CK(cudaMemcpyAsync(L.dtv, h, sizeof(h), cudaMemcpyHostToDevice, L.stream));
+    CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
+    // graphs of two steps (buffer c -> 1-c -> c), built once per starting buffer
+    auto one_step = [&](int src) -> int {
+        int rc = launch_hydro(src, L.dtv, 0.);
+        if (rc) return rc;
+        dt_finalize_kernel<<<1, 1, 0, L.stream>>>(L.dtv, L.rate_max, L.prm.cfl, f, dtmin, dtmax, L.err);
+        return cudaGetLastError() == cudaSuccess ? FXB_OK : fail(FXB_ECUDA, "dt kernel launch");
+    };
+    CK(cudaEventRecord(L.ev0, L.stream));
+    int done = 0;
+    if (nsteps >= 2) {
+        int c = L.cur;
+        if (!L.graph_exec[c]) {
+            cudaGraph_t graph;
+            CK(cudaStreamBeginCapture(L.stream, cudaStreamCaptureModeThreadLocal));
+            int rc = one_step(c);
+            if (!rc) rc = one_step(1 - c);
+            cudaError_t e = cudaStreamEndCapture(L.stream, &graph);
+            if (rc) return rc;
+            if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&L.graph_exec[c], graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+            // f, dtmin, dtmax are baked into the graph; rebuild when they change
+        }
+        for (; done + 2 <= nsteps; done += 2) CK(cudaGraphLaunch(L.graph_exec[c], L.stream));
+    }
+    for (; done < nsteps; done++) {
+        int rc = one_step(L.cur);
+        if (rc) return rc;
+        L.cur = 1 - L.cur;
+    }
+    CK(cudaEventRecord(L.ev1, L.stream));
+    CK(cudaMemcpyAsync(h, L.dtv, sizeof(h), cudaMemcpyDeviceToHost, L.stream));
+    CK(cudaStreamSynchronize(L.stream));
+    *dt = h[0];
+    *dt_old = h[1];
+    L.rate_valid = false;
+    L.last_launches = 2 * nsteps;
+    L.timing_valid = true;
+    return check_err_word();
+}
+
+extern "C" int fxb_integrals(double out[7])
+{
+    if (!L.attached) return fail(FXB_EARG, "fxb_integrals: no UNK attached");
+    double dv = cell_dx(0) * cell_dx(1) * cell_dx(2);
+    integrals_kernel<<<L.npartials, 256, 0, L.stream>>>(L.buf[L.cur], L.vstride, L.ncell, dv, L.partials);
+    integrals_final_kernel<<<1, 32, 0, L.stream>>>(L.partials, L.npartials, L.partials + L.npartials * 7);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, L.partials + L.npartials * 7, 7 * sizeof(double), cudaMemcpyDeviceToHost, L.stream));
+    CK(cudaStreamSynchronize(L.stream));
+    return FXB_OK;
+}
+
+extern "C" int fxb_last_timing(double *ms, int *kernel_launches)
+{
+    if (!L.timing_valid) return fail(FXB_EARG, "fxb_last_timing: nothing timed yet");
+    float f = 0.f;
+    CK(cudaEventSynchronize(L.ev1));
+    CK(cudaEventElapsedTime(&f, L.ev0, L.ev1));
+    if (ms) *ms = f;
+    if (kernel_launches) *kernel_launches = L.last_launches;
+    return FXB_OK;
+}
+
+extern "C" void *fxb_stream(void) { return (void *)L.stream; }
+
+extern "C" int fxb_last_error(fxb_error *err)
+{
+    if (err) *err = L.lasterr;
+    return L.lasterr.code;
+}
+
+extern "C" void fxb_finalize(void)
+{
+    if (L.stream) cudaStreamSynchronize(L.stream);
+    free_all();
+}

@@ -1,0 +1,467 @@
+// fxb_device.cuh -- per-cell device math of the unsplit hydro path.
+//
+// Templated on the reconstruction type R (double for the FP64 path, float
+// for the mixed path).  The primitive eigensystem of the pure-hydro solver
+// is sparse (OnlyHydro/hy_eigenVector.F90:87-167: 7 nonzero left and 9
+// nonzero right entries out of 25 each), so every dot product and
+// projection below is written with only its nonzero terms, added in the
+// reference's summation order.  Dropping a 0*x term from a left-to-right sum
+// changes at most the sign of an exact zero, never a nonzero value, so the
+// FP64 path built with -fmad=false reproduces the oracle's values.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fxb {
+
+// primitive slots (UHD.h HY_DENS..HY_EINT, 0-based); device arrays use the
+// same order for their first eight variables, then ENER and TEMP.
+enum { D = 0, VX = 1, VY = 2, VZ = 3, P = 4, GC = 5, GE = 6, EI = 7 };
+enum { NV_DEV = 10, DV_ENER = 8, DV_TEMP = 9 };
+// flux slots (UHD.h HY_DENS_FLUX..HY_VOLU_FLUX)
+enum { FD = 0, FMX = 1, FMY = 2, FMZ = 3, FE = 4, FP = 5, FEI = 6, FVOL = 7, NF = 8 };
+
+enum { LIM_MINMOD = 1, LIM_MC = 2, LIM_VANLEER = 3, LIM_HYBRID = 4, LIM_LIMITED = 5 };
+enum { ERR_SOUND = 1, ERR_RIEMANN = 2 };
+
+struct DevParams {
+    int order, weno_method, riemann, limiter, char_limiting, use_3d_full_ctu, use_aux_eint, use_gravity;
+    double grav[3];
+    double cfl, gamma, eint_switch, small_dens, small_e, small_p, tiny, fpres, limited_beta, gas_constant, abar;
+};
+
+// ---- precision helpers ---------------------------------------------------
+template <class R> __device__ __forceinline__ R rdiv(R a, R b);
+template <> __device__ __forceinline__ double rdiv<double>(double a, double b) { return a / b; }
+template <> __device__ __forceinline__ float rdiv<float>(float a, float b) { return __fdividef(a, b); }
+template <class R> __device__ __forceinline__ R rsqrt_(R a);
+template <> __device__ __forceinline__ double rsqrt_<double>(double a) { return sqrt(a); }
+template <> __device__ __forceinline__ float rsqrt_<float>(float a) { return __fsqrt_rn(a); }
+
+// Fortran MIN/MAX with gfortran's argument order: mvar = a1; if (a2 < mvar) mvar = a2
+template <class R> __device__ __forceinline__ R fmin2(R a, R b) { return (b < a) ? b : a; }
+template <class R> __device__ __forceinline__ R fmax2(R a, R b) { return (b > a) ? b : a; }
+template <class R> __device__ __forceinline__ R sgn1(R b) { return copysign(R(1), b); }
+
+// ---- limiters (hy_slopeLimiters.F90) ----------------------------------------
+template <class R> __device__ __forceinline__ R lim_minmod(R a, R b)
+{ return R(.5) * (sgn1(a) + sgn1(b)) * fmin2(fabs(a), fabs(b)); }
+template <class R> __device__ __forceinline__ R lim_mc(R a, R b)
+{ return (sgn1(a) + sgn1(b)) * fmin2(fmin2(fabs(a), R(.25) * fabs(a + b)), fabs(b)); }
+template <class R> __device__ __forceinline__ R lim_vanleer(R a, R b)
+{ return (a * b <= R(0)) ? R(0) : rdiv(R(2) * a * b, a + b); }
+template <class R> __device__ __forceinline__ R lim_limited(R a, R b, R beta)
+{
+    if (b > R(0)) return fmax2(fmax2(R(0), fmin2(beta * a, b)), fmin2(a, beta * b));
+    return fmin2(fmin2(R(0), fmax2(beta * a, b)), fmax2(a, beta * b));
+}
+// limiter used on characteristic wave w (w = -1: a primitive variable of kind k)
+template <class R> __device__ __forceinline__ R limit(int lim, int w, int k, R a, R b, R beta)
+{
+    switch (lim) {
+    case LIM_MINMOD:  return lim_minmod(a, b);
+    case LIM_MC:      return lim_mc(a, b);
+    case LIM_VANLEER: return lim_vanleer(a, b);
+    case LIM_HYBRID:
+        // characteristic: minmod on the acoustic/shear waves, mc on entropy (hy_TVDslope.F90:146-174);
+        // primitive: mc on dens/gamc/game, minmod on velocities and pressure (:176-191)
+        if (w >= 0) return (w == 2) ? lim_mc(a, b) : lim_minmod(a, b);
+        return (k == D || k == GC || k == GE) ? lim_mc(a, b) : (k <= P ? lim_minmod(a, b) : R(0));
+    default:          return lim_limited(a, b, beta);
+    }
+}
+
+// ---- eigensystem (hy_eigenParameters.F90:84-100, hy_eigenValue.F90:58-62,
+//      OnlyHydro/hy_eigenVector.F90:87-127) --------------------------------
+template <class R> struct Eig {
+    R lam0, un, lam4;       // u-c, u (slow/entropy/slow), u+c
+    R cf, rho, ahinv, lp, a2inv, rp;
+};
+
+// returns false on a2 <= 0 (the reference aborts there)
+template <class R> __device__ __forceinline__ bool eigen(R rho, R un, R p, R gamc, Eig<R> &e)
+{
+    R a2 = rdiv(gamc * p, rho);
+    if (a2 <= R(0)) return false;
+    R cf = rsqrt_(a2);
+    e.lam0 = un - cf; e.un = un; e.lam4 = un + cf;
+    R dinv = rdiv(R(1), rho);
+    R aa2 = cf * cf;
+    e.a2inv = rdiv(R(1), aa2);
+    e.ahinv = rdiv(R(.5), cf);
+    R Na = R(.5) * e.a2inv;
+    e.lp = dinv * Na;
+    e.cf = cf; e.rho = rho; e.rp = rho * aa2;
+    return true;
+}
+
+// Left-eigenvector dot products L(:,w) . x for the five waves; x indexed by
+// D, v1 (normal), v2, v3 (transverse, cyclic), P.
+template <class R> struct Five { R w[5]; };
+template <class R> __device__ __forceinline__ Five<R> ldot(const Eig<R> &e, R xD, R x1, R x2, R x3, R xP)
+{
+    Five<R> o;
+    o.w[0] = e.lp * xP - e.ahinv * x1;
+    o.w[1] = x2;
+    o.w[2] = xD - e.a2inv * xP;
+    o.w[3] = x3;
+    o.w[4] = e.ahinv * x1 + e.lp * xP;
+    return o;
+}
+
+// ---- TVD slope (hy_TVDslope.F90:65-276) projected to primitives ---------------
+// Inputs: the three states along the sweep (D, v1, v2, v3, P, EI order).
+// Output db[6] = limited slopes of D, v1, v2, v3, P (projected with R when
+// charLimiting) and EI (primitive).
+template <class R>
+__device__ __forceinline__ void tvd_slope(const DevParams &prm, const Eig<R> &e,
+                                          const R *VL, const R *V0, const R *VR, R db[6])
+{
+    R dL[6], dR[6];
+#pragma unroll
+    for (int k = 0; k < 6; k++) { dL[k] = V0[k] - VL[k]; dR[k] = VR[k] - V0[k]; }
+    const R beta = R(prm.limited_beta);
+    if (prm.char_limiting) {
+        Five<R> a = ldot(e, dL[0], dL[1], dL[2], dL[3], dL[4]);
+        Five<R> b = ldot(e, dR[0], dR[1], dR[2], dR[3], dR[4]);
+        R d[5];
+#pragma unroll
+        for (int w = 0; w < 5; w++) d[w] = limit(prm.limiter, w, -1, a.w[w], b.w[w], beta);
+        // R * delbar, summed over waves FASTLEFT..FASTRGHT (hy_DataReconstructNormalDir_PPM.F90:539-581)
+        db[0] = (e.rho * d[0] + d[2]) + e.rho * d[4];
+        db[1] = e.cf * d[4] - e.cf * d[0];
+        db[2] = d[1];
+        db[3] = d[3];
+        db[4] = e.rp * d[0] + e.rp * d[4];
+        // gamc/game/eint keep primitive limiting; the hybrid choice is mc for them here (:165-170)
+        db[5] = (prm.limiter == LIM_HYBRID) ? lim_mc(dL[5], dR[5]) : limit(prm.limiter, -1, (int)EI, dL[5], dR[5], beta);
+    } else {
+        const int kind[6] = {D, VX, VY, VZ, P, EI};
+#pragma unroll
+        for (int k = 0; k < 6; k++) db[k] = limit(prm.limiter, -1, kind[k], dL[k], dR[k], beta);
+    }
+}
+
+// ---- upwind transverse flux sig (hy_upwindTransverseFlux.F90:54-222) --------
+// m, c, p: states along the transverse direction in (D, v1, v2, v3, P, EI)
+// order; sig is returned in the same order.
+template <class R>
+__device__ __forceinline__ void trans_flux(const Eig<R> &e, const R *m, const R *c, const R *p, bool aux, R sig[6])
+{
+    R t[6];
+    // wave 0 (u-c)
+    const bool up0 = e.lam0 > R(0);
+#pragma unroll
+    for (int k = 0; k < 5; k++) t[k] = up0 ? c[k] - m[k] : p[k] - c[k];
+    R d0 = e.lp * t[4] - e.ahinv * t[1];
+    R sD = (e.lam0 * e.rho) * d0;
+    R s1 = (e.lam0 * (-e.cf)) * d0;
+    R sP = (e.lam0 * e.rp) * d0;
+    // waves 1..3 (u)
+    const bool upu = e.un > R(0);
+#pragma unroll
+    for (int k = 0; k < 5; k++) t[k] = upu ? c[k] - m[k] : p[k] - c[k];
+    R s2 = e.un * t[2];
+    sD = sD + e.un * (t[0] - e.a2inv * t[4]);
+    R s3 = e.un * t[3];
+    // wave 4 (u+c)
+    const bool up4 = e.lam4 > R(0);
+#pragma unroll
+    for (int k = 0; k < 5; k++) t[k] = up4 ? c[k] - m[k] : p[k] - c[k];
+    R d4 = e.ahinv * t[1] + e.lp * t[4];
+    sD = sD + (e.lam4 * e.rho) * d4;
+    s1 = s1 + (e.lam4 * e.cf) * d4;
+    sP = sP + (e.lam4 * e.rp) * d4;
+    sig[0] = sD; sig[1] = s1; sig[2] = s2; sig[3] = s3; sig[4] = sP;
+    sig[5] = aux ? e.un * (upu ? c[5] - m[5] : p[5] - c[5]) : R(0);
+}
+
+// ---- PPM/WENO common tail: monotonicity, initial guesses and characteristic
+// tracing (hy_DataReconstructNormalDir_PPM.F90:697-853).  vecL/vecR hold the
+// interface values of D, v1, v2, v3, P, EI; Wm/Wp receive the traced states.
+template <class R>
+__device__ __forceinline__ void ppm_trace(const Eig<R> &e, R dtn, R hdtn, const R *Vc,
+                                          R *vecL, R *vecR, R Wm[6], R Wp[6])
+{
+    R delW[6], W6[6];
+#pragma unroll
+    for (int n = 0; n < 6; n++) {
+        R L = vecL[n], Rr = vecR[n], C = Vc[n];
+        if ((Rr - C) * (C - L) <= R(0)) { L = C; Rr = C; }
+        if (R(6) * (Rr - L) * (C - R(.5) * (L + Rr)) > (Rr - L) * (Rr - L)) L = R(3) * C - R(2) * Rr;
+        if (R(6) * (Rr - L) * (C - R(.5) * (L + Rr)) < -((Rr - L) * (Rr - L))) Rr = R(3) * C - R(2) * L;
+        vecL[n] = L; vecR[n] = Rr;
+        delW[n] = Rr - L;
+        W6[n] = R(6) * (C - R(.5) * (Rr + L));
+    }
+    // secondary variable EI: initial guess survives (gamc/game are reset to Vc)
+    {
+        R lmax = fmax2(e.un, R(0));
+        Wp[5] = vecR[5] - lmax * hdtn * (delW[5] - (R(1.0) - lmax * hdtn * R(4.) / R(3.)) * W6[5]);
+        R lmin = -fmin2(e.un, R(0));
+        Wm[5] = vecL[5] + lmin * hdtn * (delW[5] + (R(1.0) - lmin * hdtn * R(4.) / R(3.)) * W6[5]);
+    }
+    // tracing over the five waves, HLL-type branch
+    Five<R> cA = ldot(e, delW[0], delW[1], delW[2], delW[3], delW[4]);
+    Five<R> cB;
+    cB.w[0] = e.ahinv * W6[1] - e.lp * W6[4];
+    cB.w[1] = -W6[2];
+    cB.w[2] = -W6[0] + e.a2inv * W6[4];
+    cB.w[3] = -W6[3];
+    cB.w[4] = -(e.ahinv * W6[1]) - e.lp * W6[4];
+    const R c43 = R(4.) / R(3.);
+    R aL[3], bL[3], aR[3], bR[3];
+    const R lams[3] = {e.lam0, e.un, e.lam4};
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        R lam = lams[q];
+        R lt = dtn * lam;
+        aL[q] = R(.5) * (R(-1.) - dtn * lam);
+        bL[q] = R(.25) * (R(1.) + R(2.) * dtn * lam + c43 * (lt * lt));
+        aR[q] = R(.5) * (R(1.) - dtn * lam);
+        bR[q] = R(.25) * (R(1.) - R(2.) * dtn * lam + c43 * (lt * lt));
+    }
+    // wave 0
+    R sLD = (aL[0] * e.rho) * cA.w[0] + (bL[0] * e.rho) * cB.w[0];
+    R sRD = (aR[0] * e.rho) * cA.w[0] + (bR[0] * e.rho) * cB.w[0];
+    R sL1 = (aL[0] * (-e.cf)) * cA.w[0] + (bL[0] * (-e.cf)) * cB.w[0];
+    R sR1 = (aR[0] * (-e.cf)) * cA.w[0] + (bR[0] * (-e.cf)) * cB.w[0];
+    R sLP = (aL[0] * e.rp) * cA.w[0] + (bL[0] * e.rp) * cB.w[0];
+    R sRP = (aR[0] * e.rp) * cA.w[0] + (bR[0] * e.rp) * cB.w[0];
+    // waves 1..3 (right eigenvector entries equal to one)
+    R sL2 = aL[1] * cA.w[1] + bL[1] * cB.w[1];
+    R sR2 = aR[1] * cA.w[1] + bR[1] * cB.w[1];
+    sLD = sLD + (aL[1] * cA.w[2] + bL[1] * cB.w[2]);
+    sRD = sRD + (aR[1] * cA.w[2] + bR[1] * cB.w[2]);
+    R sL3 = aL[1] * cA.w[3] + bL[1] * cB.w[3];
+    R sR3 = aR[1] * cA.w[3] + bR[1] * cB.w[3];
+    // wave 4
+    sLD = sLD + ((aL[2] * e.rho) * cA.w[4] + (bL[2] * e.rho) * cB.w[4]);
+    sRD = sRD + ((aR[2] * e.rho) * cA.w[4] + (bR[2] * e.rho) * cB.w[4]);
+    sL1 = sL1 + ((aL[2] * e.cf) * cA.w[4] + (bL[2] * e.cf) * cB.w[4]);
+    sR1 = sR1 + ((aR[2] * e.cf) * cA.w[4] + (bR[2] * e.cf) * cB.w[4]);
+    sLP = sLP + ((aL[2] * e.rp) * cA.w[4] + (bL[2] * e.rp) * cB.w[4]);
+    sRP = sRP + ((aR[2] * e.rp) * cA.w[4] + (bR[2] * e.rp) * cB.w[4]);
+    const R sl[5] = {sLD, sL1, sL2, sL3, sLP}, sr[5] = {sRD, sR1, sR2, sR3, sRP};
+#pragma unroll
+    for (int v = 0; v < 5; v++) {
+        R base = Vc[v] + W6[v] / R(12.);
+        Wm[v] = base + sl[v];
+        Wp[v] = base + sr[v];
+    }
+}
+
+// PPM interface values (hy_DataReconstructNormalDir_PPM.F90:590-593)
+template <class R>
+__device__ __forceinline__ void ppm_interfaces(const R *Vm, const R *Vc, const R *Vp,
+                                               const R *dbN, const R *db0, const R *dbP, R vecL[6], R vecR[6])
+{
+#pragma unroll
+    for (int n = 0; n < 6; n++) {
+        vecL[n] = R(.5) * (Vc[n] + Vm[n]) - (db0[n] - dbN[n]) / R(6.);
+        vecR[n] = R(.5) * (Vc[n] + Vp[n]) - (dbP[n] - db0[n]) / R(6.);
+    }
+}
+
+// WENO5 / WENO-Z interface values of one scalar stencil
+// (hy_DataReconstructNormalDir_WENO.F90:458-560, tiny = 1e-36, wenoExp = 1)
+template <class R>
+__device__ __forceinline__ void weno_scalar(int method, R I0, R I1, R I2, R I3, R I4, R &vr, R &vl)
+{
+    const R c6 = R(6.);
+    const R p00 = R(2.) / c6, p01 = R(-7.) / c6, p02 = R(11.) / c6;
+    const R p10 = R(-1.) / c6, p11 = R(5.) / c6, p12 = R(2.) / c6;
+    const R p20 = R(2.) / c6, p21 = R(5.) / c6, p22 = R(-1.) / c6;
+    const R m00 = R(-1.) / c6, m01 = R(5.) / c6, m02 = R(2.) / c6;
+    const R m10 = R(2.) / c6, m11 = R(5.) / c6, m12 = R(-1.) / c6;
+    const R m20 = R(11.) / c6, m21 = R(-7.) / c6, m22 = R(2.) / c6;
+    R w5p0 = p00 * I0 + p01 * I1 + p02 * I2;
+    R w5p1 = p10 * I1 + p11 * I2 + p12 * I3;
+    R w5p2 = p20 * I2 + p21 * I3 + p22 * I4;
+    R w5m0 = m00 * I0 + m01 * I1 + m02 * I2;
+    R w5m1 = m10 * I1 + m11 * I2 + m12 * I3;
+    R w5m2 = m20 * I2 + m21 * I3 + m22 * I4;
+    const R c1312 = R(13.) / R(12.);
+    R t1, t2;
+    t1 = I0 - R(2.) * I1 + I2; t2 = I0 - R(4.) * I1 + R(3.) * I2;
+    R b0 = c1312 * (t1 * t1) + R(0.25) * (t2 * t2);
+    t1 = I1 - R(2.) * I2 + I3; t2 = I1 - I3;
+    R b1 = c1312 * (t1 * t1) + R(0.25) * (t2 * t2);
+    t1 = I2 - R(2.) * I3 + I4; t2 = R(3.) * I2 - R(4.) * I3 + I4;
+    R b2 = c1312 * (t1 * t1) + R(0.25) * (t2 * t2);
+    const R tiny = R(1.e-36);
+    R a0, a1, a2, s;
+    // i+1/2, gammas (0.1, 0.6, 0.3)
+    if (method == 2) {
+        R tau = fabs(b0 - b2);
+        a0 = R(0.1) * (R(1.) + rdiv(tau, tiny + b0));
+        a1 = R(0.6) * (R(1.) + rdiv(tau, tiny + b1));
+        a2 = R(0.3) * (R(1.) + rdiv(tau, tiny + b2));
+    } else {
+        a0 = rdiv(R(0.1), tiny + b0); a1 = rdiv(R(0.6), tiny + b1); a2 = rdiv(R(0.3), tiny + b2);
+    }
+    s = a0 + a1 + a2;
+    vr = rdiv(a0, s) * w5p0 + rdiv(a1, s) * w5p1 + rdiv(a2, s) * w5p2;
+    // i-1/2, gammas (0.3, 0.6, 0.1)
+    if (method == 2) {
+        R tau = fabs(b0 - b2);
+        a0 = R(0.3) * (R(1.) + rdiv(tau, tiny + b0));
+        a1 = R(0.6) * (R(1.) + rdiv(tau, tiny + b1));
+        a2 = R(0.1) * (R(1.) + rdiv(tau, tiny + b2));
+    } else {
+        a0 = rdiv(R(0.3), tiny + b0); a1 = rdiv(R(0.6), tiny + b1); a2 = rdiv(R(0.1), tiny + b2);
+    }
+    s = a0 + a1 + a2;
+    vl = rdiv(a0, s) * w5m0 + rdiv(a1, s) * w5m1 + rdiv(a2, s) * w5m2;
+}
+
+// WENO interface values of D, v1, v2, v3, P (characteristic when charLimiting)
+// and EI (primitive).  S[0..4][6] = Vmm, Vm, Vc, Vp, Vpp.
+template <class R>
+__device__ __forceinline__ void weno_interfaces(const DevParams &prm, const Eig<R> &e, const R S[5][6],
+                                                R vecL[6], R vecR[6])
+{
+    if (prm.char_limiting) {
+        Five<R> w[5];
+#pragma unroll
+        for (int s = 0; s < 5; s++) w[s] = ldot(e, S[s][0], S[s][1], S[s][2], S[s][3], S[s][4]);
+        R cr[5], cl[5];
+#pragma unroll
+        for (int n = 0; n < 5; n++)
+            weno_scalar(prm.weno_method, w[0].w[n], w[1].w[n], w[2].w[n], w[3].w[n], w[4].w[n], cr[n], cl[n]);
+        vecR[0] = (e.rho * cr[0] + cr[2]) + e.rho * cr[4];
+        vecR[1] = e.cf * cr[4] - e.cf * cr[0];
+        vecR[2] = cr[1]; vecR[3] = cr[3];
+        vecR[4] = e.rp * cr[0] + e.rp * cr[4];
+        vecL[0] = (e.rho * cl[0] + cl[2]) + e.rho * cl[4];
+        vecL[1] = e.cf * cl[4] - e.cf * cl[0];
+        vecL[2] = cl[1]; vecL[3] = cl[3];
+        vecL[4] = e.rp * cl[0] + e.rp * cl[4];
+    } else {
+#pragma unroll
+        for (int n = 0; n < 5; n++)
+            weno_scalar(prm.weno_method, S[0][n], S[1][n], S[2][n], S[3][n], S[4][n], vecR[n], vecL[n]);
+    }
+    weno_scalar(prm.weno_method, S[0][5], S[1][5], S[2][5], S[3][5], S[4][5], vecR[5], vecL[5]);
+}
+
+// ---- Riemann solvers (hy_HLLC.F90:64-335, hy_HLL.F90:64-182) ---------------
+// Vm/Vp: 6-vectors D, VX, VY, VZ, P (global axes), EI; gamc/game passed separately.
+// F[8] receives the HY_*_FLUX slots including the aux-eint pair.
+template <class R>
+__device__ __forceinline__ int riemann(const DevParams &prm, int dir, const R *Vm, R gcL, R geL,
+                                       const R *Vp, R gcR, R geR, R F[8])
+{
+    const R velNL = Vm[1 + dir], velNR = Vp[1 + dir];
+    const R aL2 = rdiv(gcL * Vm[P], Vm[D]);
+    const R aR2 = rdiv(gcR * Vp[P], Vp[D]);
+    const bool hllc = prm.riemann == 4;
+    const R tiny = hllc ? R(prm.tiny) : R(1.e-32);
+    if ((Vm[D] < tiny && Vm[D] > R(0)) || (Vp[D] < tiny && Vp[D] > R(0)) ||
+        (Vm[P] < tiny && Vm[P] > R(0)) || (Vp[P] < tiny && Vp[P] > R(0))) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) F[k] = R(0);
+    } else if (aL2 < R(0) || aR2 < R(0)) {
+        return ERR_RIEMANN;
+    } else {
+        const R cfL = rsqrt_(aL2), cfR = rsqrt_(aR2);
+        const R SL = fmin2(velNL - cfL, velNR - cfR);
+        const R SR = fmax2(velNL + cfL, velNR + cfR);
+        // prim2con / prim2flx (hy_prim2con.F90:48-62, hy_prim2flx.F90:49-95)
+        R u2L = Vm[VX] * Vm[VX]; u2L = u2L + Vm[VY] * Vm[VY]; u2L = u2L + Vm[VZ] * Vm[VZ];
+        R u2R = Vp[VX] * Vp[VX]; u2R = u2R + Vp[VY] * Vp[VY]; u2R = u2R + Vp[VZ] * Vp[VZ];
+        const R EL = R(0.5) * Vm[D] * u2L + rdiv(Vm[P], geL - R(1.));
+        const R ER = R(0.5) * Vp[D] * u2R + rdiv(Vp[P], geR - R(1.));
+        R UL[5] = {Vm[D], Vm[D] * Vm[VX], Vm[D] * Vm[VY], Vm[D] * Vm[VZ], EL};
+        R UR[5] = {Vp[D], Vp[D] * Vp[VX], Vp[D] * Vp[VY], Vp[D] * Vp[VZ], ER};
+        const R fP = R(prm.fpres);
+        R FL[6], FR[6];
+        FL[0] = Vm[D] * velNL; FR[0] = Vp[D] * velNR;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            FL[1 + d] = FL[0] * Vm[1 + d];
+            FR[1 + d] = FR[0] * Vp[1 + d];
+        }
+        FL[1 + dir] = FL[1 + dir] + fP * Vm[P];
+        FR[1 + dir] = FR[1 + dir] + fP * Vp[P];
+        FL[4] = (EL + Vm[P]) * velNL; FR[4] = (ER + Vp[P]) * velNR;
+        FL[5] = Vm[P]; FR[5] = Vp[P];
+        if (hllc) {
+            R qStar = Vp[D] * velNR * (SR - velNR) - Vm[D] * velNL * (SL - velNL) + Vm[P] - Vp[P];
+            qStar = rdiv(qStar, Vp[D] * (SR - velNR) - Vm[D] * (SL - velNL));
+            if (SL >= R(0)) {
+#pragma unroll
+                for (int k = 0; k < 6; k++) F[k] = FL[k];
+            } else if (SL < R(0) && qStar >= R(0)) {
+                const R numerL = SL - velNL, denomL = SL - qStar;
+                const R pStar = Vm[D] * numerL * (qStar - velNL) + Vm[P];
+                const R dStar = rdiv(UL[0] * numerL, denomL);
+                R UC[5];
+                UC[0] = dStar;
+                UC[4] = rdiv(UL[4] * numerL, denomL) + rdiv(pStar * qStar - Vm[P] * velNL, denomL);
+#pragma unroll
+                for (int d = 0; d < 3; d++) UC[1 + d] = (d == dir) ? dStar * qStar : rdiv(UL[1 + d] * numerL, denomL);
+#pragma unroll
+                for (int k = 0; k < 5; k++) F[k] = FL[k] + SL * (UC[k] - UL[k]);
+                F[5] = FL[5];
+            } else if (qStar < R(0) && SR >= R(0)) {
+                const R numerR = SR - velNR, denomR = SR - qStar;
+                const R numerL = SL - velNL;
+                const R pStar = Vm[D] * numerL * (qStar - velNL) + Vm[P];
+                const R dStar = rdiv(UR[0] * numerR, denomR);
+                R UC[5];
+                UC[0] = dStar;
+                UC[4] = rdiv(UR[4] * numerR, denomR) + rdiv(pStar * qStar - Vp[P] * velNR, denomR);
+#pragma unroll
+                for (int d = 0; d < 3; d++) UC[1 + d] = (d == dir) ? dStar * qStar : rdiv(UR[1 + d] * numerR, denomR);
+#pragma unroll
+                for (int k = 0; k < 5; k++) F[k] = FR[k] + SR * (UC[k] - UR[k]);
+                F[5] = FR[5];
+            } else {
+#pragma unroll
+                for (int k = 0; k < 6; k++) F[k] = FR[k];
+            }
+        } else {
+            if (SL > R(0)) {
+#pragma unroll
+                for (int k = 0; k < 6; k++) F[k] = FL[k];
+            } else if (SR < R(0)) {
+#pragma unroll
+                for (int k = 0; k < 6; k++) F[k] = FR[k];
+            } else {
+                const R inv = SR - SL;
+#pragma unroll
+                for (int k = 0; k < 5; k++) F[k] = rdiv(SR * FL[k] - SL * FR[k] + SR * SL * (UR[k] - UL[k]), inv);
+                F[5] = rdiv(SR * FL[5] - SL * FR[5] + SR * SL * (R(0.0) - R(0.0)), inv);
+            }
+        }
+    }
+    // aux internal-energy and volume fluxes (hy_getFaceFlux.F90:444-453)
+    if (prm.use_aux_eint) {
+        if (F[0] > R(0)) { F[FVOL] = rdiv(F[0], Vm[D]); F[FEI] = F[0] * Vm[5]; }
+        else             { F[FVOL] = rdiv(F[0], Vp[D]); F[FEI] = F[0] * Vp[5]; }
+    } else { F[FVOL] = R(0); F[FEI] = R(0); }
+    return 0;
+}
+
+// ---- boundary index mapping for guard cells resolved on load ------------------
+// Maps a global index g in [-NG, n+NG) of one axis to an interior index;
+// *s becomes -1 when a reflecting face flips the normal velocity
+// (Grid_bcApplyToRegion.F90:458-531 for OUTFLOW and REFLECTING; periodic wrap
+// as the UG exchange of gr_shiftData.F90).
+__device__ __forceinline__ int map_axis(int g, int n, int bclo, int bchi, double *s)
+{
+    if (g < 0) {
+        if (bclo == 0) return g + n;
+        if (bclo == 1) return 0;
+        *s = -1.0; return -1 - g;
+    }
+    if (g >= n) {
+        if (bchi == 0) return g - n;
+        if (bchi == 1) return n - 1;
+        *s = -1.0; return 2 * n - 1 - g;
+    }
+    return g;
+}
+
+} // namespace fxb

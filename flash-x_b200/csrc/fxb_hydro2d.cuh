@@ -1,0 +1,321 @@
+// fxb_hydro2d.cuh -- fused 2-D unsplit hydro step, one CTA per 16x16 tile.
+//
+// Replaces, for every leaf block, UHD/hy_computeFluxes.F90:87-417 (with
+// Uout => Uin, levelFlux/Hydro.F90:191-212): hy_getRiemannState,
+// hy_getFaceFlux, hy_unsplitUpdate, hy_energyFix, Eos_wrapped(MODE_DENS_EI),
+// and the per-cell part of Hydro_computeDt.F90:151-242.
+//
+// Data: one FP64 array per variable over the whole uniform grid (x fastest),
+// read from `in` and written to `out` (ping-pong), so blocks need no stored
+// guard cells: the load stage resolves every halo cell from the neighbouring
+// tile or from the physical boundary condition (map_axis), which is what
+// Grid_fillGuardCells followed by the per-block copy would have provided.
+//
+// Stages (s = shared memory, R = reconstruction type):
+//   A  load the 22x22 window (tile + 3 halo) of D,VX,VY,VZ,P,GC,GE,EI -> s.V
+//   B  x: eigensystem + limited slopes of cells i=-2..17, j=0..15      -> s.DB
+//   C  x: PPM/WENO face states of i=-1..16, j=0..15, minus dt/2dy*sig_y -> s.W
+//   D  x: HLLC/HLL on faces i=0..16                                     -> s.F
+//   E  owner threads: x part of the conserved and aux-eint update (registers)
+//   F..H the same for y
+//   I  owner threads: y update, energyFix, Eos, store, CFL rate max
+#pragma once
+#include "fxb_device.cuh"
+
+namespace fxb {
+
+struct Args2D {
+    const double *in;
+    double *out;
+    long vstride;            // elements between variables
+    int nx, ny;
+    int bc[4];
+    double dx, dy;
+    double dt_arg;           // used when dtv == nullptr
+    const double *dtv;       // device dt (dtv[0]) for graph-captured loops
+    double gam1inv, ggprodinv;
+    DevParams prm;
+    unsigned long long *rate_max;
+    int *err;
+};
+
+constexpr int T2 = 16;             // tile edge
+constexpr int WIN = T2 + 6;        // window edge
+constexpr int NT2 = 320;           // threads per CTA
+constexpr int NDB = (T2 + 4) * T2; // 320 slope cells
+constexpr int NW = (T2 + 2) * T2;  // 288 face-state cells
+constexpr int NFC = (T2 + 1) * T2; // 272 faces
+
+template <class R> struct Smem2D {
+    R V[8][WIN][WIN];
+    R DBF[NF * NFC];               // slopes [6][NDB], then fluxes [8][NFC]
+    R W[12][NW];                   // Wp (D,VX,VY,VZ,P,EI), then Wm
+};
+
+// rotate a global-order 6-vector (D,VX,VY,VZ,P,EI) into sweep order
+// (D, v_normal, v2, v3, P, EI) with v2/v3 as in hy_eigenVector.F90:67-79
+template <class R> __device__ __forceinline__ void rot(int dir, const R *g, R *r)
+{
+    r[0] = g[0]; r[4] = g[4]; r[5] = g[5];
+    if (dir == 0)      { r[1] = g[1]; r[2] = g[2]; r[3] = g[3]; }
+    else if (dir == 1) { r[1] = g[2]; r[2] = g[3]; r[3] = g[1]; }
+    else               { r[1] = g[3]; r[2] = g[1]; r[3] = g[2]; }
+}
+template <class R> __device__ __forceinline__ void unrot(int dir, const R *r, R *g)
+{
+    g[0] = r[0]; g[4] = r[4]; g[5] = r[5];
+    if (dir == 0)      { g[1] = r[1]; g[2] = r[2]; g[3] = r[3]; }
+    else if (dir == 1) { g[2] = r[1]; g[3] = r[2]; g[1] = r[3]; }
+    else               { g[3] = r[1]; g[1] = r[2]; g[2] = r[3]; }
+}
+
+template <class R> __device__ __forceinline__ void win6(const Smem2D<R> &s, int wx, int wy, R *g)
+{
+    g[0] = s.V[D][wy][wx]; g[1] = s.V[VX][wy][wx]; g[2] = s.V[VY][wy][wx];
+    g[3] = s.V[VZ][wy][wx]; g[4] = s.V[P][wy][wx]; g[5] = s.V[EI][wy][wx];
+}
+
+__device__ __forceinline__ void set_err(int *err, int code) { atomicOr(err, code); }
+
+template <class R>
+__device__ __forceinline__ void slopes_stage(const Args2D &a, Smem2D<R> &s, int dir, int t, int wx, int wy)
+{
+    const int ox = dir == 0, oy = dir == 1;
+    R g[3][6], Vm[6], Vc[6], Vp[6], db[6];
+    win6(s, wx - ox, wy - oy, g[0]); win6(s, wx, wy, g[1]); win6(s, wx + ox, wy + oy, g[2]);
+    rot(dir, g[0], Vm); rot(dir, g[1], Vc); rot(dir, g[2], Vp);
+    Eig<R> e;
+    if (!eigen(Vc[0], Vc[1], Vc[4], s.V[GC][wy][wx], e)) set_err(a.err, ERR_SOUND);
+    tvd_slope(a.prm, e, Vm, Vc, Vp, db);
+#pragma unroll
+    for (int k = 0; k < 6; k++) s.DBF[k * NDB + t] = db[k];
+}
+
+// face states of one cell along dir, with the transverse correction of the
+// other direction (hy_dataReconstOneStep.F90:931-936) and the negativity
+// fallback (:1131-1165); stores global-order Wp/Wm into s.W[.][t].
+template <class R>
+__device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int dir, int t, int wx, int wy,
+                                             int dbi, int dbstep, R dtn, R hdtn, R hdtt)
+{
+    const int ox = dir == 0, oy = dir == 1;
+    R g[6], Vm[6], Vc[6], Vp[6], vecL[6], vecR[6], Wm[6], Wp[6];
+    win6(s, wx, wy, g); rot(dir, g, Vc);
+    Eig<R> e;
+    if (!eigen(Vc[0], Vc[1], Vc[4], s.V[GC][wy][wx], e)) set_err(a.err, ERR_SOUND);
+    if (a.prm.order == 5) {
+        R S[5][6];
+#pragma unroll
+        for (int o = -2; o <= 2; o++) { win6(s, wx + o * ox, wy + o * oy, g); rot(dir, g, S[o + 2]); }
+        weno_interfaces(a.prm, e, S, vecL, vecR);
+#pragma unroll
+        for (int k = 0; k < 6; k++) { Vm[k] = S[1][k]; Vp[k] = S[3][k]; }
+    } else {
+        win6(s, wx - ox, wy - oy, g); rot(dir, g, Vm);
+        win6(s, wx + ox, wy + oy, g); rot(dir, g, Vp);
+        R dbN[6], db0[6], dbP[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            dbN[k] = s.DBF[k * NDB + dbi - dbstep];
+            db0[k] = s.DBF[k * NDB + dbi];
+            dbP[k] = s.DBF[k * NDB + dbi + dbstep];
+        }
+        ppm_interfaces(Vm, Vc, Vp, dbN, db0, dbP, vecL, vecR);
+    }
+    R wm[6], wp[6];
+    ppm_trace(e, dtn, hdtn, Vc, vecL, vecR, wm, wp);
+    unrot(dir, wm, Wm); unrot(dir, wp, Wp);
+    // transverse flux of the other direction at this cell
+    {
+        const int td = 1 - dir, tx = td == 0, ty = td == 1;
+        R m[6], c[6], p[6], sr[6], sg[6];
+        win6(s, wx - tx, wy - ty, g); rot(td, g, m);
+        win6(s, wx, wy, g); rot(td, g, c);
+        win6(s, wx + tx, wy + ty, g); rot(td, g, p);
+        Eig<R> et;
+        if (!eigen(c[0], c[1], c[4], s.V[GC][wy][wx], et)) set_err(a.err, ERR_SOUND);
+        trans_flux(et, m, c, p, a.prm.use_aux_eint != 0, sr);
+        unrot(td, sr, sg);
+#pragma unroll
+        for (int k = 0; k < 6; k++) { Wm[k] = Wm[k] - hdtt * sg[k]; Wp[k] = Wp[k] - hdtt * sg[k]; }
+    }
+    if (Wm[0] < R(0) || Wp[0] < R(0) || Wm[4] < R(0) || Wp[4] < R(0)) {
+        win6(s, wx, wy, g);
+#pragma unroll
+        for (int k = 0; k < 6; k++) { Wm[k] = g[k]; Wp[k] = g[k]; }
+    }
+#pragma unroll
+    for (int k = 0; k < 6; k++) { s.W[k][t] = Wp[k]; s.W[6 + k][t] = Wm[k]; }
+}
+
+template <class R>
+__device__ __forceinline__ void faces_stage(const Args2D &a, Smem2D<R> &s, int dir, int t, int wl, int wr,
+                                            int wxl, int wyl, int wxr, int wyr)
+{
+    R VL[6], VR[6], F[8];
+#pragma unroll
+    for (int k = 0; k < 6; k++) { VL[k] = s.W[k][wl]; VR[k] = s.W[6 + k][wr]; }
+    int e = riemann(a.prm, dir, VL, s.V[GC][wyl][wxl], s.V[GE][wyl][wxl],
+                    VR, s.V[GC][wyr][wxr], s.V[GE][wyr][wxr], F);
+    if (e) set_err(a.err, e);
+#pragma unroll
+    for (int k = 0; k < NF; k++) s.DBF[k * NFC + t] = F[k];
+}
+
+template <class R>
+__global__ void __launch_bounds__(NT2, 1) hydro2d_kernel(const Args2D a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem2D<R> &s = *reinterpret_cast<Smem2D<R> *>(smem_raw);
+    const int tid = threadIdx.x;
+    const int tx0 = blockIdx.x * T2, ty0 = blockIdx.y * T2;
+    const double dt = a.dtv ? a.dtv[0] : a.dt_arg;
+
+    // ---- A: window load with guard cells resolved on the fly
+    for (int e = tid; e < 8 * WIN * WIN; e += NT2) {
+        int v = e / (WIN * WIN), r = e - v * (WIN * WIN);
+        int wy = r / WIN, wx = r - wy * WIN;
+        double sx = 1.0, sy = 1.0;
+        int gx = map_axis(tx0 + wx - 3, a.nx, a.bc[0], a.bc[1], &sx);
+        int gy = map_axis(ty0 + wy - 3, a.ny, a.bc[2], a.bc[3], &sy);
+        double val = __ldg(a.in + v * a.vstride + (long)gy * a.nx + gx);
+        if (v == VX) val = val * sx;
+        if (v == VY) val = val * sy;
+        s.V[v][wy][wx] = (R)val;
+    }
+    __syncthreads();
+
+    const R dtnx = R(dt / a.dx), hdtnx = R(0.5 * (dt / a.dx));
+    const R dtny = R(dt / a.dy), hdtny = R(0.5 * (dt / a.dy));
+    const R hdtx = R(0.5 * dt / a.dx), hdty = R(0.5 * dt / a.dy);
+    const bool ppm = a.prm.order != 5;
+
+    // ---- B: x slopes
+    if (ppm && tid < NDB) {
+        int ii = tid % (T2 + 4) - 2, jj = tid / (T2 + 4);
+        slopes_stage(a, s, 0, tid, ii + 3, jj + 3);
+    }
+    __syncthreads();
+    // ---- C: x face states
+    if (tid < NW) {
+        int ii = tid % (T2 + 2) - 1, jj = tid / (T2 + 2);
+        states_stage(a, s, 0, tid, ii + 3, jj + 3, jj * (T2 + 4) + ii + 2, 1, dtnx, hdtnx, hdty);
+    }
+    __syncthreads();
+    // ---- D: x faces
+    if (tid < NFC) {
+        int fi = tid % (T2 + 1), jj = tid / (T2 + 1);
+        faces_stage(a, s, 0, tid, jj * (T2 + 2) + fi, jj * (T2 + 2) + fi + 1, fi + 2, jj + 3, fi + 3, jj + 3);
+    }
+    __syncthreads();
+
+    // ---- E: owner threads, x part of the update
+    const bool owner = tid < T2 * T2;
+    const int oi = tid % T2, oj = tid / T2;
+    const long gidx = (long)(ty0 + oj) * a.nx + (tx0 + oi);
+    double U0[5], dens0 = 0., Ax = 0., Bx = 0., pav = 0., SphX = 0., eint0 = 0.;
+    const double dtdx = dt / a.dx, dtdy = dt / a.dy;
+    if (owner) {
+        dens0 = __ldg(a.in + D * a.vstride + gidx);
+        double vx = __ldg(a.in + VX * a.vstride + gidx), vy = __ldg(a.in + VY * a.vstride + gidx);
+        double vz = __ldg(a.in + VZ * a.vstride + gidx), en = __ldg(a.in + DV_ENER * a.vstride + gidx);
+        eint0 = __ldg(a.in + EI * a.vstride + gidx);
+        U0[0] = dens0; U0[1] = vx * dens0; U0[2] = vy * dens0; U0[3] = vz * dens0; U0[4] = dens0 * en;
+        int fl = oj * (T2 + 1) + oi, fr = fl + 1;
+#pragma unroll
+        for (int v = 0; v < 5; v++)
+            U0[v] = U0[v] - dtdx * ((double)s.DBF[v * NFC + fr] - (double)s.DBF[v * NFC + fl]);
+        Ax = (double)s.DBF[FEI * NFC + fl] - (double)s.DBF[FEI * NFC + fr];
+        Bx = (double)s.DBF[FVOL * NFC + fl] - (double)s.DBF[FVOL * NFC + fr];
+        SphX = ((double)s.DBF[FP * NFC + fl] - (double)s.DBF[FP * NFC + fr]) * (1.0 - a.prm.fpres) / a.dx;
+        int w = oj * (T2 + 2) + oi + 1;
+        pav = 0.5 * ((double)s.W[6 + P][w] + (double)s.W[P][w]);
+    }
+    __syncthreads();
+
+    // ---- F: y slopes
+    if (ppm && tid < NDB) {
+        int ii = tid % T2, jj = tid / T2 - 2;
+        slopes_stage(a, s, 1, tid, ii + 3, jj + 3);
+    }
+    __syncthreads();
+    // ---- G: y face states
+    if (tid < NW) {
+        int ii = tid % T2, jj = tid / T2 - 1;
+        states_stage(a, s, 1, tid, ii + 3, jj + 3, (jj + 2) * T2 + ii, T2, dtny, hdtny, hdtx);
+    }
+    __syncthreads();
+    // ---- H: y faces
+    if (tid < NFC) {
+        int ii = tid % T2, fj = tid / T2;
+        faces_stage(a, s, 1, tid, fj * T2 + ii, (fj + 1) * T2 + ii, ii + 3, fj + 2, ii + 3, fj + 3);
+    }
+    __syncthreads();
+
+    // ---- I: finish the update, energyFix, Eos, store, CFL rate
+    double rate = 0.;
+    if (owner) {
+        const DevParams &prm = a.prm;
+        int fl = oj * T2 + oi, fr = fl + T2;
+#pragma unroll
+        for (int v = 0; v < 5; v++)
+            U0[v] = U0[v] - dtdy * ((double)s.DBF[v * NFC + fr] - (double)s.DBF[v * NFC + fl]);
+        double Ay = (double)s.DBF[FEI * NFC + fl] - (double)s.DBF[FEI * NFC + fr];
+        double By = (double)s.DBF[FVOL * NFC + fl] - (double)s.DBF[FVOL * NFC + fr];
+        double SphY = ((double)s.DBF[FP * NFC + fl] - (double)s.DBF[FP * NFC + fr]) * (1.0 - prm.fpres) / a.dy;
+        int w = (oj + 1) * T2 + oi;
+        pav = pav * 0.5 + ((double)s.W[6 + P][w] + (double)s.W[P][w]) * 0.25;
+        double inten = 0.;
+        if (prm.use_aux_eint) {
+            inten = dens0 * eint0;
+            inten = inten + dtdx * (Ax + pav * Bx);
+            inten = inten + dtdy * (Ay + pav * By);
+            inten = inten + dt * 0.0;
+        }
+        const double Sph[5] = {0., SphX, SphY, 0., 0.};
+        double momOld[3] = {U0[1], U0[2], U0[3]};
+        (void)momOld;
+#pragma unroll
+        for (int v = 0; v < 5; v++) U0[v] = U0[v] + dt * (0. + Sph[v]);
+        double dens = fmax2(U0[0], prm.small_dens);
+        double vx = U0[1] / dens, vy = U0[2] / dens, vz = U0[3] / dens;
+        double ener = U0[4] / dens;
+        double eint = prm.use_aux_eint ? inten / dens : eint0;
+        // hy_energyFix.F90:240-260
+        double ekin = vx * vx; ekin = ekin + vy * vy; ekin = ekin + vz * vz; ekin = 0.5 * ekin;
+        double ee = ener - ekin - 0.0;
+        double newE = (!prm.use_aux_eint || ee > prm.eint_switch * (ekin + 0.0)) ? fmax2(prm.small_e, ee)
+                                                                                : fmax2(prm.small_e, eint);
+        ener = newE + ekin;
+        eint = newE;
+        // Eos_wrapped(MODE_DENS_EI)
+        double ek2 = 0.5 * (vx * vx + vy * vy + vz * vz);
+        double eg = eint;
+        if (ener - ek2 > fmax2(prm.small_e, prm.eint_switch * ek2)) eg = ener - ek2;
+        double pres = dens * eg * a.gam1inv;
+        double temp = eg * a.ggprodinv * prm.abar;
+        double game = pres / (eg * dens) + 1;
+        double* o = a.out;
+        const long vs = a.vstride;
+        o[D * vs + gidx] = dens; o[VX * vs + gidx] = vx; o[VY * vs + gidx] = vy; o[VZ * vs + gidx] = vz;
+        o[P * vs + gidx] = pres; o[GC * vs + gidx] = prm.gamma; o[GE * vs + gidx] = game;
+        o[EI * vs + gidx] = eg; o[DV_ENER * vs + gidx] = eg + ek2; o[DV_TEMP * vs + gidx] = temp;
+        // Hydro_computeDt.F90:215-222 rate, in FP64
+        double cs = sqrt(prm.gamma * pres / dens);
+        rate = (fabs(vx - 0.) + cs) * (1.0 / a.dx);
+        rate = fmax2(rate, (fabs(vy - 0.) + cs) * (1.0 / a.dy));
+    }
+    // CTA max, then one atomic per CTA (positive doubles order like their bits)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) rate = fmax(rate, __shfl_xor_sync(0xffffffffu, rate, off));
+    __shared__ double red[NT2 / 32];
+    if ((tid & 31) == 0) red[tid >> 5] = rate;
+    __syncthreads();
+    if (tid == 0) {
+        double m = red[0];
+        for (int w = 1; w < NT2 / 32; w++) m = fmax(m, red[w]);
+        atomicMax(a.rate_max, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+} // namespace fxb

@@ -1,0 +1,13 @@
+// FP64 instantiation of the 2-D fused kernel (built with -fmad=false).
+#include "fxb_launch.h"
+namespace fxb {
+cudaError_t setup_hydro2d_fp64()
+{
+    return cudaFuncSetAttribute(hydro2d_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(Smem2D<double>));
+}
+void launch_hydro2d_fp64(const Args2D &a, dim3 grid, cudaStream_t s)
+{
+    hydro2d_kernel<double><<<grid, NT2, sizeof(Smem2D<double>), s>>>(a);
+}
+} // namespace fxb

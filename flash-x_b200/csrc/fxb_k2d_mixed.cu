@@ -1,0 +1,15 @@
+// Mixed-precision instantiation of the 2-D fused kernel: FP32 reconstruction,
+// characteristic projection and Riemann solve; FP64 conserved update,
+// internal-energy recovery, Eos and CFL rate.
+#include "fxb_launch.h"
+namespace fxb {
+cudaError_t setup_hydro2d_mixed()
+{
+    return cudaFuncSetAttribute(hydro2d_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(Smem2D<float>));
+}
+void launch_hydro2d_mixed(const Args2D &a, dim3 grid, cudaStream_t s)
+{
+    hydro2d_kernel<float><<<grid, NT2, sizeof(Smem2D<float>), s>>>(a);
+}
+} // namespace fxb

@@ -1,0 +1,19 @@
+// fxb_launch.h -- launchers of the fused hydro kernels.  Each precision lives
+// in its own translation unit so that the FP64 path can be compiled with
+// -fmad=false (every product and sum rounded as written, matching the
+// oracle bit for bit) while the mixed path keeps fused multiply-adds.
+#pragma once
+#include <cuda_runtime.h>
+#include "fxb_hydro2d.cuh"
+#include "fxb_hydro3d.cuh"
+
+namespace fxb {
+cudaError_t setup_hydro2d_fp64();
+cudaError_t setup_hydro2d_mixed();
+void launch_hydro2d_fp64(const Args2D &a, dim3 grid, cudaStream_t s);
+void launch_hydro2d_mixed(const Args2D &a, dim3 grid, cudaStream_t s);
+cudaError_t setup_hydro3d_fp64();
+cudaError_t setup_hydro3d_mixed();
+void launch_hydro3d_fp64(const Args3D &a, cudaStream_t s);
+void launch_hydro3d_mixed(const Args3D &a, cudaStream_t s);
+} // namespace fxb

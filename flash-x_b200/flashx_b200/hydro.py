@@ -1,0 +1,257 @@
+"""Host-side mirror of the Flash-X hydro interface over libflashx_b200.so.
+
+The reference's Fortran driver calls Hydro(simTime, dt, dtOld) once per step
+(FX/physics/Hydro/Hydro_interface.F90, impl unsplit/levelFlux/Hydro.F90:20),
+Hydro_computeDt per leaf block from Driver_computeDt (unsplit/
+Hydro_computeDt.F90:28-34, reduced by MPI_AllReduce MIN in
+Driver/DriverMain/Driver_computeDt.F90:373,383) and Grid_fillGuardCells before
+any stencil use (Grid/Grid_fillGuardCells.F90:283).  `HydroDevice` exposes the
+same three operations with the same argument meaning; the work runs in the
+CUDA library (ctypes, plain C ABI).  There is no CPU fallback: if the library
+or a GPU is missing every call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from .params import Geometry, HydroParams, NUNK, UNK_VARS
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.normpath(os.path.join(HERE, "..", "libflashx_b200.so"))
+BUILD_DIR = os.path.normpath(os.path.join(HERE, ".."))
+
+FXB_OK, FXB_EARG, FXB_ECUDA, FXB_ESOUND, FXB_ERIEMANN, FXB_EDT, FXB_EUNSUPPORTED = range(7)
+FXB_FP64, FXB_MIXED = 0, 1
+# enum fxb_var order of include/flashx_b200.h
+FXB_VARS = ("dens", "eint", "ener", "gamc", "game", "pres", "temp", "velx", "vely", "velz")
+
+# entry points declared in include/flashx_b200.h
+ABI_SYMBOLS = ("fxb_init", "fxb_register_blocks", "fxb_attach_unk", "fxb_fill_guardcells",
+               "fxb_hydro_step", "fxb_compute_dt", "fxb_advance", "fxb_eos", "fxb_sync_to_host",
+               "fxb_sync_from_host", "fxb_integrals", "fxb_last_timing", "fxb_stream",
+               "fxb_last_error", "fxb_finalize")
+
+
+class FxbParams(ctypes.Structure):
+    _fields_ = [
+        ("order", ctypes.c_int), ("weno_method", ctypes.c_int), ("riemann", ctypes.c_int),
+        ("limiter", ctypes.c_int), ("char_limiting", ctypes.c_int), ("use_3d_full_ctu", ctypes.c_int),
+        ("use_aux_eint", ctypes.c_int), ("use_gravity", ctypes.c_int),
+        ("grav", ctypes.c_double * 3),
+        ("cfl", ctypes.c_double), ("gamma", ctypes.c_double), ("eint_switch", ctypes.c_double),
+        ("small_dens", ctypes.c_double), ("small_e", ctypes.c_double), ("small_p", ctypes.c_double),
+        ("tiny", ctypes.c_double), ("fpres", ctypes.c_double), ("limited_beta", ctypes.c_double),
+        ("gas_constant", ctypes.c_double), ("abar", ctypes.c_double),
+        ("precision", ctypes.c_int),
+    ]
+
+
+class FxbDomain(ctypes.Structure):
+    _fields_ = [
+        ("ndim", ctypes.c_int), ("nxb", ctypes.c_int), ("nyb", ctypes.c_int), ("nzb", ctypes.c_int),
+        ("nguard", ctypes.c_int), ("nblockx", ctypes.c_int), ("nblocky", ctypes.c_int),
+        ("nblockz", ctypes.c_int), ("bbox", (ctypes.c_double * 2) * 3), ("bc", ctypes.c_int * 6),
+    ]
+
+
+class FxbBlockDesc(ctypes.Structure):
+    _fields_ = [("level", ctypes.c_int), ("bcoord", ctypes.c_int * 3)]
+
+
+class FxbError(ctypes.Structure):
+    _fields_ = [("code", ctypes.c_int), ("message", ctypes.c_char * 256)]
+
+
+class FlashXError(RuntimeError):
+    """Raised where the reference would call Driver_abort."""
+
+    def __init__(self, code, message):
+        super().__init__(f"[flashx_b200 error {code}] {message}")
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FlashXError(FXB_ECUDA, f"{path} not found: build it with `make -C {BUILD_DIR}`")
+    L = ctypes.CDLL(path)
+    D = ctypes.POINTER(ctypes.c_double)
+    I32 = ctypes.POINTER(ctypes.c_int32)
+    L.fxb_init.argtypes = [ctypes.POINTER(FxbParams), ctypes.POINTER(FxbDomain), I32, ctypes.c_int]
+    L.fxb_register_blocks.argtypes = [ctypes.POINTER(FxbBlockDesc), ctypes.c_int]
+    L.fxb_attach_unk.argtypes = [D]
+    L.fxb_fill_guardcells.argtypes = [D]
+    L.fxb_hydro_step.argtypes = [ctypes.c_double] * 3
+    L.fxb_compute_dt.argtypes = [D, I32]
+    L.fxb_advance.argtypes = [ctypes.c_int, D, D, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    L.fxb_eos.argtypes = []
+    L.fxb_sync_to_host.argtypes = [D]
+    L.fxb_sync_from_host.argtypes = [D]
+    L.fxb_integrals.argtypes = [D]
+    L.fxb_last_timing.argtypes = [D, ctypes.POINTER(ctypes.c_int)]
+    L.fxb_stream.restype = ctypes.c_void_p
+    L.fxb_last_error.argtypes = [ctypes.POINTER(FxbError)]
+    L.fxb_finalize.restype = None
+    for name in ABI_SYMBOLS:
+        if name not in ("fxb_stream", "fxb_finalize"):
+            getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != FXB_OK:
+        err = FxbError()
+        _lib.fxb_last_error(ctypes.byref(err))
+        raise FlashXError(rc, err.message.decode(errors="replace"))
+
+
+def _dp(a):
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("UNK must be a C-contiguous float64 array (Fortran unk(var,i,j,k,blk))")
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def make_fxb_params(hp: HydroParams, precision="fp64"):
+    hp.validate()
+    p = FxbParams()
+    p.order = hp.order
+    p.weno_method = 2 if hp.wenoMethod.upper() == "WENOZ" else 1
+    p.riemann = 4 if hp.RiemannSolver.upper() == "HLLC" else 3
+    p.limiter = {"minmod": 1, "mc": 2, "vanleer": 3, "hybrid": 4, "limited": 5}[hp.slopeLimiter.lower()]
+    p.char_limiting = int(hp.charLimiting)
+    p.use_3d_full_ctu = int(hp.use_3dFullCTU)
+    p.use_aux_eint = int(hp.use_auxEintEqn)
+    p.use_gravity = int(hp.useGravity)
+    for i in range(3):
+        p.grav[i] = hp.gravity[i]
+    p.cfl, p.gamma, p.eint_switch = hp.cfl, hp.gamma, hp.eintSwitch
+    p.small_dens, p.small_e, p.small_p, p.tiny = hp.smlrho, hp.smalle, hp.smallp, hp.tiny
+    p.fpres, p.limited_beta = hp.hy_fPresInMomFlux, hp.LimitedSlopeBeta
+    p.gas_constant, p.abar = hp.gasConstant, hp.eos_singleSpeciesA
+    p.precision = {"fp64": FXB_FP64, "mixed": FXB_MIXED}[precision]
+    return p
+
+
+def make_fxb_domain(geom: Geometry):
+    d = FxbDomain()
+    d.ndim, d.nxb, d.nyb, d.nzb, d.nguard = geom.ndim, geom.nxb, geom.nyb, geom.nzb, geom.nguard
+    d.nblockx, d.nblocky, d.nblockz = geom.nblockx, geom.nblocky, geom.nblockz
+    for a in range(3):
+        d.bbox[a][0], d.bbox[a][1] = geom.bbox[a]
+    for i in range(6):
+        d.bc[i] = geom.bc[i]
+    return d
+
+
+def default_var_map():
+    """0-based UNK slots (Simulation.h *_VAR - 1) of the UHD + Gamma setup."""
+    vm = (ctypes.c_int32 * len(FXB_VARS))()
+    for i, name in enumerate(FXB_VARS):
+        vm[i] = UNK_VARS.index(name)
+    return vm
+
+
+def leaf_blocks(geom: Geometry):
+    """Leaf-block list of a uniform block grid in Flash-X block order."""
+    n = geom.nblocks
+    arr = (FxbBlockDesc * n)()
+    b = 0
+    for bz in range(geom.nblockz if geom.ndim == 3 else 1):
+        for by in range(geom.nblocky if geom.ndim >= 2 else 1):
+            for bx in range(geom.nblockx):
+                arr[b].level = 1
+                arr[b].bcoord[0], arr[b].bcoord[1], arr[b].bcoord[2] = bx, by, bz
+                b += 1
+    return arr
+
+
+class HydroDevice:
+    """The unsplit hydro solver on one B200, behind the reference interface."""
+
+    def __init__(self, geom: Geometry, hp: HydroParams, precision="fp64"):
+        self.lib = load_library()
+        self.geom, self.hp, self.precision = geom, hp, precision
+        self._p = make_fxb_params(hp, precision)
+        self._d = make_fxb_domain(geom)
+        self._vm = default_var_map()
+        _check(self.lib.fxb_init(ctypes.byref(self._p), ctypes.byref(self._d), self._vm, NUNK))
+        blocks = leaf_blocks(geom)
+        _check(self.lib.fxb_register_blocks(blocks, geom.nblocks))
+        self.unk = None
+
+    # ---- data movement
+    def attach_unk(self, unk):
+        """Take the host UNK (Fortran unk(var,i,j,k,blk) as a C-order array)."""
+        if unk.shape != self.geom.unk_shape:
+            raise ValueError(f"UNK shape {unk.shape} != {self.geom.unk_shape}")
+        self.unk = unk
+        _check(self.lib.fxb_attach_unk(_dp(unk)))
+
+    def sync_to_host(self, unk=None):
+        unk = self.unk if unk is None else unk
+        _check(self.lib.fxb_sync_to_host(_dp(unk)))
+        return unk
+
+    # ---- the reference interface
+    def Grid_fillGuardCells(self, unk=None):
+        """Fill the guard cells (and interiors) of the host UNK from the device."""
+        unk = self.unk if unk is None else unk
+        _check(self.lib.fxb_fill_guardcells(_dp(unk)))
+        return unk
+
+    def Hydro(self, simTime, dt, dtOld):
+        _check(self.lib.fxb_hydro_step(float(simTime), float(dt), float(dtOld)))
+
+    def Hydro_computeDt(self):
+        """Global CFL time step of the current state (min over blocks)."""
+        out = ctypes.c_double()
+        loc = (ctypes.c_int32 * 5)()
+        _check(self.lib.fxb_compute_dt(ctypes.byref(out), loc))
+        return out.value
+
+    def Eos_wrapped(self):
+        _check(self.lib.fxb_eos())
+
+    # ---- driver helpers
+    def advance(self, nsteps, dt, dt_old):
+        """nsteps of Hydro + Driver_computeDt on the device (CUDA graph)."""
+        a, b = ctypes.c_double(dt), ctypes.c_double(dt_old)
+        hp = self.hp
+        _check(self.lib.fxb_advance(int(nsteps), ctypes.byref(a), ctypes.byref(b),
+                                    hp.tstep_change_factor, hp.dtmin, hp.dtmax))
+        return a.value, b.value
+
+    def integrals(self):
+        out = np.zeros(7)
+        _check(self.lib.fxb_integrals(_dp(out)))
+        return out
+
+    def last_timing(self):
+        ms = ctypes.c_double()
+        n = ctypes.c_int()
+        _check(self.lib.fxb_last_timing(ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+    def close(self):
+        self.lib.fxb_finalize()
+
+
+def driver_dt(dt_cfl, dt_old, hp: HydroParams):
+    """Driver_computeDt.F90:452,460: growth limit, then clamp."""
+    dt_new = dt_cfl if dt_cfl < dt_old * hp.tstep_change_factor else dt_old * hp.tstep_change_factor
+    dt_new = dt_new if dt_new > hp.dtmin else hp.dtmin
+    return dt_new if dt_new < hp.dtmax else hp.dtmax
+
+
+def initial_dt(dt_cfl, hp: HydroParams):
+    """Driver_verifyInitDt.F90:234-250."""
+    slow = 0.1
+    return slow * dt_cfl if hp.dtinit > slow * dt_cfl else hp.dtinit

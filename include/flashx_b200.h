@@ -1,0 +1,145 @@
+/*
+ * flashx_b200.h -- C ABI of libflashx_b200.so, the B200 (sm_100a) drop-in for
+ * the Flash-X unsplit compressible-hydro hot path.
+ *
+ * Plain C types only: the Fortran driver binds these with ISO_C_BINDING
+ * (see INTEGRATION.md), Python with ctypes.  Every function returns an int
+ * status: FXB_OK (0) or one of the FXB_E* codes; fxb_last_error() gives the
+ * message.  The library never calls exit() or abort().
+ *
+ * Reference interfaces replaced (paths inside the Flash-X project):
+ *   Hydro(simTime, dt, dtOld)                 source/physics/Hydro/Hydro_interface.F90,
+ *                                             impl .../HydroMain/unsplit/levelFlux/Hydro.F90:20
+ *   Hydro_computeDt(tileDesc, ..., U, dtCheck, dtMinLoc, extraInfo)
+ *                                             .../HydroMain/unsplit/Hydro_computeDt.F90:28-34
+ *   Grid_fillGuardCells(gridDataStruct, idir, ...)
+ *                                             source/Grid/Grid_fillGuardCells.F90:283,
+ *                                             impl source/Grid/GridMain/UG/Grid_fillGuardCells.F90
+ *   Eos_wrapped(MODE_DENS_EI, range, U)       source/physics/Eos/EosMain/Eos_wrapped.F90:60-189
+ *   IO_writeIntegralQuantities sums           source/IO/IOMain/IO_writeIntegralQuantities.F90:60-224
+ *
+ * Data contract: the caller owns unk(var,i,j,k,blk) in host memory (FP64,
+ * Fortran order, NGUARD guard cells per side, var_map giving the 0-based
+ * slot of each UHD variable as Simulation.h's *_VAR - 1).  The library
+ * keeps a device mirror in its own layout (one FP64 array per variable over
+ * the whole uniform grid) and all scratch; steady-state steps never cross
+ * PCIe.  Single host thread, not re-entrant; one CUDA stream per library
+ * instance.
+ */
+#ifndef FLASHX_B200_H
+#define FLASHX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define FXB_OK              0
+#define FXB_EARG            1   /* bad argument or call order */
+#define FXB_ECUDA           2   /* CUDA runtime error (no device, launch failure, OOM) */
+#define FXB_ESOUND          3   /* zero or imaginary sound speed (hy_eigenParameters.F90:94-100) */
+#define FXB_ERIEMANN        4   /* Riemann solver ierr (hy_getFaceFlux.F90:337-378) */
+#define FXB_EDT             5   /* computed dt not positive (Hydro_computeDt.F90:286-288) */
+#define FXB_EUNSUPPORTED    6   /* option combination this path does not implement */
+
+/* variables of the UHD + Gamma solution vector, used to index var_map */
+enum fxb_var { FXB_DENS = 0, FXB_EINT, FXB_ENER, FXB_GAMC, FXB_GAME, FXB_PRES,
+               FXB_TEMP, FXB_VELX, FXB_VELY, FXB_VELZ, FXB_NVAR };
+
+enum fxb_bc { FXB_BC_PERIODIC = 0, FXB_BC_OUTFLOW = 1, FXB_BC_REFLECTING = 2 };
+enum fxb_precision { FXB_FP64 = 0, FXB_MIXED = 1 };   /* MIXED: FP32 reconstruction and
+                                                          Riemann solve, FP64 update/eint/sums/dt */
+
+/* Resolved runtime parameters (names as in the Flash-X Config files). */
+typedef struct fxb_params {
+    int    order;              /* 3 = PPM, 5 = WENO                                  */
+    int    weno_method;        /* 1 = WENO5, 2 = WENOZ                               */
+    int    riemann;            /* 3 = HLL, 4 = HLLC (UHD.h numbering)                */
+    int    limiter;            /* 1 minmod, 2 mc, 3 vanLeer, 4 hybrid, 5 limited     */
+    int    char_limiting;      /* charLimiting                                       */
+    int    use_3d_full_ctu;    /* use_3dFullCTU                                      */
+    int    use_aux_eint;       /* use_auxEintEqn                                     */
+    int    use_gravity;        /* constant gravity (Gravity/GravityMain/Constant)    */
+    double grav[3];
+    double cfl, gamma, eint_switch, small_dens, small_e, small_p, tiny;
+    double fpres;              /* hy_fPresInMomFlux                                  */
+    double limited_beta;       /* LimitedSlopeBeta                                   */
+    double gas_constant, abar; /* Eos Gamma: ideal gas constant, eos_singleSpeciesA  */
+    int    precision;          /* enum fxb_precision                                 */
+} fxb_params;
+
+/* Domain of a uniform block grid. */
+typedef struct fxb_domain {
+    int    ndim;               /* 2 or 3 */
+    int    nxb, nyb, nzb;      /* block interior (nzb = 1 in 2-D) */
+    int    nguard;             /* NGUARD (4) */
+    int    nblockx, nblocky, nblockz;
+    double bbox[3][2];         /* xmin xmax, ymin ymax, zmin zmax */
+    int    bc[6];              /* xl xr yl yr zl zr, enum fxb_bc */
+} fxb_domain;
+
+/* One leaf block: its position in the uniform block grid (0-based block
+ * coordinates).  Flash-X's blkLimits follow from it; refinement level 1. */
+typedef struct fxb_block_desc {
+    int    level;
+    int    bcoord[3];
+} fxb_block_desc;
+
+typedef struct fxb_error {
+    int    code;
+    char   message[256];
+} fxb_error;
+
+/* Hydro_init + Grid_init: resolve parameters, select the device, allocate the
+ * device mirror.  var_map[FXB_NVAR] gives each variable's 0-based slot in a
+ * UNK cell vector of nunk doubles. */
+int fxb_init(const fxb_params *params, const fxb_domain *domain,
+             const int32_t *var_map, int nunk);
+/* The leaf-block list (Grid_getTileIterator(LEAF)); nblk must cover the grid. */
+int fxb_register_blocks(const fxb_block_desc *blocks, int nblk);
+/* Copy the host UNK (all blocks, guard cells included) into the device mirror. */
+int fxb_attach_unk(const double *unk_host);
+/* Grid_fillGuardCells(CENTER, ALLDIR): the device mirror has no stored guard
+ * cells (the hydro kernel resolves neighbour and boundary cells on load), so
+ * this writes the filled guard cells, with the interiors, into unk_host. */
+int fxb_fill_guardcells(double *unk_host);
+/* Hydro(simTime, dt, dtOld): one unsplit step of every leaf block on the
+ * device (guard resolution, reconstruction, Riemann solve, conserved update,
+ * energyFix, Eos), followed on the device by the CFL reduction that
+ * fxb_compute_dt reports. */
+int fxb_hydro_step(double sim_time, double dt, double dt_old);
+/* Hydro_computeDt reduced over all blocks (Driver_computeDt's MPI_AllReduce
+ * MIN of the per-block dtCheck): the CFL time step of the current state.
+ * loc[5] receives i, j, k (1-based block-local, guard offset included),
+ * level and block id of a limiting cell when loc is not NULL. */
+int fxb_compute_dt(double *dt_out, int32_t loc[5]);
+/* Driver loop on the device: nsteps of Hydro + Driver_computeDt dt control
+ * (dtNew = min(dtCFL, tstep_change_factor*dtOld), clamped to [dtmin, dtmax]),
+ * captured once as a CUDA graph.  *dt and *dt_old are read and updated. */
+int fxb_advance(int nsteps, double *dt, double *dt_old, double tstep_change_factor,
+                double dtmin, double dtmax);
+/* Eos_wrapped(MODE_DENS_EI) on all block interiors of the device mirror. */
+int fxb_eos(void);
+/* Copy the device mirror back into unk_host (interiors and guard cells). */
+int fxb_sync_to_host(double *unk_host);
+/* Re-read unk_host after a host-side write (init, restart, regrid). */
+int fxb_sync_from_host(const double *unk_host);
+/* Volume integrals: mass, x/y/z momentum, total, internal, kinetic energy. */
+int fxb_integrals(double out[7]);
+/* Device time of the last fxb_hydro_step / fxb_advance, measured with CUDA
+ * events on the library stream (milliseconds), and the number of kernel
+ * launches it made. */
+int fxb_last_timing(double *ms, int *kernel_launches);
+/* The library's CUDA stream (cudaStream_t), for callers that order their own
+ * work after the library's. */
+void *fxb_stream(void);
+int fxb_last_error(fxb_error *err);
+void fxb_finalize(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLASHX_B200_H */

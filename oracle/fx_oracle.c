@@ -953,4 +953,20 @@ int fxo_integrals(const fxo_params *p, const double *unk, double out[7])
 
 double fxo_flops_last_step(void) { return 0.; }
 
+int fxo_riemann(const fxo_params *p, int dir, const double VL[8], const double VR[8], double F[8])
+{
+    double vl[H_NV], vr[H_NV], Fs[6], speed;
+    for (int k = 0; k < 8; k++) { vl[k] = VL[k]; vr[k] = VR[k]; }
+    vl[H_GR] = 0.; vr[H_GR] = 0.;
+    int err = (p->riemann == FXO_HLL) ? riemann_hll(p, dir, vl, vr, Fs, &speed)
+                                      : riemann_hllc(p, dir, vl, vr, Fs, &speed);
+    if (err) return err;
+    for (int k = 0; k < 6; k++) F[k] = Fs[k];
+    if (p->use_aux_eint) {
+        if (F[F_D] > 0.) { F[F_VOL] = F[F_D] / vl[H_D]; F[F_EI] = F[F_D] * vl[H_EI]; }
+        else             { F[F_VOL] = F[F_D] / vr[H_D]; F[F_EI] = F[F_D] * vr[H_EI]; }
+    } else { F[F_VOL] = 0.; F[F_EI] = 0.; }
+    return 0;
+}
+
 #include "fx_oracle_weno.inc"

@@ -78,6 +78,10 @@ double fxo_driver_dt(double dt_cfl, double dt_old, double tstep_change_factor,
 /* Volume integrals of mass, x/y/z momentum, total energy, internal energy,
  * kinetic energy (IO_writeIntegralQuantities.F90:60-224). */
 int fxo_integrals(const fxo_params *p, const double *unk, double out[7]);
+/* One Riemann problem (hy_HLLC / hy_HLL + the aux-eint fluxes of
+ * hy_getFaceFlux.F90:444-453).  V = dens velx vely velz pres gamc game eint;
+ * F = dens xmom ymom zmom ener pres eint volume fluxes.  Returns ierr. */
+int fxo_riemann(const fxo_params *p, int dir, const double VL[8], const double VR[8], double F[8]);
 /* Number of flops counted by the instrumented build (0 otherwise). */
 double fxo_flops_last_step(void);
 

@@ -69,6 +69,7 @@ def lib():
         L.fxo_driver_dt.argtypes = [ctypes.c_double] * 5
         L.fxo_driver_dt.restype = ctypes.c_double
         L.fxo_integrals.argtypes = [P, D, D]
+        L.fxo_riemann.argtypes = [P, ctypes.c_int, D, D, D]
         _lib = L
     return _lib
 
@@ -137,3 +138,14 @@ def integrals(p, unk):
     out = np.zeros(7)
     lib().fxo_integrals(ctypes.byref(p), _dp(unk), _dp(out))
     return out
+
+
+def riemann(p, direction, VL, VR):
+    """Flux of one Riemann problem; VL/VR = dens velx vely velz pres gamc game eint."""
+    vl = np.ascontiguousarray(VL, dtype=np.float64)
+    vr = np.ascontiguousarray(VR, dtype=np.float64)
+    F = np.zeros(8)
+    rc = lib().fxo_riemann(ctypes.byref(p), direction, _dp(vl), _dp(vr), _dp(F))
+    if rc:
+        raise RuntimeError("Riemann solver ierr")
+    return F

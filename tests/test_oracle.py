@@ -1,0 +1,244 @@
+"""CPU tests of the oracle (the checker the CUDA path is compared with).
+
+The reference ships no golden vectors for this path (its Comparison-test
+checkpoints live off-tree), so the oracle is pinned by known answers:
+the exact Sod solution (Sod/shocktube.pro), hand Riemann problems, Eos
+identities, guard-cell semantics and conservation, plus committed fixtures
+that guard it against regressions (tests/golden/gen_golden.py).
+"""
+import math
+import sys
+import os
+
+import numpy as np
+import pytest
+
+from flashx_b200 import simulations as S
+from flashx_b200.params import (BC_OUTFLOW, BC_PERIODIC, BC_REFLECTING, DENS, EINT, ENER, GAMC, GAME,
+                                Geometry, HydroParams, PRES, TEMP, VELX, VELY)
+from exact_sod import sod_exact
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def run_oracle(O, geom, hp, unk, tmax=None, nsteps=None):
+    p = O.make_params(geom.as_dict(), hp)
+    dt_cfl = O.compute_dt(p, unk)
+    dt = 0.1 * dt_cfl if hp.dtinit > 0.1 * dt_cfl else hp.dtinit
+    dt_old = dt
+    t, n = 0.0, 0
+    while (tmax is None or t < tmax) and (nsteps is None or n < nsteps):
+        if tmax is not None and t + dt > tmax:
+            dt = tmax - t
+        O.hydro_step(p, unk, dt, dt_old)
+        t += dt
+        n += 1
+        dt_old = dt
+        dt = O.driver_dt(O.compute_dt(p, unk), dt_old)
+    return t, n
+
+
+def test_sod_2d_matches_exact_solution(oracle):
+    """2-D Sod at 45 degrees, 128^2: density along the diagonal vs the exact
+    solution at t=0.2 (the analytic check of Sod/shocktube.pro, soderror.pro)."""
+    geom = Geometry(2, 16, 16, 1, 8, 8, 1, bc=(BC_OUTFLOW,) * 6)
+    hp = HydroParams()
+    unk = S.sod(geom, hp)
+    t, n = run_oracle(oracle, geom, hp, unk, tmax=0.2)
+    assert abs(t - 0.2) < 1e-12 and n > 50
+    g = S.gather_global(geom, unk)[0]
+    N = g.shape[0]
+    dx = 1.0 / N
+    idx = np.arange(N)
+    x = (idx + 0.5) * dx
+    xi = (2 * x - 1.0) / math.sqrt(2.0) + 0.5          # coordinate along the tube normal
+    rho_ex, u_ex, p_ex = sod_exact(xi, 0.2)
+    rho = g[idx, idx, DENS]
+    pres = g[idx, idx, PRES]
+    vn = (g[idx, idx, VELX] + g[idx, idx, VELY]) / math.sqrt(2.0)
+    keep = (xi > 0.05) & (xi < 0.95)
+    l1 = lambda a, b: np.mean(np.abs(a[keep] - b[keep]))
+    assert l1(rho, rho_ex) < 0.01
+    assert l1(pres, p_ex) < 0.01
+    assert l1(vn, u_ex) < 0.02
+    # plateau values between contact and shock
+    mid = (xi > 0.74) & (xi < 0.80)
+    assert np.allclose(rho[mid], 0.26557, atol=5e-3)
+    assert np.allclose(pres[mid], 0.30313, atol=3e-3)
+
+
+def test_conservation_periodic_kh(oracle):
+    """Mass, momentum and total energy are conserved to roundoff on a periodic domain."""
+    geom = Geometry(2, 16, 16, 1, 4, 4, 1, bc=(BC_PERIODIC,) * 6)
+    hp = HydroParams()
+    unk = S.kelvin_helmholtz(geom, hp)
+    p = oracle.make_params(geom.as_dict(), hp)
+    I0 = oracle.integrals(p, unk)
+    run_oracle(oracle, geom, hp, unk, nsteps=20)
+    I1 = oracle.integrals(p, unk)
+    assert abs(I1[0] - I0[0]) / I0[0] < 1e-13
+    assert abs(I1[1] - I0[1]) < 1e-13 * I0[0]
+    assert abs(I1[4] - I0[4]) / I0[4] < 1e-13
+
+
+def test_eos_dens_ei_identities(oracle):
+    geom = Geometry(2, 16, 16, 1, 2, 2, 1)
+    hp = HydroParams()
+    unk = S.kelvin_helmholtz(geom, hp)
+    p = oracle.make_params(geom.as_dict(), hp)
+    oracle.eos_interior(p, unk)
+    g = S.gather_global(geom, unk)[0]
+    assert np.allclose(g[..., PRES], (hp.gamma - 1) * g[..., DENS] * g[..., EINT], rtol=1e-14)
+    assert np.allclose(g[..., GAME], hp.gamma, rtol=1e-14)
+    assert np.all(g[..., GAMC] == hp.gamma)
+    ekin = 0.5 * (g[..., VELX] ** 2 + g[..., VELY] ** 2)
+    assert np.allclose(g[..., ENER], g[..., EINT] + ekin, rtol=1e-14)
+    assert np.allclose(g[..., TEMP], g[..., EINT] * (hp.gamma - 1) / hp.gasConstant, rtol=1e-13)
+
+
+def _state(rho, u, v, w, p, g=1.4):
+    return np.array([rho, u, v, w, p, g, g, p / ((g - 1) * rho)])
+
+
+def _phys_flux(V, d, g=1.4):
+    rho, vel, p = V[0], V[1:4], V[4]
+    E = 0.5 * rho * np.dot(vel, vel) + p / (g - 1)
+    F = np.zeros(6)
+    F[0] = rho * vel[d]
+    F[1:4] = rho * vel[d] * vel
+    F[1 + d] += p
+    F[4] = (E + p) * vel[d]
+    F[5] = p
+    return F
+
+
+@pytest.mark.parametrize("solver", ["HLLC", "HLL"])
+def test_riemann_known_answers(oracle, solver):
+    geom = Geometry(2, 16, 16, 1, 1, 1, 1)
+    hp = HydroParams(RiemannSolver=solver)
+    p = oracle.make_params(geom.as_dict(), hp)
+    # identical states: the physical flux
+    V = _state(1.3, 0.2, -0.1, 0.05, 0.9)
+    for d in range(3):
+        F = oracle.riemann(p, d, V, V)
+        assert np.allclose(F[:6], _phys_flux(V, d), rtol=1e-14, atol=1e-15)
+    # supersonic to the right: upwind flux of the left state
+    VL, VR = _state(1.0, 5.0, 0, 0, 1.0), _state(0.5, 4.0, 0, 0, 0.3)
+    F = oracle.riemann(p, 0, VL, VR)
+    assert np.allclose(F[:6], _phys_flux(VL, 0), rtol=1e-14)
+    # aux-eint fluxes follow the mass flux upwind (hy_getFaceFlux.F90:444-453)
+    assert F[7] == pytest.approx(F[0] / VL[0]) and F[6] == pytest.approx(F[0] * VL[7])
+    # stationary contact: HLLC resolves it exactly (zero mass flux), HLL diffuses it
+    VL, VR = _state(1.0, 0, 0, 0, 1.0), _state(0.1, 0, 0, 0, 1.0)
+    F = oracle.riemann(p, 0, VL, VR)
+    if solver == "HLLC":
+        assert F[0] == 0.0 and F[1] == pytest.approx(1.0, rel=1e-15)
+    else:
+        assert F[0] > 1e-3
+    # vacuum guard returns zero flux
+    VL = _state(1e-40, 0, 0, 0, 1.0)
+    F = oracle.riemann(p, 0, VL, VR)
+    assert np.all(F[:6] == 0.0)
+    # imaginary sound speed is an error (ierr=1)
+    bad = _state(1.0, 0, 0, 0, 1.0)
+    bad[5] = -1.4
+    with pytest.raises(RuntimeError):
+        oracle.riemann(p, 0, bad, VR)
+
+
+@pytest.mark.parametrize("bc", [BC_OUTFLOW, BC_REFLECTING, BC_PERIODIC])
+def test_guardcell_fill_semantics(oracle, bc):
+    """Grid_fillGuardCells: outflow copies the first interior cell, reflecting
+    mirrors and flips the normal velocity, periodic wraps
+    (Grid_bcApplyToRegion.F90:458-531, UG/gr_shiftData.F90)."""
+    geom = Geometry(2, 16, 16, 1, 2, 2, 1, bc=(bc,) * 6)
+    rng = np.random.default_rng(1)
+    unk = S.scatter_global(geom, rng.random((1, 32, 32, 11)) + 0.5)
+    glob = S.gather_global(geom, unk)[0]
+    p = oracle.make_params(geom.as_dict(), HydroParams())
+    oracle.fill_guardcells(p, unk)
+    blk0 = unk[0, 0]           # block at the low-x, low-y corner; (j, i, var), guard 4
+    # low-x guard column i=3 (one cell outside) at interior row j=4..19
+    col = blk0[4:20, 3, :]
+    if bc == BC_OUTFLOW:
+        assert np.array_equal(col, glob[0:16, 0, :])
+    elif bc == BC_REFLECTING:
+        ref = glob[0:16, 0, :].copy()
+        ref[:, VELX] *= -1
+        assert np.array_equal(col, ref)
+    else:
+        assert np.array_equal(col, glob[0:16, 31, :])
+    # interior-block boundary: block 1 (bx=1) guard column i=3 holds block 0's last column
+    assert np.array_equal(unk[1, 0][4:20, 3, :], glob[0:16, 15, :])
+    # corner guard (3,3) of block 0
+    c = blk0[3, 3, :]
+    if bc == BC_OUTFLOW:
+        assert np.array_equal(c, glob[0, 0, :])
+    elif bc == BC_PERIODIC:
+        assert np.array_equal(c, glob[31, 31, :])
+    else:
+        ref = glob[0, 0, :].copy()
+        ref[VELX] *= -1
+        ref[VELY] *= -1
+        assert np.array_equal(c, ref)
+
+
+def test_driver_dt_control(oracle):
+    # Driver_computeDt.F90:452,460
+    assert oracle.driver_dt(1.0, 0.1) == pytest.approx(0.2)
+    assert oracle.driver_dt(0.15, 0.1) == 0.15
+    assert oracle.driver_dt(1e-20, 0.1) == 1e-10
+    from flashx_b200.hydro import driver_dt, initial_dt
+    hp = HydroParams()
+    for a, b in [(1.0, 0.1), (0.15, 0.1), (1e-20, 0.1)]:
+        assert driver_dt(a, b, hp) == oracle.driver_dt(a, b)
+    assert initial_dt(1.0, hp) == 1e-10 and initial_dt(1e-12, hp) == pytest.approx(1e-13)
+
+
+def test_weno_and_hll_paths_run_and_conserve(oracle):
+    geom = Geometry(2, 16, 16, 1, 2, 2, 1, bc=(BC_PERIODIC,) * 6)
+    for hp in (HydroParams(order=5), HydroParams(order=5, wenoMethod="WENOZ"),
+               HydroParams(RiemannSolver="HLL", slopeLimiter="minmod"),
+               HydroParams(slopeLimiter="vanLeer", charLimiting=False)):
+        unk = S.kelvin_helmholtz(geom, hp)
+        p = oracle.make_params(geom.as_dict(), hp)
+        I0 = oracle.integrals(p, unk)
+        run_oracle(oracle, geom, hp, unk, nsteps=5)
+        I1 = oracle.integrals(p, unk)
+        assert np.all(np.isfinite(unk))
+        assert abs(I1[0] - I0[0]) / I0[0] < 1e-13
+        assert abs(I1[4] - I0[4]) / I0[4] < 1e-13
+
+
+def test_3d_oracle_sod_and_conservation(oracle):
+    """3-D PPM with full CTU corner coupling: Sod along x stays planar, and a
+    periodic noisy gas conserves mass and energy."""
+    geom = Geometry(3, 16, 16, 16, 2, 1, 1, bc=(BC_OUTFLOW,) * 6)
+    hp = HydroParams()
+    unk = S.sod(geom, hp, xangle=0.0, yangle=90.0, posn=0.5)
+    run_oracle(oracle, geom, hp, unk, nsteps=10)
+    g = S.gather_global(geom, unk)
+    assert np.allclose(g[:, :, :, DENS], g[0:1, 0:1, :, DENS], rtol=0, atol=1e-14)
+    geom = Geometry(3, 16, 16, 16, 1, 1, 1, bc=(BC_PERIODIC,) * 6)
+    hp = HydroParams(gamma=5.0 / 3.0)
+    unk = S.noisy_gas(geom, hp)
+    p = oracle.make_params(geom.as_dict(), hp)
+    I0 = oracle.integrals(p, unk)
+    run_oracle(oracle, geom, hp, unk, nsteps=3)
+    I1 = oracle.integrals(p, unk)
+    assert abs(I1[0] - I0[0]) / I0[0] < 1e-13
+    assert abs(I1[4] - I0[4]) / I0[4] < 1e-13
+
+
+@pytest.mark.parametrize("name", ["sod2d_1step", "kh2d_3step"])
+def test_golden_fixtures(oracle, name):
+    """Committed oracle outputs (tests/golden/gen_golden.py) reproduce bit for bit."""
+    path = os.path.join(GOLDEN, name + ".npz")
+    z = np.load(path)
+    sys.path.insert(0, GOLDEN)
+    from gen_golden import CASES
+    geom, hp, init, nsteps = CASES[name]()
+    unk = init(geom, hp)
+    run_oracle(oracle, geom, hp, unk, nsteps=nsteps)
+    g = S.gather_global(geom, unk)
+    assert np.array_equal(g, z["state"])
