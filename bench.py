@@ -16,14 +16,10 @@ to the oracle); the FP32-reconstruction/FP64-update path is reported under
 (2 x 10 x 4.2M FP64 = 671 MB) exceed the 126 MB L2, so no flush is needed.
 """
 import argparse
-import csv
-import io
 import json
 import os
 import statistics
-import subprocess
 import sys
-import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -42,8 +38,8 @@ TRAFFIC_FILE = os.path.join(ROOT, "profiles", "hydro2d_kh2048_traffic.json")
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="kh2d")
     ap.add_argument("--no-mixed", action="store_true")
@@ -61,45 +57,63 @@ def measured_peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """Polls SM clocks and clock-event (throttle) reasons through NVML every
+    10 ms while the timed region runs (read-only queries)."""
 
-    def __init__(self, gpu_index):
-        self.gpu = gpu_index
-        self.proc = None
-        self.tmp = None
+    def __init__(self, cuda_index):
+        self.cuda_index = cuda_index
+        self.samples = []
+        self._stop = None
+        self._thr = None
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.cuda_index)
+            bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.cuda_index)
 
     def start(self):
+        import threading
         try:
-            self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=self.tmp, stderr=subprocess.DEVNULL)
+            import pynvml
+            h = self._handle()
         except Exception:
-            self.proc = None
+            self._thr = None
+            return
+        self.smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        self._stop = threading.Event()
+        bits = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap,
+                "hw_power_brake": pynvml.nvmlClocksEventReasonHwPowerBrakeSlowdown}
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((sm, [k for k, b in bits.items() if r & b]))
+                except Exception:
+                    pass
+                self._stop.wait(0.01)
+        self._thr = threading.Thread(target=run, daemon=True)
+        self._thr.start()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        self.tmp.flush()
-        self.tmp.seek(0)
-        rows = [r for r in csv.reader(io.StringIO(self.tmp.read())) if len(r) >= 9]
-        os.unlink(self.tmp.name)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(rows)}
+        if self._thr is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"]}
+        self._stop.set()
+        self._thr.join()
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.smax, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(s for s, _ in self.samples), "sm_max_mhz": self.smax,
+                "reasons": sorted({r for _, rs in self.samples for r in rs}), "samples": len(self.samples)}
 
 
 def dist_setup(args, backend):
@@ -146,7 +160,7 @@ def run_reference(args):
         return
     from flashx_b200 import simulations as S
     from oracle import fx_oracle as O
-    geom, hp, init = S.config(args.config, scale=1 / 2)
+    geom, hp, init = S.config(args.config, scale=1 / 4)
     unk = init(geom, hp)
     p = O.make_params(geom.as_dict(), hp)
     dt = 0.5 * O.compute_dt(p, unk)
