@@ -163,7 +163,7 @@ __device__ __forceinline__ void faces_stage(const Args2D &a, Smem2D<R> &s, int d
 }
 
 template <class R>
-__global__ void __launch_bounds__(NT2, 1) hydro2d_kernel(const Args2D a)
+__global__ void __launch_bounds__(NT2, 2) hydro2d_kernel(const Args2D a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem2D<R> &s = *reinterpret_cast<Smem2D<R> *>(smem_raw);
