@@ -305,6 +305,11 @@ void free_all()
 
 } // namespace
 
+namespace fxb {
+// lets other translation units of the library report through fxb_last_error
+int record_error(int code, const char *msg) { return fail(code, msg); }
+} // namespace fxb
+
 // ====================================================================== ABI
 extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, const int32_t *var_map, int nunk)
 {

@@ -29,7 +29,7 @@ FXB_VARS = ("dens", "eint", "ener", "gamc", "game", "pres", "temp", "velx", "vel
 # entry points declared in include/flashx_b200.h
 ABI_SYMBOLS = ("fxb_init", "fxb_register_blocks", "fxb_attach_unk", "fxb_fill_guardcells",
                "fxb_hydro_step", "fxb_compute_dt", "fxb_advance", "fxb_eos", "fxb_sync_to_host",
-               "fxb_sync_from_host", "fxb_integrals", "fxb_last_timing", "fxb_stream",
+               "fxb_sync_from_host", "fxb_integrals", "fxb_integrals_noalloc", "fxb_last_timing", "fxb_stream",
                "fxb_last_error", "fxb_finalize")
 
 
@@ -95,6 +95,8 @@ def load_library(path=LIB_PATH):
     L.fxb_sync_to_host.argtypes = [D]
     L.fxb_sync_from_host.argtypes = [D]
     L.fxb_integrals.argtypes = [D]
+    L.fxb_integrals_noalloc.argtypes = [ctypes.c_void_p] * 6 + [ctypes.c_long, ctypes.c_double,
+                                                                 ctypes.c_void_p, ctypes.c_void_p]
     L.fxb_last_timing.argtypes = [D, ctypes.POINTER(ctypes.c_int)]
     L.fxb_stream.restype = ctypes.c_void_p
     L.fxb_last_error.argtypes = [ctypes.POINTER(FxbError)]

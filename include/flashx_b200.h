@@ -129,6 +129,20 @@ int fxb_sync_to_host(double *unk_host);
 int fxb_sync_from_host(const double *unk_host);
 /* Volume integrals: mass, x/y/z momentum, total, internal, kinetic energy. */
 int fxb_integrals(double out[7]);
+/* Volume integrals of caller-owned device arrays without allocating any
+ * device memory (no counterpart in the reference: an addition of this
+ * library).  For callers that cannot call cudaMalloc, e.g. a Fortran code
+ * whose GPU memory belongs to another runtime's pool.  Inputs are device
+ * pointers to ncell FP64 values each; out_dev receives the 7 sums of
+ * fxb_integrals in device memory; work is queued on `stream` (0 = legacy
+ * default stream) and not synchronised.  Scratch lives in a fixed static
+ * device array (8192 partial sums of 4096 cells: at most 33,554,432 cells,
+ * larger ncell is rejected with FXB_EARG).  The first call on each device
+ * looks up that array's address, so make it before any stream capture;
+ * calls that overlap on one GPU race on the shared array. */
+int fxb_integrals_noalloc(const double *dens, const double *velx, const double *vely,
+                          const double *velz, const double *ener, const double *eint,
+                          long ncell, double cell_volume, double *out_dev, void *stream);
 /* Device time of the last fxb_hydro_step / fxb_advance, measured with CUDA
  * events on the library stream (milliseconds), and the number of kernel
  * launches it made. */
