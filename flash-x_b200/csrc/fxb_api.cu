@@ -43,6 +43,7 @@ struct Lib {
     bool timing_valid = false;
     cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};   // two steps starting from buffer 0 / 1
     double gam1inv = 0., ggprodinv = 0.;
+    void *sig3 = nullptr, *w3[3] = {nullptr, nullptr, nullptr}, *f3[3] = {nullptr, nullptr, nullptr};
     fxb_error lasterr{};
 };
 Lib L;
@@ -256,6 +257,8 @@ int launch_hydro(int src, const double *dtv, double dt)
         a.dt_arg = dt; a.dtv = dtv;
         a.gam1inv = L.gam1inv; a.ggprodinv = L.ggprodinv;
         a.prm = L.dprm; a.rate_max = L.rate_max; a.err = L.err;
+        a.sig = L.sig3;
+        for (int d = 0; d < 3; d++) { a.wst[d] = L.w3[d]; a.flx[d] = L.f3[d]; }
         if (L.prm.precision == FXB_MIXED) launch_hydro3d_mixed(a, L.stream);
         else launch_hydro3d_fp64(a, L.stream);
     }
@@ -295,6 +298,11 @@ void free_all()
     if (L.rate_max) cudaFree(L.rate_max);
     if (L.err) cudaFree(L.err);
     if (L.partials) cudaFree(L.partials);
+    if (L.sig3) cudaFree(L.sig3);
+    for (int d = 0; d < 3; d++) {
+        if (L.w3[d]) cudaFree(L.w3[d]);
+        if (L.f3[d]) cudaFree(L.f3[d]);
+    }
     if (L.ev0) cudaEventDestroy(L.ev0);
     if (L.ev1) cudaEventDestroy(L.ev1);
     if (L.stream) cudaStreamDestroy(L.stream);
@@ -391,6 +399,13 @@ extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, cons
     } else {
         CK(setup_hydro3d_fp64());
         CK(setup_hydro3d_mixed());
+        // intermediates of the unfused 3-D pipeline, in the reconstruction type
+        size_t rsz = p.precision == FXB_MIXED ? sizeof(float) : sizeof(double);
+        CK(cudaMalloc(&L.sig3, sig3d_bytes(L.nx, L.ny, L.nz, rsz)));
+        for (int dd = 0; dd < 3; dd++) {
+            CK(cudaMalloc(&L.w3[dd], w3d_bytes(dd, L.nx, L.ny, L.nz, rsz)));
+            CK(cudaMalloc(&L.f3[dd], f3d_bytes(dd, L.nx, L.ny, L.nz, rsz)));
+        }
     }
     CK(cudaStreamSynchronize(L.stream));
     L.inited = true;

@@ -38,6 +38,12 @@ template <class R> __device__ __forceinline__ R rsqrt_(R a);
 template <> __device__ __forceinline__ double rsqrt_<double>(double a) { return sqrt(a); }
 template <> __device__ __forceinline__ float rsqrt_<float>(float a) { return __fsqrt_rn(a); }
 
+// division by a literal constant: exact IEEE division in FP64 (the oracle's
+// operation), multiplication by the rounded reciprocal in the FP32 path
+template <class R> __device__ __forceinline__ R divc(R x, double c);
+template <> __device__ __forceinline__ double divc<double>(double x, double c) { return x / c; }
+template <> __device__ __forceinline__ float divc<float>(float x, double c) { return x * (float)(1.0 / c); }
+
 // Fortran MIN/MAX with gfortran's argument order: mvar = a1; if (a2 < mvar) mvar = a2
 template <class R> __device__ __forceinline__ R fmin2(R a, R b) { return (b < a) ? b : a; }
 template <class R> __device__ __forceinline__ R fmax2(R a, R b) { return (b > a) ? b : a; }
@@ -197,9 +203,9 @@ __device__ __forceinline__ void ppm_trace(const Eig<R> &e, R dtn, R hdtn, const 
     // secondary variable EI: initial guess survives (gamc/game are reset to Vc)
     {
         R lmax = fmax2(e.un, R(0));
-        Wp[5] = vecR[5] - lmax * hdtn * (delW[5] - (R(1.0) - lmax * hdtn * R(4.) / R(3.)) * W6[5]);
+        Wp[5] = vecR[5] - lmax * hdtn * (delW[5] - (R(1.0) - divc(lmax * hdtn * R(4.), 3.)) * W6[5]);
         R lmin = -fmin2(e.un, R(0));
-        Wm[5] = vecL[5] + lmin * hdtn * (delW[5] + (R(1.0) - lmin * hdtn * R(4.) / R(3.)) * W6[5]);
+        Wm[5] = vecL[5] + lmin * hdtn * (delW[5] + (R(1.0) - divc(lmin * hdtn * R(4.), 3.)) * W6[5]);
     }
     // tracing over the five waves, HLL-type branch
     Five<R> cA = ldot(e, delW[0], delW[1], delW[2], delW[3], delW[4]);
@@ -245,7 +251,7 @@ __device__ __forceinline__ void ppm_trace(const Eig<R> &e, R dtn, R hdtn, const 
     const R sl[5] = {sLD, sL1, sL2, sL3, sLP}, sr[5] = {sRD, sR1, sR2, sR3, sRP};
 #pragma unroll
     for (int v = 0; v < 5; v++) {
-        R base = Vc[v] + W6[v] / R(12.);
+        R base = Vc[v] + divc(W6[v], 12.);
         Wm[v] = base + sl[v];
         Wp[v] = base + sr[v];
     }
@@ -258,8 +264,8 @@ __device__ __forceinline__ void ppm_interfaces(const R *Vm, const R *Vc, const R
 {
 #pragma unroll
     for (int n = 0; n < 6; n++) {
-        vecL[n] = R(.5) * (Vc[n] + Vm[n]) - (db0[n] - dbN[n]) / R(6.);
-        vecR[n] = R(.5) * (Vc[n] + Vp[n]) - (dbP[n] - db0[n]) / R(6.);
+        vecL[n] = R(.5) * (Vc[n] + Vm[n]) - divc(db0[n] - dbN[n], 6.);
+        vecR[n] = R(.5) * (Vc[n] + Vp[n]) - divc(dbP[n] - db0[n], 6.);
     }
 }
 
@@ -343,6 +349,24 @@ __device__ __forceinline__ void weno_interfaces(const DevParams &prm, const Eig<
             weno_scalar(prm.weno_method, S[0][n], S[1][n], S[2][n], S[3][n], S[4][n], vecR[n], vecL[n]);
     }
     weno_scalar(prm.weno_method, S[0][5], S[1][5], S[2][5], S[3][5], S[4][5], vecR[5], vecL[5]);
+}
+
+// Reconstructed face values of the (constant) gravity component along the
+// sweep: PPM returns the constant exactly; WENO's weighted interpolants may
+// differ from it by rounding, and the monotonicity check of CW84 eq. 1.10 then
+// decides what survives (hy_DataReconstructNormalDir_WENO.F90:772-790, [7-d]).
+template <class R>
+__device__ __forceinline__ void gravity_faces(const DevParams &prm, R g, R &gl, R &gr)
+{
+    gl = g; gr = g;
+    if (prm.order != 5) return;
+    R vr, vl;
+    weno_scalar(prm.weno_method, g, g, g, g, g, vr, vl);
+    R L = vl, Rr = vr, C = g;
+    if ((Rr - C) * (C - L) <= R(0)) { L = C; Rr = C; }
+    if (R(6) * (Rr - L) * (C - R(.5) * (L + Rr)) > (Rr - L) * (Rr - L)) L = R(3) * C - R(2) * Rr;
+    if (R(6) * (Rr - L) * (C - R(.5) * (L + Rr)) < -((Rr - L) * (Rr - L))) Rr = R(3) * C - R(2) * L;
+    gl = L; gr = Rr;
 }
 
 // ---- Riemann solvers (hy_HLLC.F90:64-335, hy_HLL.F90:64-182) ---------------

@@ -46,10 +46,17 @@ constexpr int NDB = (T2 + 4) * T2; // 320 slope cells
 constexpr int NW = (T2 + 2) * T2;  // 288 face-state cells
 constexpr int NFC = (T2 + 1) * T2; // 272 faces
 
+// The FP32 path keeps the slope stage's eigensystem in shared memory for the
+// state stage; the FP64 path recomputes it (identical operations), because the
+// extra 23 KB and the register traffic cost it more than the four divisions
+// and one square root it saves (measured on B200).
+template <class R> struct CacheEig { static constexpr bool value = sizeof(R) == 4; };
+
 template <class R> struct Smem2D {
     R V[8][WIN][WIN];
     R DBF[NF * NFC];               // slopes [6][NDB], then fluxes [8][NFC]
     R W[12][NW];                   // Wp (D,VX,VY,VZ,P,EI), then Wm
+    R EG[9][CacheEig<R>::value ? NDB : 1];   // eigensystem of the slope cells (PPM)
 };
 
 // rotate a global-order 6-vector (D,VX,VY,VZ,P,EI) into sweep order
@@ -89,6 +96,10 @@ __device__ __forceinline__ void slopes_stage(const Args2D &a, Smem2D<R> &s, int 
     tvd_slope(a.prm, e, Vm, Vc, Vp, db);
 #pragma unroll
     for (int k = 0; k < 6; k++) s.DBF[k * NDB + t] = db[k];
+    if (CacheEig<R>::value) {
+        s.EG[0][t] = e.lam0; s.EG[1][t] = e.un; s.EG[2][t] = e.lam4; s.EG[3][t] = e.cf; s.EG[4][t] = e.rho;
+        s.EG[5][t] = e.ahinv; s.EG[6][t] = e.lp; s.EG[7][t] = e.a2inv; s.EG[8][t] = e.rp;
+    }
 }
 
 // face states of one cell along dir, with the transverse correction of the
@@ -102,7 +113,8 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
     R g[6], Vm[6], Vc[6], Vp[6], vecL[6], vecR[6], Wm[6], Wp[6];
     win6(s, wx, wy, g); rot(dir, g, Vc);
     Eig<R> e;
-    if (!eigen(Vc[0], Vc[1], Vc[4], s.V[GC][wy][wx], e)) set_err(a.err, ERR_SOUND);
+    if (a.prm.order == 5 || !CacheEig<R>::value)
+        if (!eigen(Vc[0], Vc[1], Vc[4], s.V[GC][wy][wx], e)) set_err(a.err, ERR_SOUND);
     if (a.prm.order == 5) {
         R S[5][6];
 #pragma unroll
@@ -111,6 +123,11 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
 #pragma unroll
         for (int k = 0; k < 6; k++) { Vm[k] = S[1][k]; Vp[k] = S[3][k]; }
     } else {
+        if (CacheEig<R>::value) {   // the slope stage computed this cell's eigensystem
+            e.lam0 = s.EG[0][dbi]; e.un = s.EG[1][dbi]; e.lam4 = s.EG[2][dbi]; e.cf = s.EG[3][dbi];
+            e.rho = s.EG[4][dbi]; e.ahinv = s.EG[5][dbi]; e.lp = s.EG[6][dbi]; e.a2inv = s.EG[7][dbi];
+            e.rp = s.EG[8][dbi];
+        }
         win6(s, wx - ox, wy - oy, g); rot(dir, g, Vm);
         win6(s, wx + ox, wy + oy, g); rot(dir, g, Vp);
         R dbN[6], db0[6], dbP[6];

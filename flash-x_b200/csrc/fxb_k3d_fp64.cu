@@ -1,6 +1,6 @@
-// FP64 instantiation of the 3-D fused kernel (placeholder until built).
+// FP64 instantiation of the 3-D kernels (built with -fmad=false).
 #include "fxb_launch.h"
 namespace fxb {
-cudaError_t setup_hydro3d_fp64() { return cudaErrorNotSupported; }
-void launch_hydro3d_fp64(const Args3D &, cudaStream_t) {}
+cudaError_t setup_hydro3d_fp64() { return cudaSuccess; }
+void launch_hydro3d_fp64(const Args3D &a, cudaStream_t s) { launch_hydro3d_t<double>(a, s); }
 } // namespace fxb
