@@ -32,7 +32,16 @@ import numpy as np  # noqa: E402
 METRIC = "zone-updates/s FP64 vs FP32+FP64-update at stated L1 err; % HBM roofline"
 UNIT = "zone-updates/s"
 BYTES_PER_ZONE = 152   # 9 FP64 reads + 10 FP64 writes per zone-update (algorithmic)
-TRAFFIC_FILE = os.path.join(ROOT, "profiles", "hydro2d_kh2048_traffic.json")
+TRAFFIC_FILES = {"kh2d": os.path.join(ROOT, "profiles", "hydro2d_kh2048_traffic.json"),
+                 "rt3d": os.path.join(ROOT, "profiles", "hydro3d_rt256_traffic.json")}
+WORKLOADS = {
+    "kh2d": "kh2d: 2-D Kelvin-Helmholtz 2048^2 (128x128 blocks of 16^2), periodic, PPM+HLLC, "
+            "mc/char limiting, CFL 0.8, gamma 1.4",
+    "sod2d": "sod2d: 2-D Sod at 45 deg, 256^2 (16x16 blocks of 16^2), outflow, PPM+HLLC, CFL 0.8",
+    "rt3d": "rt3d: 3-D Rayleigh-Taylor 256^3 (4096 blocks of 16^3), WENO5+HLLC, g_z=-0.1, periodic x/y, "
+            "reflecting z, full CTU",
+    "sweep3d": "sweep3d: 3-D noisy gas 64^3 (64 blocks of 16^3), periodic, PPM+HLLC, gamma 5/3",
+}
 
 
 def parse():
@@ -41,7 +50,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="kh2d")
+    ap.add_argument("--config", default="kh2d", choices=["kh2d", "sod2d", "rt3d", "sweep3d"],
+                    help="kh2d (default, the headline workload) or another benchmark problem")
+    ap.add_argument("--scale", type=float, default=1.0, help="block count per axis relative to the config")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -195,7 +206,7 @@ def run_ours(args):
     from flashx_b200 import simulations as S
     from flashx_b200.hydro import HydroDevice, driver_dt
 
-    geom, hp, init = S.config(args.config)
+    geom, hp, init = S.config(args.config, scale=args.scale)
     unk0 = init(geom, hp)
     ncell = geom.ncells
     K, W = args.steps, args.warmup
@@ -235,7 +246,7 @@ def run_ours(args):
             barrier()
             clocks = clk.stop()
             ms = e0.elapsed_time(e1)
-            launches = 2 * K
+            launches = (2 if geom.ndim == 2 else 9) * K
         else:
             dt_old = dt
             for _ in range(W):
@@ -252,7 +263,7 @@ def run_ours(args):
             barrier()
             clocks = clk.stop()
             ms = e0.elapsed_time(e1)
-            launches = K
+            launches = (1 if geom.ndim == 2 else 8) * K
         ms = max_over_ranks(ms)
         return dev, ms, launches, clocks
 
@@ -288,16 +299,17 @@ def run_ours(args):
     achieved = BYTES_PER_ZONE * ncell / (kernel_ms / 1e3) / 1e9
     traffic = None
     try:
-        with open(TRAFFIC_FILE) as f:
-            traffic = json.load(f).get("bytes_per_launch")
+        with open(TRAFFIC_FILES[args.config]) as f:
+            tj = json.load(f)
+        if tj.get("zones") == ncell:
+            traffic = tj.get("bytes_per_launch")
     except Exception:
         pass
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded Philox4x32-10 KH initial state)",
-            "config": {"workload": "kh2d: 2-D Kelvin-Helmholtz 2048^2 (128x128 blocks of 16^2), periodic, "
-                                   "PPM+HLLC, mc/char limiting, CFL 0.8, gamma 1.4",
+            "config": {"workload": WORKLOADS[args.config] + ("" if args.scale == 1.0 else f" at scale {args.scale}"),
                        "zones_per_gpu": ncell, "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (671 MB state vs 126 MB L2)",
                        "timing": "CUDA events on the library stream, device dt loop (CUDA graph)"},
@@ -305,7 +317,9 @@ def run_ours(args):
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "hydro2d_kernel<double>", "kernel_ms": kernel_ms,
+                         "kernel": "hydro2d_kernel<double>" if geom.ndim == 2 else
+                                   "3-D pipeline (sig3d, states3d x3, flux3d x3, update3d)<double>",
+                         "kernel_ms": kernel_ms,
                          "algorithmic_bytes_per_zone": BYTES_PER_ZONE},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24, "d2h_bytes_per_step": 8,
                     "note": "host loop via fxb_hydro_step/fxb_compute_dt: (t, dt, dtOld) in, dt out per step; "
@@ -332,7 +346,7 @@ def run_ours(args):
                          "dtype": "f32 reconstruction/Riemann + f64 update", "clocks": mclk}
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_run(args.config)
+        line["cpu_baseline"] = cpu_baseline_run(args.config, scale=args.scale / 4 if geom.ndim == 2 else args.scale / 4)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
