@@ -52,11 +52,17 @@ constexpr int NFC = (T2 + 1) * T2; // 272 faces
 // and one square root it saves (measured on B200).
 template <class R> struct CacheEig { static constexpr bool value = sizeof(R) == 4; };
 
+constexpr int NOWN = T2 * T2;      // owner cells of a tile
+
 template <class R> struct Smem2D {
     R V[8][WIN][WIN];
     R DBF[NF * NFC];               // slopes [6][NDB], then fluxes [8][NFC]
+    R SG[6][NDB];                  // sigma of the other direction at the slope cells (global order)
     R W[12][NW];                   // Wp (D,VX,VY,VZ,P,EI), then Wm
     R EG[9][CacheEig<R>::value ? NDB : 1];   // eigensystem of the slope cells (PPM)
+    // FP64 update inputs of the owner cells that the window does not hold
+    // exactly: ENER, and in the FP32 path also D, VX, VY, VZ, EINT
+    double OWN[CacheEig<R>::value ? 6 : 1][NOWN];
 };
 
 // rotate a global-order 6-vector (D,VX,VY,VZ,P,EI) into sweep order
@@ -84,22 +90,40 @@ template <class R> __device__ __forceinline__ void win6(const Smem2D<R> &s, int 
 
 __device__ __forceinline__ void set_err(int *err, int code) { atomicOr(err, code); }
 
+// Per-cell analysis along dir at a slope cell: the eigensystem and limited
+// slopes (PPM), and the upwind transverse flux sigma of the other direction
+// (hy_upwindTransverseFlux), which the state stage of dir subtracts.
 template <class R>
-__device__ __forceinline__ void slopes_stage(const Args2D &a, Smem2D<R> &s, int dir, int t, int wx, int wy)
+__device__ __forceinline__ void analysis_stage(const Args2D &a, Smem2D<R> &s, int dir, int t, int wx, int wy,
+                                               bool ppm)
 {
-    const int ox = dir == 0, oy = dir == 1;
-    R g[3][6], Vm[6], Vc[6], Vp[6], db[6];
-    win6(s, wx - ox, wy - oy, g[0]); win6(s, wx, wy, g[1]); win6(s, wx + ox, wy + oy, g[2]);
-    rot(dir, g[0], Vm); rot(dir, g[1], Vc); rot(dir, g[2], Vp);
-    Eig<R> e;
-    if (!eigen(Vc[0], Vc[1], Vc[4], s.V[GC][wy][wx], e)) set_err(a.err, ERR_SOUND);
-    tvd_slope(a.prm, e, Vm, Vc, Vp, db);
+    R g[6], c[6];
+    win6(s, wx, wy, g);
+    if (ppm) {
+        const int ox = dir == 0, oy = dir == 1;
+        R gm[6], gp[6], Vm[6], Vp[6], db[6];
+        win6(s, wx - ox, wy - oy, gm); win6(s, wx + ox, wy + oy, gp);
+        rot(dir, gm, Vm); rot(dir, g, c); rot(dir, gp, Vp);
+        Eig<R> e;
+        if (!eigen(c[0], c[1], c[4], s.V[GC][wy][wx], e)) set_err(a.err, ERR_SOUND);
+        tvd_slope(a.prm, e, Vm, c, Vp, db);
 #pragma unroll
-    for (int k = 0; k < 6; k++) s.DBF[k * NDB + t] = db[k];
-    if (CacheEig<R>::value) {
-        s.EG[0][t] = e.lam0; s.EG[1][t] = e.un; s.EG[2][t] = e.lam4; s.EG[3][t] = e.cf; s.EG[4][t] = e.rho;
-        s.EG[5][t] = e.ahinv; s.EG[6][t] = e.lp; s.EG[7][t] = e.a2inv; s.EG[8][t] = e.rp;
+        for (int k = 0; k < 6; k++) s.DBF[k * NDB + t] = db[k];
+        if (CacheEig<R>::value) {
+            s.EG[0][t] = e.lam0; s.EG[1][t] = e.un; s.EG[2][t] = e.lam4; s.EG[3][t] = e.cf; s.EG[4][t] = e.rho;
+            s.EG[5][t] = e.ahinv; s.EG[6][t] = e.lp; s.EG[7][t] = e.a2inv; s.EG[8][t] = e.rp;
+        }
     }
+    const int td = 1 - dir, tx = td == 0, ty = td == 1;
+    R gm[6], gp[6], m[6], p[6], sr[6], sg[6];
+    win6(s, wx - tx, wy - ty, gm); win6(s, wx + tx, wy + ty, gp);
+    rot(td, gm, m); rot(td, g, c); rot(td, gp, p);
+    Eig<R> et;
+    if (!eigen(c[0], c[1], c[4], s.V[GC][wy][wx], et)) set_err(a.err, ERR_SOUND);
+    trans_flux(et, m, c, p, a.prm.use_aux_eint != 0, sr);
+    unrot(td, sr, sg);
+#pragma unroll
+    for (int k = 0; k < 6; k++) s.SG[k][t] = sg[k];
 }
 
 // face states of one cell along dir, with the transverse correction of the
@@ -142,19 +166,12 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
     R wm[6], wp[6];
     ppm_trace(e, dtn, hdtn, Vc, vecL, vecR, wm, wp);
     unrot(dir, wm, Wm); unrot(dir, wp, Wp);
-    // transverse flux of the other direction at this cell
-    {
-        const int td = 1 - dir, tx = td == 0, ty = td == 1;
-        R m[6], c[6], p[6], sr[6], sg[6];
-        win6(s, wx - tx, wy - ty, g); rot(td, g, m);
-        win6(s, wx, wy, g); rot(td, g, c);
-        win6(s, wx + tx, wy + ty, g); rot(td, g, p);
-        Eig<R> et;
-        if (!eigen(c[0], c[1], c[4], s.V[GC][wy][wx], et)) set_err(a.err, ERR_SOUND);
-        trans_flux(et, m, c, p, a.prm.use_aux_eint != 0, sr);
-        unrot(td, sr, sg);
+    // transverse flux of the other direction at this cell (from the analysis stage)
 #pragma unroll
-        for (int k = 0; k < 6; k++) { Wm[k] = Wm[k] - hdtt * sg[k]; Wp[k] = Wp[k] - hdtt * sg[k]; }
+    for (int k = 0; k < 6; k++) {
+        R sg = s.SG[k][dbi];
+        Wm[k] = Wm[k] - hdtt * sg;
+        Wp[k] = Wp[k] - hdtt * sg;
     }
     if (Wm[0] < R(0) || Wp[0] < R(0) || Wm[4] < R(0) || Wp[4] < R(0)) {
         win6(s, wx, wy, g);
@@ -188,17 +205,53 @@ __global__ void __launch_bounds__(NT2, 2) hydro2d_kernel(const Args2D a)
     const int tx0 = blockIdx.x * T2, ty0 = blockIdx.y * T2;
     const double dt = a.dtv ? a.dtv[0] : a.dt_arg;
 
-    // ---- A: window load with guard cells resolved on the fly
-    for (int e = tid; e < 8 * WIN * WIN; e += NT2) {
-        int v = e / (WIN * WIN), r = e - v * (WIN * WIN);
-        int wy = r / WIN, wx = r - wy * WIN;
-        double sx = 1.0, sy = 1.0;
-        int gx = map_axis(tx0 + wx - 3, a.nx, a.bc[0], a.bc[1], &sx);
-        int gy = map_axis(ty0 + wy - 3, a.ny, a.bc[2], a.bc[3], &sy);
-        double val = __ldg(a.in + v * a.vstride + (long)gy * a.nx + gx);
-        if (v == VX) val = val * sx;
-        if (v == VY) val = val * sy;
-        s.V[v][wy][wx] = (R)val;
+    // ---- A: window load with guard cells resolved on the fly.  All of a
+    // thread's loads are issued before any is consumed, so they are in flight
+    // together; owner threads also fetch the FP64 update inputs.
+    constexpr int NEL = 8 * WIN * WIN, NLD = (NEL + NT2 - 1) / NT2;
+    const bool owner = tid < NOWN;
+    const int oi = tid % T2, oj = tid / T2;
+    const long gidx = (long)(ty0 + oj) * a.nx + (tx0 + oi);
+    {
+        double buf[NLD];
+#pragma unroll
+        for (int q = 0; q < NLD; q++) {
+            const int e = tid + q * NT2;
+            buf[q] = 0.;
+            if (e < NEL) {
+                int v = e / (WIN * WIN), r = e - v * (WIN * WIN);
+                int wy = r / WIN, wx = r - wy * WIN;
+                double sx = 1.0, sy = 1.0;
+                int gx = map_axis(tx0 + wx - 3, a.nx, a.bc[0], a.bc[1], &sx);
+                int gy = map_axis(ty0 + wy - 3, a.ny, a.bc[2], a.bc[3], &sy);
+                double val = __ldg(a.in + v * a.vstride + (long)gy * a.nx + gx);
+                buf[q] = v == VX ? val * sx : (v == VY ? val * sy : val);
+            }
+        }
+        double own[CacheEig<R>::value ? 6 : 1];
+        if (owner) {
+            own[0] = __ldg(a.in + DV_ENER * a.vstride + gidx);
+            if (CacheEig<R>::value) {
+                own[CacheEig<R>::value ? 1 : 0] = __ldg(a.in + D * a.vstride + gidx);
+                own[CacheEig<R>::value ? 2 : 0] = __ldg(a.in + VX * a.vstride + gidx);
+                own[CacheEig<R>::value ? 3 : 0] = __ldg(a.in + VY * a.vstride + gidx);
+                own[CacheEig<R>::value ? 4 : 0] = __ldg(a.in + VZ * a.vstride + gidx);
+                own[CacheEig<R>::value ? 5 : 0] = __ldg(a.in + EI * a.vstride + gidx);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NLD; q++) {
+            const int e = tid + q * NT2;
+            if (e < NEL) {
+                int v = e / (WIN * WIN), r = e - v * (WIN * WIN);
+                int wy = r / WIN, wx = r - wy * WIN;
+                s.V[v][wy][wx] = (R)buf[q];
+            }
+        }
+        if (owner) {
+#pragma unroll
+            for (int q = 0; q < (CacheEig<R>::value ? 6 : 1); q++) s.OWN[q][tid] = own[q];
+        }
     }
     __syncthreads();
 
@@ -207,10 +260,10 @@ __global__ void __launch_bounds__(NT2, 2) hydro2d_kernel(const Args2D a)
     const R hdtx = R(0.5 * dt / a.dx), hdty = R(0.5 * dt / a.dy);
     const bool ppm = a.prm.order != 5;
 
-    // ---- B: x slopes
-    if (ppm && tid < NDB) {
+    // ---- B: x slopes and sigma_y
+    if (tid < NDB) {
         int ii = tid % (T2 + 4) - 2, jj = tid / (T2 + 4);
-        slopes_stage(a, s, 0, tid, ii + 3, jj + 3);
+        analysis_stage(a, s, 0, tid, ii + 3, jj + 3, ppm);
     }
     __syncthreads();
     // ---- C: x face states
@@ -227,16 +280,19 @@ __global__ void __launch_bounds__(NT2, 2) hydro2d_kernel(const Args2D a)
     __syncthreads();
 
     // ---- E: owner threads, x part of the update
-    const bool owner = tid < T2 * T2;
-    const int oi = tid % T2, oj = tid / T2;
-    const long gidx = (long)(ty0 + oj) * a.nx + (tx0 + oi);
     double U0[5], dens0 = 0., Ax = 0., Bx = 0., pav = 0., SphX = 0., eint0 = 0.;
     const double dtdx = dt / a.dx, dtdy = dt / a.dy;
     if (owner) {
-        dens0 = __ldg(a.in + D * a.vstride + gidx);
-        double vx = __ldg(a.in + VX * a.vstride + gidx), vy = __ldg(a.in + VY * a.vstride + gidx);
-        double vz = __ldg(a.in + VZ * a.vstride + gidx), en = __ldg(a.in + DV_ENER * a.vstride + gidx);
-        eint0 = __ldg(a.in + EI * a.vstride + gidx);
+        double vx, vy, vz, en = s.OWN[0][tid];
+        if (CacheEig<R>::value) {
+            dens0 = s.OWN[CacheEig<R>::value ? 1 : 0][tid]; vx = s.OWN[CacheEig<R>::value ? 2 : 0][tid];
+            vy = s.OWN[CacheEig<R>::value ? 3 : 0][tid]; vz = s.OWN[CacheEig<R>::value ? 4 : 0][tid];
+            eint0 = s.OWN[CacheEig<R>::value ? 5 : 0][tid];
+        } else {   // the FP64 window holds these values exactly
+            dens0 = (double)s.V[D][oj + 3][oi + 3]; vx = (double)s.V[VX][oj + 3][oi + 3];
+            vy = (double)s.V[VY][oj + 3][oi + 3]; vz = (double)s.V[VZ][oj + 3][oi + 3];
+            eint0 = (double)s.V[EI][oj + 3][oi + 3];
+        }
         U0[0] = dens0; U0[1] = vx * dens0; U0[2] = vy * dens0; U0[3] = vz * dens0; U0[4] = dens0 * en;
         int fl = oj * (T2 + 1) + oi, fr = fl + 1;
 #pragma unroll
@@ -250,10 +306,10 @@ __global__ void __launch_bounds__(NT2, 2) hydro2d_kernel(const Args2D a)
     }
     __syncthreads();
 
-    // ---- F: y slopes
-    if (ppm && tid < NDB) {
+    // ---- F: y slopes and sigma_x
+    if (tid < NDB) {
         int ii = tid % T2, jj = tid / T2 - 2;
-        slopes_stage(a, s, 1, tid, ii + 3, jj + 3);
+        analysis_stage(a, s, 1, tid, ii + 3, jj + 3, ppm);
     }
     __syncthreads();
     // ---- G: y face states
