@@ -223,12 +223,7 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def global_min(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MIN)
-        return float(t.item())
+    from flashx_b200.parallel import allreduce_min as global_min   # Driver_computeDt's AllReduce(MIN)
 
     def timed_run(precision):
         dev = HydroDevice(geom, hp, precision)
