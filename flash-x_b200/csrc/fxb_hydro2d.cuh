@@ -41,7 +41,18 @@ struct Args2D {
 
 constexpr int T2 = 16;             // tile edge
 constexpr int WIN = T2 + 6;        // window edge
-constexpr int NT2 = 320;           // threads per CTA
+// Threads per CTA.  Two CTAs share an SM's 64K registers, so the count sets
+// the register budget.  320 threads (10 warps, 96 registers) measured fastest
+// for both precisions on B200: 288 threads (112 registers) cannot place 18
+// warps evenly on the four SM sub-partitions and drops to one CTA per SM;
+// 256 threads (128 registers, fewer spills) needs a second pass in every
+// stage.  Every stage loops, so other counts remain valid.
+#ifndef FXB_FP64_THREADS
+#define FXB_FP64_THREADS 320
+#endif
+template <class R> struct Threads2D { static constexpr int value = sizeof(R) == 8 ? FXB_FP64_THREADS : 320; };
+// registers per thread for two CTAs per SM (multiple of 8)
+template <class R> struct Regs2D { static constexpr int value = (65536 / (2 * Threads2D<R>::value)) / 8 * 8; };
 constexpr int NDB = (T2 + 4) * T2; // 320 slope cells
 constexpr int NW = (T2 + 2) * T2;  // 288 face-state cells
 constexpr int NFC = (T2 + 1) * T2; // 272 faces
@@ -197,10 +208,11 @@ __device__ __forceinline__ void faces_stage(const Args2D &a, Smem2D<R> &s, int d
 }
 
 template <class R>
-__global__ void __launch_bounds__(NT2, 2) hydro2d_kernel(const Args2D a)
+__global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::value) hydro2d_kernel(const Args2D a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem2D<R> &s = *reinterpret_cast<Smem2D<R> *>(smem_raw);
+    constexpr int NT2 = Threads2D<R>::value;
     const int tid = threadIdx.x;
     const int tx0 = blockIdx.x * T2, ty0 = blockIdx.y * T2;
     const double dt = a.dtv ? a.dtv[0] : a.dt_arg;
@@ -261,21 +273,21 @@ __global__ void __launch_bounds__(NT2, 2) hydro2d_kernel(const Args2D a)
     const bool ppm = a.prm.order != 5;
 
     // ---- B: x slopes and sigma_y
-    if (tid < NDB) {
-        int ii = tid % (T2 + 4) - 2, jj = tid / (T2 + 4);
-        analysis_stage(a, s, 0, tid, ii + 3, jj + 3, ppm);
+    for (int t = tid; t < NDB; t += NT2) {
+        int ii = t % (T2 + 4) - 2, jj = t / (T2 + 4);
+        analysis_stage(a, s, 0, t, ii + 3, jj + 3, ppm);
     }
     __syncthreads();
     // ---- C: x face states
-    if (tid < NW) {
-        int ii = tid % (T2 + 2) - 1, jj = tid / (T2 + 2);
-        states_stage(a, s, 0, tid, ii + 3, jj + 3, jj * (T2 + 4) + ii + 2, 1, dtnx, hdtnx, hdty);
+    for (int t = tid; t < NW; t += NT2) {
+        int ii = t % (T2 + 2) - 1, jj = t / (T2 + 2);
+        states_stage(a, s, 0, t, ii + 3, jj + 3, jj * (T2 + 4) + ii + 2, 1, dtnx, hdtnx, hdty);
     }
     __syncthreads();
     // ---- D: x faces
-    if (tid < NFC) {
-        int fi = tid % (T2 + 1), jj = tid / (T2 + 1);
-        faces_stage(a, s, 0, tid, jj * (T2 + 2) + fi, jj * (T2 + 2) + fi + 1, fi + 2, jj + 3, fi + 3, jj + 3);
+    for (int t = tid; t < NFC; t += NT2) {
+        int fi = t % (T2 + 1), jj = t / (T2 + 1);
+        faces_stage(a, s, 0, t, jj * (T2 + 2) + fi, jj * (T2 + 2) + fi + 1, fi + 2, jj + 3, fi + 3, jj + 3);
     }
     __syncthreads();
 
@@ -307,21 +319,21 @@ __global__ void __launch_bounds__(NT2, 2) hydro2d_kernel(const Args2D a)
     __syncthreads();
 
     // ---- F: y slopes and sigma_x
-    if (tid < NDB) {
-        int ii = tid % T2, jj = tid / T2 - 2;
-        analysis_stage(a, s, 1, tid, ii + 3, jj + 3, ppm);
+    for (int t = tid; t < NDB; t += NT2) {
+        int ii = t % T2, jj = t / T2 - 2;
+        analysis_stage(a, s, 1, t, ii + 3, jj + 3, ppm);
     }
     __syncthreads();
     // ---- G: y face states
-    if (tid < NW) {
-        int ii = tid % T2, jj = tid / T2 - 1;
-        states_stage(a, s, 1, tid, ii + 3, jj + 3, (jj + 2) * T2 + ii, T2, dtny, hdtny, hdtx);
+    for (int t = tid; t < NW; t += NT2) {
+        int ii = t % T2, jj = t / T2 - 1;
+        states_stage(a, s, 1, t, ii + 3, jj + 3, (jj + 2) * T2 + ii, T2, dtny, hdtny, hdtx);
     }
     __syncthreads();
     // ---- H: y faces
-    if (tid < NFC) {
-        int ii = tid % T2, fj = tid / T2;
-        faces_stage(a, s, 1, tid, fj * T2 + ii, (fj + 1) * T2 + ii, ii + 3, fj + 2, ii + 3, fj + 3);
+    for (int t = tid; t < NFC; t += NT2) {
+        int ii = t % T2, fj = t / T2;
+        faces_stage(a, s, 1, t, fj * T2 + ii, (fj + 1) * T2 + ii, ii + 3, fj + 2, ii + 3, fj + 3);
     }
     __syncthreads();
 

@@ -8,6 +8,6 @@ cudaError_t setup_hydro2d_fp64()
 }
 void launch_hydro2d_fp64(const Args2D &a, dim3 grid, cudaStream_t s)
 {
-    hydro2d_kernel<double><<<grid, NT2, sizeof(Smem2D<double>), s>>>(a);
+    hydro2d_kernel<double><<<grid, Threads2D<double>::value, sizeof(Smem2D<double>), s>>>(a);
 }
 } // namespace fxb

@@ -10,6 +10,6 @@ cudaError_t setup_hydro2d_mixed()
 }
 void launch_hydro2d_mixed(const Args2D &a, dim3 grid, cudaStream_t s)
 {
-    hydro2d_kernel<float><<<grid, NT2, sizeof(Smem2D<float>), s>>>(a);
+    hydro2d_kernel<float><<<grid, Threads2D<float>::value, sizeof(Smem2D<float>), s>>>(a);
 }
 } // namespace fxb
