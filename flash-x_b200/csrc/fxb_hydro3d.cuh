@@ -164,8 +164,22 @@ __device__ __forceinline__ void ctu_term(const Args3D &a, const Grid3 &G, const 
 }
 
 // ---- face states of direction d ------------------------------------------------
-template <class R>
-__global__ void __launch_bounds__(256) states3d_kernel(const Args3D a, int d)
+// One instantiation per reconstruction order, so the register allocation of
+// the PPM path (three eigensystems and slopes) and of the WENO path (one
+// eigensystem, five projected cells) do not add up.  The minimum number of
+// resident 256-thread CTAs per SM bounds the registers per thread: two CTAs
+// (128 registers, a few hundred bytes of spills in FP64) measured 18 % faster
+// on B200 than one CTA with 244-255 registers, and three CTAs (80 registers)
+// lost again to spill traffic.
+#ifndef FXB_S3_MINB_FP64
+#define FXB_S3_MINB_FP64 2
+#endif
+#ifndef FXB_S3_MINB_FP32
+#define FXB_S3_MINB_FP32 2
+#endif
+template <class R> struct MinB3D { static constexpr int value = sizeof(R) == 8 ? FXB_S3_MINB_FP64 : FXB_S3_MINB_FP32; };
+template <class R, int ORDER>
+__global__ void __launch_bounds__(256, MinB3D<R>::value) states3d_kernel(const Args3D a, int d)
 {
     Grid3 G{a.nx, a.ny, a.nz};
     const double dt = a.dtv ? a.dtv[0] : a.dt_arg;
@@ -190,7 +204,7 @@ __global__ void __launch_bounds__(256) states3d_kernel(const Args3D a, int d)
         Eig<R> e;
         if (!eigen(S[2][0], S[2][1], S[2][4], vc[GC], e)) atomicOr(a.err, ERR_SOUND);
         R vecL[6], vecR[6];
-        if (a.prm.order == 5) {
+        if constexpr (ORDER == 5) {
             weno_interfaces(a.prm, e, S, vecL, vecR);
         } else {
             Eig<R> eN, eP;
@@ -406,7 +420,10 @@ template <class R> void launch_hydro3d_t(const Args3D &a, cudaStream_t s)
 {
     const int nb = 148 * 8;
     sig3d_kernel<R><<<nb, 256, 0, s>>>(a);
-    for (int d = 0; d < 3; d++) states3d_kernel<R><<<nb, 256, 0, s>>>(a, d);
+    for (int d = 0; d < 3; d++) {
+        if (a.prm.order == 5) states3d_kernel<R, 5><<<nb, 256, 0, s>>>(a, d);
+        else states3d_kernel<R, 3><<<nb, 256, 0, s>>>(a, d);
+    }
     for (int d = 0; d < 3; d++) flux3d_kernel<R><<<nb, 256, 0, s>>>(a, d);
     update3d_kernel<R><<<nb, 256, 0, s>>>(a);
 }
