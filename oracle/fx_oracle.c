@@ -27,6 +27,7 @@
  */
 #include "fx_oracle.h"
 
+#include <limits.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -970,3 +971,4 @@ int fxo_riemann(const fxo_params *p, int dir, const double VL[8], const double V
 }
 
 #include "fx_oracle_weno.inc"
+#include "fx_oracle_amr.inc"

@@ -85,6 +85,29 @@ int fxo_riemann(const fxo_params *p, int dir, const double VL[8], const double V
 /* Number of flops counted by the instrumented build (0 otherwise). */
 double fxo_flops_last_step(void);
 
+/* ---- block-structured AMR (PARAMESH) -------------------------------------
+ * Leaves are given by level (1-based) and block coordinates at that level;
+ * the oracle derives the parents, checks that the leaves tile the domain
+ * with 2:1 balance across faces, edges and corners, and keeps restricted
+ * parent data internally.  Leaf UNK is unk(var,i,j,k,leaf) as above, with
+ * cell sizes halving per level.  Error codes of create: 1 bad geometry,
+ * 2 level/coordinate out of range, 3 overlapping leaves, 4 incomplete tree,
+ * 5 not 2:1 balanced.  Step/fill codes: 3 unsupported options, 6 a guard
+ * cell with no covering block (unbalanced tree). */
+typedef struct fxo_amr fxo_amr;
+fxo_amr *fxo_amr_create(const fxo_params *p, int nleaf, const int *level, const int *bcoord, int *err);
+void fxo_amr_free(fxo_amr *a);
+int fxo_amr_info(const fxo_amr *a, int *nblk, int *maxlev);
+void fxo_amr_leaf_flags(const fxo_amr *a, int leaf, int finer[6], int eos[27]);
+/* Grid_fillGuardCells: restriction, same-level copies, prolongation,
+ * boundary conditions, Eos on the guard regions next to other levels. */
+int fxo_amr_fill_guardcells(fxo_amr *a, double *unk);
+/* levelFlux Hydro(): guard fill, fluxes of every leaf, flux correction at
+ * fine/coarse faces, update, energyFix, Eos. */
+int fxo_amr_hydro_step(fxo_amr *a, double *unk, double dt, int nthreads);
+int fxo_amr_compute_dt(const fxo_amr *a, const double *unk, double *dt_out);
+int fxo_amr_integrals(const fxo_amr *a, const double *unk, double out[7]);
+
 #ifdef __cplusplus
 }
 #endif

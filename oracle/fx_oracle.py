@@ -70,6 +70,16 @@ def lib():
         L.fxo_driver_dt.restype = ctypes.c_double
         L.fxo_integrals.argtypes = [P, D, D]
         L.fxo_riemann.argtypes = [P, ctypes.c_int, D, D, D]
+        I = ctypes.POINTER(ctypes.c_int)
+        L.fxo_amr_create.argtypes = [P, ctypes.c_int, I, I, I]
+        L.fxo_amr_create.restype = ctypes.c_void_p
+        L.fxo_amr_free.argtypes = [ctypes.c_void_p]
+        L.fxo_amr_info.argtypes = [ctypes.c_void_p, I, I]
+        L.fxo_amr_leaf_flags.argtypes = [ctypes.c_void_p, ctypes.c_int, I, I]
+        L.fxo_amr_fill_guardcells.argtypes = [ctypes.c_void_p, D]
+        L.fxo_amr_hydro_step.argtypes = [ctypes.c_void_p, D, ctypes.c_double, ctypes.c_int]
+        L.fxo_amr_compute_dt.argtypes = [ctypes.c_void_p, D, D]
+        L.fxo_amr_integrals.argtypes = [ctypes.c_void_p, D, D]
         _lib = L
     return _lib
 
@@ -149,3 +159,68 @@ def riemann(p, direction, VL, VR):
     if rc:
         raise RuntimeError("Riemann solver ierr")
     return F
+
+
+class Amr:
+    """Oracle of the block-structured AMR step (fx_oracle_amr.inc).  `levels`
+    and `bcoords` list the leaves (level from 1, block coordinates at that
+    level); leaf UNK arrays are (nleaf, k, j, i, var) with guard cells."""
+
+    ERRORS = {1: "bad geometry", 2: "level or coordinate out of range", 3: "overlapping leaves",
+              4: "incomplete tree", 5: "not 2:1 balanced"}
+
+    def __init__(self, p, levels, bcoords):
+        self.p = p
+        lv = np.ascontiguousarray(levels, dtype=np.int32)
+        bc = np.ascontiguousarray(bcoords, dtype=np.int32).reshape(-1, 3)
+        err = ctypes.c_int()
+        I = ctypes.POINTER(ctypes.c_int)
+        self.h = lib().fxo_amr_create(ctypes.byref(p), len(lv), lv.ctypes.data_as(I),
+                                      bc.ctypes.data_as(I), ctypes.byref(err))
+        if not self.h:
+            raise ValueError(f"oracle AMR tree rejected: {self.ERRORS.get(err.value, err.value)}")
+        self.nleaf = len(lv)
+
+    def close(self):
+        if self.h:
+            lib().fxo_amr_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self):
+        nb, ml = ctypes.c_int(), ctypes.c_int()
+        lib().fxo_amr_info(self.h, ctypes.byref(nb), ctypes.byref(ml))
+        return nb.value, ml.value
+
+    def leaf_flags(self, leaf):
+        fin = (ctypes.c_int * 6)()
+        eos = (ctypes.c_int * 27)()
+        lib().fxo_amr_leaf_flags(self.h, leaf, fin, eos)
+        return list(fin), list(eos)
+
+    def fill_guardcells(self, unk):
+        rc = lib().fxo_amr_fill_guardcells(self.h, _dp(unk))
+        if rc:
+            raise RuntimeError(f"oracle AMR guard fill failed with code {rc}")
+
+    def hydro_step(self, unk, dt, nthreads=0):
+        rc = lib().fxo_amr_hydro_step(self.h, _dp(unk), dt, nthreads)
+        if rc:
+            raise RuntimeError(f"oracle AMR hydro step failed with code {rc}")
+
+    def compute_dt(self, unk):
+        out = ctypes.c_double()
+        rc = lib().fxo_amr_compute_dt(self.h, _dp(unk), ctypes.byref(out))
+        if rc:
+            raise RuntimeError("oracle: computed dt is not positive")
+        return out.value
+
+    def integrals(self, unk):
+        out = np.zeros(7)
+        lib().fxo_amr_integrals(self.h, _dp(unk), _dp(out))
+        return out
