@@ -1,0 +1,879 @@
+// fxb_amr.cu -- block-structured AMR (PARAMESH layout) for the 3-D hydro path.
+//
+// One Hydro() step on a frozen mesh of leaf blocks at several refinement
+// levels, as levelFlux/Hydro.F90:161-270 does it with PARAMESH:
+//   1. restriction of every parent from its children, deepest level first,
+//      in conserved form (mpi_amr_1blk_restrict.F90:303-325,813 with the
+//      order-1 weights of amr_restrict_unk_genorder.F90)
+//   2. guard cells of every leaf: copied from the same-level block (leaf, or
+//      parent holding restricted data) or, where the neighbour is coarser,
+//      interpolated multilinearly from the parent level in conserved form
+//      (amr_1blk_cc_prol_linear.F90 with the index map of
+//      amr_prolong_cc_fun_init.F90, PER_MASS variables multiplied by dens
+//      before and divided after: flash_(un)convert_cc_hook.F90); boundary
+//      conditions map positions into the domain first; Eos(MODE_DENS_EI) on
+//      the guard regions whose neighbour is at another level
+//      (Eos_guardCells.F90 with corners and skipSrl)
+//   3. fluxes of every leaf with the 3-D pipeline of fxb_hydro3d.cuh,
+//      boundary fluxes saved (Grid_putFluxData), fluxes on faces next to
+//      finer leaves replaced by the restricted fine fluxes
+//      (Grid_conserveFluxes, amr_restrict_red.F90), then the update,
+//      energyFix, Eos and the CFL rate of every leaf.
+// The leaves' interiors live in two stores swapped every step; guard-filled
+// blocks and the pipeline intermediates exist for one batch of leaves at a
+// time, sized to the free device memory.
+#include "fxb_amr.h"
+#include "fxb_launch.h"
+
+#include <algorithm>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <type_traits>
+#include <unordered_map>
+#include <vector>
+
+namespace fxb {
+namespace {
+
+struct HBlock {
+    int level;
+    int c[3];
+    int parent;
+    int child[8];
+    int leaf;        // leaf slot or -1
+    int nodetype;    // 1 leaf, 2 parent with a leaf child, 3 other parent
+};
+
+struct DevBlk {
+    int level, c0, c1, c2, parent;
+};
+
+// device-side description of the mesh for the guard-fill kernels
+struct MeshArgs {
+    const DevBlk *blk;
+    const int *ntab;            // [block][27] same-level neighbour, -1 none, -2 boundary
+    const double *store;        // interior store [block][var][cell]
+    long vstride, bstride;      // cells per block, NV_DEV * cells
+    int n, ng;                  // cells per block side, guard layers
+    int nb1[3];                 // root blocks per axis
+    int bc[6];
+    int *err;
+};
+
+constexpr int ERR_AMR = 16;     // guard cell without a covering block (device error word)
+
+struct State {
+    bool active = false;
+    AmrCommon C{};
+    int n = 0, ng = 0, nleaf = 0, nblk = 0, maxlev = 1;
+    std::vector<HBlock> blk;
+    std::vector<int> leaf_blk;
+    std::vector<std::vector<int>> parents_at;     // per level (1-based index)
+    // device
+    double *store[2] = {nullptr, nullptr};
+    int cur = 0;
+    long vstride = 0, bstride = 0;
+    DevBlk *d_blk = nullptr;
+    int *d_ntab = nullptr, *d_child = nullptr, *d_plist = nullptr;
+    std::vector<long> plist_off;                  // per level offset into d_plist
+    unsigned *d_eosmask = nullptr;
+    int *d_finer = nullptr, *d_fine = nullptr;
+    double *d_dxl = nullptr;
+    AmrEntry3 *d_entries = nullptr;               // [all][all, finer ones skipped][finer ones]
+    int batch = 0;
+    double *gcb = nullptr;
+    void *sig = nullptr, *w[3] = {nullptr, nullptr, nullptr}, *f[3] = {nullptr, nullptr, nullptr};
+    void *bflux = nullptr;
+    long nfc = 0;
+    double *stage = nullptr;                      // UNK staging for attach / sync
+    int stage_leaves = 0;
+    int *leaf_blk_dev = nullptr, *d_dmap = nullptr;
+    int nfiner = 0;
+    std::unordered_map<uint64_t, int> map;
+};
+State S;
+
+uint64_t key(int lev, const int c[3])
+{
+    return ((uint64_t)lev << 60) | ((uint64_t)(uint32_t)c[0] << 40) | ((uint64_t)(uint32_t)c[1] << 20) |
+           (uint64_t)(uint32_t)c[2];
+}
+
+int find(int lev, const int c[3])
+{
+    auto it = S.map.find(key(lev, c));
+    return it == S.map.end() ? -1 : it->second;
+}
+
+int nb_at(int lev, int d)
+{
+    const fxb_domain &D = S.C.dom;
+    int n0 = d == 0 ? D.nblockx : d == 1 ? D.nblocky : D.nblockz;
+    return n0 << (lev - 1);
+}
+
+int new_block(int lev, const int c[3])
+{
+    HBlock b;
+    b.level = lev;
+    for (int d = 0; d < 3; d++) b.c[d] = c[d];
+    b.parent = -1;
+    for (int q = 0; q < 8; q++) b.child[q] = -1;
+    b.leaf = -1;
+    b.nodetype = 3;
+    S.blk.push_back(b);
+    int id = (int)S.blk.size() - 1;
+    S.map[key(lev, c)] = id;
+    return id;
+}
+
+// same-level neighbour: block, -1 none at that level, -2 outside a non-periodic boundary
+int neigh(int b, int di, int dj, int dk)
+{
+    const HBlock &B = S.blk[b];
+    int off[3] = {di, dj, dk}, c[3];
+    for (int d = 0; d < 3; d++) {
+        c[d] = B.c[d] + off[d];
+        int nb = nb_at(B.level, d);
+        if (c[d] < 0 || c[d] >= nb) {
+            if (S.C.dom.bc[2 * d + (c[d] >= nb)] != FXB_BC_PERIODIC) return -2;
+            c[d] = (c[d] + nb) % nb;
+        }
+    }
+    return find(B.level, c);
+}
+
+// Grid_getBlkNeighLevels(trackBdry) + Eos_guardCells(corners, skipSrl): bit r
+// set for every guard region r = (rk+1)*9 + (rj+1)*3 + (ri+1) whose
+// neighbour level differs from the block's own
+unsigned eos_regions(int b)
+{
+    const int me = S.blk[b].level;
+    int lev[3][3][3], bnd[3][3][3];
+    for (int k = -1; k <= 1; k++) for (int j = -1; j <= 1; j++) for (int i = -1; i <= 1; i++) {
+        int nb = (i | j | k) ? neigh(b, i, j, k) : b;
+        bnd[i + 1][j + 1][k + 1] = nb == -2;
+        if (nb == -1) lev[i + 1][j + 1][k + 1] = me - 1;
+        else if (nb >= 0 && S.blk[nb].nodetype == 2) lev[i + 1][j + 1][k + 1] = me + 1;
+        else lev[i + 1][j + 1][k + 1] = me;
+    }
+    for (int pass = 2; pass <= 3; pass++) {
+        for (int k = -1; k <= 1; k++) for (int j = -1; j <= 1; j++) for (int i = -1; i <= 1; i++) {
+            if (abs(i) + abs(j) + abs(k) != pass) continue;
+            if (lev[i + 1][j + 1][k + 1] != me || !bnd[i + 1][j + 1][k + 1]) continue;
+            // the k range of the reference ends at min(1, j+1)
+            int klo = std::max(-1, k - 1), khi = std::min(1, j + 1);
+            int ilo = std::max(-1, i - 1), ihi = std::min(1, i + 1);
+            int jlo = std::max(-1, j - 1), jhi = std::min(1, j + 1);
+            int mn = INT32_MAX, mx = INT32_MIN;
+            for (int kk = klo; kk <= khi; kk++) for (int jj = jlo; jj <= jhi; jj++) for (int ii = ilo; ii <= ihi; ii++) {
+                mn = std::min(mn, lev[ii + 1][jj + 1][kk + 1]);
+                mx = std::max(mx, lev[ii + 1][jj + 1][kk + 1]);
+            }
+            lev[i + 1][j + 1][k + 1] = mn < me ? mn : mx;
+        }
+    }
+    unsigned mask = 0;
+    for (int k = -1; k <= 1; k++) for (int j = -1; j <= 1; j++) for (int i = -1; i <= 1; i++)
+        if ((i | j | k) && lev[i + 1][j + 1][k + 1] != me) mask |= 1u << ((k + 1) * 9 + (j + 1) * 3 + (i + 1));
+    return mask;
+}
+
+int build_tree(const fxb_block_desc *leaves, int nleaf, std::vector<int> &finer, std::vector<int> &fine)
+{
+    S.blk.clear();
+    S.map.clear();
+    S.blk.reserve(2 * (size_t)nleaf + 64);
+    S.leaf_blk.assign(nleaf, -1);
+    S.maxlev = 1;
+    for (int l = 0; l < nleaf; l++) {
+        int lev = leaves[l].level;
+        int c[3] = {leaves[l].bcoord[0], leaves[l].bcoord[1], leaves[l].bcoord[2]};
+        if (lev < 1 || lev > 15) return record_error(FXB_EARG, "fxb_register_blocks: refinement level out of range");
+        for (int d = 0; d < 3; d++)
+            if (c[d] < 0 || c[d] >= nb_at(lev, d))
+                return record_error(FXB_EARG, "fxb_register_blocks: block coordinate out of range");
+        if (find(lev, c) >= 0) return record_error(FXB_EARG, "fxb_register_blocks: duplicate leaf");
+        int id = new_block(lev, c);
+        S.blk[id].leaf = l;
+        S.blk[id].nodetype = 1;
+        S.leaf_blk[l] = id;
+        S.maxlev = std::max(S.maxlev, lev);
+    }
+    for (int l = 0; l < nleaf; l++) {
+        int id = S.leaf_blk[l];
+        while (S.blk[id].level > 1) {
+            int pc[3] = {S.blk[id].c[0] / 2, S.blk[id].c[1] / 2, S.blk[id].c[2] / 2};
+            int plev = S.blk[id].level - 1;
+            int pid = find(plev, pc);
+            if (pid < 0) pid = new_block(plev, pc);
+            else if (S.blk[pid].leaf >= 0)
+                return record_error(FXB_EARG, "fxb_register_blocks: a leaf overlaps another leaf's parent");
+            int q = (S.blk[id].c[0] & 1) | ((S.blk[id].c[1] & 1) << 1) | ((S.blk[id].c[2] & 1) << 2);
+            S.blk[pid].child[q] = id;
+            S.blk[id].parent = pid;
+            id = pid;
+        }
+    }
+    long roots = 0, nroot = (long)nb_at(1, 0) * nb_at(1, 1) * nb_at(1, 2);
+    for (auto &B : S.blk) {
+        if (B.level == 1) roots++;
+        if (B.leaf >= 0) continue;
+        bool any_leaf = false;
+        for (int q = 0; q < 8; q++) {
+            if (B.child[q] < 0) return record_error(FXB_EARG, "fxb_register_blocks: the leaves do not tile the domain");
+            if (S.blk[B.child[q]].leaf >= 0) any_leaf = true;
+        }
+        B.nodetype = any_leaf ? 2 : 3;
+    }
+    if (roots != nroot) return record_error(FXB_EARG, "fxb_register_blocks: the leaves do not tile the domain");
+    S.nblk = (int)S.blk.size();
+    // 2:1 balance across faces, edges and corners
+    for (int l = 0; l < nleaf; l++) {
+        int b = S.leaf_blk[l];
+        for (int k = -1; k <= 1; k++) for (int j = -1; j <= 1; j++) for (int i = -1; i <= 1; i++) {
+            if (!(i | j | k)) continue;
+            int nb = neigh(b, i, j, k);
+            if (nb >= 0 && S.blk[nb].nodetype == 3)
+                return record_error(FXB_EARG, "fxb_register_blocks: neighbouring leaves differ by more than one level");
+            if (nb == -1) {
+                int off[3] = {i, j, k}, c[3];
+                for (int d = 0; d < 3; d++) {
+                    int nbd = nb_at(S.blk[b].level, d);
+                    c[d] = ((S.blk[b].c[d] + off[d]) % nbd + nbd) % nbd / 2;
+                }
+                int cov = find(S.blk[b].level - 1, c);
+                if (cov < 0 || S.blk[cov].leaf < 0)
+                    return record_error(FXB_EARG, "fxb_register_blocks: neighbouring leaves differ by more than one level");
+            }
+        }
+    }
+    // faces next to refined regions and the fine leaves across them
+    finer.assign(nleaf, 0);
+    fine.assign((size_t)nleaf * 24, -1);
+    for (int l = 0; l < nleaf; l++) {
+        int b = S.leaf_blk[l];
+        for (int f = 0; f < 6; f++) {
+            int d = f >> 1, side = f & 1;
+            int off[3] = {0, 0, 0};
+            off[d] = side ? 1 : -1;
+            int nb = neigh(b, off[0], off[1], off[2]);
+            if (nb < 0 || S.blk[nb].nodetype != 2) continue;
+            finer[l] |= 1 << f;
+            int a1 = d == 0 ? 1 : 0, a2 = d == 2 ? 1 : 2;
+            for (int q = 0; q < 4; q++) {
+                int cc[3];
+                cc[d] = S.blk[nb].c[d] * 2 + (side ? 0 : 1);
+                cc[a1] = 2 * S.blk[nb].c[a1] + (q & 1);
+                cc[a2] = 2 * S.blk[nb].c[a2] + (q >> 1);
+                int fb = find(S.blk[b].level + 1, cc);
+                if (fb < 0 || S.blk[fb].leaf < 0)
+                    return record_error(FXB_EARG, "fxb_register_blocks: neighbouring leaves differ by more than one level");
+                fine[(size_t)l * 24 + f * 4 + q] = S.blk[fb].leaf;
+            }
+        }
+    }
+    return FXB_OK;
+}
+
+// ------------------------------------------------------------------ device
+__device__ __forceinline__ int fdiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+// PER_MASS variables of UNK (velx vely velz ener eint) in device order
+__device__ __forceinline__ bool per_mass(int v) { return v == VX || v == VY || v == VZ || v == DV_ENER || v == EI; }
+
+// Eos_wrapped(MODE_DENS_EI) of one cell (Gamma/Eos.F90:238-250)
+__device__ void eos_cell_dev(double u[NV_DEV], const DevParams &prm, double gam1inv, double ggprodinv)
+{
+    double ekin = 0.5 * (u[VX] * u[VX] + u[VY] * u[VY] + u[VZ] * u[VZ]);
+    double eint = u[EI];
+    if (u[DV_ENER] - ekin > fmax2(prm.small_e, prm.eint_switch * ekin)) eint = u[DV_ENER] - ekin;
+    double dens = u[D];
+    double pres = dens * eint * gam1inv;
+    u[P] = pres;
+    u[DV_TEMP] = eint * ggprodinv * prm.abar;
+    u[GC] = prm.gamma;
+    u[EI] = eint;
+    u[DV_ENER] = eint + ekin;
+    u[GE] = pres / (eint * dens) + 1;
+}
+
+// non-periodic boundary map of one level-l cell index along axis a
+__device__ __forceinline__ int bc_map(const MeshArgs &m, int lev, int a, int x, double *sg)
+{
+    const int N = (m.nb1[a] << (lev - 1)) * m.n;
+    if (x < 0) {
+        int bc = m.bc[2 * a];
+        if (bc == FXB_BC_OUTFLOW) return 0;
+        if (bc == FXB_BC_REFLECTING) { *sg = -*sg; return -1 - x; }
+    } else if (x >= N) {
+        int bc = m.bc[2 * a + 1];
+        if (bc == FXB_BC_OUTFLOW) return N - 1;
+        if (bc == FXB_BC_REFLECTING) { *sg = -*sg; return 2 * N - 1 - x; }
+    }
+    return x;   // inside, or periodic (left unwrapped: the neighbour table wraps)
+}
+
+// value of the level-lev cell x (unwrapped along periodic axes, inside along
+// the others) from the block holding it among block b's 27 neighbours
+__device__ __forceinline__ bool same_level(const MeshArgs &m, int b, const DevBlk &B, const int x[3], double out[NV_DEV])
+{
+    int r[3], loc[3];
+    const int bc[3] = {B.c0, B.c1, B.c2};
+    for (int a = 0; a < 3; a++) {
+        r[a] = fdiv(x[a] - bc[a] * m.n, m.n);
+        if (r[a] < -1 || r[a] > 1) return false;
+        loc[a] = x[a] - (bc[a] + r[a]) * m.n;
+    }
+    int nb = m.ntab[(long)b * 27 + (r[2] + 1) * 9 + (r[1] + 1) * 3 + (r[0] + 1)];
+    if (nb < 0) return false;
+    const double *s = m.store + (long)nb * m.bstride + ((long)loc[2] * m.n + loc[1]) * m.n + loc[0];
+#pragma unroll
+    for (int v = 0; v < NV_DEV; v++) out[v] = s[v * m.vstride];
+    return true;
+}
+
+// guard value of leaf block b at level-lev cell x
+__device__ bool guard_value(const MeshArgs &m, int b, const int xin[3], double out[NV_DEV])
+{
+    const DevBlk B = m.blk[b];
+    int x[3];
+    double sg[3] = {1., 1., 1.};
+    for (int a = 0; a < 3; a++) x[a] = bc_map(m, B.level, a, xin[a], &sg[a]);
+    if (same_level(m, b, B, x, out)) {
+        out[VX] = out[VX] * sg[0]; out[VY] = out[VY] * sg[1]; out[VZ] = out[VZ] * sg[2];
+        return true;
+    }
+    if (B.parent < 0) return false;
+    // coarser neighbour: amr_1blk_cc_prol_linear from the parent level, conserved form
+    const int pb = B.parent;
+    const DevBlk PB = m.blk[pb];
+    int p1[3];
+    double wl[3];
+    for (int a = 0; a < 3; a++) {
+        p1[a] = fdiv(x[a] + 1, 2) - 1;
+        wl[a] = ((x[a] & 1) == 0) ? 0.25 : 0.75;
+    }
+    double S8[2][2][2][NV_DEV];
+    for (int kk = 0; kk < 2; kk++) for (int jj = 0; jj < 2; jj++) for (int ii = 0; ii < 2; ii++) {
+        int q[3] = {p1[0] + ii, p1[1] + jj, p1[2] + kk};
+        double sq[3] = {1., 1., 1.};
+        for (int a = 0; a < 3; a++) q[a] = bc_map(m, PB.level, a, q[a], &sq[a]);
+        double *s = S8[kk][jj][ii];
+        if (!same_level(m, pb, PB, q, s)) return false;
+        s[VX] = s[VX] * sq[0]; s[VY] = s[VY] * sq[1]; s[VZ] = s[VZ] * sq[2];
+#pragma unroll
+        for (int v = 0; v < NV_DEV; v++)
+            if (per_mass(v)) s[v] = s[D] * s[v];
+    }
+    const double dx = wl[0], cx = 1. - wl[0], dy = wl[1], cy = 1. - wl[1], dz = wl[2], cz = 1. - wl[2];
+#pragma unroll
+    for (int v = 0; v < NV_DEV; v++)
+        out[v] = dz * (dy * (dx * S8[0][0][0][v] + cx * S8[0][0][1][v]) + cy * (dx * S8[0][1][0][v] + cx * S8[0][1][1][v])) +
+                 cz * (dy * (dx * S8[1][0][0][v] + cx * S8[1][0][1][v]) + cy * (dx * S8[1][1][0][v] + cx * S8[1][1][1][v]));
+    double dinv = out[D] == 0.0 ? 0.0 : 1. / out[D];
+#pragma unroll
+    for (int v = 0; v < NV_DEV; v++)
+        if (per_mass(v)) out[v] = dinv * out[v];
+    out[VX] = out[VX] * sg[0]; out[VY] = out[VY] * sg[1]; out[VZ] = out[VZ] * sg[2];
+    return true;
+}
+
+// guard-filled copies of a batch of leaves: gcb[entry][var][nz+2g][ny+2g][nx+2g]
+__global__ void __launch_bounds__(256) amr_fill_kernel(MeshArgs m, const AmrEntry3 *entries, const int *leaf_blk,
+                                                       const unsigned *eosmask, double *gcb, long gvs, long gbs,
+                                                       DevParams prm, double gam1inv, double ggprodinv)
+{
+    const AmrEntry3 e = entries[blockIdx.y];
+    const int b = leaf_blk[e.leaf];
+    const DevBlk B = m.blk[b];
+    const unsigned mask = eosmask[e.leaf];
+    const int n = m.n, g = m.ng, ne = n + 2 * g;
+    const long ncell = (long)ne * ne * ne;
+    double *dst = gcb + (long)blockIdx.y * gbs;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < ncell; idx += (long)gridDim.x * blockDim.x) {
+        int i = (int)(idx % ne) - g, j = (int)((idx / ne) % ne) - g, k = (int)(idx / ((long)ne * ne)) - g;
+        double u[NV_DEV];
+        int ri = i < 0 ? -1 : i >= n ? 1 : 0, rj = j < 0 ? -1 : j >= n ? 1 : 0, rk = k < 0 ? -1 : k >= n ? 1 : 0;
+        if (!(ri | rj | rk)) {
+            const double *s = m.store + (long)b * m.bstride + ((long)k * n + j) * n + i;
+#pragma unroll
+            for (int v = 0; v < NV_DEV; v++) u[v] = s[v * m.vstride];
+        } else {
+            int x[3] = {B.c0 * n + i, B.c1 * n + j, B.c2 * n + k};
+            if (!guard_value(m, b, x, u)) {
+                atomicOr(m.err, ERR_AMR);
+#pragma unroll
+                for (int v = 0; v < NV_DEV; v++) u[v] = 0.;
+            } else if ((mask >> ((rk + 1) * 9 + (rj + 1) * 3 + (ri + 1))) & 1u) {
+                eos_cell_dev(u, prm, gam1inv, ggprodinv);
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < NV_DEV; v++) dst[v * gvs + idx] = u[v];
+    }
+}
+
+// restriction of the parents of one level (amr_restrict_unk_genorder, order 1)
+__global__ void __launch_bounds__(256) amr_restrict_kernel(double *store, long vstride, long bstride, int n,
+                                                           const int *plist, int np, const int *child)
+{
+    const long per = (long)n * n * n;
+    const int h = n / 2;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)np * per; idx += (long)gridDim.x * blockDim.x) {
+        const int p = plist[idx / per];
+        const long c = idx % per;
+        const int pi = (int)(c % n), pj = (int)((c / n) % n), pk = (int)(c / ((long)n * n));
+        const int q = (pi >= h) | ((pj >= h) << 1) | ((pk >= h) << 2);
+        const int ch = child[(long)p * 8 + q];
+        const int i0 = 2 * (pi - (q & 1) * h), j0 = 2 * (pj - ((q >> 1) & 1) * h), k0 = 2 * (pk - ((q >> 2) & 1) * h);
+        const double *cs = store + (long)ch * bstride;
+        double s[NV_DEV];
+#pragma unroll
+        for (int v = 0; v < NV_DEV; v++) s[v] = 0.;
+        const double w = 0.5 * 0.5 * 0.5;
+        for (int kk = 0; kk < 2; kk++) for (int jj = 0; jj < 2; jj++) for (int ii = 0; ii < 2; ii++) {
+            const long cc = ((long)(k0 + kk) * n + (j0 + jj)) * n + (i0 + ii);
+            const double dens = cs[D * vstride + cc];
+#pragma unroll
+            for (int v = 0; v < NV_DEV; v++) {
+                double x = cs[v * vstride + cc];
+                if (per_mass(v)) x = dens * x;
+                s[v] = s[v] + w * x;
+            }
+        }
+        double dinv = s[D] == 0.0 ? 0.0 : 1. / s[D];
+        double *ps = store + (long)p * bstride + c;
+#pragma unroll
+        for (int v = 0; v < NV_DEV; v++) ps[v * vstride] = per_mass(v) ? dinv * s[v] : s[v];
+    }
+}
+
+// UNK staging (leaf, k, j, i, var with guard cells) <-> interior store / guard-filled blocks
+__global__ void amr_unk_to_store_kernel(const double *unk, int l0, int nl, const int *leaf_blk, double *store,
+                                        long vstride, long bstride, int n, int ng, int nunk, const int *dmap)
+{
+    const long per = (long)n * n * n;
+    const int ne = n + 2 * ng;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)nl * per; idx += (long)gridDim.x * blockDim.x) {
+        const int l = (int)(idx / per);
+        const long c = idx % per;
+        const int i = (int)(c % n), j = (int)((c / n) % n), k = (int)(c / ((long)n * n));
+        const double *u = unk + ((((long)l * ne + k + ng) * ne + j + ng) * ne + i + ng) * nunk;
+        double *s = store + (long)leaf_blk[l0 + l] * bstride + c;
+        for (int v = 0; v < NV_DEV; v++) s[v * vstride] = u[dmap[v]];
+    }
+}
+
+__global__ void amr_gcb_to_unk_kernel(const double *gcb, long gvs, long gbs, int nl, double *unk, int ne, int nunk,
+                                      const int *dmap)
+{
+    const long per = (long)ne * ne * ne;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)nl * per; idx += (long)gridDim.x * blockDim.x) {
+        const int l = (int)(idx / per);
+        const long c = idx % per;
+        const double *g = gcb + (long)l * gbs + c;
+        double *u = unk + idx * nunk;
+        for (int v = 0; v < NV_DEV; v++) u[dmap[v]] = g[v * gvs];
+    }
+}
+
+// Eos, CFL rate and volume integrals over the leaves' interiors
+__global__ void amr_eos_kernel(double *store, long vstride, long bstride, int n, const int *leaf_blk, int nleaf,
+                               DevParams prm, double gam1inv, double ggprodinv)
+{
+    const long per = (long)n * n * n;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)nleaf * per; idx += (long)gridDim.x * blockDim.x) {
+        double *s = store + (long)leaf_blk[idx / per] * bstride + idx % per;
+        double u[NV_DEV];
+        for (int v = 0; v < NV_DEV; v++) u[v] = s[v * vstride];
+        eos_cell_dev(u, prm, gam1inv, ggprodinv);
+        for (int v = 0; v < NV_DEV; v++) s[v * vstride] = u[v];
+    }
+}
+
+__global__ void amr_rate_kernel(const double *store, long vstride, long bstride, int n, const int *leaf_blk,
+                                const DevBlk *blk, const double *dxl, int nleaf, unsigned long long *rate_max)
+{
+    const long per = (long)n * n * n;
+    double r = 0.;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)nleaf * per; idx += (long)gridDim.x * blockDim.x) {
+        const int b = leaf_blk[idx / per];
+        const double *s = store + (long)b * bstride + idx % per;
+        const double *dl = dxl + 3 * (blk[b].level - 1);
+        double cs = sqrt(s[GC * vstride] * s[P * vstride] / s[D * vstride]);
+        double t = (fabs(s[VX * vstride] - 0.) + cs) * (1.0 / dl[0]);
+        t = fmax2(t, (fabs(s[VY * vstride] - 0.) + cs) * (1.0 / dl[1]));
+        t = fmax2(t, (fabs(s[VZ * vstride] - 0.) + cs) * (1.0 / dl[2]));
+        r = fmax2(r, t);
+    }
+    for (int off = 16; off > 0; off >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, off));
+    if ((threadIdx.x & 31) == 0) atomicMax(rate_max, (unsigned long long)__double_as_longlong(r));
+}
+
+__global__ void amr_integrals_kernel(const double *store, long vstride, long bstride, int n, const int *leaf_blk,
+                                     const DevBlk *blk, const double *dxl, int nleaf, double *partials)
+{
+    const long per = (long)n * n * n;
+    double s[7] = {0., 0., 0., 0., 0., 0., 0.};
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)nleaf * per; idx += (long)gridDim.x * blockDim.x) {
+        const int b = leaf_blk[idx / per];
+        const double *c = store + (long)b * bstride + idx % per;
+        const double *dl = dxl + 3 * (blk[b].level - 1);
+        const double dv = dl[0] * dl[1] * dl[2];
+        double rho = c[D * vstride], vx = c[VX * vstride], vy = c[VY * vstride], vz = c[VZ * vstride];
+        s[0] += rho * dv; s[1] += rho * vx * dv; s[2] += rho * vy * dv; s[3] += rho * vz * dv;
+        s[4] += rho * c[DV_ENER * vstride] * dv; s[5] += rho * c[EI * vstride] * dv;
+        s[6] += 0.5 * rho * (vx * vx + vy * vy + vz * vz) * dv;
+    }
+    __shared__ double sh[7][256];
+    for (int q = 0; q < 7; q++) sh[q][threadIdx.x] = s[q];
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int q = 0; q < 7; q++) sh[q][threadIdx.x] += sh[q][threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 7; q++) partials[blockIdx.x * 7 + q] = sh[q][0];
+}
+
+__global__ void amr_integrals_final_kernel(const double *partials, int np, double *out)
+{
+    if (threadIdx.x < 7) {
+        double t = 0.;
+        for (int b = 0; b < np; b++) t += partials[b * 7 + threadIdx.x];
+        out[threadIdx.x] = t;
+    }
+}
+
+// ------------------------------------------------------------------ host
+#define CKA(call)                                                                          \
+    do {                                                                                   \
+        cudaError_t _e = (call);                                                           \
+        if (_e != cudaSuccess) {                                                           \
+            char _b[256];                                                                  \
+            snprintf(_b, sizeof(_b), "%s: %s", #call, cudaGetErrorString(_e));             \
+            return record_error(FXB_ECUDA, _b);                                            \
+        }                                                                                  \
+    } while (0)
+
+template <class T> void dfree(T *&p)
+{
+    if (p) cudaFree((void *)p);
+    p = nullptr;
+}
+
+MeshArgs mesh_args(int which)
+{
+    MeshArgs m;
+    m.blk = S.d_blk; m.ntab = S.d_ntab; m.store = S.store[which];
+    m.vstride = S.vstride; m.bstride = S.bstride; m.n = S.n; m.ng = S.ng;
+    m.nb1[0] = S.C.dom.nblockx; m.nb1[1] = S.C.dom.nblocky; m.nb1[2] = S.C.dom.nblockz;
+    for (int i = 0; i < 6; i++) m.bc[i] = S.C.dom.bc[i];
+    m.err = S.C.err;
+    return m;
+}
+
+size_t rsize() { return S.C.prm.precision == FXB_MIXED ? sizeof(float) : sizeof(double); }
+long ne3() { long e = S.n + 2 * S.ng; return e * e * e; }
+
+Args3D batch_args(const double *dtv, double dt)
+{
+    Args3D a;
+    memset(&a, 0, sizeof(a));
+    a.nx = a.ny = a.nz = S.n;
+    for (int i = 0; i < 6; i++) a.bc[i] = S.C.dom.bc[i];
+    a.dt_arg = dt; a.dtv = dtv;
+    a.gam1inv = S.C.gam1inv; a.ggprodinv = S.C.ggprodinv;
+    a.prm = S.C.dprm; a.rate_max = S.C.rate_max; a.err = S.C.err;
+    a.sig = S.sig;
+    for (int d = 0; d < 3; d++) { a.wst[d] = S.w[d]; a.flx[d] = S.f[d]; }
+    a.gcb = S.gcb; a.gcb_vstride = ne3(); a.gcb_bstride = ne3() * NV_DEV; a.ng = S.ng;
+    a.dxl = S.d_dxl;
+    a.odata = S.store[1 - S.cur]; a.o_vstride = S.vstride; a.o_bstride = S.bstride;
+    const size_t r = rsize();
+    a.sig_bstride = (long)(sig3d_bytes(S.n, S.n, S.n, r) / r);
+    for (int d = 0; d < 3; d++) {
+        a.w_bstride[d] = (long)(w3d_bytes(d, S.n, S.n, S.n, r) / r);
+        a.f_bstride[d] = (long)(f3d_bytes(d, S.n, S.n, S.n, r) / r);
+    }
+    return a;
+}
+
+void restrict_all(int which)
+{
+    for (int lev = S.maxlev - 1; lev >= 1; lev--) {
+        int np = (int)S.parents_at[lev].size();
+        if (!np) continue;
+        long work = (long)np * S.n * S.n * S.n;
+        int grid = (int)std::min<long>((work + 255) / 256, 148L * 16);
+        amr_restrict_kernel<<<grid, 256, 0, S.C.stream>>>(S.store[which], S.vstride, S.bstride, S.n,
+                                                          S.d_plist + S.plist_off[lev], np, S.d_child);
+    }
+}
+
+void fill_batch(const AmrEntry3 *entries, int cnt, int which)
+{
+    amr_fill_kernel<<<dim3(8, cnt), 256, 0, S.C.stream>>>(mesh_args(which), entries, S.leaf_blk_dev, S.d_eosmask,
+                                                         S.gcb, ne3(), ne3() * NV_DEV, S.C.dprm, S.C.gam1inv,
+                                                         S.C.ggprodinv);
+}
+
+} // namespace
+
+// ----------------------------------------------------------------- interface
+bool amr_active() { return S.active; }
+int amr_cur() { return S.cur; }
+long amr_leaf_cells() { return (long)S.nleaf * S.n * S.n * S.n; }
+
+void amr_destroy()
+{
+    dfree(S.store[0]); dfree(S.store[1]);
+    dfree(S.d_blk); dfree(S.d_ntab); dfree(S.d_child); dfree(S.d_plist); dfree(S.d_eosmask);
+    dfree(S.d_finer); dfree(S.d_fine); dfree(S.d_dxl); dfree(S.d_entries); dfree(S.leaf_blk_dev);
+    dfree(S.gcb); dfree(S.sig);
+    for (int d = 0; d < 3; d++) { dfree(S.w[d]); dfree(S.f[d]); }
+    dfree(S.bflux); dfree(S.stage); dfree(S.d_dmap);
+    S = State();
+}
+
+int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
+{
+    amr_destroy();
+    S.C = c;
+    const fxb_domain &D = c.dom;
+    if (D.ndim != 3) return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: AMR meshes are implemented for 3-D");
+    if (D.nxb != D.nyb || D.nxb != D.nzb || D.nxb % 2 || D.nxb < D.nguard)
+        return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: AMR blocks must be cubes of an even size >= NGUARD");
+    if (c.prm.use_gravity) return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: gravity is not implemented on AMR meshes");
+    S.n = D.nxb;
+    S.ng = D.nguard;
+    S.nleaf = nleaf;
+    std::vector<int> finer, fine;
+    int rc = build_tree(leaves, nleaf, finer, fine);
+    if (rc) { S = State(); return rc; }
+    S.parents_at.assign(S.maxlev + 1, {});
+    for (int b = 0; b < S.nblk; b++)
+        if (S.blk[b].leaf < 0) S.parents_at[S.blk[b].level].push_back(b);
+    std::vector<int> plist;
+    S.plist_off.assign(S.maxlev + 1, 0);
+    for (int lev = 1; lev <= S.maxlev; lev++) {
+        S.plist_off[lev] = (long)plist.size();
+        plist.insert(plist.end(), S.parents_at[lev].begin(), S.parents_at[lev].end());
+    }
+    std::vector<DevBlk> hb(S.nblk);
+    std::vector<int> ntab((size_t)S.nblk * 27), child((size_t)S.nblk * 8);
+    for (int b = 0; b < S.nblk; b++) {
+        const HBlock &B = S.blk[b];
+        hb[b] = DevBlk{B.level, B.c[0], B.c[1], B.c[2], B.parent};
+        for (int k = -1; k <= 1; k++) for (int j = -1; j <= 1; j++) for (int i = -1; i <= 1; i++)
+            ntab[(size_t)b * 27 + (k + 1) * 9 + (j + 1) * 3 + (i + 1)] = (i | j | k) ? neigh(b, i, j, k) : b;
+        for (int q = 0; q < 8; q++) child[(size_t)b * 8 + q] = B.child[q];
+    }
+    std::vector<unsigned> eos(nleaf);
+    for (int l = 0; l < nleaf; l++) eos[l] = eos_regions(S.leaf_blk[l]);
+    std::vector<double> dxl(3 * (size_t)S.maxlev);
+    double d0[3];
+    for (int a = 0; a < 3; a++) {
+        int nb = a == 0 ? D.nblockx : a == 1 ? D.nblocky : D.nblockz;
+        int nn = a == 0 ? D.nxb : a == 1 ? D.nyb : D.nzb;
+        d0[a] = (D.bbox[a][1] - D.bbox[a][0]) / (1.0 * nn * nb);   // gr_initSpecific.F90:172-178
+    }
+    for (int lev = 1; lev <= S.maxlev; lev++)
+        for (int a = 0; a < 3; a++) {
+            dxl[3 * (lev - 1) + a] = d0[a];
+            d0[a] = d0[a] / 2.0;
+        }
+    std::vector<AmrEntry3> ent;
+    ent.reserve(2 * (size_t)nleaf + 64);
+    for (int pass = 0; pass < 2; pass++)
+        for (int l = 0; l < nleaf; l++)
+            ent.push_back(AmrEntry3{S.leaf_blk[l], S.blk[S.leaf_blk[l]].level, l,
+                                    (pass == 1 && finer[l]) ? (int)AMR_SKIP_UPDATE : 0});
+    for (int l = 0; l < nleaf; l++)
+        if (finer[l]) ent.push_back(AmrEntry3{S.leaf_blk[l], S.blk[S.leaf_blk[l]].level, l, 0});
+    S.nfiner = (int)ent.size() - 2 * nleaf;
+
+    cudaStream_t st = c.stream;
+    S.vstride = (long)S.n * S.n * S.n;
+    S.bstride = S.vstride * NV_DEV;
+    auto up = [&](auto *&dst, const auto &v) -> cudaError_t {
+        using T = typename std::remove_const<typename std::remove_reference<decltype(v[0])>::type>::type;
+        cudaError_t e = cudaMalloc((void **)&dst, sizeof(T) * std::max<size_t>(1, v.size()));
+        if (e != cudaSuccess) return e;
+        if (v.empty()) return cudaSuccess;
+        return cudaMemcpyAsync((void *)dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st);
+    };
+    for (int i = 0; i < 2; i++) {
+        CKA(cudaMalloc(&S.store[i], sizeof(double) * S.bstride * S.nblk));
+        CKA(cudaMemsetAsync(S.store[i], 0, sizeof(double) * S.bstride * S.nblk, st));
+    }
+    CKA(up(S.d_blk, hb));
+    CKA(up(S.d_ntab, ntab));
+    CKA(up(S.d_child, child));
+    CKA(up(S.d_plist, plist));
+    CKA(up(S.d_eosmask, eos));
+    CKA(up(S.d_finer, finer));
+    CKA(up(S.d_fine, fine));
+    CKA(up(S.d_dxl, dxl));
+    CKA(up(S.d_entries, ent));
+    CKA(up(S.leaf_blk_dev, S.leaf_blk));
+    std::vector<int> dm(c.dmap, c.dmap + NV_DEV);
+    CKA(up(S.d_dmap, dm));
+    const size_t r = rsize();
+    S.nfc = (long)S.n * S.n;
+    CKA(cudaMalloc(&S.bflux, r * 6 * NF * S.nfc * (size_t)nleaf));
+    // UNK staging for attach/sync: chunks of up to 1 GiB
+    const size_t per_unk = sizeof(double) * ne3() * c.nunk;
+    S.stage_leaves = (int)std::max<size_t>(1, std::min<size_t>(nleaf, (1ull << 30) / per_unk));
+    CKA(cudaMalloc(&S.stage, per_unk * S.stage_leaves));
+    // batch of guard-filled blocks + pipeline intermediates: up to 60 % of what is free
+    const size_t per_entry = sizeof(double) * NV_DEV * ne3() + sig3d_bytes(S.n, S.n, S.n, r) +
+                             w3d_bytes(0, S.n, S.n, S.n, r) + w3d_bytes(1, S.n, S.n, S.n, r) + w3d_bytes(2, S.n, S.n, S.n, r) +
+                             f3d_bytes(0, S.n, S.n, S.n, r) + f3d_bytes(1, S.n, S.n, S.n, r) + f3d_bytes(2, S.n, S.n, S.n, r);
+    size_t fr = 0, tot = 0;
+    CKA(cudaMemGetInfo(&fr, &tot));
+    long cap = (long)((fr * 6 / 10) / per_entry);
+    if (cap < 1) return record_error(FXB_ECUDA, "fxb_register_blocks: not enough device memory for one AMR block");
+    S.batch = (int)std::min<long>(std::min<long>(cap, nleaf), 65535);
+    // FXB_AMR_MAX_BATCH caps the leaves processed per batch (device memory for
+    // guard-filled blocks and pipeline intermediates grows with it)
+    if (const char *ev = getenv("FXB_AMR_MAX_BATCH")) {
+        long mb = atol(ev);
+        if (mb >= 1) S.batch = (int)std::min<long>(S.batch, mb);
+    }
+    CKA(cudaMalloc(&S.gcb, sizeof(double) * NV_DEV * ne3() * S.batch));
+    CKA(cudaMalloc(&S.sig, sig3d_bytes(S.n, S.n, S.n, r) * S.batch));
+    for (int d = 0; d < 3; d++) {
+        CKA(cudaMalloc(&S.w[d], w3d_bytes(d, S.n, S.n, S.n, r) * S.batch));
+        CKA(cudaMalloc(&S.f[d], f3d_bytes(d, S.n, S.n, S.n, r) * S.batch));
+    }
+    CKA(cudaStreamSynchronize(st));
+    S.cur = 0;
+    S.active = true;
+    return FXB_OK;
+}
+
+int amr_attach(const double *unk_host)
+{
+    const size_t per_unk = (size_t)ne3() * S.C.nunk;
+    for (int l0 = 0; l0 < S.nleaf; l0 += S.stage_leaves) {
+        int nl = std::min(S.stage_leaves, S.nleaf - l0);
+        CKA(cudaMemcpyAsync(S.stage, unk_host + per_unk * l0, sizeof(double) * per_unk * nl, cudaMemcpyHostToDevice,
+                            S.C.stream));
+        long work = (long)nl * S.vstride;
+        int grid = (int)std::min<long>((work + 255) / 256, 148L * 16);
+        amr_unk_to_store_kernel<<<grid, 256, 0, S.C.stream>>>(S.stage, l0, nl, S.leaf_blk_dev, S.store[S.cur],
+                                                             S.vstride, S.bstride, S.n, S.ng, S.C.nunk, S.d_dmap);
+        CKA(cudaGetLastError());
+    }
+    CKA(cudaStreamSynchronize(S.C.stream));
+    return FXB_OK;
+}
+
+int amr_sync_to_host(double *unk_host)
+{
+    const size_t per_unk = (size_t)ne3() * S.C.nunk;
+    restrict_all(S.cur);
+    const int chunk = std::min(S.stage_leaves, S.batch);
+    for (int l0 = 0; l0 < S.nleaf; l0 += chunk) {
+        int nl = std::min(chunk, S.nleaf - l0);
+        // variables the device does not hold keep their host values
+        CKA(cudaMemcpyAsync(S.stage, unk_host + per_unk * l0, sizeof(double) * per_unk * nl, cudaMemcpyHostToDevice,
+                            S.C.stream));
+        fill_batch(S.d_entries + l0, nl, S.cur);
+        long work = (long)nl * ne3();
+        int grid = (int)std::min<long>((work + 255) / 256, 148L * 16);
+        amr_gcb_to_unk_kernel<<<grid, 256, 0, S.C.stream>>>(S.gcb, ne3(), ne3() * NV_DEV, nl, S.stage,
+                                                           S.n + 2 * S.ng, S.C.nunk, S.d_dmap);
+        CKA(cudaGetLastError());
+        CKA(cudaMemcpyAsync(unk_host + per_unk * l0, S.stage, sizeof(double) * per_unk * nl, cudaMemcpyDeviceToHost,
+                            S.C.stream));
+    }
+    CKA(cudaStreamSynchronize(S.C.stream));
+    return FXB_OK;
+}
+
+int amr_step(const double *dtv, double dt, int *launches)
+{
+    const bool mixed = S.C.prm.precision == FXB_MIXED;
+    int nl = 0;
+    restrict_all(S.cur);
+    nl += S.maxlev - 1;
+    Args3D a = batch_args(dtv, dt);
+    auto fluxes = [&](int cnt) {
+        if (mixed) launch_amr3d_fluxes_mixed(a, cnt, S.C.stream); else launch_amr3d_fluxes_fp64(a, cnt, S.C.stream);
+    };
+    auto emit = [&](int cnt) {
+        if (mixed) launch_amr3d_emit_mixed(a, cnt, S.bflux, S.nfc, S.C.stream);
+        else launch_amr3d_emit_fp64(a, cnt, S.bflux, S.nfc, S.C.stream);
+    };
+    auto correct = [&](int cnt) {
+        if (mixed) launch_amr3d_correct_mixed(a, cnt, S.bflux, S.nfc, S.d_fine, S.d_finer, S.C.stream);
+        else launch_amr3d_correct_fp64(a, cnt, S.bflux, S.nfc, S.d_fine, S.d_finer, S.C.stream);
+    };
+    auto update = [&](int cnt) {
+        if (mixed) launch_amr3d_update_mixed(a, cnt, S.C.stream); else launch_amr3d_update_fp64(a, cnt, S.C.stream);
+    };
+    if (S.nleaf <= S.batch) {
+        a.batch = S.d_entries;
+        fill_batch(a.batch, S.nleaf, S.cur);
+        fluxes(S.nleaf); emit(S.nleaf); correct(S.nleaf); update(S.nleaf);
+        nl += 11;
+    } else {
+        for (int l0 = 0; l0 < S.nleaf; l0 += S.batch) {
+            int cnt = std::min(S.batch, S.nleaf - l0);
+            a.batch = S.d_entries + S.nleaf + l0;
+            fill_batch(a.batch, cnt, S.cur);
+            fluxes(cnt); emit(cnt); update(cnt);
+            nl += 10;
+        }
+        for (int l0 = 0; l0 < S.nfiner; l0 += S.batch) {
+            int cnt = std::min(S.batch, S.nfiner - l0);
+            a.batch = S.d_entries + 2 * S.nleaf + l0;
+            fill_batch(a.batch, cnt, S.cur);
+            fluxes(cnt); correct(cnt); update(cnt);
+            nl += 10;
+        }
+    }
+    CKA(cudaGetLastError());
+    S.cur = 1 - S.cur;
+    if (launches) *launches = nl;
+    return FXB_OK;
+}
+
+int amr_rate()
+{
+    long work = amr_leaf_cells();
+    int grid = (int)std::min<long>((work + 255) / 256, 148L * 16);
+    amr_rate_kernel<<<grid, 256, 0, S.C.stream>>>(S.store[S.cur], S.vstride, S.bstride, S.n, S.leaf_blk_dev, S.d_blk,
+                                                  S.d_dxl, S.nleaf, S.C.rate_max);
+    CKA(cudaGetLastError());
+    return FXB_OK;
+}
+
+int amr_eos()
+{
+    long work = amr_leaf_cells();
+    int grid = (int)std::min<long>((work + 255) / 256, 148L * 16);
+    amr_eos_kernel<<<grid, 256, 0, S.C.stream>>>(S.store[S.cur], S.vstride, S.bstride, S.n, S.leaf_blk_dev, S.nleaf,
+                                                 S.C.dprm, S.C.gam1inv, S.C.ggprodinv);
+    CKA(cudaGetLastError());
+    return FXB_OK;
+}
+
+int amr_integrals(double *out7, double *partials, int npartials)
+{
+    amr_integrals_kernel<<<npartials, 256, 0, S.C.stream>>>(S.store[S.cur], S.vstride, S.bstride, S.n, S.leaf_blk_dev,
+                                                            S.d_blk, S.d_dxl, S.nleaf, partials);
+    amr_integrals_final_kernel<<<1, 32, 0, S.C.stream>>>(partials, npartials, partials + (long)npartials * 7);
+    CKA(cudaGetLastError());
+    CKA(cudaMemcpyAsync(out7, partials + (long)npartials * 7, 7 * sizeof(double), cudaMemcpyDeviceToHost, S.C.stream));
+    CKA(cudaStreamSynchronize(S.C.stream));
+    return FXB_OK;
+}
+
+} // namespace fxb

@@ -1,0 +1,43 @@
+// fxb_amr.h -- block-structured AMR mode of the library (3-D).
+//
+// fxb_register_blocks switches the library to this mode when the leaf list
+// is not the uniform level-1 block grid.  The leaves keep their UNK slots
+// (the order of the list); parents are derived and live only on the device.
+#pragma once
+#include <cuda_runtime.h>
+#include "../../include/flashx_b200.h"
+#include "fxb_device.cuh"
+
+namespace fxb {
+
+// what the AMR mode shares with the rest of the library
+struct AmrCommon {
+    cudaStream_t stream;
+    fxb_params prm;
+    fxb_domain dom;
+    DevParams dprm;
+    int nunk;
+    int dmap[NV_DEV];             // device variable -> UNK slot
+    int *err;                     // device error word
+    unsigned long long *rate_max; // device CFL rate (bits of a double)
+    double *dtv;                  // device [dt, dtOld]
+    double gam1inv, ggprodinv;
+};
+
+int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf);
+bool amr_active();
+int amr_cur();      // which interior store holds the current state
+void amr_destroy();
+int amr_attach(const double *unk_host);
+int amr_sync_to_host(double *unk_host);
+// one Hydro() step enqueued on the stream; dt from dtv when dtv != nullptr
+int amr_step(const double *dtv, double dt, int *launches);
+int amr_rate();
+int amr_eos();
+int amr_integrals(double *out7, double *partials, int npartials);
+long amr_leaf_cells();
+
+// reports through fxb_last_error (defined in fxb_api.cu)
+int record_error(int code, const char *msg);
+
+} // namespace fxb

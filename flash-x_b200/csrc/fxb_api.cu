@@ -4,6 +4,7 @@
 // stream, kernel launches, CUDA graphs and error reporting.
 #include "../../include/flashx_b200.h"
 #include "fxb_launch.h"
+#include "fxb_amr.h"
 
 #include <cuda_runtime.h>
 #include <stdio.h>
@@ -278,6 +279,7 @@ int check_err_word()
             return fail(FXB_ESOUND, "[hy_eigenParameters]: Zero or imaginary sound speed has obtained!");
         if (h & ERR_RIEMANN) return fail(FXB_ERIEMANN, "[hy_getFaceFlux]: Riemann solver returned ierr /= 0");
         if (h & 8) return fail(FXB_EDT, "[Hydro]: Computed dt is not positive! Aborting!");
+        if (h & 16) return fail(FXB_EARG, "[Grid_fillGuardCells]: AMR guard cell without a covering block");
         return fail(FXB_ECUDA, "device error word set");
     }
     return FXB_OK;
@@ -285,6 +287,7 @@ int check_err_word()
 
 void free_all()
 {
+    amr_destroy();
     for (int i = 0; i < 2; i++) {
         if (L.graph_exec[i]) cudaGraphExecDestroy(L.graph_exec[i]);
         L.graph_exec[i] = nullptr;
@@ -415,7 +418,25 @@ extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, cons
 extern "C" int fxb_register_blocks(const fxb_block_desc *blocks, int nblk)
 {
     if (!L.inited) return fail(FXB_EARG, "fxb_register_blocks: call fxb_init first");
-    if (!blocks || nblk != L.nblk) return fail(FXB_EARG, "fxb_register_blocks: the block list must cover the grid");
+    if (!blocks || nblk <= 0) return fail(FXB_EARG, "fxb_register_blocks: empty block list");
+    bool refined = nblk != L.nblk;
+    for (int b = 0; b < nblk && !refined; b++) refined = blocks[b].level != 1;
+    L.attached = false;
+    L.rate_valid = false;
+    for (int i = 0; i < 2; i++) {
+        if (L.graph_exec[i]) cudaGraphExecDestroy(L.graph_exec[i]);
+        L.graph_exec[i] = nullptr;
+    }
+    if (refined) {
+        // block-structured AMR mesh: parents derived, leaves keep their UNK slots
+        AmrCommon c;
+        c.stream = L.stream; c.prm = L.prm; c.dom = L.dom; c.dprm = L.dprm; c.nunk = L.nunk;
+        for (int v = 0; v < NV_DEV; v++) c.dmap[v] = L.dmap[v];
+        c.err = L.err; c.rate_max = L.rate_max; c.dtv = L.dtv;
+        c.gam1inv = L.gam1inv; c.ggprodinv = L.ggprodinv;
+        return amr_create(c, blocks, nblk);
+    }
+    amr_destroy();
     int nb[3] = {L.dom.nblockx, L.dom.ndim >= 2 ? L.dom.nblocky : 1, L.dom.ndim == 3 ? L.dom.nblockz : 1};
     int *h = new int[3 * nblk];
     char *seen = new char[nblk]();
@@ -444,8 +465,15 @@ extern "C" int fxb_register_blocks(const fxb_block_desc *blocks, int nblk)
 
 extern "C" int fxb_attach_unk(const double *unk_host)
 {
-    if (!L.inited || !L.bcoord) return fail(FXB_EARG, "fxb_attach_unk: call fxb_init and fxb_register_blocks first");
     if (!unk_host) return fail(FXB_EARG, "fxb_attach_unk: null UNK");
+    if (amr_active()) {
+        int rc = amr_attach(unk_host);
+        if (rc) return rc;
+        L.attached = true;
+        L.rate_valid = false;
+        return FXB_OK;
+    }
+    if (!L.inited || !L.bcoord) return fail(FXB_EARG, "fxb_attach_unk: call fxb_init and fxb_register_blocks first");
     CK(cudaMemcpyAsync(L.unk_dev, unk_host, sizeof(double) * L.unk_doubles, cudaMemcpyHostToDevice, L.stream));
     UnkGeom g = unk_geom();
     unk_to_state_kernel<<<1184, 256, 0, L.stream>>>(L.unk_dev, L.buf[L.cur], g, L.bcoord, L.dmap_dev, L.nblk);
@@ -462,6 +490,10 @@ extern "C" int fxb_sync_to_host(double *unk_host)
 {
     if (!L.attached) return fail(FXB_EARG, "fxb_sync_to_host: no UNK attached");
     if (!unk_host) return fail(FXB_EARG, "fxb_sync_to_host: null UNK");
+    if (amr_active()) {
+        int rc = amr_sync_to_host(unk_host);
+        return rc ? rc : check_err_word();
+    }
     UnkGeom g = unk_geom();
     state_to_unk_kernel<<<1184, 256, 0, L.stream>>>(L.buf[L.cur], L.unk_dev, g, L.bcoord, L.dmap_dev, L.nblk);
     CK(cudaGetLastError());
@@ -475,6 +507,10 @@ extern "C" int fxb_fill_guardcells(double *unk_host) { return fxb_sync_to_host(u
 extern "C" int fxb_eos(void)
 {
     if (!L.attached) return fail(FXB_EARG, "fxb_eos: no UNK attached");
+    if (amr_active()) {
+        L.rate_valid = false;
+        return amr_eos();
+    }
     eos_kernel<<<1184, 256, 0, L.stream>>>(L.buf[L.cur], L.vstride, L.ncell, L.dprm, L.gam1inv, L.ggprodinv);
     CK(cudaGetLastError());
     L.rate_valid = false;
@@ -488,12 +524,19 @@ extern "C" int fxb_hydro_step(double sim_time, double dt, double dt_old)
     if (!(dt > 0.)) return fail(FXB_EARG, "fxb_hydro_step: dt must be positive");
     CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
     CK(cudaEventRecord(L.ev0, L.stream));
-    int rc = launch_hydro(L.cur, nullptr, dt);
-    if (rc) return rc;
+    int nl = 1;
+    if (amr_active()) {
+        int rc = amr_step(nullptr, dt, &nl);
+        if (rc) return rc;
+    } else {
+        int rc = launch_hydro(L.cur, nullptr, dt);
+        if (rc) return rc;
+        L.cur = 1 - L.cur;
+        nl = L.dom.ndim == 2 ? 1 : 8;
+    }
     CK(cudaEventRecord(L.ev1, L.stream));
-    L.cur = 1 - L.cur;
     L.rate_valid = true;
-    L.last_launches = 1;
+    L.last_launches = nl;
     L.timing_valid = true;
     return FXB_OK;
 }
@@ -502,6 +545,12 @@ extern "C" int fxb_compute_dt(double *dt_out, int32_t loc[5])
 {
     if (!L.attached) return fail(FXB_EARG, "fxb_compute_dt: no UNK attached");
     if (!dt_out) return fail(FXB_EARG, "fxb_compute_dt: null output");
+    if (!L.rate_valid && amr_active()) {
+        CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
+        int rc = amr_rate();
+        if (rc) return rc;
+        L.rate_valid = true;
+    }
     if (!L.rate_valid) {
         CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
         rate_kernel<<<1184, 256, 0, L.stream>>>(L.buf[L.cur], L.vstride, L.nx, L.ny, L.nz, L.dom.ndim,
@@ -531,8 +580,10 @@ extern "C" int fxb_advance(int nsteps, double *dt, double *dt_old, double f, dou
     CK(cudaMemcpyAsync(L.dtv, h, sizeof(h), cudaMemcpyHostToDevice, L.stream));
     CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
     // graphs of two steps (buffer c -> 1-c -> c), built once per starting buffer
+    const bool amr = amr_active();
+    int step_launches = L.dom.ndim == 2 ? 1 : 8;
     auto one_step = [&](int src) -> int {
-        int rc = launch_hydro(src, L.dtv, 0.);
+        int rc = amr ? amr_step(L.dtv, 0., &step_launches) : launch_hydro(src, L.dtv, 0.);
         if (rc) return rc;
         dt_finalize_kernel<<<1, 1, 0, L.stream>>>(L.dtv, L.rate_max, L.prm.cfl, f, dtmin, dtmax, L.err);
         return cudaGetLastError() == cudaSuccess ? FXB_OK : fail(FXB_ECUDA, "dt kernel launch");
@@ -540,7 +591,7 @@ extern "C" int fxb_advance(int nsteps, double *dt, double *dt_old, double f, dou
     CK(cudaEventRecord(L.ev0, L.stream));
     int done = 0;
     if (nsteps >= 2) {
-        int c = L.cur;
+        int c = amr ? amr_cur() : L.cur;
         if (!L.graph_exec[c]) {
             cudaGraph_t graph;
             CK(cudaStreamBeginCapture(L.stream, cudaStreamCaptureModeThreadLocal));
@@ -559,7 +610,7 @@ extern "C" int fxb_advance(int nsteps, double *dt, double *dt_old, double f, dou
     for (; done < nsteps; done++) {
         int rc = one_step(L.cur);
         if (rc) return rc;
-        L.cur = 1 - L.cur;
+        if (!amr) L.cur = 1 - L.cur;
     }
     CK(cudaEventRecord(L.ev1, L.stream));
     CK(cudaMemcpyAsync(h, L.dtv, sizeof(h), cudaMemcpyDeviceToHost, L.stream));
@@ -567,7 +618,7 @@ extern "C" int fxb_advance(int nsteps, double *dt, double *dt_old, double f, dou
     *dt = h[0];
     *dt_old = h[1];
     L.rate_valid = false;
-    L.last_launches = 2 * nsteps;
+    L.last_launches = (step_launches + 1) * nsteps;
     L.timing_valid = true;
     return check_err_word();
 }
@@ -575,6 +626,7 @@ extern "C" int fxb_advance(int nsteps, double *dt, double *dt_old, double f, dou
 extern "C" int fxb_integrals(double out[7])
 {
     if (!L.attached) return fail(FXB_EARG, "fxb_integrals: no UNK attached");
+    if (amr_active()) return amr_integrals(out, L.partials, L.npartials);
     double dv = cell_dx(0) * cell_dx(1) * cell_dx(2);
     integrals_kernel<<<L.npartials, 256, 0, L.stream>>>(L.buf[L.cur], L.vstride, L.ncell, dv, L.partials);
     integrals_final_kernel<<<1, 32, 0, L.stream>>>(L.partials, L.npartials, L.partials + L.npartials * 7);

@@ -12,10 +12,25 @@
 //             (hy_unsplitUpdate.F90:1195-1250, hy_addGravity.F90), energyFix,
 //             Eos, store, CFL rate
 // Guard cells are resolved on load through map_axis, as in the 2-D kernel.
+//
+// The same kernels run in AMR batch mode (template flag AMR): blockIdx.y
+// selects one leaf block of a batch whose guard cells were filled by the
+// AMR guard-cell kernels; every block is then a small grid of nx*ny*nz
+// cells with its own cell size (its refinement level) and its own slice of
+// the intermediates, and the update writes the leaf's interior store.
 #pragma once
 #include "fxb_device.cuh"
 
 namespace fxb {
+
+// one entry of an AMR batch
+struct AmrEntry3 {
+    int out_blk;    // block index of the leaf in the interior store
+    int level;      // refinement level, 1-based
+    int leaf;       // leaf slot (UNK block index)
+    int flags;      // AMR_SKIP_UPDATE: the update waits for corrected fluxes
+};
+enum { AMR_SKIP_UPDATE = 1 };
 
 struct Args3D {
     const double *in;
@@ -33,6 +48,15 @@ struct Args3D {
     void *sig;      // [3][6][(nx+2)(ny+2)(nz+2)] of R
     void *wst[3];   // per direction [12][cells with that coordinate in [-1, n]]
     void *flx[3];   // per direction [8][faces]
+    // AMR batch mode
+    const double *gcb;          // guard-filled blocks [entry][var][nz+2g][ny+2g][nx+2g]
+    long gcb_vstride, gcb_bstride;
+    int ng;
+    const AmrEntry3 *batch;
+    const double *dxl;          // cell sizes [level-1][3]
+    double *odata;              // interior store [block][var][cell]
+    long o_vstride, o_bstride;
+    long sig_bstride, w_bstride[3], f_bstride[3];   // elements of R per batch entry
 };
 
 // 3-D tile extents accepted by fxb_init (the unfused kernels take any size)
@@ -80,6 +104,55 @@ __device__ __forceinline__ void load_cell(const Args3D &a, int i, int j, int k, 
     }
 }
 
+// Geometry, source and intermediates of one kernel invocation: the whole
+// uniform grid, or (AMR) the batch entry blockIdx.y.
+template <class R, bool AMR> struct Ctx3 {
+    Grid3 G;
+    const double *src;
+    long svs;
+    int sx, sy, so;
+    R *sig, *wst[3], *flx[3];
+    double dx, dy, dz;
+    AmrEntry3 m;
+    __device__ explicit Ctx3(const Args3D &a)
+    {
+        G = Grid3{a.nx, a.ny, a.nz};
+        if constexpr (AMR) {
+            const int bb = blockIdx.y;
+            m = a.batch[bb];
+            src = a.gcb + (long)bb * a.gcb_bstride;
+            svs = a.gcb_vstride;
+            so = a.ng; sx = a.nx + 2 * a.ng; sy = a.ny + 2 * a.ng;
+            sig = (R *)a.sig + (long)bb * a.sig_bstride;
+            for (int d = 0; d < 3; d++) {
+                wst[d] = (R *)a.wst[d] + (long)bb * a.w_bstride[d];
+                flx[d] = (R *)a.flx[d] + (long)bb * a.f_bstride[d];
+            }
+            dx = a.dxl[3 * (m.level - 1)]; dy = a.dxl[3 * (m.level - 1) + 1]; dz = a.dxl[3 * (m.level - 1) + 2];
+        } else {
+            m = AmrEntry3{0, 1, 0, 0};
+            src = a.in; svs = a.vstride; so = 0; sx = a.nx; sy = a.ny;
+            sig = (R *)a.sig;
+            for (int d = 0; d < 3; d++) { wst[d] = (R *)a.wst[d]; flx[d] = (R *)a.flx[d]; }
+            dx = a.dx; dy = a.dy; dz = a.dz;
+        }
+    }
+    // primitive 8-vector of cell (i,j,k); AMR blocks hold their guard cells
+    __device__ __forceinline__ void load(const Args3D &a, int i, int j, int k, R v[8]) const
+    {
+        if constexpr (AMR) {
+            long c = ((long)(k + so) * sy + (j + so)) * sx + (i + so);
+#pragma unroll
+            for (int q = 0; q < 8; q++) v[q] = (R)__ldg(src + q * svs + c);
+        } else {
+            load_cell(a, i, j, k, v);
+        }
+    }
+    // offset of interior cell (i,j,k) in the source arrays
+    __device__ __forceinline__ long cell(int i, int j, int k) const
+    { return ((long)(k + so) * sy + (j + so)) * sx + (i + so); }
+};
+
 template <class R> __device__ __forceinline__ void six(const R v[8], R g[6])
 { g[0] = v[D]; g[1] = v[VX]; g[2] = v[VY]; g[3] = v[VZ]; g[4] = v[P]; g[5] = v[EI]; }
 
@@ -102,25 +175,26 @@ __device__ __forceinline__ void offs(int d, int o, int &di, int &dj, int &dk)
 { di = d == 0 ? o : 0; dj = d == 1 ? o : 0; dk = d == 2 ? o : 0; }
 
 // ---- sigma_d of every padded cell --------------------------------------------
-template <class R>
+template <class R, bool AMR>
 __global__ void __launch_bounds__(256) sig3d_kernel(const Args3D a)
 {
-    Grid3 G{a.nx, a.ny, a.nz};
-    R *sig = (R *)a.sig;
+    const Ctx3<R, AMR> X(a);
+    const Grid3 &G = X.G;
+    R *sig = X.sig;
     const long np = G.npad();
     for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < np; idx += (long)gridDim.x * blockDim.x) {
         int i = (int)(idx % (a.nx + 2)) - 1;
         int j = (int)((idx / (a.nx + 2)) % (a.ny + 2)) - 1;
         int k = (int)(idx / ((long)(a.nx + 2) * (a.ny + 2))) - 1;
         R vc[8];
-        load_cell(a, i, j, k, vc);
+        X.load(a, i, j, k, vc);
         R gc[6]; six(vc, gc);
         for (int d = 0; d < 3; d++) {
             int di, dj, dk;
             offs(d, 1, di, dj, dk);
             R vm[8], vp[8], g[6], m[6], c[6], p[6], sr[6], sg[6];
-            load_cell(a, i - di, j - dj, k - dk, vm);
-            load_cell(a, i + di, j + dj, k + dk, vp);
+            X.load(a, i - di, j - dj, k - dk, vm);
+            X.load(a, i + di, j + dj, k + dk, vp);
             six(vm, g); rot3(d, g, m);
             rot3(d, gc, c);
             six(vp, g); rot3(d, g, p);
@@ -135,9 +209,8 @@ __global__ void __launch_bounds__(256) sig3d_kernel(const Args3D a)
 }
 
 template <class R>
-__device__ __forceinline__ void read_sig(const Args3D &a, const Grid3 &G, int d, int i, int j, int k, R s[6])
+__device__ __forceinline__ void read_sig(const R *sig, const Grid3 &G, int d, int i, int j, int k, R s[6])
 {
-    const R *sig = (const R *)a.sig;
     long np = G.npad(), p = G.pidx(i, j, k);
 #pragma unroll
     for (int q = 0; q < 6; q++) s[q] = sig[((long)d * 6 + q) * np + p];
@@ -146,15 +219,15 @@ __device__ __forceinline__ void read_sig(const Args3D &a, const Grid3 &G, int d,
 // CTU cross term of one transverse pair: upwinding along e of sigma_s at the
 // cell's e-neighbours, with the e-direction eigensystem of the cell
 template <class R>
-__device__ __forceinline__ void ctu_term(const Args3D &a, const Grid3 &G, const R vc[8], int e, int s,
+__device__ __forceinline__ void ctu_term(const Args3D &a, const R *sigp, const Grid3 &G, const R vc[8], int e, int s,
                                         int i, int j, int k, R T[6])
 {
     int di, dj, dk;
     offs(e, 1, di, dj, dk);
     R sm[6], sc[6], sp[6], m[6], c[6], p[6], gcell[6], r[6], tr[6];
-    read_sig(a, G, s, i - di, j - dj, k - dk, sm);
-    read_sig(a, G, s, i, j, k, sc);
-    read_sig(a, G, s, i + di, j + dj, k + dk, sp);
+    read_sig(sigp, G, s, i - di, j - dj, k - dk, sm);
+    read_sig(sigp, G, s, i, j, k, sc);
+    read_sig(sigp, G, s, i + di, j + dj, k + dk, sp);
     rot3(e, sm, m); rot3(e, sc, c); rot3(e, sp, p);
     six(vc, gcell); rot3(e, gcell, r);
     Eig<R> ev;
@@ -178,15 +251,16 @@ __device__ __forceinline__ void ctu_term(const Args3D &a, const Grid3 &G, const 
 #define FXB_S3_MINB_FP32 2
 #endif
 template <class R> struct MinB3D { static constexpr int value = sizeof(R) == 8 ? FXB_S3_MINB_FP64 : FXB_S3_MINB_FP32; };
-template <class R, int ORDER>
+template <class R, int ORDER, bool AMR>
 __global__ void __launch_bounds__(256, MinB3D<R>::value) states3d_kernel(const Args3D a, int d)
 {
-    Grid3 G{a.nx, a.ny, a.nz};
+    const Ctx3<R, AMR> X(a);
+    const Grid3 &G = X.G;
     const double dt = a.dtv ? a.dtv[0] : a.dt_arg;
-    const double del[3] = {a.dx, a.dy, a.dz};
+    const double del[3] = {X.dx, X.dy, X.dz};
     const R dtn = R(dt / del[d]), hdtn = R(0.5 * (dt / del[d]));
-    const R hdtx = R(0.5 * dt / a.dx), hdty = R(0.5 * dt / a.dy), hdtz = R(0.5 * dt / a.dz);
-    R *w = (R *)a.wst[d];
+    const R hdtx = R(0.5 * dt / X.dx), hdty = R(0.5 * dt / X.dy), hdtz = R(0.5 * dt / X.dz);
+    R *w = X.wst[d];
     const long nw = G.nw(d);
     const int lx = a.nx + (d == 0 ? 2 : 0), ly = a.ny + (d == 1 ? 2 : 0);
     for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < nw; idx += (long)gridDim.x * blockDim.x) {
@@ -197,7 +271,7 @@ __global__ void __launch_bounds__(256, MinB3D<R>::value) states3d_kernel(const A
         R S8[5][8], S[5][6], g[6];
 #pragma unroll
         for (int o = -2; o <= 2; o++) {
-            load_cell(a, i + o * di, j + o * dj, k + o * dk, S8[o + 2]);
+            X.load(a, i + o * di, j + o * dj, k + o * dk, S8[o + 2]);
             six(S8[o + 2], g); rot3(d, g, S[o + 2]);
         }
         const R *vc = S8[2];
@@ -222,21 +296,21 @@ __global__ void __launch_bounds__(256, MinB3D<R>::value) states3d_kernel(const A
         // transverse terms, hy_dataReconstOneStep.F90:931-962
         R s1[6], s2[6];
         if (d == 0) {
-            read_sig(a, G, 1, i, j, k, s1); read_sig(a, G, 2, i, j, k, s2);
+            read_sig(X.sig, G, 1, i, j, k, s1); read_sig(X.sig, G, 2, i, j, k, s2);
 #pragma unroll
             for (int q = 0; q < 6; q++) {
                 Wm[q] = Wm[q] - hdty * s1[q]; Wp[q] = Wp[q] - hdty * s1[q];
                 Wm[q] = Wm[q] - hdtz * s2[q]; Wp[q] = Wp[q] - hdtz * s2[q];
             }
         } else if (d == 1) {
-            read_sig(a, G, 0, i, j, k, s1); read_sig(a, G, 2, i, j, k, s2);
+            read_sig(X.sig, G, 0, i, j, k, s1); read_sig(X.sig, G, 2, i, j, k, s2);
 #pragma unroll
             for (int q = 0; q < 6; q++) {
                 Wm[q] = Wm[q] - hdtx * s1[q]; Wp[q] = Wp[q] - hdtx * s1[q];
                 Wm[q] = Wm[q] - hdtz * s2[q]; Wp[q] = Wp[q] - hdtz * s2[q];
             }
         } else {
-            read_sig(a, G, 0, i, j, k, s1); read_sig(a, G, 1, i, j, k, s2);
+            read_sig(X.sig, G, 0, i, j, k, s1); read_sig(X.sig, G, 1, i, j, k, s2);
 #pragma unroll
             for (int q = 0; q < 6; q++) {
                 Wm[q] = Wm[q] - hdtx * s1[q] - hdty * s2[q];
@@ -262,12 +336,12 @@ __global__ void __launch_bounds__(256, MinB3D<R>::value) states3d_kernel(const A
         }
         if (a.prm.use_3d_full_ctu) {
             int e1, s1d, e2, s2d; double fac;
-            if (d == 0)      { e1 = 1; s1d = 2; e2 = 2; s2d = 1; fac = dt * dt / (6. * a.dy * a.dz); }
-            else if (d == 1) { e1 = 2; s1d = 0; e2 = 0; s2d = 2; fac = dt * dt / (6. * a.dz * a.dx); }
-            else             { e1 = 0; s1d = 1; e2 = 1; s2d = 0; fac = dt * dt / (6. * a.dx * a.dy); }
+            if (d == 0)      { e1 = 1; s1d = 2; e2 = 2; s2d = 1; fac = dt * dt / (6. * X.dy * X.dz); }
+            else if (d == 1) { e1 = 2; s1d = 0; e2 = 0; s2d = 2; fac = dt * dt / (6. * X.dz * X.dx); }
+            else             { e1 = 0; s1d = 1; e2 = 1; s2d = 0; fac = dt * dt / (6. * X.dx * X.dy); }
             R T1[6], T2[6];
-            ctu_term(a, G, vc, e1, s1d, i, j, k, T1);
-            ctu_term(a, G, vc, e2, s2d, i, j, k, T2);
+            ctu_term(a, X.sig, G, vc, e1, s1d, i, j, k, T1);
+            ctu_term(a, X.sig, G, vc, e2, s2d, i, j, k, T2);
             const R f = R(fac);
 #pragma unroll
             for (int q = 0; q < 6; q++) {
@@ -285,12 +359,13 @@ __global__ void __launch_bounds__(256, MinB3D<R>::value) states3d_kernel(const A
 }
 
 // ---- Riemann fluxes of direction d ---------------------------------------------
-template <class R>
+template <class R, bool AMR>
 __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a, int d)
 {
-    Grid3 G{a.nx, a.ny, a.nz};
-    const R *w = (const R *)a.wst[d];
-    R *f = (R *)a.flx[d];
+    const Ctx3<R, AMR> X(a);
+    const Grid3 &G = X.G;
+    const R *w = X.wst[d];
+    R *f = X.flx[d];
     const long nf = G.nf(d), nw = G.nw(d);
     const int lx = a.nx + (d == 0 ? 1 : 0), ly = a.ny + (d == 1 ? 1 : 0);
     for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < nf; idx += (long)gridDim.x * blockDim.x) {
@@ -301,8 +376,8 @@ __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a, int d)
         R VL[6], VR[6], F[8], cl[8], cr[8];
 #pragma unroll
         for (int q = 0; q < 6; q++) { VL[q] = w[(long)q * nw + wl]; VR[q] = w[(long)(6 + q) * nw + wr]; }
-        load_cell(a, i - di, j - dj, k - dk, cl);
-        load_cell(a, i, j, k, cr);
+        X.load(a, i - di, j - dj, k - dk, cl);
+        X.load(a, i, j, k, cr);
         int e = riemann(a.prm, d, VL, cl[GC], cl[GE], VR, cr[GC], cr[GE], F);
         if (e) atomicOr(a.err, e);
 #pragma unroll
@@ -311,27 +386,32 @@ __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a, int d)
 }
 
 // ---- update, energyFix, Eos, CFL rate -------------------------------------------
-template <class R>
+template <class R, bool AMR>
 __global__ void __launch_bounds__(256) update3d_kernel(const Args3D a)
 {
-    Grid3 G{a.nx, a.ny, a.nz};
+    const Ctx3<R, AMR> X(a);
+    const Grid3 &G = X.G;
+    if (AMR && (X.m.flags & AMR_SKIP_UPDATE)) return;
     const double dt = a.dtv ? a.dtv[0] : a.dt_arg;
     const DevParams &prm = a.prm;
     const long n = (long)a.nx * a.ny * a.nz;
-    const double del[3] = {a.dx, a.dy, a.dz};
+    const double del[3] = {X.dx, X.dy, X.dz};
+    double *out = AMR ? a.odata + (long)X.m.out_blk * a.o_bstride : a.out;
+    const long ovs = AMR ? a.o_vstride : a.vstride;
     double rate = 0.;
     for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
         int i = (int)(c % a.nx), j = (int)((c / a.nx) % a.ny), k = (int)(c / ((long)a.nx * a.ny));
-        const long vs = a.vstride;
-        double dens0 = a.in[D * vs + c];
-        double vx0 = a.in[VX * vs + c], vy0 = a.in[VY * vs + c], vz0 = a.in[VZ * vs + c];
-        double en0 = a.in[DV_ENER * vs + c], eint0 = a.in[EI * vs + c];
+        const long vs = X.svs;
+        const double *in = X.src + X.cell(i, j, k);
+        double dens0 = in[D * vs];
+        double vx0 = in[VX * vs], vy0 = in[VY * vs], vz0 = in[VZ * vs];
+        double en0 = in[DV_ENER * vs], eint0 = in[EI * vs];
         double U0[5] = {dens0, vx0 * dens0, vy0 * dens0, vz0 * dens0, dens0 * en0};
         double Sph[5] = {0., 0., 0., 0., 0.};
         double A[3], B[3], pav = 0.;
         for (int d = 0; d < 3; d++) {
-            const R *f = (const R *)a.flx[d];
-            const R *w = (const R *)a.wst[d];
+            const R *f = X.flx[d];
+            const R *w = X.wst[d];
             long nf = G.nf(d), nw = G.nw(d);
             int di, dj, dk;
             offs(d, 1, di, dj, dk);
@@ -387,14 +467,14 @@ __global__ void __launch_bounds__(256) update3d_kernel(const Args3D a)
         double pres = dens * eg * a.gam1inv;
         double temp = eg * a.ggprodinv * prm.abar;
         double game = pres / (eg * dens) + 1;
-        double *o = a.out;
-        o[D * vs + c] = dens; o[VX * vs + c] = vx; o[VY * vs + c] = vy; o[VZ * vs + c] = vz;
-        o[P * vs + c] = pres; o[GC * vs + c] = prm.gamma; o[GE * vs + c] = game;
-        o[EI * vs + c] = eg; o[DV_ENER * vs + c] = eg + ek2; o[DV_TEMP * vs + c] = temp;
+        double *o = out + c;
+        o[D * ovs] = dens; o[VX * ovs] = vx; o[VY * ovs] = vy; o[VZ * ovs] = vz;
+        o[P * ovs] = pres; o[GC * ovs] = prm.gamma; o[GE * ovs] = game;
+        o[EI * ovs] = eg; o[DV_ENER * ovs] = eg + ek2; o[DV_TEMP * ovs] = temp;
         double cs = sqrt(prm.gamma * pres / dens);
-        double r = (fabs(vx - 0.) + cs) * (1.0 / a.dx);
-        r = fmax2(r, (fabs(vy - 0.) + cs) * (1.0 / a.dy));
-        r = fmax2(r, (fabs(vz - 0.) + cs) * (1.0 / a.dz));
+        double r = (fabs(vx - 0.) + cs) * (1.0 / X.dx);
+        r = fmax2(r, (fabs(vy - 0.) + cs) * (1.0 / X.dy));
+        r = fmax2(r, (fabs(vz - 0.) + cs) * (1.0 / X.dz));
         rate = fmax2(rate, r);
     }
 #pragma unroll
@@ -419,13 +499,102 @@ inline size_t f3d_bytes(int d, int nx, int ny, int nz, size_t rsz)
 template <class R> void launch_hydro3d_t(const Args3D &a, cudaStream_t s)
 {
     const int nb = 148 * 8;
-    sig3d_kernel<R><<<nb, 256, 0, s>>>(a);
+    sig3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
     for (int d = 0; d < 3; d++) {
-        if (a.prm.order == 5) states3d_kernel<R, 5><<<nb, 256, 0, s>>>(a, d);
-        else states3d_kernel<R, 3><<<nb, 256, 0, s>>>(a, d);
+        if (a.prm.order == 5) states3d_kernel<R, 5, false><<<nb, 256, 0, s>>>(a, d);
+        else states3d_kernel<R, 3, false><<<nb, 256, 0, s>>>(a, d);
     }
-    for (int d = 0; d < 3; d++) flux3d_kernel<R><<<nb, 256, 0, s>>>(a, d);
-    update3d_kernel<R><<<nb, 256, 0, s>>>(a);
+    for (int d = 0; d < 3; d++) flux3d_kernel<R, false><<<nb, 256, 0, s>>>(a, d);
+    update3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
+}
+
+// ---- AMR batch: boundary fluxes for flux correction ------------------------------
+// Grid_putFluxData: the fluxes on the six boundary faces of every entry,
+// [leaf][face][slot][t2 * n1 + t1] with (t1, t2) the face's transverse cell
+// (x faces: (y, z); y faces: (x, z); z faces: (x, y)).
+template <class R>
+__global__ void __launch_bounds__(256) amr_emit_flux_kernel(const Args3D a, R *bflux, long nfc)
+{
+    const Ctx3<R, true> X(a);
+    const Grid3 &G = X.G;
+    const int n[3] = {a.nx, a.ny, a.nz};
+    R *dst = bflux + (long)X.m.leaf * 6 * NF * nfc;
+    for (int f = 0; f < 6; f++) {
+        const int d = f >> 1, side = f & 1;
+        const int a1 = d == 0 ? 1 : 0, a2 = d == 2 ? 1 : 2;
+        const long nface = (long)n[a1] * n[a2];
+        const long nfd = G.nf(d);
+        for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nface * NF; t += (long)gridDim.x * blockDim.x) {
+            const int v = (int)(t / nface);
+            const long tt = t - v * nface;
+            const int t1 = (int)(tt % n[a1]), t2 = (int)(tt / n[a1]);
+            int c[3];
+            c[d] = side ? n[d] : 0; c[a1] = t1; c[a2] = t2;
+            dst[((long)f * NF + v) * nfc + tt] = X.flx[d][(long)v * nfd + G.fidx(d, c[0], c[1], c[2])];
+        }
+    }
+}
+
+// Grid_conserveFluxes: on a face whose same-level neighbour is refined, the
+// fluxes become the fine fluxes restricted as amr_restrict_red does:
+// (((f(a) + f(a+e1)) + f(a+e2)) + f(a+e1+e2)) * 0.25.  fine[leaf*24 + face*4 + q]
+// is the fine leaf across the face at transverse child position q = o1 + 2*o2.
+template <class R>
+__global__ void __launch_bounds__(256) amr_correct_flux_kernel(const Args3D a, const R *bflux, long nfc,
+                                                               const int *fine, const int *finer_mask)
+{
+    const Ctx3<R, true> X(a);
+    const Grid3 &G = X.G;
+    const int mask = finer_mask[X.m.leaf];
+    if (!mask) return;
+    const int n[3] = {a.nx, a.ny, a.nz};
+    for (int f = 0; f < 6; f++) {
+        if (!((mask >> f) & 1)) continue;
+        const int d = f >> 1, side = f & 1;
+        const int a1 = d == 0 ? 1 : 0, a2 = d == 2 ? 1 : 2;
+        const long nface = (long)n[a1] * n[a2];
+        const long nfd = G.nf(d);
+        const int ff = f ^ 1;      // the fine leaves' face toward this block
+        for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nface * NF; t += (long)gridDim.x * blockDim.x) {
+            const int v = (int)(t / nface);
+            const long tt = t - v * nface;
+            const int t1 = (int)(tt % n[a1]), t2 = (int)(tt / n[a1]);
+            const int o1 = (2 * t1) / n[a1], o2 = (2 * t2) / n[a2];
+            const int f1 = 2 * t1 - o1 * n[a1], f2 = 2 * t2 - o2 * n[a2];
+            const int fl = fine[(long)X.m.leaf * 24 + f * 4 + o1 + 2 * o2];
+            const R *src = bflux + (((long)fl * 6 + ff) * NF + v) * nfc;
+            const R fa = src[(long)f2 * n[a1] + f1], fb = src[(long)f2 * n[a1] + f1 + 1];
+            const R fc = src[(long)(f2 + 1) * n[a1] + f1], fd = src[(long)(f2 + 1) * n[a1] + f1 + 1];
+            int c[3];
+            c[d] = side ? n[d] : 0; c[a1] = t1; c[a2] = t2;
+            X.flx[d][(long)v * nfd + G.fidx(d, c[0], c[1], c[2])] = (((fa + fb) + fc) + fd) * R(0.25);
+        }
+    }
+}
+
+// The 3-D pipeline over one AMR batch of `entries` guard-filled blocks.
+template <class R> void launch_amr3d_fluxes_t(const Args3D &a, int entries, cudaStream_t s)
+{
+    const dim3 g(4, entries);
+    sig3d_kernel<R, true><<<g, 256, 0, s>>>(a);
+    for (int d = 0; d < 3; d++) {
+        if (a.prm.order == 5) states3d_kernel<R, 5, true><<<g, 256, 0, s>>>(a, d);
+        else states3d_kernel<R, 3, true><<<g, 256, 0, s>>>(a, d);
+    }
+    for (int d = 0; d < 3; d++) flux3d_kernel<R, true><<<g, 256, 0, s>>>(a, d);
+}
+template <class R> void launch_amr3d_emit_t(const Args3D &a, int entries, void *bflux, long nfc, cudaStream_t s)
+{
+    amr_emit_flux_kernel<R><<<dim3(2, entries), 256, 0, s>>>(a, (R *)bflux, nfc);
+}
+template <class R> void launch_amr3d_correct_t(const Args3D &a, int entries, const void *bflux, long nfc,
+                                               const int *fine, const int *finer_mask, cudaStream_t s)
+{
+    amr_correct_flux_kernel<R><<<dim3(2, entries), 256, 0, s>>>(a, (const R *)bflux, nfc, fine, finer_mask);
+}
+template <class R> void launch_amr3d_update_t(const Args3D &a, int entries, cudaStream_t s)
+{
+    update3d_kernel<R, true><<<dim3(4, entries), 256, 0, s>>>(a);
 }
 
 } // namespace fxb

@@ -175,25 +175,44 @@ def leaf_blocks(geom: Geometry):
     return arr
 
 
-class HydroDevice:
-    """The unsplit hydro solver on one B200, behind the reference interface."""
+def mesh_blocks(levels, bcoords):
+    """Leaf-block list of an AMR mesh (levels from 1, block coordinates at
+    each leaf's level), in UNK slot order."""
+    n = len(levels)
+    arr = (FxbBlockDesc * n)()
+    for b in range(n):
+        arr[b].level = int(levels[b])
+        arr[b].bcoord[0], arr[b].bcoord[1], arr[b].bcoord[2] = (int(v) for v in bcoords[b])
+    return arr
 
-    def __init__(self, geom: Geometry, hp: HydroParams, precision="fp64"):
+
+class HydroDevice:
+    """The unsplit hydro solver on one B200, behind the reference interface.
+
+    `mesh` (a flashx_b200.amr.AmrMesh over `geom`'s root blocks) selects a
+    block-structured AMR mesh; without it the blocks form the uniform grid."""
+
+    def __init__(self, geom: Geometry, hp: HydroParams, precision="fp64", mesh=None):
         self.lib = load_library()
-        self.geom, self.hp, self.precision = geom, hp, precision
+        self.geom, self.hp, self.precision, self.mesh = geom, hp, precision, mesh
         self._p = make_fxb_params(hp, precision)
         self._d = make_fxb_domain(geom)
         self._vm = default_var_map()
         _check(self.lib.fxb_init(ctypes.byref(self._p), ctypes.byref(self._d), self._vm, NUNK))
-        blocks = leaf_blocks(geom)
-        _check(self.lib.fxb_register_blocks(blocks, geom.nblocks))
+        if mesh is None:
+            blocks, n = leaf_blocks(geom), geom.nblocks
+            self.unk_shape = geom.unk_shape
+        else:
+            blocks, n = mesh_blocks(mesh.levels, mesh.bcoords), mesh.nleaf
+            self.unk_shape = mesh.unk_shape
+        _check(self.lib.fxb_register_blocks(blocks, n))
         self.unk = None
 
     # ---- data movement
     def attach_unk(self, unk):
         """Take the host UNK (Fortran unk(var,i,j,k,blk) as a C-order array)."""
-        if unk.shape != self.geom.unk_shape:
-            raise ValueError(f"UNK shape {unk.shape} != {self.geom.unk_shape}")
+        if unk.shape != self.unk_shape:
+            raise ValueError(f"UNK shape {unk.shape} != {self.unk_shape}")
         self.unk = unk
         _check(self.lib.fxb_attach_unk(_dp(unk)))
 

@@ -81,8 +81,10 @@ typedef struct fxb_domain {
     int    bc[6];              /* xl xr yl yr zl zr, enum fxb_bc */
 } fxb_domain;
 
-/* One leaf block: its position in the uniform block grid (0-based block
- * coordinates).  Flash-X's blkLimits follow from it; refinement level 1. */
+/* One leaf block: its refinement level (1 = the root block grid of
+ * fxb_domain) and its 0-based block coordinates at that level, in
+ * [0, nblock * 2^(level-1)) per axis.  Flash-X's blkLimits, deltas and
+ * bounding box follow from them (PARAMESH lrefine and the block's position). */
 typedef struct fxb_block_desc {
     int    level;
     int    bcoord[3];
@@ -98,7 +100,19 @@ typedef struct fxb_error {
  * UNK cell vector of nunk doubles. */
 int fxb_init(const fxb_params *params, const fxb_domain *domain,
              const int32_t *var_map, int nunk);
-/* The leaf-block list (Grid_getTileIterator(LEAF)); nblk must cover the grid. */
+/* The leaf-block list (Grid_getTileIterator(LEAF)); block b is UNK slot b.
+ * All leaves at level 1 covering the root grid: the uniform-grid path.
+ * Otherwise (3-D only) a block-structured AMR mesh: the leaves must tile the
+ * domain with neighbours, across faces, edges and corners, at most one level
+ * apart (PARAMESH proper nesting); parents are derived and kept on the device.
+ * Each Hydro() step then restricts the parents, fills guard cells by
+ * same-level copy or multilinear prolongation (PARAMESH's default
+ * interpolation, conserved form), applies Eos to the guard regions next to
+ * other levels and corrects the fluxes on fine/coarse faces
+ * (Paramesh4/Grid_fillGuardCells.F90:446-541, levelFlux/Hydro.F90:161-270,
+ * levelFlux/Grid_conserveFluxes.F90).  Errors: FXB_EARG for a list that does
+ * not tile the domain or is not balanced, FXB_EUNSUPPORTED for 2-D AMR,
+ * non-cubic blocks or gravity on AMR meshes. */
 int fxb_register_blocks(const fxb_block_desc *blocks, int nblk);
 /* Copy the host UNK (all blocks, guard cells included) into the device mirror. */
 int fxb_attach_unk(const double *unk_host);
