@@ -63,7 +63,7 @@ def _gpu(root, hp, mesh, unk, dts, precision="fp64"):
     ((BC_PERIODIC,) * 6, 3, 5),
 ])
 def test_amr_step_fp64_matches_oracle(oracle, need_gpu, bc, maxlev, order):
-    root, hp, mesh, unk = _case(bc, maxlev, nroot=4 if maxlev == 2 else 2, order=order)
+    root, hp, mesh, unk = _case(bc, maxlev, order=order)
     am = oracle.Amr(oracle.make_params(root.as_dict(), hp), mesh.levels, mesh.bcoords)
     dt = 0.5 * am.compute_dt(unk)
     _, ref = _oracle(oracle, root, hp, mesh, unk, [dt, dt])
@@ -75,7 +75,7 @@ def test_amr_step_fp64_matches_oracle(oracle, need_gpu, bc, maxlev, order):
 
 
 def test_amr_guard_fill_matches_oracle(oracle, need_gpu):
-    root, hp, mesh, unk = _case(maxlev=3, nroot=2)
+    root, hp, mesh, unk = _case(maxlev=3)
     am = oracle.Amr(oracle.make_params(root.as_dict(), hp), mesh.levels, mesh.bcoords)
     ref = unk.copy()
     am.fill_guardcells(ref)
