@@ -41,7 +41,34 @@ WORKLOADS = {
     "rt3d": "rt3d: 3-D Rayleigh-Taylor 256^3 (4096 blocks of 16^3), WENO5+HLLC, g_z=-0.1, periodic x/y, "
             "reflecting z, full CTU",
     "sweep3d": "sweep3d: 3-D noisy gas 64^3 (64 blocks of 16^3), periodic, PPM+HLLC, gamma 5/3",
+    "amr3d": "amr3d: 3-D block-structured AMR, 16^3 blocks on 4^3 roots, levels 1-4 refined where "
+             "|grad rho|/rho > 0.1 around a seeded level-set interface (rho 1 vs 10), periodic, PPM+HLLC, "
+             "PARAMESH guard fill + flux correction every step",
 }
+
+
+def make_problem(name, scale=1.0):
+    """(geom, hp, leaf UNK, mesh or None, zones) of a benchmark problem."""
+    from flashx_b200 import simulations as S
+    if name == "amr3d":
+        from flashx_b200 import amr as A
+        from flashx_b200.params import BC_PERIODIC, Geometry, HydroParams
+        nroot = max(1, int(round(4 * scale)))
+        geom = Geometry(3, 16, 16, 16, nroot, nroot, nroot, bc=(BC_PERIODIC,) * 6)
+        hp = HydroParams()
+        mesh, unk = A.levelset_problem(geom, hp, maxlev=4)
+        return geom, hp, unk, mesh, mesh.ncells()
+    geom, hp, init = S.config(name, scale=scale)
+    return geom, hp, init(geom, hp), None, geom.ncells
+
+
+def interiors(geom, unk, mesh):
+    """Cell values of all (leaf) block interiors, (cells, var)."""
+    from flashx_b200 import simulations as S
+    if mesh is None:
+        return S.gather_global(geom, unk).reshape(-1, unk.shape[-1])
+    g = geom.nguard
+    return unk[:, g:-g, g:-g, g:-g, :].reshape(-1, unk.shape[-1])
 
 
 def parse():
@@ -50,7 +77,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="kh2d", choices=["kh2d", "sod2d", "rt3d", "sweep3d"],
+    ap.add_argument("--config", default="kh2d", choices=["kh2d", "sod2d", "rt3d", "sweep3d", "amr3d"],
                     help="kh2d (default, the headline workload) or another benchmark problem")
     ap.add_argument("--scale", type=float, default=1.0, help="block count per axis relative to the config")
     ap.add_argument("--no-mixed", action="store_true")
@@ -139,10 +166,31 @@ def dist_setup(args, backend):
     return None, 1, 0, local
 
 
+def cpu_baseline_amr(seconds=10.0):
+    """The oracle's AMR step (OpenMP over leaves, all host cores) on the full
+    AMR workload, as many steps as fit in `seconds` (at least one)."""
+    from oracle import fx_oracle as O
+    geom, hp, unk, mesh, ncell = make_problem("amr3d")
+    am = O.Amr(O.make_params(geom.as_dict(), hp), mesh.levels, mesh.bcoords)
+    dt = 0.5 * am.compute_dt(unk)
+    n, t0 = 0, time.perf_counter()
+    while n == 0 or time.perf_counter() - t0 < seconds:
+        am.hydro_step(unk, dt)
+        dt = O.driver_dt(am.compute_dt(unk), dt)
+        n += 1
+    el = time.perf_counter() - t0
+    cores = os.cpu_count()
+    return {"value": ncell * n / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"amr3d {mesh.nleaf} leaves ({ncell} zones), {n} steps in {el:.1f} s, "
+                      f"OpenMP over leaves on {cores} threads"}
+
+
 def cpu_baseline_run(name, seconds=10.0, scale=1 / 4):
     """The oracle (OpenMP over blocks, all host cores) on a bounded sample of
     the workload: the same problem at reduced resolution, as many steps as fit
     in `seconds`."""
+    if name == "amr3d":
+        return cpu_baseline_amr(seconds)
     from flashx_b200 import simulations as S
     from oracle import fx_oracle as O
     geom, hp, init = S.config(name, scale=scale)
@@ -169,30 +217,40 @@ def run_reference(args):
         if dist:
             dist.destroy_process_group()
         return
-    from flashx_b200 import simulations as S
     from oracle import fx_oracle as O
-    geom, hp, init = S.config(args.config, scale=1 / 4)
-    unk = init(geom, hp)
-    p = O.make_params(geom.as_dict(), hp)
-    dt = 0.5 * O.compute_dt(p, unk)
-    for _ in range(args.warmup):
-        O.hydro_step(p, unk, dt, dt)
-        dt = O.driver_dt(O.compute_dt(p, unk), dt)
+    if args.config == "amr3d":
+        geom, hp, unk, mesh, ncell = make_problem("amr3d")
+        am = O.Amr(O.make_params(geom.as_dict(), hp), mesh.levels, mesh.bcoords)
+        step = lambda dt: am.hydro_step(unk, dt)
+        cfl_dt = lambda: am.compute_dt(unk)
+        steps, warm = max(1, min(args.steps, 3)), min(args.warmup, 1)
+        sample = f"amr3d {mesh.nleaf} leaves ({ncell} zones) per step"
+    else:
+        geom, hp, unk, mesh, ncell = make_problem(args.config, scale=1 / 4)
+        p = O.make_params(geom.as_dict(), hp)
+        step = lambda dt: O.hydro_step(p, unk, dt, dt)
+        cfl_dt = lambda: O.compute_dt(p, unk)
+        steps, warm = args.steps, args.warmup
+        sample = f"{args.config} {geom.nxb * geom.nblockx}^{geom.ndim} per step"
+    dt = 0.5 * cfl_dt()
+    for _ in range(warm):
+        step(dt)
+        dt = O.driver_dt(cfl_dt(), dt)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        O.hydro_step(p, unk, dt, dt)
-        dt = O.driver_dt(O.compute_dt(p, unk), dt)
+    for _ in range(steps):
+        step(dt)
+        dt = O.driver_dt(cfl_dt(), dt)
     el = time.perf_counter() - t0
-    v = geom.ncells * args.steps / el
-    nx = geom.nxb * geom.nblockx
-    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+    v = ncell * steps / el
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+            "warmup": warm, "ms_per_step": 1e3 * el / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "kh2d 2048^2 PPM+HLLC, sampled at %d^2 per step" % nx},
+            "config": {"workload": WORKLOADS[args.config] + f"; sampled as {sample}"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                              "sample": f"oracle restatement of the Flash-X unsplit solver (the Fortran reference "
-                                       f"cannot be built here), {nx}^2 KH per step, OpenMP on {os.cpu_count()} threads"},
+                                       f"cannot be built here), {sample}, {steps} timed steps, "
+                                       f"OpenMP on {os.cpu_count()} threads"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     if dist:
@@ -206,9 +264,7 @@ def run_ours(args):
     from flashx_b200 import simulations as S
     from flashx_b200.hydro import HydroDevice, driver_dt
 
-    geom, hp, init = S.config(args.config, scale=args.scale)
-    unk0 = init(geom, hp)
-    ncell = geom.ncells
+    geom, hp, unk0, mesh, ncell = make_problem(args.config, scale=args.scale)
     K, W = args.steps, args.warmup
 
     def barrier():
@@ -226,7 +282,7 @@ def run_ours(args):
     from flashx_b200.parallel import allreduce_min as global_min   # Driver_computeDt's AllReduce(MIN)
 
     def timed_run(precision):
-        dev = HydroDevice(geom, hp, precision)
+        dev = HydroDevice(geom, hp, precision, mesh=mesh)
         dev.attach_unk(unk0.copy())
         dt = global_min(0.5 * dev.Hydro_computeDt())
         ext = torch.cuda.ExternalStream(dev.lib.fxb_stream())
@@ -241,7 +297,7 @@ def run_ours(args):
             barrier()
             clocks = clk.stop()
             ms = e0.elapsed_time(e1)
-            launches = (2 if geom.ndim == 2 else 9) * K
+            launches = dev.last_timing()[1]
         else:
             dt_old = dt
             for _ in range(W):
@@ -258,7 +314,7 @@ def run_ours(args):
             barrier()
             clocks = clk.stop()
             ms = e0.elapsed_time(e1)
-            launches = (1 if geom.ndim == 2 else 8) * K
+            launches = dev.last_timing()[1] * K
         ms = max_over_ranks(ms)
         return dev, ms, launches, clocks
 
@@ -273,7 +329,7 @@ def run_ours(args):
         kms.append(dev.last_timing()[0])
     dev.Hydro_computeDt()
     kernel_ms = statistics.mean(kms)
-    fp64_state = np.zeros(geom.unk_shape)
+    fp64_state = np.zeros(unk0.shape)
     # e2e: host-driven loop through the C ABI, dt crossing PCIe every step
     dev.attach_unk(unk0.copy())
     dt = dt_old = 0.5 * dev.Hydro_computeDt()
@@ -288,7 +344,7 @@ def run_ours(args):
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e_value = world * ncell * K / e2e_s
     dev.sync_to_host(fp64_state)
-    ref_after = S.gather_global(geom, fp64_state)
+    ref_after = interiors(geom, fp64_state, mesh)
 
     peak, peak_kind = measured_peaks()
     achieved = BYTES_PER_ZONE * ncell / (kernel_ms / 1e3) / 1e9
@@ -303,28 +359,32 @@ def run_ours(args):
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (seeded Philox4x32-10 KH initial state)",
+            "dtype": "f64", "data": "synthetic (seeded initial state of the workload, Philox4x32-10 where random)",
             "config": {"workload": WORKLOADS[args.config] + ("" if args.scale == 1.0 else f" at scale {args.scale}"),
                        "zones_per_gpu": ncell, "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "inputs larger than L2 (671 MB state vs 126 MB L2)",
+                       "l2": "inputs larger than L2 (state %.0f MB vs 126 MB L2)" % (2 * 10 * 8 * ncell / 1e6),
                        "timing": "CUDA events on the library stream, device dt loop (CUDA graph)"},
             "clocks": clocks,
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "hydro2d_kernel<double>" if geom.ndim == 2 else
-                                   "3-D pipeline (sig3d, states3d x3, flux3d x3, update3d)<double>",
+                                   ("AMR step (restriction, guard fill, 3-D pipeline, flux correction, update)<double>"
+                                    if mesh is not None else
+                                    "3-D pipeline (sig3d, states3d x3, flux3d x3, update3d)<double>"),
                          "kernel_ms": kernel_ms,
                          "algorithmic_bytes_per_zone": BYTES_PER_ZONE},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24, "d2h_bytes_per_step": 8,
                     "note": "host loop via fxb_hydro_step/fxb_compute_dt: (t, dt, dtOld) in, dt out per step; "
                             "UNK stays resident on the device"}}
+    if mesh is not None:
+        line["config"]["leaves_per_level"] = mesh.level_counts()
     dev.close()
 
     # ---- mixed precision
     if not args.no_mixed:
         mdev, mms, mlaunch, mclk = timed_run("mixed")
-        mstate = np.zeros(geom.unk_shape)
+        mstate = np.zeros(unk0.shape)
         # same steps as the FP64 e2e run for the error estimate
         mdev.attach_unk(unk0.copy())
         dt = dt_old = 0.5 * mdev.Hydro_computeDt()
@@ -332,7 +392,7 @@ def run_ours(args):
             mdev.Hydro(0.0, dt, dt_old)
             dt_old, dt = dt, driver_dt(global_min(mdev.Hydro_computeDt()), dt, hp)
         mdev.sync_to_host(mstate)
-        m_after = S.gather_global(geom, mstate)
+        m_after = interiors(geom, mstate, mesh)
         mdev.close()
         l1 = {v: float(np.mean(np.abs(m_after[..., i] - ref_after[..., i])) / max(np.mean(np.abs(ref_after[..., i])), 1e-300))
               for v, i in (("dens", 0), ("pres", 5), ("velx", 8), ("vely", 9))}
