@@ -91,6 +91,9 @@ struct State {
     int stage_leaves = 0;
     int *leaf_blk_dev = nullptr, *d_dmap = nullptr;
     int nfiner = 0;
+    int cta[4] = {4, 4, 4, 4};                    // CTAs per block: sig, states, flux, update
+    int fill_cta = 8;
+    char tune_log[256] = "";
     std::unordered_map<uint64_t, int> map;
 };
 State S;
@@ -593,6 +596,7 @@ Args3D batch_args(const double *dtv, double dt)
     for (int d = 0; d < 3; d++) { a.wst[d] = S.w[d]; a.flx[d] = S.f[d]; }
     a.gcb = S.gcb; a.gcb_vstride = ne3(); a.gcb_bstride = ne3() * NV_DEV; a.ng = S.ng;
     a.dxl = S.d_dxl;
+    for (int q = 0; q < 4; q++) a.cta[q] = S.cta[q];
     a.odata = S.store[1 - S.cur]; a.o_vstride = S.vstride; a.o_bstride = S.bstride;
     const size_t r = rsize();
     a.sig_bstride = (long)(sig3d_bytes(S.n, S.n, S.n, r) / r);
@@ -617,7 +621,7 @@ void restrict_all(int which)
 
 void fill_batch(const AmrEntry3 *entries, int cnt, int which)
 {
-    amr_fill_kernel<<<dim3(8, cnt), 256, 0, S.C.stream>>>(mesh_args(which), entries, S.leaf_blk_dev, S.d_eosmask,
+    amr_fill_kernel<<<dim3(S.fill_cta, cnt), 256, 0, S.C.stream>>>(mesh_args(which), entries, S.leaf_blk_dev, S.d_eosmask,
                                                          S.gcb, ne3(), ne3() * NV_DEV, S.C.dprm, S.C.gam1inv,
                                                          S.C.ggprodinv);
 }
@@ -757,6 +761,65 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     return FXB_OK;
 }
 
+// Launch-shape search on the attached state: every stage of one batch is
+// timed with 1, 2, 4, 8 and 16 CTAs per block (one warm-up pass, one timed
+// pass each) and the fastest count per stage is kept.  The stages compute
+// cells independently, so the choice changes timings, never results.  The
+// update writes the other interior store, which the next step overwrites.
+int amr_tune()
+{
+    const char *ev = getenv("FXB_AMR_TUNE");
+    if (ev && atoi(ev) == 0) {
+        snprintf(S.tune_log, sizeof(S.tune_log), "AMR launch shape (CTAs per block): fill=%d sig=%d states=%d flux=%d "
+                 "update=%d, defaults (tuning off)", S.fill_cta, S.cta[0], S.cta[1], S.cta[2], S.cta[3]);
+        return FXB_OK;
+    }
+    const bool mixed = S.C.prm.precision == FXB_MIXED;
+    const int cand[5] = {1, 2, 4, 8, 16};
+    const int cnt = std::min(S.nleaf, S.batch);
+    cudaEvent_t e[6];
+    for (int i = 0; i < 6; i++) CKA(cudaEventCreate(&e[i]));
+    float best[5] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
+    int pick[5] = {S.fill_cta, S.cta[0], S.cta[1], S.cta[2], S.cta[3]};
+    restrict_all(S.cur);
+    for (int c : cand) {
+        S.fill_cta = c;
+        for (int q = 0; q < 4; q++) S.cta[q] = c;
+        Args3D a = batch_args(nullptr, 0.0);
+        a.batch = S.d_entries;
+        float t[5] = {0, 0, 0, 0, 0};
+        for (int rep = 0; rep < 2; rep++) {
+            CKA(cudaEventRecord(e[0], S.C.stream));
+            fill_batch(a.batch, cnt, S.cur);
+            CKA(cudaEventRecord(e[1], S.C.stream));
+            for (int st = 0; st < 3; st++) {
+                if (mixed) launch_amr3d_fluxes_mixed(a, cnt, 1 << st, S.C.stream);
+                else launch_amr3d_fluxes_fp64(a, cnt, 1 << st, S.C.stream);
+                CKA(cudaEventRecord(e[2 + st], S.C.stream));
+            }
+            if (mixed) launch_amr3d_update_mixed(a, cnt, S.C.stream); else launch_amr3d_update_fp64(a, cnt, S.C.stream);
+            CKA(cudaEventRecord(e[5], S.C.stream));
+            CKA(cudaGetLastError());
+            CKA(cudaEventSynchronize(e[5]));
+            for (int k = 0; k < 5; k++) CKA(cudaEventElapsedTime(&t[k], e[k], e[k + 1]));
+        }
+        for (int k = 0; k < 5; k++)
+            if (t[k] < best[k]) { best[k] = t[k]; pick[k] = c; }
+    }
+    for (int i = 0; i < 6; i++) cudaEventDestroy(e[i]);
+    S.fill_cta = pick[0];
+    for (int q = 0; q < 4; q++) S.cta[q] = pick[1 + q];
+    CKA(cudaMemsetAsync(S.C.rate_max, 0, sizeof(unsigned long long), S.C.stream));
+    CKA(cudaStreamSynchronize(S.C.stream));
+    snprintf(S.tune_log, sizeof(S.tune_log),
+             "AMR launch shape (CTAs of 256 per block, %d blocks of %d^3): fill=%d sig=%d states=%d flux=%d update=%d "
+             "(ms %.3f %.3f %.3f %.3f %.3f)", cnt, S.n, pick[0], pick[1], pick[2], pick[3], pick[4],
+             best[0], best[1], best[2], best[3], best[4]);
+    return FXB_OK;
+}
+
+const char *amr_tuning_log() { return S.tune_log; }
+
 int amr_attach(const double *unk_host)
 {
     const size_t per_unk = (size_t)ne3() * S.C.nunk;
@@ -771,7 +834,7 @@ int amr_attach(const double *unk_host)
         CKA(cudaGetLastError());
     }
     CKA(cudaStreamSynchronize(S.C.stream));
-    return FXB_OK;
+    return amr_tune();
 }
 
 int amr_sync_to_host(double *unk_host)
@@ -805,7 +868,9 @@ int amr_step(const double *dtv, double dt, int *launches)
     nl += S.maxlev - 1;
     Args3D a = batch_args(dtv, dt);
     auto fluxes = [&](int cnt) {
-        if (mixed) launch_amr3d_fluxes_mixed(a, cnt, S.C.stream); else launch_amr3d_fluxes_fp64(a, cnt, S.C.stream);
+        const int all = AMR_SIG | AMR_STATES | AMR_FLUX;
+        if (mixed) launch_amr3d_fluxes_mixed(a, cnt, all, S.C.stream);
+        else launch_amr3d_fluxes_fp64(a, cnt, all, S.C.stream);
     };
     auto emit = [&](int cnt) {
         if (mixed) launch_amr3d_emit_mixed(a, cnt, S.bflux, S.nfc, S.C.stream);

@@ -36,6 +36,8 @@ int amr_rate();
 int amr_eos();
 int amr_integrals(double *out7, double *partials, int npartials);
 long amr_leaf_cells();
+// the launch shape chosen at the last attach, as text
+const char *amr_tuning_log();
 
 // reports through fxb_last_error (defined in fxb_api.cu)
 int record_error(int code, const char *msg);

@@ -649,6 +649,15 @@ extern "C" int fxb_last_timing(double *ms, int *kernel_launches)
 
 extern "C" void *fxb_stream(void) { return (void *)L.stream; }
 
+extern "C" int fxb_tuning(char *buf, int len)
+{
+    if (!buf || len <= 0) return fail(FXB_EARG, "fxb_tuning: null or empty buffer");
+    if (amr_active()) snprintf(buf, len, "%s", amr_tuning_log());
+    else if (L.dom.ndim == 2) snprintf(buf, len, "uniform grid 2-D: one CTA of %d threads per 16x16 tile (fixed)", 320);
+    else snprintf(buf, len, "uniform grid 3-D: %d CTAs of 256 threads per stage (fixed)", 148 * 8);
+    return FXB_OK;
+}
+
 extern "C" int fxb_last_error(fxb_error *err)
 {
     if (err) *err = L.lasterr;

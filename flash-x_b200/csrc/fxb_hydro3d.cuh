@@ -57,7 +57,9 @@ struct Args3D {
     double *odata;              // interior store [block][var][cell]
     long o_vstride, o_bstride;
     long sig_bstride, w_bstride[3], f_bstride[3];   // elements of R per batch entry
+    int cta[4];                 // CTAs per batch entry: sig3d, states3d, flux3d, update3d
 };
+enum { AMR_SIG = 1, AMR_STATES = 2, AMR_FLUX = 4 };
 
 // 3-D tile extents accepted by fxb_init (the unfused kernels take any size)
 constexpr int T3X = 1, T3Y = 1, T3Z = 1;
@@ -572,16 +574,18 @@ __global__ void __launch_bounds__(256) amr_correct_flux_kernel(const Args3D a, c
     }
 }
 
-// The 3-D pipeline over one AMR batch of `entries` guard-filled blocks.
-template <class R> void launch_amr3d_fluxes_t(const Args3D &a, int entries, cudaStream_t s)
+// The 3-D pipeline over one AMR batch of `entries` guard-filled blocks; `which`
+// selects the stages (AMR_SIG | AMR_STATES | AMR_FLUX), a.cta[] the CTAs per block.
+template <class R> void launch_amr3d_fluxes_t(const Args3D &a, int entries, int which, cudaStream_t s)
 {
-    const dim3 g(4, entries);
-    sig3d_kernel<R, true><<<g, 256, 0, s>>>(a);
-    for (int d = 0; d < 3; d++) {
-        if (a.prm.order == 5) states3d_kernel<R, 5, true><<<g, 256, 0, s>>>(a, d);
-        else states3d_kernel<R, 3, true><<<g, 256, 0, s>>>(a, d);
-    }
-    for (int d = 0; d < 3; d++) flux3d_kernel<R, true><<<g, 256, 0, s>>>(a, d);
+    if (which & AMR_SIG) sig3d_kernel<R, true><<<dim3(a.cta[0], entries), 256, 0, s>>>(a);
+    if (which & AMR_STATES)
+        for (int d = 0; d < 3; d++) {
+            if (a.prm.order == 5) states3d_kernel<R, 5, true><<<dim3(a.cta[1], entries), 256, 0, s>>>(a, d);
+            else states3d_kernel<R, 3, true><<<dim3(a.cta[1], entries), 256, 0, s>>>(a, d);
+        }
+    if (which & AMR_FLUX)
+        for (int d = 0; d < 3; d++) flux3d_kernel<R, true><<<dim3(a.cta[2], entries), 256, 0, s>>>(a, d);
 }
 template <class R> void launch_amr3d_emit_t(const Args3D &a, int entries, void *bflux, long nfc, cudaStream_t s)
 {
@@ -594,7 +598,7 @@ template <class R> void launch_amr3d_correct_t(const Args3D &a, int entries, con
 }
 template <class R> void launch_amr3d_update_t(const Args3D &a, int entries, cudaStream_t s)
 {
-    update3d_kernel<R, true><<<dim3(4, entries), 256, 0, s>>>(a);
+    update3d_kernel<R, true><<<dim3(a.cta[3], entries), 256, 0, s>>>(a);
 }
 
 } // namespace fxb

@@ -3,7 +3,8 @@
 namespace fxb {
 cudaError_t setup_hydro3d_fp64() { return cudaSuccess; }
 void launch_hydro3d_fp64(const Args3D &a, cudaStream_t s) { launch_hydro3d_t<double>(a, s); }
-void launch_amr3d_fluxes_fp64(const Args3D &a, int entries, cudaStream_t s) { launch_amr3d_fluxes_t<double>(a, entries, s); }
+void launch_amr3d_fluxes_fp64(const Args3D &a, int entries, int which, cudaStream_t s)
+{ launch_amr3d_fluxes_t<double>(a, entries, which, s); }
 void launch_amr3d_emit_fp64(const Args3D &a, int entries, void *bflux, long nfc, cudaStream_t s)
 { launch_amr3d_emit_t<double>(a, entries, bflux, nfc, s); }
 void launch_amr3d_correct_fp64(const Args3D &a, int entries, const void *bflux, long nfc, const int *fine,

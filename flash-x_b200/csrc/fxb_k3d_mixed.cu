@@ -4,7 +4,8 @@
 namespace fxb {
 cudaError_t setup_hydro3d_mixed() { return cudaSuccess; }
 void launch_hydro3d_mixed(const Args3D &a, cudaStream_t s) { launch_hydro3d_t<float>(a, s); }
-void launch_amr3d_fluxes_mixed(const Args3D &a, int entries, cudaStream_t s) { launch_amr3d_fluxes_t<float>(a, entries, s); }
+void launch_amr3d_fluxes_mixed(const Args3D &a, int entries, int which, cudaStream_t s)
+{ launch_amr3d_fluxes_t<float>(a, entries, which, s); }
 void launch_amr3d_emit_mixed(const Args3D &a, int entries, void *bflux, long nfc, cudaStream_t s)
 { launch_amr3d_emit_t<float>(a, entries, bflux, nfc, s); }
 void launch_amr3d_correct_mixed(const Args3D &a, int entries, const void *bflux, long nfc, const int *fine,

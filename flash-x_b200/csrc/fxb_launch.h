@@ -16,12 +16,12 @@ cudaError_t setup_hydro3d_fp64();
 cudaError_t setup_hydro3d_mixed();
 void launch_hydro3d_fp64(const Args3D &a, cudaStream_t s);
 void launch_hydro3d_mixed(const Args3D &a, cudaStream_t s);
-void launch_amr3d_fluxes_fp64(const Args3D &a, int entries, cudaStream_t s);
+void launch_amr3d_fluxes_fp64(const Args3D &a, int entries, int which, cudaStream_t s);
 void launch_amr3d_emit_fp64(const Args3D &a, int entries, void *bflux, long nfc, cudaStream_t s);
 void launch_amr3d_correct_fp64(const Args3D &a, int entries, const void *bflux, long nfc, const int *fine,
                                const int *finer_mask, cudaStream_t s);
 void launch_amr3d_update_fp64(const Args3D &a, int entries, cudaStream_t s);
-void launch_amr3d_fluxes_mixed(const Args3D &a, int entries, cudaStream_t s);
+void launch_amr3d_fluxes_mixed(const Args3D &a, int entries, int which, cudaStream_t s);
 void launch_amr3d_emit_mixed(const Args3D &a, int entries, void *bflux, long nfc, cudaStream_t s);
 void launch_amr3d_correct_mixed(const Args3D &a, int entries, const void *bflux, long nfc, const int *fine,
                                const int *finer_mask, cudaStream_t s);

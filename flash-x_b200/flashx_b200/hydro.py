@@ -29,7 +29,7 @@ FXB_VARS = ("dens", "eint", "ener", "gamc", "game", "pres", "temp", "velx", "vel
 # entry points declared in include/flashx_b200.h
 ABI_SYMBOLS = ("fxb_init", "fxb_register_blocks", "fxb_attach_unk", "fxb_fill_guardcells",
                "fxb_hydro_step", "fxb_compute_dt", "fxb_advance", "fxb_eos", "fxb_sync_to_host",
-               "fxb_sync_from_host", "fxb_integrals", "fxb_integrals_noalloc", "fxb_last_timing", "fxb_stream",
+               "fxb_sync_from_host", "fxb_integrals", "fxb_integrals_noalloc", "fxb_last_timing", "fxb_stream", "fxb_tuning",
                "fxb_last_error", "fxb_finalize")
 
 
@@ -98,6 +98,7 @@ def load_library(path=LIB_PATH):
     L.fxb_integrals_noalloc.argtypes = [ctypes.c_void_p] * 6 + [ctypes.c_long, ctypes.c_double,
                                                                  ctypes.c_void_p, ctypes.c_void_p]
     L.fxb_last_timing.argtypes = [D, ctypes.POINTER(ctypes.c_int)]
+    L.fxb_tuning.argtypes = [ctypes.c_char_p, ctypes.c_int]
     L.fxb_stream.restype = ctypes.c_void_p
     L.fxb_last_error.argtypes = [ctypes.POINTER(FxbError)]
     L.fxb_finalize.restype = None
@@ -254,6 +255,12 @@ class HydroDevice:
         out = np.zeros(7)
         _check(self.lib.fxb_integrals(_dp(out)))
         return out
+
+    def tuning(self):
+        """The launch shape in use (the batched-block path tunes it at attach)."""
+        buf = ctypes.create_string_buffer(256)
+        _check(self.lib.fxb_tuning(buf, 256))
+        return buf.value.decode()
 
     def last_timing(self):
         ms = ctypes.c_double()

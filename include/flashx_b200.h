@@ -164,6 +164,11 @@ int fxb_last_timing(double *ms, int *kernel_launches);
 /* The library's CUDA stream (cudaStream_t), for callers that order their own
  * work after the library's. */
 void *fxb_stream(void);
+/* The kernel launch shape in use, as text (no reference counterpart: the
+ * batched-block path picks its CTAs per block for each stage by timing 1, 2,
+ * 4, 8 and 16 at fxb_attach_unk; FXB_AMR_TUNE=0 in the environment keeps the
+ * defaults).  The choice changes timings, never results. */
+int fxb_tuning(char *buf, int len);
 int fxb_last_error(fxb_error *err);
 void fxb_finalize(void);
 
