@@ -516,6 +516,25 @@ __global__ void amr_rate_kernel(const double *store, long vstride, long bstride,
     if ((threadIdx.x & 31) == 0) atomicMax(rate_max, (unsigned long long)__double_as_longlong(r));
 }
 
+// limiting cell of the leaves: first (leaf, k, j, i) whose rate equals the maximum
+__global__ void amr_locate_kernel(const double *store, long vstride, long bstride, int n, const int *leaf_blk,
+                                  const DevBlk *blk, const double *dxl, int nleaf, const unsigned long long *rate_max,
+                                  unsigned long long *key)
+{
+    const long per = (long)n * n * n;
+    const unsigned long long rm = *rate_max;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)nleaf * per; idx += (long)gridDim.x * blockDim.x) {
+        const int b = leaf_blk[idx / per];
+        const double *s = store + (long)b * bstride + idx % per;
+        const double *dl = dxl + 3 * (blk[b].level - 1);
+        double cs = sqrt(s[GC * vstride] * s[P * vstride] / s[D * vstride]);
+        double t = (fabs(s[VX * vstride] - 0.) + cs) * (1.0 / dl[0]);
+        t = fmax2(t, (fabs(s[VY * vstride] - 0.) + cs) * (1.0 / dl[1]));
+        t = fmax2(t, (fabs(s[VZ * vstride] - 0.) + cs) * (1.0 / dl[2]));
+        if ((unsigned long long)__double_as_longlong(t) == rm) atomicMin(key, (unsigned long long)idx);
+    }
+}
+
 __global__ void amr_integrals_kernel(const double *store, long vstride, long bstride, int n, const int *leaf_blk,
                                      const DevBlk *blk, const double *dxl, int nleaf, double *partials)
 {
@@ -929,6 +948,18 @@ int amr_eos()
     CKA(cudaGetLastError());
     return FXB_OK;
 }
+
+int amr_locate(unsigned long long *key)
+{
+    long work = amr_leaf_cells();
+    int grid = (int)std::min<long>((work + 255) / 256, 148L * 16);
+    amr_locate_kernel<<<grid, 256, 0, S.C.stream>>>(S.store[S.cur], S.vstride, S.bstride, S.n, S.leaf_blk_dev, S.d_blk,
+                                                    S.d_dxl, S.nleaf, S.C.rate_max, key);
+    CKA(cudaGetLastError());
+    return FXB_OK;
+}
+
+int amr_leaf_level(int leaf) { return (leaf >= 0 && leaf < S.nleaf) ? S.blk[S.leaf_blk[leaf]].level : 0; }
 
 int amr_integrals(double *out7, double *partials, int npartials)
 {

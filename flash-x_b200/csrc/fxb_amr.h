@@ -36,6 +36,9 @@ int amr_rate();
 int amr_eos();
 int amr_integrals(double *out7, double *partials, int npartials);
 long amr_leaf_cells();
+// first leaf cell (leaf, k, j, i linear index) whose CFL rate equals the reduced maximum
+int amr_locate(unsigned long long *key);
+int amr_leaf_level(int leaf);
 // the launch shape chosen at the last attach, as text
 const char *amr_tuning_log();
 

@@ -147,22 +147,48 @@ __global__ void eos_kernel(double *st, long vstride, long ncell, DevParams prm, 
     }
 }
 
+// Hydro_computeDt.F90:215-225 rate of one cell; the hydro kernels' epilogues
+// compute the same expression from the values they store
+__device__ __forceinline__ double cell_rate(const double *st, long vstride, long c, int ndim,
+                                            double dx, double dy, double dz)
+{
+    double dens = st[D * vstride + c], pres = st[P * vstride + c], gamc = st[GC * vstride + c];
+    double cs = sqrt(gamc * pres / dens);
+    double t = (fabs(st[VX * vstride + c] - 0.) + cs) * (1.0 / dx);
+    if (ndim > 1) t = fmax2(t, (fabs(st[VY * vstride + c] - 0.) + cs) * (1.0 / dy));
+    if (ndim > 2) t = fmax2(t, (fabs(st[VZ * vstride + c] - 0.) + cs) * (1.0 / dz));
+    return t;
+}
+
 // Hydro_computeDt rate over a state (used when no fused step produced it)
 __global__ void rate_kernel(const double *st, long vstride, int nx, int ny, int nz, int ndim,
                             double dx, double dy, double dz, unsigned long long *rate_max)
 {
     long ncell = (long)nx * ny * nz;
     double r = 0.;
-    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < ncell; c += (long)gridDim.x * blockDim.x) {
-        double dens = st[D * vstride + c], pres = st[P * vstride + c], gamc = st[GC * vstride + c];
-        double cs = sqrt(gamc * pres / dens);
-        double t = (fabs(st[VX * vstride + c] - 0.) + cs) * (1.0 / dx);
-        if (ndim > 1) t = fmax2(t, (fabs(st[VY * vstride + c] - 0.) + cs) * (1.0 / dy));
-        if (ndim > 2) t = fmax2(t, (fabs(st[VZ * vstride + c] - 0.) + cs) * (1.0 / dz));
-        r = fmax2(r, t);
-    }
+    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < ncell; c += (long)gridDim.x * blockDim.x)
+        r = fmax2(r, cell_rate(st, vstride, c, ndim, dx, dy, dz));
     for (int off = 16; off > 0; off >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, off));
     if ((threadIdx.x & 31) == 0) atomicMax(rate_max, (unsigned long long)__double_as_longlong(r));
+}
+
+// the limiting cell: the first (block in list order, then k, j, i) whose rate
+// equals the reduced maximum, as Hydro_computeDt's strict '>' scan keeps it
+__global__ void locate_kernel(const double *st, long vstride, int nx, int ny, int nz, int ndim, double dx,
+                              double dy, double dz, const unsigned long long *rate_max, int nxb, int nyb, int nzb,
+                              unsigned long long *key)
+{
+    const unsigned long long rm = *rate_max;
+    const long ncell = (long)nx * ny * nz;
+    const int nbx = nx / nxb, nby = ny / nyb;
+    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < ncell; c += (long)gridDim.x * blockDim.x) {
+        double r = cell_rate(st, vstride, c, ndim, dx, dy, dz);
+        if ((unsigned long long)__double_as_longlong(r) != rm) continue;
+        long gx = c % nx, gy = (c / nx) % ny, gz = c / ((long)nx * ny);
+        long b = ((gz / nzb) * nby + gy / nyb) * nbx + gx / nxb;
+        unsigned long long k = (unsigned long long)((((b * nzb) + gz % nzb) * nyb + gy % nyb) * nxb + gx % nxb);
+        atomicMin(key, k);
+    }
 }
 
 // Driver_computeDt on the device: dtNew = min(cfl/rate, f*dtOld), clamp.
@@ -558,7 +584,23 @@ extern "C" int fxb_compute_dt(double *dt_out, int32_t loc[5])
         CK(cudaGetLastError());
         L.rate_valid = true;
     }
-    unsigned long long bits = 0;
+    unsigned long long bits = 0, key = ~0ull;
+    if (loc) {
+        // L.partials doubles as the 8-byte key (fxb_integrals rewrites it before use)
+        unsigned long long *dkey = (unsigned long long *)L.partials;
+        CK(cudaMemsetAsync(dkey, 0xff, sizeof(unsigned long long), L.stream));
+        if (amr_active()) {
+            int rc = amr_locate(dkey);
+            if (rc) return rc;
+        } else {
+            locate_kernel<<<1184, 256, 0, L.stream>>>(L.buf[L.cur], L.vstride, L.nx, L.ny, L.nz, L.dom.ndim, cell_dx(0),
+                                                      cell_dx(1), cell_dx(2), L.rate_max, L.dom.nxb,
+                                                      L.dom.ndim >= 2 ? L.dom.nyb : 1, L.dom.ndim == 3 ? L.dom.nzb : 1,
+                                                      dkey);
+            CK(cudaGetLastError());
+        }
+        CK(cudaMemcpyAsync(&key, dkey, sizeof(key), cudaMemcpyDeviceToHost, L.stream));
+    }
     CK(cudaMemcpyAsync(&bits, L.rate_max, sizeof(bits), cudaMemcpyDeviceToHost, L.stream));
     CK(cudaStreamSynchronize(L.stream));
     int rc = check_err_word();
@@ -566,7 +608,22 @@ extern "C" int fxb_compute_dt(double *dt_out, int32_t loc[5])
     double r;
     memcpy(&r, &bits, sizeof(r));
     double dt = (r != 0.) ? L.prm.cfl / r : 1.79769313486231570e308;
-    if (loc) { loc[0] = 0; loc[1] = 0; loc[2] = 0; loc[3] = 1; loc[4] = 0; }
+    if (loc) {
+        // Hydro_computeDt.F90:231-235: i, j, k in the block's guard-inclusive
+        // 1-based index space, then the refinement level; the fifth entry is
+        // the 1-based UNK block (the reference keeps its MPI rank there)
+        for (int q = 0; q < 5; q++) loc[q] = 0;
+        if (key != ~0ull) {
+            const int ndim = L.dom.ndim, ng = L.dom.nguard;
+            const long nxb = L.dom.nxb, nyb = ndim >= 2 ? L.dom.nyb : 1, nzb = ndim == 3 ? L.dom.nzb : 1;
+            long i = key % nxb, j = (key / nxb) % nyb, k = (key / (nxb * nyb)) % nzb, b = key / (nxb * nyb * nzb);
+            loc[0] = (int32_t)(i + ng + 1);
+            loc[1] = (int32_t)(j + (ndim >= 2 ? ng + 1 : 1));
+            loc[2] = (int32_t)(k + (ndim == 3 ? ng + 1 : 1));
+            loc[3] = amr_active() ? amr_leaf_level((int)b) : 1;
+            loc[4] = (int32_t)(b + 1);
+        }
+    }
     *dt_out = dt;
     if (!(dt > 0.)) return fail(FXB_EDT, "[Hydro]: Computed dt is not positive! Aborting!");
     return FXB_OK;

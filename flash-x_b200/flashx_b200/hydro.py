@@ -232,12 +232,14 @@ class HydroDevice:
     def Hydro(self, simTime, dt, dtOld):
         _check(self.lib.fxb_hydro_step(float(simTime), float(dt), float(dtOld)))
 
-    def Hydro_computeDt(self):
-        """Global CFL time step of the current state (min over blocks)."""
+    def Hydro_computeDt(self, location=False):
+        """Global CFL time step of the current state (min over blocks).  With
+        location=True also the limiting cell as Flash-X's dtMinLoc: i, j, k
+        (1-based, guard cells counted), refinement level, 1-based block."""
         out = ctypes.c_double()
-        loc = (ctypes.c_int32 * 5)()
+        loc = (ctypes.c_int32 * 5)() if location else None
         _check(self.lib.fxb_compute_dt(ctypes.byref(out), loc))
-        return out.value
+        return (out.value, list(loc)) if location else out.value
 
     def Eos_wrapped(self):
         _check(self.lib.fxb_eos())

@@ -127,8 +127,12 @@ int fxb_fill_guardcells(double *unk_host);
 int fxb_hydro_step(double sim_time, double dt, double dt_old);
 /* Hydro_computeDt reduced over all blocks (Driver_computeDt's MPI_AllReduce
  * MIN of the per-block dtCheck): the CFL time step of the current state.
- * loc[5] receives i, j, k (1-based block-local, guard offset included),
- * level and block id of a limiting cell when loc is not NULL. */
+ * loc[5] receives, when loc is not NULL, the limiting cell as
+ * Hydro_computeDt.F90:231-235 records it: i, j, k in the block's 1-based
+ * guard-inclusive index space and the refinement level; the fifth entry is
+ * the 1-based UNK block (the reference keeps its MPI rank there).  Ties go to
+ * the first cell in block order, then k, j, i, as the reference's strict '>'
+ * scan does.  Locating costs one read of the state. */
 int fxb_compute_dt(double *dt_out, int32_t loc[5]);
 /* Driver loop on the device: nsteps of Hydro + Driver_computeDt dt control
  * (dtNew = min(dtCFL, tstep_change_factor*dtOld), clamped to [dtmin, dtmax]),

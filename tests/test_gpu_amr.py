@@ -150,3 +150,15 @@ def test_amr_rejects_unbalanced_mesh(need_gpu):
     mesh = A.mesh_from_levels(root, leaves)
     with pytest.raises(FlashXError, match="more than one level"):
         HydroDevice(root, hp, "fp64", mesh=mesh)
+
+
+def test_amr_compute_dt_location(need_gpu):
+    from test_gpu_parity import _expected_loc
+    root, hp, mesh, unk = _case(maxlev=2)
+    dev = HydroDevice(root, hp, "fp64", mesh=mesh)
+    dev.attach_unk(unk.copy())
+    dt, loc = dev.Hydro_computeDt(location=True)
+    dl = [mesh.deltas(int(l)) for l in mesh.levels]
+    assert loc == _expected_loc(root, unk, mesh.levels, dl)
+    assert loc[3] == int(mesh.levels[loc[4] - 1])
+    dev.close()

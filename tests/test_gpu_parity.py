@@ -251,3 +251,47 @@ def test_3d_conservation_and_mixed(need_gpu):
         outs[prec] = S.gather_global(geom, o)
     a, b = outs["mixed"], outs["fp64"]
     assert np.mean(np.abs(a[..., DENS] - b[..., DENS])) / np.mean(b[..., DENS]) <= L1_TOL_MIXED
+
+
+def _expected_loc(geom, unk, levels=None, deltas=None):
+    """Flash-X dtMinLoc from a host UNK: first cell (block, k, j, i) of maximal rate."""
+    g = geom.nguard
+    k0 = g if geom.ndim == 3 else 0
+    j0 = g if geom.ndim >= 2 else 0
+    nk = geom.nzb if geom.ndim == 3 else 1
+    nj = geom.nyb if geom.ndim >= 2 else 1
+    best, loc = -1.0, None
+    for b in range(unk.shape[0]):
+        u = unk[b, k0:k0 + nk, j0:j0 + nj, g:g + geom.nxb, :]
+        dx, dy, dz = deltas[b] if deltas is not None else geom.deltas()
+        cs = np.sqrt(u[..., GAMC] * u[..., PRES] / u[..., DENS])
+        r = (np.abs(u[..., VELX] - 0.) + cs) * (1.0 / dx)
+        if geom.ndim > 1:
+            r = np.maximum(r, (np.abs(u[..., VELY] - 0.) + cs) * (1.0 / dy))
+        if geom.ndim > 2:
+            r = np.maximum(r, (np.abs(u[..., VELZ] - 0.) + cs) * (1.0 / dz))
+        m = r.max()
+        if m > best:
+            best = m
+            k, j, i = np.unravel_index(np.argmax(r), r.shape)
+            loc = [int(i) + g + 1, int(j) + j0 + 1, int(k) + k0 + 1,
+                   int(levels[b]) if levels is not None else 1, b + 1]
+    return loc
+
+
+@pytest.mark.parametrize("name", ["kh2d", "sweep3d"])
+def test_compute_dt_location(need_gpu, name):
+    """fxb_compute_dt's limiting cell equals the first cell of maximal CFL rate,
+    in Hydro_computeDt's index convention, before and after a step."""
+    geom, hp, init = S.config(name, scale=0.25 if name == "kh2d" else 0.5)
+    unk = init(geom, hp)
+    dev = HydroDevice(geom, hp, "fp64")
+    dev.attach_unk(unk.copy())
+    dt, loc = dev.Hydro_computeDt(location=True)
+    assert loc == _expected_loc(geom, unk)
+    dev.Hydro(0.0, 0.5 * dt, 0.5 * dt)
+    dt2, loc2 = dev.Hydro_computeDt(location=True)
+    out = np.zeros(geom.unk_shape)
+    dev.sync_to_host(out)
+    assert loc2 == _expected_loc(geom, out)
+    dev.close()
