@@ -45,6 +45,7 @@ struct Lib {
     cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};   // two steps starting from buffer 0 / 1
     double gam1inv = 0., ggprodinv = 0.;
     void *sig3 = nullptr, *w3[3] = {nullptr, nullptr, nullptr}, *f3[3] = {nullptr, nullptr, nullptr};
+    void *slp3 = nullptr;          // PPM slopes of one direction (3-D)
     fxb_error lasterr{};
 };
 Lib L;
@@ -285,6 +286,8 @@ int launch_hydro(int src, const double *dtv, double dt)
         a.gam1inv = L.gam1inv; a.ggprodinv = L.ggprodinv;
         a.prm = L.dprm; a.rate_max = L.rate_max; a.err = L.err;
         a.sig = L.sig3;
+        a.slp = L.slp3;
+        a.slp_bstride = 0;
         for (int d = 0; d < 3; d++) { a.wst[d] = L.w3[d]; a.flx[d] = L.f3[d]; }
         if (L.prm.precision == FXB_MIXED) launch_hydro3d_mixed(a, L.stream);
         else launch_hydro3d_fp64(a, L.stream);
@@ -328,6 +331,7 @@ void free_all()
     if (L.err) cudaFree(L.err);
     if (L.partials) cudaFree(L.partials);
     if (L.sig3) cudaFree(L.sig3);
+    if (L.slp3) cudaFree(L.slp3);
     for (int d = 0; d < 3; d++) {
         if (L.w3[d]) cudaFree(L.w3[d]);
         if (L.f3[d]) cudaFree(L.f3[d]);
@@ -431,6 +435,7 @@ extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, cons
         // intermediates of the unfused 3-D pipeline, in the reconstruction type
         size_t rsz = p.precision == FXB_MIXED ? sizeof(float) : sizeof(double);
         CK(cudaMalloc(&L.sig3, sig3d_bytes(L.nx, L.ny, L.nz, rsz)));
+        if (p.order == 3) CK(cudaMalloc(&L.slp3, slp3d_bytes(L.nx, L.ny, L.nz, rsz)));
         for (int dd = 0; dd < 3; dd++) {
             CK(cudaMalloc(&L.w3[dd], w3d_bytes(dd, L.nx, L.ny, L.nz, rsz)));
             CK(cudaMalloc(&L.f3[dd], f3d_bytes(dd, L.nx, L.ny, L.nz, rsz)));
@@ -558,7 +563,7 @@ extern "C" int fxb_hydro_step(double sim_time, double dt, double dt_old)
         int rc = launch_hydro(L.cur, nullptr, dt);
         if (rc) return rc;
         L.cur = 1 - L.cur;
-        nl = L.dom.ndim == 2 ? 1 : 8;
+        nl = L.dom.ndim == 2 ? 1 : (L.prm.order == 3 ? 11 : 8);
     }
     CK(cudaEventRecord(L.ev1, L.stream));
     L.rate_valid = true;
@@ -638,7 +643,7 @@ extern "C" int fxb_advance(int nsteps, double *dt, double *dt_old, double f, dou
     CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
     // graphs of two steps (buffer c -> 1-c -> c), built once per starting buffer
     const bool amr = amr_active();
-    int step_launches = L.dom.ndim == 2 ? 1 : 8;
+    int step_launches = L.dom.ndim == 2 ? 1 : (L.prm.order == 3 ? 11 : 8);
     auto one_step = [&](int src) -> int {
         int rc = amr ? amr_step(L.dtv, 0., &step_launches) : launch_hydro(src, L.dtv, 0.);
         if (rc) return rc;

@@ -48,6 +48,8 @@ struct Args3D {
     void *sig;      // [3][6][(nx+2)(ny+2)(nz+2)] of R
     void *wst[3];   // per direction [12][cells with that coordinate in [-1, n]]
     void *flx[3];   // per direction [8][faces]
+    void *slp;      // PPM: characteristic-limited slopes of the current direction [6][Grid3::ns(d)]
+    long slp_bstride;           // AMR: elements of R per batch entry
     // AMR batch mode
     const double *gcb;          // guard-filled blocks [entry][var][nz+2g][ny+2g][nx+2g]
     long gcb_vstride, gcb_bstride;
@@ -85,6 +87,15 @@ struct Grid3 {
         if (d == 1) return ((long)k * (ny + 1) + j) * nx + i;
         return ((long)k * ny + j) * nx + i;
     }
+    // slope cells of direction d: coordinate d in [-2, n_d + 1], the others interior
+    __device__ long ns(int d) const {
+        return d == 0 ? (long)(nx + 4) * ny * nz : d == 1 ? (long)nx * (ny + 4) * nz : (long)nx * ny * (nz + 4);
+    }
+    __device__ long sidx(int d, int i, int j, int k) const {
+        if (d == 0) return ((long)k * ny + j) * (nx + 4) + (i + 2);
+        if (d == 1) return ((long)k * (ny + 4) + (j + 2)) * nx + i;
+        return ((long)(k + 2) * ny + j) * nx + i;
+    }
 };
 
 // primitive 8-vector (D,VX,VY,VZ,P,GC,GE,EI) of a possibly virtual cell
@@ -113,7 +124,7 @@ template <class R, bool AMR> struct Ctx3 {
     const double *src;
     long svs;
     int sx, sy, so;
-    R *sig, *wst[3], *flx[3];
+    R *sig, *wst[3], *flx[3], *slp;
     double dx, dy, dz;
     AmrEntry3 m;
     __device__ explicit Ctx3(const Args3D &a)
@@ -126,6 +137,7 @@ template <class R, bool AMR> struct Ctx3 {
             svs = a.gcb_vstride;
             so = a.ng; sx = a.nx + 2 * a.ng; sy = a.ny + 2 * a.ng;
             sig = (R *)a.sig + (long)bb * a.sig_bstride;
+            slp = (R *)a.slp + (long)bb * a.slp_bstride;
             for (int d = 0; d < 3; d++) {
                 wst[d] = (R *)a.wst[d] + (long)bb * a.w_bstride[d];
                 flx[d] = (R *)a.flx[d] + (long)bb * a.f_bstride[d];
@@ -135,6 +147,7 @@ template <class R, bool AMR> struct Ctx3 {
             m = AmrEntry3{0, 1, 0, 0};
             src = a.in; svs = a.vstride; so = 0; sx = a.nx; sy = a.ny;
             sig = (R *)a.sig;
+            slp = (R *)a.slp;
             for (int d = 0; d < 3; d++) { wst[d] = (R *)a.wst[d]; flx[d] = (R *)a.flx[d]; }
             dx = a.dx; dy = a.dy; dz = a.dz;
         }
@@ -238,6 +251,38 @@ __device__ __forceinline__ void ctu_term(const Args3D &a, const R *sigp, const G
     unrot3(e, tr, T);
 }
 
+// ---- PPM slopes of direction d ----------------------------------------------
+// hy_TVDslope of every cell once (eigensystem of the cell, characteristic or
+// primitive limiting over its two neighbours along d), in the rotated frame
+// of direction d; each face-state cell then reads the slopes of itself and of
+// its two neighbours instead of recomputing them.
+template <class R, bool AMR>
+__global__ void __launch_bounds__(256) slope3d_kernel(const Args3D a, int d)
+{
+    const Ctx3<R, AMR> X(a);
+    const Grid3 &G = X.G;
+    const long ns = G.ns(d);
+    const int lx = a.nx + (d == 0 ? 4 : 0), ly = a.ny + (d == 1 ? 4 : 0);
+    int di, dj, dk;
+    offs(d, 1, di, dj, dk);
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < ns; idx += (long)gridDim.x * blockDim.x) {
+        int i = (int)(idx % lx), j = (int)((idx / lx) % ly), k = (int)(idx / ((long)lx * ly));
+        if (d == 0) i -= 2; else if (d == 1) j -= 2; else k -= 2;
+        R S8[3][8], S[3][6], g[6];
+#pragma unroll
+        for (int o = -1; o <= 1; o++) {
+            X.load(a, i + o * di, j + o * dj, k + o * dk, S8[o + 1]);
+            six(S8[o + 1], g); rot3(d, g, S[o + 1]);
+        }
+        Eig<R> e;
+        if (!eigen(S[1][0], S[1][1], S[1][4], S8[1][GC], e)) atomicOr(a.err, ERR_SOUND);
+        R db[6];
+        tvd_slope(a.prm, e, S[0], S[1], S[2], db);
+#pragma unroll
+        for (int q = 0; q < 6; q++) X.slp[(long)q * ns + idx] = db[q];
+    }
+}
+
 // ---- face states of direction d ------------------------------------------------
 // One instantiation per reconstruction order, so the register allocation of
 // the PPM path (three eigensystems and slopes) and of the WENO path (one
@@ -273,6 +318,7 @@ __global__ void __launch_bounds__(256, MinB3D<R>::value) states3d_kernel(const A
         R S8[5][8], S[5][6], g[6];
 #pragma unroll
         for (int o = -2; o <= 2; o++) {
+            if (ORDER == 3 && (o == -2 || o == 2)) continue;   // PPM reads its neighbours' slopes instead
             X.load(a, i + o * di, j + o * dj, k + o * dk, S8[o + 2]);
             six(S8[o + 2], g); rot3(d, g, S[o + 2]);
         }
@@ -283,13 +329,16 @@ __global__ void __launch_bounds__(256, MinB3D<R>::value) states3d_kernel(const A
         if constexpr (ORDER == 5) {
             weno_interfaces(a.prm, e, S, vecL, vecR);
         } else {
-            Eig<R> eN, eP;
-            if (!eigen(S[1][0], S[1][1], S[1][4], S8[1][GC], eN)) atomicOr(a.err, ERR_SOUND);
-            if (!eigen(S[3][0], S[3][1], S[3][4], S8[3][GC], eP)) atomicOr(a.err, ERR_SOUND);
+            // slopes of the cell and its two neighbours from slope3d_kernel
+            const long ns = G.ns(d);
+            const long sN = G.sidx(d, i - di, j - dj, k - dk), s0 = G.sidx(d, i, j, k), sP = G.sidx(d, i + di, j + dj, k + dk);
             R dbN[6], db0[6], dbP[6];
-            tvd_slope(a.prm, eN, S[0], S[1], S[2], dbN);
-            tvd_slope(a.prm, e, S[1], S[2], S[3], db0);
-            tvd_slope(a.prm, eP, S[2], S[3], S[4], dbP);
+#pragma unroll
+            for (int q = 0; q < 6; q++) {
+                dbN[q] = X.slp[(long)q * ns + sN];
+                db0[q] = X.slp[(long)q * ns + s0];
+                dbP[q] = X.slp[(long)q * ns + sP];
+            }
             ppm_interfaces(S[1], S[2], S[3], dbN, db0, dbP, vecL, vecR);
         }
         R wm[6], wp[6], Wm[6], Wp[6];
@@ -492,6 +541,14 @@ inline size_t w3d_bytes(int d, int nx, int ny, int nz, size_t rsz)
     size_t n = d == 0 ? (size_t)(nx + 2) * ny * nz : d == 1 ? (size_t)nx * (ny + 2) * nz : (size_t)nx * ny * (nz + 2);
     return rsz * 12 * n;
 }
+// the PPM slope buffer, sized for the largest direction
+inline size_t slp3d_bytes(int nx, int ny, int nz, size_t rsz)
+{
+    size_t m = (size_t)(nx + 4) * ny * nz;
+    m = m > (size_t)nx * (ny + 4) * nz ? m : (size_t)nx * (ny + 4) * nz;
+    m = m > (size_t)nx * ny * (nz + 4) ? m : (size_t)nx * ny * (nz + 4);
+    return rsz * 6 * m;
+}
 inline size_t f3d_bytes(int d, int nx, int ny, int nz, size_t rsz)
 {
     size_t n = d == 0 ? (size_t)(nx + 1) * ny * nz : d == 1 ? (size_t)nx * (ny + 1) * nz : (size_t)nx * ny * (nz + 1);
@@ -503,8 +560,12 @@ template <class R> void launch_hydro3d_t(const Args3D &a, cudaStream_t s)
     const int nb = 148 * 8;
     sig3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
     for (int d = 0; d < 3; d++) {
-        if (a.prm.order == 5) states3d_kernel<R, 5, false><<<nb, 256, 0, s>>>(a, d);
-        else states3d_kernel<R, 3, false><<<nb, 256, 0, s>>>(a, d);
+        if (a.prm.order == 5) {
+            states3d_kernel<R, 5, false><<<nb, 256, 0, s>>>(a, d);
+        } else {
+            slope3d_kernel<R, false><<<nb, 256, 0, s>>>(a, d);
+            states3d_kernel<R, 3, false><<<nb, 256, 0, s>>>(a, d);
+        }
     }
     for (int d = 0; d < 3; d++) flux3d_kernel<R, false><<<nb, 256, 0, s>>>(a, d);
     update3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
@@ -581,8 +642,12 @@ template <class R> void launch_amr3d_fluxes_t(const Args3D &a, int entries, int 
     if (which & AMR_SIG) sig3d_kernel<R, true><<<dim3(a.cta[0], entries), 256, 0, s>>>(a);
     if (which & AMR_STATES)
         for (int d = 0; d < 3; d++) {
-            if (a.prm.order == 5) states3d_kernel<R, 5, true><<<dim3(a.cta[1], entries), 256, 0, s>>>(a, d);
-            else states3d_kernel<R, 3, true><<<dim3(a.cta[1], entries), 256, 0, s>>>(a, d);
+            if (a.prm.order == 5) {
+                states3d_kernel<R, 5, true><<<dim3(a.cta[1], entries), 256, 0, s>>>(a, d);
+            } else {
+                slope3d_kernel<R, true><<<dim3(a.cta[1], entries), 256, 0, s>>>(a, d);
+                states3d_kernel<R, 3, true><<<dim3(a.cta[1], entries), 256, 0, s>>>(a, d);
+            }
         }
     if (which & AMR_FLUX)
         for (int d = 0; d < 3; d++) flux3d_kernel<R, true><<<dim3(a.cta[2], entries), 256, 0, s>>>(a, d);
