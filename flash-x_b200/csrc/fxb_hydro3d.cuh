@@ -163,6 +163,22 @@ template <class R, bool AMR> struct Ctx3 {
             load_cell(a, i, j, k, v);
         }
     }
+    // the two Eos gammas of cell (i,j,k), all the Riemann solver needs of it
+    __device__ __forceinline__ void load_gammas(const Args3D &a, int i, int j, int k, R &gc, R &ge) const
+    {
+        long c;
+        if constexpr (AMR) {
+            c = ((long)(k + so) * sy + (j + so)) * sx + (i + so);
+        } else {
+            double s_ = 1.0;
+            int mi = map_axis(i, a.nx, a.bc[0], a.bc[1], &s_);
+            int mj = map_axis(j, a.ny, a.bc[2], a.bc[3], &s_);
+            int mk = map_axis(k, a.nz, a.bc[4], a.bc[5], &s_);
+            c = ((long)mk * a.ny + mj) * a.nx + mi;
+        }
+        gc = (R)__ldg(src + GC * svs + c);
+        ge = (R)__ldg(src + GE * svs + c);
+    }
     // offset of interior cell (i,j,k) in the source arrays
     __device__ __forceinline__ long cell(int i, int j, int k) const
     { return ((long)(k + so) * sy + (j + so)) * sx + (i + so); }
@@ -298,9 +314,10 @@ __global__ void __launch_bounds__(256) slope3d_kernel(const Args3D a, int d)
 #define FXB_S3_MINB_FP32 2
 #endif
 template <class R> struct MinB3D { static constexpr int value = sizeof(R) == 8 ? FXB_S3_MINB_FP64 : FXB_S3_MINB_FP32; };
-template <class R, int ORDER, bool AMR>
-__global__ void __launch_bounds__(256, MinB3D<R>::value) states3d_kernel(const Args3D a, int d)
+template <class R, int ORDER, bool AMR, int DIR>
+__global__ void __launch_bounds__(256, MinB3D<R>::value) states3d_kernel(const Args3D a)
 {
+    constexpr int d = DIR;
     const Ctx3<R, AMR> X(a);
     const Grid3 &G = X.G;
     const double dt = a.dtv ? a.dtv[0] : a.dt_arg;
@@ -410,9 +427,12 @@ __global__ void __launch_bounds__(256, MinB3D<R>::value) states3d_kernel(const A
 }
 
 // ---- Riemann fluxes of direction d ---------------------------------------------
-template <class R, bool AMR>
-__global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a, int d)
+// the direction is a template parameter so that the solver's per-direction
+// indexing of the state vectors resolves at compile time (no local memory)
+template <class R, bool AMR, int DIR>
+__global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
 {
+    constexpr int d = DIR;
     const Ctx3<R, AMR> X(a);
     const Grid3 &G = X.G;
     const R *w = X.wst[d];
@@ -424,12 +444,12 @@ __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a, int d)
         int di, dj, dk;
         offs(d, 1, di, dj, dk);
         long wl = G.widx(d, i - di, j - dj, k - dk), wr = G.widx(d, i, j, k);
-        R VL[6], VR[6], F[8], cl[8], cr[8];
+        R VL[6], VR[6], F[8], gcl, gel, gcr, ger;
 #pragma unroll
         for (int q = 0; q < 6; q++) { VL[q] = w[(long)q * nw + wl]; VR[q] = w[(long)(6 + q) * nw + wr]; }
-        X.load(a, i - di, j - dj, k - dk, cl);
-        X.load(a, i, j, k, cr);
-        int e = riemann(a.prm, d, VL, cl[GC], cl[GE], VR, cr[GC], cr[GE], F);
+        X.load_gammas(a, i - di, j - dj, k - dk, gcl, gel);
+        X.load_gammas(a, i, j, k, gcr, ger);
+        int e = riemann(a.prm, d, VL, gcl, gel, VR, gcr, ger, F);
         if (e) atomicOr(a.err, e);
 #pragma unroll
         for (int q = 0; q < NF; q++) f[(long)q * nf + idx] = F[q];
@@ -555,19 +575,27 @@ inline size_t f3d_bytes(int d, int nx, int ny, int nz, size_t rsz)
     return rsz * 8 * n;
 }
 
+// face states of one direction: PPM reads the slopes of slope3d_kernel
+template <class R, bool AMR, int DIR> void launch_states3d(const Args3D &a, dim3 g, cudaStream_t s)
+{
+    if (a.prm.order == 5) {
+        states3d_kernel<R, 5, AMR, DIR><<<g, 256, 0, s>>>(a);
+    } else {
+        slope3d_kernel<R, AMR><<<g, 256, 0, s>>>(a, DIR);
+        states3d_kernel<R, 3, AMR, DIR><<<g, 256, 0, s>>>(a);
+    }
+}
+
 template <class R> void launch_hydro3d_t(const Args3D &a, cudaStream_t s)
 {
     const int nb = 148 * 8;
     sig3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
-    for (int d = 0; d < 3; d++) {
-        if (a.prm.order == 5) {
-            states3d_kernel<R, 5, false><<<nb, 256, 0, s>>>(a, d);
-        } else {
-            slope3d_kernel<R, false><<<nb, 256, 0, s>>>(a, d);
-            states3d_kernel<R, 3, false><<<nb, 256, 0, s>>>(a, d);
-        }
-    }
-    for (int d = 0; d < 3; d++) flux3d_kernel<R, false><<<nb, 256, 0, s>>>(a, d);
+    launch_states3d<R, false, 0>(a, dim3(nb), s);
+    launch_states3d<R, false, 1>(a, dim3(nb), s);
+    launch_states3d<R, false, 2>(a, dim3(nb), s);
+    flux3d_kernel<R, false, 0><<<nb, 256, 0, s>>>(a);
+    flux3d_kernel<R, false, 1><<<nb, 256, 0, s>>>(a);
+    flux3d_kernel<R, false, 2><<<nb, 256, 0, s>>>(a);
     update3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
 }
 
@@ -640,17 +668,16 @@ __global__ void __launch_bounds__(256) amr_correct_flux_kernel(const Args3D a, c
 template <class R> void launch_amr3d_fluxes_t(const Args3D &a, int entries, int which, cudaStream_t s)
 {
     if (which & AMR_SIG) sig3d_kernel<R, true><<<dim3(a.cta[0], entries), 256, 0, s>>>(a);
-    if (which & AMR_STATES)
-        for (int d = 0; d < 3; d++) {
-            if (a.prm.order == 5) {
-                states3d_kernel<R, 5, true><<<dim3(a.cta[1], entries), 256, 0, s>>>(a, d);
-            } else {
-                slope3d_kernel<R, true><<<dim3(a.cta[1], entries), 256, 0, s>>>(a, d);
-                states3d_kernel<R, 3, true><<<dim3(a.cta[1], entries), 256, 0, s>>>(a, d);
-            }
-        }
-    if (which & AMR_FLUX)
-        for (int d = 0; d < 3; d++) flux3d_kernel<R, true><<<dim3(a.cta[2], entries), 256, 0, s>>>(a, d);
+    if (which & AMR_STATES) {
+        launch_states3d<R, true, 0>(a, dim3(a.cta[1], entries), s);
+        launch_states3d<R, true, 1>(a, dim3(a.cta[1], entries), s);
+        launch_states3d<R, true, 2>(a, dim3(a.cta[1], entries), s);
+    }
+    if (which & AMR_FLUX) {
+        flux3d_kernel<R, true, 0><<<dim3(a.cta[2], entries), 256, 0, s>>>(a);
+        flux3d_kernel<R, true, 1><<<dim3(a.cta[2], entries), 256, 0, s>>>(a);
+        flux3d_kernel<R, true, 2><<<dim3(a.cta[2], entries), 256, 0, s>>>(a);
+    }
 }
 template <class R> void launch_amr3d_emit_t(const Args3D &a, int entries, void *bflux, long nfc, cudaStream_t s)
 {
