@@ -86,6 +86,7 @@ struct State {
     double *gcb = nullptr;
     void *sig = nullptr, *w[3] = {nullptr, nullptr, nullptr}, *f[3] = {nullptr, nullptr, nullptr};
     void *slp = nullptr;                          // PPM slopes of one direction per batch entry
+    void *flat = nullptr;                         // flattening coefficients per batch entry
     void *bflux = nullptr;
     long nfc = 0;
     double *stage = nullptr;                      // UNK staging for attach / sync
@@ -614,6 +615,7 @@ Args3D batch_args(const double *dtv, double dt)
     a.prm = S.C.dprm; a.rate_max = S.C.rate_max; a.err = S.C.err;
     a.sig = S.sig;
     a.slp = S.slp;
+    a.flat = S.flat;
     for (int d = 0; d < 3; d++) { a.wst[d] = S.w[d]; a.flx[d] = S.f[d]; }
     a.gcb = S.gcb; a.gcb_vstride = ne3(); a.gcb_bstride = ne3() * NV_DEV; a.ng = S.ng;
     a.dxl = S.d_dxl;
@@ -622,6 +624,7 @@ Args3D batch_args(const double *dtv, double dt)
     const size_t r = rsize();
     a.sig_bstride = (long)(sig3d_bytes(S.n, S.n, S.n, r) / r);
     a.slp_bstride = (long)(slp3d_bytes(S.n, S.n, S.n, r) / r);
+    a.flat_bstride = 3L * (S.n + 2) * (S.n + 2) * (S.n + 2);
     for (int d = 0; d < 3; d++) {
         a.w_bstride[d] = (long)(w3d_bytes(d, S.n, S.n, S.n, r) / r);
         a.f_bstride[d] = (long)(f3d_bytes(d, S.n, S.n, S.n, r) / r);
@@ -660,7 +663,7 @@ void amr_destroy()
     dfree(S.store[0]); dfree(S.store[1]);
     dfree(S.d_blk); dfree(S.d_ntab); dfree(S.d_child); dfree(S.d_plist); dfree(S.d_eosmask);
     dfree(S.d_finer); dfree(S.d_fine); dfree(S.d_dxl); dfree(S.d_entries); dfree(S.leaf_blk_dev);
-    dfree(S.gcb); dfree(S.sig); dfree(S.slp);
+    dfree(S.gcb); dfree(S.sig); dfree(S.slp); dfree(S.flat);
     for (int d = 0; d < 3; d++) { dfree(S.w[d]); dfree(S.f[d]); }
     dfree(S.bflux); dfree(S.stage); dfree(S.d_dmap);
     S = State();
@@ -760,7 +763,8 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     const size_t per_entry = sizeof(double) * NV_DEV * ne3() + sig3d_bytes(S.n, S.n, S.n, r) +
                              w3d_bytes(0, S.n, S.n, S.n, r) + w3d_bytes(1, S.n, S.n, S.n, r) + w3d_bytes(2, S.n, S.n, S.n, r) +
                              f3d_bytes(0, S.n, S.n, S.n, r) + f3d_bytes(1, S.n, S.n, S.n, r) + f3d_bytes(2, S.n, S.n, S.n, r) +
-                             (c.prm.order == 3 ? slp3d_bytes(S.n, S.n, S.n, r) : 0);
+                             (c.prm.order == 3 ? slp3d_bytes(S.n, S.n, S.n, r) : 0) +
+                             (c.prm.flattening ? r * 3 * (size_t)(S.n + 2) * (S.n + 2) * (S.n + 2) : 0);
     size_t fr = 0, tot = 0;
     CKA(cudaMemGetInfo(&fr, &tot));
     long cap = (long)((fr * 6 / 10) / per_entry);
@@ -775,6 +779,7 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     CKA(cudaMalloc(&S.gcb, sizeof(double) * NV_DEV * ne3() * S.batch));
     CKA(cudaMalloc(&S.sig, sig3d_bytes(S.n, S.n, S.n, r) * S.batch));
     if (c.prm.order == 3) CKA(cudaMalloc(&S.slp, slp3d_bytes(S.n, S.n, S.n, r) * S.batch));
+    if (c.prm.flattening) CKA(cudaMalloc(&S.flat, r * 3 * (size_t)(S.n + 2) * (S.n + 2) * (S.n + 2) * S.batch));
     for (int d = 0; d < 3; d++) {
         CKA(cudaMalloc(&S.w[d], w3d_bytes(d, S.n, S.n, S.n, r) * S.batch));
         CKA(cudaMalloc(&S.f[d], f3d_bytes(d, S.n, S.n, S.n, r) * S.batch));

@@ -46,6 +46,7 @@ struct Lib {
     double gam1inv = 0., ggprodinv = 0.;
     void *sig3 = nullptr, *w3[3] = {nullptr, nullptr, nullptr}, *f3[3] = {nullptr, nullptr, nullptr};
     void *slp3 = nullptr;          // PPM slopes of one direction (3-D)
+    void *flat = nullptr;          // flattening coefficients (2-D and 3-D)
     fxb_error lasterr{};
 };
 Lib L;
@@ -273,6 +274,7 @@ int launch_hydro(int src, const double *dtv, double dt)
         a.dt_arg = dt; a.dtv = dtv;
         a.gam1inv = L.gam1inv; a.ggprodinv = L.ggprodinv;
         a.prm = L.dprm; a.rate_max = L.rate_max; a.err = L.err;
+        a.flat = L.flat;
         dim3 grid(L.nx / T2, L.ny / T2);
         if (L.prm.precision == FXB_MIXED) launch_hydro2d_mixed(a, grid, L.stream);
         else launch_hydro2d_fp64(a, grid, L.stream);
@@ -288,6 +290,8 @@ int launch_hydro(int src, const double *dtv, double dt)
         a.sig = L.sig3;
         a.slp = L.slp3;
         a.slp_bstride = 0;
+        a.flat = L.flat;
+        a.flat_bstride = 0;
         for (int d = 0; d < 3; d++) { a.wst[d] = L.w3[d]; a.flx[d] = L.f3[d]; }
         if (L.prm.precision == FXB_MIXED) launch_hydro3d_mixed(a, L.stream);
         else launch_hydro3d_fp64(a, L.stream);
@@ -332,6 +336,7 @@ void free_all()
     if (L.partials) cudaFree(L.partials);
     if (L.sig3) cudaFree(L.sig3);
     if (L.slp3) cudaFree(L.slp3);
+    if (L.flat) cudaFree(L.flat);
     for (int d = 0; d < 3; d++) {
         if (L.w3[d]) cudaFree(L.w3[d]);
         if (L.f3[d]) cudaFree(L.f3[d]);
@@ -365,6 +370,7 @@ extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, cons
     if (p.limiter < 1 || p.limiter > 5) return fail(FXB_EARG, "fxb_init: unknown slope limiter");
     if (p.precision != FXB_FP64 && p.precision != FXB_MIXED) return fail(FXB_EARG, "fxb_init: unknown precision");
     if (d.ndim == 2 && p.use_gravity) return fail(FXB_EUNSUPPORTED, "fxb_init: gravity is implemented for 3-D only");
+    if (p.flattening && p.use_gravity) return fail(FXB_EUNSUPPORTED, "fxb_init: use_flattening with gravity is not implemented");
     for (int i = 0; i < 2 * d.ndim; i++)
         if (d.bc[i] < 0 || d.bc[i] > 2) return fail(FXB_EARG, "fxb_init: unknown boundary condition");
     for (int a = 0; a < d.ndim; a++) {
@@ -399,6 +405,7 @@ extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, cons
     q.cfl = p.cfl; q.gamma = p.gamma; q.eint_switch = p.eint_switch; q.small_dens = p.small_dens;
     q.small_e = p.small_e; q.small_p = p.small_p; q.tiny = p.tiny; q.fpres = p.fpres;
     q.limited_beta = p.limited_beta; q.gas_constant = p.gas_constant; q.abar = p.abar;
+    q.flattening = p.flattening ? 1 : 0;
     // Gamma/Eos_init.F90:86 and Gamma/Eos.F90:177,240-241
     double gammam1 = 1.0 / (p.gamma - 1.0);
     L.gam1inv = 1. / gammam1;
@@ -426,6 +433,11 @@ extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, cons
     CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
     L.npartials = 1024;
     CK(cudaMalloc(&L.partials, sizeof(double) * (L.npartials * 7 + 8)));
+    if (p.flattening) {
+        size_t rsz0 = p.precision == FXB_MIXED ? sizeof(float) : sizeof(double);
+        size_t npad = (size_t)(L.nx + 2) * (L.ny + 2) * (d.ndim == 3 ? L.nz + 2 : 1);
+        CK(cudaMalloc(&L.flat, rsz0 * d.ndim * npad));
+    }
     if (d.ndim == 2) {
         CK(setup_hydro2d_fp64());
         CK(setup_hydro2d_mixed());
@@ -563,7 +575,7 @@ extern "C" int fxb_hydro_step(double sim_time, double dt, double dt_old)
         int rc = launch_hydro(L.cur, nullptr, dt);
         if (rc) return rc;
         L.cur = 1 - L.cur;
-        nl = L.dom.ndim == 2 ? 1 : (L.prm.order == 3 ? 11 : 8);
+        nl = (L.dom.ndim == 2 ? 1 : (L.prm.order == 3 ? 11 : 8)) + (L.prm.flattening ? 1 : 0);
     }
     CK(cudaEventRecord(L.ev1, L.stream));
     L.rate_valid = true;
@@ -643,7 +655,7 @@ extern "C" int fxb_advance(int nsteps, double *dt, double *dt_old, double f, dou
     CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
     // graphs of two steps (buffer c -> 1-c -> c), built once per starting buffer
     const bool amr = amr_active();
-    int step_launches = L.dom.ndim == 2 ? 1 : (L.prm.order == 3 ? 11 : 8);
+    int step_launches = (L.dom.ndim == 2 ? 1 : (L.prm.order == 3 ? 11 : 8)) + (L.prm.flattening ? 1 : 0);
     auto one_step = [&](int src) -> int {
         int rc = amr ? amr_step(L.dtv, 0., &step_launches) : launch_hydro(src, L.dtv, 0.);
         if (rc) return rc;

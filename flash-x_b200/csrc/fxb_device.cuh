@@ -28,6 +28,7 @@ struct DevParams {
     int order, weno_method, riemann, limiter, char_limiting, use_3d_full_ctu, use_aux_eint, use_gravity;
     double grav[3];
     double cfl, gamma, eint_switch, small_dens, small_e, small_p, tiny, fpres, limited_beta, gas_constant, abar;
+    int flattening;
 };
 
 // ---- precision helpers ---------------------------------------------------
@@ -254,6 +255,40 @@ __device__ __forceinline__ void ppm_trace(const Eig<R> &e, R dtn, R hdtn, const 
         R base = Vc[v] + divc(W6[v], 12.);
         Wm[v] = base + sl[v];
         Wp[v] = base + sr[v];
+    }
+}
+
+// ---- flattening (hy_getRiemannState.F90:367-465) ----------------------------
+// FlatTilde of a cell from the pressures one and two cells either side and the
+// normal velocity one cell either side along the sweep
+template <class R>
+__device__ __forceinline__ R flat_tilde(R pm2, R pm1, R pp1, R pp2, R vm1, R vp1)
+{
+    R dp1 = (pp1 - pm1);
+    R dp2 = (pp2 - pm2);
+    R dv1 = vp1 - vm1;
+    R Sp = (fabs(dp2) > R(1.e-15)) ? rdiv(dp1, dp2) - R(0.75) : R(0.);
+    R ft = fmax2(R(0.), fmin2(R(1.), R(10.) * Sp));
+    if ((rdiv(fabs(dp1), fmin2(pm1, pp1)) < divc(R(1.), 3.)) || dv1 > R(0.)) ft = R(0.);
+    return ft;
+}
+// FlatCoeff: the larger FlatTilde of the cell and its upstream neighbour in pressure
+template <class R>
+__device__ __forceinline__ R flat_coeff(R dp1, R ftm, R ft0, R ftp)
+{
+    if (dp1 < R(0.)) return fmax2(ft0, ftp);
+    if (dp1 == R(0.)) return ft0;
+    return fmax2(ft0, ftm);
+}
+// [5] of the PPM/WENO reconstructions: interface values pulled toward the
+// cell value by the flattening coefficient
+template <class R>
+__device__ __forceinline__ void flatten(R F, const R *Vc, R vecL[6], R vecR[6])
+{
+#pragma unroll
+    for (int n = 0; n < 6; n++) {
+        vecL[n] = F * Vc[n] + (R(1.0) - F) * vecL[n];
+        vecR[n] = F * Vc[n] + (R(1.0) - F) * vecR[n];
     }
 }
 

@@ -37,6 +37,7 @@ struct Args2D {
     DevParams prm;
     unsigned long long *rate_max;
     int *err;
+    const void *flat;        // flattening coefficients [2][(nx+2)(ny+2)] of R, padded by one cell
 };
 
 constexpr int T2 = 16;             // tile edge
@@ -173,6 +174,12 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
             dbP[k] = s.DBF[k * NDB + dbi + dbstep];
         }
         ppm_interfaces(Vm, Vc, Vp, dbN, db0, dbP, vecL, vecR);
+    }
+    if (a.prm.flattening) {
+        // the window origin is the tile origin minus three cells
+        const long gx = (long)blockIdx.x * T2 + wx - 3, gy = (long)blockIdx.y * T2 + wy - 3;
+        const long np = (long)(a.nx + 2) * (a.ny + 2);
+        flatten(((const R *)a.flat)[dir * np + (gy + 1) * (a.nx + 2) + gx + 1], Vc, vecL, vecR);
     }
     R wm[6], wp[6];
     ppm_trace(e, dtn, hdtn, Vc, vecL, vecR, wm, wp);
@@ -400,6 +407,34 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
         double m = red[0];
         for (int w = 1; w < NT2 / 32; w++) m = fmax(m, red[w]);
         atomicMax(a.rate_max, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+// flattening coefficients of every cell of the grid padded by one layer, both
+// directions (hy_getRiemannState.F90:367-465); neighbours through map_axis
+template <class R>
+__global__ void __launch_bounds__(256) flat2d_kernel(const Args2D a, R *flat)
+{
+    const long np = (long)(a.nx + 2) * (a.ny + 2);
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < np; idx += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % (a.nx + 2)) - 1, j = (int)(idx / (a.nx + 2)) - 1;
+        for (int d = 0; d < 2; d++) {
+            R p[7], v[5];
+#pragma unroll
+            for (int o = -3; o <= 3; o++) {
+                double sx = 1.0, sy = 1.0;
+                int gx = map_axis(i + (d == 0 ? o : 0), a.nx, a.bc[0], a.bc[1], &sx);
+                int gy = map_axis(j + (d == 1 ? o : 0), a.ny, a.bc[2], a.bc[3], &sy);
+                long c = (long)gy * a.nx + gx;
+                p[o + 3] = (R)__ldg(a.in + P * a.vstride + c);
+                if (o >= -2 && o <= 2)
+                    v[o + 2] = (R)(d == 0 ? __ldg(a.in + VX * a.vstride + c) * sx : __ldg(a.in + VY * a.vstride + c) * sy);
+            }
+            R ftm = flat_tilde(p[0], p[1], p[3], p[4], v[0], v[2]);
+            R ft0 = flat_tilde(p[1], p[2], p[4], p[5], v[1], v[3]);
+            R ftp = flat_tilde(p[2], p[3], p[5], p[6], v[2], v[4]);
+            flat[d * np + idx] = flat_coeff(p[4] - p[2], ftm, ft0, ftp);
+        }
     }
 }
 

@@ -50,6 +50,8 @@ struct Args3D {
     void *flx[3];   // per direction [8][faces]
     void *slp;      // PPM: characteristic-limited slopes of the current direction [6][Grid3::ns(d)]
     long slp_bstride;           // AMR: elements of R per batch entry
+    void *flat;     // flattening coefficients [3][(nx+2)(ny+2)(nz+2)] of R
+    long flat_bstride;          // AMR: elements of R per batch entry
     // AMR batch mode
     const double *gcb;          // guard-filled blocks [entry][var][nz+2g][ny+2g][nx+2g]
     long gcb_vstride, gcb_bstride;
@@ -124,7 +126,7 @@ template <class R, bool AMR> struct Ctx3 {
     const double *src;
     long svs;
     int sx, sy, so;
-    R *sig, *wst[3], *flx[3], *slp;
+    R *sig, *wst[3], *flx[3], *slp, *flat;
     double dx, dy, dz;
     AmrEntry3 m;
     __device__ explicit Ctx3(const Args3D &a)
@@ -138,6 +140,7 @@ template <class R, bool AMR> struct Ctx3 {
             so = a.ng; sx = a.nx + 2 * a.ng; sy = a.ny + 2 * a.ng;
             sig = (R *)a.sig + (long)bb * a.sig_bstride;
             slp = (R *)a.slp + (long)bb * a.slp_bstride;
+            flat = (R *)a.flat + (long)bb * a.flat_bstride;
             for (int d = 0; d < 3; d++) {
                 wst[d] = (R *)a.wst[d] + (long)bb * a.w_bstride[d];
                 flx[d] = (R *)a.flx[d] + (long)bb * a.f_bstride[d];
@@ -148,6 +151,7 @@ template <class R, bool AMR> struct Ctx3 {
             src = a.in; svs = a.vstride; so = 0; sx = a.nx; sy = a.ny;
             sig = (R *)a.sig;
             slp = (R *)a.slp;
+            flat = (R *)a.flat;
             for (int d = 0; d < 3; d++) { wst[d] = (R *)a.wst[d]; flx[d] = (R *)a.flx[d]; }
             dx = a.dx; dy = a.dy; dz = a.dz;
         }
@@ -235,6 +239,38 @@ __global__ void __launch_bounds__(256) sig3d_kernel(const Args3D a)
             unrot3(d, sr, sg);
 #pragma unroll
             for (int q = 0; q < 6; q++) sig[((long)d * 6 + q) * np + idx] = sg[q];
+        }
+    }
+}
+
+// ---- flattening coefficients of every padded cell, three directions ----------
+// (hy_getRiemannState.F90:367-465; FlatTilde of the cell and its two
+// neighbours along d from pressures three cells either side)
+template <class R, bool AMR>
+__global__ void __launch_bounds__(256) flat3d_kernel(const Args3D a)
+{
+    const Ctx3<R, AMR> X(a);
+    const Grid3 &G = X.G;
+    const long np = G.npad();
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < np; idx += (long)gridDim.x * blockDim.x) {
+        int i = (int)(idx % (a.nx + 2)) - 1;
+        int j = (int)((idx / (a.nx + 2)) % (a.ny + 2)) - 1;
+        int k = (int)(idx / ((long)(a.nx + 2) * (a.ny + 2))) - 1;
+        for (int d = 0; d < 3; d++) {
+            int di, dj, dk;
+            offs(d, 1, di, dj, dk);
+            R p[7], v[5];
+#pragma unroll
+            for (int o = -3; o <= 3; o++) {
+                R c[8];
+                X.load(a, i + o * di, j + o * dj, k + o * dk, c);
+                p[o + 3] = c[P];
+                if (o >= -2 && o <= 2) v[o + 2] = c[VX + d];
+            }
+            R ftm = flat_tilde(p[0], p[1], p[3], p[4], v[0], v[2]);
+            R ft0 = flat_tilde(p[1], p[2], p[4], p[5], v[1], v[3]);
+            R ftp = flat_tilde(p[2], p[3], p[5], p[6], v[2], v[4]);
+            X.flat[(long)d * np + idx] = flat_coeff(p[4] - p[2], ftm, ft0, ftp);
         }
     }
 }
@@ -358,6 +394,7 @@ __global__ void __launch_bounds__(256, MinB3D<R>::value) states3d_kernel(const A
             }
             ppm_interfaces(S[1], S[2], S[3], dbN, db0, dbP, vecL, vecR);
         }
+        if (a.prm.flattening) flatten(X.flat[(long)d * G.npad() + G.pidx(i, j, k)], S[2], vecL, vecR);
         R wm[6], wp[6], Wm[6], Wp[6];
         ppm_trace(e, dtn, hdtn, S[2], vecL, vecR, wm, wp);
         unrot3(d, wm, Wm); unrot3(d, wp, Wp);
@@ -589,6 +626,7 @@ template <class R, bool AMR, int DIR> void launch_states3d(const Args3D &a, dim3
 template <class R> void launch_hydro3d_t(const Args3D &a, cudaStream_t s)
 {
     const int nb = 148 * 8;
+    if (a.prm.flattening) flat3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
     sig3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
     launch_states3d<R, false, 0>(a, dim3(nb), s);
     launch_states3d<R, false, 1>(a, dim3(nb), s);
@@ -667,6 +705,7 @@ __global__ void __launch_bounds__(256) amr_correct_flux_kernel(const Args3D a, c
 // selects the stages (AMR_SIG | AMR_STATES | AMR_FLUX), a.cta[] the CTAs per block.
 template <class R> void launch_amr3d_fluxes_t(const Args3D &a, int entries, int which, cudaStream_t s)
 {
+    if ((which & AMR_SIG) && a.prm.flattening) flat3d_kernel<R, true><<<dim3(a.cta[0], entries), 256, 0, s>>>(a);
     if (which & AMR_SIG) sig3d_kernel<R, true><<<dim3(a.cta[0], entries), 256, 0, s>>>(a);
     if (which & AMR_STATES) {
         launch_states3d<R, true, 0>(a, dim3(a.cta[1], entries), s);

@@ -8,6 +8,7 @@ cudaError_t setup_hydro2d_fp64()
 }
 void launch_hydro2d_fp64(const Args2D &a, dim3 grid, cudaStream_t s)
 {
+    if (a.prm.flattening) flat2d_kernel<double><<<148 * 8, 256, 0, s>>>(a, (double *)a.flat);
     hydro2d_kernel<double><<<grid, Threads2D<double>::value, sizeof(Smem2D<double>), s>>>(a);
 }
 } // namespace fxb

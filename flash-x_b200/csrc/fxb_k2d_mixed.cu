@@ -10,6 +10,7 @@ cudaError_t setup_hydro2d_mixed()
 }
 void launch_hydro2d_mixed(const Args2D &a, dim3 grid, cudaStream_t s)
 {
+    if (a.prm.flattening) flat2d_kernel<float><<<148 * 8, 256, 0, s>>>(a, (float *)a.flat);
     hydro2d_kernel<float><<<grid, Threads2D<float>::value, sizeof(Smem2D<float>), s>>>(a);
 }
 } // namespace fxb

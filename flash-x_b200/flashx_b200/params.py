@@ -67,7 +67,9 @@ class HydroParams:
             raise ValueError("wenoMethod must be WENO5 or WENOZ")
         if self.transOrder != 1:
             raise ValueError("[hy_upwindTransverseFlux]: No high-order transFlux support! Please set transOrder=1.")
-        for flag in ("use_flattening", "use_steepening", "use_upwindTVD", "use_avisc", "use_hybridOrder"):
+        if self.use_flattening and self.useGravity:
+            raise ValueError("use_flattening with gravity is not supported by this path")
+        for flag in ("use_steepening", "use_upwindTVD", "use_avisc", "use_hybridOrder"):
             if getattr(self, flag):
                 raise ValueError(flag + " is not supported by this path")
         if self.hydroComputeDtOption != -1:

@@ -69,6 +69,7 @@ typedef struct fxb_params {
     double limited_beta;       /* LimitedSlopeBeta                                   */
     double gas_constant, abar; /* Eos Gamma: ideal gas constant, eos_singleSpeciesA  */
     int    precision;          /* enum fxb_precision                                 */
+    int    flattening;         /* use_flattening (not combined with gravity)         */
 } fxb_params;
 
 /* Domain of a uniform block grid. */

@@ -184,7 +184,7 @@ static void upwind_trans(const fxo_params *p, const double *vm1, const double *v
 /* ---- hy_DataReconstructNormalDir_PPM.F90:84-969 ------------------------ */
 /* S[0..4] = Vmm, Vm, Vc, Vp, Vpp (Vmm/Vpp unused when trans_only). */
 static int recon_ppm(const fxo_params *p, int dir, double dt, double delta,
-                     const double *S[5], int trans_only,
+                     const double *S[5], int trans_only, double flat,
                      double lam0[5], double L0[5][5], double R0[5][5],
                      double Wp[H_NV], double Wm[H_NV], double sig[H_NV])
 {
@@ -219,6 +219,12 @@ static int recon_ppm(const fxo_params *p, int dir, double dt, double delta,
         vecL[n] = 0.5 * (Vc[n] + Vm[n]) - (db0[n] - dbN[n]) / 6.;
         vecR[n] = 0.5 * (Vc[n] + Vp[n]) - (dbP[n] - db0[n]) / 6.;
     }
+    /* [5] flattening, hy_DataReconstructNormalDir_PPM.F90:687-690 */
+    if (p->flattening)
+        for (int n = 0; n < nend; n++) {
+            vecL[n] = flat * Vc[n] + (1.0 - flat) * vecL[n];
+            vecR[n] = flat * Vc[n] + (1.0 - flat) * vecR[n];
+        }
     /* monotonicity, CW84 eq. 1.10 */
     for (int n = 0; n < nend; n++) {
         if ((vecR[n] - Vc[n]) * (Vc[n] - vecL[n]) <= 0.) { vecL[n] = Vc[n]; vecR[n] = Vc[n]; }
@@ -267,7 +273,7 @@ static int recon_ppm(const fxo_params *p, int dir, double dt, double delta,
 
 /* ---- WENO5 / WENO-Z reconstruction: see recon_weno below --------------- */
 static int recon_weno(const fxo_params *p, int dir, double dt, double delta,
-                      const double *S[5], int trans_only,
+                      const double *S[5], int trans_only, double flat,
                       double lam0[5], double L0[5][5], double R0[5][5],
                       double Wp[H_NV], double Wm[H_NV], double sig[H_NV]);
 
@@ -396,6 +402,7 @@ typedef struct {
     double *leig;       /* [cell][3][5][5] */
     double *reig;       /* [cell][3][5][5] */
     double *pav;        /* VAR1 averaged pressure [cell] */
+    double *flat;       /* flattening: FlatTilde [3][cell], then FlatCoeff [3][cell] */
 } scratch_t;
 
 static void scratch_alloc(scratch_t *s, long ncell)
@@ -409,11 +416,12 @@ static void scratch_alloc(scratch_t *s, long ncell)
     s->leig = (double *)calloc((size_t)ncell * 75, sizeof(double));
     s->reig = (double *)calloc((size_t)ncell * 75, sizeof(double));
     s->pav = (double *)calloc((size_t)ncell, sizeof(double));
+    s->flat = (double *)calloc((size_t)ncell * 6, sizeof(double));
 }
 static void scratch_free(scratch_t *s)
 {
     for (int d = 0; d < 3; d++) { free(s->scr[d]); free(s->flx[d]); }
-    free(s->sig); free(s->lam); free(s->leig); free(s->reig); free(s->pav);
+    free(s->sig); free(s->lam); free(s->leig); free(s->reig); free(s->pav); free(s->flat);
 }
 
 static void blk_init(blk_t *b, const fxo_params *p)
@@ -444,6 +452,53 @@ static int riemann_states(const blk_t *b, const double *U, double dt, scratch_t 
     const int nev = n_end_vars(p);
     const int klo = b->k3 ? b->k0 - 1 : 0, khi = b->k3 ? b->kmax + 1 : 0;
     const int jlo = b->k2 ? b->j0 - 1 : 0, jhi = b->k2 ? b->jmax + 1 : 0;
+    double *FT = s->flat, *FC = s->flat + 3 * b->ncell;
+    if (p->flattening) {
+        /* hy_getRiemannState.F90:367-465: FlatTilde on [lo-2, hi+2] (zero
+         * elsewhere), then FlatCoeff on the same range (kHydro = 0) */
+        memset(s->flat, 0, sizeof(double) * 6 * b->ncell);
+        const int fk0 = b->k3 ? b->k0 - 2 : 0, fk1 = b->k3 ? b->kmax + 2 : 0;
+        const int fj0 = b->k2 ? b->j0 - 2 : 0, fj1 = b->k2 ? b->jmax + 2 : 0;
+        for (int k = fk0; k <= fk1; k++)
+        for (int j = fj0; j <= fj1; j++)
+        for (int i = b->i0 - 2; i <= b->imax + 2; i++)
+            for (int d = 0; d < ndim; d++) {
+                int di = d == 0, dj = d == 1, dk = d == 2;
+                const double *um2 = U + cidx(b, i - 2 * di, j - 2 * dj, k - 2 * dk) * FXO_NUNK;
+                const double *um1 = U + cidx(b, i - di, j - dj, k - dk) * FXO_NUNK;
+                const double *up1 = U + cidx(b, i + di, j + dj, k + dk) * FXO_NUNK;
+                const double *up2 = U + cidx(b, i + 2 * di, j + 2 * dj, k + 2 * dk) * FXO_NUNK;
+                double dp1 = (up1[FXO_PRES] - um1[FXO_PRES]);
+                double dp2 = (up2[FXO_PRES] - um2[FXO_PRES]);
+                double dv1 = up1[FXO_VELX + d] - um1[FXO_VELX + d];
+                double presL = um1[FXO_PRES], presR = up1[FXO_PRES];
+                double Sp = (fabs(dp2) > 1.e-15) ? dp1 / dp2 - 0.75 : 0.;
+                double ft = fmax2(0.0, fmin2(1.0, 10.0 * Sp));
+                if ((fabs(dp1) / fmin2(presL, presR) < 1. / 3.) || dv1 > 0.) ft = 0.;
+                FT[d * b->ncell + cidx(b, i, j, k)] = ft;
+            }
+        for (int k = fk0; k <= fk1; k++)
+        for (int j = fj0; j <= fj1; j++)
+        for (int i = b->i0 - 2; i <= b->imax + 2; i++)
+            for (int d = 0; d < ndim; d++) {
+                int di = d == 0, dj = d == 1, dk = d == 2;
+                long c = cidx(b, i, j, k);
+                double dp1 = (U[cidx(b, i + di, j + dj, k + dk) * FXO_NUNK + FXO_PRES] -
+                              U[cidx(b, i - di, j - dj, k - dk) * FXO_NUNK + FXO_PRES]);
+                double f0 = FT[d * b->ncell + c];
+                /* FlatTilde beyond the computed range is zero */
+                int ip = i + di, jp = j + dj, kp = k + dk, im = i - di, jm = j - dj, km = k - dk;
+                int inP = ip <= b->imax + 2 && jp <= fj1 && kp <= fk1;
+                int inM = im >= b->i0 - 2 && jm >= fj0 && km >= fk0;
+                double fP = inP ? FT[d * b->ncell + cidx(b, ip, jp, kp)] : 0.;
+                double fM = inM ? FT[d * b->ncell + cidx(b, im, jm, km)] : 0.;
+                double fc;
+                if (dp1 < 0.0) fc = fmax2(f0, fP);
+                else if (dp1 == 0.) fc = f0;
+                else fc = fmax2(f0, fM);
+                FC[d * b->ncell + c] = fc;
+            }
+    }
     for (int k = klo; k <= khi; k++)
     for (int j = jlo; j <= jhi; j++)
     for (int i = b->i0 - 1; i <= b->imax + 1; i++) {
@@ -474,9 +529,10 @@ static int riemann_states(const blk_t *b, const double *U, double dt, scratch_t 
                 load_v(p, U + cidx(b, ii, jj, kk) * FXO_NUNK, p->grav[d], V[o + 2]);
                 S[o + 2] = V[o + 2];
             }
+            double flat = p->flattening ? FC[d * b->ncell + c] : 0.;
             int err = (p->order == 5)
-                ? recon_weno(p, d, dt, del[d], S, tr[d], lam + 5 * d, leig[d], reig[d], Wp[d], Wn[d], sig + 9 * d)
-                : recon_ppm(p, d, dt, del[d], S, tr[d], lam + 5 * d, leig[d], reig[d], Wp[d], Wn[d], sig + 9 * d);
+                ? recon_weno(p, d, dt, del[d], S, tr[d], flat, lam + 5 * d, leig[d], reig[d], Wp[d], Wn[d], sig + 9 * d)
+                : recon_ppm(p, d, dt, del[d], S, tr[d], flat, lam + 5 * d, leig[d], reig[d], Wp[d], Wn[d], sig + 9 * d);
             if (err) return 1;
         }
         /* transverse contributions, hy_dataReconstOneStep.F90:931-962 */

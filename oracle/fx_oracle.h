@@ -54,6 +54,7 @@ typedef struct {
     double fpres;                   /* hy_fPresInMomFlux */
     double limited_beta;            /* LimitedSlopeBeta */
     double gas_constant, abar;      /* Eos Gamma: R and singleSpeciesA */
+    int flattening;                 /* use_flattening */
 } fxo_params;
 
 /* Number of doubles in one UNK array for the given geometry. */

@@ -42,6 +42,7 @@ class FxoParams(ctypes.Structure):
         ("tiny", ctypes.c_double), ("fpres", ctypes.c_double),
         ("limited_beta", ctypes.c_double),
         ("gas_constant", ctypes.c_double), ("abar", ctypes.c_double),
+        ("flattening", ctypes.c_int),
     ]
 
 
@@ -110,6 +111,7 @@ def make_params(geom, hp):
     p.eint_switch, p.small_dens, p.small_e, p.small_p = hp.eintSwitch, hp.smlrho, hp.smalle, hp.smallp
     p.tiny, p.fpres, p.limited_beta = hp.tiny, hp.hy_fPresInMomFlux, hp.LimitedSlopeBeta
     p.gas_constant, p.abar = hp.gasConstant, hp.eos_singleSpeciesA
+    p.flattening = int(hp.use_flattening)
     return p
 
 

@@ -29,8 +29,8 @@ def _interior(geom, u):
     return u[:, g:-g, g:-g, g:-g, :][..., HYDRO_VARS]
 
 
-def _case(bc=(BC_PERIODIC,) * 6, maxlev=2, nroot=4, order=5):
-    hp = HydroParams(order=order)
+def _case(bc=(BC_PERIODIC,) * 6, maxlev=2, nroot=4, order=5, flattening=False):
+    hp = HydroParams(order=order, use_flattening=flattening)
     root = Geometry(3, 8, 8, 8, nroot, nroot, nroot, bc=bc)
     mesh, unk = A.levelset_problem(root, hp, maxlev)
     assert len(set(mesh.levels)) == maxlev
@@ -57,13 +57,14 @@ def _gpu(root, hp, mesh, unk, dts, precision="fp64"):
     return dev, out
 
 
-@pytest.mark.parametrize("bc,maxlev,order", [
-    ((BC_PERIODIC,) * 6, 2, 5),
-    ((BC_OUTFLOW, BC_OUTFLOW, BC_PERIODIC, BC_PERIODIC, BC_REFLECTING, BC_REFLECTING), 2, 3),
-    ((BC_PERIODIC,) * 6, 3, 5),
+@pytest.mark.parametrize("bc,maxlev,order,flat", [
+    ((BC_PERIODIC,) * 6, 2, 5, False),
+    ((BC_OUTFLOW, BC_OUTFLOW, BC_PERIODIC, BC_PERIODIC, BC_REFLECTING, BC_REFLECTING), 2, 3, False),
+    ((BC_PERIODIC,) * 6, 3, 5, False),
+    ((BC_PERIODIC,) * 6, 2, 3, True),
 ])
-def test_amr_step_fp64_matches_oracle(oracle, need_gpu, bc, maxlev, order):
-    root, hp, mesh, unk = _case(bc, maxlev, order=order)
+def test_amr_step_fp64_matches_oracle(oracle, need_gpu, bc, maxlev, order, flat):
+    root, hp, mesh, unk = _case(bc, maxlev, order=order, flattening=flat)
     am = oracle.Amr(oracle.make_params(root.as_dict(), hp), mesh.levels, mesh.bcoords)
     dt = 0.5 * am.compute_dt(unk)
     _, ref = _oracle(oracle, root, hp, mesh, unk, [dt, dt])

@@ -108,6 +108,20 @@ def test_options_one_step_fp64(oracle, need_gpu, opts):
     assert np.array_equal(g, r)
 
 
+@pytest.mark.parametrize("order", [3, 5])
+def test_flattening_2d_fp64(oracle, need_gpu, order):
+    """use_flattening on the 45-degree Sod problem, where the shock switches it on."""
+    geom, _, init = S.config("sod2d", scale=0.25)
+    hp = HydroParams(order=order, use_flattening=True)
+    unk = init(geom, hp)
+    p = oracle.make_params(geom.as_dict(), hp)
+    dts, ref = oracle_dts(oracle, geom, hp, unk, 5, first=0.5 * oracle.compute_dt(p, unk))
+    _, out = gpu_run(geom, hp, unk, dts)
+    g, r = compare(geom, out, ref)
+    assert np.max(_rel(g, r)) <= REL_TOL_ONE_STEP
+    assert np.array_equal(g, r)
+
+
 @pytest.mark.parametrize("bc", [BC_OUTFLOW, BC_REFLECTING, BC_PERIODIC])
 def test_fill_guardcells_matches_oracle(oracle, need_gpu, bc):
     geom = Geometry(2, 16, 16, 1, 2, 3, 1, bc=(bc,) * 6)
@@ -198,7 +212,8 @@ def test_negative_pressure_reports_status(need_gpu):
 
 
 # ---------------------------------------------------------------- 3-D
-@pytest.mark.parametrize("case", ["ppm_periodic", "sod_outflow", "rt_weno_gravity", "hll_noctu", "wenoz_reflect"])
+@pytest.mark.parametrize("case", ["ppm_periodic", "sod_outflow", "rt_weno_gravity", "hll_noctu", "wenoz_reflect",
+                                  "sod_flattening", "weno_flattening_reflect"])
 def test_3d_fp64_matches_oracle(oracle, need_gpu, case):
     """3-D path (full CTU corner coupling, gravity, WENO) against the oracle,
     three steps, bit for bit."""
@@ -219,6 +234,14 @@ def test_3d_fp64_matches_oracle(oracle, need_gpu, case):
         geom = Geometry(3, 16, 16, 16, 1, 2, 1, bc=(BC_PERIODIC,) * 6)
         hp = HydroParams(RiemannSolver="HLL", use_3dFullCTU=False, slopeLimiter="minmod")
         unk = S.noisy_gas(geom, hp)
+    elif case == "sod_flattening":
+        geom = Geometry(3, 16, 16, 16, 2, 1, 1, bc=(BC_OUTFLOW,) * 6)
+        hp = HydroParams(use_flattening=True)
+        unk = S.sod(geom, hp, xangle=30.0, yangle=70.0, posn=0.6)
+    elif case == "weno_flattening_reflect":
+        geom = Geometry(3, 16, 16, 16, 1, 1, 1, bc=(BC_REFLECTING,) * 6)
+        hp = HydroParams(order=5, use_flattening=True)
+        unk = S.sod(geom, hp, xangle=30.0, yangle=70.0, posn=0.6)
     else:
         geom = Geometry(3, 16, 16, 16, 1, 1, 1, bc=(BC_REFLECTING,) * 6)
         hp = HydroParams(order=5, wenoMethod="WENOZ")
