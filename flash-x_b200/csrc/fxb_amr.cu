@@ -340,6 +340,21 @@ __device__ __forceinline__ bool same_level(const MeshArgs &m, int b, const DevBl
     return true;
 }
 
+// address of the level-lev cell x among block b's 27 neighbours (variable 0), or null
+__device__ __forceinline__ const double *same_level_ptr(const MeshArgs &m, int b, const DevBlk &B, const int x[3])
+{
+    int r[3], loc[3];
+    const int bc[3] = {B.c0, B.c1, B.c2};
+    for (int a = 0; a < 3; a++) {
+        r[a] = fdiv(x[a] - bc[a] * m.n, m.n);
+        if (r[a] < -1 || r[a] > 1) return nullptr;
+        loc[a] = x[a] - (bc[a] + r[a]) * m.n;
+    }
+    int nb = m.ntab[(long)b * 27 + (r[2] + 1) * 9 + (r[1] + 1) * 3 + (r[0] + 1)];
+    if (nb < 0) return nullptr;
+    return m.store + (long)nb * m.bstride + ((long)loc[2] * m.n + loc[1]) * m.n + loc[0];
+}
+
 // guard value of leaf block b at level-lev cell x
 __device__ bool guard_value(const MeshArgs &m, int b, const int xin[3], double out[NV_DEV])
 {
@@ -361,23 +376,35 @@ __device__ bool guard_value(const MeshArgs &m, int b, const int xin[3], double o
         p1[a] = fdiv(x[a] + 1, 2) - 1;
         wl[a] = ((x[a] & 1) == 0) ? 0.25 : 0.75;
     }
-    double S8[2][2][2][NV_DEV];
-    for (int kk = 0; kk < 2; kk++) for (int jj = 0; jj < 2; jj++) for (int ii = 0; ii < 2; ii++) {
+    // the eight parent-level stencil cells: their addresses, sign flips and densities
+    const double *ptr[8];
+    unsigned flip[8];
+    double dn[8];
+#pragma unroll
+    for (int s8 = 0; s8 < 8; s8++) {
+        const int ii = s8 & 1, jj = (s8 >> 1) & 1, kk = s8 >> 2;
         int q[3] = {p1[0] + ii, p1[1] + jj, p1[2] + kk};
         double sq[3] = {1., 1., 1.};
         for (int a = 0; a < 3; a++) q[a] = bc_map(m, PB.level, a, q[a], &sq[a]);
-        double *s = S8[kk][jj][ii];
-        if (!same_level(m, pb, PB, q, s)) return false;
-        s[VX] = s[VX] * sq[0]; s[VY] = s[VY] * sq[1]; s[VZ] = s[VZ] * sq[2];
-#pragma unroll
-        for (int v = 0; v < NV_DEV; v++)
-            if (per_mass(v)) s[v] = s[D] * s[v];
+        ptr[s8] = same_level_ptr(m, pb, PB, q);
+        if (!ptr[s8]) return false;
+        flip[s8] = (sq[0] < 0. ? 1u : 0u) | (sq[1] < 0. ? 2u : 0u) | (sq[2] < 0. ? 4u : 0u);
+        dn[s8] = ptr[s8][D * m.vstride];
     }
     const double dx = wl[0], cx = 1. - wl[0], dy = wl[1], cy = 1. - wl[1], dz = wl[2], cz = 1. - wl[2];
 #pragma unroll
-    for (int v = 0; v < NV_DEV; v++)
-        out[v] = dz * (dy * (dx * S8[0][0][0][v] + cx * S8[0][0][1][v]) + cy * (dx * S8[0][1][0][v] + cx * S8[0][1][1][v])) +
-                 cz * (dy * (dx * S8[1][0][0][v] + cx * S8[1][0][1][v]) + cy * (dx * S8[1][1][0][v] + cx * S8[1][1][1][v]));
+    for (int v = 0; v < NV_DEV; v++) {
+        double S[8];
+#pragma unroll
+        for (int s8 = 0; s8 < 8; s8++) {
+            double x8 = ptr[s8][v * m.vstride];
+            if (v >= VX && v <= VZ && ((flip[s8] >> (v - VX)) & 1u)) x8 = x8 * -1.;
+            S[s8] = per_mass(v) ? dn[s8] * x8 : x8;
+        }
+        // S[(kk*2 + jj)*2 + ii]
+        out[v] = dz * (dy * (dx * S[0] + cx * S[1]) + cy * (dx * S[2] + cx * S[3])) +
+                 cz * (dy * (dx * S[4] + cx * S[5]) + cy * (dx * S[6] + cx * S[7]));
+    }
     double dinv = out[D] == 0.0 ? 0.0 : 1. / out[D];
 #pragma unroll
     for (int v = 0; v < NV_DEV; v++)
