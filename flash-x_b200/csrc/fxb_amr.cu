@@ -83,7 +83,7 @@ struct State {
     double *d_dxl = nullptr;
     AmrEntry3 *d_entries = nullptr;               // [all][all, finer ones skipped][finer ones]
     int batch = 0;
-    double *gcb = nullptr;
+    void *gcb = nullptr;                          // guard-filled blocks in the reconstruction type
     void *sig = nullptr, *w[3] = {nullptr, nullptr, nullptr}, *f[3] = {nullptr, nullptr, nullptr};
     void *slp = nullptr;                          // PPM slopes of one direction per batch entry
     void *flat = nullptr;                         // flattening coefficients per batch entry
@@ -413,9 +413,13 @@ __device__ bool guard_value(const MeshArgs &m, int b, const int xin[3], double o
     return true;
 }
 
-// guard-filled copies of a batch of leaves: gcb[entry][var][nz+2g][ny+2g][nx+2g]
+// guard-filled copies of a batch of leaves, in the reconstruction type T:
+// out[entry][var][nz+2g][ny+2g][nx+2g]; with TO_UNK the FP64 values go into
+// UNK staging instead, out[leaf][k][j][i][nunk] at the variables' UNK slots
+template <class T, bool TO_UNK>
 __global__ void __launch_bounds__(256) amr_fill_kernel(MeshArgs m, const AmrEntry3 *entries, const int *leaf_blk,
-                                                       const unsigned *eosmask, double *gcb, long gvs, long gbs,
+                                                       const unsigned *eosmask, T *out, long gvs, long gbs,
+                                                       int nunk, const int *dmap,
                                                        DevParams prm, double gam1inv, double ggprodinv)
 {
     const AmrEntry3 e = entries[blockIdx.y];
@@ -424,7 +428,7 @@ __global__ void __launch_bounds__(256) amr_fill_kernel(MeshArgs m, const AmrEntr
     const unsigned mask = eosmask[e.leaf];
     const int n = m.n, g = m.ng, ne = n + 2 * g;
     const long ncell = (long)ne * ne * ne;
-    double *dst = gcb + (long)blockIdx.y * gbs;
+    T *dst = out + (long)blockIdx.y * gbs;
     for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < ncell; idx += (long)gridDim.x * blockDim.x) {
         int i = (int)(idx % ne) - g, j = (int)((idx / ne) % ne) - g, k = (int)(idx / ((long)ne * ne)) - g;
         double u[NV_DEV];
@@ -443,8 +447,13 @@ __global__ void __launch_bounds__(256) amr_fill_kernel(MeshArgs m, const AmrEntr
                 eos_cell_dev(u, prm, gam1inv, ggprodinv);
             }
         }
+        if constexpr (TO_UNK) {
 #pragma unroll
-        for (int v = 0; v < NV_DEV; v++) dst[v * gvs + idx] = u[v];
+            for (int v = 0; v < NV_DEV; v++) dst[idx * nunk + dmap[v]] = (T)u[v];
+        } else {
+#pragma unroll
+            for (int v = 0; v < NV_DEV; v++) dst[v * gvs + idx] = (T)u[v];
+        }
     }
 }
 
@@ -496,19 +505,6 @@ __global__ void amr_unk_to_store_kernel(const double *unk, int l0, int nl, const
         const double *u = unk + ((((long)l * ne + k + ng) * ne + j + ng) * ne + i + ng) * nunk;
         double *s = store + (long)leaf_blk[l0 + l] * bstride + c;
         for (int v = 0; v < NV_DEV; v++) s[v * vstride] = u[dmap[v]];
-    }
-}
-
-__global__ void amr_gcb_to_unk_kernel(const double *gcb, long gvs, long gbs, int nl, double *unk, int ne, int nunk,
-                                      const int *dmap)
-{
-    const long per = (long)ne * ne * ne;
-    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)nl * per; idx += (long)gridDim.x * blockDim.x) {
-        const int l = (int)(idx / per);
-        const long c = idx % per;
-        const double *g = gcb + (long)l * gbs + c;
-        double *u = unk + idx * nunk;
-        for (int v = 0; v < NV_DEV; v++) u[dmap[v]] = g[v * gvs];
     }
 }
 
@@ -645,6 +641,7 @@ Args3D batch_args(const double *dtv, double dt)
     a.flat = S.flat;
     for (int d = 0; d < 3; d++) { a.wst[d] = S.w[d]; a.flx[d] = S.f[d]; }
     a.gcb = S.gcb; a.gcb_vstride = ne3(); a.gcb_bstride = ne3() * NV_DEV; a.ng = S.ng;
+    a.istore = S.store[S.cur];
     a.dxl = S.d_dxl;
     for (int q = 0; q < 4; q++) a.cta[q] = S.cta[q];
     a.odata = S.store[1 - S.cur]; a.o_vstride = S.vstride; a.o_bstride = S.bstride;
@@ -673,9 +670,15 @@ void restrict_all(int which)
 
 void fill_batch(const AmrEntry3 *entries, int cnt, int which)
 {
-    amr_fill_kernel<<<dim3(S.fill_cta, cnt), 256, 0, S.C.stream>>>(mesh_args(which), entries, S.leaf_blk_dev, S.d_eosmask,
-                                                         S.gcb, ne3(), ne3() * NV_DEV, S.C.dprm, S.C.gam1inv,
-                                                         S.C.ggprodinv);
+    const dim3 g(S.fill_cta, cnt);
+    if (S.C.prm.precision == FXB_MIXED)
+        amr_fill_kernel<float, false><<<g, 256, 0, S.C.stream>>>(mesh_args(which), entries, S.leaf_blk_dev, S.d_eosmask,
+                                                                (float *)S.gcb, ne3(), ne3() * NV_DEV, 0, nullptr,
+                                                                S.C.dprm, S.C.gam1inv, S.C.ggprodinv);
+    else
+        amr_fill_kernel<double, false><<<g, 256, 0, S.C.stream>>>(mesh_args(which), entries, S.leaf_blk_dev, S.d_eosmask,
+                                                                 (double *)S.gcb, ne3(), ne3() * NV_DEV, 0, nullptr,
+                                                                 S.C.dprm, S.C.gam1inv, S.C.ggprodinv);
 }
 
 } // namespace
@@ -787,7 +790,7 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     S.stage_leaves = (int)std::max<size_t>(1, std::min<size_t>(nleaf, (1ull << 30) / per_unk));
     CKA(cudaMalloc(&S.stage, per_unk * S.stage_leaves));
     // batch of guard-filled blocks + pipeline intermediates: up to 60 % of what is free
-    const size_t per_entry = sizeof(double) * NV_DEV * ne3() + sig3d_bytes(S.n, S.n, S.n, r) +
+    const size_t per_entry = r * NV_DEV * ne3() + sig3d_bytes(S.n, S.n, S.n, r) +
                              w3d_bytes(0, S.n, S.n, S.n, r) + w3d_bytes(1, S.n, S.n, S.n, r) + w3d_bytes(2, S.n, S.n, S.n, r) +
                              f3d_bytes(0, S.n, S.n, S.n, r) + f3d_bytes(1, S.n, S.n, S.n, r) + f3d_bytes(2, S.n, S.n, S.n, r) +
                              (c.prm.order == 3 ? slp3d_bytes(S.n, S.n, S.n, r) : 0) +
@@ -803,7 +806,7 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
         long mb = atol(ev);
         if (mb >= 1) S.batch = (int)std::min<long>(S.batch, mb);
     }
-    CKA(cudaMalloc(&S.gcb, sizeof(double) * NV_DEV * ne3() * S.batch));
+    CKA(cudaMalloc(&S.gcb, r * NV_DEV * ne3() * S.batch));
     CKA(cudaMalloc(&S.sig, sig3d_bytes(S.n, S.n, S.n, r) * S.batch));
     if (c.prm.order == 3) CKA(cudaMalloc(&S.slp, slp3d_bytes(S.n, S.n, S.n, r) * S.batch));
     if (c.prm.flattening) CKA(cudaMalloc(&S.flat, r * 3 * (size_t)(S.n + 2) * (S.n + 2) * (S.n + 2) * S.batch));
@@ -897,17 +900,16 @@ int amr_sync_to_host(double *unk_host)
 {
     const size_t per_unk = (size_t)ne3() * S.C.nunk;
     restrict_all(S.cur);
-    const int chunk = std::min(S.stage_leaves, S.batch);
+    const int chunk = S.stage_leaves;
     for (int l0 = 0; l0 < S.nleaf; l0 += chunk) {
         int nl = std::min(chunk, S.nleaf - l0);
         // variables the device does not hold keep their host values
         CKA(cudaMemcpyAsync(S.stage, unk_host + per_unk * l0, sizeof(double) * per_unk * nl, cudaMemcpyHostToDevice,
                             S.C.stream));
-        fill_batch(S.d_entries + l0, nl, S.cur);
-        long work = (long)nl * ne3();
-        int grid = (int)std::min<long>((work + 255) / 256, 148L * 16);
-        amr_gcb_to_unk_kernel<<<grid, 256, 0, S.C.stream>>>(S.gcb, ne3(), ne3() * NV_DEV, nl, S.stage,
-                                                           S.n + 2 * S.ng, S.C.nunk, S.d_dmap);
+        // guard fill straight into the FP64 staging copy
+        amr_fill_kernel<double, true><<<dim3(S.fill_cta, nl), 256, 0, S.C.stream>>>(
+            mesh_args(S.cur), S.d_entries + l0, S.leaf_blk_dev, S.d_eosmask, S.stage, 0, (long)per_unk, S.C.nunk,
+            S.d_dmap, S.C.dprm, S.C.gam1inv, S.C.ggprodinv);
         CKA(cudaGetLastError());
         CKA(cudaMemcpyAsync(unk_host + per_unk * l0, S.stage, sizeof(double) * per_unk * nl, cudaMemcpyDeviceToHost,
                             S.C.stream));

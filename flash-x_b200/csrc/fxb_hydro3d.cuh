@@ -53,8 +53,9 @@ struct Args3D {
     void *flat;     // flattening coefficients [3][(nx+2)(ny+2)(nz+2)] of R
     long flat_bstride;          // AMR: elements of R per batch entry
     // AMR batch mode
-    const double *gcb;          // guard-filled blocks [entry][var][nz+2g][ny+2g][nx+2g]
+    const void *gcb;            // guard-filled blocks [entry][var][nz+2g][ny+2g][nx+2g] of R
     long gcb_vstride, gcb_bstride;
+    const double *istore;       // interior store holding the step's input state (FP64)
     int ng;
     const AmrEntry3 *batch;
     const double *dxl;          // cell sizes [level-1][3]
@@ -123,7 +124,8 @@ __device__ __forceinline__ void load_cell(const Args3D &a, int i, int j, int k, 
 // uniform grid, or (AMR) the batch entry blockIdx.y.
 template <class R, bool AMR> struct Ctx3 {
     Grid3 G;
-    const double *src;
+    const double *src;          // uniform grid: the FP64 state
+    const R *srcR;              // AMR: the guard-filled block in the reconstruction type
     long svs;
     int sx, sy, so;
     R *sig, *wst[3], *flx[3], *slp, *flat;
@@ -135,7 +137,8 @@ template <class R, bool AMR> struct Ctx3 {
         if constexpr (AMR) {
             const int bb = blockIdx.y;
             m = a.batch[bb];
-            src = a.gcb + (long)bb * a.gcb_bstride;
+            src = nullptr;
+            srcR = (const R *)a.gcb + (long)bb * a.gcb_bstride;
             svs = a.gcb_vstride;
             so = a.ng; sx = a.nx + 2 * a.ng; sy = a.ny + 2 * a.ng;
             sig = (R *)a.sig + (long)bb * a.sig_bstride;
@@ -148,7 +151,7 @@ template <class R, bool AMR> struct Ctx3 {
             dx = a.dxl[3 * (m.level - 1)]; dy = a.dxl[3 * (m.level - 1) + 1]; dz = a.dxl[3 * (m.level - 1) + 2];
         } else {
             m = AmrEntry3{0, 1, 0, 0};
-            src = a.in; svs = a.vstride; so = 0; sx = a.nx; sy = a.ny;
+            src = a.in; srcR = nullptr; svs = a.vstride; so = 0; sx = a.nx; sy = a.ny;
             sig = (R *)a.sig;
             slp = (R *)a.slp;
             flat = (R *)a.flat;
@@ -162,7 +165,7 @@ template <class R, bool AMR> struct Ctx3 {
         if constexpr (AMR) {
             long c = ((long)(k + so) * sy + (j + so)) * sx + (i + so);
 #pragma unroll
-            for (int q = 0; q < 8; q++) v[q] = (R)__ldg(src + q * svs + c);
+            for (int q = 0; q < 8; q++) v[q] = __ldg(srcR + q * svs + c);
         } else {
             load_cell(a, i, j, k, v);
         }
@@ -180,8 +183,13 @@ template <class R, bool AMR> struct Ctx3 {
             int mk = map_axis(k, a.nz, a.bc[4], a.bc[5], &s_);
             c = ((long)mk * a.ny + mj) * a.nx + mi;
         }
-        gc = (R)__ldg(src + GC * svs + c);
-        ge = (R)__ldg(src + GE * svs + c);
+        if constexpr (AMR) {
+            gc = __ldg(srcR + GC * svs + c);
+            ge = __ldg(srcR + GE * svs + c);
+        } else {
+            gc = (R)__ldg(src + GC * svs + c);
+            ge = (R)__ldg(src + GE * svs + c);
+        }
     }
     // offset of interior cell (i,j,k) in the source arrays
     __device__ __forceinline__ long cell(int i, int j, int k) const
@@ -509,8 +517,9 @@ __global__ void __launch_bounds__(256) update3d_kernel(const Args3D a)
     double rate = 0.;
     for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
         int i = (int)(c % a.nx), j = (int)((c / a.nx) % a.ny), k = (int)(c / ((long)a.nx * a.ny));
-        const long vs = X.svs;
-        const double *in = X.src + X.cell(i, j, k);
+        // the update starts from the FP64 state: the grid, or the leaf's interior store
+        const long vs = AMR ? a.o_vstride : X.svs;
+        const double *in = AMR ? a.istore + (long)X.m.out_blk * a.o_bstride + c : X.src + X.cell(i, j, k);
         double dens0 = in[D * vs];
         double vx0 = in[VX * vs], vy0 = in[VY * vs], vz0 = in[VZ * vs];
         double en0 = in[DV_ENER * vs], eint0 = in[EI * vs];
