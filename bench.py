@@ -382,6 +382,7 @@ def run_ours(args):
                             "UNK stays resident on the device"}}
     if mesh is not None:
         line["config"]["leaves_per_level"] = mesh.level_counts()
+        line["config"]["tuning"] = dev.tuning()
     dev.close()
 
     # ---- mixed precision

@@ -93,6 +93,8 @@ struct State {
     int stage_leaves = 0;
     int *leaf_blk_dev = nullptr, *d_dmap = nullptr;
     int nfiner = 0;
+    int *d_glist = nullptr;                       // guard cells the pipeline reads (extended-block offsets)
+    int nglist = 0;
     int cta[4] = {4, 4, 4, 4};                    // CTAs per block: sig, states, flux, update
     int fill_cta = 8;
     char tune_log[256] = "";
@@ -415,11 +417,19 @@ __device__ bool guard_value(const MeshArgs &m, int b, const int xin[3], double o
 
 // guard-filled copies of a batch of leaves, in the reconstruction type T:
 // out[entry][var][nz+2g][ny+2g][nx+2g]; with TO_UNK the FP64 values go into
-// UNK staging instead, out[leaf][k][j][i][nunk] at the variables' UNK slots
+// UNK staging instead, out[leaf][k][j][i][nunk] at the variables' UNK slots.
+// Three resident 256-thread CTAs per SM (80 registers) measured faster on
+// B200 than two (96) or four (64, with spills).
+#ifndef FXB_FILL_MINB
+#define FXB_FILL_MINB 3
+#endif
+// With a guard list (glist != nullptr) only the interior and the listed guard
+// cells (linear offsets in the extended block) are filled: the cells the
+// pipeline kernels read; without one every cell of the extended block is.
 template <class T, bool TO_UNK>
-__global__ void __launch_bounds__(256) amr_fill_kernel(MeshArgs m, const AmrEntry3 *entries, const int *leaf_blk,
+__global__ void __launch_bounds__(256, FXB_FILL_MINB) amr_fill_kernel(MeshArgs m, const AmrEntry3 *entries, const int *leaf_blk,
                                                        const unsigned *eosmask, T *out, long gvs, long gbs,
-                                                       int nunk, const int *dmap,
+                                                       int nunk, const int *dmap, const int *glist, int nlist,
                                                        DevParams prm, double gam1inv, double ggprodinv)
 {
     const AmrEntry3 e = entries[blockIdx.y];
@@ -427,9 +437,18 @@ __global__ void __launch_bounds__(256) amr_fill_kernel(MeshArgs m, const AmrEntr
     const DevBlk B = m.blk[b];
     const unsigned mask = eosmask[e.leaf];
     const int n = m.n, g = m.ng, ne = n + 2 * g;
-    const long ncell = (long)ne * ne * ne;
+    const long nint = (long)n * n * n;
+    const long ncell = glist ? nint + nlist : (long)ne * ne * ne;
     T *dst = out + (long)blockIdx.y * gbs;
-    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < ncell; idx += (long)gridDim.x * blockDim.x) {
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < ncell; t += (long)gridDim.x * blockDim.x) {
+        long idx;
+        if (!glist) {
+            idx = t;
+        } else if (t < nint) {
+            idx = ((t / ((long)n * n) + g) * ne + (t / n) % n + g) * ne + t % n + g;
+        } else {
+            idx = glist[t - nint];
+        }
         int i = (int)(idx % ne) - g, j = (int)((idx / ne) % ne) - g, k = (int)(idx / ((long)ne * ne)) - g;
         double u[NV_DEV];
         int ri = i < 0 ? -1 : i >= n ? 1 : 0, rj = j < 0 ? -1 : j >= n ? 1 : 0, rk = k < 0 ? -1 : k >= n ? 1 : 0;
@@ -674,11 +693,13 @@ void fill_batch(const AmrEntry3 *entries, int cnt, int which)
     if (S.C.prm.precision == FXB_MIXED)
         amr_fill_kernel<float, false><<<g, 256, 0, S.C.stream>>>(mesh_args(which), entries, S.leaf_blk_dev, S.d_eosmask,
                                                                 (float *)S.gcb, ne3(), ne3() * NV_DEV, 0, nullptr,
-                                                                S.C.dprm, S.C.gam1inv, S.C.ggprodinv);
+                                                                S.d_glist, S.nglist, S.C.dprm, S.C.gam1inv,
+                                                                S.C.ggprodinv);
     else
         amr_fill_kernel<double, false><<<g, 256, 0, S.C.stream>>>(mesh_args(which), entries, S.leaf_blk_dev, S.d_eosmask,
                                                                  (double *)S.gcb, ne3(), ne3() * NV_DEV, 0, nullptr,
-                                                                 S.C.dprm, S.C.gam1inv, S.C.ggprodinv);
+                                                                 S.d_glist, S.nglist, S.C.dprm, S.C.gam1inv,
+                                                                 S.C.ggprodinv);
 }
 
 } // namespace
@@ -695,7 +716,7 @@ void amr_destroy()
     dfree(S.d_finer); dfree(S.d_fine); dfree(S.d_dxl); dfree(S.d_entries); dfree(S.leaf_blk_dev);
     dfree(S.gcb); dfree(S.sig); dfree(S.slp); dfree(S.flat);
     for (int d = 0; d < 3; d++) { dfree(S.w[d]); dfree(S.f[d]); }
-    dfree(S.bflux); dfree(S.stage); dfree(S.d_dmap);
+    dfree(S.bflux); dfree(S.stage); dfree(S.d_dmap); dfree(S.d_glist);
     S = State();
 }
 
@@ -782,6 +803,34 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     CKA(up(S.leaf_blk_dev, S.leaf_blk));
     std::vector<int> dm(c.dmap, c.dmap + NV_DEV);
     CKA(up(S.d_dmap, dm));
+    // guard cells the 3-D pipeline reads: the padded box [-1, n]^3, and
+    // outside it cells with one coordinate out: layers -2 and n+1 with the
+    // others in [-1, n] (sigma), layers -3 and n+2 with the others interior
+    // (PPM slopes, WENO stencils); with flattening (pressures three cells
+    // either side of the padded box) every layer with the others in [-1, n]
+    {
+        std::vector<int> gl;
+        const int n = S.n, g = S.ng, ne = n + 2 * g;
+        auto in_box = [&](int x) { return x >= -1 && x <= n; };
+        auto in_int = [&](int x) { return x >= 0 && x < n; };
+        for (int k = -g; k < n + g; k++) for (int j = -g; j < n + g; j++) for (int i = -g; i < n + g; i++) {
+            if (in_int(i) && in_int(j) && in_int(k)) continue;           // interior: copied separately
+            int x[3] = {i, j, k}, outside = 0, ax = -1;
+            for (int a = 0; a < 3; a++) if (!in_box(x[a])) { outside++; ax = a; }
+            bool need = false;
+            if (outside == 0) need = true;
+            else if (outside == 1) {
+                int o1 = x[(ax + 1) % 3], o2 = x[(ax + 2) % 3];
+                bool depth1 = x[ax] == -2 || x[ax] == n + 1;
+                bool depth2 = x[ax] == -3 || x[ax] == n + 2;
+                if (c.prm.flattening || depth1) need = in_box(o1) && in_box(o2);
+                else if (depth2) need = in_int(o1) && in_int(o2);
+            }
+            if (need) gl.push_back(((k + g) * ne + (j + g)) * ne + (i + g));
+        }
+        S.nglist = (int)gl.size();
+        CKA(up(S.d_glist, gl));
+    }
     const size_t r = rsize();
     S.nfc = (long)S.n * S.n;
     CKA(cudaMalloc(&S.bflux, r * 6 * NF * S.nfc * (size_t)nleaf));
@@ -909,7 +958,7 @@ int amr_sync_to_host(double *unk_host)
         // guard fill straight into the FP64 staging copy
         amr_fill_kernel<double, true><<<dim3(S.fill_cta, nl), 256, 0, S.C.stream>>>(
             mesh_args(S.cur), S.d_entries + l0, S.leaf_blk_dev, S.d_eosmask, S.stage, 0, (long)per_unk, S.C.nunk,
-            S.d_dmap, S.C.dprm, S.C.gam1inv, S.C.ggprodinv);
+            S.d_dmap, nullptr, 0, S.C.dprm, S.C.gam1inv, S.C.ggprodinv);
         CKA(cudaGetLastError());
         CKA(cudaMemcpyAsync(unk_host + per_unk * l0, S.stage, sizeof(double) * per_unk * nl, cudaMemcpyDeviceToHost,
                             S.C.stream));
