@@ -95,6 +95,10 @@ struct State {
     int nfiner = 0;
     int *d_glist = nullptr;                       // guard cells the pipeline reads (extended-block offsets)
     int nglist = 0;
+    void *d_plan = nullptr;                       // GuardPlan [leaf][nglist]
+    void *d_prol = nullptr;                       // ProlRec, per leaf from d_poff[leaf]
+    int *d_poff = nullptr;
+    long nprol = 0;
     int cta[4] = {4, 4, 4, 4};                    // CTAs per block: sig, states, flux, update
     int fill_cta = 8;
     char tune_log[256] = "";
@@ -323,84 +327,100 @@ __device__ __forceinline__ int bc_map(const MeshArgs &m, int lev, int a, int x, 
     return x;   // inside, or periodic (left unwrapped: the neighbour table wraps)
 }
 
-// value of the level-lev cell x (unwrapped along periodic axes, inside along
-// the others) from the block holding it among block b's 27 neighbours
-__device__ __forceinline__ bool same_level(const MeshArgs &m, int b, const DevBlk &B, const int x[3], double out[NV_DEV])
+// store offset (variable 0) of the level-lev cell x (unwrapped along periodic
+// axes, inside along the others) in the block holding it among block b's 27
+// neighbours, or -1
+__device__ __forceinline__ long same_level_off(const MeshArgs &m, int b, const DevBlk &B, const int x[3])
 {
     int r[3], loc[3];
     const int bc[3] = {B.c0, B.c1, B.c2};
     for (int a = 0; a < 3; a++) {
         r[a] = fdiv(x[a] - bc[a] * m.n, m.n);
-        if (r[a] < -1 || r[a] > 1) return false;
+        if (r[a] < -1 || r[a] > 1) return -1;
         loc[a] = x[a] - (bc[a] + r[a]) * m.n;
     }
     int nb = m.ntab[(long)b * 27 + (r[2] + 1) * 9 + (r[1] + 1) * 3 + (r[0] + 1)];
-    if (nb < 0) return false;
-    const double *s = m.store + (long)nb * m.bstride + ((long)loc[2] * m.n + loc[1]) * m.n + loc[0];
-#pragma unroll
-    for (int v = 0; v < NV_DEV; v++) out[v] = s[v * m.vstride];
-    return true;
+    if (nb < 0) return -1;
+    return (long)nb * m.bstride + ((long)loc[2] * m.n + loc[1]) * m.n + loc[0];
 }
 
-// address of the level-lev cell x among block b's 27 neighbours (variable 0), or null
-__device__ __forceinline__ const double *same_level_ptr(const MeshArgs &m, int b, const DevBlk &B, const int x[3])
-{
-    int r[3], loc[3];
-    const int bc[3] = {B.c0, B.c1, B.c2};
-    for (int a = 0; a < 3; a++) {
-        r[a] = fdiv(x[a] - bc[a] * m.n, m.n);
-        if (r[a] < -1 || r[a] > 1) return nullptr;
-        loc[a] = x[a] - (bc[a] + r[a]) * m.n;
-    }
-    int nb = m.ntab[(long)b * 27 + (r[2] + 1) * 9 + (r[1] + 1) * 3 + (r[0] + 1)];
-    if (nb < 0) return nullptr;
-    return m.store + (long)nb * m.bstride + ((long)loc[2] * m.n + loc[1]) * m.n + loc[0];
-}
+// Where the guard value of one cell of a leaf comes from: a same-level cell
+// (a leaf or a restricted parent), or the eight parent-level cells of the
+// prolongation stencil, as store offsets of variable 0, with the sign flips
+// of reflecting boundaries (bit a: the velocity along axis a changes sign).
+enum { GS_SAME = 0, GS_PROL = 1, GS_NONE = 2 };
+struct GuardSrc {
+    int kind;
+    unsigned own;       // flips of the cell's own boundary map
+    unsigned parity;    // prolongation weights: bit a = x[a] & 1
+    unsigned flips;     // prolongation: three flip bits per stencil cell
+    long off[8];
+};
 
-// guard value of leaf block b at level-lev cell x
-__device__ bool guard_value(const MeshArgs &m, int b, const int xin[3], double out[NV_DEV])
+__device__ __forceinline__ void guard_resolve(const MeshArgs &m, int b, const int xin[3], GuardSrc &gs)
 {
     const DevBlk B = m.blk[b];
     int x[3];
     double sg[3] = {1., 1., 1.};
     for (int a = 0; a < 3; a++) x[a] = bc_map(m, B.level, a, xin[a], &sg[a]);
-    if (same_level(m, b, B, x, out)) {
-        out[VX] = out[VX] * sg[0]; out[VY] = out[VY] * sg[1]; out[VZ] = out[VZ] * sg[2];
-        return true;
-    }
-    if (B.parent < 0) return false;
-    // coarser neighbour: amr_1blk_cc_prol_linear from the parent level, conserved form
+    gs.own = (sg[0] < 0. ? 1u : 0u) | (sg[1] < 0. ? 2u : 0u) | (sg[2] < 0. ? 4u : 0u);
+    gs.parity = 0; gs.flips = 0;
+    gs.off[0] = same_level_off(m, b, B, x);
+    if (gs.off[0] >= 0) { gs.kind = GS_SAME; return; }
+    gs.kind = GS_NONE;
+    if (B.parent < 0) return;
+    // coarser neighbour: amr_1blk_cc_prol_linear from the parent level
     const int pb = B.parent;
     const DevBlk PB = m.blk[pb];
     int p1[3];
-    double wl[3];
     for (int a = 0; a < 3; a++) {
         p1[a] = fdiv(x[a] + 1, 2) - 1;
-        wl[a] = ((x[a] & 1) == 0) ? 0.25 : 0.75;
+        gs.parity |= (unsigned)(x[a] & 1) << a;
     }
-    // the eight parent-level stencil cells: their addresses, sign flips and densities
-    const double *ptr[8];
-    unsigned flip[8];
-    double dn[8];
 #pragma unroll
     for (int s8 = 0; s8 < 8; s8++) {
         const int ii = s8 & 1, jj = (s8 >> 1) & 1, kk = s8 >> 2;
         int q[3] = {p1[0] + ii, p1[1] + jj, p1[2] + kk};
         double sq[3] = {1., 1., 1.};
         for (int a = 0; a < 3; a++) q[a] = bc_map(m, PB.level, a, q[a], &sq[a]);
-        ptr[s8] = same_level_ptr(m, pb, PB, q);
-        if (!ptr[s8]) return false;
-        flip[s8] = (sq[0] < 0. ? 1u : 0u) | (sq[1] < 0. ? 2u : 0u) | (sq[2] < 0. ? 4u : 0u);
-        dn[s8] = ptr[s8][D * m.vstride];
+        gs.off[s8] = same_level_off(m, pb, PB, q);
+        if (gs.off[s8] < 0) return;
+        gs.flips |= ((sq[0] < 0. ? 1u : 0u) | (sq[1] < 0. ? 2u : 0u) | (sq[2] < 0. ? 4u : 0u)) << (3 * s8);
     }
-    const double dx = wl[0], cx = 1. - wl[0], dy = wl[1], cy = 1. - wl[1], dz = wl[2], cz = 1. - wl[2];
+    gs.kind = GS_PROL;
+}
+
+// same-level guard value: the cell's variables, velocities flipped at reflecting boundaries
+__device__ __forceinline__ void guard_eval_same(const double *store, long vstride, long off, unsigned own,
+                                                double out[NV_DEV])
+{
+    const double *s = store + off;
+#pragma unroll
+    for (int v = 0; v < NV_DEV; v++) out[v] = s[v * vstride];
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+        if ((own >> a) & 1u) out[VX + a] = out[VX + a] * -1.;
+}
+
+// prolonged guard value (amr_1blk_cc_prol_linear, conserved form): weights
+// 0.25 / 0.75 by the cell's parity per axis, per-mass variables times the
+// stencil cells' densities, divided by the interpolated density after
+__device__ __forceinline__ void guard_eval_prol(const double *store, long vstride, const long off[8], unsigned flips,
+                                                unsigned parity, unsigned own, double out[NV_DEV])
+{
+    double dn[8];
+#pragma unroll
+    for (int s8 = 0; s8 < 8; s8++) dn[s8] = store[off[s8] + D * vstride];
+    const double wx = (parity & 1u) ? 0.75 : 0.25, wy = ((parity >> 1) & 1u) ? 0.75 : 0.25,
+                 wz = ((parity >> 2) & 1u) ? 0.75 : 0.25;
+    const double dx = wx, cx = 1. - wx, dy = wy, cy = 1. - wy, dz = wz, cz = 1. - wz;
 #pragma unroll
     for (int v = 0; v < NV_DEV; v++) {
         double S[8];
 #pragma unroll
         for (int s8 = 0; s8 < 8; s8++) {
-            double x8 = ptr[s8][v * m.vstride];
-            if (v >= VX && v <= VZ && ((flip[s8] >> (v - VX)) & 1u)) x8 = x8 * -1.;
+            double x8 = store[off[s8] + v * vstride];
+            if (v >= VX && v <= VZ && ((flips >> (3 * s8 + v - VX)) & 1u)) x8 = x8 * -1.;
             S[s8] = per_mass(v) ? dn[s8] * x8 : x8;
         }
         // S[(kk*2 + jj)*2 + ii]
@@ -411,8 +431,19 @@ __device__ bool guard_value(const MeshArgs &m, int b, const int xin[3], double o
 #pragma unroll
     for (int v = 0; v < NV_DEV; v++)
         if (per_mass(v)) out[v] = dinv * out[v];
-    out[VX] = out[VX] * sg[0]; out[VY] = out[VY] * sg[1]; out[VZ] = out[VZ] * sg[2];
-    return true;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+        if ((own >> a) & 1u) out[VX + a] = out[VX + a] * -1.;
+}
+
+// guard value of leaf block b at level-lev cell x
+__device__ __forceinline__ bool guard_value(const MeshArgs &m, int b, const int xin[3], double out[NV_DEV])
+{
+    GuardSrc gs;
+    guard_resolve(m, b, xin, gs);
+    if (gs.kind == GS_SAME) guard_eval_same(m.store, m.vstride, gs.off[0], gs.own, out);
+    else if (gs.kind == GS_PROL) guard_eval_prol(m.store, m.vstride, gs.off, gs.flips, gs.parity, gs.own, out);
+    return gs.kind != GS_NONE;
 }
 
 // guard-filled copies of a batch of leaves, in the reconstruction type T:
@@ -473,6 +504,150 @@ __global__ void __launch_bounds__(256, FXB_FILL_MINB) amr_fill_kernel(MeshArgs m
 #pragma unroll
             for (int v = 0; v < NV_DEV; v++) dst[v * gvs + idx] = (T)u[v];
         }
+    }
+}
+
+// ---- guard-fill plan ----------------------------------------------------------
+// The mesh does not change between steps, so where every guard cell the
+// pipeline reads comes from is resolved once: per leaf and guard-list entry a
+// GuardPlan (same-level source, or a prolongation record), and per leaf the
+// prolongation records in guard-list order.  The step's fill then copies the
+// same-level cells in one light kernel and interpolates the prolonged ones
+// in another, with the arithmetic of the direct path.
+struct GuardPlan {
+    unsigned off;       // same-level source: store offset of variable 0
+    unsigned flags;     // bits 0-2 own flips, bit 3 Eos, bits 4-5 kind
+};
+struct __align__(16) ProlRec {
+    unsigned idx;       // extended-block offset of the guard cell
+    unsigned flags;     // bits 0-2 parity, 3-5 own flips, 6 Eos, 8-31 stencil flips
+    unsigned off[8];    // stencil cells' store offsets (variable 0)
+    unsigned pad[2];
+};
+
+__device__ __forceinline__ void ext_coords(long idx, int ne, int g, int &i, int &j, int &k)
+{
+    i = (int)(idx % ne) - g; j = (int)((idx / ne) % ne) - g; k = (int)(idx / ((long)ne * ne)) - g;
+}
+
+// one CTA per leaf; pass 0 writes the plan and counts the prolonged cells,
+// pass 1 writes the prolongation records at poff[leaf] in guard-list order
+__global__ void __launch_bounds__(256) amr_plan_kernel(MeshArgs m, const int *leaf_blk, const unsigned *eosmask,
+                                                       const int *glist, int nglist, GuardPlan *plan, int *pcount,
+                                                       ProlRec *prol, const int *poff, int pass)
+{
+    __shared__ int wsum[8];
+    const int leaf = blockIdx.x;
+    const int b = leaf_blk[leaf];
+    const DevBlk B = m.blk[b];
+    const unsigned mask = eosmask[leaf];
+    const int n = m.n, g = m.ng, ne = n + 2 * g;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int base = pass ? poff[leaf] : 0;
+    for (int g0 = 0; g0 < nglist; g0 += blockDim.x) {
+        const int t = g0 + threadIdx.x;
+        GuardSrc gs;
+        gs.kind = GS_NONE;
+        unsigned eos = 0, idx = 0;
+        if (t < nglist) {
+            idx = (unsigned)glist[t];
+            int i, j, k;
+            ext_coords(idx, ne, g, i, j, k);
+            const int x[3] = {B.c0 * n + i, B.c1 * n + j, B.c2 * n + k};
+            guard_resolve(m, b, x, gs);
+            const int ri = i < 0 ? -1 : i >= n ? 1 : 0, rj = j < 0 ? -1 : j >= n ? 1 : 0,
+                      rk = k < 0 ? -1 : k >= n ? 1 : 0;
+            eos = (mask >> ((rk + 1) * 9 + (rj + 1) * 3 + (ri + 1))) & 1u;
+            if (!pass) {
+                GuardPlan gp;
+                gp.off = gs.kind == GS_SAME ? (unsigned)gs.off[0] : 0u;
+                gp.flags = gs.own | (eos << 3) | ((unsigned)gs.kind << 4);
+                plan[(long)leaf * nglist + t] = gp;
+            }
+        }
+        const bool pr = t < nglist && gs.kind == GS_PROL;
+        const unsigned bal = __ballot_sync(0xffffffffu, pr);
+        if (lane == 0) wsum[w] = __popc(bal);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) { if (q < w) before += wsum[q]; total += wsum[q]; }
+        if (pass && pr) {
+            ProlRec r;
+            r.idx = idx;
+            r.flags = gs.parity | (gs.own << 3) | (eos << 6) | (gs.flips << 8);
+#pragma unroll
+            for (int s8 = 0; s8 < 8; s8++) r.off[s8] = (unsigned)gs.off[s8];
+            r.pad[0] = r.pad[1] = 0;
+            prol[base + before + __popc(bal & ((1u << lane) - 1u))] = r;
+        }
+        base += total;
+        __syncthreads();
+    }
+    if (!pass && threadIdx.x == 0) pcount[leaf] = base;
+}
+
+// interior cells and same-level guard cells of a batch from the plan
+template <class T>
+__global__ void __launch_bounds__(256) amr_copy_kernel(MeshArgs m, const AmrEntry3 *entries, const int *leaf_blk,
+                                                       const GuardPlan *plan, const int *glist, int nglist, T *out,
+                                                       long gvs, long gbs, DevParams prm, double gam1inv,
+                                                       double ggprodinv)
+{
+    const AmrEntry3 e = entries[blockIdx.y];
+    const int b = leaf_blk[e.leaf];
+    const int n = m.n, g = m.ng, ne = n + 2 * g;
+    const long nint = (long)n * n * n;
+    const long ncell = nint + nglist;
+    T *dst = out + (long)blockIdx.y * gbs;
+    const GuardPlan *pl = plan + (long)e.leaf * nglist;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < ncell; t += (long)gridDim.x * blockDim.x) {
+        double u[NV_DEV];
+        long idx;
+        if (t < nint) {
+            idx = ((t / ((long)n * n) + g) * ne + (t / n) % n + g) * ne + t % n + g;
+            const double *s = m.store + (long)b * m.bstride + t;
+#pragma unroll
+            for (int v = 0; v < NV_DEV; v++) u[v] = s[v * m.vstride];
+        } else {
+            const GuardPlan gp = pl[t - nint];
+            const unsigned kind = (gp.flags >> 4) & 3u;
+            if (kind == GS_PROL) continue;
+            idx = glist[t - nint];
+            if (kind == GS_NONE) {
+                atomicOr(m.err, ERR_AMR);
+#pragma unroll
+                for (int v = 0; v < NV_DEV; v++) u[v] = 0.;
+            } else {
+                guard_eval_same(m.store, m.vstride, gp.off, gp.flags & 7u, u);
+                if ((gp.flags >> 3) & 1u) eos_cell_dev(u, prm, gam1inv, ggprodinv);
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < NV_DEV; v++) dst[v * gvs + idx] = (T)u[v];
+    }
+}
+
+// prolonged guard cells of a batch from the plan's records
+template <class T>
+__global__ void __launch_bounds__(256, FXB_FILL_MINB) amr_prolong_kernel(MeshArgs m, const AmrEntry3 *entries,
+                                                                         const ProlRec *prol, const int *poff, T *out,
+                                                                         long gvs, long gbs, DevParams prm,
+                                                                         double gam1inv, double ggprodinv)
+{
+    const AmrEntry3 e = entries[blockIdx.y];
+    const int r0 = poff[e.leaf], r1 = poff[e.leaf + 1];
+    T *dst = out + (long)blockIdx.y * gbs;
+    for (int r = r0 + blockIdx.x * blockDim.x + threadIdx.x; r < r1; r += gridDim.x * blockDim.x) {
+        const uint4 *q = reinterpret_cast<const uint4 *>(prol + r);
+        const uint4 a = q[0], bq = q[1], c = q[2];
+        const long off[8] = {(long)a.z, (long)a.w, (long)bq.x, (long)bq.y, (long)bq.z, (long)bq.w, (long)c.x, (long)c.y};
+        const unsigned fl = a.y;
+        double u[NV_DEV];
+        guard_eval_prol(m.store, m.vstride, off, fl >> 8, fl & 7u, (fl >> 3) & 7u, u);
+        if ((fl >> 6) & 1u) eos_cell_dev(u, prm, gam1inv, ggprodinv);
+        const long idx = a.x;
+#pragma unroll
+        for (int v = 0; v < NV_DEV; v++) dst[v * gvs + idx] = (T)u[v];
     }
 }
 
@@ -687,9 +862,26 @@ void restrict_all(int which)
     }
 }
 
+template <class T> void fill_planned(const AmrEntry3 *entries, int cnt, int which)
+{
+    const dim3 g(S.fill_cta, cnt);
+    amr_copy_kernel<T><<<g, 256, 0, S.C.stream>>>(mesh_args(which), entries, S.leaf_blk_dev, (const GuardPlan *)S.d_plan,
+                                                  S.d_glist, S.nglist, (T *)S.gcb, ne3(), ne3() * NV_DEV, S.C.dprm,
+                                                  S.C.gam1inv, S.C.ggprodinv);
+    if (S.nprol)
+        amr_prolong_kernel<T><<<g, 256, 0, S.C.stream>>>(mesh_args(which), entries, (const ProlRec *)S.d_prol, S.d_poff,
+                                                         (T *)S.gcb, ne3(), ne3() * NV_DEV, S.C.dprm, S.C.gam1inv,
+                                                         S.C.ggprodinv);
+}
+
 void fill_batch(const AmrEntry3 *entries, int cnt, int which)
 {
     const dim3 g(S.fill_cta, cnt);
+    if (S.d_plan) {
+        if (S.C.prm.precision == FXB_MIXED) fill_planned<float>(entries, cnt, which);
+        else fill_planned<double>(entries, cnt, which);
+        return;
+    }
     if (S.C.prm.precision == FXB_MIXED)
         amr_fill_kernel<float, false><<<g, 256, 0, S.C.stream>>>(mesh_args(which), entries, S.leaf_blk_dev, S.d_eosmask,
                                                                 (float *)S.gcb, ne3(), ne3() * NV_DEV, 0, nullptr,
@@ -717,6 +909,7 @@ void amr_destroy()
     dfree(S.gcb); dfree(S.sig); dfree(S.slp); dfree(S.flat);
     for (int d = 0; d < 3; d++) { dfree(S.w[d]); dfree(S.f[d]); }
     dfree(S.bflux); dfree(S.stage); dfree(S.d_dmap); dfree(S.d_glist);
+    dfree(S.d_plan); dfree(S.d_prol); dfree(S.d_poff);
     S = State();
 }
 
@@ -830,6 +1023,27 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
         }
         S.nglist = (int)gl.size();
         CKA(up(S.d_glist, gl));
+    }
+    // guard-fill plan, when every store offset fits 32 bits
+    if ((unsigned long long)S.bstride * S.nblk < (1ull << 32) && S.nglist > 0) {
+        int *d_cnt = nullptr;
+        CKA(cudaMalloc(&S.d_plan, sizeof(GuardPlan) * (size_t)nleaf * S.nglist));
+        CKA(cudaMalloc(&d_cnt, sizeof(int) * (size_t)nleaf));
+        amr_plan_kernel<<<nleaf, 256, 0, st>>>(mesh_args(0), S.leaf_blk_dev, S.d_eosmask, S.d_glist, S.nglist,
+                                               (GuardPlan *)S.d_plan, d_cnt, nullptr, nullptr, 0);
+        CKA(cudaGetLastError());
+        std::vector<int> cnt(nleaf), poff(nleaf + 1, 0);
+        CKA(cudaMemcpyAsync(cnt.data(), d_cnt, sizeof(int) * (size_t)nleaf, cudaMemcpyDeviceToHost, st));
+        CKA(cudaStreamSynchronize(st));
+        cudaFree(d_cnt);
+        for (int l = 0; l < nleaf; l++) poff[l + 1] = poff[l] + cnt[l];
+        S.nprol = poff[nleaf];
+        CKA(up(S.d_poff, poff));
+        CKA(cudaMalloc(&S.d_prol, sizeof(ProlRec) * std::max<size_t>(1, (size_t)S.nprol)));
+        if (S.nprol)
+            amr_plan_kernel<<<nleaf, 256, 0, st>>>(mesh_args(0), S.leaf_blk_dev, S.d_eosmask, S.d_glist, S.nglist,
+                                                   nullptr, nullptr, (ProlRec *)S.d_prol, S.d_poff, 1);
+        CKA(cudaGetLastError());
     }
     const size_t r = rsize();
     S.nfc = (long)S.n * S.n;

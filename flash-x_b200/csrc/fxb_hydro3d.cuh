@@ -347,15 +347,16 @@ __global__ void __launch_bounds__(256) slope3d_kernel(const Args3D a, int d)
 // One instantiation per reconstruction order, so the register allocation of
 // the PPM path (three eigensystems and slopes) and of the WENO path (one
 // eigensystem, five projected cells) do not add up.  The minimum number of
-// resident 256-thread CTAs per SM bounds the registers per thread: two CTAs
-// (128 registers, a few hundred bytes of spills in FP64) measured 18 % faster
-// on B200 than one CTA with 244-255 registers, and three CTAs (80 registers)
-// lost again to spill traffic.
+// resident 256-thread CTAs per SM bounds the registers per thread.  FP64: two
+// CTAs (128 registers, a few hundred bytes of spills) measured 18 % faster on
+// B200 than one CTA with 244-255 registers, and three CTAs (80 registers)
+// lost again to spill traffic.  FP32: three CTAs (80 registers, ~140 bytes
+// of spills) measured 5-12 % faster than two.
 #ifndef FXB_S3_MINB_FP64
 #define FXB_S3_MINB_FP64 2
 #endif
 #ifndef FXB_S3_MINB_FP32
-#define FXB_S3_MINB_FP32 2
+#define FXB_S3_MINB_FP32 3
 #endif
 template <class R> struct MinB3D { static constexpr int value = sizeof(R) == 8 ? FXB_S3_MINB_FP64 : FXB_S3_MINB_FP32; };
 template <class R, int ORDER, bool AMR, int DIR>
@@ -502,8 +503,13 @@ __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
 }
 
 // ---- update, energyFix, Eos, CFL rate -------------------------------------------
+// three resident CTAs per SM (80 registers, ~140 bytes of spills) measured
+// 8-15 % faster on B200 than two (128 registers)
+#ifndef FXB_UPD_MINB
+#define FXB_UPD_MINB 3
+#endif
 template <class R, bool AMR>
-__global__ void __launch_bounds__(256) update3d_kernel(const Args3D a)
+__global__ void __launch_bounds__(256, FXB_UPD_MINB) update3d_kernel(const Args3D a)
 {
     const Ctx3<R, AMR> X(a);
     const Grid3 &G = X.G;
