@@ -600,11 +600,13 @@ __global__ void __launch_bounds__(256) amr_copy_kernel(MeshArgs m, const AmrEntr
     const long ncell = nint + nglist;
     T *dst = out + (long)blockIdx.y * gbs;
     const GuardPlan *pl = plan + (long)e.leaf * nglist;
-    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < ncell; t += (long)gridDim.x * blockDim.x) {
+    for (int t = (int)(blockIdx.x * blockDim.x + threadIdx.x); t < (int)ncell; t += (int)(gridDim.x * blockDim.x)) {
         double u[NV_DEV];
-        long idx;
+        int idx;
         if (t < nint) {
-            idx = ((t / ((long)n * n) + g) * ne + (t / n) % n + g) * ne + t % n + g;
+            int i, j, k;
+            unflatten(t, n, n, i, j, k);
+            idx = ((k + g) * ne + j + g) * ne + i + g;
             const double *s = m.store + (long)b * m.bstride + t;
 #pragma unroll
             for (int v = 0; v < NV_DEV; v++) u[v] = s[v * m.vstride];

@@ -391,6 +391,9 @@ extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, cons
         return fail(FXB_EUNSUPPORTED, "fxb_init: 2-D grid extents must be multiples of 16");
     if (d.ndim == 3 && (L.nx % T3X || L.ny % T3Y || L.nz % T3Z))
         return fail(FXB_EUNSUPPORTED, "fxb_init: 3-D grid extents must be multiples of the 3-D tile");
+    // the 3-D kernels walk padded boxes with 32-bit indices
+    if (d.ndim == 3 && (long)(L.nx + 4) * (L.ny + 4) * (L.nz + 4) >= (1L << 30))
+        return fail(FXB_EUNSUPPORTED, "fxb_init: 3-D grid larger than 2^30 cells");
     L.ncell = (long)L.nx * L.ny * L.nz;
     L.vstride = (L.ncell + 31) / 32 * 32;
     L.nblk = d.nblockx * (d.ndim >= 2 ? d.nblocky : 1) * (d.ndim == 3 ? d.nblockz : 1);

@@ -217,6 +217,17 @@ template <class R> __device__ __forceinline__ void unrot3(int dir, const R *r, R
 __device__ __forceinline__ void offs(int d, int o, int &di, int &dj, int &dk)
 { di = d == 0 ? o : 0; dj = d == 1 ? o : 0; dk = d == 2 ? o : 0; }
 
+// (i, j, k) of the linear index of an lx * ly * lz box, in 32-bit arithmetic:
+// every box a kernel walks holds fewer than 2^30 cells (checked by fxb_init)
+__device__ __forceinline__ void unflatten(unsigned idx, unsigned lx, unsigned ly, int &i, int &j, int &k)
+{
+    const unsigned q = idx / lx, r = q / ly;
+    i = (int)(idx - q * lx); j = (int)(q - r * ly); k = (int)r;
+}
+// grid-stride loop bounds of one launch in 32-bit arithmetic
+#define FXB_GRID_LOOP(idx, count) \
+    for (int idx = (int)(blockIdx.x * blockDim.x + threadIdx.x); idx < (int)(count); idx += (int)(gridDim.x * blockDim.x))
+
 // ---- sigma_d of every padded cell --------------------------------------------
 template <class R, bool AMR>
 __global__ void __launch_bounds__(256) sig3d_kernel(const Args3D a)
@@ -225,10 +236,10 @@ __global__ void __launch_bounds__(256) sig3d_kernel(const Args3D a)
     const Grid3 &G = X.G;
     R *sig = X.sig;
     const long np = G.npad();
-    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < np; idx += (long)gridDim.x * blockDim.x) {
-        int i = (int)(idx % (a.nx + 2)) - 1;
-        int j = (int)((idx / (a.nx + 2)) % (a.ny + 2)) - 1;
-        int k = (int)(idx / ((long)(a.nx + 2) * (a.ny + 2))) - 1;
+    FXB_GRID_LOOP(idx, np) {
+        int i, j, k;
+        unflatten(idx, a.nx + 2, a.ny + 2, i, j, k);
+        i -= 1; j -= 1; k -= 1;
         R vc[8];
         X.load(a, i, j, k, vc);
         R gc[6]; six(vc, gc);
@@ -260,10 +271,10 @@ __global__ void __launch_bounds__(256) flat3d_kernel(const Args3D a)
     const Ctx3<R, AMR> X(a);
     const Grid3 &G = X.G;
     const long np = G.npad();
-    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < np; idx += (long)gridDim.x * blockDim.x) {
-        int i = (int)(idx % (a.nx + 2)) - 1;
-        int j = (int)((idx / (a.nx + 2)) % (a.ny + 2)) - 1;
-        int k = (int)(idx / ((long)(a.nx + 2) * (a.ny + 2))) - 1;
+    FXB_GRID_LOOP(idx, np) {
+        int i, j, k;
+        unflatten(idx, a.nx + 2, a.ny + 2, i, j, k);
+        i -= 1; j -= 1; k -= 1;
         for (int d = 0; d < 3; d++) {
             int di, dj, dk;
             offs(d, 1, di, dj, dk);
@@ -325,8 +336,9 @@ __global__ void __launch_bounds__(256) slope3d_kernel(const Args3D a, int d)
     const int lx = a.nx + (d == 0 ? 4 : 0), ly = a.ny + (d == 1 ? 4 : 0);
     int di, dj, dk;
     offs(d, 1, di, dj, dk);
-    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < ns; idx += (long)gridDim.x * blockDim.x) {
-        int i = (int)(idx % lx), j = (int)((idx / lx) % ly), k = (int)(idx / ((long)lx * ly));
+    FXB_GRID_LOOP(idx, ns) {
+        int i, j, k;
+        unflatten(idx, lx, ly, i, j, k);
         if (d == 0) i -= 2; else if (d == 1) j -= 2; else k -= 2;
         R S8[3][8], S[3][6], g[6];
 #pragma unroll
@@ -372,8 +384,9 @@ __global__ void __launch_bounds__(256, MinB3D<R>::value) states3d_kernel(const A
     R *w = X.wst[d];
     const long nw = G.nw(d);
     const int lx = a.nx + (d == 0 ? 2 : 0), ly = a.ny + (d == 1 ? 2 : 0);
-    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < nw; idx += (long)gridDim.x * blockDim.x) {
-        int i = (int)(idx % lx), j = (int)((idx / lx) % ly), k = (int)(idx / ((long)lx * ly));
+    FXB_GRID_LOOP(idx, nw) {
+        int i, j, k;
+        unflatten(idx, lx, ly, i, j, k);
         if (d == 0) i -= 1; else if (d == 1) j -= 1; else k -= 1;
         int di, dj, dk;
         offs(d, 1, di, dj, dk);
@@ -485,8 +498,9 @@ __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
     R *f = X.flx[d];
     const long nf = G.nf(d), nw = G.nw(d);
     const int lx = a.nx + (d == 0 ? 1 : 0), ly = a.ny + (d == 1 ? 1 : 0);
-    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < nf; idx += (long)gridDim.x * blockDim.x) {
-        int i = (int)(idx % lx), j = (int)((idx / lx) % ly), k = (int)(idx / ((long)lx * ly));
+    FXB_GRID_LOOP(idx, nf) {
+        int i, j, k;
+        unflatten(idx, lx, ly, i, j, k);
         int di, dj, dk;
         offs(d, 1, di, dj, dk);
         long wl = G.widx(d, i - di, j - dj, k - dk), wr = G.widx(d, i, j, k);
@@ -521,8 +535,9 @@ __global__ void __launch_bounds__(256, FXB_UPD_MINB) update3d_kernel(const Args3
     double *out = AMR ? a.odata + (long)X.m.out_blk * a.o_bstride : a.out;
     const long ovs = AMR ? a.o_vstride : a.vstride;
     double rate = 0.;
-    for (long c = blockIdx.x * (long)blockDim.x + threadIdx.x; c < n; c += (long)gridDim.x * blockDim.x) {
-        int i = (int)(c % a.nx), j = (int)((c / a.nx) % a.ny), k = (int)(c / ((long)a.nx * a.ny));
+    FXB_GRID_LOOP(c, n) {
+        int i, j, k;
+        unflatten(c, a.nx, a.ny, i, j, k);
         // the update starts from the FP64 state: the grid, or the leaf's interior store
         const long vs = AMR ? a.o_vstride : X.svs;
         const double *in = AMR ? a.istore + (long)X.m.out_blk * a.o_bstride + c : X.src + X.cell(i, j, k);
