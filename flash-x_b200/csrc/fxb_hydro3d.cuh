@@ -32,6 +32,20 @@ struct AmrEntry3 {
 };
 enum { AMR_SKIP_UPDATE = 1 };
 
+// Division by a launch-invariant divisor d as a multiply-high, an add and a
+// shift (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994): with 2^s >= d and m = floor(2^32 (2^s - d) / d) + 1,
+// x / d = (umulhi(x, m) + x) >> s for every x below 2^31.
+struct FastDiv {
+    unsigned d, m, s;
+};
+inline FastDiv make_fastdiv(unsigned d)
+{
+    unsigned s = 0;
+    while ((1ull << s) < d) s++;
+    return FastDiv{d, (unsigned)((((1ull << 32) * ((1ull << s) - d)) / d) + 1), s};
+}
+
 struct Args3D {
     const double *in;
     double *out;
@@ -63,7 +77,15 @@ struct Args3D {
     long o_vstride, o_bstride;
     long sig_bstride, w_bstride[3], f_bstride[3];   // elements of R per batch entry
     int cta[4];                 // CTAs per batch entry: sig3d, states3d, flux3d, update3d
+    FastDiv fdx[5], fdy[5];     // divisors nx + e and ny + e (e = 0, 1, 2, 4), set by the launchers
 };
+// the launchers' copy of the arguments with the index divisors filled in
+inline Args3D with_divisors(const Args3D &a)
+{
+    Args3D b = a;
+    for (int e = 0; e <= 4; e++) { b.fdx[e] = make_fastdiv((unsigned)a.nx + e); b.fdy[e] = make_fastdiv((unsigned)a.ny + e); }
+    return b;
+}
 enum { AMR_SIG = 1, AMR_STATES = 2, AMR_FLUX = 4 };
 
 // 3-D tile extents accepted by fxb_init (the unfused kernels take any size)
@@ -224,6 +246,12 @@ __device__ __forceinline__ void unflatten(unsigned idx, unsigned lx, unsigned ly
     const unsigned q = idx / lx, r = q / ly;
     i = (int)(idx - q * lx); j = (int)(q - r * ly); k = (int)r;
 }
+__device__ __forceinline__ unsigned fast_div(unsigned x, const FastDiv &f) { return (__umulhi(x, f.m) + x) >> f.s; }
+__device__ __forceinline__ void unflatten(unsigned idx, const FastDiv &fx, const FastDiv &fy, int &i, int &j, int &k)
+{
+    const unsigned q = fast_div(idx, fx), r = fast_div(q, fy);
+    i = (int)(idx - q * fx.d); j = (int)(q - r * fy.d); k = (int)r;
+}
 // grid-stride loop bounds of one launch in 32-bit arithmetic
 #define FXB_GRID_LOOP(idx, count) \
     for (int idx = (int)(blockIdx.x * blockDim.x + threadIdx.x); idx < (int)(count); idx += (int)(gridDim.x * blockDim.x))
@@ -238,7 +266,7 @@ __global__ void __launch_bounds__(256) sig3d_kernel(const Args3D a)
     const long np = G.npad();
     FXB_GRID_LOOP(idx, np) {
         int i, j, k;
-        unflatten(idx, a.nx + 2, a.ny + 2, i, j, k);
+        unflatten(idx, a.fdx[2], a.fdy[2], i, j, k);
         i -= 1; j -= 1; k -= 1;
         R vc[8];
         X.load(a, i, j, k, vc);
@@ -273,7 +301,7 @@ __global__ void __launch_bounds__(256) flat3d_kernel(const Args3D a)
     const long np = G.npad();
     FXB_GRID_LOOP(idx, np) {
         int i, j, k;
-        unflatten(idx, a.nx + 2, a.ny + 2, i, j, k);
+        unflatten(idx, a.fdx[2], a.fdy[2], i, j, k);
         i -= 1; j -= 1; k -= 1;
         for (int d = 0; d < 3; d++) {
             int di, dj, dk;
@@ -333,12 +361,11 @@ __global__ void __launch_bounds__(256) slope3d_kernel(const Args3D a, int d)
     const Ctx3<R, AMR> X(a);
     const Grid3 &G = X.G;
     const long ns = G.ns(d);
-    const int lx = a.nx + (d == 0 ? 4 : 0), ly = a.ny + (d == 1 ? 4 : 0);
     int di, dj, dk;
     offs(d, 1, di, dj, dk);
     FXB_GRID_LOOP(idx, ns) {
         int i, j, k;
-        unflatten(idx, lx, ly, i, j, k);
+        unflatten(idx, a.fdx[d == 0 ? 4 : 0], a.fdy[d == 1 ? 4 : 0], i, j, k);
         if (d == 0) i -= 2; else if (d == 1) j -= 2; else k -= 2;
         R S8[3][8], S[3][6], g[6];
 #pragma unroll
@@ -383,10 +410,9 @@ __global__ void __launch_bounds__(256, MinB3D<R>::value) states3d_kernel(const A
     const R hdtx = R(0.5 * dt / X.dx), hdty = R(0.5 * dt / X.dy), hdtz = R(0.5 * dt / X.dz);
     R *w = X.wst[d];
     const long nw = G.nw(d);
-    const int lx = a.nx + (d == 0 ? 2 : 0), ly = a.ny + (d == 1 ? 2 : 0);
     FXB_GRID_LOOP(idx, nw) {
         int i, j, k;
-        unflatten(idx, lx, ly, i, j, k);
+        unflatten(idx, a.fdx[d == 0 ? 2 : 0], a.fdy[d == 1 ? 2 : 0], i, j, k);
         if (d == 0) i -= 1; else if (d == 1) j -= 1; else k -= 1;
         int di, dj, dk;
         offs(d, 1, di, dj, dk);
@@ -497,10 +523,9 @@ __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
     const R *w = X.wst[d];
     R *f = X.flx[d];
     const long nf = G.nf(d), nw = G.nw(d);
-    const int lx = a.nx + (d == 0 ? 1 : 0), ly = a.ny + (d == 1 ? 1 : 0);
     FXB_GRID_LOOP(idx, nf) {
         int i, j, k;
-        unflatten(idx, lx, ly, i, j, k);
+        unflatten(idx, a.fdx[d == 0 ? 1 : 0], a.fdy[d == 1 ? 1 : 0], i, j, k);
         int di, dj, dk;
         offs(d, 1, di, dj, dk);
         long wl = G.widx(d, i - di, j - dj, k - dk), wr = G.widx(d, i, j, k);
@@ -517,10 +542,10 @@ __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
 }
 
 // ---- update, energyFix, Eos, CFL rate -------------------------------------------
-// three resident CTAs per SM (80 registers, ~140 bytes of spills) measured
-// 8-15 % faster on B200 than two (128 registers)
+// four resident CTAs per SM (64 registers, ~200 bytes of spills) measured
+// faster on B200 than three (80 registers) and 10-20 % faster than two (128)
 #ifndef FXB_UPD_MINB
-#define FXB_UPD_MINB 3
+#define FXB_UPD_MINB 4
 #endif
 template <class R, bool AMR>
 __global__ void __launch_bounds__(256, FXB_UPD_MINB) update3d_kernel(const Args3D a)
@@ -537,7 +562,7 @@ __global__ void __launch_bounds__(256, FXB_UPD_MINB) update3d_kernel(const Args3
     double rate = 0.;
     FXB_GRID_LOOP(c, n) {
         int i, j, k;
-        unflatten(c, a.nx, a.ny, i, j, k);
+        unflatten(c, a.fdx[0], a.fdy[0], i, j, k);
         // the update starts from the FP64 state: the grid, or the leaf's interior store
         const long vs = AMR ? a.o_vstride : X.svs;
         const double *in = AMR ? a.istore + (long)X.m.out_blk * a.o_bstride + c : X.src + X.cell(i, j, k);
@@ -653,8 +678,9 @@ template <class R, bool AMR, int DIR> void launch_states3d(const Args3D &a, dim3
     }
 }
 
-template <class R> void launch_hydro3d_t(const Args3D &a, cudaStream_t s)
+template <class R> void launch_hydro3d_t(const Args3D &a0, cudaStream_t s)
 {
+    const Args3D a = with_divisors(a0);
     const int nb = 148 * 8;
     if (a.prm.flattening) flat3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
     sig3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
@@ -733,8 +759,9 @@ __global__ void __launch_bounds__(256) amr_correct_flux_kernel(const Args3D a, c
 
 // The 3-D pipeline over one AMR batch of `entries` guard-filled blocks; `which`
 // selects the stages (AMR_SIG | AMR_STATES | AMR_FLUX), a.cta[] the CTAs per block.
-template <class R> void launch_amr3d_fluxes_t(const Args3D &a, int entries, int which, cudaStream_t s)
+template <class R> void launch_amr3d_fluxes_t(const Args3D &a0, int entries, int which, cudaStream_t s)
 {
+    const Args3D a = with_divisors(a0);
     if ((which & AMR_SIG) && a.prm.flattening) flat3d_kernel<R, true><<<dim3(a.cta[0], entries), 256, 0, s>>>(a);
     if (which & AMR_SIG) sig3d_kernel<R, true><<<dim3(a.cta[0], entries), 256, 0, s>>>(a);
     if (which & AMR_STATES) {
@@ -757,8 +784,9 @@ template <class R> void launch_amr3d_correct_t(const Args3D &a, int entries, con
 {
     amr_correct_flux_kernel<R><<<dim3(2, entries), 256, 0, s>>>(a, (const R *)bflux, nfc, fine, finer_mask);
 }
-template <class R> void launch_amr3d_update_t(const Args3D &a, int entries, cudaStream_t s)
+template <class R> void launch_amr3d_update_t(const Args3D &a0, int entries, cudaStream_t s)
 {
+    const Args3D a = with_divisors(a0);
     update3d_kernel<R, true><<<dim3(a.cta[3], entries), 256, 0, s>>>(a);
 }
 
