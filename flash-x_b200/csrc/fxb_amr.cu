@@ -62,7 +62,10 @@ struct MeshArgs {
     int *err;
 };
 
-constexpr int ERR_AMR = 16;     // guard cell without a covering block (device error word)
+constexpr int ERR_AMR = 16;
+// variables of the guard-filled blocks: D..EI, all the 3-D pipeline reads
+// (ENER feeds the guard cells' Eos, TEMP nothing)
+constexpr int NV_GCB = EI + 1;     // guard cell without a covering block (device error word)
 
 struct State {
     bool active = false;
@@ -99,6 +102,8 @@ struct State {
     void *d_prol = nullptr;                       // ProlRec, per leaf from d_poff[leaf]
     int *d_poff = nullptr;
     long nprol = 0;
+    int2 *d_rlist = nullptr;                      // parent cells the plan needs, per level (restriction order)
+    std::vector<long> rlist_off;                  // per level offset into d_rlist, size maxlev + 1
     int cta[4] = {4, 4, 4, 4};                    // CTAs per block: sig, states, flux, update
     int fill_cta = 8;
     char tune_log[256] = "";
@@ -390,13 +395,14 @@ __device__ __forceinline__ void guard_resolve(const MeshArgs &m, int b, const in
     gs.kind = GS_PROL;
 }
 
-// same-level guard value: the cell's variables, velocities flipped at reflecting boundaries
+// same-level guard value: the cell's first NV variables, velocities flipped at reflecting boundaries
+template <int NV = NV_DEV>
 __device__ __forceinline__ void guard_eval_same(const double *store, long vstride, long off, unsigned own,
                                                 double out[NV_DEV])
 {
     const double *s = store + off;
 #pragma unroll
-    for (int v = 0; v < NV_DEV; v++) out[v] = s[v * vstride];
+    for (int v = 0; v < NV; v++) out[v] = s[v * vstride];
 #pragma unroll
     for (int a = 0; a < 3; a++)
         if ((own >> a) & 1u) out[VX + a] = out[VX + a] * -1.;
@@ -502,7 +508,7 @@ __global__ void __launch_bounds__(256, FXB_FILL_MINB) amr_fill_kernel(MeshArgs m
             for (int v = 0; v < NV_DEV; v++) dst[idx * nunk + dmap[v]] = (T)u[v];
         } else {
 #pragma unroll
-            for (int v = 0; v < NV_DEV; v++) dst[v * gvs + idx] = (T)u[v];
+            for (int v = 0; v < NV_GCB; v++) dst[v * gvs + idx] = (T)u[v];
         }
     }
 }
@@ -609,7 +615,7 @@ __global__ void __launch_bounds__(256) amr_copy_kernel(MeshArgs m, const AmrEntr
             idx = ((k + g) * ne + j + g) * ne + i + g;
             const double *s = m.store + (long)b * m.bstride + t;
 #pragma unroll
-            for (int v = 0; v < NV_DEV; v++) u[v] = s[v * m.vstride];
+            for (int v = 0; v < NV_GCB; v++) u[v] = s[v * m.vstride];
         } else {
             const GuardPlan gp = pl[t - nint];
             const unsigned kind = (gp.flags >> 4) & 3u;
@@ -619,13 +625,15 @@ __global__ void __launch_bounds__(256) amr_copy_kernel(MeshArgs m, const AmrEntr
                 atomicOr(m.err, ERR_AMR);
 #pragma unroll
                 for (int v = 0; v < NV_DEV; v++) u[v] = 0.;
+            } else if ((gp.flags >> 3) & 1u) {
+                guard_eval_same<NV_DEV>(m.store, m.vstride, gp.off, gp.flags & 7u, u);
+                eos_cell_dev(u, prm, gam1inv, ggprodinv);
             } else {
-                guard_eval_same(m.store, m.vstride, gp.off, gp.flags & 7u, u);
-                if ((gp.flags >> 3) & 1u) eos_cell_dev(u, prm, gam1inv, ggprodinv);
+                guard_eval_same<NV_GCB>(m.store, m.vstride, gp.off, gp.flags & 7u, u);
             }
         }
 #pragma unroll
-        for (int v = 0; v < NV_DEV; v++) dst[v * gvs + idx] = (T)u[v];
+        for (int v = 0; v < NV_GCB; v++) dst[v * gvs + idx] = (T)u[v];
     }
 }
 
@@ -649,43 +657,75 @@ __global__ void __launch_bounds__(256, FXB_FILL_MINB) amr_prolong_kernel(MeshArg
         if ((fl >> 6) & 1u) eos_cell_dev(u, prm, gam1inv, ggprodinv);
         const long idx = a.x;
 #pragma unroll
-        for (int v = 0; v < NV_DEV; v++) dst[v * gvs + idx] = (T)u[v];
+        for (int v = 0; v < NV_GCB; v++) dst[v * gvs + idx] = (T)u[v];
     }
 }
 
-// restriction of the parents of one level (amr_restrict_unk_genorder, order 1)
+// restriction of parent cell c of block p from its eight children cells
+// (amr_restrict_unk_genorder, order 1): conserved form, weights 1/8 in k, j, i order
+__device__ __forceinline__ void restrict_cell(double *store, long vstride, long bstride, int n, int p, int c,
+                                              const int *child)
+{
+    const int h = n / 2;
+    const int pi = c % n, pj = (c / n) % n, pk = c / (n * n);
+    const int q = (pi >= h) | ((pj >= h) << 1) | ((pk >= h) << 2);
+    const int ch = child[(long)p * 8 + q];
+    const int i0 = 2 * (pi - (q & 1) * h), j0 = 2 * (pj - ((q >> 1) & 1) * h), k0 = 2 * (pk - ((q >> 2) & 1) * h);
+    const double *cs = store + (long)ch * bstride;
+    double s[NV_DEV];
+#pragma unroll
+    for (int v = 0; v < NV_DEV; v++) s[v] = 0.;
+    const double w = 0.5 * 0.5 * 0.5;
+    for (int kk = 0; kk < 2; kk++) for (int jj = 0; jj < 2; jj++) for (int ii = 0; ii < 2; ii++) {
+        const long cc = ((long)(k0 + kk) * n + (j0 + jj)) * n + (i0 + ii);
+        const double dens = cs[D * vstride + cc];
+#pragma unroll
+        for (int v = 0; v < NV_DEV; v++) {
+            double x = cs[v * vstride + cc];
+            if (per_mass(v)) x = dens * x;
+            s[v] = s[v] + w * x;
+        }
+    }
+    double dinv = s[D] == 0.0 ? 0.0 : 1. / s[D];
+    double *ps = store + (long)p * bstride + c;
+#pragma unroll
+    for (int v = 0; v < NV_DEV; v++) ps[v * vstride] = per_mass(v) ? dinv * s[v] : s[v];
+}
+
+// every cell of the parents of one level
 __global__ void __launch_bounds__(256) amr_restrict_kernel(double *store, long vstride, long bstride, int n,
                                                            const int *plist, int np, const int *child)
 {
     const long per = (long)n * n * n;
-    const int h = n / 2;
-    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)np * per; idx += (long)gridDim.x * blockDim.x) {
-        const int p = plist[idx / per];
-        const long c = idx % per;
-        const int pi = (int)(c % n), pj = (int)((c / n) % n), pk = (int)(c / ((long)n * n));
-        const int q = (pi >= h) | ((pj >= h) << 1) | ((pk >= h) << 2);
-        const int ch = child[(long)p * 8 + q];
-        const int i0 = 2 * (pi - (q & 1) * h), j0 = 2 * (pj - ((q >> 1) & 1) * h), k0 = 2 * (pk - ((q >> 2) & 1) * h);
-        const double *cs = store + (long)ch * bstride;
-        double s[NV_DEV];
-#pragma unroll
-        for (int v = 0; v < NV_DEV; v++) s[v] = 0.;
-        const double w = 0.5 * 0.5 * 0.5;
-        for (int kk = 0; kk < 2; kk++) for (int jj = 0; jj < 2; jj++) for (int ii = 0; ii < 2; ii++) {
-            const long cc = ((long)(k0 + kk) * n + (j0 + jj)) * n + (i0 + ii);
-            const double dens = cs[D * vstride + cc];
-#pragma unroll
-            for (int v = 0; v < NV_DEV; v++) {
-                double x = cs[v * vstride + cc];
-                if (per_mass(v)) x = dens * x;
-                s[v] = s[v] + w * x;
-            }
-        }
-        double dinv = s[D] == 0.0 ? 0.0 : 1. / s[D];
-        double *ps = store + (long)p * bstride + c;
-#pragma unroll
-        for (int v = 0; v < NV_DEV; v++) ps[v * vstride] = per_mass(v) ? dinv * s[v] : s[v];
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)np * per; idx += (long)gridDim.x * blockDim.x)
+        restrict_cell(store, vstride, bstride, n, plist[idx / per], (int)(idx % per), child);
+}
+
+// the listed (parent, cell) pairs of one level
+__global__ void __launch_bounds__(256) amr_restrict_list_kernel(double *store, long vstride, long bstride, int n,
+                                                                const int2 *list, int cnt, const int *child)
+{
+    for (int t = (int)(blockIdx.x * blockDim.x + threadIdx.x); t < cnt; t += (int)(gridDim.x * blockDim.x)) {
+        const int2 pc = list[t];
+        restrict_cell(store, vstride, bstride, n, pc.x, pc.y, child);
     }
+}
+
+// parent-block cells the guard-fill plan reads (same-level copies and prolongation stencils)
+__global__ void __launch_bounds__(256) amr_need_kernel(const GuardPlan *plan, long nplan, const ProlRec *prol, long nprol,
+                                                       long vstride, long bstride, unsigned char *need)
+{
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nplan; t += stride) {
+        const GuardPlan gp = plan[t];
+        if (((gp.flags >> 4) & 3u) == GS_SAME) need[(gp.off / bstride) * vstride + gp.off % bstride] = 1;
+    }
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nprol; t += stride)
+#pragma unroll
+        for (int s8 = 0; s8 < 8; s8++) {
+            const unsigned off = prol[t].off[s8];
+            need[(off / bstride) * vstride + off % bstride] = 1;
+        }
 }
 
 // UNK staging (leaf, k, j, i, var with guard cells) <-> interior store / guard-filled blocks
@@ -836,7 +876,7 @@ Args3D batch_args(const double *dtv, double dt)
     a.slp = S.slp;
     a.flat = S.flat;
     for (int d = 0; d < 3; d++) { a.wst[d] = S.w[d]; a.flx[d] = S.f[d]; }
-    a.gcb = S.gcb; a.gcb_vstride = ne3(); a.gcb_bstride = ne3() * NV_DEV; a.ng = S.ng;
+    a.gcb = S.gcb; a.gcb_vstride = ne3(); a.gcb_bstride = ne3() * NV_GCB; a.ng = S.ng;
     a.istore = S.store[S.cur];
     a.dxl = S.d_dxl;
     for (int q = 0; q < 4; q++) a.cta[q] = S.cta[q];
@@ -868,32 +908,51 @@ template <class T> void fill_planned(const AmrEntry3 *entries, int cnt, int whic
 {
     const dim3 g(S.fill_cta, cnt);
     amr_copy_kernel<T><<<g, 256, 0, S.C.stream>>>(mesh_args(which), entries, S.leaf_blk_dev, (const GuardPlan *)S.d_plan,
-                                                  S.d_glist, S.nglist, (T *)S.gcb, ne3(), ne3() * NV_DEV, S.C.dprm,
+                                                  S.d_glist, S.nglist, (T *)S.gcb, ne3(), ne3() * NV_GCB, S.C.dprm,
                                                   S.C.gam1inv, S.C.ggprodinv);
     if (S.nprol)
         amr_prolong_kernel<T><<<g, 256, 0, S.C.stream>>>(mesh_args(which), entries, (const ProlRec *)S.d_prol, S.d_poff,
-                                                         (T *)S.gcb, ne3(), ne3() * NV_DEV, S.C.dprm, S.C.gam1inv,
+                                                         (T *)S.gcb, ne3(), ne3() * NV_GCB, S.C.dprm, S.C.gam1inv,
                                                          S.C.ggprodinv);
 }
 
-void fill_batch(const AmrEntry3 *entries, int cnt, int which)
+// restriction of only the parent cells the guard-fill plan reads (every cell
+// without a plan); returns the number of launches
+int restrict_needed(int which)
+{
+    if (!S.d_rlist) { restrict_all(which); return S.maxlev - 1; }
+    int nl = 0;
+    for (int lev = S.maxlev - 1; lev >= 1; lev--) {
+        const long cnt = S.rlist_off[lev + 1] - S.rlist_off[lev];
+        if (!cnt) continue;
+        nl++;
+        int grid = (int)std::min<long>((cnt + 255) / 256, 148L * 16);
+        amr_restrict_list_kernel<<<grid, 256, 0, S.C.stream>>>(S.store[which], S.vstride, S.bstride, S.n,
+                                                               S.d_rlist + S.rlist_off[lev], (int)cnt, S.d_child);
+    }
+    return nl;
+}
+
+// guard fill of one batch; returns the number of launches
+int fill_batch(const AmrEntry3 *entries, int cnt, int which)
 {
     const dim3 g(S.fill_cta, cnt);
     if (S.d_plan) {
         if (S.C.prm.precision == FXB_MIXED) fill_planned<float>(entries, cnt, which);
         else fill_planned<double>(entries, cnt, which);
-        return;
+        return S.nprol ? 2 : 1;
     }
     if (S.C.prm.precision == FXB_MIXED)
         amr_fill_kernel<float, false><<<g, 256, 0, S.C.stream>>>(mesh_args(which), entries, S.leaf_blk_dev, S.d_eosmask,
-                                                                (float *)S.gcb, ne3(), ne3() * NV_DEV, 0, nullptr,
+                                                                (float *)S.gcb, ne3(), ne3() * NV_GCB, 0, nullptr,
                                                                 S.d_glist, S.nglist, S.C.dprm, S.C.gam1inv,
                                                                 S.C.ggprodinv);
     else
         amr_fill_kernel<double, false><<<g, 256, 0, S.C.stream>>>(mesh_args(which), entries, S.leaf_blk_dev, S.d_eosmask,
-                                                                 (double *)S.gcb, ne3(), ne3() * NV_DEV, 0, nullptr,
+                                                                 (double *)S.gcb, ne3(), ne3() * NV_GCB, 0, nullptr,
                                                                  S.d_glist, S.nglist, S.C.dprm, S.C.gam1inv,
                                                                  S.C.ggprodinv);
+    return 1;
 }
 
 } // namespace
@@ -911,7 +970,7 @@ void amr_destroy()
     dfree(S.gcb); dfree(S.sig); dfree(S.slp); dfree(S.flat);
     for (int d = 0; d < 3; d++) { dfree(S.w[d]); dfree(S.f[d]); }
     dfree(S.bflux); dfree(S.stage); dfree(S.d_dmap); dfree(S.d_glist);
-    dfree(S.d_plan); dfree(S.d_prol); dfree(S.d_poff);
+    dfree(S.d_plan); dfree(S.d_prol); dfree(S.d_poff); dfree(S.d_rlist);
     S = State();
 }
 
@@ -1046,6 +1105,45 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
             amr_plan_kernel<<<nleaf, 256, 0, st>>>(mesh_args(0), S.leaf_blk_dev, S.d_eosmask, S.d_glist, S.nglist,
                                                    nullptr, nullptr, (ProlRec *)S.d_prol, S.d_poff, 1);
         CKA(cudaGetLastError());
+        // parent cells the plan reads, and below them the parent cells their
+        // restriction reads (coarse to fine); listed per level for the step
+        const size_t ncb = (size_t)S.nblk * S.vstride;
+        unsigned char *d_need = nullptr;
+        CKA(cudaMalloc(&d_need, ncb));
+        CKA(cudaMemsetAsync(d_need, 0, ncb, st));
+        const long nplan = (long)nleaf * S.nglist;
+        const int grid = (int)std::min<long>((std::max(nplan, S.nprol) + 255) / 256, 148L * 16);
+        amr_need_kernel<<<grid, 256, 0, st>>>((const GuardPlan *)S.d_plan, nplan, (const ProlRec *)S.d_prol, S.nprol,
+                                               S.vstride, S.bstride, d_need);
+        CKA(cudaGetLastError());
+        std::vector<unsigned char> need(ncb);
+        CKA(cudaMemcpyAsync(need.data(), d_need, ncb, cudaMemcpyDeviceToHost, st));
+        CKA(cudaStreamSynchronize(st));
+        cudaFree(d_need);
+        const int n = S.n, h = n / 2;
+        for (int lev = 1; lev < S.maxlev; lev++)
+            for (int p : S.parents_at[lev])
+                for (int cidx = 0; cidx < S.vstride; cidx++) {
+                    if (!need[(size_t)p * S.vstride + cidx]) continue;
+                    const int pi = cidx % n, pj = (cidx / n) % n, pk = cidx / (n * n);
+                    const int q = (pi >= h) | ((pj >= h) << 1) | ((pk >= h) << 2);
+                    const int ch = S.blk[p].child[q];
+                    if (S.blk[ch].leaf >= 0) continue;
+                    const int i0 = 2 * (pi - (q & 1) * h), j0 = 2 * (pj - ((q >> 1) & 1) * h),
+                              k0 = 2 * (pk - ((q >> 2) & 1) * h);
+                    for (int kk = 0; kk < 2; kk++) for (int jj = 0; jj < 2; jj++) for (int ii = 0; ii < 2; ii++)
+                        need[(size_t)ch * S.vstride + ((k0 + kk) * n + (j0 + jj)) * n + (i0 + ii)] = 1;
+                }
+        std::vector<int2> rl;
+        S.rlist_off.assign(S.maxlev + 1, 0);
+        for (int lev = 1; lev <= S.maxlev; lev++) {
+            S.rlist_off[lev] = (long)rl.size();
+            if (lev == S.maxlev) break;
+            for (int p : S.parents_at[lev])
+                for (int cidx = 0; cidx < S.vstride; cidx++)
+                    if (need[(size_t)p * S.vstride + cidx]) rl.push_back(make_int2(p, cidx));
+        }
+        CKA(up(S.d_rlist, rl));
     }
     const size_t r = rsize();
     S.nfc = (long)S.n * S.n;
@@ -1055,7 +1153,7 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     S.stage_leaves = (int)std::max<size_t>(1, std::min<size_t>(nleaf, (1ull << 30) / per_unk));
     CKA(cudaMalloc(&S.stage, per_unk * S.stage_leaves));
     // batch of guard-filled blocks + pipeline intermediates: up to 60 % of what is free
-    const size_t per_entry = r * NV_DEV * ne3() + sig3d_bytes(S.n, S.n, S.n, r) +
+    const size_t per_entry = r * NV_GCB * ne3() + sig3d_bytes(S.n, S.n, S.n, r) +
                              w3d_bytes(0, S.n, S.n, S.n, r) + w3d_bytes(1, S.n, S.n, S.n, r) + w3d_bytes(2, S.n, S.n, S.n, r) +
                              f3d_bytes(0, S.n, S.n, S.n, r) + f3d_bytes(1, S.n, S.n, S.n, r) + f3d_bytes(2, S.n, S.n, S.n, r) +
                              (c.prm.order == 3 ? slp3d_bytes(S.n, S.n, S.n, r) : 0) +
@@ -1071,7 +1169,7 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
         long mb = atol(ev);
         if (mb >= 1) S.batch = (int)std::min<long>(S.batch, mb);
     }
-    CKA(cudaMalloc(&S.gcb, r * NV_DEV * ne3() * S.batch));
+    CKA(cudaMalloc(&S.gcb, r * NV_GCB * ne3() * S.batch));
     CKA(cudaMalloc(&S.sig, sig3d_bytes(S.n, S.n, S.n, r) * S.batch));
     if (c.prm.order == 3) CKA(cudaMalloc(&S.slp, slp3d_bytes(S.n, S.n, S.n, r) * S.batch));
     if (c.prm.flattening) CKA(cudaMalloc(&S.flat, r * 3 * (size_t)(S.n + 2) * (S.n + 2) * (S.n + 2) * S.batch));
@@ -1187,8 +1285,7 @@ int amr_step(const double *dtv, double dt, int *launches)
 {
     const bool mixed = S.C.prm.precision == FXB_MIXED;
     int nl = 0;
-    restrict_all(S.cur);
-    nl += S.maxlev - 1;
+    nl += restrict_needed(S.cur);
     Args3D a = batch_args(dtv, dt);
     auto fluxes = [&](int cnt) {
         const int all = AMR_SIG | AMR_STATES | AMR_FLUX;
@@ -1206,25 +1303,27 @@ int amr_step(const double *dtv, double dt, int *launches)
     auto update = [&](int cnt) {
         if (mixed) launch_amr3d_update_mixed(a, cnt, S.C.stream); else launch_amr3d_update_fp64(a, cnt, S.C.stream);
     };
+    // sigma (+ flattening), slopes and states (PPM) or states (WENO5) of three directions, three fluxes
+    const int pipe = 1 + (S.C.prm.flattening ? 1 : 0) + (S.C.prm.order == 3 ? 6 : 3) + 3;
     if (S.nleaf <= S.batch) {
         a.batch = S.d_entries;
-        fill_batch(a.batch, S.nleaf, S.cur);
+        nl += fill_batch(a.batch, S.nleaf, S.cur);
         fluxes(S.nleaf); emit(S.nleaf); correct(S.nleaf); update(S.nleaf);
-        nl += 11 + (S.C.prm.order == 3 ? 3 : 0);
+        nl += pipe + 3;
     } else {
         for (int l0 = 0; l0 < S.nleaf; l0 += S.batch) {
             int cnt = std::min(S.batch, S.nleaf - l0);
             a.batch = S.d_entries + S.nleaf + l0;
-            fill_batch(a.batch, cnt, S.cur);
+            nl += fill_batch(a.batch, cnt, S.cur);
             fluxes(cnt); emit(cnt); update(cnt);
-            nl += 10 + (S.C.prm.order == 3 ? 3 : 0);
+            nl += pipe + 2;
         }
         for (int l0 = 0; l0 < S.nfiner; l0 += S.batch) {
             int cnt = std::min(S.batch, S.nfiner - l0);
             a.batch = S.d_entries + 2 * S.nleaf + l0;
-            fill_batch(a.batch, cnt, S.cur);
+            nl += fill_batch(a.batch, cnt, S.cur);
             fluxes(cnt); correct(cnt); update(cnt);
-            nl += 10 + (S.C.prm.order == 3 ? 3 : 0);
+            nl += pipe + 2;
         }
     }
     CKA(cudaGetLastError());
