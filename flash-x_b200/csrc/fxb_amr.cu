@@ -104,7 +104,7 @@ struct State {
     long nprol = 0;
     int2 *d_rlist = nullptr;                      // parent cells the plan needs, per level (restriction order)
     std::vector<long> rlist_off;                  // per level offset into d_rlist, size maxlev + 1
-    int cta[4] = {4, 4, 4, 4};                    // CTAs per block: sig, states, flux, update
+    int cta[4] = {4, 4, 4, 4};                    // CTAs per block: sig, slopes, (unused), update
     int fill_cta = 8;
     char tune_log[256] = "";
     std::unordered_map<uint64_t, int> map;
@@ -1183,60 +1183,65 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     return FXB_OK;
 }
 
-// Launch-shape search on the attached state: every stage of one batch is
-// timed with 1, 2, 4, 8 and 16 CTAs per block (one warm-up pass, one timed
-// pass each) and the fastest count per stage is kept.  The stages compute
-// cells independently, so the choice changes timings, never results.  The
-// update writes the other interior store, which the next step overwrites.
+// Launch-shape search on the attached state: the guard fill, sigma, the PPM
+// slopes and the update are timed with 1, 2, 4, 8 and 16 CTAs per block (one
+// warm-up pass, one timed pass each) and the fastest count per stage is kept
+// (the face-state and flux kernel has fixed tiles and is timed with the
+// slopes).  The stages compute cells independently, so the choice changes
+// timings, never results.  The update writes the other interior store, which
+// the next step overwrites.
 int amr_tune()
 {
     const char *ev = getenv("FXB_AMR_TUNE");
     if (ev && atoi(ev) == 0) {
-        snprintf(S.tune_log, sizeof(S.tune_log), "AMR launch shape (CTAs per block): fill=%d sig=%d states=%d flux=%d "
-                 "update=%d, defaults (tuning off)", S.fill_cta, S.cta[0], S.cta[1], S.cta[2], S.cta[3]);
+        snprintf(S.tune_log, sizeof(S.tune_log), "AMR launch shape (CTAs per block): fill=%d sig=%d slopes=%d "
+                 "update=%d, defaults (tuning off)", S.fill_cta, S.cta[0], S.cta[1], S.cta[3]);
         return FXB_OK;
     }
     const bool mixed = S.C.prm.precision == FXB_MIXED;
     const int cand[5] = {1, 2, 4, 8, 16};
     const int cnt = std::min(S.nleaf, S.batch);
-    cudaEvent_t e[6];
-    for (int i = 0; i < 6; i++) CKA(cudaEventCreate(&e[i]));
-    float best[5] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
-    int pick[5] = {S.fill_cta, S.cta[0], S.cta[1], S.cta[2], S.cta[3]};
+    cudaEvent_t e[5];
+    for (int i = 0; i < 5; i++) CKA(cudaEventCreate(&e[i]));
+    float best[4] = {1e30f, 1e30f, 1e30f, 1e30f};
+    int pick[4] = {S.fill_cta, S.cta[0], S.cta[1], S.cta[3]};
     restrict_all(S.cur);
     for (int c : cand) {
         S.fill_cta = c;
         for (int q = 0; q < 4; q++) S.cta[q] = c;
         Args3D a = batch_args(nullptr, 0.0);
         a.batch = S.d_entries;
-        float t[5] = {0, 0, 0, 0, 0};
+        float t[4] = {0, 0, 0, 0};
         for (int rep = 0; rep < 2; rep++) {
             CKA(cudaEventRecord(e[0], S.C.stream));
             fill_batch(a.batch, cnt, S.cur);
             CKA(cudaEventRecord(e[1], S.C.stream));
-            for (int st = 0; st < 3; st++) {
+            for (int st = 0; st < 2; st++) {
                 if (mixed) launch_amr3d_fluxes_mixed(a, cnt, 1 << st, S.C.stream);
                 else launch_amr3d_fluxes_fp64(a, cnt, 1 << st, S.C.stream);
                 CKA(cudaEventRecord(e[2 + st], S.C.stream));
             }
             if (mixed) launch_amr3d_update_mixed(a, cnt, S.C.stream); else launch_amr3d_update_fp64(a, cnt, S.C.stream);
-            CKA(cudaEventRecord(e[5], S.C.stream));
+            CKA(cudaEventRecord(e[4], S.C.stream));
             CKA(cudaGetLastError());
-            CKA(cudaEventSynchronize(e[5]));
-            for (int k = 0; k < 5; k++) CKA(cudaEventElapsedTime(&t[k], e[k], e[k + 1]));
+            CKA(cudaEventSynchronize(e[4]));
+            for (int k = 0; k < 4; k++) CKA(cudaEventElapsedTime(&t[k], e[k], e[k + 1]));
         }
-        for (int k = 0; k < 5; k++)
+        for (int k = 0; k < 4; k++)
             if (t[k] < best[k]) { best[k] = t[k]; pick[k] = c; }
     }
-    for (int i = 0; i < 6; i++) cudaEventDestroy(e[i]);
+    for (int i = 0; i < 5; i++) cudaEventDestroy(e[i]);
     S.fill_cta = pick[0];
-    for (int q = 0; q < 4; q++) S.cta[q] = pick[1 + q];
+    S.cta[0] = pick[1];
+    S.cta[1] = pick[2];
+    S.cta[2] = pick[2];
+    S.cta[3] = pick[3];
     CKA(cudaMemsetAsync(S.C.rate_max, 0, sizeof(unsigned long long), S.C.stream));
     CKA(cudaStreamSynchronize(S.C.stream));
     snprintf(S.tune_log, sizeof(S.tune_log),
-             "AMR launch shape (CTAs of 256 per block, %d blocks of %d^3): fill=%d sig=%d states=%d flux=%d update=%d "
-             "(ms %.3f %.3f %.3f %.3f %.3f)", cnt, S.n, pick[0], pick[1], pick[2], pick[3], pick[4],
-             best[0], best[1], best[2], best[3], best[4]);
+             "AMR launch shape (CTAs of 256 per block, %d blocks of %d^3): fill=%d sig=%d slopes=%d update=%d "
+             "(ms fill %.3f, sigma %.3f, slopes + face states + fluxes %.3f, update %.3f)", cnt, S.n, pick[0], pick[1],
+             pick[2], pick[3], best[0], best[1], best[2], best[3]);
     return FXB_OK;
 }
 
@@ -1288,7 +1293,7 @@ int amr_step(const double *dtv, double dt, int *launches)
     nl += restrict_needed(S.cur);
     Args3D a = batch_args(dtv, dt);
     auto fluxes = [&](int cnt) {
-        const int all = AMR_SIG | AMR_STATES | AMR_FLUX;
+        const int all = AMR_SIG | AMR_STATES;
         if (mixed) launch_amr3d_fluxes_mixed(a, cnt, all, S.C.stream);
         else launch_amr3d_fluxes_fp64(a, cnt, all, S.C.stream);
     };
@@ -1303,8 +1308,9 @@ int amr_step(const double *dtv, double dt, int *launches)
     auto update = [&](int cnt) {
         if (mixed) launch_amr3d_update_mixed(a, cnt, S.C.stream); else launch_amr3d_update_fp64(a, cnt, S.C.stream);
     };
-    // sigma (+ flattening), slopes and states (PPM) or states (WENO5) of three directions, three fluxes
-    const int pipe = 1 + (S.C.prm.flattening ? 1 : 0) + (S.C.prm.order == 3 ? 6 : 3) + 3;
+    // sigma (+ flattening), then per direction the slopes (PPM), the face
+    // states and the fluxes (one fused kernel in FP32, two in FP64)
+    const int pipe = 1 + (S.C.prm.flattening ? 1 : 0) + 3 * ((S.C.prm.order == 3 ? 1 : 0) + (mixed ? 1 : 2));
     if (S.nleaf <= S.batch) {
         a.batch = S.d_entries;
         nl += fill_batch(a.batch, S.nleaf, S.cur);

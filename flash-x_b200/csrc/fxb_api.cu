@@ -301,6 +301,14 @@ int launch_hydro(int src, const double *dtv, double dt)
     return FXB_OK;
 }
 
+// kernels of one 3-D step: sigma, per direction the slopes (PPM), the face
+// states and the fluxes (one fused kernel in FP32, two in FP64), the update
+int hydro3d_launches(const fxb_params &p)
+{
+    const int per_dir = (p.order == 3 ? 1 : 0) + (p.precision == FXB_MIXED ? 1 : 2);
+    return 1 + 3 * per_dir + 1;
+}
+
 int check_err_word()
 {
     int h = 0;
@@ -578,7 +586,7 @@ extern "C" int fxb_hydro_step(double sim_time, double dt, double dt_old)
         int rc = launch_hydro(L.cur, nullptr, dt);
         if (rc) return rc;
         L.cur = 1 - L.cur;
-        nl = (L.dom.ndim == 2 ? 1 : (L.prm.order == 3 ? 11 : 8)) + (L.prm.flattening ? 1 : 0);
+        nl = (L.dom.ndim == 2 ? 1 : hydro3d_launches(L.prm)) + (L.prm.flattening ? 1 : 0);
     }
     CK(cudaEventRecord(L.ev1, L.stream));
     L.rate_valid = true;
@@ -658,7 +666,7 @@ extern "C" int fxb_advance(int nsteps, double *dt, double *dt_old, double f, dou
     CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
     // graphs of two steps (buffer c -> 1-c -> c), built once per starting buffer
     const bool amr = amr_active();
-    int step_launches = (L.dom.ndim == 2 ? 1 : (L.prm.order == 3 ? 11 : 8)) + (L.prm.flattening ? 1 : 0);
+    int step_launches = (L.dom.ndim == 2 ? 1 : hydro3d_launches(L.prm)) + (L.prm.flattening ? 1 : 0);
     auto one_step = [&](int src) -> int {
         int rc = amr ? amr_step(L.dtv, 0., &step_launches) : launch_hydro(src, L.dtv, 0.);
         if (rc) return rc;

@@ -60,7 +60,7 @@ struct Args3D {
     unsigned long long *rate_max;
     int *err;
     void *sig;      // [3][6][(nx+2)(ny+2)(nz+2)] of R
-    void *wst[3];   // per direction [12][cells with that coordinate in [-1, n]]
+    void *wst[3];   // per direction [2][cells with that coordinate in [-1, n]]: Wp, Wm pressures
     void *flx[3];   // per direction [8][faces]
     void *slp;      // PPM: characteristic-limited slopes of the current direction [6][Grid3::ns(d)]
     long slp_bstride;           // AMR: elements of R per batch entry
@@ -76,17 +76,44 @@ struct Args3D {
     double *odata;              // interior store [block][var][cell]
     long o_vstride, o_bstride;
     long sig_bstride, w_bstride[3], f_bstride[3];   // elements of R per batch entry
-    int cta[4];                 // CTAs per batch entry: sig3d, states3d, flux3d, update3d
+    int cta[4];                 // CTAs per batch entry: sig3d, slope3d, (unused), update3d
     FastDiv fdx[5], fdy[5];     // divisors nx + e and ny + e (e = 0, 1, 2, 4), set by the launchers
+    int sf_len[3], sf_lines[3]; // face-state tiles per direction (cells along d, lines), set by the launchers
 };
-// the launchers' copy of the arguments with the index divisors filled in
+// Face-state tile of direction d (N cells along d, N1 along the t1 axis):
+// the fewest warp lanes in total (the N + 1 faces split into segments of
+// Ls - 1, each needing Ls cells, on lines grouped T1 at a time, CTAs rounded
+// up to whole warps), then the largest CTA; lines along y or z group at least
+// 8 x-neighbours (coalescing).
+#ifndef FXB_SF_MAXT
+#define FXB_SF_MAXT 288
+#endif
+inline void sflux_tile(int d, int N, int N1, int &Ls, int &T1)
+{
+    long best = -1;
+    Ls = 3; T1 = 1;
+    const int cand[5] = {16, 8, 4, 2, 1};
+    for (int t1 : cand) {
+        if (t1 > N1) continue;
+        if (d != 0 && t1 < (N1 < 8 ? N1 : 8)) continue;
+        for (int ls = 3; ls * t1 <= FXB_SF_MAXT; ls++) {
+            const long nseg = (N + ls - 1) / (ls - 1);
+            const long work = nseg * (long)((N1 + t1 - 1) / t1) * ((ls * t1 + 31) / 32 * 32);
+            if (best < 0 || work < best || (work == best && ls * t1 > Ls * T1)) { best = work; Ls = ls; T1 = t1; }
+        }
+    }
+}
+
+// the launchers' copy of the arguments with the index divisors and the face-state tiles filled in
 inline Args3D with_divisors(const Args3D &a)
 {
     Args3D b = a;
     for (int e = 0; e <= 4; e++) { b.fdx[e] = make_fastdiv((unsigned)a.nx + e); b.fdy[e] = make_fastdiv((unsigned)a.ny + e); }
+    const int n[3] = {a.nx, a.ny, a.nz};
+    for (int d = 0; d < 3; d++) sflux_tile(d, n[d], d == 0 ? a.ny : a.nx, b.sf_len[d], b.sf_lines[d]);
     return b;
 }
-enum { AMR_SIG = 1, AMR_STATES = 2, AMR_FLUX = 4 };
+enum { AMR_SIG = 1, AMR_STATES = 2 };   // sigma (+ flattening); slopes, face states and fluxes
 
 // 3-D tile extents accepted by fxb_init (the unfused kernels take any size)
 constexpr int T3X = 1, T3Y = 1, T3Z = 1;
@@ -382,24 +409,134 @@ __global__ void __launch_bounds__(256) slope3d_kernel(const Args3D a, int d)
     }
 }
 
-// ---- face states of direction d ------------------------------------------------
+// ---- face states of one cell in direction d ------------------------------------
 // One instantiation per reconstruction order, so the register allocation of
 // the PPM path (three eigensystems and slopes) and of the WENO path (one
-// eigensystem, five projected cells) do not add up.  The minimum number of
-// resident 256-thread CTAs per SM bounds the registers per thread.  FP64: two
-// CTAs (128 registers, a few hundred bytes of spills) measured 18 % faster on
-// B200 than one CTA with 244-255 registers, and three CTAs (80 registers)
-// lost again to spill traffic.  FP32: three CTAs (80 registers, ~140 bytes
-// of spills) measured 5-12 % faster than two.
+// eigensystem, five projected cells) do not add up.
+template <class R, int ORDER, bool AMR, int DIR>
+__device__ __forceinline__ void face_states(const Args3D &a, const Ctx3<R, AMR> &X, const double dt, const R dtn,
+                                            const R hdtn, const R hdtx, const R hdty, const R hdtz, int i, int j,
+                                            int k, R Wm_out[6], R Wp_out[6], R &gc_out, R &ge_out)
+{
+    constexpr int d = DIR;
+    const Grid3 &G = X.G;
+    int di, dj, dk;
+    offs(d, 1, di, dj, dk);
+    R S8[5][8], S[5][6], g[6];
+#pragma unroll
+    for (int o = -2; o <= 2; o++) {
+        if (ORDER == 3 && (o == -2 || o == 2)) continue;   // PPM reads its neighbours' slopes instead
+        X.load(a, i + o * di, j + o * dj, k + o * dk, S8[o + 2]);
+        six(S8[o + 2], g); rot3(d, g, S[o + 2]);
+    }
+    const R *vc = S8[2];
+    Eig<R> e;
+    if (!eigen(S[2][0], S[2][1], S[2][4], vc[GC], e)) atomicOr(a.err, ERR_SOUND);
+    R vecL[6], vecR[6];
+    if constexpr (ORDER == 5) {
+        weno_interfaces(a.prm, e, S, vecL, vecR);
+    } else {
+        // slopes of the cell and its two neighbours from slope3d_kernel
+        const long ns = G.ns(d);
+        const long sN = G.sidx(d, i - di, j - dj, k - dk), s0 = G.sidx(d, i, j, k), sP = G.sidx(d, i + di, j + dj, k + dk);
+        R dbN[6], db0[6], dbP[6];
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            dbN[q] = X.slp[(long)q * ns + sN];
+            db0[q] = X.slp[(long)q * ns + s0];
+            dbP[q] = X.slp[(long)q * ns + sP];
+        }
+        ppm_interfaces(S[1], S[2], S[3], dbN, db0, dbP, vecL, vecR);
+    }
+    if (a.prm.flattening) flatten(X.flat[(long)d * G.npad() + G.pidx(i, j, k)], S[2], vecL, vecR);
+    R wm[6], wp[6], Wm[6], Wp[6];
+    ppm_trace(e, dtn, hdtn, S[2], vecL, vecR, wm, wp);
+    unrot3(d, wm, Wm); unrot3(d, wp, Wp);
+    // transverse terms, hy_dataReconstOneStep.F90:931-962
+    R s1[6], s2[6];
+    if (d == 0) {
+        read_sig(X.sig, G, 1, i, j, k, s1); read_sig(X.sig, G, 2, i, j, k, s2);
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            Wm[q] = Wm[q] - hdty * s1[q]; Wp[q] = Wp[q] - hdty * s1[q];
+            Wm[q] = Wm[q] - hdtz * s2[q]; Wp[q] = Wp[q] - hdtz * s2[q];
+        }
+    } else if (d == 1) {
+        read_sig(X.sig, G, 0, i, j, k, s1); read_sig(X.sig, G, 2, i, j, k, s2);
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            Wm[q] = Wm[q] - hdtx * s1[q]; Wp[q] = Wp[q] - hdtx * s1[q];
+            Wm[q] = Wm[q] - hdtz * s2[q]; Wp[q] = Wp[q] - hdtz * s2[q];
+        }
+    } else {
+        read_sig(X.sig, G, 0, i, j, k, s1); read_sig(X.sig, G, 1, i, j, k, s2);
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            Wm[q] = Wm[q] - hdtx * s1[q] - hdty * s2[q];
+            Wp[q] = Wp[q] - hdtx * s1[q] - hdty * s2[q];
+        }
+    }
+    R gvc[6]; six(vc, gvc);
+    if (Wm[0] < R(0) || Wp[0] < R(0) || Wm[4] < R(0) || Wp[4] < R(0)) {
+#pragma unroll
+        for (int q = 0; q < 6; q++) { Wm[q] = gvc[q]; Wp[q] = gvc[q]; }
+    }
+    if (a.prm.use_gravity) {   // hy_getRiemannState.F90:843-885
+        const R hdt = R(0.5 * dt);
+        R gl, gr;
+        gravity_faces(a.prm, R(a.prm.grav[d]), gl, gr);
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            R gp = q == d ? gr : R(a.prm.grav[q]);
+            R gn = q == d ? gl : R(a.prm.grav[q]);
+            Wp[1 + q] = Wp[1 + q] + hdt * gp;
+            Wm[1 + q] = Wm[1 + q] + hdt * gn;
+        }
+    }
+    if (a.prm.use_3d_full_ctu) {
+        int e1, s1d, e2, s2d; double fac;
+        if (d == 0)      { e1 = 1; s1d = 2; e2 = 2; s2d = 1; fac = dt * dt / (6. * X.dy * X.dz); }
+        else if (d == 1) { e1 = 2; s1d = 0; e2 = 0; s2d = 2; fac = dt * dt / (6. * X.dz * X.dx); }
+        else             { e1 = 0; s1d = 1; e2 = 1; s2d = 0; fac = dt * dt / (6. * X.dx * X.dy); }
+        R T1[6], T2[6];
+        ctu_term(a, X.sig, G, vc, e1, s1d, i, j, k, T1);
+        ctu_term(a, X.sig, G, vc, e2, s2d, i, j, k, T2);
+        const R f = R(fac);
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            Wp[q] = Wp[q] + (T1[q] + T2[q]) * f;
+            Wm[q] = Wm[q] + (T1[q] + T2[q]) * f;
+        }
+        if (Wp[0] <= R(0) || Wm[0] <= R(0) || Wp[4] <= R(0) || Wm[4] <= R(0)) {
+#pragma unroll
+            for (int q = 0; q < 6; q++) { Wm[q] = gvc[q]; Wp[q] = gvc[q]; }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++) { Wm_out[q] = Wm[q]; Wp_out[q] = Wp[q]; }
+    gc_out = vc[GC]; ge_out = vc[GE];
+}
+
+// ---- face states and Riemann fluxes as two kernels (FP64) --------------------------
+// In FP64 the fused kernel below measured slower on B200 (its barrier between
+// the face states and the fluxes idles two CTAs of long FP64 warps), so the
+// FP64 path stores all twelve face-state values and solves the Riemann
+// problems in a second kernel.  FP32 fuses them.
+template <class R> struct FusedFaces { static constexpr bool value = sizeof(R) == 4; };
+// slots of the Wp and Wm pressures in the face-state arrays
+template <class R> struct PwSlots {
+    static constexpr int wp = FusedFaces<R>::value ? 0 : P, wm = FusedFaces<R>::value ? 1 : 6 + P;
+};
+
+// The minimum number of resident 256-thread CTAs per SM bounds the registers
+// per thread: two CTAs (128 registers, a few hundred bytes of spills)
+// measured 18 % faster on B200 than one CTA with 244-255 registers, and three
+// CTAs (80 registers) lost again to spill traffic.
 #ifndef FXB_S3_MINB_FP64
 #define FXB_S3_MINB_FP64 2
 #endif
-#ifndef FXB_S3_MINB_FP32
-#define FXB_S3_MINB_FP32 3
-#endif
-template <class R> struct MinB3D { static constexpr int value = sizeof(R) == 8 ? FXB_S3_MINB_FP64 : FXB_S3_MINB_FP32; };
 template <class R, int ORDER, bool AMR, int DIR>
-__global__ void __launch_bounds__(256, MinB3D<R>::value) states3d_kernel(const Args3D a)
+__global__ void __launch_bounds__(256, FXB_S3_MINB_FP64) states3d_kernel(const Args3D a)
 {
     constexpr int d = DIR;
     const Ctx3<R, AMR> X(a);
@@ -414,98 +551,8 @@ __global__ void __launch_bounds__(256, MinB3D<R>::value) states3d_kernel(const A
         int i, j, k;
         unflatten(idx, a.fdx[d == 0 ? 2 : 0], a.fdy[d == 1 ? 2 : 0], i, j, k);
         if (d == 0) i -= 1; else if (d == 1) j -= 1; else k -= 1;
-        int di, dj, dk;
-        offs(d, 1, di, dj, dk);
-        R S8[5][8], S[5][6], g[6];
-#pragma unroll
-        for (int o = -2; o <= 2; o++) {
-            if (ORDER == 3 && (o == -2 || o == 2)) continue;   // PPM reads its neighbours' slopes instead
-            X.load(a, i + o * di, j + o * dj, k + o * dk, S8[o + 2]);
-            six(S8[o + 2], g); rot3(d, g, S[o + 2]);
-        }
-        const R *vc = S8[2];
-        Eig<R> e;
-        if (!eigen(S[2][0], S[2][1], S[2][4], vc[GC], e)) atomicOr(a.err, ERR_SOUND);
-        R vecL[6], vecR[6];
-        if constexpr (ORDER == 5) {
-            weno_interfaces(a.prm, e, S, vecL, vecR);
-        } else {
-            // slopes of the cell and its two neighbours from slope3d_kernel
-            const long ns = G.ns(d);
-            const long sN = G.sidx(d, i - di, j - dj, k - dk), s0 = G.sidx(d, i, j, k), sP = G.sidx(d, i + di, j + dj, k + dk);
-            R dbN[6], db0[6], dbP[6];
-#pragma unroll
-            for (int q = 0; q < 6; q++) {
-                dbN[q] = X.slp[(long)q * ns + sN];
-                db0[q] = X.slp[(long)q * ns + s0];
-                dbP[q] = X.slp[(long)q * ns + sP];
-            }
-            ppm_interfaces(S[1], S[2], S[3], dbN, db0, dbP, vecL, vecR);
-        }
-        if (a.prm.flattening) flatten(X.flat[(long)d * G.npad() + G.pidx(i, j, k)], S[2], vecL, vecR);
-        R wm[6], wp[6], Wm[6], Wp[6];
-        ppm_trace(e, dtn, hdtn, S[2], vecL, vecR, wm, wp);
-        unrot3(d, wm, Wm); unrot3(d, wp, Wp);
-        // transverse terms, hy_dataReconstOneStep.F90:931-962
-        R s1[6], s2[6];
-        if (d == 0) {
-            read_sig(X.sig, G, 1, i, j, k, s1); read_sig(X.sig, G, 2, i, j, k, s2);
-#pragma unroll
-            for (int q = 0; q < 6; q++) {
-                Wm[q] = Wm[q] - hdty * s1[q]; Wp[q] = Wp[q] - hdty * s1[q];
-                Wm[q] = Wm[q] - hdtz * s2[q]; Wp[q] = Wp[q] - hdtz * s2[q];
-            }
-        } else if (d == 1) {
-            read_sig(X.sig, G, 0, i, j, k, s1); read_sig(X.sig, G, 2, i, j, k, s2);
-#pragma unroll
-            for (int q = 0; q < 6; q++) {
-                Wm[q] = Wm[q] - hdtx * s1[q]; Wp[q] = Wp[q] - hdtx * s1[q];
-                Wm[q] = Wm[q] - hdtz * s2[q]; Wp[q] = Wp[q] - hdtz * s2[q];
-            }
-        } else {
-            read_sig(X.sig, G, 0, i, j, k, s1); read_sig(X.sig, G, 1, i, j, k, s2);
-#pragma unroll
-            for (int q = 0; q < 6; q++) {
-                Wm[q] = Wm[q] - hdtx * s1[q] - hdty * s2[q];
-                Wp[q] = Wp[q] - hdtx * s1[q] - hdty * s2[q];
-            }
-        }
-        R gvc[6]; six(vc, gvc);
-        if (Wm[0] < R(0) || Wp[0] < R(0) || Wm[4] < R(0) || Wp[4] < R(0)) {
-#pragma unroll
-            for (int q = 0; q < 6; q++) { Wm[q] = gvc[q]; Wp[q] = gvc[q]; }
-        }
-        if (a.prm.use_gravity) {   // hy_getRiemannState.F90:843-885
-            const R hdt = R(0.5 * dt);
-            R gl, gr;
-            gravity_faces(a.prm, R(a.prm.grav[d]), gl, gr);
-#pragma unroll
-            for (int q = 0; q < 3; q++) {
-                R gp = q == d ? gr : R(a.prm.grav[q]);
-                R gn = q == d ? gl : R(a.prm.grav[q]);
-                Wp[1 + q] = Wp[1 + q] + hdt * gp;
-                Wm[1 + q] = Wm[1 + q] + hdt * gn;
-            }
-        }
-        if (a.prm.use_3d_full_ctu) {
-            int e1, s1d, e2, s2d; double fac;
-            if (d == 0)      { e1 = 1; s1d = 2; e2 = 2; s2d = 1; fac = dt * dt / (6. * X.dy * X.dz); }
-            else if (d == 1) { e1 = 2; s1d = 0; e2 = 0; s2d = 2; fac = dt * dt / (6. * X.dz * X.dx); }
-            else             { e1 = 0; s1d = 1; e2 = 1; s2d = 0; fac = dt * dt / (6. * X.dx * X.dy); }
-            R T1[6], T2[6];
-            ctu_term(a, X.sig, G, vc, e1, s1d, i, j, k, T1);
-            ctu_term(a, X.sig, G, vc, e2, s2d, i, j, k, T2);
-            const R f = R(fac);
-#pragma unroll
-            for (int q = 0; q < 6; q++) {
-                Wp[q] = Wp[q] + (T1[q] + T2[q]) * f;
-                Wm[q] = Wm[q] + (T1[q] + T2[q]) * f;
-            }
-            if (Wp[0] <= R(0) || Wm[0] <= R(0) || Wp[4] <= R(0) || Wm[4] <= R(0)) {
-#pragma unroll
-                for (int q = 0; q < 6; q++) { Wm[q] = gvc[q]; Wp[q] = gvc[q]; }
-            }
-        }
+        R Wm[6], Wp[6], gc, ge;
+        face_states<R, ORDER, AMR, DIR>(a, X, dt, dtn, hdtn, hdtx, hdty, hdtz, i, j, k, Wm, Wp, gc, ge);
 #pragma unroll
         for (int q = 0; q < 6; q++) { w[(long)q * nw + idx] = Wp[q]; w[(long)(6 + q) * nw + idx] = Wm[q]; }
     }
@@ -538,6 +585,75 @@ __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
         if (e) atomicOr(a.err, e);
 #pragma unroll
         for (int q = 0; q < NF; q++) f[(long)q * nf + idx] = F[q];
+    }
+}
+
+// ---- face states and Riemann fluxes of direction d --------------------------------
+// A CTA takes Ls consecutive cells (a segment seg: cells seg*S - 1 ..
+// seg*S + S - 1 along d, S = Ls - 1) of T1 neighbouring lines, computes their
+// face states, keeps the right-face states in shared memory and solves the
+// Riemann problems of the S faces seg*S .. seg*S + S - 1 (the left face of
+// each of its cells but the first), so the face states never leave the SM;
+// only the pressures of the interior cells' two face states are stored, for
+// the update's pressure average.  Threads run along d for d = 0 and along x
+// otherwise, so the loads of neighbouring threads are coalesced.  The
+// register cap keeps three CTAs of up to 288 threads per SM in FP32 and two
+// in FP64.
+template <class R> struct SfluxRegs {
+    static constexpr int value = (65536 / ((sizeof(R) == 8 ? 2 : 3) * FXB_SF_MAXT)) / 8 * 8;
+};
+template <class R, int ORDER, bool AMR, int DIR>
+__global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) sflux3d_kernel(const Args3D a)
+{
+    constexpr int d = DIR;
+    extern __shared__ __align__(16) unsigned char sflux_smem[];
+    R *sW = reinterpret_cast<R *>(sflux_smem);     // [8][threads]: right-face state, then gamc, game
+    const Ctx3<R, AMR> X(a);
+    const Grid3 &G = X.G;
+    const double dt = a.dtv ? a.dtv[0] : a.dt_arg;
+    const double del[3] = {X.dx, X.dy, X.dz};
+    const R dtn = R(dt / del[d]), hdtn = R(0.5 * (dt / del[d]));
+    const R hdtx = R(0.5 * dt / X.dx), hdty = R(0.5 * dt / X.dy), hdtz = R(0.5 * dt / X.dz);
+    const int N = d == 0 ? a.nx : d == 1 ? a.ny : a.nz;
+    const int N1 = d == 0 ? a.ny : a.nx, N2 = d == 2 ? a.ny : a.nz;
+    const int Ls = a.sf_len[d], T1 = a.sf_lines[d], S = Ls - 1;
+    const int nseg = (N + S) / S, nt1 = (N1 + T1 - 1) / T1;
+    const int t = threadIdx.x, nt = blockDim.x;
+    const int ld = d == 0 ? t % Ls : t / T1;
+    const int l1 = d == 0 ? t / Ls : t % T1;
+    int b = blockIdx.x;
+    const int seg = b % nseg;
+    b /= nseg;
+    const int t1 = (b % nt1) * T1 + l1, t2 = b / nt1;
+    const int c = seg * S - 1 + ld;
+    const bool active = t1 < N1 && t2 < N2 && c <= N;
+    const int i = d == 0 ? c : t1, j = d == 0 ? t1 : d == 1 ? c : t2, k = d == 2 ? c : t2;
+    R Wm[6], Wp[6], gc = R(0), ge = R(0);
+    if (active) {
+        face_states<R, ORDER, AMR, DIR>(a, X, dt, dtn, hdtn, hdtx, hdty, hdtz, i, j, k, Wm, Wp, gc, ge);
+#pragma unroll
+        for (int q = 0; q < 6; q++) sW[q * nt + t] = Wp[q];
+        sW[6 * nt + t] = gc;
+        sW[7 * nt + t] = ge;
+        if (c >= 0 && c < N) {
+            R *pw = X.wst[d];
+            const long nw = G.nw(d), wc = G.widx(d, i, j, k);
+            pw[PwSlots<R>::wp * nw + wc] = Wp[P];
+            pw[PwSlots<R>::wm * nw + wc] = Wm[P];
+        }
+    }
+    __syncthreads();
+    if (active && ld >= 1) {
+        const int tl = d == 0 ? t - 1 : t - T1;
+        R VL[6], F[NF];
+#pragma unroll
+        for (int q = 0; q < 6; q++) VL[q] = sW[q * nt + tl];
+        const int e = riemann(a.prm, d, VL, sW[6 * nt + tl], sW[7 * nt + tl], Wm, gc, ge, F);
+        if (e) atomicOr(a.err, e);
+        R *f = X.flx[d];
+        const long nf = G.nf(d), fi = G.fidx(d, i, j, k);
+#pragma unroll
+        for (int q = 0; q < NF; q++) f[q * nf + fi] = F[q];
     }
 }
 
@@ -587,7 +703,7 @@ __global__ void __launch_bounds__(256, FXB_UPD_MINB) update3d_kernel(const Args3
             B[d] = (double)f[(long)FVOL * nf + fl] - (double)f[(long)FVOL * nf + fr];
             Sph[1 + d] = ((double)f[(long)FP * nf + fl] - (double)f[(long)FP * nf + fr]) * (1.0 - prm.fpres) / del[d];
             long wc = G.widx(d, i, j, k);
-            double sum = (double)w[(long)(6 + P) * nw + wc] + (double)w[(long)P * nw + wc];
+            double sum = (double)w[(long)PwSlots<R>::wm * nw + wc] + (double)w[(long)PwSlots<R>::wp * nw + wc];
             if (d == 0) pav = 0.5 * sum;
             else if (d == 1) pav = pav * 0.5 + sum * 0.25;
             else pav = (pav * 4.0 + sum) / 6.0;
@@ -648,10 +764,12 @@ __global__ void __launch_bounds__(256, FXB_UPD_MINB) update3d_kernel(const Args3
 // bytes of the 3-D intermediates for R of the given size
 inline size_t sig3d_bytes(int nx, int ny, int nz, size_t rsz)
 { return rsz * 18 * (size_t)(nx + 2) * (ny + 2) * (nz + 2); }
+// face states of every cell of direction d: all twelve values (FP64), or the
+// pressures of the two (FP32, fused with the fluxes)
 inline size_t w3d_bytes(int d, int nx, int ny, int nz, size_t rsz)
 {
     size_t n = d == 0 ? (size_t)(nx + 2) * ny * nz : d == 1 ? (size_t)nx * (ny + 2) * nz : (size_t)nx * ny * (nz + 2);
-    return rsz * 12 * n;
+    return rsz * (rsz == 4 ? 2 : 12) * n;
 }
 // the PPM slope buffer, sized for the largest direction
 inline size_t slp3d_bytes(int nx, int ny, int nz, size_t rsz)
@@ -667,14 +785,31 @@ inline size_t f3d_bytes(int d, int nx, int ny, int nz, size_t rsz)
     return rsz * 8 * n;
 }
 
-// face states of one direction: PPM reads the slopes of slope3d_kernel
+// face states and fluxes of one direction (PPM: slopes first); g.x CTAs per
+// block for the grid-stride kernels, g.y batch entries
 template <class R, bool AMR, int DIR> void launch_states3d(const Args3D &a, dim3 g, cudaStream_t s)
 {
-    if (a.prm.order == 5) {
-        states3d_kernel<R, 5, AMR, DIR><<<g, 256, 0, s>>>(a);
+    if constexpr (!FusedFaces<R>::value) {
+        if (a.prm.order == 5) {
+            states3d_kernel<R, 5, AMR, DIR><<<g, 256, 0, s>>>(a);
+        } else {
+            slope3d_kernel<R, AMR><<<g, 256, 0, s>>>(a, DIR);
+            states3d_kernel<R, 3, AMR, DIR><<<g, 256, 0, s>>>(a);
+        }
+        flux3d_kernel<R, AMR, DIR><<<dim3(AMR ? a.cta[2] : g.x, g.y), 256, 0, s>>>(a);
     } else {
-        slope3d_kernel<R, AMR><<<g, 256, 0, s>>>(a, DIR);
-        states3d_kernel<R, 3, AMR, DIR><<<g, 256, 0, s>>>(a);
+        const int N = DIR == 0 ? a.nx : DIR == 1 ? a.ny : a.nz;
+        const int N1 = DIR == 0 ? a.ny : a.nx, N2 = DIR == 2 ? a.ny : a.nz;
+        const int Ls = a.sf_len[DIR], T1 = a.sf_lines[DIR];
+        const int nseg = (N + Ls - 1) / (Ls - 1), nt1 = (N1 + T1 - 1) / T1;
+        const dim3 gs((unsigned)(nseg * nt1 * N2), g.y);
+        const size_t sm = 8 * sizeof(R) * (size_t)(Ls * T1);
+        if (a.prm.order == 5) {
+            sflux3d_kernel<R, 5, AMR, DIR><<<gs, Ls * T1, sm, s>>>(a);
+        } else {
+            slope3d_kernel<R, AMR><<<g, 256, 0, s>>>(a, DIR);
+            sflux3d_kernel<R, 3, AMR, DIR><<<gs, Ls * T1, sm, s>>>(a);
+        }
     }
 }
 
@@ -687,9 +822,6 @@ template <class R> void launch_hydro3d_t(const Args3D &a0, cudaStream_t s)
     launch_states3d<R, false, 0>(a, dim3(nb), s);
     launch_states3d<R, false, 1>(a, dim3(nb), s);
     launch_states3d<R, false, 2>(a, dim3(nb), s);
-    flux3d_kernel<R, false, 0><<<nb, 256, 0, s>>>(a);
-    flux3d_kernel<R, false, 1><<<nb, 256, 0, s>>>(a);
-    flux3d_kernel<R, false, 2><<<nb, 256, 0, s>>>(a);
     update3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
 }
 
@@ -758,7 +890,8 @@ __global__ void __launch_bounds__(256) amr_correct_flux_kernel(const Args3D a, c
 }
 
 // The 3-D pipeline over one AMR batch of `entries` guard-filled blocks; `which`
-// selects the stages (AMR_SIG | AMR_STATES | AMR_FLUX), a.cta[] the CTAs per block.
+// selects the stages (AMR_SIG | AMR_STATES), a.cta[] the CTAs per block of the
+// grid-stride kernels (the face-state kernel has its own tiles).
 template <class R> void launch_amr3d_fluxes_t(const Args3D &a0, int entries, int which, cudaStream_t s)
 {
     const Args3D a = with_divisors(a0);
@@ -768,11 +901,6 @@ template <class R> void launch_amr3d_fluxes_t(const Args3D &a0, int entries, int
         launch_states3d<R, true, 0>(a, dim3(a.cta[1], entries), s);
         launch_states3d<R, true, 1>(a, dim3(a.cta[1], entries), s);
         launch_states3d<R, true, 2>(a, dim3(a.cta[1], entries), s);
-    }
-    if (which & AMR_FLUX) {
-        flux3d_kernel<R, true, 0><<<dim3(a.cta[2], entries), 256, 0, s>>>(a);
-        flux3d_kernel<R, true, 1><<<dim3(a.cta[2], entries), 256, 0, s>>>(a);
-        flux3d_kernel<R, true, 2><<<dim3(a.cta[2], entries), 256, 0, s>>>(a);
     }
 }
 template <class R> void launch_amr3d_emit_t(const Args3D &a, int entries, void *bflux, long nfc, cudaStream_t s)
