@@ -85,20 +85,38 @@ template <class R> struct Eig {
     R cf, rho, ahinv, lp, a2inv, rp;
 };
 
-// returns false on a2 <= 0 (the reference aborts there)
-template <class R> __device__ __forceinline__ bool eigen(R rho, R un, R p, R gamc, Eig<R> &e)
+// The direction-independent part of a cell's eigensystem: everything but the
+// normal velocity (the divisions and the square root), shared by the
+// eigensystems of one cell in several directions.  Returns false on a2 <= 0
+// (the reference aborts there).
+template <class R> struct EigBase {
+    R cf, rho, ahinv, lp, a2inv, rp;
+};
+template <class R> __device__ __forceinline__ bool eigen_base(R rho, R p, R gamc, EigBase<R> &b)
 {
     R a2 = rdiv(gamc * p, rho);
     if (a2 <= R(0)) return false;
     R cf = rsqrt_(a2);
-    e.lam0 = un - cf; e.un = un; e.lam4 = un + cf;
     R dinv = rdiv(R(1), rho);
     R aa2 = cf * cf;
-    e.a2inv = rdiv(R(1), aa2);
-    e.ahinv = rdiv(R(.5), cf);
-    R Na = R(.5) * e.a2inv;
-    e.lp = dinv * Na;
-    e.cf = cf; e.rho = rho; e.rp = rho * aa2;
+    b.a2inv = rdiv(R(1), aa2);
+    b.ahinv = rdiv(R(.5), cf);
+    R Na = R(.5) * b.a2inv;
+    b.lp = dinv * Na;
+    b.cf = cf; b.rho = rho; b.rp = rho * aa2;
+    return true;
+}
+// the eigensystem along a direction with normal velocity un
+template <class R> __device__ __forceinline__ void eigen_dir(const EigBase<R> &b, R un, Eig<R> &e)
+{
+    e.lam0 = un - b.cf; e.un = un; e.lam4 = un + b.cf;
+    e.cf = b.cf; e.rho = b.rho; e.ahinv = b.ahinv; e.lp = b.lp; e.a2inv = b.a2inv; e.rp = b.rp;
+}
+template <class R> __device__ __forceinline__ bool eigen(R rho, R un, R p, R gamc, Eig<R> &e)
+{
+    EigBase<R> b;
+    if (!eigen_base(rho, p, gamc, b)) return false;
+    eigen_dir(b, un, e);
     return true;
 }
 

@@ -111,13 +111,16 @@ __device__ __forceinline__ void analysis_stage(const Args2D &a, Smem2D<R> &s, in
 {
     R g[6], c[6];
     win6(s, wx, wy, g);
+    // one eigensystem base for the slope direction and the transverse one
+    EigBase<R> eb;
+    if (!eigen_base(g[0], g[4], s.V[GC][wy][wx], eb)) set_err(a.err, ERR_SOUND);
     if (ppm) {
         const int ox = dir == 0, oy = dir == 1;
         R gm[6], gp[6], Vm[6], Vp[6], db[6];
         win6(s, wx - ox, wy - oy, gm); win6(s, wx + ox, wy + oy, gp);
         rot(dir, gm, Vm); rot(dir, g, c); rot(dir, gp, Vp);
         Eig<R> e;
-        if (!eigen(c[0], c[1], c[4], s.V[GC][wy][wx], e)) set_err(a.err, ERR_SOUND);
+        eigen_dir(eb, c[1], e);
         tvd_slope(a.prm, e, Vm, c, Vp, db);
 #pragma unroll
         for (int k = 0; k < 6; k++) s.DBF[k * NDB + t] = db[k];
@@ -131,7 +134,7 @@ __device__ __forceinline__ void analysis_stage(const Args2D &a, Smem2D<R> &s, in
     win6(s, wx - tx, wy - ty, gm); win6(s, wx + tx, wy + ty, gp);
     rot(td, gm, m); rot(td, g, c); rot(td, gp, p);
     Eig<R> et;
-    if (!eigen(c[0], c[1], c[4], s.V[GC][wy][wx], et)) set_err(a.err, ERR_SOUND);
+    eigen_dir(eb, c[1], et);
     trans_flux(et, m, c, p, a.prm.use_aux_eint != 0, sr);
     unrot(td, sr, sg);
 #pragma unroll

@@ -298,6 +298,9 @@ __global__ void __launch_bounds__(256) sig3d_kernel(const Args3D a)
         R vc[8];
         X.load(a, i, j, k, vc);
         R gc[6]; six(vc, gc);
+        EigBase<R> eb;
+        const bool eok = eigen_base(vc[D], vc[P], vc[GC], eb);
+        if (!eok) atomicOr(a.err, ERR_SOUND);
         for (int d = 0; d < 3; d++) {
             int di, dj, dk;
             offs(d, 1, di, dj, dk);
@@ -308,7 +311,7 @@ __global__ void __launch_bounds__(256) sig3d_kernel(const Args3D a)
             rot3(d, gc, c);
             six(vp, g); rot3(d, g, p);
             Eig<R> e;
-            if (!eigen(c[0], c[1], c[4], vc[GC], e)) atomicOr(a.err, ERR_SOUND);
+            eigen_dir(eb, c[1], e);
             trans_flux(e, m, c, p, a.prm.use_aux_eint != 0, sr);
             unrot3(d, sr, sg);
 #pragma unroll
@@ -360,8 +363,8 @@ __device__ __forceinline__ void read_sig(const R *sig, const Grid3 &G, int d, in
 // CTU cross term of one transverse pair: upwinding along e of sigma_s at the
 // cell's e-neighbours, with the e-direction eigensystem of the cell
 template <class R>
-__device__ __forceinline__ void ctu_term(const Args3D &a, const R *sigp, const Grid3 &G, const R vc[8], int e, int s,
-                                        int i, int j, int k, R T[6])
+__device__ __forceinline__ void ctu_term(const Args3D &a, const R *sigp, const Grid3 &G, const R vc[8],
+                                        const EigBase<R> &eb, int e, int s, int i, int j, int k, R T[6])
 {
     int di, dj, dk;
     offs(e, 1, di, dj, dk);
@@ -372,7 +375,7 @@ __device__ __forceinline__ void ctu_term(const Args3D &a, const R *sigp, const G
     rot3(e, sm, m); rot3(e, sc, c); rot3(e, sp, p);
     six(vc, gcell); rot3(e, gcell, r);
     Eig<R> ev;
-    if (!eigen(r[0], r[1], r[4], vc[GC], ev)) atomicOr(a.err, ERR_SOUND);
+    eigen_dir(eb, r[1], ev);
     trans_flux(ev, m, c, p, a.prm.use_aux_eint != 0, tr);
     unrot3(e, tr, T);
 }
@@ -430,8 +433,11 @@ __device__ __forceinline__ void face_states(const Args3D &a, const Ctx3<R, AMR> 
         six(S8[o + 2], g); rot3(d, g, S[o + 2]);
     }
     const R *vc = S8[2];
+    // the cell's eigensystem along d, and (CTU) along the two other directions
+    EigBase<R> eb;
+    if (!eigen_base(S[2][0], S[2][4], vc[GC], eb)) atomicOr(a.err, ERR_SOUND);
     Eig<R> e;
-    if (!eigen(S[2][0], S[2][1], S[2][4], vc[GC], e)) atomicOr(a.err, ERR_SOUND);
+    eigen_dir(eb, S[2][1], e);
     R vecL[6], vecR[6];
     if constexpr (ORDER == 5) {
         weno_interfaces(a.prm, e, S, vecL, vecR);
@@ -499,8 +505,8 @@ __device__ __forceinline__ void face_states(const Args3D &a, const Ctx3<R, AMR> 
         else if (d == 1) { e1 = 2; s1d = 0; e2 = 0; s2d = 2; fac = dt * dt / (6. * X.dz * X.dx); }
         else             { e1 = 0; s1d = 1; e2 = 1; s2d = 0; fac = dt * dt / (6. * X.dx * X.dy); }
         R T1[6], T2[6];
-        ctu_term(a, X.sig, G, vc, e1, s1d, i, j, k, T1);
-        ctu_term(a, X.sig, G, vc, e2, s2d, i, j, k, T2);
+        ctu_term(a, X.sig, G, vc, eb, e1, s1d, i, j, k, T1);
+        ctu_term(a, X.sig, G, vc, eb, e2, s2d, i, j, k, T2);
         const R f = R(fac);
 #pragma unroll
         for (int q = 0; q < 6; q++) {
