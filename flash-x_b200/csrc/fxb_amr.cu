@@ -1156,7 +1156,7 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     const size_t per_entry = r * NV_GCB * ne3() + sig3d_bytes(S.n, S.n, S.n, r) +
                              w3d_bytes(0, S.n, S.n, S.n, r) + w3d_bytes(1, S.n, S.n, S.n, r) + w3d_bytes(2, S.n, S.n, S.n, r) +
                              f3d_bytes(0, S.n, S.n, S.n, r) + f3d_bytes(1, S.n, S.n, S.n, r) + f3d_bytes(2, S.n, S.n, S.n, r) +
-                             (c.prm.order == 3 ? slp3d_bytes(S.n, S.n, S.n, r) : 0) +
+                             (c.prm.order == 3 && r == 8 ? slp3d_bytes(S.n, S.n, S.n, r) : 0) +
                              (c.prm.flattening ? r * 3 * (size_t)(S.n + 2) * (S.n + 2) * (S.n + 2) : 0);
     size_t fr = 0, tot = 0;
     CKA(cudaMemGetInfo(&fr, &tot));
@@ -1171,7 +1171,8 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     }
     CKA(cudaMalloc(&S.gcb, r * NV_GCB * ne3() * S.batch));
     CKA(cudaMalloc(&S.sig, sig3d_bytes(S.n, S.n, S.n, r) * S.batch));
-    if (c.prm.order == 3) CKA(cudaMalloc(&S.slp, slp3d_bytes(S.n, S.n, S.n, r) * S.batch));
+    // PPM slopes in memory: FP64 only (the FP32 face-state kernel computes them itself)
+    if (c.prm.order == 3 && r == 8) CKA(cudaMalloc(&S.slp, slp3d_bytes(S.n, S.n, S.n, r) * S.batch));
     if (c.prm.flattening) CKA(cudaMalloc(&S.flat, r * 3 * (size_t)(S.n + 2) * (S.n + 2) * (S.n + 2) * S.batch));
     for (int d = 0; d < 3; d++) {
         CKA(cudaMalloc(&S.w[d], w3d_bytes(d, S.n, S.n, S.n, r) * S.batch));
@@ -1308,9 +1309,10 @@ int amr_step(const double *dtv, double dt, int *launches)
     auto update = [&](int cnt) {
         if (mixed) launch_amr3d_update_mixed(a, cnt, S.C.stream); else launch_amr3d_update_fp64(a, cnt, S.C.stream);
     };
-    // sigma (+ flattening), then per direction the slopes (PPM), the face
-    // states and the fluxes (one fused kernel in FP32, two in FP64)
-    const int pipe = 1 + (S.C.prm.flattening ? 1 : 0) + 3 * ((S.C.prm.order == 3 ? 1 : 0) + (mixed ? 1 : 2));
+    // sigma (+ flattening), then per direction the slopes, face states and
+    // fluxes (one fused kernel in FP32; slopes (PPM), face states and fluxes
+    // as separate kernels in FP64)
+    const int pipe = 1 + (S.C.prm.flattening ? 1 : 0) + 3 * (mixed ? 1 : (S.C.prm.order == 3 ? 3 : 2));
     if (S.nleaf <= S.batch) {
         a.batch = S.d_entries;
         nl += fill_batch(a.batch, S.nleaf, S.cur);

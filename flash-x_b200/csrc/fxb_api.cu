@@ -301,11 +301,12 @@ int launch_hydro(int src, const double *dtv, double dt)
     return FXB_OK;
 }
 
-// kernels of one 3-D step: sigma, per direction the slopes (PPM), the face
-// states and the fluxes (one fused kernel in FP32, two in FP64), the update
+// kernels of one 3-D step: sigma, per direction the slopes, face states and
+// fluxes (one fused kernel in FP32; slopes (PPM), face states and fluxes as
+// separate kernels in FP64), the update
 int hydro3d_launches(const fxb_params &p)
 {
-    const int per_dir = (p.order == 3 ? 1 : 0) + (p.precision == FXB_MIXED ? 1 : 2);
+    const int per_dir = p.precision == FXB_MIXED ? 1 : (p.order == 3 ? 3 : 2);
     return 1 + 3 * per_dir + 1;
 }
 
@@ -458,7 +459,8 @@ extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, cons
         // intermediates of the unfused 3-D pipeline, in the reconstruction type
         size_t rsz = p.precision == FXB_MIXED ? sizeof(float) : sizeof(double);
         CK(cudaMalloc(&L.sig3, sig3d_bytes(L.nx, L.ny, L.nz, rsz)));
-        if (p.order == 3) CK(cudaMalloc(&L.slp3, slp3d_bytes(L.nx, L.ny, L.nz, rsz)));
+        // PPM slopes in memory: FP64 only (the FP32 face-state kernel computes them itself)
+        if (p.order == 3 && p.precision == FXB_FP64) CK(cudaMalloc(&L.slp3, slp3d_bytes(L.nx, L.ny, L.nz, rsz)));
         for (int dd = 0; dd < 3; dd++) {
             CK(cudaMalloc(&L.w3[dd], w3d_bytes(dd, L.nx, L.ny, L.nz, rsz)));
             CK(cudaMalloc(&L.f3[dd], f3d_bytes(dd, L.nx, L.ny, L.nz, rsz)));

@@ -88,7 +88,7 @@ struct Args3D {
 #ifndef FXB_SF_MAXT
 #define FXB_SF_MAXT 288
 #endif
-inline void sflux_tile(int d, int N, int N1, int &Ls, int &T1)
+inline void sflux_tile(int d, int N, int N1, int halo, int &Ls, int &T1)
 {
     long best = -1;
     Ls = 3; T1 = 1;
@@ -96,21 +96,24 @@ inline void sflux_tile(int d, int N, int N1, int &Ls, int &T1)
     for (int t1 : cand) {
         if (t1 > N1) continue;
         if (d != 0 && t1 < (N1 < 8 ? N1 : 8)) continue;
-        for (int ls = 3; ls * t1 <= FXB_SF_MAXT; ls++) {
+        for (int ls = 3; (ls + halo) * t1 <= FXB_SF_MAXT; ls++) {
             const long nseg = (N + ls - 1) / (ls - 1);
-            const long work = nseg * (long)((N1 + t1 - 1) / t1) * ((ls * t1 + 31) / 32 * 32);
-            if (best < 0 || work < best || (work == best && ls * t1 > Ls * T1)) { best = work; Ls = ls; T1 = t1; }
+            const long work = nseg * (long)((N1 + t1 - 1) / t1) * (((ls + halo) * t1 + 31) / 32 * 32);
+            if (best < 0 || work < best || (work == best && (ls + halo) * t1 > (Ls + halo) * T1)) {
+                best = work; Ls = ls; T1 = t1;
+            }
         }
     }
 }
 
-// the launchers' copy of the arguments with the index divisors and the face-state tiles filled in
-inline Args3D with_divisors(const Args3D &a)
+// the launchers' copy of the arguments with the index divisors and the
+// face-state tiles filled in (halo: extra slope cells per line segment)
+inline Args3D with_divisors(const Args3D &a, int halo = 0)
 {
     Args3D b = a;
     for (int e = 0; e <= 4; e++) { b.fdx[e] = make_fastdiv((unsigned)a.nx + e); b.fdy[e] = make_fastdiv((unsigned)a.ny + e); }
     const int n[3] = {a.nx, a.ny, a.nz};
-    for (int d = 0; d < 3; d++) sflux_tile(d, n[d], d == 0 ? a.ny : a.nx, b.sf_len[d], b.sf_lines[d]);
+    for (int d = 0; d < 3; d++) sflux_tile(d, n[d], d == 0 ? a.ny : a.nx, halo, b.sf_len[d], b.sf_lines[d]);
     return b;
 }
 enum { AMR_SIG = 1, AMR_STATES = 2 };   // sigma (+ flattening); slopes, face states and fluxes
@@ -412,51 +415,20 @@ __global__ void __launch_bounds__(256) slope3d_kernel(const Args3D a, int d)
     }
 }
 
-// ---- face states of one cell in direction d ------------------------------------
-// One instantiation per reconstruction order, so the register allocation of
-// the PPM path (three eigensystems and slopes) and of the WENO path (one
-// eigensystem, five projected cells) do not add up.
-template <class R, int ORDER, bool AMR, int DIR>
-__device__ __forceinline__ void face_states(const Args3D &a, const Ctx3<R, AMR> &X, const double dt, const R dtn,
-                                            const R hdtn, const R hdtx, const R hdty, const R hdtz, int i, int j,
-                                            int k, R Wm_out[6], R Wp_out[6], R &gc_out, R &ge_out)
+// The face states of one cell from its interface values: flattening,
+// characteristic tracing, transverse terms, negativity fallback, gravity and
+// the 3-D full-CTU terms.  Sc: the cell's rotated primitives, vc its 8-vector.
+template <class R, bool AMR, int DIR>
+__device__ __forceinline__ void face_states_tail(const Args3D &a, const Ctx3<R, AMR> &X, const double dt, const R dtn,
+                                                 const R hdtn, const R hdtx, const R hdty, const R hdtz, int i, int j,
+                                                 int k, const R Sc[6], const R vc[8], const EigBase<R> &eb,
+                                                 const Eig<R> &e, R vecL[6], R vecR[6], R Wm_out[6], R Wp_out[6])
 {
     constexpr int d = DIR;
     const Grid3 &G = X.G;
-    int di, dj, dk;
-    offs(d, 1, di, dj, dk);
-    R S8[5][8], S[5][6], g[6];
-#pragma unroll
-    for (int o = -2; o <= 2; o++) {
-        if (ORDER == 3 && (o == -2 || o == 2)) continue;   // PPM reads its neighbours' slopes instead
-        X.load(a, i + o * di, j + o * dj, k + o * dk, S8[o + 2]);
-        six(S8[o + 2], g); rot3(d, g, S[o + 2]);
-    }
-    const R *vc = S8[2];
-    // the cell's eigensystem along d, and (CTU) along the two other directions
-    EigBase<R> eb;
-    if (!eigen_base(S[2][0], S[2][4], vc[GC], eb)) atomicOr(a.err, ERR_SOUND);
-    Eig<R> e;
-    eigen_dir(eb, S[2][1], e);
-    R vecL[6], vecR[6];
-    if constexpr (ORDER == 5) {
-        weno_interfaces(a.prm, e, S, vecL, vecR);
-    } else {
-        // slopes of the cell and its two neighbours from slope3d_kernel
-        const long ns = G.ns(d);
-        const long sN = G.sidx(d, i - di, j - dj, k - dk), s0 = G.sidx(d, i, j, k), sP = G.sidx(d, i + di, j + dj, k + dk);
-        R dbN[6], db0[6], dbP[6];
-#pragma unroll
-        for (int q = 0; q < 6; q++) {
-            dbN[q] = X.slp[(long)q * ns + sN];
-            db0[q] = X.slp[(long)q * ns + s0];
-            dbP[q] = X.slp[(long)q * ns + sP];
-        }
-        ppm_interfaces(S[1], S[2], S[3], dbN, db0, dbP, vecL, vecR);
-    }
-    if (a.prm.flattening) flatten(X.flat[(long)d * G.npad() + G.pidx(i, j, k)], S[2], vecL, vecR);
+    if (a.prm.flattening) flatten(X.flat[(long)d * G.npad() + G.pidx(i, j, k)], Sc, vecL, vecR);
     R wm[6], wp[6], Wm[6], Wp[6];
-    ppm_trace(e, dtn, hdtn, S[2], vecL, vecR, wm, wp);
+    ppm_trace(e, dtn, hdtn, Sc, vecL, vecR, wm, wp);
     unrot3(d, wm, Wm); unrot3(d, wp, Wp);
     // transverse terms, hy_dataReconstOneStep.F90:931-962
     R s1[6], s2[6];
@@ -520,15 +492,65 @@ __device__ __forceinline__ void face_states(const Args3D &a, const Ctx3<R, AMR> 
     }
 #pragma unroll
     for (int q = 0; q < 6; q++) { Wm_out[q] = Wm[q]; Wp_out[q] = Wp[q]; }
+}
+
+// ---- face states of one cell in direction d ------------------------------------
+// One instantiation per reconstruction order, so the register allocation of
+// the PPM path (three eigensystems and slopes) and of the WENO path (one
+// eigensystem, five projected cells) do not add up.
+template <class R, int ORDER, bool AMR, int DIR>
+__device__ __forceinline__ void face_states(const Args3D &a, const Ctx3<R, AMR> &X, const double dt, const R dtn,
+                                            const R hdtn, const R hdtx, const R hdty, const R hdtz, int i, int j,
+                                            int k, R Wm_out[6], R Wp_out[6], R &gc_out, R &ge_out)
+{
+    constexpr int d = DIR;
+    const Grid3 &G = X.G;
+    int di, dj, dk;
+    offs(d, 1, di, dj, dk);
+    R S8[5][8], S[5][6], g[6];
+#pragma unroll
+    for (int o = -2; o <= 2; o++) {
+        if (ORDER == 3 && (o == -2 || o == 2)) continue;   // PPM reads its neighbours' slopes instead
+        X.load(a, i + o * di, j + o * dj, k + o * dk, S8[o + 2]);
+        six(S8[o + 2], g); rot3(d, g, S[o + 2]);
+    }
+    const R *vc = S8[2];
+    // the cell's eigensystem along d, and (CTU) along the two other directions
+    EigBase<R> eb;
+    if (!eigen_base(S[2][0], S[2][4], vc[GC], eb)) atomicOr(a.err, ERR_SOUND);
+    Eig<R> e;
+    eigen_dir(eb, S[2][1], e);
+    R vecL[6], vecR[6];
+    if constexpr (ORDER == 5) {
+        weno_interfaces(a.prm, e, S, vecL, vecR);
+    } else {
+        // slopes of the cell and its two neighbours from slope3d_kernel
+        const long ns = G.ns(d);
+        const long sN = G.sidx(d, i - di, j - dj, k - dk), s0 = G.sidx(d, i, j, k), sP = G.sidx(d, i + di, j + dj, k + dk);
+        R dbN[6], db0[6], dbP[6];
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            dbN[q] = X.slp[(long)q * ns + sN];
+            db0[q] = X.slp[(long)q * ns + s0];
+            dbP[q] = X.slp[(long)q * ns + sP];
+        }
+        ppm_interfaces(S[1], S[2], S[3], dbN, db0, dbP, vecL, vecR);
+    }
+    face_states_tail<R, AMR, DIR>(a, X, dt, dtn, hdtn, hdtx, hdty, hdtz, i, j, k, S[2], vc, eb, e, vecL, vecR, Wm_out,
+                                  Wp_out);
     gc_out = vc[GC]; ge_out = vc[GE];
 }
+
 
 // ---- face states and Riemann fluxes as two kernels (FP64) --------------------------
 // In FP64 the fused kernel below measured slower on B200 (its barrier between
 // the face states and the fluxes idles two CTAs of long FP64 warps), so the
 // FP64 path stores all twelve face-state values and solves the Riemann
 // problems in a second kernel.  FP32 fuses them.
-template <class R> struct FusedFaces { static constexpr bool value = sizeof(R) == 4; };
+#ifndef FXB_FUSE_FP64
+#define FXB_FUSE_FP64 0
+#endif
+template <class R> struct FusedFaces { static constexpr bool value = sizeof(R) == 4 || FXB_FUSE_FP64; };
 // slots of the Wp and Wm pressures in the face-state arrays
 template <class R> struct PwSlots {
     static constexpr int wp = FusedFaces<R>::value ? 0 : P, wm = FusedFaces<R>::value ? 1 : 6 + P;
@@ -612,8 +634,10 @@ template <class R, int ORDER, bool AMR, int DIR>
 __global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) sflux3d_kernel(const Args3D a)
 {
     constexpr int d = DIR;
+    constexpr int H = ORDER == 3 ? 1 : 0;          // PPM: one slope cell either side of the face-state cells
     extern __shared__ __align__(16) unsigned char sflux_smem[];
     R *sW = reinterpret_cast<R *>(sflux_smem);     // [8][threads]: right-face state, then gamc, game
+    R *sD = sW + 8 * blockDim.x;                   // PPM: [6][threads] limited slopes
     const Ctx3<R, AMR> X(a);
     const Grid3 &G = X.G;
     const double dt = a.dtv ? a.dtv[0] : a.dt_arg;
@@ -622,21 +646,63 @@ __global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) 
     const R hdtx = R(0.5 * dt / X.dx), hdty = R(0.5 * dt / X.dy), hdtz = R(0.5 * dt / X.dz);
     const int N = d == 0 ? a.nx : d == 1 ? a.ny : a.nz;
     const int N1 = d == 0 ? a.ny : a.nx, N2 = d == 2 ? a.ny : a.nz;
-    const int Ls = a.sf_len[d], T1 = a.sf_lines[d], S = Ls - 1;
+    const int Ls = a.sf_len[d], T1 = a.sf_lines[d], S = Ls - 1, Lt = Ls + 2 * H;
     const int nseg = (N + S) / S, nt1 = (N1 + T1 - 1) / T1;
     const int t = threadIdx.x, nt = blockDim.x;
-    const int ld = d == 0 ? t % Ls : t / T1;
-    const int l1 = d == 0 ? t / Ls : t % T1;
+    const int ld = d == 0 ? t % Lt : t / T1;
+    const int l1 = d == 0 ? t / Lt : t % T1;
+    const int step = d == 0 ? 1 : T1;              // the neighbour along d, in threads
     int b = blockIdx.x;
     const int seg = b % nseg;
     b /= nseg;
     const int t1 = (b % nt1) * T1 + l1, t2 = b / nt1;
-    const int c = seg * S - 1 + ld;
-    const bool active = t1 < N1 && t2 < N2 && c <= N;
+    const int c = seg * S - 1 - H + ld;
+    const bool line = t1 < N1 && t2 < N2;
+    const bool st = line && ld >= H && ld < Lt - H && c <= N;   // a face-state cell
     const int i = d == 0 ? c : t1, j = d == 0 ? t1 : d == 1 ? c : t2, k = d == 2 ? c : t2;
     R Wm[6], Wp[6], gc = R(0), ge = R(0);
-    if (active) {
-        face_states<R, ORDER, AMR, DIR>(a, X, dt, dtn, hdtn, hdtx, hdty, hdtz, i, j, k, Wm, Wp, gc, ge);
+    if constexpr (ORDER == 3) {
+        // the slope of every cell of the segment and its two neighbours (cells
+        // -2 .. N+1), then the face states from the slopes in shared memory;
+        // a face-state cell reuses its slope's loads and eigensystem
+        R S8[3][8], Sr[3][6];
+        EigBase<R> eb;
+        Eig<R> e;
+        if (line && c <= N + 1) {
+            int di, dj, dk;
+            offs(d, 1, di, dj, dk);
+            R g[6];
+#pragma unroll
+            for (int o = -1; o <= 1; o++) {
+                X.load(a, i + o * di, j + o * dj, k + o * dk, S8[o + 1]);
+                six(S8[o + 1], g); rot3(d, g, Sr[o + 1]);
+            }
+            if (!eigen_base(Sr[1][0], Sr[1][4], S8[1][GC], eb)) atomicOr(a.err, ERR_SOUND);
+            eigen_dir(eb, Sr[1][1], e);
+            R db[6];
+            tvd_slope(a.prm, e, Sr[0], Sr[1], Sr[2], db);
+#pragma unroll
+            for (int q = 0; q < 6; q++) sD[q * nt + t] = db[q];
+        }
+        __syncthreads();
+        if (st) {
+            R dbN[6], db0[6], dbP[6], vecL[6], vecR[6];
+#pragma unroll
+            for (int q = 0; q < 6; q++) {
+                dbN[q] = sD[q * nt + t - step];
+                db0[q] = sD[q * nt + t];
+                dbP[q] = sD[q * nt + t + step];
+            }
+            ppm_interfaces(Sr[0], Sr[1], Sr[2], dbN, db0, dbP, vecL, vecR);
+            face_states_tail<R, AMR, DIR>(a, X, dt, dtn, hdtn, hdtx, hdty, hdtz, i, j, k, Sr[1], S8[1], eb, e, vecL,
+                                          vecR, Wm, Wp);
+            gc = S8[1][GC];
+            ge = S8[1][GE];
+        }
+    } else {
+        if (st) face_states<R, ORDER, AMR, DIR>(a, X, dt, dtn, hdtn, hdtx, hdty, hdtz, i, j, k, Wm, Wp, gc, ge);
+    }
+    if (st) {
 #pragma unroll
         for (int q = 0; q < 6; q++) sW[q * nt + t] = Wp[q];
         sW[6 * nt + t] = gc;
@@ -649,8 +715,8 @@ __global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) 
         }
     }
     __syncthreads();
-    if (active && ld >= 1) {
-        const int tl = d == 0 ? t - 1 : t - T1;
+    if (st && ld >= H + 1) {
+        const int tl = t - step;
         R VL[6], F[NF];
 #pragma unroll
         for (int q = 0; q < 6; q++) VL[q] = sW[q * nt + tl];
@@ -809,19 +875,21 @@ template <class R, bool AMR, int DIR> void launch_states3d(const Args3D &a, dim3
         const int Ls = a.sf_len[DIR], T1 = a.sf_lines[DIR];
         const int nseg = (N + Ls - 1) / (Ls - 1), nt1 = (N1 + T1 - 1) / T1;
         const dim3 gs((unsigned)(nseg * nt1 * N2), g.y);
-        const size_t sm = 8 * sizeof(R) * (size_t)(Ls * T1);
         if (a.prm.order == 5) {
-            sflux3d_kernel<R, 5, AMR, DIR><<<gs, Ls * T1, sm, s>>>(a);
-        } else {
-            slope3d_kernel<R, AMR><<<g, 256, 0, s>>>(a, DIR);
-            sflux3d_kernel<R, 3, AMR, DIR><<<gs, Ls * T1, sm, s>>>(a);
+            sflux3d_kernel<R, 5, AMR, DIR><<<gs, Ls * T1, 8 * sizeof(R) * (size_t)(Ls * T1), s>>>(a);
+        } else {   // the slopes are computed in the kernel: two more cells per line
+            const int nt = (Ls + 2) * T1;
+            sflux3d_kernel<R, 3, AMR, DIR><<<gs, nt, 14 * sizeof(R) * (size_t)nt, s>>>(a);
         }
     }
 }
 
+// slope cells a face-state tile adds per line: two when the FP32 kernel computes the PPM slopes itself
+template <class R> int sflux_halo(const Args3D &a) { return (FusedFaces<R>::value && a.prm.order == 3) ? 2 : 0; }
+
 template <class R> void launch_hydro3d_t(const Args3D &a0, cudaStream_t s)
 {
-    const Args3D a = with_divisors(a0);
+    const Args3D a = with_divisors(a0, sflux_halo<R>(a0));
     const int nb = 148 * 8;
     if (a.prm.flattening) flat3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
     sig3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
@@ -900,7 +968,7 @@ __global__ void __launch_bounds__(256) amr_correct_flux_kernel(const Args3D a, c
 // grid-stride kernels (the face-state kernel has its own tiles).
 template <class R> void launch_amr3d_fluxes_t(const Args3D &a0, int entries, int which, cudaStream_t s)
 {
-    const Args3D a = with_divisors(a0);
+    const Args3D a = with_divisors(a0, sflux_halo<R>(a0));
     if ((which & AMR_SIG) && a.prm.flattening) flat3d_kernel<R, true><<<dim3(a.cta[0], entries), 256, 0, s>>>(a);
     if (which & AMR_SIG) sig3d_kernel<R, true><<<dim3(a.cta[0], entries), 256, 0, s>>>(a);
     if (which & AMR_STATES) {
