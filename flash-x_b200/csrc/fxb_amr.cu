@@ -103,6 +103,10 @@ struct State {
     int *d_poff = nullptr;
     long nprol = 0;
     int2 *d_rlist = nullptr;                      // parent cells the plan needs, per level (restriction order)
+    std::vector<int> act_blk;                     // leaves and parents with a leaf child (refinement marking)
+    int *d_active = nullptr;
+    unsigned *d_act_eos = nullptr, *d_act_bnd = nullptr;
+    double *d_ext = nullptr, *d_err = nullptr;    // marking scratch, allocated at the first marking
     std::vector<long> rlist_off;                  // per level offset into d_rlist, size maxlev + 1
     int cta[4] = {4, 4, 4, 4};                    // CTAs per block: sig, slopes, (unused), update
     int fill_cta = 8;
@@ -661,6 +665,118 @@ __global__ void __launch_bounds__(256, FXB_FILL_MINB) amr_prolong_kernel(MeshArg
     }
 }
 
+// ---- refinement marking (Grid_markRefineDerefine) -------------------------------
+// guard-filled copy of one variable of every active block (leaves and parents
+// with a leaf child), all 4 guard layers, Eos on the guard regions of the
+// block's Eos mask when need_eos (the variable is an Eos output)
+__global__ void __launch_bounds__(256) amr_ext_fill_kernel(MeshArgs m, const int *active, const unsigned *act_eos,
+                                                           int dv, int need_eos, double *ext, DevParams prm,
+                                                           double gam1inv, double ggprodinv)
+{
+    const int sb = blockIdx.y;
+    const int b = active[sb];
+    const DevBlk B = m.blk[b];
+    const unsigned mask = act_eos[sb];
+    const int n = m.n, g = m.ng, ne = n + 2 * g;
+    const int ncell = ne * ne * ne;
+    double *E = ext + (long)sb * ncell;
+    for (int idx = (int)(blockIdx.x * blockDim.x + threadIdx.x); idx < ncell; idx += (int)(gridDim.x * blockDim.x)) {
+        int i, j, k;
+        unflatten(idx, ne, ne, i, j, k);
+        i -= g; j -= g; k -= g;
+        const int ri = i < 0 ? -1 : i >= n ? 1 : 0, rj = j < 0 ? -1 : j >= n ? 1 : 0, rk = k < 0 ? -1 : k >= n ? 1 : 0;
+        double u[NV_DEV];
+        if (!(ri | rj | rk)) {
+            const double *s = m.store + (long)b * m.bstride + ((long)k * n + j) * n + i;
+#pragma unroll
+            for (int v = 0; v < NV_DEV; v++) u[v] = s[v * m.vstride];
+        } else {
+            const int x[3] = {B.c0 * n + i, B.c1 * n + j, B.c2 * n + k};
+            if (!guard_value(m, b, x, u)) {
+                atomicOr(m.err, ERR_AMR);
+#pragma unroll
+                for (int v = 0; v < NV_DEV; v++) u[v] = 0.;
+            } else if (need_eos && ((mask >> ((rk + 1) * 9 + (rj + 1) * 3 + (ri + 1))) & 1u)) {
+                eos_cell_dev(u, prm, gam1inv, ggprodinv);
+            }
+        }
+        double val = u[0];
+#pragma unroll
+        for (int v = 1; v < NV_DEV; v++) if (v == dv) val = u[v];
+        E[idx] = val;
+    }
+}
+
+// gr_estimateBlkError (GridMain/AMR/gr_estimateBlkError.F90, Cartesian) of
+// every active block: the largest ratio of second differences to first
+// differences plus filter times magnitudes over the cells grd = max(NGUARD-2, 2)
+// layers in from the guard-cell edge (not past the interior at a non-periodic
+// domain boundary); the first differences are recomputed per use with the
+// same operations.  One CTA per block.  A cell with zero denominator and
+// nonzero numerator makes the error HUGE, as the reference's assignment does
+// whenever the other ratios are finite.
+__global__ void __launch_bounds__(256) amr_error_kernel(const double *ext, const unsigned *act_bnd, const int *active,
+                                                        const DevBlk *blk, const double *dxl, int n, int g,
+                                                        double filter, double *err)
+{
+    __shared__ double smax[8];
+    __shared__ int shuge[8];
+    const int sb = blockIdx.x;
+    const int ne = n + 2 * g;
+    const double *E = ext + (long)sb * ne * ne * ne;
+    const int lev = blk[active[sb]].level;
+    const double del[3] = {0.5e0 / dxl[3 * (lev - 1)], 0.5e0 / dxl[3 * (lev - 1) + 1], 0.5e0 / dxl[3 * (lev - 1) + 2]};
+    const unsigned bnd = act_bnd[sb];
+    const int grd = g - 2 > 2 ? g - 2 : 2;
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; a++) {
+        lo[a] = ((bnd >> a) & 1u) ? (grd > g ? grd : g) : grd;
+        hi[a] = ((bnd >> (3 + a)) & 1u) ? (ne - 1 - grd < g + n - 1 ? ne - 1 - grd : g + n - 1) : ne - 1 - grd;
+    }
+    const int lx = hi[0] - lo[0] + 1, ly = hi[1] - lo[1] + 1, lz = hi[2] - lo[2] + 1;
+    const int st[3] = {1, ne, ne * ne};
+    double m = 0.;
+    int huge = 0;
+    for (int t = threadIdx.x; t < lx * ly * lz; t += blockDim.x) {
+        const int i = lo[0] + t % lx, j = lo[1] + (t / lx) % ly, k = lo[2] + t / (lx * ly);
+        const int p = (k * ne + j) * ne + i;
+        // (1,x) (1,y) (2,x) (2,y) (1,z) (2,z) (3,x) (3,y) (3,z)
+        const int comp[9] = {0, 0, 1, 1, 0, 1, 2, 2, 2}, axis[9] = {0, 1, 0, 1, 2, 2, 0, 1, 2};
+        double num = 0., denom = 0.;
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+            const int c = comp[q], ax = axis[q];
+            const int pp = p + st[ax], pm = p - st[ax];
+            const double dup = (E[pp + st[c]] - E[pp - st[c]]) * del[c];
+            const double dum = (E[pm + st[c]] - E[pm - st[c]]) * del[c];
+            const double duap = (fabs(E[pp + st[c]]) + fabs(E[pp - st[c]])) * del[c];
+            const double duam = (fabs(E[pm + st[c]]) + fabs(E[pm - st[c]])) * del[c];
+            const double d2 = (dup - dum) * del[ax];
+            const double d3 = (fabs(dup) + fabs(dum)) * del[ax];
+            const double d4 = (duap + duam) * del[ax];
+            num = num + d2 * d2;
+            const double s2 = d3 + (filter * d4);
+            denom = denom + s2 * s2;
+        }
+        if (denom == 0.0 && num != 0.0) huge = 1;
+        else if (denom != 0.0) m = fmax2(m, num / denom);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        m = fmax2(m, __shfl_xor_sync(0xffffffffu, m, off));
+        huge |= __shfl_xor_sync(0xffffffffu, huge, off);
+    }
+    if ((threadIdx.x & 31) == 0) { smax[threadIdx.x >> 5] = m; shuge[threadIdx.x >> 5] = huge; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0.;
+        int h = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) { r = fmax2(r, smax[w]); h |= shuge[w]; }
+        if (h) r = fmax2(0x1.fffffffffffffp+1023, r);
+        err[sb] = sqrt(r);
+    }
+}
+
 // restriction of parent cell c of block p from its eight children cells
 // (amr_restrict_unk_genorder, order 1): conserved form, weights 1/8 in k, j, i order
 __device__ __forceinline__ void restrict_cell(double *store, long vstride, long bstride, int n, int p, int c,
@@ -971,6 +1087,7 @@ void amr_destroy()
     for (int d = 0; d < 3; d++) { dfree(S.w[d]); dfree(S.f[d]); }
     dfree(S.bflux); dfree(S.stage); dfree(S.d_dmap); dfree(S.d_glist);
     dfree(S.d_plan); dfree(S.d_prol); dfree(S.d_poff); dfree(S.d_rlist);
+    dfree(S.d_active); dfree(S.d_act_eos); dfree(S.d_act_bnd); dfree(S.d_ext); dfree(S.d_err);
     S = State();
 }
 
@@ -1144,6 +1261,25 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
                     if (need[(size_t)p * S.vstride + cidx]) rl.push_back(make_int2(p, cidx));
         }
         CKA(up(S.d_rlist, rl));
+    }
+    // active blocks for refinement marking: Eos masks and non-periodic domain faces
+    {
+        std::vector<unsigned> aeos, abnd;
+        for (int b = 0; b < S.nblk; b++) {
+            const HBlock &B = S.blk[b];
+            if (B.nodetype != 1 && B.nodetype != 2) continue;
+            S.act_blk.push_back(b);
+            aeos.push_back(eos_regions(b));
+            unsigned bits = 0;
+            for (int a = 0; a < 3; a++) {
+                if (B.c[a] == 0 && D.bc[2 * a] != FXB_BC_PERIODIC) bits |= 1u << a;
+                if (B.c[a] == nb_at(B.level, a) - 1 && D.bc[2 * a + 1] != FXB_BC_PERIODIC) bits |= 1u << (3 + a);
+            }
+            abnd.push_back(bits);
+        }
+        CKA(up(S.d_active, S.act_blk));
+        CKA(up(S.d_act_eos, aeos));
+        CKA(up(S.d_act_bnd, abnd));
     }
     const size_t r = rsize();
     S.nfc = (long)S.n * S.n;
@@ -1367,6 +1503,53 @@ int amr_locate(unsigned long long *key)
     amr_locate_kernel<<<grid, 256, 0, S.C.stream>>>(S.store[S.cur], S.vstride, S.bstride, S.n, S.leaf_blk_dev, S.d_blk,
                                                     S.d_dxl, S.nleaf, S.C.rate_max, key);
     CKA(cudaGetLastError());
+    return FXB_OK;
+}
+
+int amr_mark_refine(int nvars, const int *dvar, const int *need_eos, const double *refine_cutoff,
+                    const double *derefine_cutoff, const double *refine_filter, int max_refine, int *flags,
+                    double *error_out)
+{
+    const int nact = (int)S.act_blk.size();
+    const long next = ne3();
+    if (!S.d_ext) {
+        CKA(cudaMalloc(&S.d_ext, sizeof(double) * next * std::max(1, nact)));
+        CKA(cudaMalloc(&S.d_err, sizeof(double) * std::max(1, nact)));
+    }
+    restrict_all(S.cur);
+    std::vector<double> err(S.nblk, 0.), e(nact);
+    std::vector<unsigned char> refine(S.nblk, 0), derefine(S.nblk, 0), stay(S.nblk, 0);
+    int any_eos = 0;
+    for (int l = 0; l < nvars; l++) any_eos |= need_eos[l];
+    for (int l = 0; l < nvars; l++) {
+        amr_ext_fill_kernel<<<dim3(8, nact), 256, 0, S.C.stream>>>(mesh_args(S.cur), S.d_active, S.d_act_eos, dvar[l],
+                                                                  any_eos, S.d_ext, S.C.dprm, S.C.gam1inv,
+                                                                  S.C.ggprodinv);
+        amr_error_kernel<<<nact, 256, 0, S.C.stream>>>(S.d_ext, S.d_act_bnd, S.d_active, S.d_blk, S.d_dxl, S.n, S.ng,
+                                                       refine_filter[l], S.d_err);
+        CKA(cudaGetLastError());
+        CKA(cudaMemcpyAsync(e.data(), S.d_err, sizeof(double) * nact, cudaMemcpyDeviceToHost, S.C.stream));
+        CKA(cudaStreamSynchronize(S.C.stream));
+        // Paramesh4/gr_markRefineDerefine.F90:110-160
+        std::fill(err.begin(), err.end(), 0.);
+        for (int s = 0; s < nact; s++) err[S.act_blk[s]] = e[s];
+        for (int b : S.act_blk) {
+            const HBlock &B = S.blk[b];
+            const double ep = B.parent >= 0 ? err[B.parent] : 0.;
+            if (B.nodetype == 1 && !refine[b] && !stay[b] && err[b] <= derefine_cutoff[l] && ep <= derefine_cutoff[l])
+                derefine[b] = 1;
+            else
+                derefine[b] = 0;
+            if (err[b] > refine_cutoff[l]) { derefine[b] = 0; refine[b] = 1; }
+            if ((B.nodetype == 1 && err[b] > derefine_cutoff[l]) || ep > derefine_cutoff[l]) stay[b] = 1;
+            if (B.level >= max_refine) refine[b] = 0;
+        }
+    }
+    for (int l = 0; l < S.nleaf; l++) {
+        const int b = S.leaf_blk[l];
+        flags[l] = refine[b] ? 1 : derefine[b] ? -1 : 0;
+        if (error_out) error_out[l] = err[b];
+    }
     return FXB_OK;
 }
 

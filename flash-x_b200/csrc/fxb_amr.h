@@ -39,6 +39,11 @@ long amr_leaf_cells();
 // first leaf cell (leaf, k, j, i linear index) whose CFL rate equals the reduced maximum
 int amr_locate(unsigned long long *key);
 int amr_leaf_level(int leaf);
+// Grid_markRefineDerefine on the leaves; dvar: device variables, need_eos:
+// the variable is an Eos output (the guard regions get the Eos)
+int amr_mark_refine(int nvars, const int *dvar, const int *need_eos, const double *refine_cutoff,
+                    const double *derefine_cutoff, const double *refine_filter, int max_refine, int *flags,
+                    double *error_out);
 // the launch shape chosen at the last attach, as text
 const char *amr_tuning_log();
 

@@ -723,6 +723,30 @@ extern "C" int fxb_integrals(double out[7])
     return FXB_OK;
 }
 
+extern "C" int fxb_mark_refine_derefine(int nvars, const int *refine_var, const double *refine_cutoff,
+                                        const double *derefine_cutoff, const double *refine_filter, int max_refine,
+                                        int *flags, double *error)
+{
+    if (!L.attached) return fail(FXB_EARG, "fxb_mark_refine_derefine: no UNK attached");
+    if (!amr_active()) return fail(FXB_EUNSUPPORTED, "fxb_mark_refine_derefine: needs a registered AMR mesh");
+    if (nvars <= 0 || nvars > FXB_NVAR || !refine_var || !refine_cutoff || !derefine_cutoff || !refine_filter || !flags)
+        return fail(FXB_EARG, "fxb_mark_refine_derefine: bad argument");
+    int dvar[FXB_NVAR], need_eos[FXB_NVAR];
+    for (int l = 0; l < nvars; l++) {
+        dvar[l] = -1;
+        for (int v = 0; v < NV_DEV; v++)
+            if (kDevToVar[v] == refine_var[l]) dvar[l] = v;
+        if (dvar[l] < 0) return fail(FXB_EARG, "fxb_mark_refine_derefine: unknown refinement variable");
+        // gr_makeMaskConsistent.F90:376-395 (one temperature, MODE_DENS_EI, constant gamc)
+        const int r = refine_var[l];
+        need_eos[l] = r == FXB_PRES || r == FXB_TEMP || r == FXB_ENER || r == FXB_EINT || r == FXB_GAME;
+    }
+    int rc = amr_mark_refine(nvars, dvar, need_eos, refine_cutoff, derefine_cutoff, refine_filter, max_refine, flags,
+                             error);
+    if (rc) return rc;
+    return check_err_word();
+}
+
 extern "C" int fxb_last_timing(double *ms, int *kernel_launches)
 {
     if (!L.timing_valid) return fail(FXB_EARG, "fxb_last_timing: nothing timed yet");

@@ -29,8 +29,8 @@ FXB_VARS = ("dens", "eint", "ener", "gamc", "game", "pres", "temp", "velx", "vel
 # entry points declared in include/flashx_b200.h
 ABI_SYMBOLS = ("fxb_init", "fxb_register_blocks", "fxb_attach_unk", "fxb_fill_guardcells",
                "fxb_hydro_step", "fxb_compute_dt", "fxb_advance", "fxb_eos", "fxb_sync_to_host",
-               "fxb_sync_from_host", "fxb_integrals", "fxb_integrals_noalloc", "fxb_last_timing", "fxb_stream", "fxb_tuning",
-               "fxb_last_error", "fxb_finalize")
+               "fxb_sync_from_host", "fxb_integrals", "fxb_integrals_noalloc", "fxb_mark_refine_derefine",
+               "fxb_last_timing", "fxb_stream", "fxb_tuning", "fxb_last_error", "fxb_finalize")
 
 
 class FxbParams(ctypes.Structure):
@@ -258,6 +258,25 @@ class HydroDevice:
         out = np.zeros(7)
         _check(self.lib.fxb_integrals(_dp(out)))
         return out
+
+    def Grid_markRefineDerefine(self, refine_vars, max_refine):
+        """Grid_markRefineDerefine on the registered AMR mesh.  refine_vars:
+        (variable name, refine_cutoff, derefine_cutoff, refine_filter) per
+        refinement variable, names as in UNK ("dens", "pres", ...).
+        Returns (flags, errors) per leaf: 1 refine, -1 derefine, 0 neither;
+        the error estimate of the last variable."""
+        nv = len(refine_vars)
+        ids = [FXB_VARS.index(r[0]) for r in refine_vars]
+        iv = (ctypes.c_int * nv)(*ids)
+        rc_ = (ctypes.c_double * nv)(*[float(r[1]) for r in refine_vars])
+        dc = (ctypes.c_double * nv)(*[float(r[2]) for r in refine_vars])
+        fl = (ctypes.c_double * nv)(*[float(r[3]) for r in refine_vars])
+        n = self.unk_shape[0]
+        flags = np.zeros(n, dtype=np.int32)
+        err = np.zeros(n)
+        _check(self.lib.fxb_mark_refine_derefine(nv, iv, rc_, dc, fl, int(max_refine),
+                                                 flags.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(err)))
+        return flags, err
 
     def tuning(self):
         """The launch shape in use (the batched-block path tunes it at attach)."""

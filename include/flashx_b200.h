@@ -148,6 +148,22 @@ int fxb_sync_to_host(double *unk_host);
 int fxb_sync_from_host(const double *unk_host);
 /* Volume integrals: mass, x/y/z momentum, total, internal, kinetic energy. */
 int fxb_integrals(double out[7]);
+/* Grid_markRefineDerefine (Grid/GridMain/AMR/Grid_markRefineDerefine.F90:77-150)
+ * on the registered AMR mesh, from the attached state: a guard fill of the
+ * leaves and of the parents with a leaf child (Eos on the guard regions when
+ * a refinement variable is an Eos output: pres, temp, ener, eint or game),
+ * then per refinement variable the error of gr_estimateBlkError.F90 for every
+ * such block and the marks of Paramesh4/gr_markRefineDerefine.F90:110-160.
+ * refine_var[nvars]: fxb_var ids; the cutoffs and filters are the runtime
+ * parameters refine_cutoff_#, derefine_cutoff_#, refine_filter_#;
+ * max_refine = lrefine_max.  flags[nleaf] (registration order): 1 refine,
+ * -1 derefine, 0 neither; error[nleaf] (may be NULL): the error estimate of
+ * the last variable.  The tree update itself stays with the caller's PARAMESH
+ * (amr_refine_derefine), after which the new leaf list is registered again.
+ * FXB_EUNSUPPORTED on a uniform grid. */
+int fxb_mark_refine_derefine(int nvars, const int *refine_var, const double *refine_cutoff,
+                             const double *derefine_cutoff, const double *refine_filter, int max_refine,
+                             int *flags, double *error);
 /* Volume integrals of caller-owned device arrays without allocating any
  * device memory (no counterpart in the reference: an addition of this
  * library).  For callers that cannot call cudaMalloc, e.g. a Fortran code

@@ -27,6 +27,7 @@
  */
 #include "fx_oracle.h"
 
+#include <float.h>
 #include <limits.h>
 #include <math.h>
 #include <stdlib.h>

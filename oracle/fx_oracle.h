@@ -108,6 +108,12 @@ int fxo_amr_fill_guardcells(fxo_amr *a, double *unk);
 int fxo_amr_hydro_step(fxo_amr *a, double *unk, double dt, int nthreads);
 int fxo_amr_compute_dt(const fxo_amr *a, const double *unk, double *dt_out);
 int fxo_amr_integrals(const fxo_amr *a, const double *unk, double out[7]);
+/* Grid_markRefineDerefine on the leaves: flags[leaf] = 1 refine, -1 derefine,
+ * 0 neither; error_out[leaf] (may be NULL) the error of the last variable;
+ * ivar: UNK indices (FXO_DENS ...); 0 or 6 (guard cell without a source). */
+int fxo_amr_mark_refine(fxo_amr *a, const double *unk, int nvars, const int *ivar, const double *refine_cutoff,
+                        const double *derefine_cutoff, const double *refine_filter, int max_refine, int *flags,
+                        double *error_out);
 
 #ifdef __cplusplus
 }

@@ -81,6 +81,7 @@ def lib():
         L.fxo_amr_hydro_step.argtypes = [ctypes.c_void_p, D, ctypes.c_double, ctypes.c_int]
         L.fxo_amr_compute_dt.argtypes = [ctypes.c_void_p, D, D]
         L.fxo_amr_integrals.argtypes = [ctypes.c_void_p, D, D]
+        L.fxo_amr_mark_refine.argtypes = [ctypes.c_void_p, D, ctypes.c_int, I, D, D, D, ctypes.c_int, I, D]
         _lib = L
     return _lib
 
@@ -221,6 +222,25 @@ class Amr:
         if rc:
             raise RuntimeError("oracle: computed dt is not positive")
         return out.value
+
+    def mark_refine_derefine(self, unk, refine_vars, max_refine):
+        """Grid_markRefineDerefine on the leaves.  refine_vars: (UNK index,
+        refine_cutoff, derefine_cutoff, refine_filter) per refinement variable.
+        Returns (flags, errors): 1 refine, -1 derefine, 0 neither; the error
+        estimate of the last variable per leaf."""
+        nv = len(refine_vars)
+        iv = (ctypes.c_int * nv)(*[int(r[0]) for r in refine_vars])
+        rc_ = (ctypes.c_double * nv)(*[float(r[1]) for r in refine_vars])
+        dc = (ctypes.c_double * nv)(*[float(r[2]) for r in refine_vars])
+        fl = (ctypes.c_double * nv)(*[float(r[3]) for r in refine_vars])
+        flags = np.zeros(self.nleaf, dtype=np.int32)
+        err = np.zeros(self.nleaf)
+        I = ctypes.POINTER(ctypes.c_int)
+        rc = lib().fxo_amr_mark_refine(self.h, _dp(unk), nv, iv, rc_, dc, fl, int(max_refine),
+                                       flags.ctypes.data_as(I), _dp(err))
+        if rc:
+            raise RuntimeError(f"oracle AMR refinement marking failed with code {rc}")
+        return flags, err
 
     def integrals(self, unk):
         out = np.zeros(7)

@@ -163,3 +163,25 @@ def test_amr_compute_dt_location(need_gpu):
     assert loc == _expected_loc(root, unk, mesh.levels, dl)
     assert loc[3] == int(mesh.levels[loc[4] - 1])
     dev.close()
+
+
+@pytest.mark.parametrize("bc,maxlev,crit,max_refine", [
+    ((BC_PERIODIC,) * 6, 3, [("dens", 0.8, 0.2, 0.01)], 4),
+    ((BC_OUTFLOW, BC_OUTFLOW, BC_PERIODIC, BC_PERIODIC, BC_REFLECTING, BC_REFLECTING), 2,
+     [("pres", 0.5, 0.05, 0.01), ("dens", 0.3, 0.1, 0.02)], 2),
+])
+def test_mark_refine_derefine_matches_oracle(oracle, need_gpu, bc, maxlev, crit, max_refine):
+    """Grid_markRefineDerefine: the error estimates of every leaf bit for bit
+    (guard fill of leaves and parents, Eos for the pressure criterion, the
+    domain-boundary ranges) and the refine/derefine marks."""
+    root, hp, mesh, unk = _case(bc, maxlev)
+    am = oracle.Amr(oracle.make_params(root.as_dict(), hp), mesh.levels, mesh.bcoords)
+    names = {"dens": DENS, "pres": PRES}
+    ref_flags, ref_err = am.mark_refine_derefine(unk, [(names[c[0]],) + tuple(c[1:]) for c in crit], max_refine)
+    dev = HydroDevice(root, hp, "fp64", mesh=mesh)
+    dev.attach_unk(unk.copy())
+    flags, err = dev.Grid_markRefineDerefine(crit, max_refine)
+    assert np.array_equal(err, ref_err)
+    assert np.array_equal(flags, ref_flags)
+    assert set(np.unique(flags)) <= {-1, 0, 1} and np.any(err > 0)
+    dev.close()
