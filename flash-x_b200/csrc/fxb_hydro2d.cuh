@@ -58,11 +58,13 @@ constexpr int NDB = (T2 + 4) * T2; // 320 slope cells
 constexpr int NW = (T2 + 2) * T2;  // 288 face-state cells
 constexpr int NFC = (T2 + 1) * T2; // 272 faces
 
-// The FP32 path keeps the slope stage's eigensystem in shared memory for the
-// state stage; the FP64 path recomputes it (identical operations), because the
-// extra 23 KB and the register traffic cost it more than the four divisions
-// and one square root it saves (measured on B200).
-template <class R> struct CacheEig { static constexpr bool value = sizeof(R) == 4; };
+// The FP32 path keeps the direction-independent part of each slope cell's
+// eigensystem (the four values that cost a square root and three divisions)
+// in shared memory for the state stage of the same direction, and the FP64
+// update inputs of the owner cells (OWN).  The FP64 path recomputes the
+// eigensystem: its 10 KB more shared memory leaves too little L1 for its
+// register spills (29 % slower measured on B200).
+template <class R> struct KeepOwn { static constexpr bool value = sizeof(R) == 4; };
 
 constexpr int NOWN = T2 * T2;      // owner cells of a tile
 
@@ -71,10 +73,10 @@ template <class R> struct Smem2D {
     R DBF[NF * NFC];               // slopes [6][NDB], then fluxes [8][NFC]
     R SG[6][NDB];                  // sigma of the other direction at the slope cells (global order)
     R W[12][NW];                   // Wp (D,VX,VY,VZ,P,EI), then Wm
-    R EG[9][CacheEig<R>::value ? NDB : 1];   // eigensystem of the slope cells (PPM)
+    R EB[4][KeepOwn<R>::value ? NDB : 1];   // eigensystem base of the slope cells: cf, ahinv, lp, a2inv
     // FP64 update inputs of the owner cells that the window does not hold
     // exactly: ENER, and in the FP32 path also D, VX, VY, VZ, EINT
-    double OWN[CacheEig<R>::value ? 6 : 1][NOWN];
+    double OWN[KeepOwn<R>::value ? 6 : 1][NOWN];
 };
 
 // rotate a global-order 6-vector (D,VX,VY,VZ,P,EI) into sweep order
@@ -114,6 +116,7 @@ __device__ __forceinline__ void analysis_stage(const Args2D &a, Smem2D<R> &s, in
     // one eigensystem base for the slope direction and the transverse one
     EigBase<R> eb;
     if (!eigen_base(g[0], g[4], s.V[GC][wy][wx], eb)) set_err(a.err, ERR_SOUND);
+    if (KeepOwn<R>::value) { s.EB[0][t] = eb.cf; s.EB[1][t] = eb.ahinv; s.EB[2][t] = eb.lp; s.EB[3][t] = eb.a2inv; }
     if (ppm) {
         const int ox = dir == 0, oy = dir == 1;
         R gm[6], gp[6], Vm[6], Vp[6], db[6];
@@ -124,10 +127,6 @@ __device__ __forceinline__ void analysis_stage(const Args2D &a, Smem2D<R> &s, in
         tvd_slope(a.prm, e, Vm, c, Vp, db);
 #pragma unroll
         for (int k = 0; k < 6; k++) s.DBF[k * NDB + t] = db[k];
-        if (CacheEig<R>::value) {
-            s.EG[0][t] = e.lam0; s.EG[1][t] = e.un; s.EG[2][t] = e.lam4; s.EG[3][t] = e.cf; s.EG[4][t] = e.rho;
-            s.EG[5][t] = e.ahinv; s.EG[6][t] = e.lp; s.EG[7][t] = e.a2inv; s.EG[8][t] = e.rp;
-        }
     }
     const int td = 1 - dir, tx = td == 0, ty = td == 1;
     R gm[6], gp[6], m[6], p[6], sr[6], sg[6];
@@ -151,9 +150,17 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
     const int ox = dir == 0, oy = dir == 1;
     R g[6], Vm[6], Vc[6], Vp[6], vecL[6], vecR[6], Wm[6], Wp[6];
     win6(s, wx, wy, g); rot(dir, g, Vc);
+    // the cell's eigensystem along dir (FP32: from the base the slope stage kept)
     Eig<R> e;
-    if (a.prm.order == 5 || !CacheEig<R>::value)
-        if (!eigen(Vc[0], Vc[1], Vc[4], s.V[GC][wy][wx], e)) set_err(a.err, ERR_SOUND);
+    if (KeepOwn<R>::value) {
+        EigBase<R> eb;
+        eb.cf = s.EB[0][dbi]; eb.ahinv = s.EB[1][dbi]; eb.lp = s.EB[2][dbi]; eb.a2inv = s.EB[3][dbi];
+        eb.rho = Vc[0];
+        eb.rp = eb.rho * (eb.cf * eb.cf);
+        eigen_dir(eb, Vc[1], e);
+    } else if (!eigen(Vc[0], Vc[1], Vc[4], s.V[GC][wy][wx], e)) {
+        set_err(a.err, ERR_SOUND);
+    }
     if (a.prm.order == 5) {
         R S[5][6];
 #pragma unroll
@@ -162,11 +169,6 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
 #pragma unroll
         for (int k = 0; k < 6; k++) { Vm[k] = S[1][k]; Vp[k] = S[3][k]; }
     } else {
-        if (CacheEig<R>::value) {   // the slope stage computed this cell's eigensystem
-            e.lam0 = s.EG[0][dbi]; e.un = s.EG[1][dbi]; e.lam4 = s.EG[2][dbi]; e.cf = s.EG[3][dbi];
-            e.rho = s.EG[4][dbi]; e.ahinv = s.EG[5][dbi]; e.lp = s.EG[6][dbi]; e.a2inv = s.EG[7][dbi];
-            e.rp = s.EG[8][dbi];
-        }
         win6(s, wx - ox, wy - oy, g); rot(dir, g, Vm);
         win6(s, wx + ox, wy + oy, g); rot(dir, g, Vp);
         R dbN[6], db0[6], dbP[6];
@@ -250,15 +252,15 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
                 buf[q] = v == VX ? val * sx : (v == VY ? val * sy : val);
             }
         }
-        double own[CacheEig<R>::value ? 6 : 1];
+        double own[KeepOwn<R>::value ? 6 : 1];
         if (owner) {
             own[0] = __ldg(a.in + DV_ENER * a.vstride + gidx);
-            if (CacheEig<R>::value) {
-                own[CacheEig<R>::value ? 1 : 0] = __ldg(a.in + D * a.vstride + gidx);
-                own[CacheEig<R>::value ? 2 : 0] = __ldg(a.in + VX * a.vstride + gidx);
-                own[CacheEig<R>::value ? 3 : 0] = __ldg(a.in + VY * a.vstride + gidx);
-                own[CacheEig<R>::value ? 4 : 0] = __ldg(a.in + VZ * a.vstride + gidx);
-                own[CacheEig<R>::value ? 5 : 0] = __ldg(a.in + EI * a.vstride + gidx);
+            if (KeepOwn<R>::value) {
+                own[KeepOwn<R>::value ? 1 : 0] = __ldg(a.in + D * a.vstride + gidx);
+                own[KeepOwn<R>::value ? 2 : 0] = __ldg(a.in + VX * a.vstride + gidx);
+                own[KeepOwn<R>::value ? 3 : 0] = __ldg(a.in + VY * a.vstride + gidx);
+                own[KeepOwn<R>::value ? 4 : 0] = __ldg(a.in + VZ * a.vstride + gidx);
+                own[KeepOwn<R>::value ? 5 : 0] = __ldg(a.in + EI * a.vstride + gidx);
             }
         }
 #pragma unroll
@@ -272,7 +274,7 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
         }
         if (owner) {
 #pragma unroll
-            for (int q = 0; q < (CacheEig<R>::value ? 6 : 1); q++) s.OWN[q][tid] = own[q];
+            for (int q = 0; q < (KeepOwn<R>::value ? 6 : 1); q++) s.OWN[q][tid] = own[q];
         }
     }
     __syncthreads();
@@ -306,10 +308,10 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
     const double dtdx = dt / a.dx, dtdy = dt / a.dy;
     if (owner) {
         double vx, vy, vz, en = s.OWN[0][tid];
-        if (CacheEig<R>::value) {
-            dens0 = s.OWN[CacheEig<R>::value ? 1 : 0][tid]; vx = s.OWN[CacheEig<R>::value ? 2 : 0][tid];
-            vy = s.OWN[CacheEig<R>::value ? 3 : 0][tid]; vz = s.OWN[CacheEig<R>::value ? 4 : 0][tid];
-            eint0 = s.OWN[CacheEig<R>::value ? 5 : 0][tid];
+        if (KeepOwn<R>::value) {
+            dens0 = s.OWN[KeepOwn<R>::value ? 1 : 0][tid]; vx = s.OWN[KeepOwn<R>::value ? 2 : 0][tid];
+            vy = s.OWN[KeepOwn<R>::value ? 3 : 0][tid]; vz = s.OWN[KeepOwn<R>::value ? 4 : 0][tid];
+            eint0 = s.OWN[KeepOwn<R>::value ? 5 : 0][tid];
         } else {   // the FP64 window holds these values exactly
             dens0 = (double)s.V[D][oj + 3][oi + 3]; vx = (double)s.V[VX][oj + 3][oi + 3];
             vy = (double)s.V[VY][oj + 3][oi + 3]; vz = (double)s.V[VZ][oj + 3][oi + 3];
