@@ -432,7 +432,7 @@ __device__ __forceinline__ int riemann(const DevParams &prm, int dir, const R *V
     const R velNL = Vm[1 + dir], velNR = Vp[1 + dir];
     const R aL2 = rdiv(gcL * Vm[P], Vm[D]);
     const R aR2 = rdiv(gcR * Vp[P], Vp[D]);
-    const bool hllc = prm.riemann == 4;
+    const bool hllc = prm.riemann == 4, llf = prm.riemann == 2;
     const R tiny = hllc ? R(prm.tiny) : R(1.e-32);
     if ((Vm[D] < tiny && Vm[D] > R(0)) || (Vp[D] < tiny && Vp[D] > R(0)) ||
         (Vm[P] < tiny && Vm[P] > R(0)) || (Vp[P] < tiny && Vp[P] > R(0))) {
@@ -463,7 +463,27 @@ __device__ __forceinline__ int riemann(const DevParams &prm, int dir, const R *V
         FR[1 + dir] = FR[1 + dir] + fP * Vp[P];
         FL[4] = (EL + Vm[P]) * velNL; FR[4] = (ER + Vp[P]) * velNR;
         FL[5] = Vm[P]; FR[5] = Vp[P];
-        if (hllc) {
+        if (llf) {
+            // hy_LLF.F90:62-183: the largest |eigenvalue| (hy_eigenValue.F90) of the
+            // mean state of hy_avgState.F90:34-60 (gamc upwind of its normal
+            // velocity) and of the two states, times the conserved jump
+            const R un = R(.5) * (velNL + velNR);
+            const R sig = un == R(0) ? R(0) : (un > R(0) ? R(1) : R(-1));
+            const R gcA = R(0.5) * ((R(1.) + sig) * gcL + (R(1.) - sig) * gcR);
+            const R a2 = rdiv(gcA * (R(.5) * (Vm[P] + Vp[P])), R(.5) * (Vm[D] + Vp[D]));
+            if (a2 <= R(0) || aL2 <= R(0) || aR2 <= R(0)) return ERR_SOUND;   // hy_eigenParameters aborts
+            const R cf = rsqrt_(a2);
+            auto maxabs = [](R u, R c) {
+                R m = fabs(u - c);
+                if (fabs(u) > m) m = fabs(u);
+                if (fabs(u + c) > m) m = fabs(u + c);
+                return m;
+            };
+            const R smax = fmax2(fmax2(maxabs(un, cf), maxabs(velNL, cfL)), maxabs(velNR, cfR));
+#pragma unroll
+            for (int k = 0; k < 5; k++) F[k] = (FR[k] + FL[k] - smax * (UR[k] - UL[k])) * R(0.5);
+            F[5] = (FR[5] + FL[5] - smax * (R(0.0) - R(0.0))) * R(0.5);
+        } else if (hllc) {
             R qStar = Vp[D] * velNR * (SR - velNR) - Vm[D] * velNL * (SL - velNL) + Vm[P] - Vp[P];
             qStar = rdiv(qStar, Vp[D] * (SR - velNR) - Vm[D] * (SL - velNL));
             if (SL >= R(0)) {

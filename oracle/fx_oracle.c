@@ -392,6 +392,70 @@ static int riemann_hll(const fxo_params *p, int dir, const double *Vm, const dou
     return 0;
 }
 
+/* hy_slopeLimiters.F90:74-82 */
+static double signum_(double x) { return x == 0. ? 0. : (x > 0. ? 1. : -1.); }
+
+/* largest |eigenvalue| of hy_eigenValue.F90 (hydro: u-c, u, u, u, u+c), in maxval order */
+static double maxabs_lambda(double un, double cf)
+{
+    const double l[5] = {un - cf, un, un, un, un + cf};
+    double m = fabs(l[0]);
+    for (int k = 1; k < 5; k++) if (fabs(l[k]) > m) m = fabs(l[k]);
+    return m;
+}
+
+/* hy_LLF.F90:62-183 (hydro): the largest |wave speed| of the averaged
+ * (hy_avgState.F90:34-60), left and right states (hy_eigenParameters.F90:
+ * 83-100, which aborts on a2 <= 0) times the jump of the conserved state,
+ * subtracted from the mean of the two physical fluxes. */
+static int riemann_llf(const fxo_params *p, int dir, const double *Vm, const double *Vp, double Fs[6], double *speed)
+{
+    const double tiny = 1.e-32;
+    double aL2 = Vm[H_GC] * Vm[H_P] / Vm[H_D];
+    double aR2 = Vp[H_GC] * Vp[H_P] / Vp[H_D];
+    if ((Vm[H_D] < tiny && Vm[H_D] > 0.) || (Vp[H_D] < tiny && Vp[H_D] > 0.) ||
+        (Vm[H_P] < tiny && Vm[H_P] > 0.) || (Vp[H_P] < tiny && Vp[H_P] > 0.)) {
+        for (int k = 0; k < 6; k++) Fs[k] = 0.;
+        *speed = 0.;
+        return 0;
+    } else if (aL2 < 0. || aR2 < 0.) {
+        return 1;
+    }
+    /* hy_avgState: the mean state, gammas taken upwind of the mean normal velocity */
+    double Va[H_NV];
+    for (int k = 0; k < H_NV; k++) Va[k] = 0.;
+    Va[H_D] = .5 * (Vm[H_D] + Vp[H_D]);
+    Va[H_VX] = .5 * (Vm[H_VX] + Vp[H_VX]);
+    Va[H_VY] = .5 * (Vm[H_VY] + Vp[H_VY]);
+    Va[H_VZ] = .5 * (Vm[H_VZ] + Vp[H_VZ]);
+    Va[H_P] = .5 * (Vm[H_P] + Vp[H_P]);
+    const double sig = signum_(Va[H_VX + dir]);
+    Va[H_GC] = 0.5 * ((1. + sig) * Vm[H_GC] + (1. - sig) * Vp[H_GC]);
+    Va[H_GE] = 0.5 * ((1. + sig) * Vm[H_GE] + (1. - sig) * Vp[H_GE]);
+    const double a2 = Va[H_GC] * Va[H_P] / Va[H_D];
+    const double a2L = Vm[H_GC] * Vm[H_P] / Vm[H_D], a2R = Vp[H_GC] * Vp[H_P] / Vp[H_D];
+    if (a2 <= 0. || a2L <= 0. || a2R <= 0.) return 1;
+    const double lm = maxabs_lambda(Va[H_VX + dir], sqrt(a2));
+    const double lL = maxabs_lambda(Vm[H_VX + dir], sqrt(a2L));
+    const double lR = maxabs_lambda(Vp[H_VX + dir], sqrt(a2R));
+    const double smax = fmax2(fmax2(lm, lL), lR);
+    *speed = fabs(Vp[H_VX + dir]) + fabs(sqrt(a2R));
+    double UL[6], UR[6], FL[6], FR[6];
+    prim2con(Vm, UL); prim2con(Vp, UR);
+    UL[5] = 0.; UR[5] = 0.;
+    prim2flx(p, dir, Vm, FL); prim2flx(p, dir, Vp, FR);
+    for (int k = 0; k < 6; k++) Fs[k] = (FR[k] + FL[k] - smax * (UR[k] - UL[k])) * 0.5;
+    return 0;
+}
+
+/* the Riemann solver of the runtime parameter RiemannSolver */
+static int riemann_solve(const fxo_params *p, int dir, const double *Vm, const double *Vp, double Fs[6], double *speed)
+{
+    if (p->riemann == FXO_HLL) return riemann_hll(p, dir, Vm, Vp, Fs, speed);
+    if (p->riemann == FXO_LLF) return riemann_llf(p, dir, Vm, Vp, Fs, speed);
+    return riemann_hllc(p, dir, Vm, Vp, Fs, speed);
+}
+
 /* ======================================================================= */
 /* Per-block hy_computeFluxes with in-place update (Uout => Uin).          */
 /* ======================================================================= */
@@ -651,8 +715,7 @@ static int face_fluxes(const blk_t *b, scratch_t *s)
             for (int v = 0; v < 8; v++) { VL[v] = s->scr[d][cm * 16 + v]; VR[v] = s->scr[d][c * 16 + 8 + v]; }
             VL[H_GR] = 0.; VR[H_GR] = 0.;
             double F[6], speed;
-            int err = (p->riemann == FXO_HLL) ? riemann_hll(p, d, VL, VR, F, &speed)
-                                              : riemann_hllc(p, d, VL, VR, F, &speed);
+            int err = riemann_solve(p, d, VL, VR, F, &speed);
             if (err) return 2;
             double *fl = s->flx[d] + c * 8;
             for (int v = 0; v < 6; v++) fl[v] = F[v];
@@ -1016,8 +1079,7 @@ int fxo_riemann(const fxo_params *p, int dir, const double VL[8], const double V
     double vl[H_NV], vr[H_NV], Fs[6], speed;
     for (int k = 0; k < 8; k++) { vl[k] = VL[k]; vr[k] = VR[k]; }
     vl[H_GR] = 0.; vr[H_GR] = 0.;
-    int err = (p->riemann == FXO_HLL) ? riemann_hll(p, dir, vl, vr, Fs, &speed)
-                                      : riemann_hllc(p, dir, vl, vr, Fs, &speed);
+    int err = riemann_solve(p, dir, vl, vr, Fs, &speed);
     if (err) return err;
     for (int k = 0; k < 6; k++) F[k] = Fs[k];
     if (p->use_aux_eint) {

@@ -78,6 +78,7 @@ def test_calls_before_init_are_rejected():
 def test_parameter_validation_mirrors_hydro_init():
     HydroParams().validate()
     HydroParams(use_flattening=True).validate()
+    HydroParams(RiemannSolver="LLF").validate()
     for bad in (dict(order=2), dict(RiemannSolver="Roe"), dict(slopeLimiter="superbee"),
                 dict(transOrder=3), dict(use_steepening=True), dict(use_flattening=True, useGravity=True),
                 dict(hydroComputeDtOption=0)):

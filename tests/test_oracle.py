@@ -112,7 +112,12 @@ def _phys_flux(V, d, g=1.4):
     return F
 
 
-@pytest.mark.parametrize("solver", ["HLLC", "HLL"])
+def _cons(V):
+    rho, vel, p, g = V[0], np.array(V[1:4]), V[4], V[6]
+    return np.array([rho, *(rho * vel), 0.5 * rho * np.dot(vel, vel) + p / (g - 1), 0.0])
+
+
+@pytest.mark.parametrize("solver", ["HLLC", "HLL", "LLF"])
 def test_riemann_known_answers(oracle, solver):
     geom = Geometry(2, 16, 16, 1, 1, 1, 1)
     hp = HydroParams(RiemannSolver=solver)
@@ -122,13 +127,22 @@ def test_riemann_known_answers(oracle, solver):
     for d in range(3):
         F = oracle.riemann(p, d, V, V)
         assert np.allclose(F[:6], _phys_flux(V, d), rtol=1e-14, atol=1e-15)
-    # supersonic to the right: upwind flux of the left state
+    # supersonic to the right: HLL(C) give the upwind flux of the left state;
+    # LLF (hy_LLF.F90) the mean flux less the largest |u| + c of the mean,
+    # left and right states times the conserved jump
     VL, VR = _state(1.0, 5.0, 0, 0, 1.0), _state(0.5, 4.0, 0, 0, 0.3)
     F = oracle.riemann(p, 0, VL, VR)
-    assert np.allclose(F[:6], _phys_flux(VL, 0), rtol=1e-14)
+    if solver == "LLF":
+        c = lambda V: np.sqrt(V[5] * V[4] / V[0])
+        Va = 0.5 * (np.array(VL) + np.array(VR))
+        smax = max(abs(Va[1]) + np.sqrt(Va[5] * Va[4] / Va[0]), abs(VL[1]) + c(VL), abs(VR[1]) + c(VR))
+        want = 0.5 * (_phys_flux(VR, 0) + _phys_flux(VL, 0) - smax * (_cons(VR) - _cons(VL)))
+        assert np.allclose(F[:6], want, rtol=1e-14)
+    else:
+        assert np.allclose(F[:6], _phys_flux(VL, 0), rtol=1e-14)
     # aux-eint fluxes follow the mass flux upwind (hy_getFaceFlux.F90:444-453)
     assert F[7] == pytest.approx(F[0] / VL[0]) and F[6] == pytest.approx(F[0] * VL[7])
-    # stationary contact: HLLC resolves it exactly (zero mass flux), HLL diffuses it
+    # stationary contact: HLLC resolves it exactly (zero mass flux), HLL and LLF diffuse it
     VL, VR = _state(1.0, 0, 0, 0, 1.0), _state(0.1, 0, 0, 0, 1.0)
     F = oracle.riemann(p, 0, VL, VR)
     if solver == "HLLC":
