@@ -375,8 +375,8 @@ extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, cons
     if (d.ndim != 2 && d.ndim != 3) return fail(FXB_EUNSUPPORTED, "fxb_init: ndim must be 2 or 3");
     if (d.nguard < 4) return fail(FXB_EARG, "fxb_init: NGUARD must be at least 4");
     if (p.order != 3 && p.order != 5) return fail(FXB_EUNSUPPORTED, "fxb_init: order must be 3 (PPM) or 5 (WENO)");
-    if (p.riemann != 2 && p.riemann != 3 && p.riemann != 4)
-        return fail(FXB_EUNSUPPORTED, "fxb_init: RiemannSolver must be LLF, HLL or HLLC");
+    if (p.riemann < 1 || p.riemann > 4)
+        return fail(FXB_EUNSUPPORTED, "fxb_init: RiemannSolver must be Roe, LLF, HLL or HLLC");
     if (p.limiter < 1 || p.limiter > 5) return fail(FXB_EARG, "fxb_init: unknown slope limiter");
     if (p.precision != FXB_FP64 && p.precision != FXB_MIXED) return fail(FXB_EARG, "fxb_init: unknown precision");
     if (d.ndim == 2 && p.use_gravity) return fail(FXB_EUNSUPPORTED, "fxb_init: gravity is implemented for 3-D only");

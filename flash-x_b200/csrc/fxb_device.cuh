@@ -425,14 +425,78 @@ __device__ __forceinline__ void gravity_faces(const DevParams &prm, R g, R &gl, 
 // ---- Riemann solvers (hy_HLLC.F90:64-335, hy_HLL.F90:64-182) ---------------
 // Vm/Vp: 6-vectors D, VX, VY, VZ, P (global axes), EI; gamc/game passed separately.
 // F[8] receives the HY_*_FLUX slots including the aux-eint pair.
+// hy_Roe.F90:62-205 (entropy = .false.): the mean state of hy_avgState, its
+// conservative eigenvectors (OnlyHydro/hy_eigenVector.F90:128-166) and
+// F = (FL + FR - sum_w |lambda_w| r_w (l_w . (UR - UL))) / 2, the dot products
+// over all five rows, zeros included, as dot_product does.  Only the kernels
+// instantiated for RiemannSolver = Roe contain it, so the other solvers keep
+// their register allocation.
 template <class R>
+__device__ __forceinline__ int riemann_roe(int dir, const R *Vm, R gcL, R geL, const R *Vp, R gcR, R geR,
+                                        const R UL[5], const R UR[5], const R FL[6], const R FR[6], R F[8])
+{
+    const R Va[5] = {R(.5) * (Vm[D] + Vp[D]), R(.5) * (Vm[VX] + Vp[VX]), R(.5) * (Vm[VY] + Vp[VY]),
+                     R(.5) * (Vm[VZ] + Vp[VZ]), R(.5) * (Vm[P] + Vp[P])};
+    const R unA = Va[1 + dir];
+    const R sig = unA == R(0) ? R(0) : (unA > R(0) ? R(1) : R(-1));
+    const R gcA = R(0.5) * ((R(1.) + sig) * gcL + (R(1.) - sig) * gcR);
+    const R geA = R(0.5) * ((R(1.) + sig) * geL + (R(1.) - sig) * geR);
+    const R a2 = rdiv(gcA * Va[4], Va[0]);
+    if (a2 <= R(0)) return ERR_SOUND;   // hy_eigenParameters aborts
+    const R cf = rsqrt_(a2);
+    const R lam[5] = {unA - cf, unA, unA, unA, unA + cf};
+    const int v1 = 1 + dir, v2 = 1 + (dir + 1) % 3, v3 = 1 + (dir + 2) % 3;
+    const R V1 = Va[v1], V2 = Va[v2], V3 = Va[v3];
+    const R k = R(1.) - geA;
+    const R a2e = cf * cf, a2inv = rdiv(R(1.), a2e), Na = R(0.5) * a2inv;
+    R u2 = R(0.);
+    u2 = u2 + Va[1] * Va[1]; u2 = u2 + Va[2] * Va[2]; u2 = u2 + Va[3] * Va[3];
+    u2 = R(0.5) * u2;
+    const R H = rdiv(Va[0] * u2 - rdiv(Va[4], k) + Va[4], Va[0]);
+    R L[5][5], Rv[5][5];
+#pragma unroll
+    for (int a = 0; a < 5; a++)
+#pragma unroll
+        for (int w = 0; w < 5; w++) { L[a][w] = R(0); Rv[a][w] = R(0); }
+    L[0][0] = Na * (-(k * u2) + V1 * cf); L[v1][0] = -(Na * (-(k * V1) + cf));
+    L[v2][0] = Na * k * V2; L[v3][0] = Na * k * V3; L[4][0] = -(Na * k);
+    L[0][1] = -V2; L[v2][1] = R(1.);
+    L[0][2] = R(1.) + Na * k * u2 * R(2.);
+    L[v1][2] = -(k * V1 * a2inv); L[v2][2] = -(k * V2 * a2inv); L[v3][2] = -(k * V3 * a2inv);
+    L[4][2] = k * a2inv;
+    L[0][3] = -V3; L[v3][3] = R(1.);
+    L[0][4] = Na * (-(k * u2) - V1 * cf); L[v1][4] = -(Na * (-(k * V1) - cf));
+    L[v2][4] = Na * k * V2; L[v3][4] = Na * k * V3; L[4][4] = -(Na * k);
+    Rv[0][0] = R(1.); Rv[v1][0] = V1 - cf; Rv[v2][0] = V2; Rv[v3][0] = V3; Rv[4][0] = H - V1 * cf;
+    Rv[v2][1] = R(1.); Rv[4][1] = V2;
+    Rv[0][2] = R(1.); Rv[v1][2] = V1; Rv[v2][2] = V2; Rv[v3][2] = V3; Rv[4][2] = u2;
+    Rv[v3][3] = R(1.); Rv[4][3] = V3;
+    Rv[0][4] = R(1.); Rv[v1][4] = V1 + cf; Rv[v2][4] = V2; Rv[v3][4] = V3; Rv[4][4] = H + V1 * cf;
+    R dU[5], sigF[5] = {R(0), R(0), R(0), R(0), R(0)};
+#pragma unroll
+    for (int a = 0; a < 5; a++) dU[a] = UR[a] - UL[a];
+#pragma unroll
+    for (int w = 0; w < 5; w++) {
+        R dp = R(0.);
+#pragma unroll
+        for (int a = 0; a < 5; a++) dp = dp + L[a][w] * dU[a];
+#pragma unroll
+        for (int a = 0; a < 5; a++) sigF[a] = sigF[a] + fabs(lam[w]) * Rv[a][w] * dp;
+    }
+#pragma unroll
+    for (int a = 0; a < 5; a++) F[a] = (FR[a] + FL[a] - sigF[a]) * R(0.5);
+    F[5] = (FR[5] + FL[5] - R(0.)) * R(0.5);
+    return 0;
+}
+
+template <class R, bool ROE>
 __device__ __forceinline__ int riemann(const DevParams &prm, int dir, const R *Vm, R gcL, R geL,
                                        const R *Vp, R gcR, R geR, R F[8])
 {
     const R velNL = Vm[1 + dir], velNR = Vp[1 + dir];
     const R aL2 = rdiv(gcL * Vm[P], Vm[D]);
     const R aR2 = rdiv(gcR * Vp[P], Vp[D]);
-    const bool hllc = prm.riemann == 4, llf = prm.riemann == 2;
+    const bool hllc = !ROE && prm.riemann == 4, llf = !ROE && prm.riemann == 2;
     const R tiny = hllc ? R(prm.tiny) : R(1.e-32);
     if ((Vm[D] < tiny && Vm[D] > R(0)) || (Vp[D] < tiny && Vp[D] > R(0)) ||
         (Vm[P] < tiny && Vm[P] > R(0)) || (Vp[P] < tiny && Vp[P] > R(0))) {
@@ -483,6 +547,9 @@ __device__ __forceinline__ int riemann(const DevParams &prm, int dir, const R *V
 #pragma unroll
             for (int k = 0; k < 5; k++) F[k] = (FR[k] + FL[k] - smax * (UR[k] - UL[k])) * R(0.5);
             F[5] = (FR[5] + FL[5] - smax * (R(0.0) - R(0.0))) * R(0.5);
+        } else if (ROE) {
+            const int e = riemann_roe(dir, Vm, gcL, geL, Vp, gcR, geR, UL, UR, FL, FR, F);
+            if (e) return e;
         } else if (hllc) {
             R qStar = Vp[D] * velNR * (SR - velNR) - Vm[D] * velNL * (SL - velNL) + Vm[P] - Vp[P];
             qStar = rdiv(qStar, Vp[D] * (SR - velNR) - Vm[D] * (SL - velNL));

@@ -205,21 +205,21 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
     for (int k = 0; k < 6; k++) { s.W[k][t] = Wp[k]; s.W[6 + k][t] = Wm[k]; }
 }
 
-template <class R>
+template <class R, bool ROE>
 __device__ __forceinline__ void faces_stage(const Args2D &a, Smem2D<R> &s, int dir, int t, int wl, int wr,
                                             int wxl, int wyl, int wxr, int wyr)
 {
     R VL[6], VR[6], F[8];
 #pragma unroll
     for (int k = 0; k < 6; k++) { VL[k] = s.W[k][wl]; VR[k] = s.W[6 + k][wr]; }
-    int e = riemann(a.prm, dir, VL, s.V[GC][wyl][wxl], s.V[GE][wyl][wxl],
+    int e = riemann<R, ROE>(a.prm, dir, VL, s.V[GC][wyl][wxl], s.V[GE][wyl][wxl],
                     VR, s.V[GC][wyr][wxr], s.V[GE][wyr][wxr], F);
     if (e) set_err(a.err, e);
 #pragma unroll
     for (int k = 0; k < NF; k++) s.DBF[k * NFC + t] = F[k];
 }
 
-template <class R>
+template <class R, bool ROE>
 __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::value) hydro2d_kernel(const Args2D a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
     // ---- D: x faces
     for (int t = tid; t < NFC; t += NT2) {
         int fi = t % (T2 + 1), jj = t / (T2 + 1);
-        faces_stage(a, s, 0, t, jj * (T2 + 2) + fi, jj * (T2 + 2) + fi + 1, fi + 2, jj + 3, fi + 3, jj + 3);
+        faces_stage<R, ROE>(a, s, 0, t, jj * (T2 + 2) + fi, jj * (T2 + 2) + fi + 1, fi + 2, jj + 3, fi + 3, jj + 3);
     }
     __syncthreads();
 
@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
     // ---- H: y faces
     for (int t = tid; t < NFC; t += NT2) {
         int ii = t % T2, fj = t / T2;
-        faces_stage(a, s, 1, t, fj * T2 + ii, (fj + 1) * T2 + ii, ii + 3, fj + 2, ii + 3, fj + 3);
+        faces_stage<R, ROE>(a, s, 1, t, fj * T2 + ii, (fj + 1) * T2 + ii, ii + 3, fj + 2, ii + 3, fj + 3);
     }
     __syncthreads();
 

@@ -589,7 +589,7 @@ __global__ void __launch_bounds__(256, FXB_S3_MINB_FP64) states3d_kernel(const A
 // ---- Riemann fluxes of direction d ---------------------------------------------
 // the direction is a template parameter so that the solver's per-direction
 // indexing of the state vectors resolves at compile time (no local memory)
-template <class R, bool AMR, int DIR>
+template <class R, bool AMR, int DIR, bool ROE>
 __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
 {
     constexpr int d = DIR;
@@ -609,7 +609,7 @@ __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
         for (int q = 0; q < 6; q++) { VL[q] = w[(long)q * nw + wl]; VR[q] = w[(long)(6 + q) * nw + wr]; }
         X.load_gammas(a, i - di, j - dj, k - dk, gcl, gel);
         X.load_gammas(a, i, j, k, gcr, ger);
-        int e = riemann(a.prm, d, VL, gcl, gel, VR, gcr, ger, F);
+        int e = riemann<R, ROE>(a.prm, d, VL, gcl, gel, VR, gcr, ger, F);
         if (e) atomicOr(a.err, e);
 #pragma unroll
         for (int q = 0; q < NF; q++) f[(long)q * nf + idx] = F[q];
@@ -630,7 +630,7 @@ __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
 template <class R> struct SfluxRegs {
     static constexpr int value = (65536 / ((sizeof(R) == 8 ? 2 : 3) * FXB_SF_MAXT)) / 8 * 8;
 };
-template <class R, int ORDER, bool AMR, int DIR>
+template <class R, int ORDER, bool AMR, int DIR, bool ROE>
 __global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) sflux3d_kernel(const Args3D a)
 {
     constexpr int d = DIR;
@@ -720,7 +720,7 @@ __global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) 
         R VL[6], F[NF];
 #pragma unroll
         for (int q = 0; q < 6; q++) VL[q] = sW[q * nt + tl];
-        const int e = riemann(a.prm, d, VL, sW[6 * nt + tl], sW[7 * nt + tl], Wm, gc, ge, F);
+        const int e = riemann<R, ROE>(a.prm, d, VL, sW[6 * nt + tl], sW[7 * nt + tl], Wm, gc, ge, F);
         if (e) atomicOr(a.err, e);
         R *f = X.flx[d];
         const long nf = G.nf(d), fi = G.fidx(d, i, j, k);
@@ -859,7 +859,7 @@ inline size_t f3d_bytes(int d, int nx, int ny, int nz, size_t rsz)
 
 // face states and fluxes of one direction (PPM: slopes first); g.x CTAs per
 // block for the grid-stride kernels, g.y batch entries
-template <class R, bool AMR, int DIR> void launch_states3d(const Args3D &a, dim3 g, cudaStream_t s)
+template <class R, bool AMR, int DIR, bool ROE> void launch_states3d_rs(const Args3D &a, dim3 g, cudaStream_t s)
 {
     if constexpr (!FusedFaces<R>::value) {
         if (a.prm.order == 5) {
@@ -868,7 +868,7 @@ template <class R, bool AMR, int DIR> void launch_states3d(const Args3D &a, dim3
             slope3d_kernel<R, AMR><<<g, 256, 0, s>>>(a, DIR);
             states3d_kernel<R, 3, AMR, DIR><<<g, 256, 0, s>>>(a);
         }
-        flux3d_kernel<R, AMR, DIR><<<dim3(AMR ? a.cta[2] : g.x, g.y), 256, 0, s>>>(a);
+        flux3d_kernel<R, AMR, DIR, ROE><<<dim3(AMR ? a.cta[2] : g.x, g.y), 256, 0, s>>>(a);
     } else {
         const int N = DIR == 0 ? a.nx : DIR == 1 ? a.ny : a.nz;
         const int N1 = DIR == 0 ? a.ny : a.nx, N2 = DIR == 2 ? a.ny : a.nz;
@@ -876,12 +876,18 @@ template <class R, bool AMR, int DIR> void launch_states3d(const Args3D &a, dim3
         const int nseg = (N + Ls - 1) / (Ls - 1), nt1 = (N1 + T1 - 1) / T1;
         const dim3 gs((unsigned)(nseg * nt1 * N2), g.y);
         if (a.prm.order == 5) {
-            sflux3d_kernel<R, 5, AMR, DIR><<<gs, Ls * T1, 8 * sizeof(R) * (size_t)(Ls * T1), s>>>(a);
+            sflux3d_kernel<R, 5, AMR, DIR, ROE><<<gs, Ls * T1, 8 * sizeof(R) * (size_t)(Ls * T1), s>>>(a);
         } else {   // the slopes are computed in the kernel: two more cells per line
             const int nt = (Ls + 2) * T1;
-            sflux3d_kernel<R, 3, AMR, DIR><<<gs, nt, 14 * sizeof(R) * (size_t)nt, s>>>(a);
+            sflux3d_kernel<R, 3, AMR, DIR, ROE><<<gs, nt, 14 * sizeof(R) * (size_t)nt, s>>>(a);
         }
     }
+}
+// the Roe solver has its own kernel instantiations
+template <class R, bool AMR, int DIR> void launch_states3d(const Args3D &a, dim3 g, cudaStream_t s)
+{
+    if (a.prm.riemann == 1) launch_states3d_rs<R, AMR, DIR, true>(a, g, s);
+    else launch_states3d_rs<R, AMR, DIR, false>(a, g, s);
 }
 
 // slope cells a face-state tile adds per line: two when the FP32 kernel computes the PPM slopes itself

@@ -3,12 +3,18 @@
 namespace fxb {
 cudaError_t setup_hydro2d_fp64()
 {
-    return cudaFuncSetAttribute(hydro2d_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(hydro2d_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(Smem2D<double>));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(hydro2d_kernel<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(Smem2D<double>));
 }
 void launch_hydro2d_fp64(const Args2D &a, dim3 grid, cudaStream_t s)
 {
     if (a.prm.flattening) flat2d_kernel<double><<<148 * 8, 256, 0, s>>>(a, (double *)a.flat);
-    hydro2d_kernel<double><<<grid, Threads2D<double>::value, sizeof(Smem2D<double>), s>>>(a);
+    if (a.prm.riemann == 1)   // Roe: its own instantiation
+        hydro2d_kernel<double, true><<<grid, Threads2D<double>::value, sizeof(Smem2D<double>), s>>>(a);
+    else
+        hydro2d_kernel<double, false><<<grid, Threads2D<double>::value, sizeof(Smem2D<double>), s>>>(a);
 }
 } // namespace fxb

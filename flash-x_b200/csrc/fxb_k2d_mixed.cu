@@ -5,12 +5,18 @@
 namespace fxb {
 cudaError_t setup_hydro2d_mixed()
 {
-    return cudaFuncSetAttribute(hydro2d_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(hydro2d_kernel<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(Smem2D<float>));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(hydro2d_kernel<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(Smem2D<float>));
 }
 void launch_hydro2d_mixed(const Args2D &a, dim3 grid, cudaStream_t s)
 {
     if (a.prm.flattening) flat2d_kernel<float><<<148 * 8, 256, 0, s>>>(a, (float *)a.flat);
-    hydro2d_kernel<float><<<grid, Threads2D<float>::value, sizeof(Smem2D<float>), s>>>(a);
+    if (a.prm.riemann == 1)   // Roe: its own instantiation
+        hydro2d_kernel<float, true><<<grid, Threads2D<float>::value, sizeof(Smem2D<float>), s>>>(a);
+    else
+        hydro2d_kernel<float, false><<<grid, Threads2D<float>::value, sizeof(Smem2D<float>), s>>>(a);
 }
 } // namespace fxb

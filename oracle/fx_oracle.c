@@ -448,11 +448,84 @@ static int riemann_llf(const fxo_params *p, int dir, const double *Vm, const dou
     return 0;
 }
 
+/* hy_Roe.F90:62-205 (hydro, entropy = .false.): the mean state of
+ * hy_avgState, its eigenvalues and conservative eigenvectors
+ * (OnlyHydro/hy_eigenVector.F90:128-166, cons = .true.), and the flux
+ * (FL + FR - sum_k |lambda_k| r_k (l_k . (UR - UL))) / 2; the dot products
+ * run over all five rows, zeros included, as dot_product does. */
+static int riemann_roe(const fxo_params *p, int dir, const double *Vm, const double *Vp, double Fs[6], double *speed)
+{
+    const double tiny = 1.e-32;
+    double aL2 = Vm[H_GC] * Vm[H_P] / Vm[H_D];
+    double aR2 = Vp[H_GC] * Vp[H_P] / Vp[H_D];
+    if ((Vm[H_D] < tiny && Vm[H_D] > 0.) || (Vp[H_D] < tiny && Vp[H_D] > 0.) ||
+        (Vm[H_P] < tiny && Vm[H_P] > 0.) || (Vp[H_P] < tiny && Vp[H_P] > 0.)) {
+        for (int k = 0; k < 6; k++) Fs[k] = 0.;
+        *speed = 0.;
+        return 0;
+    } else if (aL2 < 0. || aR2 < 0.) {
+        return 1;
+    }
+    double Va[H_NV];
+    for (int k = 0; k < H_NV; k++) Va[k] = 0.;
+    Va[H_D] = .5 * (Vm[H_D] + Vp[H_D]);
+    Va[H_VX] = .5 * (Vm[H_VX] + Vp[H_VX]);
+    Va[H_VY] = .5 * (Vm[H_VY] + Vp[H_VY]);
+    Va[H_VZ] = .5 * (Vm[H_VZ] + Vp[H_VZ]);
+    Va[H_P] = .5 * (Vm[H_P] + Vp[H_P]);
+    const double sig = signum_(Va[H_VX + dir]);
+    Va[H_GC] = 0.5 * ((1. + sig) * Vm[H_GC] + (1. - sig) * Vp[H_GC]);
+    Va[H_GE] = 0.5 * ((1. + sig) * Vm[H_GE] + (1. - sig) * Vp[H_GE]);
+    const double a2 = Va[H_GC] * Va[H_P] / Va[H_D];
+    if (a2 <= 0.) return 1;
+    const double cf = sqrt(a2), un = Va[H_VX + dir];
+    const double lam[5] = {un - cf, un, un, un, un + cf};
+    /* conservative eigenvectors: rows D, MX, MY, MZ, E; columns the five waves */
+    const int v1 = H_VX + dir, v2 = H_VX + (dir + 1) % 3, v3 = H_VX + (dir + 2) % 3;
+    const double V1 = Va[v1], V2 = Va[v2], V3 = Va[v3];
+    const double k = 1. - Va[H_GE];
+    const double a2e = cf * cf, a2inv = 1. / a2e, Na = 0.5 * a2inv;
+    double u2 = 0.;
+    u2 = u2 + Va[H_VX] * Va[H_VX]; u2 = u2 + Va[H_VY] * Va[H_VY]; u2 = u2 + Va[H_VZ] * Va[H_VZ];
+    u2 = 0.5 * u2;
+    const double H = (Va[H_D] * u2 - Va[H_P] / k + Va[H_P]) / Va[H_D];
+    double L[5][5], R[5][5];
+    memset(L, 0, sizeof(L)); memset(R, 0, sizeof(R));
+    const int E = H_P;
+    L[H_D][0] = Na * (-(k * u2) + V1 * cf); L[v1][0] = -(Na * (-(k * V1) + cf));
+    L[v2][0] = Na * k * V2; L[v3][0] = Na * k * V3; L[E][0] = -(Na * k);
+    L[H_D][1] = -V2; L[v2][1] = 1.;
+    L[H_D][2] = 1. + Na * k * u2 * 2.;
+    L[v1][2] = -(k * V1 * a2inv); L[v2][2] = -(k * V2 * a2inv); L[v3][2] = -(k * V3 * a2inv); L[E][2] = k * a2inv;
+    L[H_D][3] = -V3; L[v3][3] = 1.;
+    L[H_D][4] = Na * (-(k * u2) - V1 * cf); L[v1][4] = -(Na * (-(k * V1) - cf));
+    L[v2][4] = Na * k * V2; L[v3][4] = Na * k * V3; L[E][4] = -(Na * k);
+    R[H_D][0] = 1.; R[v1][0] = V1 - cf; R[v2][0] = V2; R[v3][0] = V3; R[E][0] = H - V1 * cf;
+    R[v2][1] = 1.; R[E][1] = V2;
+    R[H_D][2] = 1.; R[v1][2] = V1; R[v2][2] = V2; R[v3][2] = V3; R[E][2] = u2;
+    R[v3][3] = 1.; R[E][3] = V3;
+    R[H_D][4] = 1.; R[v1][4] = V1 + cf; R[v2][4] = V2; R[v3][4] = V3; R[E][4] = H + V1 * cf;
+    *speed = fabs(un) + fabs(cf);
+    double UL[5], UR[5], FL[6], FR[6], dU[5];
+    prim2con(Vm, UL); prim2con(Vp, UR);
+    prim2flx(p, dir, Vm, FL); prim2flx(p, dir, Vp, FR);
+    for (int v = 0; v < 5; v++) dU[v] = UR[v] - UL[v];
+    double sigF[6] = {0., 0., 0., 0., 0., 0.};
+    for (int w = 0; w < 5; w++) {
+        double dp = 0.;
+        for (int v = 0; v < 5; v++) dp = dp + L[v][w] * dU[v];
+        for (int v = 0; v < 5; v++) sigF[v] = sigF[v] + fabs(lam[w]) * R[v][w] * dp;
+    }
+    for (int v = 0; v < 6; v++) Fs[v] = (FR[v] + FL[v] - sigF[v]) * 0.5;
+    return 0;
+}
+
 /* the Riemann solver of the runtime parameter RiemannSolver */
 static int riemann_solve(const fxo_params *p, int dir, const double *Vm, const double *Vp, double Fs[6], double *speed)
 {
     if (p->riemann == FXO_HLL) return riemann_hll(p, dir, Vm, Vp, Fs, speed);
     if (p->riemann == FXO_LLF) return riemann_llf(p, dir, Vm, Vp, Fs, speed);
+    if (p->riemann == FXO_ROE) return riemann_roe(p, dir, Vm, Vp, Fs, speed);
     return riemann_hllc(p, dir, Vm, Vp, Fs, speed);
 }
 

@@ -54,7 +54,7 @@ def test_init_validation_codes():
     assert lib.fxb_init(ctypes.byref(p), ctypes.byref(d), H.default_var_map(), 11) == H.FXB_EARG
     d.nguard = 4; p.order = 2
     assert lib.fxb_init(ctypes.byref(p), ctypes.byref(d), H.default_var_map(), 11) == H.FXB_EUNSUPPORTED
-    p.order = 3; p.riemann = 1
+    p.order = 3; p.riemann = 5
     assert lib.fxb_init(ctypes.byref(p), ctypes.byref(d), H.default_var_map(), 11) == H.FXB_EUNSUPPORTED
     p.riemann = 4
     vm = H.default_var_map(); vm[0] = 11
@@ -79,7 +79,8 @@ def test_parameter_validation_mirrors_hydro_init():
     HydroParams().validate()
     HydroParams(use_flattening=True).validate()
     HydroParams(RiemannSolver="LLF").validate()
-    for bad in (dict(order=2), dict(RiemannSolver="Roe"), dict(slopeLimiter="superbee"),
+    HydroParams(RiemannSolver="Roe").validate()
+    for bad in (dict(order=2), dict(RiemannSolver="Marquina"), dict(slopeLimiter="superbee"),
                 dict(transOrder=3), dict(use_steepening=True), dict(use_flattening=True, useGravity=True),
                 dict(hydroComputeDtOption=0)):
         with pytest.raises(ValueError):

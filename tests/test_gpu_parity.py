@@ -92,6 +92,7 @@ def test_100_steps_fp64_l1(oracle, need_gpu, name):
 
 @pytest.mark.parametrize("opts", [
     dict(order=5), dict(order=5, wenoMethod="WENOZ"), dict(RiemannSolver="HLL"), dict(RiemannSolver="LLF"),
+    dict(RiemannSolver="Roe"),
     dict(slopeLimiter="minmod"), dict(slopeLimiter="vanLeer"), dict(slopeLimiter="hybrid"),
     dict(slopeLimiter="limited", LimitedSlopeBeta=1.5), dict(charLimiting=False),
     dict(charLimiting=False, slopeLimiter="hybrid"), dict(use_auxEintEqn=False), dict(hy_fPresInMomFlux=0.5),
@@ -213,7 +214,7 @@ def test_negative_pressure_reports_status(need_gpu):
 
 # ---------------------------------------------------------------- 3-D
 @pytest.mark.parametrize("case", ["ppm_periodic", "sod_outflow", "rt_weno_gravity", "hll_noctu", "wenoz_reflect",
-                                  "sod_flattening", "weno_flattening_reflect", "llf_sod"])
+                                  "sod_flattening", "weno_flattening_reflect", "llf_sod", "roe_sod_reflect"])
 def test_3d_fp64_matches_oracle(oracle, need_gpu, case):
     """3-D path (full CTU corner coupling, gravity, WENO) against the oracle,
     three steps, bit for bit."""
@@ -237,6 +238,10 @@ def test_3d_fp64_matches_oracle(oracle, need_gpu, case):
     elif case == "llf_sod":
         geom = Geometry(3, 16, 16, 16, 2, 1, 1, bc=(BC_OUTFLOW,) * 6)
         hp = HydroParams(RiemannSolver="LLF")
+        unk = S.sod(geom, hp, xangle=30.0, yangle=70.0, posn=0.6)
+    elif case == "roe_sod_reflect":
+        geom = Geometry(3, 16, 16, 16, 1, 2, 1, bc=(BC_REFLECTING,) * 6)
+        hp = HydroParams(RiemannSolver="Roe", order=5)
         unk = S.sod(geom, hp, xangle=30.0, yangle=70.0, posn=0.6)
     elif case == "sod_flattening":
         geom = Geometry(3, 16, 16, 16, 2, 1, 1, bc=(BC_OUTFLOW,) * 6)

@@ -117,7 +117,7 @@ def _cons(V):
     return np.array([rho, *(rho * vel), 0.5 * rho * np.dot(vel, vel) + p / (g - 1), 0.0])
 
 
-@pytest.mark.parametrize("solver", ["HLLC", "HLL", "LLF"])
+@pytest.mark.parametrize("solver", ["HLLC", "HLL", "LLF", "Roe"])
 def test_riemann_known_answers(oracle, solver):
     geom = Geometry(2, 16, 16, 1, 1, 1, 1)
     hp = HydroParams(RiemannSolver=solver)
@@ -132,7 +132,14 @@ def test_riemann_known_answers(oracle, solver):
     # left and right states times the conserved jump
     VL, VR = _state(1.0, 5.0, 0, 0, 1.0), _state(0.5, 4.0, 0, 0, 0.3)
     F = oracle.riemann(p, 0, VL, VR)
-    if solver == "LLF":
+    if solver == "Roe":
+        # supersonic: every wave speed of the mean state is positive, so the
+        # conserved fluxes are the left flux up to the mean-state linearisation
+        # (the mass flux exactly); the pressure slot is the mean pressure
+        assert F[0] == pytest.approx(_phys_flux(VL, 0)[0], rel=1e-15)
+        assert np.allclose(F[:5], _phys_flux(VL, 0)[:5], rtol=0.01)
+        assert F[5] == 0.5 * (VL[4] + VR[4])
+    elif solver == "LLF":
         c = lambda V: np.sqrt(V[5] * V[4] / V[0])
         Va = 0.5 * (np.array(VL) + np.array(VR))
         smax = max(abs(Va[1]) + np.sqrt(Va[5] * Va[4] / Va[0]), abs(VL[1]) + c(VL), abs(VR[1]) + c(VR))
@@ -142,10 +149,10 @@ def test_riemann_known_answers(oracle, solver):
         assert np.allclose(F[:6], _phys_flux(VL, 0), rtol=1e-14)
     # aux-eint fluxes follow the mass flux upwind (hy_getFaceFlux.F90:444-453)
     assert F[7] == pytest.approx(F[0] / VL[0]) and F[6] == pytest.approx(F[0] * VL[7])
-    # stationary contact: HLLC resolves it exactly (zero mass flux), HLL and LLF diffuse it
+    # stationary contact: HLLC and Roe resolve it exactly (zero mass flux), HLL and LLF diffuse it
     VL, VR = _state(1.0, 0, 0, 0, 1.0), _state(0.1, 0, 0, 0, 1.0)
     F = oracle.riemann(p, 0, VL, VR)
-    if solver == "HLLC":
+    if solver in ("HLLC", "Roe"):
         assert F[0] == 0.0 and F[1] == pytest.approx(1.0, rel=1e-15)
     else:
         assert F[0] > 1e-3
