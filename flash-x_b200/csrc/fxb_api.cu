@@ -381,6 +381,7 @@ extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, cons
     if (p.precision != FXB_FP64 && p.precision != FXB_MIXED) return fail(FXB_EARG, "fxb_init: unknown precision");
     if (d.ndim == 2 && p.use_gravity) return fail(FXB_EUNSUPPORTED, "fxb_init: gravity is implemented for 3-D only");
     if (p.flattening && p.use_gravity) return fail(FXB_EUNSUPPORTED, "fxb_init: use_flattening with gravity is not implemented");
+    if (p.entropy_fix < 0 || p.entropy_fix > 2) return fail(FXB_EARG, "fxb_init: unknown entropyFixMethod");
     for (int i = 0; i < 2 * d.ndim; i++)
         if (d.bc[i] < 0 || d.bc[i] > 2) return fail(FXB_EARG, "fxb_init: unknown boundary condition");
     for (int a = 0; a < d.ndim; a++) {
@@ -419,6 +420,7 @@ extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, cons
     q.small_e = p.small_e; q.small_p = p.small_p; q.tiny = p.tiny; q.fpres = p.fpres;
     q.limited_beta = p.limited_beta; q.gas_constant = p.gas_constant; q.abar = p.abar;
     q.flattening = p.flattening ? 1 : 0;
+    q.entropy_fix = p.entropy_fix;
     // Gamma/Eos_init.F90:86 and Gamma/Eos.F90:177,240-241
     double gammam1 = 1.0 / (p.gamma - 1.0);
     L.gam1inv = 1. / gammam1;

@@ -29,6 +29,7 @@ struct DevParams {
     double grav[3];
     double cfl, gamma, eint_switch, small_dens, small_e, small_p, tiny, fpres, limited_beta, gas_constant, abar;
     int flattening;
+    int entropy_fix;           // Roe: 0 off, 1 Harten-Hyman, 2 Harten
 };
 
 // ---- precision helpers ---------------------------------------------------
@@ -425,14 +426,15 @@ __device__ __forceinline__ void gravity_faces(const DevParams &prm, R g, R &gl, 
 // ---- Riemann solvers (hy_HLLC.F90:64-335, hy_HLL.F90:64-182) ---------------
 // Vm/Vp: 6-vectors D, VX, VY, VZ, P (global axes), EI; gamc/game passed separately.
 // F[8] receives the HY_*_FLUX slots including the aux-eint pair.
-// hy_Roe.F90:62-205 (entropy = .false.): the mean state of hy_avgState, its
+// hy_Roe.F90:62-205 (acoustic eigenvalues entropy-fixed by hy_entropyFix.F90
+// when entropy = .true.): the mean state of hy_avgState, its
 // conservative eigenvectors (OnlyHydro/hy_eigenVector.F90:128-166) and
 // F = (FL + FR - sum_w |lambda_w| r_w (l_w . (UR - UL))) / 2, the dot products
 // over all five rows, zeros included, as dot_product does.  Only the kernels
 // instantiated for RiemannSolver = Roe contain it, so the other solvers keep
 // their register allocation.
 template <class R>
-__device__ __forceinline__ int riemann_roe(int dir, const R *Vm, R gcL, R geL, const R *Vp, R gcR, R geR,
+__device__ __forceinline__ int riemann_roe(int dir, int entropy_fix, const R *Vm, R gcL, R geL, const R *Vp, R gcR, R geR,
                                         const R UL[5], const R UR[5], const R FL[6], const R FR[6], R F[8])
 {
     const R Va[5] = {R(.5) * (Vm[D] + Vp[D]), R(.5) * (Vm[VX] + Vp[VX]), R(.5) * (Vm[VY] + Vp[VY]),
@@ -444,7 +446,30 @@ __device__ __forceinline__ int riemann_roe(int dir, const R *Vm, R gcL, R geL, c
     const R a2 = rdiv(gcA * Va[4], Va[0]);
     if (a2 <= R(0)) return ERR_SOUND;   // hy_eigenParameters aborts
     const R cf = rsqrt_(a2);
-    const R lam[5] = {unA - cf, unA, unA, unA, unA + cf};
+    R lam[5] = {unA - cf, unA, unA, unA, unA + cf};
+    if (entropy_fix) {   // hy_entropyFix.F90 on the two acoustic waves
+        const R a2L = rdiv(gcL * Vm[P], Vm[D]), a2R = rdiv(gcR * Vp[P], Vp[D]);
+        if (a2L <= R(0) || a2R <= R(0)) return ERR_SOUND;
+        const R uL = Vm[1 + dir], uR = Vp[1 + dir], cL = rsqrt_(a2L), cR = rsqrt_(a2R);
+        const R lL[2] = {uL - cL, uL + cL}, lR[2] = {uR - cR, uR + cR};
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            const int w = 4 * q;
+            if (lR[q] > R(0.) && lL[q] < R(0.)) {
+                if (entropy_fix == 1) {            // HartenHyman
+                    const R Lh = rdiv(lL[q] * (lR[q] - lam[w]), lR[q] - lL[q]);
+                    const R Rh = rdiv(lR[q] * (lam[w] - lL[q]), lR[q] - lL[q]);
+                    lam[w] = Rh - Lh;
+                } else {                            // Harten
+                    const R dl = fmax2(R(4.0) * (lR[q] - lL[q]), R(0.0));
+                    if (fabs(lam[w]) < R(0.5) * dl) {
+                        if (lam[w] >= R(0.0)) lam[w] = (rdiv(lam[w] * lam[w], dl) + R(.25) * dl);
+                        else lam[w] = -(rdiv(lam[w] * lam[w], dl) + R(.25) * dl);
+                    }
+                }
+            }
+        }
+    }
     const int v1 = 1 + dir, v2 = 1 + (dir + 1) % 3, v3 = 1 + (dir + 2) % 3;
     const R V1 = Va[v1], V2 = Va[v2], V3 = Va[v3];
     const R k = R(1.) - geA;
@@ -548,7 +573,7 @@ __device__ __forceinline__ int riemann(const DevParams &prm, int dir, const R *V
             for (int k = 0; k < 5; k++) F[k] = (FR[k] + FL[k] - smax * (UR[k] - UL[k])) * R(0.5);
             F[5] = (FR[5] + FL[5] - smax * (R(0.0) - R(0.0))) * R(0.5);
         } else if (ROE) {
-            const int e = riemann_roe(dir, Vm, gcL, geL, Vp, gcR, geR, UL, UR, FL, FR, F);
+            const int e = riemann_roe(dir, prm.entropy_fix, Vm, gcL, geL, Vp, gcR, geR, UL, UR, FL, FR, F);
             if (e) return e;
         } else if (hllc) {
             R qStar = Vp[D] * velNR * (SR - velNR) - Vm[D] * velNL * (SL - velNL) + Vm[P] - Vp[P];

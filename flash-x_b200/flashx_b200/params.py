@@ -31,6 +31,8 @@ class HydroParams:
     use_auxEintEqn: bool = True
     transOrder: int = 1
     use_flattening: bool = False
+    entropy: bool = False               # Roe's entropy fix (hy_entropyFix.F90)
+    entropyFixMethod: str = "HartenHyman"   # HartenHyman | Harten
     use_steepening: bool = False
     use_upwindTVD: bool = False
     use_avisc: bool = False
@@ -67,6 +69,8 @@ class HydroParams:
             raise ValueError("wenoMethod must be WENO5 or WENOZ")
         if self.transOrder != 1:
             raise ValueError("[hy_upwindTransverseFlux]: No high-order transFlux support! Please set transOrder=1.")
+        if self.entropyFixMethod.upper() not in ("HARTENHYMAN", "HARTEN"):
+            raise ValueError("entropyFixMethod must be HartenHyman or Harten")
         if self.use_flattening and self.useGravity:
             raise ValueError("use_flattening with gravity is not supported by this path")
         for flag in ("use_steepening", "use_upwindTVD", "use_avisc", "use_hybridOrder"):

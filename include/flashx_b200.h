@@ -70,6 +70,8 @@ typedef struct fxb_params {
     double gas_constant, abar; /* Eos Gamma: ideal gas constant, eos_singleSpeciesA  */
     int    precision;          /* enum fxb_precision                                 */
     int    flattening;         /* use_flattening (not combined with gravity)         */
+    int    entropy_fix;        /* Roe: entropy = .false. (0), entropyFixMethod
+                                  HartenHyman (1) or Harten (2)                     */
 } fxb_params;
 
 /* Domain of a uniform block grid. */

@@ -448,9 +448,10 @@ static int riemann_llf(const fxo_params *p, int dir, const double *Vm, const dou
     return 0;
 }
 
-/* hy_Roe.F90:62-205 (hydro, entropy = .false.): the mean state of
- * hy_avgState, its eigenvalues and conservative eigenvectors
- * (OnlyHydro/hy_eigenVector.F90:128-166, cons = .true.), and the flux
+/* hy_Roe.F90:62-205 (hydro): the mean state of hy_avgState, its eigenvalues
+ * (the acoustic ones corrected by hy_entropyFix.F90 when entropy = .true.)
+ * and conservative eigenvectors (OnlyHydro/hy_eigenVector.F90:128-166,
+ * cons = .true.), and the flux
  * (FL + FR - sum_k |lambda_k| r_k (l_k . (UR - UL))) / 2; the dot products
  * run over all five rows, zeros included, as dot_product does. */
 static int riemann_roe(const fxo_params *p, int dir, const double *Vm, const double *Vp, double Fs[6], double *speed)
@@ -479,7 +480,28 @@ static int riemann_roe(const fxo_params *p, int dir, const double *Vm, const dou
     const double a2 = Va[H_GC] * Va[H_P] / Va[H_D];
     if (a2 <= 0.) return 1;
     const double cf = sqrt(a2), un = Va[H_VX + dir];
-    const double lam[5] = {un - cf, un, un, un, un + cf};
+    double lam[5] = {un - cf, un, un, un, un + cf};
+    if (p->entropy_fix) {   /* hy_entropyFix.F90 on the two acoustic waves */
+        const double a2L = Vm[H_GC] * Vm[H_P] / Vm[H_D], a2R = Vp[H_GC] * Vp[H_P] / Vp[H_D];
+        if (a2L <= 0. || a2R <= 0.) return 1;
+        const double uL = Vm[H_VX + dir], uR = Vp[H_VX + dir], cL = sqrt(a2L), cR = sqrt(a2R);
+        const double lL[5] = {uL - cL, uL, uL, uL, uL + cL}, lR[5] = {uR - cR, uR, uR, uR, uR + cR};
+        for (int w = 0; w < 5; w += 4) {
+            if (lR[w] > 0. && lL[w] < 0.) {
+                if (p->entropy_fix == 1) {          /* HartenHyman */
+                    const double Lh = lL[w] * (lR[w] - lam[w]) / (lR[w] - lL[w]);
+                    const double Rh = lR[w] * (lam[w] - lL[w]) / (lR[w] - lL[w]);
+                    lam[w] = Rh - Lh;
+                } else {                             /* Harten */
+                    const double dl = fmax2(4.0 * (lR[w] - lL[w]), 0.0);
+                    if (fabs(lam[w]) < 0.5 * dl) {
+                        if (lam[w] >= 0.0) lam[w] = (lam[w] * lam[w] / dl + .25 * dl);
+                        else lam[w] = -(lam[w] * lam[w] / dl + .25 * dl);
+                    }
+                }
+            }
+        }
+    }
     /* conservative eigenvectors: rows D, MX, MY, MZ, E; columns the five waves */
     const int v1 = H_VX + dir, v2 = H_VX + (dir + 1) % 3, v3 = H_VX + (dir + 2) % 3;
     const double V1 = Va[v1], V2 = Va[v2], V3 = Va[v3];

@@ -55,6 +55,7 @@ typedef struct {
     double limited_beta;            /* LimitedSlopeBeta */
     double gas_constant, abar;      /* Eos Gamma: R and singleSpeciesA */
     int flattening;                 /* use_flattening */
+    int entropy_fix;                /* Roe: entropy off (0), HartenHyman (1), Harten (2) */
 } fxo_params;
 
 /* Number of doubles in one UNK array for the given geometry. */

@@ -80,7 +80,9 @@ def test_parameter_validation_mirrors_hydro_init():
     HydroParams(use_flattening=True).validate()
     HydroParams(RiemannSolver="LLF").validate()
     HydroParams(RiemannSolver="Roe").validate()
-    for bad in (dict(order=2), dict(RiemannSolver="Marquina"), dict(slopeLimiter="superbee"),
+    HydroParams(RiemannSolver="Roe", entropy=True, entropyFixMethod="Harten").validate()
+    for bad in (dict(order=2), dict(RiemannSolver="Marquina"), dict(entropyFixMethod="Einfeldt"),
+                dict(slopeLimiter="superbee"),
                 dict(transOrder=3), dict(use_steepening=True), dict(use_flattening=True, useGravity=True),
                 dict(hydroComputeDtOption=0)):
         with pytest.raises(ValueError):

@@ -327,3 +327,34 @@ def test_compute_dt_location(need_gpu, name):
     dev.sync_to_host(out)
     assert loc2 == _expected_loc(geom, out)
     dev.close()
+
+
+def _transonic_rarefaction(hp):
+    """Toro's test 1 along x (rho, u, p = 1, 0.75, 1 | 0.125, 0, 0.1 at x = 0.3):
+    its left rarefaction is sonic, so the acoustic eigenvalues change sign
+    across faces and Roe's entropy fix acts."""
+    geom = Geometry(2, 16, 16, 1, 4, 1, 1, bc=(BC_OUTFLOW,) * 4 + (BC_OUTFLOW, BC_OUTFLOW))
+    nx, ny = geom.nxb * geom.nblockx, geom.nyb * geom.nblocky
+    xc = (np.arange(nx) + 0.5) / nx
+    X = np.broadcast_to(xc, (1, ny, nx))
+    left = X < 0.3
+    rho = np.where(left, 1.0, 0.125)
+    vx = np.where(left, 0.75, 0.0)
+    p = np.where(left, 1.0, 0.1)
+    f = S._finish(hp, rho, vx, 0 * X, 0 * X, p)
+    return geom, S.scatter_global(geom, f)
+
+
+@pytest.mark.parametrize("entropy,method", [(False, "HartenHyman"), (True, "HartenHyman"), (True, "Harten")])
+def test_roe_entropy_fix_fp64(oracle, need_gpu, entropy, method):
+    hp = HydroParams(RiemannSolver="Roe", entropy=entropy, entropyFixMethod=method)
+    geom, unk = _transonic_rarefaction(hp)
+    p = oracle.make_params(geom.as_dict(), hp)
+    dts, ref = oracle_dts(oracle, geom, hp, unk, 5, first=0.5 * oracle.compute_dt(p, unk))
+    _, out = gpu_run(geom, hp, unk, dts)
+    g, r = compare(geom, out, ref)
+    assert np.array_equal(g, r)
+    if entropy:   # the fix changes the solution here
+        hp0 = HydroParams(RiemannSolver="Roe")
+        _, ref0 = oracle_dts(oracle, geom, hp0, unk, 5, first=dts[0])
+        assert not np.array_equal(ref, ref0)
