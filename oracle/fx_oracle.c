@@ -448,6 +448,37 @@ static int riemann_llf(const fxo_params *p, int dir, const double *Vm, const dou
     return 0;
 }
 
+/* OnlyHydro/hy_eigenVector.F90:128-166 (cons = .true.): conservative left
+ * and right eigenvectors of state V (D, VX, VY, VZ, P, GC, GE), rows D, MX,
+ * MY, MZ, E, columns the five waves */
+static void cons_eigen(const double *Va, int dir, double cf, double L[5][5], double R[5][5])
+{
+    /* conservative eigenvectors: rows D, MX, MY, MZ, E; columns the five waves */
+    const int v1 = H_VX + dir, v2 = H_VX + (dir + 1) % 3, v3 = H_VX + (dir + 2) % 3;
+    const double V1 = Va[v1], V2 = Va[v2], V3 = Va[v3];
+    const double k = 1. - Va[H_GE];
+    const double a2e = cf * cf, a2inv = 1. / a2e, Na = 0.5 * a2inv;
+    double u2 = 0.;
+    u2 = u2 + Va[H_VX] * Va[H_VX]; u2 = u2 + Va[H_VY] * Va[H_VY]; u2 = u2 + Va[H_VZ] * Va[H_VZ];
+    u2 = 0.5 * u2;
+    const double H = (Va[H_D] * u2 - Va[H_P] / k + Va[H_P]) / Va[H_D];
+    memset(L, 0, sizeof(double) * 25); memset(R, 0, sizeof(double) * 25);
+    const int E = H_P;
+    L[H_D][0] = Na * (-(k * u2) + V1 * cf); L[v1][0] = -(Na * (-(k * V1) + cf));
+    L[v2][0] = Na * k * V2; L[v3][0] = Na * k * V3; L[E][0] = -(Na * k);
+    L[H_D][1] = -V2; L[v2][1] = 1.;
+    L[H_D][2] = 1. + Na * k * u2 * 2.;
+    L[v1][2] = -(k * V1 * a2inv); L[v2][2] = -(k * V2 * a2inv); L[v3][2] = -(k * V3 * a2inv); L[E][2] = k * a2inv;
+    L[H_D][3] = -V3; L[v3][3] = 1.;
+    L[H_D][4] = Na * (-(k * u2) - V1 * cf); L[v1][4] = -(Na * (-(k * V1) - cf));
+    L[v2][4] = Na * k * V2; L[v3][4] = Na * k * V3; L[E][4] = -(Na * k);
+    R[H_D][0] = 1.; R[v1][0] = V1 - cf; R[v2][0] = V2; R[v3][0] = V3; R[E][0] = H - V1 * cf;
+    R[v2][1] = 1.; R[E][1] = V2;
+    R[H_D][2] = 1.; R[v1][2] = V1; R[v2][2] = V2; R[v3][2] = V3; R[E][2] = u2;
+    R[v3][3] = 1.; R[E][3] = V3;
+    R[H_D][4] = 1.; R[v1][4] = V1 + cf; R[v2][4] = V2; R[v3][4] = V3; R[E][4] = H + V1 * cf;
+}
+
 /* hy_Roe.F90:62-205 (hydro): the mean state of hy_avgState, its eigenvalues
  * (the acoustic ones corrected by hy_entropyFix.F90 when entropy = .true.)
  * and conservative eigenvectors (OnlyHydro/hy_eigenVector.F90:128-166,
@@ -502,31 +533,8 @@ static int riemann_roe(const fxo_params *p, int dir, const double *Vm, const dou
             }
         }
     }
-    /* conservative eigenvectors: rows D, MX, MY, MZ, E; columns the five waves */
-    const int v1 = H_VX + dir, v2 = H_VX + (dir + 1) % 3, v3 = H_VX + (dir + 2) % 3;
-    const double V1 = Va[v1], V2 = Va[v2], V3 = Va[v3];
-    const double k = 1. - Va[H_GE];
-    const double a2e = cf * cf, a2inv = 1. / a2e, Na = 0.5 * a2inv;
-    double u2 = 0.;
-    u2 = u2 + Va[H_VX] * Va[H_VX]; u2 = u2 + Va[H_VY] * Va[H_VY]; u2 = u2 + Va[H_VZ] * Va[H_VZ];
-    u2 = 0.5 * u2;
-    const double H = (Va[H_D] * u2 - Va[H_P] / k + Va[H_P]) / Va[H_D];
     double L[5][5], R[5][5];
-    memset(L, 0, sizeof(L)); memset(R, 0, sizeof(R));
-    const int E = H_P;
-    L[H_D][0] = Na * (-(k * u2) + V1 * cf); L[v1][0] = -(Na * (-(k * V1) + cf));
-    L[v2][0] = Na * k * V2; L[v3][0] = Na * k * V3; L[E][0] = -(Na * k);
-    L[H_D][1] = -V2; L[v2][1] = 1.;
-    L[H_D][2] = 1. + Na * k * u2 * 2.;
-    L[v1][2] = -(k * V1 * a2inv); L[v2][2] = -(k * V2 * a2inv); L[v3][2] = -(k * V3 * a2inv); L[E][2] = k * a2inv;
-    L[H_D][3] = -V3; L[v3][3] = 1.;
-    L[H_D][4] = Na * (-(k * u2) - V1 * cf); L[v1][4] = -(Na * (-(k * V1) - cf));
-    L[v2][4] = Na * k * V2; L[v3][4] = Na * k * V3; L[E][4] = -(Na * k);
-    R[H_D][0] = 1.; R[v1][0] = V1 - cf; R[v2][0] = V2; R[v3][0] = V3; R[E][0] = H - V1 * cf;
-    R[v2][1] = 1.; R[E][1] = V2;
-    R[H_D][2] = 1.; R[v1][2] = V1; R[v2][2] = V2; R[v3][2] = V3; R[E][2] = u2;
-    R[v3][3] = 1.; R[E][3] = V3;
-    R[H_D][4] = 1.; R[v1][4] = V1 + cf; R[v2][4] = V2; R[v3][4] = V3; R[E][4] = H + V1 * cf;
+    cons_eigen(Va, dir, cf, L, R);
     *speed = fabs(un) + fabs(cf);
     double UL[5], UR[5], FL[6], FR[6], dU[5];
     prim2con(Vm, UL); prim2con(Vp, UR);

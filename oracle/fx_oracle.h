@@ -30,7 +30,7 @@ enum { FXO_DENS = 0, FXO_EINT, FXO_ENER, FXO_GAMC, FXO_GAME, FXO_PRES,
        FXO_SHOK, FXO_TEMP, FXO_VELX, FXO_VELY, FXO_VELZ, FXO_NUNK };
 
 enum { FXO_BC_PERIODIC = 0, FXO_BC_OUTFLOW = 1, FXO_BC_REFLECTING = 2 };
-enum { FXO_ROE = 1, FXO_LLF = 2, FXO_HLL = 3, FXO_HLLC = 4 };   /* UHD.h:365-372 */
+enum { FXO_ROE = 1, FXO_LLF = 2, FXO_HLL = 3, FXO_HLLC = 4 };   /* UHD.h:59-62 */
 enum { FXO_MINMOD = 1, FXO_MC = 2, FXO_VANLEER = 3, FXO_HYBRID = 4,
        FXO_LIMITED = 5 };
 
