@@ -421,6 +421,7 @@ extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, cons
     q.limited_beta = p.limited_beta; q.gas_constant = p.gas_constant; q.abar = p.abar;
     q.flattening = p.flattening ? 1 : 0;
     q.entropy_fix = p.entropy_fix;
+    q.steepening = p.steepening ? 1 : 0;
     // Gamma/Eos_init.F90:86 and Gamma/Eos.F90:177,240-241
     double gammam1 = 1.0 / (p.gamma - 1.0);
     L.gam1inv = 1. / gammam1;

@@ -30,6 +30,7 @@ struct DevParams {
     double cfl, gamma, eint_switch, small_dens, small_e, small_p, tiny, fpres, limited_beta, gas_constant, abar;
     int flattening;
     int entropy_fix;           // Roe: 0 off, 1 Harten-Hyman, 2 Harten
+    int steepening;            // PPM contact steepening
 };
 
 // ---- precision helpers ---------------------------------------------------
@@ -311,6 +312,31 @@ __device__ __forceinline__ void flatten(R F, const R *Vc, R vecL[6], R vecR[6])
     }
 }
 
+// contact steepening of the PPM density interface values
+// (hy_DataReconstructNormalDir_PPM.F90:650-681; eta1 = 20, eta2 = 0.05,
+// epsln = 0.01, K0 = 0.1 from :149).  Vm, Vc, Vp: the three cells in sweep
+// order, rhoMM / rhoPP the densities two cells out, dbN0 / dbP0 the density
+// slopes of the two neighbours, delta the cell width along the sweep.
+template <class R>
+__device__ __forceinline__ void steepen(R tiny, R delta, R rhoMM, const R *Vm, const R *Vc, const R *Vp, R rhoPP,
+                                        R gameC, R dbN0, R dbP0, R vecL[6], R vecR[6])
+{
+    const R temp1 = Vp[0] - Vm[0];
+    if (fabs(temp1) > tiny) {
+        const R d2R = rdiv(rhoPP - R(2.) * Vp[0] + Vc[0], R(6.) * delta * delta);
+        const R d2L = rdiv(Vc[0] - R(2.) * Vm[0] + rhoMM, R(6.) * delta * delta);
+        R eta = rdiv((d2L - d2R) * (delta * delta), temp1);
+        if (d2R * d2L >= R(0.)) eta = R(0.);
+        if (R(0.01) * fmin2(Vp[0], Vm[0]) - fabs(Vp[0] - Vm[0]) >= R(0.)) eta = R(0.);
+        eta = fmax2(R(0.), fmin2(R(1.), R(20.) * (eta - R(0.05))));
+        const R temp2 = rdiv(fabs(Vp[4] - Vm[4]), fmin2(Vp[4], Vm[4]));
+        const R temp3 = rdiv(fabs(Vp[0] - Vm[0]), fmin2(Vp[0], Vm[0]));
+        if (gameC * R(0.1) * temp3 - temp2 < R(0.0)) eta = R(0.);
+        vecL[0] = vecL[0] * (R(1.) - eta) + (Vm[0] + R(0.5) * dbN0) * eta;
+        vecR[0] = vecR[0] * (R(1.) - eta) + (Vp[0] - R(0.5) * dbP0) * eta;
+    }
+}
+
 // PPM interface values (hy_DataReconstructNormalDir_PPM.F90:590-593)
 template <class R>
 __device__ __forceinline__ void ppm_interfaces(const R *Vm, const R *Vc, const R *Vp,
@@ -430,9 +456,9 @@ __device__ __forceinline__ void gravity_faces(const DevParams &prm, R g, R &gl, 
 // when entropy = .true.): the mean state of hy_avgState, its
 // conservative eigenvectors (OnlyHydro/hy_eigenVector.F90:128-166) and
 // F = (FL + FR - sum_w |lambda_w| r_w (l_w . (UR - UL))) / 2, the dot products
-// over all five rows, zeros included, as dot_product does.  Only the kernels
-// instantiated for RiemannSolver = Roe contain it, so the other solvers keep
-// their register allocation.
+// over all five rows, zeros included, as dot_product does.  Only the kernel
+// instantiations for the rarely used options (EXT: Roe, contact steepening)
+// contain it, so the default kernels keep their register allocation.
 template <class R>
 __device__ __forceinline__ int riemann_roe(int dir, int entropy_fix, const R *Vm, R gcL, R geL, const R *Vp, R gcR, R geR,
                                         const R UL[5], const R UR[5], const R FL[6], const R FR[6], R F[8])
@@ -514,14 +540,15 @@ __device__ __forceinline__ int riemann_roe(int dir, int entropy_fix, const R *Vm
     return 0;
 }
 
-template <class R, bool ROE>
+template <class R, bool EXT>
 __device__ __forceinline__ int riemann(const DevParams &prm, int dir, const R *Vm, R gcL, R geL,
                                        const R *Vp, R gcR, R geR, R F[8])
 {
     const R velNL = Vm[1 + dir], velNR = Vp[1 + dir];
     const R aL2 = rdiv(gcL * Vm[P], Vm[D]);
     const R aR2 = rdiv(gcR * Vp[P], Vp[D]);
-    const bool hllc = !ROE && prm.riemann == 4, llf = !ROE && prm.riemann == 2;
+    const bool roe = EXT && prm.riemann == 1;
+    const bool hllc = !roe && prm.riemann == 4, llf = !roe && prm.riemann == 2;
     const R tiny = hllc ? R(prm.tiny) : R(1.e-32);
     if ((Vm[D] < tiny && Vm[D] > R(0)) || (Vp[D] < tiny && Vp[D] > R(0)) ||
         (Vm[P] < tiny && Vm[P] > R(0)) || (Vp[P] < tiny && Vp[P] > R(0))) {
@@ -572,7 +599,7 @@ __device__ __forceinline__ int riemann(const DevParams &prm, int dir, const R *V
 #pragma unroll
             for (int k = 0; k < 5; k++) F[k] = (FR[k] + FL[k] - smax * (UR[k] - UL[k])) * R(0.5);
             F[5] = (FR[5] + FL[5] - smax * (R(0.0) - R(0.0))) * R(0.5);
-        } else if (ROE) {
+        } else if (roe) {
             const int e = riemann_roe(dir, prm.entropy_fix, Vm, gcL, geL, Vp, gcR, geR, UL, UR, FL, FR, F);
             if (e) return e;
         } else if (hllc) {

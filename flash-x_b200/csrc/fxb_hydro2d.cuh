@@ -143,7 +143,7 @@ __device__ __forceinline__ void analysis_stage(const Args2D &a, Smem2D<R> &s, in
 // face states of one cell along dir, with the transverse correction of the
 // other direction (hy_dataReconstOneStep.F90:931-936) and the negativity
 // fallback (:1131-1165); stores global-order Wp/Wm into s.W[.][t].
-template <class R>
+template <class R, bool EXT>
 __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int dir, int t, int wx, int wy,
                                              int dbi, int dbstep, R dtn, R hdtn, R hdtt)
 {
@@ -179,6 +179,9 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
             dbP[k] = s.DBF[k * NDB + dbi + dbstep];
         }
         ppm_interfaces(Vm, Vc, Vp, dbN, db0, dbP, vecL, vecR);
+        if (EXT && a.prm.steepening)
+            steepen(R(a.prm.tiny), R(dir == 0 ? a.dx : a.dy), s.V[D][wy - 2 * oy][wx - 2 * ox], Vm, Vc, Vp,
+                    s.V[D][wy + 2 * oy][wx + 2 * ox], s.V[GE][wy][wx], dbN[0], dbP[0], vecL, vecR);
     }
     if (a.prm.flattening) {
         // the window origin is the tile origin minus three cells
@@ -205,21 +208,21 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
     for (int k = 0; k < 6; k++) { s.W[k][t] = Wp[k]; s.W[6 + k][t] = Wm[k]; }
 }
 
-template <class R, bool ROE>
+template <class R, bool EXT>
 __device__ __forceinline__ void faces_stage(const Args2D &a, Smem2D<R> &s, int dir, int t, int wl, int wr,
                                             int wxl, int wyl, int wxr, int wyr)
 {
     R VL[6], VR[6], F[8];
 #pragma unroll
     for (int k = 0; k < 6; k++) { VL[k] = s.W[k][wl]; VR[k] = s.W[6 + k][wr]; }
-    int e = riemann<R, ROE>(a.prm, dir, VL, s.V[GC][wyl][wxl], s.V[GE][wyl][wxl],
+    int e = riemann<R, EXT>(a.prm, dir, VL, s.V[GC][wyl][wxl], s.V[GE][wyl][wxl],
                     VR, s.V[GC][wyr][wxr], s.V[GE][wyr][wxr], F);
     if (e) set_err(a.err, e);
 #pragma unroll
     for (int k = 0; k < NF; k++) s.DBF[k * NFC + t] = F[k];
 }
 
-template <class R, bool ROE>
+template <class R, bool EXT>
 __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::value) hydro2d_kernel(const Args2D a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -293,13 +296,13 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
     // ---- C: x face states
     for (int t = tid; t < NW; t += NT2) {
         int ii = t % (T2 + 2) - 1, jj = t / (T2 + 2);
-        states_stage(a, s, 0, t, ii + 3, jj + 3, jj * (T2 + 4) + ii + 2, 1, dtnx, hdtnx, hdty);
+        states_stage<R, EXT>(a, s, 0, t, ii + 3, jj + 3, jj * (T2 + 4) + ii + 2, 1, dtnx, hdtnx, hdty);
     }
     __syncthreads();
     // ---- D: x faces
     for (int t = tid; t < NFC; t += NT2) {
         int fi = t % (T2 + 1), jj = t / (T2 + 1);
-        faces_stage<R, ROE>(a, s, 0, t, jj * (T2 + 2) + fi, jj * (T2 + 2) + fi + 1, fi + 2, jj + 3, fi + 3, jj + 3);
+        faces_stage<R, EXT>(a, s, 0, t, jj * (T2 + 2) + fi, jj * (T2 + 2) + fi + 1, fi + 2, jj + 3, fi + 3, jj + 3);
     }
     __syncthreads();
 
@@ -339,13 +342,13 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
     // ---- G: y face states
     for (int t = tid; t < NW; t += NT2) {
         int ii = t % T2, jj = t / T2 - 1;
-        states_stage(a, s, 1, t, ii + 3, jj + 3, (jj + 2) * T2 + ii, T2, dtny, hdtny, hdtx);
+        states_stage<R, EXT>(a, s, 1, t, ii + 3, jj + 3, (jj + 2) * T2 + ii, T2, dtny, hdtny, hdtx);
     }
     __syncthreads();
     // ---- H: y faces
     for (int t = tid; t < NFC; t += NT2) {
         int ii = t % T2, fj = t / T2;
-        faces_stage<R, ROE>(a, s, 1, t, fj * T2 + ii, (fj + 1) * T2 + ii, ii + 3, fj + 2, ii + 3, fj + 3);
+        faces_stage<R, EXT>(a, s, 1, t, fj * T2 + ii, (fj + 1) * T2 + ii, ii + 3, fj + 2, ii + 3, fj + 3);
     }
     __syncthreads();
 

@@ -498,7 +498,7 @@ __device__ __forceinline__ void face_states_tail(const Args3D &a, const Ctx3<R, 
 // One instantiation per reconstruction order, so the register allocation of
 // the PPM path (three eigensystems and slopes) and of the WENO path (one
 // eigensystem, five projected cells) do not add up.
-template <class R, int ORDER, bool AMR, int DIR>
+template <class R, int ORDER, bool AMR, int DIR, bool EXT>
 __device__ __forceinline__ void face_states(const Args3D &a, const Ctx3<R, AMR> &X, const double dt, const R dtn,
                                             const R hdtn, const R hdtx, const R hdty, const R hdtz, int i, int j,
                                             int k, R Wm_out[6], R Wp_out[6], R &gc_out, R &ge_out)
@@ -535,6 +535,13 @@ __device__ __forceinline__ void face_states(const Args3D &a, const Ctx3<R, AMR> 
             dbP[q] = X.slp[(long)q * ns + sP];
         }
         ppm_interfaces(S[1], S[2], S[3], dbN, db0, dbP, vecL, vecR);
+        if (EXT && a.prm.steepening) {   // densities two cells out along d
+            R Smm[8], Spp[8];
+            X.load(a, i - 2 * di, j - 2 * dj, k - 2 * dk, Smm);
+            X.load(a, i + 2 * di, j + 2 * dj, k + 2 * dk, Spp);
+            steepen(R(a.prm.tiny), R(d == 0 ? X.dx : d == 1 ? X.dy : X.dz), Smm[D], S[1], S[2], S[3], Spp[D], vc[GE],
+                    dbN[0], dbP[0], vecL, vecR);
+        }
     }
     face_states_tail<R, AMR, DIR>(a, X, dt, dtn, hdtn, hdtx, hdty, hdtz, i, j, k, S[2], vc, eb, e, vecL, vecR, Wm_out,
                                   Wp_out);
@@ -563,7 +570,7 @@ template <class R> struct PwSlots {
 #ifndef FXB_S3_MINB_FP64
 #define FXB_S3_MINB_FP64 2
 #endif
-template <class R, int ORDER, bool AMR, int DIR>
+template <class R, int ORDER, bool AMR, int DIR, bool EXT>
 __global__ void __launch_bounds__(256, FXB_S3_MINB_FP64) states3d_kernel(const Args3D a)
 {
     constexpr int d = DIR;
@@ -580,7 +587,7 @@ __global__ void __launch_bounds__(256, FXB_S3_MINB_FP64) states3d_kernel(const A
         unflatten(idx, a.fdx[d == 0 ? 2 : 0], a.fdy[d == 1 ? 2 : 0], i, j, k);
         if (d == 0) i -= 1; else if (d == 1) j -= 1; else k -= 1;
         R Wm[6], Wp[6], gc, ge;
-        face_states<R, ORDER, AMR, DIR>(a, X, dt, dtn, hdtn, hdtx, hdty, hdtz, i, j, k, Wm, Wp, gc, ge);
+        face_states<R, ORDER, AMR, DIR, EXT>(a, X, dt, dtn, hdtn, hdtx, hdty, hdtz, i, j, k, Wm, Wp, gc, ge);
 #pragma unroll
         for (int q = 0; q < 6; q++) { w[(long)q * nw + idx] = Wp[q]; w[(long)(6 + q) * nw + idx] = Wm[q]; }
     }
@@ -589,7 +596,7 @@ __global__ void __launch_bounds__(256, FXB_S3_MINB_FP64) states3d_kernel(const A
 // ---- Riemann fluxes of direction d ---------------------------------------------
 // the direction is a template parameter so that the solver's per-direction
 // indexing of the state vectors resolves at compile time (no local memory)
-template <class R, bool AMR, int DIR, bool ROE>
+template <class R, bool AMR, int DIR, bool EXT>
 __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
 {
     constexpr int d = DIR;
@@ -609,7 +616,7 @@ __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
         for (int q = 0; q < 6; q++) { VL[q] = w[(long)q * nw + wl]; VR[q] = w[(long)(6 + q) * nw + wr]; }
         X.load_gammas(a, i - di, j - dj, k - dk, gcl, gel);
         X.load_gammas(a, i, j, k, gcr, ger);
-        int e = riemann<R, ROE>(a.prm, d, VL, gcl, gel, VR, gcr, ger, F);
+        int e = riemann<R, EXT>(a.prm, d, VL, gcl, gel, VR, gcr, ger, F);
         if (e) atomicOr(a.err, e);
 #pragma unroll
         for (int q = 0; q < NF; q++) f[(long)q * nf + idx] = F[q];
@@ -630,7 +637,7 @@ __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
 template <class R> struct SfluxRegs {
     static constexpr int value = (65536 / ((sizeof(R) == 8 ? 2 : 3) * FXB_SF_MAXT)) / 8 * 8;
 };
-template <class R, int ORDER, bool AMR, int DIR, bool ROE>
+template <class R, int ORDER, bool AMR, int DIR, bool EXT>
 __global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) sflux3d_kernel(const Args3D a)
 {
     constexpr int d = DIR;
@@ -694,13 +701,22 @@ __global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) 
                 dbP[q] = sD[q * nt + t + step];
             }
             ppm_interfaces(Sr[0], Sr[1], Sr[2], dbN, db0, dbP, vecL, vecR);
+            if (EXT && a.prm.steepening) {   // densities two cells out along d
+                int di, dj, dk;
+                offs(d, 1, di, dj, dk);
+                R Smm[8], Spp[8];
+                X.load(a, i - 2 * di, j - 2 * dj, k - 2 * dk, Smm);
+                X.load(a, i + 2 * di, j + 2 * dj, k + 2 * dk, Spp);
+                steepen(R(a.prm.tiny), R(d == 0 ? X.dx : d == 1 ? X.dy : X.dz), Smm[D], Sr[0], Sr[1], Sr[2], Spp[D],
+                        S8[1][GE], dbN[0], dbP[0], vecL, vecR);
+            }
             face_states_tail<R, AMR, DIR>(a, X, dt, dtn, hdtn, hdtx, hdty, hdtz, i, j, k, Sr[1], S8[1], eb, e, vecL,
                                           vecR, Wm, Wp);
             gc = S8[1][GC];
             ge = S8[1][GE];
         }
     } else {
-        if (st) face_states<R, ORDER, AMR, DIR>(a, X, dt, dtn, hdtn, hdtx, hdty, hdtz, i, j, k, Wm, Wp, gc, ge);
+        if (st) face_states<R, ORDER, AMR, DIR, EXT>(a, X, dt, dtn, hdtn, hdtx, hdty, hdtz, i, j, k, Wm, Wp, gc, ge);
     }
     if (st) {
 #pragma unroll
@@ -720,7 +736,7 @@ __global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) 
         R VL[6], F[NF];
 #pragma unroll
         for (int q = 0; q < 6; q++) VL[q] = sW[q * nt + tl];
-        const int e = riemann<R, ROE>(a.prm, d, VL, sW[6 * nt + tl], sW[7 * nt + tl], Wm, gc, ge, F);
+        const int e = riemann<R, EXT>(a.prm, d, VL, sW[6 * nt + tl], sW[7 * nt + tl], Wm, gc, ge, F);
         if (e) atomicOr(a.err, e);
         R *f = X.flx[d];
         const long nf = G.nf(d), fi = G.fidx(d, i, j, k);
@@ -859,16 +875,16 @@ inline size_t f3d_bytes(int d, int nx, int ny, int nz, size_t rsz)
 
 // face states and fluxes of one direction (PPM: slopes first); g.x CTAs per
 // block for the grid-stride kernels, g.y batch entries
-template <class R, bool AMR, int DIR, bool ROE> void launch_states3d_rs(const Args3D &a, dim3 g, cudaStream_t s)
+template <class R, bool AMR, int DIR, bool EXT> void launch_states3d_rs(const Args3D &a, dim3 g, cudaStream_t s)
 {
     if constexpr (!FusedFaces<R>::value) {
         if (a.prm.order == 5) {
-            states3d_kernel<R, 5, AMR, DIR><<<g, 256, 0, s>>>(a);
+            states3d_kernel<R, 5, AMR, DIR, EXT><<<g, 256, 0, s>>>(a);
         } else {
             slope3d_kernel<R, AMR><<<g, 256, 0, s>>>(a, DIR);
-            states3d_kernel<R, 3, AMR, DIR><<<g, 256, 0, s>>>(a);
+            states3d_kernel<R, 3, AMR, DIR, EXT><<<g, 256, 0, s>>>(a);
         }
-        flux3d_kernel<R, AMR, DIR, ROE><<<dim3(AMR ? a.cta[2] : g.x, g.y), 256, 0, s>>>(a);
+        flux3d_kernel<R, AMR, DIR, EXT><<<dim3(AMR ? a.cta[2] : g.x, g.y), 256, 0, s>>>(a);
     } else {
         const int N = DIR == 0 ? a.nx : DIR == 1 ? a.ny : a.nz;
         const int N1 = DIR == 0 ? a.ny : a.nx, N2 = DIR == 2 ? a.ny : a.nz;
@@ -876,17 +892,17 @@ template <class R, bool AMR, int DIR, bool ROE> void launch_states3d_rs(const Ar
         const int nseg = (N + Ls - 1) / (Ls - 1), nt1 = (N1 + T1 - 1) / T1;
         const dim3 gs((unsigned)(nseg * nt1 * N2), g.y);
         if (a.prm.order == 5) {
-            sflux3d_kernel<R, 5, AMR, DIR, ROE><<<gs, Ls * T1, 8 * sizeof(R) * (size_t)(Ls * T1), s>>>(a);
+            sflux3d_kernel<R, 5, AMR, DIR, EXT><<<gs, Ls * T1, 8 * sizeof(R) * (size_t)(Ls * T1), s>>>(a);
         } else {   // the slopes are computed in the kernel: two more cells per line
             const int nt = (Ls + 2) * T1;
-            sflux3d_kernel<R, 3, AMR, DIR, ROE><<<gs, nt, 14 * sizeof(R) * (size_t)nt, s>>>(a);
+            sflux3d_kernel<R, 3, AMR, DIR, EXT><<<gs, nt, 14 * sizeof(R) * (size_t)nt, s>>>(a);
         }
     }
 }
-// the Roe solver has its own kernel instantiations
+// the rarely used options (Roe, contact steepening) have kernel instantiations of their own
 template <class R, bool AMR, int DIR> void launch_states3d(const Args3D &a, dim3 g, cudaStream_t s)
 {
-    if (a.prm.riemann == 1) launch_states3d_rs<R, AMR, DIR, true>(a, g, s);
+    if (a.prm.riemann == 1 || a.prm.steepening) launch_states3d_rs<R, AMR, DIR, true>(a, g, s);
     else launch_states3d_rs<R, AMR, DIR, false>(a, g, s);
 }
 

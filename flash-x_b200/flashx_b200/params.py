@@ -73,7 +73,7 @@ class HydroParams:
             raise ValueError("entropyFixMethod must be HartenHyman or Harten")
         if self.use_flattening and self.useGravity:
             raise ValueError("use_flattening with gravity is not supported by this path")
-        for flag in ("use_steepening", "use_upwindTVD", "use_avisc", "use_hybridOrder"):
+        for flag in ("use_upwindTVD", "use_avisc", "use_hybridOrder"):
             if getattr(self, flag):
                 raise ValueError(flag + " is not supported by this path")
         if self.hydroComputeDtOption != -1:

@@ -72,6 +72,7 @@ typedef struct fxb_params {
     int    flattening;         /* use_flattening (not combined with gravity)         */
     int    entropy_fix;        /* Roe: entropy = .false. (0), entropyFixMethod
                                   HartenHyman (1) or Harten (2)                     */
+    int    steepening;         /* use_steepening: PPM contact steepening            */
 } fxb_params;
 
 /* Domain of a uniform block grid. */

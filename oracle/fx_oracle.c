@@ -220,6 +220,24 @@ static int recon_ppm(const fxo_params *p, int dir, double dt, double delta,
         vecL[n] = 0.5 * (Vc[n] + Vm[n]) - (db0[n] - dbN[n]) / 6.;
         vecR[n] = 0.5 * (Vc[n] + Vp[n]) - (dbP[n] - db0[n]) / 6.;
     }
+    /* [4] contact steepening, hy_DataReconstructNormalDir_PPM.F90:650-681
+     * (eta1 = 20, eta2 = 0.05, epsln = 0.01, K0 = 0.1 from :149) */
+    if (p->steepening) {
+        const double temp1 = Vp[H_D] - Vm[H_D];
+        if (fabs(temp1) > p->tiny) {
+            const double d2R = (S[4][H_D] - 2. * Vp[H_D] + Vc[H_D]) / (6. * delta * delta);
+            const double d2L = (Vc[H_D] - 2. * Vm[H_D] + S[0][H_D]) / (6. * delta * delta);
+            double eta = (d2L - d2R) * (delta * delta) / temp1;
+            if (d2R * d2L >= 0.) eta = 0.;
+            if (0.01 * fmin2(Vp[H_D], Vm[H_D]) - fabs(Vp[H_D] - Vm[H_D]) >= 0.) eta = 0.;
+            eta = fmax2(0., fmin2(1., 20. * (eta - 0.05)));
+            const double temp2 = fabs(Vp[H_P] - Vm[H_P]) / fmin2(Vp[H_P], Vm[H_P]);
+            const double temp3 = fabs(Vp[H_D] - Vm[H_D]) / fmin2(Vp[H_D], Vm[H_D]);
+            if (Vc[H_GE] * 0.1 * temp3 - temp2 < 0.0) eta = 0.;
+            vecL[H_D] = vecL[H_D] * (1. - eta) + (Vm[H_D] + 0.5 * dbN[H_D]) * eta;
+            vecR[H_D] = vecR[H_D] * (1. - eta) + (Vp[H_D] - 0.5 * dbP[H_D]) * eta;
+        }
+    }
     /* [5] flattening, hy_DataReconstructNormalDir_PPM.F90:687-690 */
     if (p->flattening)
         for (int n = 0; n < nend; n++) {

@@ -56,6 +56,7 @@ typedef struct {
     double gas_constant, abar;      /* Eos Gamma: R and singleSpeciesA */
     int flattening;                 /* use_flattening */
     int entropy_fix;                /* Roe: entropy off (0), HartenHyman (1), Harten (2) */
+    int steepening;                 /* use_steepening (PPM contact steepening) */
 } fxo_params;
 
 /* Number of doubles in one UNK array for the given geometry. */

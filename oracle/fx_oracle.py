@@ -42,7 +42,7 @@ class FxoParams(ctypes.Structure):
         ("tiny", ctypes.c_double), ("fpres", ctypes.c_double),
         ("limited_beta", ctypes.c_double),
         ("gas_constant", ctypes.c_double), ("abar", ctypes.c_double),
-        ("flattening", ctypes.c_int), ("entropy_fix", ctypes.c_int),
+        ("flattening", ctypes.c_int), ("entropy_fix", ctypes.c_int), ("steepening", ctypes.c_int),
     ]
 
 
@@ -114,6 +114,7 @@ def make_params(geom, hp):
     p.gas_constant, p.abar = hp.gasConstant, hp.eos_singleSpeciesA
     p.flattening = int(hp.use_flattening)
     p.entropy_fix = 0 if not hp.entropy else (1 if hp.entropyFixMethod.upper() == "HARTENHYMAN" else 2)
+    p.steepening = int(hp.use_steepening)
     return p
 
 

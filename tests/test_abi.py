@@ -81,9 +81,10 @@ def test_parameter_validation_mirrors_hydro_init():
     HydroParams(RiemannSolver="LLF").validate()
     HydroParams(RiemannSolver="Roe").validate()
     HydroParams(RiemannSolver="Roe", entropy=True, entropyFixMethod="Harten").validate()
+    HydroParams(use_steepening=True).validate()
     for bad in (dict(order=2), dict(RiemannSolver="Marquina"), dict(entropyFixMethod="Einfeldt"),
                 dict(slopeLimiter="superbee"),
-                dict(transOrder=3), dict(use_steepening=True), dict(use_flattening=True, useGravity=True),
+                dict(transOrder=3), dict(use_upwindTVD=True), dict(use_flattening=True, useGravity=True),
                 dict(hydroComputeDtOption=0)):
         with pytest.raises(ValueError):
             HydroParams(**bad).validate()

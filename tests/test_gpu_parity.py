@@ -109,6 +109,23 @@ def test_options_one_step_fp64(oracle, need_gpu, opts):
     assert np.array_equal(g, r)
 
 
+@pytest.mark.parametrize("flattening", [False, True])
+def test_steepening_2d_fp64(oracle, need_gpu, flattening):
+    """use_steepening (PPM contact steepening) on the 45-degree Sod problem,
+    whose contact switches it on; with and without flattening."""
+    geom, _, init = S.config("sod2d", scale=0.25)
+    hp = HydroParams(use_steepening=True, use_flattening=flattening)
+    unk = init(geom, hp)
+    p = oracle.make_params(geom.as_dict(), hp)
+    dts, ref = oracle_dts(oracle, geom, hp, unk, 20, first=0.5 * oracle.compute_dt(p, unk))
+    _, out = gpu_run(geom, hp, unk, dts)
+    g, r = compare(geom, out, ref)
+    assert np.array_equal(g, r)
+    hp0 = HydroParams(use_flattening=flattening)
+    _, ref0 = oracle_dts(oracle, geom, hp0, unk, 20, first=dts[0])
+    assert not np.array_equal(ref, ref0)   # the steepening acted
+
+
 @pytest.mark.parametrize("order", [3, 5])
 def test_flattening_2d_fp64(oracle, need_gpu, order):
     """use_flattening on the 45-degree Sod problem, where the shock switches it on."""
@@ -214,7 +231,8 @@ def test_negative_pressure_reports_status(need_gpu):
 
 # ---------------------------------------------------------------- 3-D
 @pytest.mark.parametrize("case", ["ppm_periodic", "sod_outflow", "rt_weno_gravity", "hll_noctu", "wenoz_reflect",
-                                  "sod_flattening", "weno_flattening_reflect", "llf_sod", "roe_sod_reflect"])
+                                  "sod_flattening", "weno_flattening_reflect", "llf_sod", "roe_sod_reflect",
+                                  "sod_steepening"])
 def test_3d_fp64_matches_oracle(oracle, need_gpu, case):
     """3-D path (full CTU corner coupling, gravity, WENO) against the oracle,
     three steps, bit for bit."""
@@ -235,6 +253,10 @@ def test_3d_fp64_matches_oracle(oracle, need_gpu, case):
         geom = Geometry(3, 16, 16, 16, 1, 2, 1, bc=(BC_PERIODIC,) * 6)
         hp = HydroParams(RiemannSolver="HLL", use_3dFullCTU=False, slopeLimiter="minmod")
         unk = S.noisy_gas(geom, hp)
+    elif case == "sod_steepening":
+        geom = Geometry(3, 16, 16, 16, 2, 1, 1, bc=(BC_OUTFLOW,) * 6)
+        hp = HydroParams(use_steepening=True)
+        unk = S.sod(geom, hp, xangle=30.0, yangle=70.0, posn=0.6)
     elif case == "llf_sod":
         geom = Geometry(3, 16, 16, 16, 2, 1, 1, bc=(BC_OUTFLOW,) * 6)
         hp = HydroParams(RiemannSolver="LLF")
