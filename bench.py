@@ -62,6 +62,22 @@ def make_problem(name, scale=1.0):
     return geom, hp, init(geom, hp), None, geom.ncells
 
 
+def slab_split(geom, world, rank):
+    """N > 1 on a uniform grid: the whole grid is `world` copies of the
+    per-GPU grid stacked along its slowest axis (y in 2-D, z in 3-D), split
+    into one slab per rank with halos exchanged every step (weak scaling:
+    each GPU keeps the per-GPU grid's cells).  Returns (whole grid, slab)."""
+    import dataclasses
+    from flashx_b200.parallel import SlabDecomposition
+    ax = geom.ndim - 1
+    bbox = list(geom.bbox)
+    lo, hi = bbox[ax]
+    bbox[ax] = (lo, lo + world * (hi - lo))
+    key = "nblocky" if geom.ndim == 2 else "nblockz"
+    whole = dataclasses.replace(geom, bbox=tuple(bbox), **{key: getattr(geom, key) * world})
+    return whole, SlabDecomposition(whole, world, rank)
+
+
 def interiors(geom, unk, mesh):
     """Cell values of all (leaf) block interiors, (cells, var)."""
     from flashx_b200 import simulations as S
@@ -284,8 +300,16 @@ def run_ours(args):
 
     from flashx_b200.parallel import allreduce_min as global_min   # Driver_computeDt's AllReduce(MIN)
 
+    # uniform grids split into slabs over the ranks; AMR meshes run as replicas
+    slab = None
+    if world > 1 and mesh is None:
+        whole, slab = slab_split(geom, world, rank)
+
     def timed_run(precision):
-        dev = HydroDevice(geom, hp, precision, mesh=mesh)
+        if slab is not None:
+            dev = HydroDevice(whole, hp, precision, slab=slab)   # this rank's slab: the per-GPU grid's blocks
+        else:
+            dev = HydroDevice(geom, hp, precision, mesh=mesh)
         dev.attach_unk(unk0.copy())
         dt = global_min(0.5 * dev.Hydro_computeDt())
         ext = torch.cuda.ExternalStream(dev.lib.fxb_stream())
@@ -364,7 +388,12 @@ def run_ours(args):
             "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded initial state of the workload, Philox4x32-10 where random)",
             "config": {"workload": WORKLOADS[args.config] + ("" if args.scale == 1.0 else f" at scale {args.scale}"),
-                       "zones_per_gpu": ncell, "parallelism": "replicas" if world > 1 else "single",
+                       "zones_per_gpu": ncell,
+                       "parallelism": ("single" if world == 1 else
+                                       "replicas (one AMR mesh per GPU, common dt)" if slab is None else
+                                       f"slabs: {world} copies of the grid stacked along its slowest axis, one "
+                                       f"slab per GPU, halos of {slab.halos[0]} planes exchanged every step "
+                                       f"(NCCL send/recv), common dt (all-reduce)"),
                        "l2": "inputs larger than L2 (state %.0f MB vs 126 MB L2)" % (2 * 10 * 8 * ncell / 1e6),
                        "timing": "CUDA events on the library stream, device dt loop (CUDA graph)"},
             "clocks": clocks,

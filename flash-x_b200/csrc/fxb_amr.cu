@@ -982,7 +982,9 @@ long ne3() { long e = S.n + 2 * S.ng; return e * e * e; }
 Args3D batch_args(const double *dtv, double dt)
 {
     Args3D a;
-    memset(&a, 0, sizeof(a));
+    memset((void *)&a, 0, sizeof(a));
+    a.rate_c0 = 0;
+    a.rate_c1 = 0x7fffffffffffffffL;     // every leaf cell enters the CFL rate
     a.nx = a.ny = a.nz = S.n;
     for (int i = 0; i < 6; i++) a.bc[i] = S.C.dom.bc[i];
     a.dt_arg = dt; a.dtv = dtv;

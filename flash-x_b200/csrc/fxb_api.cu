@@ -22,8 +22,13 @@ struct Lib {
     DevParams dprm{};
     int dmap[NV_DEV];              // device variable -> UNK slot
     int nunk = 0;
-    int nx = 0, ny = 1, nz = 1;
+    int nx = 0, ny = 1, nz = 1;    // extents of the stored grid (a slab: its interior and halos)
     long ncell = 0, vstride = 0;
+    int gext[3] = {1, 1, 1};       // cells per axis of the whole grid (cell widths)
+    int kbc[6];                    // boundary handling of the stored grid (outflow beside a halo)
+    fxb_slab slab{};               // this rank's layers of the slowest axis and its halos
+    long plane = 1;                // cells in one plane of the slowest axis
+    int nint = 1;                  // interior planes of the slowest axis
     long unk_doubles = 0;
     double *buf[2] = {nullptr, nullptr};
     int cur = 0;
@@ -81,6 +86,7 @@ struct UnkGeom {
     int nx, ny, nz;
     int bc[6];
     long vstride;
+    int soff;      // stored plane of a global index of the slowest axis: global + soff
 };
 
 __global__ void unk_to_state_kernel(const double *__restrict__ unk, double *__restrict__ st, UnkGeom g,
@@ -96,8 +102,8 @@ __global__ void unk_to_state_kernel(const double *__restrict__ unk, double *__re
         int gj = g.ndim >= 2 ? g.ng : 0, gk = g.ndim == 3 ? g.ng : 0;
         long u = ((((long)blk * g.nkg + k + gk) * g.njg + j + gj) * g.nig + i + g.ng) * g.nunk;
         long gx = (long)bcoord[3 * blk] * g.nxb + i;
-        long gy = (long)bcoord[3 * blk + 1] * g.nyb + j;
-        long gz = (long)bcoord[3 * blk + 2] * g.nzb + k;
+        long gy = (long)bcoord[3 * blk + 1] * g.nyb + j + (g.ndim == 2 ? g.soff : 0);
+        long gz = (long)bcoord[3 * blk + 2] * g.nzb + k + (g.ndim == 3 ? g.soff : 0);
         long c = (gz * g.ny + gy) * g.nx + gx;
         for (int v = 0; v < NV_DEV; v++) st[v * g.vstride + c] = unk[u + dmap[v]];
     }
@@ -116,8 +122,9 @@ __global__ void state_to_unk_kernel(const double *__restrict__ st, double *__res
         int gj = g.ndim >= 2 ? g.ng : 0, gk = g.ndim == 3 ? g.ng : 0;
         double sx = 1.0, sy = 1.0, sz = 1.0;
         int mx = map_axis(bcoord[3 * blk] * g.nxb + i - g.ng, g.nx, g.bc[0], g.bc[1], &sx);
-        int my = g.ndim >= 2 ? map_axis(bcoord[3 * blk + 1] * g.nyb + j - gj, g.ny, g.bc[2], g.bc[3], &sy) : 0;
-        int mz = g.ndim == 3 ? map_axis(bcoord[3 * blk + 2] * g.nzb + k - gk, g.nz, g.bc[4], g.bc[5], &sz) : 0;
+        int my = g.ndim >= 2 ? map_axis(bcoord[3 * blk + 1] * g.nyb + j - gj + (g.ndim == 2 ? g.soff : 0), g.ny,
+                                        g.bc[2], g.bc[3], &sy) : 0;
+        int mz = g.ndim == 3 ? map_axis(bcoord[3 * blk + 2] * g.nzb + k - gk + g.soff, g.nz, g.bc[4], g.bc[5], &sz) : 0;
         long c = ((long)mz * g.ny + my) * g.nx + mx;
         long u = idx * g.nunk;
         for (int v = 0; v < NV_DEV; v++) {
@@ -249,17 +256,25 @@ UnkGeom unk_geom()
     g.nkg = g.ndim == 3 ? g.nzb + 2 * g.ng : 1;
     g.nunk = L.nunk;
     g.nx = L.nx; g.ny = L.ny; g.nz = L.nz;
-    for (int i = 0; i < 6; i++) g.bc[i] = L.dom.bc[i];
+    for (int i = 0; i < 6; i++) g.bc[i] = L.kbc[i];
     g.vstride = L.vstride;
+    const int nb = L.dom.ndim == 3 ? L.dom.nzb : L.dom.nyb;
+    g.soff = L.slab.halo_lo - L.slab.layer_lo * nb;
     return g;
 }
 
 double cell_dx(int a)
 {
-    int n = a == 0 ? L.nx : (a == 1 ? L.ny : L.nz);
     if (a >= L.dom.ndim) return 1.0;
-    return (L.dom.bbox[a][1] - L.dom.bbox[a][0]) / (double)n;
+    return (L.dom.bbox[a][1] - L.dom.bbox[a][0]) / (double)L.gext[a];
 }
+
+// the slab's own cells: first stored cell and extents (the slowest axis
+// without its halos)
+const double *interior(int buf) { return L.buf[buf] + (long)L.slab.halo_lo * L.plane; }
+int int_ny() { return L.dom.ndim == 2 ? L.nint : L.ny; }
+int int_nz() { return L.dom.ndim == 3 ? L.nint : 1; }
+bool has_halo() { return L.slab.halo_lo > 0 || L.slab.halo_hi > 0; }
 
 
 // launch one fused hydro step reading buffer `src`, writing 1-src
@@ -269,7 +284,9 @@ int launch_hydro(int src, const double *dtv, double dt)
         Args2D a;
         a.in = L.buf[src]; a.out = L.buf[1 - src]; a.vstride = L.vstride;
         a.nx = L.nx; a.ny = L.ny;
-        for (int i = 0; i < 4; i++) a.bc[i] = L.dom.bc[i];
+        for (int i = 0; i < 4; i++) a.bc[i] = L.kbc[i];
+        a.rate_c0 = (long)L.slab.halo_lo * L.plane;
+        a.rate_c1 = a.rate_c0 + (long)L.nint * L.plane;
         a.dx = cell_dx(0); a.dy = cell_dx(1);
         a.dt_arg = dt; a.dtv = dtv;
         a.gam1inv = L.gam1inv; a.ggprodinv = L.ggprodinv;
@@ -282,7 +299,9 @@ int launch_hydro(int src, const double *dtv, double dt)
         Args3D a;
         a.in = L.buf[src]; a.out = L.buf[1 - src]; a.vstride = L.vstride;
         a.nx = L.nx; a.ny = L.ny; a.nz = L.nz;
-        for (int i = 0; i < 6; i++) a.bc[i] = L.dom.bc[i];
+        for (int i = 0; i < 6; i++) a.bc[i] = L.kbc[i];
+        a.rate_c0 = (long)L.slab.halo_lo * L.plane;
+        a.rate_c1 = a.rate_c0 + (long)L.nint * L.plane;
         a.dx = cell_dx(0); a.dy = cell_dx(1); a.dz = cell_dx(2);
         a.dt_arg = dt; a.dtv = dtv;
         a.gam1inv = L.gam1inv; a.ggprodinv = L.ggprodinv;
@@ -368,6 +387,12 @@ int record_error(int code, const char *msg) { return fail(code, msg); }
 // ====================================================================== ABI
 extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, const int32_t *var_map, int nunk)
 {
+    return fxb_init_slab(params, domain, var_map, nunk, nullptr);
+}
+
+extern "C" int fxb_init_slab(const fxb_params *params, const fxb_domain *domain, const int32_t *var_map, int nunk,
+                             const fxb_slab *slab)
+{
     if (!params || !domain || !var_map) return fail(FXB_EARG, "fxb_init: null argument");
     if (L.inited) free_all();
     const fxb_domain &d = *domain;
@@ -391,15 +416,42 @@ extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, cons
     if (nunk < FXB_NVAR) return fail(FXB_EARG, "fxb_init: nunk too small");
     for (int v = 0; v < FXB_NVAR; v++)
         if (var_map[v] < 0 || var_map[v] >= nunk) return fail(FXB_EARG, "fxb_init: var_map out of range");
+    // the slab: layers of the slowest axis and halo planes (UG/Grid_fillGuardCells.F90:261-306)
+    const int sa = d.ndim - 1;                                   // split axis
+    const int nlay = sa == 1 ? d.nblocky : d.nblockz;            // block layers of the whole grid
+    const int nbs = sa == 1 ? d.nyb : d.nzb;                     // cells per block along it
+    fxb_slab sl = slab ? *slab : fxb_slab{0, nlay, 0, 0};
+    if (sl.layer_lo < 0 || sl.layer_hi > nlay || sl.layer_lo >= sl.layer_hi)
+        return fail(FXB_EARG, "fxb_init_slab: layer range outside the grid");
+    const int nint = (sl.layer_hi - sl.layer_lo) * nbs;
+    const bool periodic_s = d.bc[2 * sa] == FXB_BC_PERIODIC;
+    for (int side = 0; side < 2; side++) {
+        const int h = side ? sl.halo_hi : sl.halo_lo;
+        const bool edge = side ? sl.layer_hi == nlay : sl.layer_lo == 0;
+        if (h < 0 || h > nint || (h > 0 && h < d.nguard))
+            return fail(FXB_EARG, "fxb_init_slab: a halo must be 0 or between NGUARD and the slab's own planes");
+        if (!edge && h == 0) return fail(FXB_EARG, "fxb_init_slab: a side facing another slab needs a halo");
+        if (edge && h > 0 && !periodic_s)
+            return fail(FXB_EARG, "fxb_init_slab: a halo on a non-periodic domain boundary");
+    }
     L.prm = p;
     L.dom = d;
     L.nunk = nunk;
+    L.slab = sl;
+    L.nint = nint;
     for (int v = 0; v < NV_DEV; v++) L.dmap[v] = var_map[kDevToVar[v]];
-    L.nx = d.nxb * d.nblockx;
-    L.ny = d.ndim >= 2 ? d.nyb * d.nblocky : 1;
-    L.nz = d.ndim == 3 ? d.nzb * d.nblockz : 1;
+    for (int i = 0; i < 6; i++) L.kbc[i] = d.bc[i];
+    if (sl.halo_lo > 0) L.kbc[2 * sa] = FXB_BC_OUTFLOW;       // cells beyond a halo only feed halo cells
+    if (sl.halo_hi > 0) L.kbc[2 * sa + 1] = FXB_BC_OUTFLOW;
+    L.gext[0] = d.nxb * d.nblockx;
+    L.gext[1] = d.ndim >= 2 ? d.nyb * d.nblocky : 1;
+    L.gext[2] = d.ndim == 3 ? d.nzb * d.nblockz : 1;
+    L.nx = L.gext[0];
+    L.ny = sa == 1 ? nint + sl.halo_lo + sl.halo_hi : L.gext[1];
+    L.nz = sa == 2 ? nint + sl.halo_lo + sl.halo_hi : 1;
+    L.plane = sa == 1 ? (long)L.nx : (long)L.nx * L.ny;
     if (d.ndim == 2 && (L.nx % T2 || L.ny % T2))
-        return fail(FXB_EUNSUPPORTED, "fxb_init: 2-D grid extents must be multiples of 16");
+        return fail(FXB_EUNSUPPORTED, "fxb_init: 2-D grid extents (a slab's with its halos) must be multiples of 16");
     if (d.ndim == 3 && (L.nx % T3X || L.ny % T3Y || L.nz % T3Z))
         return fail(FXB_EUNSUPPORTED, "fxb_init: 3-D grid extents must be multiples of the 3-D tile");
     // the 3-D kernels walk padded boxes with 32-bit indices
@@ -407,7 +459,7 @@ extern "C" int fxb_init(const fxb_params *params, const fxb_domain *domain, cons
         return fail(FXB_EUNSUPPORTED, "fxb_init: 3-D grid larger than 2^30 cells");
     L.ncell = (long)L.nx * L.ny * L.nz;
     L.vstride = (L.ncell + 31) / 32 * 32;
-    L.nblk = d.nblockx * (d.ndim >= 2 ? d.nblocky : 1) * (d.ndim == 3 ? d.nblockz : 1);
+    L.nblk = d.nblockx * (d.ndim == 3 ? d.nblocky : 1) * (sl.layer_hi - sl.layer_lo);
     long per = (long)(d.nxb + 2 * d.nguard) * (d.ndim >= 2 ? d.nyb + 2 * d.nguard : 1) *
                (d.ndim == 3 ? d.nzb + 2 * d.nguard : 1);
     L.unk_doubles = per * L.nblk * nunk;
@@ -488,6 +540,9 @@ extern "C" int fxb_register_blocks(const fxb_block_desc *blocks, int nblk)
         L.graph_exec[i] = nullptr;
     }
     if (refined) {
+        const int nlay = L.dom.ndim == 3 ? L.dom.nblockz : L.dom.nblocky;
+        if (has_halo() || L.slab.layer_lo != 0 || L.slab.layer_hi != nlay)
+            return fail(FXB_EUNSUPPORTED, "fxb_register_blocks: a slab of a grid takes its level-1 blocks only");
         // block-structured AMR mesh: parents derived, leaves keep their UNK slots
         AmrCommon c;
         c.stream = L.stream; c.prm = L.prm; c.dom = L.dom; c.dprm = L.dprm; c.nunk = L.nunk;
@@ -497,17 +552,22 @@ extern "C" int fxb_register_blocks(const fxb_block_desc *blocks, int nblk)
         return amr_create(c, blocks, nblk);
     }
     amr_destroy();
+    // block coordinates stay those of the whole grid; a slab holds layers [lo, hi) of its slowest axis
+    const int sa = L.dom.ndim - 1;
+    int lo[3] = {0, 0, 0};
     int nb[3] = {L.dom.nblockx, L.dom.ndim >= 2 ? L.dom.nblocky : 1, L.dom.ndim == 3 ? L.dom.nblockz : 1};
+    lo[sa] = L.slab.layer_lo;
+    nb[sa] = L.slab.layer_hi - L.slab.layer_lo;
     int *h = new int[3 * nblk];
     char *seen = new char[nblk]();
     for (int b = 0; b < nblk; b++) {
         for (int a = 0; a < 3; a++) {
             int c = blocks[b].bcoord[a];
             if (a >= L.dom.ndim) c = 0;
-            if (c < 0 || c >= nb[a]) { delete[] h; delete[] seen; return fail(FXB_EARG, "fxb_register_blocks: block coordinate out of range"); }
+            if (c < lo[a] || c >= lo[a] + nb[a]) { delete[] h; delete[] seen; return fail(FXB_EARG, "fxb_register_blocks: block coordinate out of range"); }
             h[3 * b + a] = c;
         }
-        long lin = ((long)h[3 * b + 2] * nb[1] + h[3 * b + 1]) * nb[0] + h[3 * b];
+        long lin = ((long)(h[3 * b + 2] - lo[2]) * nb[1] + h[3 * b + 1] - lo[1]) * nb[0] + h[3 * b] - lo[0];
         if (seen[lin]) { delete[] h; delete[] seen; return fail(FXB_EARG, "fxb_register_blocks: duplicate block"); }
         seen[lin] = 1;
         if (blocks[b].level != 1) { delete[] h; delete[] seen; return fail(FXB_EUNSUPPORTED, "fxb_register_blocks: only level-1 (uniform) block lists"); }
@@ -613,7 +673,7 @@ extern "C" int fxb_compute_dt(double *dt_out, int32_t loc[5])
     }
     if (!L.rate_valid) {
         CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
-        rate_kernel<<<1184, 256, 0, L.stream>>>(L.buf[L.cur], L.vstride, L.nx, L.ny, L.nz, L.dom.ndim,
+        rate_kernel<<<1184, 256, 0, L.stream>>>(interior(L.cur), L.vstride, L.nx, int_ny(), int_nz(), L.dom.ndim,
                                                 cell_dx(0), cell_dx(1), cell_dx(2), L.rate_max);
         CK(cudaGetLastError());
         L.rate_valid = true;
@@ -627,7 +687,7 @@ extern "C" int fxb_compute_dt(double *dt_out, int32_t loc[5])
             int rc = amr_locate(dkey);
             if (rc) return rc;
         } else {
-            locate_kernel<<<1184, 256, 0, L.stream>>>(L.buf[L.cur], L.vstride, L.nx, L.ny, L.nz, L.dom.ndim, cell_dx(0),
+            locate_kernel<<<1184, 256, 0, L.stream>>>(interior(L.cur), L.vstride, L.nx, int_ny(), int_nz(), L.dom.ndim, cell_dx(0),
                                                       cell_dx(1), cell_dx(2), L.rate_max, L.dom.nxb,
                                                       L.dom.ndim >= 2 ? L.dom.nyb : 1, L.dom.ndim == 3 ? L.dom.nzb : 1,
                                                       dkey);
@@ -667,6 +727,7 @@ extern "C" int fxb_advance(int nsteps, double *dt, double *dt_old, double f, dou
 {
     if (!L.attached) return fail(FXB_EARG, "fxb_advance: no UNK attached");
     if (!dt || !dt_old || nsteps < 0) return fail(FXB_EARG, "fxb_advance: bad argument");
+    if (has_halo()) return fail(FXB_EUNSUPPORTED, "fxb_advance: a slab with halos exchanges them between steps");
     double h[2] = {*dt, *dt_old};
     CK(cudaMemcpyAsync(L.dtv, h, sizeof(h), cudaMemcpyHostToDevice, L.stream));
     CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
@@ -719,11 +780,58 @@ extern "C" int fxb_integrals(double out[7])
     if (!L.attached) return fail(FXB_EARG, "fxb_integrals: no UNK attached");
     if (amr_active()) return amr_integrals(out, L.partials, L.npartials);
     double dv = cell_dx(0) * cell_dx(1) * cell_dx(2);
-    integrals_kernel<<<L.npartials, 256, 0, L.stream>>>(L.buf[L.cur], L.vstride, L.ncell, dv, L.partials);
+    integrals_kernel<<<L.npartials, 256, 0, L.stream>>>(interior(L.cur), L.vstride, (long)L.nint * L.plane, dv,
+                                                        L.partials);
     integrals_final_kernel<<<1, 32, 0, L.stream>>>(L.partials, L.npartials, L.partials + L.npartials * 7);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, L.partials + L.npartials * 7, 7 * sizeof(double), cudaMemcpyDeviceToHost, L.stream));
     CK(cudaStreamSynchronize(L.stream));
+    return FXB_OK;
+}
+
+extern "C" long fxb_halo_doubles(int planes)
+{
+    if (!L.inited || planes < 0) return 0;
+    return (long)NV_DEV * planes * L.plane;
+}
+
+extern "C" int fxb_halo_pack(double *send_lo, int n_lo, double *send_hi, int n_hi)
+{
+    if (!L.attached) return fail(FXB_EARG, "fxb_halo_pack: no UNK attached");
+    if (n_lo < 0 || n_hi < 0 || n_lo > L.nint || n_hi > L.nint || (n_lo && !send_lo) || (n_hi && !send_hi))
+        return fail(FXB_EARG, "fxb_halo_pack: bad plane count or buffer");
+    // variable-major messages: one 2-D copy gathers the planes of all variables
+    const size_t spitch = sizeof(double) * L.vstride;
+    if (n_lo) {
+        const size_t w = sizeof(double) * n_lo * L.plane;
+        CK(cudaMemcpy2DAsync(send_lo, w, interior(L.cur), spitch, w, NV_DEV, cudaMemcpyDeviceToDevice, L.stream));
+    }
+    if (n_hi) {
+        const size_t w = sizeof(double) * n_hi * L.plane;
+        CK(cudaMemcpy2DAsync(send_hi, w, interior(L.cur) + (long)(L.nint - n_hi) * L.plane, spitch, w, NV_DEV,
+                             cudaMemcpyDeviceToDevice, L.stream));
+    }
+    return FXB_OK;
+}
+
+extern "C" int fxb_halo_unpack(const double *recv_lo, const double *recv_hi)
+{
+    if (!L.attached) return fail(FXB_EARG, "fxb_halo_unpack: no UNK attached");
+    const fxb_slab &sl = L.slab;
+    if ((sl.halo_lo && !recv_lo) || (sl.halo_hi && !recv_hi)) return fail(FXB_EARG, "fxb_halo_unpack: missing buffer");
+    const size_t dpitch = sizeof(double) * L.vstride;
+    double *st = L.buf[L.cur];
+    if (sl.halo_lo) {
+        const size_t w = sizeof(double) * sl.halo_lo * L.plane;
+        CK(cudaMemcpy2DAsync(st, dpitch, recv_lo, w, w, NV_DEV, cudaMemcpyDeviceToDevice, L.stream));
+    }
+    if (sl.halo_hi) {
+        const size_t w = sizeof(double) * sl.halo_hi * L.plane;
+        CK(cudaMemcpy2DAsync(st + (long)(sl.halo_lo + L.nint) * L.plane, dpitch, recv_hi, w, w, NV_DEV,
+                             cudaMemcpyDeviceToDevice, L.stream));
+    }
+    // the fused step's rate covers the slab's own cells only, so a halo
+    // update leaves a valid CFL rate valid
     return FXB_OK;
 }
 

@@ -38,6 +38,7 @@ struct Args2D {
     unsigned long long *rate_max;
     int *err;
     const void *flat;        // flattening coefficients [2][(nx+2)(ny+2)] of R, padded by one cell
+    long rate_c0 = 0, rate_c1 = 0x7fffffffffffffffL;   // cells [c0, c1) enter the CFL rate (a slab's own)
 };
 
 constexpr int T2 = 16;             // tile edge
@@ -404,6 +405,7 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
         double cs = sqrt(prm.gamma * pres / dens);
         rate = (fabs(vx - 0.) + cs) * (1.0 / a.dx);
         rate = fmax2(rate, (fabs(vy - 0.) + cs) * (1.0 / a.dy));
+        if (gidx < a.rate_c0 || gidx >= a.rate_c1) rate = 0.;
     }
     // CTA max, then one atomic per CTA (positive doubles order like their bits)
 #pragma unroll

@@ -79,6 +79,7 @@ struct Args3D {
     int cta[4];                 // CTAs per batch entry: sig3d, slope3d, (unused), update3d
     FastDiv fdx[5], fdy[5];     // divisors nx + e and ny + e (e = 0, 1, 2, 4), set by the launchers
     int sf_len[3], sf_lines[3]; // face-state tiles per direction (cells along d, lines), set by the launchers
+    long rate_c0 = 0, rate_c1 = 0x7fffffffffffffffL;   // cells [c0, c1) enter the CFL rate (a slab's own)
 };
 // Face-state tile of direction d (N cells along d, N1 along the t1 axis):
 // the fewest warp lanes in total (the N + 1 faces split into segments of
@@ -842,7 +843,7 @@ __global__ void __launch_bounds__(256, FXB_UPD_MINB) update3d_kernel(const Args3
         double r = (fabs(vx - 0.) + cs) * (1.0 / X.dx);
         r = fmax2(r, (fabs(vy - 0.) + cs) * (1.0 / X.dy));
         r = fmax2(r, (fabs(vz - 0.) + cs) * (1.0 / X.dz));
-        rate = fmax2(rate, r);
+        if (c >= a.rate_c0 && c < a.rate_c1) rate = fmax2(rate, r);
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) rate = fmax(rate, __shfl_xor_sync(0xffffffffu, rate, off));

@@ -30,7 +30,8 @@ FXB_VARS = ("dens", "eint", "ener", "gamc", "game", "pres", "temp", "velx", "vel
 ABI_SYMBOLS = ("fxb_init", "fxb_register_blocks", "fxb_attach_unk", "fxb_fill_guardcells",
                "fxb_hydro_step", "fxb_compute_dt", "fxb_advance", "fxb_eos", "fxb_sync_to_host",
                "fxb_sync_from_host", "fxb_integrals", "fxb_integrals_noalloc", "fxb_mark_refine_derefine",
-               "fxb_last_timing", "fxb_stream", "fxb_tuning", "fxb_last_error", "fxb_finalize")
+               "fxb_last_timing", "fxb_stream", "fxb_tuning", "fxb_last_error", "fxb_finalize",
+               "fxb_init_slab", "fxb_halo_doubles", "fxb_halo_pack", "fxb_halo_unpack")
 
 
 class FxbParams(ctypes.Structure):
@@ -58,6 +59,11 @@ class FxbDomain(ctypes.Structure):
 
 class FxbBlockDesc(ctypes.Structure):
     _fields_ = [("level", ctypes.c_int), ("bcoord", ctypes.c_int * 3)]
+
+
+class FxbSlab(ctypes.Structure):
+    _fields_ = [("layer_lo", ctypes.c_int), ("layer_hi", ctypes.c_int),
+                ("halo_lo", ctypes.c_int), ("halo_hi", ctypes.c_int)]
 
 
 class FxbError(ctypes.Structure):
@@ -103,8 +109,13 @@ def load_library(path=LIB_PATH):
     L.fxb_stream.restype = ctypes.c_void_p
     L.fxb_last_error.argtypes = [ctypes.POINTER(FxbError)]
     L.fxb_finalize.restype = None
+    L.fxb_init_slab.argtypes = L.fxb_init.argtypes + [ctypes.POINTER(FxbSlab)]
+    L.fxb_halo_doubles.argtypes = [ctypes.c_int]
+    L.fxb_halo_doubles.restype = ctypes.c_long
+    L.fxb_halo_pack.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+    L.fxb_halo_unpack.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     for name in ABI_SYMBOLS:
-        if name not in ("fxb_stream", "fxb_finalize"):
+        if name not in ("fxb_stream", "fxb_finalize", "fxb_halo_doubles"):
             getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -166,13 +177,22 @@ def default_var_map():
     return vm
 
 
-def leaf_blocks(geom: Geometry):
-    """Leaf-block list of a uniform block grid in Flash-X block order."""
-    n = geom.nblocks
+def leaf_blocks(geom: Geometry, layers=None):
+    """Leaf-block list of a uniform block grid in Flash-X block order; with
+    `layers` = (lo, hi) only the blocks of those layers of the slowest axis."""
+    ny = geom.nblocky if geom.ndim >= 2 else 1
+    nz = geom.nblockz if geom.ndim == 3 else 1
+    ys, zs = range(ny), range(nz)
+    if layers is not None:
+        if geom.ndim == 2:
+            ys = range(*layers)
+        else:
+            zs = range(*layers)
+    n = geom.nblockx * len(ys) * len(zs)
     arr = (FxbBlockDesc * n)()
     b = 0
-    for bz in range(geom.nblockz if geom.ndim == 3 else 1):
-        for by in range(geom.nblocky if geom.ndim >= 2 else 1):
+    for bz in zs:
+        for by in ys:
             for bx in range(geom.nblockx):
                 arr[b].level = 1
                 arr[b].bcoord[0], arr[b].bcoord[1], arr[b].bcoord[2] = bx, by, bz
@@ -195,16 +215,36 @@ class HydroDevice:
     """The unsplit hydro solver on one B200, behind the reference interface.
 
     `mesh` (a flashx_b200.amr.AmrMesh over `geom`'s root blocks) selects a
-    block-structured AMR mesh; without it the blocks form the uniform grid."""
+    block-structured AMR mesh; without it the blocks form the uniform grid.
+    `slab` (a flashx_b200.parallel.SlabDecomposition of `geom`) makes this
+    device one rank's slab of the uniform grid: it holds that rank's blocks
+    (UNK slots in the grid's block order) and exchanges halos with the
+    neighbouring ranks before each step and before guard cells go to the
+    host; Hydro_computeDt and integrals cover the rank's own cells, for the
+    caller to reduce over ranks."""
 
-    def __init__(self, geom: Geometry, hp: HydroParams, precision="fp64", mesh=None):
+    def __init__(self, geom: Geometry, hp: HydroParams, precision="fp64", mesh=None, slab=None):
         self.lib = load_library()
-        self.geom, self.hp, self.precision, self.mesh = geom, hp, precision, mesh
+        self.geom, self.hp, self.precision, self.mesh, self.slab = geom, hp, precision, mesh, slab
         self._p = make_fxb_params(hp, precision)
         self._d = make_fxb_domain(geom)
         self._vm = default_var_map()
-        _check(self.lib.fxb_init(ctypes.byref(self._p), ctypes.byref(self._d), self._vm, NUNK))
-        if mesh is None:
+        self.exchange = None
+        if slab is not None:
+            if mesh is not None:
+                raise ValueError("a slab splits a uniform grid, not an AMR mesh")
+            self._s = FxbSlab(slab.layer_lo, slab.layer_hi, slab.halo_lo, slab.halo_hi)
+            _check(self.lib.fxb_init_slab(ctypes.byref(self._p), ctypes.byref(self._d), self._vm, NUNK,
+                                          ctypes.byref(self._s)))
+        else:
+            _check(self.lib.fxb_init(ctypes.byref(self._p), ctypes.byref(self._d), self._vm, NUNK))
+        if slab is not None:
+            b0, b1 = slab.block_range()
+            blocks, n = leaf_blocks(geom, (slab.layer_lo, slab.layer_hi)), b1 - b0
+            self.unk_shape = (n,) + geom.block_shape
+            if slab.halo_lo or slab.halo_hi:
+                self.exchange = self._make_exchange(slab)
+        elif mesh is None:
             blocks, n = leaf_blocks(geom), geom.nblocks
             self.unk_shape = geom.unk_shape
         else:
@@ -212,6 +252,28 @@ class HydroDevice:
             self.unk_shape = mesh.unk_shape
         _check(self.lib.fxb_register_blocks(blocks, n))
         self.unk = None
+
+    def _make_exchange(self, slab):
+        import torch
+        from .parallel import HaloExchange
+        lib = self.lib
+        ptr = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())
+
+        def pack(send_lo, n_lo, send_hi, n_hi):
+            _check(lib.fxb_halo_pack(ptr(send_lo), n_lo, ptr(send_hi), n_hi))
+
+        def unpack(recv_lo, recv_hi):
+            _check(lib.fxb_halo_unpack(ptr(recv_lo), ptr(recv_hi)))
+
+        dev = torch.device("cuda", torch.cuda.current_device())
+        stream = torch.cuda.ExternalStream(lib.fxb_stream(), device=dev)
+        return HaloExchange(slab, lib.fxb_halo_doubles(1), pack, unpack, device=dev, stream=stream)
+
+    def fill_halos(self):
+        """Grid_fillGuardCells between slabs: the halo planes from the
+        neighbouring ranks (every rank calls it at the same point)."""
+        if self.exchange is not None:
+            self.exchange()
 
     # ---- data movement
     def attach_unk(self, unk):
@@ -223,6 +285,7 @@ class HydroDevice:
 
     def sync_to_host(self, unk=None):
         unk = self.unk if unk is None else unk
+        self.fill_halos()
         _check(self.lib.fxb_sync_to_host(_dp(unk)))
         return unk
 
@@ -230,10 +293,12 @@ class HydroDevice:
     def Grid_fillGuardCells(self, unk=None):
         """Fill the guard cells (and interiors) of the host UNK from the device."""
         unk = self.unk if unk is None else unk
+        self.fill_halos()
         _check(self.lib.fxb_fill_guardcells(_dp(unk)))
         return unk
 
     def Hydro(self, simTime, dt, dtOld):
+        self.fill_halos()
         _check(self.lib.fxb_hydro_step(float(simTime), float(dt), float(dtOld)))
 
     def Hydro_computeDt(self, location=False):
@@ -250,9 +315,17 @@ class HydroDevice:
 
     # ---- driver helpers
     def advance(self, nsteps, dt, dt_old):
-        """nsteps of Hydro + Driver_computeDt on the device (CUDA graph)."""
-        a, b = ctypes.c_double(dt), ctypes.c_double(dt_old)
+        """nsteps of Hydro + Driver_computeDt on the device (CUDA graph); a
+        slab with halos steps from the host instead, exchanging halos and
+        reducing dt over the ranks every step."""
         hp = self.hp
+        if self.exchange is not None:
+            from .parallel import allreduce_min
+            for _ in range(nsteps):
+                self.Hydro(0.0, dt, dt_old)
+                dt_old, dt = dt, driver_dt(allreduce_min(self.Hydro_computeDt()), dt, hp)
+            return dt, dt_old
+        a, b = ctypes.c_double(dt), ctypes.c_double(dt_old)
         _check(self.lib.fxb_advance(int(nsteps), ctypes.byref(a), ctypes.byref(b),
                                     hp.tstep_change_factor, hp.dtmin, hp.dtmax))
         return a.value, b.value

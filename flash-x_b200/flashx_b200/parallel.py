@@ -7,9 +7,12 @@ clamp, and IO_writeIntegralQuantities sums the conserved integrals with
 MPI_Reduce(SUM) (IO/IOMain/IO_writeIntegralQuantities.F90:224).  Here those two
 reductions run over torch.distributed (NCCL between GPUs, gloo on CPU).
 
-`ReplicaDriver` advances one independent problem per rank (weak scaling) with
-that common dt.  A decomposition of one domain across GPUs additionally needs
-the guard-cell exchange between ranks, which this module does not provide.
+`ReplicaDriver` advances one independent problem per rank with that common
+dt.  `SlabDecomposition` splits one uniform block grid over the ranks along
+its slowest axis and `HaloExchange` moves the guard planes between
+neighbouring slabs before every step, as the UG Grid_fillGuardCells does with
+MPI_SendRecv along each process axis (Grid/GridMain/UG/Grid_fillGuardCells.F90:
+261-306, UG/gr_shiftData.F90:63-191).
 """
 import datetime
 import os
@@ -18,6 +21,7 @@ import torch
 import torch.distributed as dist
 
 from .hydro import driver_dt, initial_dt
+from .params import BC_PERIODIC
 
 
 def init_from_env(backend, timeout_s=120):
@@ -65,7 +69,9 @@ def allreduce_sum(values):
 
 
 class ReplicaDriver:
-    """Driver_evolveAll for one problem per rank with a common dt.
+    """Driver_evolveAll for one problem per rank with a common dt, or for the
+    slabs of one grid (a HydroDevice built with a SlabDecomposition exchanges
+    its halos inside Hydro, as Hydro's own Grid_fillGuardCells).
 
     `dev` exposes the hydro interface (Hydro, Hydro_computeDt), e.g.
     flashx_b200.hydro.HydroDevice.  Every rank makes the same collective
@@ -90,3 +96,155 @@ class ReplicaDriver:
         for _ in range(nsteps):
             dt, dt_old = self.step(dt, dt_old)
         return dt, dt_old
+
+
+class SlabDecomposition:
+    """Split of a uniform block grid over `nranks` ranks along its slowest
+    axis (y in 2-D, z in 3-D): rank r holds the contiguous, balanced block
+    layers `layers[r]` (every block of each layer, so its blocks are one
+    contiguous range of the grid's block list) and halo planes below and
+    above them.  A side facing another slab, or the periodic wrap, has a halo
+    of at least NGUARD planes, widened until the stored extent (interior plus
+    halos) is a multiple of `tile` (16 for the 2-D kernels' tiles); a
+    physical boundary has none.  `self_halo` gives a single rank halos on a
+    periodic axis that it fills from its own planes (the exchange without a
+    neighbour).  Flash-X's UG places blocks on an iProcs x jProcs x kProcs
+    process grid (UG/gr_createDomain.F90); this is its one-axis case."""
+
+    def __init__(self, geom, nranks, rank, tile=None, self_halo=False):
+        if not 0 <= rank < nranks:
+            raise ValueError("rank outside [0, nranks)")
+        self.ndim = geom.ndim
+        self.axis = geom.ndim - 1
+        nlay = geom.nblocky if geom.ndim == 2 else geom.nblockz
+        self.nb = geom.nyb if geom.ndim == 2 else geom.nzb
+        self.per_layer = geom.nblockx * (geom.nblocky if geom.ndim == 3 else 1)
+        if nranks > nlay:
+            raise ValueError(f"{nranks} ranks for {nlay} block layers")
+        self.nranks, self.rank, self.nlay = nranks, rank, nlay
+        self.tile = tile if tile is not None else (16 if geom.ndim == 2 else 1)
+        self.nguard = geom.nguard
+        periodic = geom.bc[2 * self.axis] == BC_PERIODIC
+        self.layers = [(r * nlay // nranks, (r + 1) * nlay // nranks) for r in range(nranks)]
+        wrap = periodic and (nranks > 1 or self_halo)
+        self.halos = []
+        for r, (lo, hi) in enumerate(self.layers):
+            has_lo, has_hi = r > 0 or wrap, r < nranks - 1 or wrap
+            self.halos.append(self._widths((hi - lo) * self.nb, has_lo, has_hi))
+        for r in range(nranks):
+            for side, nbr in ((0, self._nbr(r, -1)), (1, self._nbr(r, +1))):
+                h = self.halos[r][side]
+                if h and h > self.interior_planes(nbr):
+                    raise ValueError(f"halo of {h} planes exceeds rank {nbr}'s {self.interior_planes(nbr)} planes")
+
+    def _widths(self, interior, has_lo, has_hi):
+        hl = self.nguard if has_lo else 0
+        hh = self.nguard if has_hi else 0
+        if (has_lo or has_hi) and self.tile > 1:
+            while (interior + hl + hh) % self.tile:
+                if has_hi and (not has_lo or hh <= hl):
+                    hh += 1
+                else:
+                    hl += 1
+        elif (interior + hl + hh) % self.tile:
+            raise ValueError("a slab without halos must fill whole tiles")
+        return hl, hh
+
+    def _nbr(self, r, step):
+        return (r + step) % self.nranks
+
+    def interior_planes(self, r=None):
+        lo, hi = self.layers[self.rank if r is None else r]
+        return (hi - lo) * self.nb
+
+    @property
+    def layer_lo(self):
+        return self.layers[self.rank][0]
+
+    @property
+    def layer_hi(self):
+        return self.layers[self.rank][1]
+
+    @property
+    def halo_lo(self):
+        return self.halos[self.rank][0]
+
+    @property
+    def halo_hi(self):
+        return self.halos[self.rank][1]
+
+    @property
+    def lo_rank(self):
+        return self._nbr(self.rank, -1) if self.halo_lo else None
+
+    @property
+    def hi_rank(self):
+        return self._nbr(self.rank, +1) if self.halo_hi else None
+
+    @property
+    def send_lo(self):
+        """Planes sent down: the lower neighbour's upper halo."""
+        return self.halos[self.lo_rank][1] if self.halo_lo else 0
+
+    @property
+    def send_hi(self):
+        """Planes sent up: the upper neighbour's lower halo."""
+        return self.halos[self.hi_rank][0] if self.halo_hi else 0
+
+    def block_range(self):
+        """This rank's blocks: [b0, b1) of the whole grid's block list."""
+        return self.layer_lo * self.per_layer, self.layer_hi * self.per_layer
+
+    def local_blocks(self, unk):
+        """This rank's part of a whole-grid UNK (a view)."""
+        b0, b1 = self.block_range()
+        return unk[b0:b1]
+
+
+class HaloExchange:
+    """One guard-plane exchange between slabs: pack this rank's boundary
+    planes, send them to the neighbours and receive theirs (point-to-point,
+    NCCL between GPUs, gloo on CPU), unpack into the halos.
+
+    pack(send_lo, n_lo, send_hi, n_hi) and unpack(recv_lo, recv_hi) move
+    planes between the state and flat FP64 tensors of
+    `doubles_per_plane` x planes values (None where a count is 0).  Messages
+    are matched per neighbour pair in issue order, downward planes (tag 0)
+    before upward planes (tag 1), so two ranks that are each other's lower
+    and upper neighbour (a periodic pair) pair them correctly.  A rank that
+    is its own neighbour packs straight into its receive buffers."""
+
+    def __init__(self, dec, doubles_per_plane, pack, unpack, device="cpu", stream=None):
+        self.dec, self.pack, self.unpack, self.stream = dec, pack, unpack, stream
+        buf = lambda n: torch.empty(n * doubles_per_plane, dtype=torch.float64, device=device) if n else None
+        self.send_lo, self.send_hi = buf(dec.send_lo), buf(dec.send_hi)
+        self.recv_lo, self.recv_hi = buf(dec.halo_lo), buf(dec.halo_hi)
+        self.own_neighbour = dec.nranks == 1
+
+    def __call__(self):
+        d = self.dec
+        if not (d.halo_lo or d.halo_hi):
+            return
+        if self.stream is not None:
+            with torch.cuda.stream(self.stream):
+                self._run(d)
+        else:
+            self._run(d)
+
+    def _run(self, d):
+        if self.own_neighbour:
+            self.pack(self.recv_hi, d.send_lo, self.recv_lo, d.send_hi)
+        else:
+            self.pack(self.send_lo, d.send_lo, self.send_hi, d.send_hi)
+            ops = []
+            if d.halo_lo:
+                ops.append(dist.P2POp(dist.isend, self.send_lo, d.lo_rank, tag=0))
+            if d.halo_hi:
+                ops.append(dist.P2POp(dist.irecv, self.recv_hi, d.hi_rank, tag=0))
+            if d.halo_hi:
+                ops.append(dist.P2POp(dist.isend, self.send_hi, d.hi_rank, tag=1))
+            if d.halo_lo:
+                ops.append(dist.P2POp(dist.irecv, self.recv_lo, d.lo_rank, tag=1))
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+        self.unpack(self.recv_lo, self.recv_hi)

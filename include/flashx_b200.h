@@ -94,6 +94,20 @@ typedef struct fxb_block_desc {
     int    bcoord[3];
 } fxb_block_desc;
 
+/* This rank's share of a uniform block grid split over ranks (one GPU each)
+ * along its slowest axis (y in 2-D, z in 3-D), as UG's iProcs x jProcs x
+ * kProcs layout with a single process axis (Grid_data gr_axisComm): the rank
+ * holds block layers [layer_lo, layer_hi) of that axis, every block of each
+ * layer, and halo_lo / halo_hi planes of cells below / above them that
+ * fxb_halo_unpack fills from the neighbouring ranks.  A halo is 0 on a side
+ * that is a physical (non-periodic) boundary of the domain and at least
+ * NGUARD, at most the rank's own interior planes, on every other side; in
+ * 2-D the interior plus both halos must be a multiple of 16 cells. */
+typedef struct fxb_slab {
+    int    layer_lo, layer_hi;
+    int    halo_lo, halo_hi;
+} fxb_slab;
+
 typedef struct fxb_error {
     int    code;
     char   message[256];
@@ -104,6 +118,19 @@ typedef struct fxb_error {
  * UNK cell vector of nunk doubles. */
 int fxb_init(const fxb_params *params, const fxb_domain *domain,
              const int32_t *var_map, int nunk);
+/* fxb_init for one slab of a uniform grid shared by several ranks: `domain`
+ * is the whole grid, `slab` this rank's part (NULL: the whole grid, no
+ * halos, which is fxb_init).  The rank then registers and attaches only its
+ * own blocks, in the order of the whole grid's block list, and calls
+ * fxb_halo_pack / fxb_halo_unpack around the exchange with its neighbours
+ * before every fxb_hydro_step and before fxb_sync_to_host (the guard cells
+ * next to another slab come from the halo).  fxb_compute_dt and
+ * fxb_integrals cover the rank's own cells; the caller reduces them over
+ * ranks (MIN and SUM).  fxb_advance needs an exchange per step and returns
+ * FXB_EUNSUPPORTED on a slab with halos.  Block-structured AMR meshes are
+ * not split (FXB_EUNSUPPORTED at fxb_register_blocks). */
+int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
+                  const int32_t *var_map, int nunk, const fxb_slab *slab);
 /* The leaf-block list (Grid_getTileIterator(LEAF)); block b is UNK slot b.
  * All leaves at level 1 covering the root grid: the uniform-grid path.
  * Otherwise (3-D only) a block-structured AMR mesh: the leaves must tile the
@@ -151,6 +178,22 @@ int fxb_sync_to_host(double *unk_host);
 int fxb_sync_from_host(const double *unk_host);
 /* Volume integrals: mass, x/y/z momentum, total, internal, kinetic energy. */
 int fxb_integrals(double out[7]);
+/* Guard-cell exchange between slabs (UG/Grid_fillGuardCells.F90:261-306 and
+ * UG/gr_shiftData.F90:63-191, which MPI_SendRecv the guard layers of each
+ * axis to the neighbours).  A message holds `planes` whole planes of the
+ * slab's cells for each of the 10 device variables (dens, velx, vely, velz,
+ * pres, gamc, game, eint, ener, temp), variable-major: fxb_halo_doubles
+ * gives its length.  fxb_halo_pack copies the current state's lowest n_lo
+ * interior planes to send_lo (for the rank below, whose halo_hi is n_lo)
+ * and its highest n_hi planes to send_hi (for the rank above, whose halo_lo
+ * is n_hi); fxb_halo_unpack stores recv_lo in the halo_lo planes below the
+ * slab and recv_hi in the halo_hi planes above it.  All buffers are device
+ * memory (NULL where the count or halo is 0); the copies are queued on the
+ * library stream (fxb_stream), so a caller orders its transfers after
+ * fxb_halo_pack and before fxb_halo_unpack on that stream. */
+long fxb_halo_doubles(int planes);
+int fxb_halo_pack(double *send_lo, int n_lo, double *send_hi, int n_hi);
+int fxb_halo_unpack(const double *recv_lo, const double *recv_hi);
 /* Grid_markRefineDerefine (Grid/GridMain/AMR/Grid_markRefineDerefine.F90:77-150)
  * on the registered AMR mesh, from the attached state: a guard fill of the
  * leaves and of the parents with a leaf child (Eos on the guard regions when

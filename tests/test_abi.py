@@ -18,7 +18,7 @@ HEADER = os.path.join(ROOT, "include", "flashx_b200.h")
 
 def declared_symbols():
     src = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|void)\s*\*?\s*(fxb_\w+)\s*\(", src, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|long|void)\s*\*?\s*(fxb_\w+)\s*\(", src, re.M)))
 
 
 def test_header_declares_the_abi():
@@ -64,6 +64,33 @@ def test_init_validation_codes():
     err = H.FxbError()
     assert lib.fxb_last_error(ctypes.byref(err)) == H.FXB_EARG
     assert b"periodic" in err.message
+
+
+def test_slab_validation_codes():
+    """fxb_init_slab: a side facing another slab needs a halo of NGUARD to the
+    slab's own planes, a non-periodic domain edge none, 2-D slabs fill 16-cell
+    tiles (argument checks come before the device query)."""
+    lib = H.load_library()
+    p = H.make_fxb_params(HydroParams())
+    geom = Geometry(2, 16, 16, 1, 2, 4, 1, bc=(BC_OUTFLOW,) * 6)
+    d = H.make_fxb_domain(geom)
+    vm = H.default_var_map()
+    init = lambda *s: lib.fxb_init_slab(ctypes.byref(p), ctypes.byref(d), vm, 11, ctypes.byref(H.FxbSlab(*s)))
+    assert init(0, 2, 0, 16) in (H.FXB_OK, H.FXB_ECUDA)
+    assert init(1, 3, 8, 8) in (H.FXB_OK, H.FXB_ECUDA)
+    assert init(2, 4, 16, 0) in (H.FXB_OK, H.FXB_ECUDA)
+    assert init(0, 5, 0, 0) == H.FXB_EARG          # layers outside the grid
+    assert init(2, 2, 8, 8) == H.FXB_EARG          # empty
+    assert init(0, 2, 0, 0) == H.FXB_EARG          # no halo towards the next slab
+    assert init(0, 2, 0, 2) == H.FXB_EARG          # halo thinner than NGUARD
+    assert init(0, 2, 0, 40) == H.FXB_EARG         # halo wider than the slab
+    assert init(0, 2, 8, 16) == H.FXB_EARG         # halo on an outflow boundary
+    assert init(0, 2, 0, 4) == H.FXB_EUNSUPPORTED  # 32 + 4 rows do not fill 16-row tiles
+    d.bc[2] = d.bc[3] = BC_PERIODIC
+    assert init(0, 4, 8, 8) in (H.FXB_OK, H.FXB_ECUDA)   # one slab exchanging with itself
+    sub = H.leaf_blocks(geom, (1, 3))
+    assert [tuple(b.bcoord) for b in sub] == [(0, 1, 0), (1, 1, 0), (0, 2, 0), (1, 2, 0)]
+    lib.fxb_finalize()
 
 
 def test_calls_before_init_are_rejected():
