@@ -366,19 +366,13 @@ struct GuardSrc {
     long off[8];
 };
 
-__device__ __forceinline__ void guard_resolve(const MeshArgs &m, int b, const int xin[3], GuardSrc &gs)
+// the prolongation stencil of the level-lev cell x (mapped into the domain) of
+// block B: amr_1blk_cc_prol_linear from the eight parent-level cells
+// floor((x+1)/2)-1 and +1 per axis, found among the parent's neighbours
+__device__ __forceinline__ void prol_resolve(const MeshArgs &m, const DevBlk &B, const int x[3], GuardSrc &gs)
 {
-    const DevBlk B = m.blk[b];
-    int x[3];
-    double sg[3] = {1., 1., 1.};
-    for (int a = 0; a < 3; a++) x[a] = bc_map(m, B.level, a, xin[a], &sg[a]);
-    gs.own = (sg[0] < 0. ? 1u : 0u) | (sg[1] < 0. ? 2u : 0u) | (sg[2] < 0. ? 4u : 0u);
-    gs.parity = 0; gs.flips = 0;
-    gs.off[0] = same_level_off(m, b, B, x);
-    if (gs.off[0] >= 0) { gs.kind = GS_SAME; return; }
     gs.kind = GS_NONE;
     if (B.parent < 0) return;
-    // coarser neighbour: amr_1blk_cc_prol_linear from the parent level
     const int pb = B.parent;
     const DevBlk PB = m.blk[pb];
     int p1[3];
@@ -397,6 +391,19 @@ __device__ __forceinline__ void guard_resolve(const MeshArgs &m, int b, const in
         gs.flips |= ((sq[0] < 0. ? 1u : 0u) | (sq[1] < 0. ? 2u : 0u) | (sq[2] < 0. ? 4u : 0u)) << (3 * s8);
     }
     gs.kind = GS_PROL;
+}
+
+__device__ __forceinline__ void guard_resolve(const MeshArgs &m, int b, const int xin[3], GuardSrc &gs)
+{
+    const DevBlk B = m.blk[b];
+    int x[3];
+    double sg[3] = {1., 1., 1.};
+    for (int a = 0; a < 3; a++) x[a] = bc_map(m, B.level, a, xin[a], &sg[a]);
+    gs.own = (sg[0] < 0. ? 1u : 0u) | (sg[1] < 0. ? 2u : 0u) | (sg[2] < 0. ? 4u : 0u);
+    gs.parity = 0; gs.flips = 0;
+    gs.off[0] = same_level_off(m, b, B, x);
+    if (gs.off[0] >= 0) { gs.kind = GS_SAME; return; }
+    prol_resolve(m, B, x, gs);
 }
 
 // same-level guard value: the cell's first NV variables, velocities flipped at reflecting boundaries
@@ -704,6 +711,54 @@ __global__ void __launch_bounds__(256) amr_ext_fill_kernel(MeshArgs m, const int
 #pragma unroll
         for (int v = 1; v < NV_DEV; v++) if (v == dv) val = u[v];
         E[idx] = val;
+    }
+}
+
+// ---- regridding (Grid_updateRefinement's data movement) ------------------------
+// blocks kept by a regrid: pairs (new block, old block), whole interiors
+__global__ void amr_copy_blocks_kernel(const double *__restrict__ src, double *__restrict__ dst,
+                                       const int2 *__restrict__ pairs, int np, long bstride)
+{
+    const long n = (long)np * bstride;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
+        const int p = (int)(idx / bstride);
+        const long off = idx - (long)p * bstride;
+        const int2 q = pairs[p];
+        dst[(long)q.x * bstride + off] = src[(long)q.y * bstride + off];
+    }
+}
+
+// new children of a regrid, all at one level: every interior cell
+// interpolated from the parent level in conserved form (amr_prolong ->
+// amr_1blk_cc_prol_gen_unk_fun with the convert hooks), reading the parent
+// and its same-level neighbours, which hold their final data when the levels
+// are processed coarse to fine
+__global__ void __launch_bounds__(256) amr_newchild_kernel(MeshArgs m, const int *__restrict__ blocks, int nb)
+{
+    const int n = m.n;
+    const long nc = (long)n * n * n;
+    double *store = const_cast<double *>(m.store);
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)nb * nc;
+         idx += (long)gridDim.x * blockDim.x) {
+        const int b = blocks[idx / nc];
+        const int c = (int)(idx % nc);
+        const int i = c % n, j = (c / n) % n, k = c / (n * n);
+        const DevBlk B = m.blk[b];
+        const int x[3] = {B.c0 * n + i, B.c1 * n + j, B.c2 * n + k};
+        GuardSrc gs;
+        gs.parity = 0; gs.flips = 0; gs.own = 0;
+        prol_resolve(m, B, x, gs);
+        double u[NV_DEV];
+        if (gs.kind == GS_PROL) {
+            guard_eval_prol(m.store, m.vstride, gs.off, gs.flips, gs.parity, 0u, u);
+        } else {
+            atomicOr(m.err, ERR_AMR);
+#pragma unroll
+            for (int v = 0; v < NV_DEV; v++) u[v] = 0.;
+        }
+        double *o = store + (long)b * m.bstride + c;
+#pragma unroll
+        for (int v = 0; v < NV_DEV; v++) o[v * m.vstride] = u[v];
     }
 }
 
@@ -1080,16 +1135,23 @@ bool amr_active() { return S.active; }
 int amr_cur() { return S.cur; }
 long amr_leaf_cells() { return (long)S.nleaf * S.n * S.n * S.n; }
 
+namespace {
+void free_device(State &s)
+{
+    dfree(s.store[0]); dfree(s.store[1]);
+    dfree(s.d_blk); dfree(s.d_ntab); dfree(s.d_child); dfree(s.d_plist); dfree(s.d_eosmask);
+    dfree(s.d_finer); dfree(s.d_fine); dfree(s.d_dxl); dfree(s.d_entries); dfree(s.leaf_blk_dev);
+    dfree(s.gcb); dfree(s.sig); dfree(s.slp); dfree(s.flat);
+    for (int d = 0; d < 3; d++) { dfree(s.w[d]); dfree(s.f[d]); }
+    dfree(s.bflux); dfree(s.stage); dfree(s.d_dmap); dfree(s.d_glist);
+    dfree(s.d_plan); dfree(s.d_prol); dfree(s.d_poff); dfree(s.d_rlist);
+    dfree(s.d_active); dfree(s.d_act_eos); dfree(s.d_act_bnd); dfree(s.d_ext); dfree(s.d_err);
+}
+} // namespace
+
 void amr_destroy()
 {
-    dfree(S.store[0]); dfree(S.store[1]);
-    dfree(S.d_blk); dfree(S.d_ntab); dfree(S.d_child); dfree(S.d_plist); dfree(S.d_eosmask);
-    dfree(S.d_finer); dfree(S.d_fine); dfree(S.d_dxl); dfree(S.d_entries); dfree(S.leaf_blk_dev);
-    dfree(S.gcb); dfree(S.sig); dfree(S.slp); dfree(S.flat);
-    for (int d = 0; d < 3; d++) { dfree(S.w[d]); dfree(S.f[d]); }
-    dfree(S.bflux); dfree(S.stage); dfree(S.d_dmap); dfree(S.d_glist);
-    dfree(S.d_plan); dfree(S.d_prol); dfree(S.d_poff); dfree(S.d_rlist);
-    dfree(S.d_active); dfree(S.d_act_eos); dfree(S.d_act_bnd); dfree(S.d_ext); dfree(S.d_err);
+    free_device(S);
     S = State();
 }
 
@@ -1476,6 +1538,97 @@ int amr_step(const double *dtv, double dt, int *launches)
     S.cur = 1 - S.cur;
     if (launches) *launches = nl;
     return FXB_OK;
+}
+
+// Grid_updateRefinement's data movement on the device after the caller's tree
+// update (Paramesh4/Grid_updateRefinement.F90:109, gr_updateRefinement.F90:
+// 130-265): the old tree's parents are restricted from their children; the
+// new mesh is built from `leaves`; each of its blocks that existed before
+// keeps its data (a derefined parent its children's average); new children,
+// level by level from coarse to fine, are prolonged from their parent in
+// conserved form (mpi_amr_prolong.F90); Eos on every leaf.  Only the old
+// interior store stays allocated while the new mesh is built.  A rejected
+// list, or a new block whose parent was not an old leaf, restores the old
+// mesh and its data.
+int amr_regrid(const fxb_block_desc *leaves, int nleaf)
+{
+    if (!S.active) return record_error(FXB_EARG, "fxb_regrid: needs a registered AMR mesh");
+    restrict_all(S.cur);
+    CKA(cudaStreamSynchronize(S.C.stream));
+    State old = std::move(S);
+    S = State();
+    double *ostore = old.store[old.cur];
+    old.store[old.cur] = nullptr;
+    free_device(old);
+    const long obstride = old.bstride;
+    std::vector<fxb_block_desc> olist(old.nleaf);
+    for (int l = 0; l < old.nleaf; l++) {
+        const HBlock &B = old.blk[old.leaf_blk[l]];
+        olist[l].level = B.level;
+        for (int a = 0; a < 3; a++) olist[l].bcoord[a] = B.c[a];
+    }
+    // the old mesh back, with its data, after a failure
+    auto restore = [&](int code) -> int {
+        amr_destroy();
+        int rc = amr_create(old.C, olist.data(), old.nleaf);
+        if (rc == FXB_OK && S.bstride == obstride)
+            cudaMemcpyAsync(S.store[0], ostore, sizeof(double) * obstride * S.nblk, cudaMemcpyDeviceToDevice,
+                            S.C.stream);
+        cudaStreamSynchronize(S.C.stream);
+        cudaFree(ostore);
+        if (rc == FXB_OK) amr_tune();
+        return code;
+    };
+    int rc = amr_create(old.C, leaves, nleaf);
+    if (rc) return restore(rc);
+    std::vector<int2> pairs;
+    std::vector<std::vector<int>> fresh(S.maxlev + 1);
+    for (int b = 0; b < S.nblk; b++) {
+        const HBlock &B = S.blk[b];
+        auto it = old.map.find(key(B.level, B.c));
+        if (it != old.map.end()) { pairs.push_back(make_int2(b, it->second)); continue; }
+        bool ok = B.parent >= 0;
+        if (ok) {
+            const HBlock &P = S.blk[B.parent];
+            auto ip = old.map.find(key(P.level, P.c));
+            ok = ip != old.map.end() && old.blk[ip->second].leaf >= 0;
+        }
+        if (!ok) {
+            record_error(FXB_EARG, "fxb_regrid: a new block's parent was not a leaf (one level of change per update)");
+            return restore(FXB_EARG);
+        }
+        fresh[B.level].push_back(b);
+    }
+    int2 *d_pairs = nullptr;
+    int *d_fresh = nullptr;
+    CKA(cudaMalloc(&d_pairs, sizeof(int2) * std::max<size_t>(1, pairs.size())));
+    CKA(cudaMalloc(&d_fresh, sizeof(int) * std::max(1, S.nblk)));
+    if (!pairs.empty()) {
+        CKA(cudaMemcpyAsync(d_pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice, S.C.stream));
+        const long work = (long)pairs.size() * S.bstride;
+        const int grid = (int)std::min<long>((work + 255) / 256, 148L * 16);
+        amr_copy_blocks_kernel<<<grid, 256, 0, S.C.stream>>>(ostore, S.store[0], d_pairs, (int)pairs.size(), S.bstride);
+        CKA(cudaGetLastError());
+    }
+    long off = 0;
+    for (int lev = 2; lev <= S.maxlev; lev++) {
+        const int nb = (int)fresh[lev].size();
+        if (!nb) continue;
+        CKA(cudaMemcpyAsync(d_fresh + off, fresh[lev].data(), sizeof(int) * nb, cudaMemcpyHostToDevice, S.C.stream));
+        const long work = (long)nb * S.vstride;
+        const int grid = (int)std::min<long>((work + 255) / 256, 148L * 16);
+        amr_newchild_kernel<<<grid, 256, 0, S.C.stream>>>(mesh_args(0), d_fresh + off, nb);
+        CKA(cudaGetLastError());
+        off += nb;
+    }
+    S.cur = 0;
+    rc = amr_eos();
+    CKA(cudaStreamSynchronize(S.C.stream));
+    cudaFree(d_pairs);
+    cudaFree(d_fresh);
+    cudaFree(ostore);
+    if (rc) return rc;
+    return amr_tune();
 }
 
 int amr_rate()

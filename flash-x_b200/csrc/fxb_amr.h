@@ -34,6 +34,9 @@ int amr_sync_to_host(double *unk_host);
 int amr_step(const double *dtv, double dt, int *launches);
 int amr_rate();
 int amr_eos();
+// the registered mesh replaced by the leaf list `leaves` (one level of change
+// per block), its data moved on the device: copies, restriction, prolongation, Eos
+int amr_regrid(const fxb_block_desc *leaves, int nleaf);
 int amr_integrals(double *out7, double *partials, int npartials);
 long amr_leaf_cells();
 // first leaf cell (leaf, k, j, i linear index) whose CFL rate equals the reduced maximum

@@ -859,6 +859,21 @@ extern "C" int fxb_mark_refine_derefine(int nvars, const int *refine_var, const 
     return check_err_word();
 }
 
+extern "C" int fxb_regrid(const fxb_block_desc *blocks, int nblk)
+{
+    if (!L.attached) return fail(FXB_EARG, "fxb_regrid: no UNK attached");
+    if (!amr_active()) return fail(FXB_EUNSUPPORTED, "fxb_regrid: needs a registered AMR mesh");
+    if (!blocks || nblk <= 0) return fail(FXB_EARG, "fxb_regrid: empty block list");
+    for (int i = 0; i < 2; i++) {
+        if (L.graph_exec[i]) cudaGraphExecDestroy(L.graph_exec[i]);
+        L.graph_exec[i] = nullptr;
+    }
+    L.rate_valid = false;
+    int rc = amr_regrid(blocks, nblk);
+    if (rc) return rc;
+    return check_err_word();
+}
+
 extern "C" int fxb_last_timing(double *ms, int *kernel_launches)
 {
     if (!L.timing_valid) return fail(FXB_EARG, "fxb_last_timing: nothing timed yet");

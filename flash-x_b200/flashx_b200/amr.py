@@ -13,8 +13,9 @@ Refinement follows the Flash-X/PARAMESH rule that neighbouring leaves,
 across faces, edges and corners, differ by at most one level
 (PARAMESH's proper nesting with diagonals = .true.); `build_mesh` refines
 where a criterion asks for it and then refines coarse neighbours until that
-holds.  Regridding during a run is not part of this module: the leaf list is
-built once and kept.
+holds.  `refine_derefine` is the tree update of a regrid during a run
+(PARAMESH's amr_refine_derefine) from per-leaf refine/derefine marks; the
+device moves the data to the new leaves (fxb_regrid).
 """
 import math
 
@@ -159,6 +160,91 @@ def _balance(geom, leaves):
                     leaves.discard(cov)
                     leaves.update(_children(geom, *cov))
                     changed = True
+
+
+def is_balanced(geom, leaves):
+    """Every leaf's neighbours (faces, edges, corners) within one level."""
+    leaves = set(leaves)
+    for lev, c in leaves:
+        for p in _neighbour_positions(geom, lev, c):
+            cov = _covering_leaf(leaves, lev, p)
+            if cov is not None and cov[0] < lev - 1:
+                return False
+    return True
+
+
+def refine_derefine(mesh: AmrMesh, flags, lrefine_min=1, lrefine_max=None):
+    """PARAMESH's tree update (PM4_package/source/mpi_amr_refine_derefine.F90)
+    for leaf marks flags[leaf] = 1 refine, -1 derefine, 0 neither (what
+    Grid_markRefineDerefine / fxb_mark_refine_derefine returns, in the mesh's
+    leaf order).  Returns the new AmrMesh.
+
+    * level limits (mpi_amr_refine_derefine.F90:157-163): no refinement at
+      lrefine_max, no derefinement at lrefine_min, refinement below it;
+    * amr_check_refine: a leaf one level coarser than a refining neighbour
+      (faces, edges, corners) refines too, until nothing changes, and is no
+      longer derefined;
+    * amr_check_derefine (mpi_amr_check_derefine.F90): a leaf derefines only
+      if it is not a root block, none of its same-level neighbours is a parent
+      or refines, and all its siblings are leaves that derefine as well; the
+      siblings are then replaced by their parent.
+    """
+    g = mesh.geom
+    lmax = lrefine_max if lrefine_max is not None else mesh.maxlev + 1
+    order = [(int(l), tuple(int(v) for v in c)) for l, c in zip(mesh.levels, mesh.bcoords)]
+    leaves = set(order)
+    flags = [int(f) for f in flags]
+    if len(flags) != len(order):
+        raise ValueError("one mark per leaf")
+    refine = {lc: f == 1 for lc, f in zip(order, flags)}
+    derefine = {lc: f == -1 for lc, f in zip(order, flags)}
+    for lc in order:
+        if lc[0] >= lmax:
+            refine[lc] = False
+        if lc[0] == lrefine_min:
+            derefine[lc] = False
+        if lc[0] < lrefine_min:
+            refine[lc] = True
+    changed = True
+    while changed:
+        changed = False
+        for lc in order:
+            if not refine[lc]:
+                continue
+            lev, c = lc
+            for p in _neighbour_positions(g, lev, c):
+                cov = _covering_leaf(leaves, lev, p)
+                if cov is not None and cov[0] < lev and not refine[cov]:
+                    refine[cov] = True
+                    derefine[cov] = False
+                    changed = True
+    nch = 8 if g.ndim == 3 else 4
+    groups = {}
+    for lc in order:
+        lev, c = lc
+        if not derefine[lc] or refine[lc] or lev == 1:
+            continue
+        blocked = False
+        for p in _neighbour_positions(g, lev, c):
+            same = (lev, p)
+            if same in leaves:
+                blocked = refine[same]
+            else:
+                blocked = _covering_leaf(leaves, lev, p) is None   # a parent at this level
+            if blocked:
+                break
+        if not blocked:
+            groups.setdefault((lev - 1, tuple(v // 2 for v in c)), []).append(lc)
+    new = set(leaves)
+    for lc in order:
+        if refine[lc]:
+            new.discard(lc)
+            new.update(_children(g, *lc))
+    for par, kids in groups.items():
+        if len(kids) == nch:
+            new.difference_update(kids)
+            new.add(par)
+    return AmrMesh(g, sorted(new))
 
 
 def mesh_from_levels(geom: Geometry, leaves):

@@ -31,7 +31,7 @@ ABI_SYMBOLS = ("fxb_init", "fxb_register_blocks", "fxb_attach_unk", "fxb_fill_gu
                "fxb_hydro_step", "fxb_compute_dt", "fxb_advance", "fxb_eos", "fxb_sync_to_host",
                "fxb_sync_from_host", "fxb_integrals", "fxb_integrals_noalloc", "fxb_mark_refine_derefine",
                "fxb_last_timing", "fxb_stream", "fxb_tuning", "fxb_last_error", "fxb_finalize",
-               "fxb_init_slab", "fxb_halo_doubles", "fxb_halo_pack", "fxb_halo_unpack")
+               "fxb_init_slab", "fxb_halo_doubles", "fxb_halo_pack", "fxb_halo_unpack", "fxb_regrid")
 
 
 class FxbParams(ctypes.Structure):
@@ -114,6 +114,7 @@ def load_library(path=LIB_PATH):
     L.fxb_halo_doubles.restype = ctypes.c_long
     L.fxb_halo_pack.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
     L.fxb_halo_unpack.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    L.fxb_regrid.argtypes = [ctypes.POINTER(FxbBlockDesc), ctypes.c_int]
     for name in ABI_SYMBOLS:
         if name not in ("fxb_stream", "fxb_finalize", "fxb_halo_doubles"):
             getattr(L, name).restype = ctypes.c_int
@@ -285,6 +286,8 @@ class HydroDevice:
 
     def sync_to_host(self, unk=None):
         unk = self.unk if unk is None else unk
+        if unk is None or unk.shape != self.unk_shape:
+            raise ValueError(f"sync_to_host needs a UNK of shape {self.unk_shape}")
         self.fill_halos()
         _check(self.lib.fxb_sync_to_host(_dp(unk)))
         return unk
@@ -353,6 +356,22 @@ class HydroDevice:
         _check(self.lib.fxb_mark_refine_derefine(nv, iv, rc_, dc, fl, int(max_refine),
                                                  flags.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _dp(err)))
         return flags, err
+
+    def Grid_updateRefinement(self, flags, lrefine_min=1, lrefine_max=None):
+        """Grid_updateRefinement after Grid_markRefineDerefine: the tree update
+        (PARAMESH's amr_refine_derefine, restated in flashx_b200.amr) on the
+        host, then the data movement on the device (fxb_regrid).  Returns the
+        new AmrMesh; the host UNK must then have its shape (`unk_shape`) for
+        sync_to_host."""
+        from .amr import refine_derefine
+        if self.mesh is None:
+            raise ValueError("Grid_updateRefinement needs an AMR mesh")
+        new = refine_derefine(self.mesh, flags, lrefine_min, lrefine_max)
+        _check(self.lib.fxb_regrid(mesh_blocks(new.levels, new.bcoords), new.nleaf))
+        self.mesh = new
+        self.unk_shape = new.unk_shape
+        self.unk = None
+        return new
 
     def tuning(self):
         """The launch shape in use (the batched-block path tunes it at attach)."""

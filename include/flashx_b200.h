@@ -210,6 +210,23 @@ int fxb_halo_unpack(const double *recv_lo, const double *recv_hi);
 int fxb_mark_refine_derefine(int nvars, const int *refine_var, const double *refine_cutoff,
                              const double *derefine_cutoff, const double *refine_filter, int max_refine,
                              int *flags, double *error);
+/* Grid_updateRefinement's data movement on the device, after the caller's
+ * tree update (Paramesh4/Grid_updateRefinement.F90:109,
+ * gr_updateRefinement.F90:130-265): `blocks` is the new leaf list of the
+ * registered AMR mesh (its order becomes the UNK slot order).  Parents of the
+ * old tree are restricted from their children first (amr_restrict); each
+ * block of the new tree that existed in the old one keeps its data, so a
+ * derefined parent holds its children's average; new children, level by
+ * level from coarse to fine, are interpolated from their parent and its
+ * same-level neighbours in conserved form (amr_prolong:
+ * amr_1blk_cc_prol_linear with flash_convert_cc_hook /
+ * flash_unconvert_cc_hook); then Eos_wrapped(MODE_DENS_EI) runs on every
+ * leaf.  The caller then resizes its UNK to the new leaf count and reads it
+ * with fxb_sync_to_host.  Errors: FXB_EARG when the list is not a balanced
+ * tiling or a new block's parent was not an old leaf (more than one level of
+ * change); the old mesh and its data are then kept.  FXB_EUNSUPPORTED on a
+ * uniform grid. */
+int fxb_regrid(const fxb_block_desc *blocks, int nblk);
 /* Volume integrals of caller-owned device arrays without allocating any
  * device memory (no counterpart in the reference: an addition of this
  * library).  For callers that cannot call cudaMalloc, e.g. a Fortran code

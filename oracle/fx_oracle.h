@@ -116,6 +116,12 @@ int fxo_amr_integrals(const fxo_amr *a, const double *unk, double out[7]);
 int fxo_amr_mark_refine(fxo_amr *a, const double *unk, int nvars, const int *ivar, const double *refine_cutoff,
                         const double *derefine_cutoff, const double *refine_filter, int max_refine, int *flags,
                         double *error_out);
+/* Grid_updateRefinement's data movement after the caller's tree update: the
+ * leaf UNK of `old` (old_unk) becomes the leaf UNK of `nw` (new_unk, guard
+ * cells zero): kept blocks copied, derefined parents restricted, new children
+ * prolonged in conserved form, Eos on every leaf; 0, 6 (stencil cell without
+ * a block) or 7 (a new block's parent was not an old leaf). */
+int fxo_amr_regrid(fxo_amr *old, const double *old_unk, fxo_amr *nw, double *new_unk);
 
 #ifdef __cplusplus
 }

@@ -82,6 +82,7 @@ def lib():
         L.fxo_amr_compute_dt.argtypes = [ctypes.c_void_p, D, D]
         L.fxo_amr_integrals.argtypes = [ctypes.c_void_p, D, D]
         L.fxo_amr_mark_refine.argtypes = [ctypes.c_void_p, D, ctypes.c_int, I, D, D, D, ctypes.c_int, I, D]
+        L.fxo_amr_regrid.argtypes = [ctypes.c_void_p, D, ctypes.c_void_p, D]
         _lib = L
     return _lib
 
@@ -247,4 +248,15 @@ class Amr:
     def integrals(self, unk):
         out = np.zeros(7)
         lib().fxo_amr_integrals(self.h, _dp(unk), _dp(out))
+        return out
+
+    def regrid(self, unk, new):
+        """Data of the leaves of `new` (an Amr of the updated tree) from this
+        tree's leaf UNK: Grid_updateRefinement's restriction, copies,
+        prolongation of new children and Eos.  Returns the new leaf UNK."""
+        out = np.zeros((new.nleaf,) + unk.shape[1:])
+        rc = lib().fxo_amr_regrid(self.h, _dp(np.ascontiguousarray(unk)), new.h, _dp(out))
+        if rc:
+            raise RuntimeError({6: "oracle regrid: stencil cell without a block",
+                                7: "oracle regrid: a new block's parent was not a leaf"}.get(rc, f"oracle regrid {rc}"))
         return out

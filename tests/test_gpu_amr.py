@@ -185,3 +185,78 @@ def test_mark_refine_derefine_matches_oracle(oracle, need_gpu, bc, maxlev, crit,
     assert np.array_equal(flags, ref_flags)
     assert set(np.unique(flags)) <= {-1, 0, 1} and np.any(err > 0)
     dev.close()
+
+
+@pytest.mark.parametrize("bc,maxlev", [
+    ((BC_PERIODIC,) * 6, 3),
+    ((BC_OUTFLOW, BC_OUTFLOW, BC_PERIODIC, BC_PERIODIC, BC_REFLECTING, BC_REFLECTING), 2),
+])
+def test_regrid_matches_oracle(oracle, need_gpu, bc, maxlev):
+    """Grid_updateRefinement: marks from the device, the tree update on the
+    host (amr.refine_derefine), the data movement on the device (fxb_regrid:
+    copies, restriction of derefined parents, prolongation of new children,
+    Eos) bit for bit equal to the oracle's; first the marks of a density
+    criterion, then every finest-level leaf derefined; two steps on the
+    final mesh."""
+    root, hp, mesh, unk = _case(bc, maxlev, order=3)
+    p = oracle.make_params(root.as_dict(), hp)
+    dev = HydroDevice(root, hp, "fp64", mesh=mesh)
+    dev.attach_unk(unk.copy())
+    flags, _ = dev.Grid_markRefineDerefine([("dens", 0.3, 0.05, 0.01)], maxlev + 1)
+    am, ref = oracle.Amr(p, mesh.levels, mesh.bcoords), unk.copy()
+    m1 = dev.Grid_updateRefinement(flags, lrefine_max=maxlev + 1)
+    old = {(int(l), tuple(int(v) for v in c)) for l, c in zip(mesh.levels, mesh.bcoords)}
+    new = {(int(l), tuple(int(v) for v in c)) for l, c in zip(m1.levels, m1.bcoords)}
+    assert any((l - 1, tuple(v // 2 for v in c)) in old for l, c in new - old), "no leaf was refined"
+    am1 = oracle.Amr(p, m1.levels, m1.bcoords)
+    ref = am.regrid(ref, am1)
+    got = np.zeros(m1.unk_shape)
+    dev.sync_to_host(got)
+    assert np.array_equal(_interior(root, got), _interior(root, ref))
+    top = int(max(m1.levels))
+    m2 = dev.Grid_updateRefinement([-1 if l == top else 0 for l in m1.levels], lrefine_max=maxlev + 1)
+    assert m2.nleaf < m1.nleaf
+    am2 = oracle.Amr(p, m2.levels, m2.bcoords)
+    ref = am1.regrid(ref, am2)
+    got = np.zeros(m2.unk_shape)
+    dev.sync_to_host(got)
+    assert np.array_equal(_interior(root, got), _interior(root, ref))
+    dt = 0.5 * am2.compute_dt(ref)
+    assert dev.Hydro_computeDt() == am2.compute_dt(ref)
+    for _ in range(2):
+        am2.hydro_step(ref, dt)
+        dev.Hydro(0.0, dt, dt)
+    dev.sync_to_host(got)
+    assert np.array_equal(_interior(root, got), _interior(root, ref))
+    dev.close()
+
+
+def test_regrid_rejects_two_levels_and_keeps_the_mesh(oracle, need_gpu):
+    """A new leaf whose parent was not an old leaf (two levels at once) is
+    refused with FXB_EARG; the registered mesh and its data stay usable."""
+    from flashx_b200.hydro import mesh_blocks
+    root, hp, mesh, unk = _case((BC_PERIODIC,) * 6, 2, order=3)
+    dev = HydroDevice(root, hp, "fp64", mesh=mesh)
+    dev.attach_unk(unk.copy())
+    lv = [(int(l), tuple(int(v) for v in c)) for l, c in zip(mesh.levels, mesh.bcoords)]
+    first = next(lc for lc in lv if lc[0] == 1)
+    bad = set(lv) - {first}
+    kids = [(2, (2 * first[1][0] + i, 2 * first[1][1] + j, 2 * first[1][2] + k))
+            for k in (0, 1) for j in (0, 1) for i in (0, 1)]
+    bad.update(kids[1:])
+    bad.update((3, (2 * kids[0][1][0] + i, 2 * kids[0][1][1] + j, 2 * kids[0][1][2] + k))
+               for k in (0, 1) for j in (0, 1) for i in (0, 1))
+    bm = A.AmrMesh(root, sorted(bad))
+    with pytest.raises(FlashXError) as e:
+        from flashx_b200 import hydro as H
+        H._check(dev.lib.fxb_regrid(mesh_blocks(bm.levels, bm.bcoords), bm.nleaf))
+    assert e.value.code == 1
+    out = unk.copy()
+    dev.sync_to_host(out)
+    assert np.array_equal(_interior(root, out), _interior(root, unk))
+    dt = 0.5 * dev.Hydro_computeDt()
+    am, ref = _oracle(oracle, root, hp, mesh, unk, [dt])
+    dev.Hydro(0.0, dt, dt)
+    dev.sync_to_host(out)
+    assert np.array_equal(_interior(root, out), _interior(root, ref))
+    dev.close()
