@@ -399,7 +399,8 @@ extern "C" int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
     const fxb_params &p = *params;
     if (d.ndim != 2 && d.ndim != 3) return fail(FXB_EUNSUPPORTED, "fxb_init: ndim must be 2 or 3");
     if (d.nguard < 4) return fail(FXB_EARG, "fxb_init: NGUARD must be at least 4");
-    if (p.order != 3 && p.order != 5) return fail(FXB_EUNSUPPORTED, "fxb_init: order must be 3 (PPM) or 5 (WENO)");
+    if (p.order != 2 && p.order != 3 && p.order != 5)
+        return fail(FXB_EUNSUPPORTED, "fxb_init: order must be 2 (MUSCL-Hancock), 3 (PPM) or 5 (WENO)");
     if (p.riemann < 1 || p.riemann > 4)
         return fail(FXB_EUNSUPPORTED, "fxb_init: RiemannSolver must be Roe, LLF, HLL or HLLC");
     if (p.limiter < 1 || p.limiter > 5) return fail(FXB_EARG, "fxb_init: unknown slope limiter");

@@ -47,6 +47,14 @@ template <class R> __device__ __forceinline__ R divc(R x, double c);
 template <> __device__ __forceinline__ double divc<double>(double x, double c) { return x / c; }
 template <> __device__ __forceinline__ float divc<float>(float x, double c) { return x * (float)(1.0 / c); }
 
+// options compiled only into kernel instantiations of their own (template
+// flag EXT), so the default kernels keep their registers: the Roe solver,
+// PPM contact steepening, MUSCL-Hancock reconstruction (order 2)
+__host__ __device__ inline bool extended_options(const DevParams &p)
+{
+    return p.riemann == 1 || p.steepening || p.order == 2;
+}
+
 // Fortran MIN/MAX with gfortran's argument order: mvar = a1; if (a2 < mvar) mvar = a2
 template <class R> __device__ __forceinline__ R fmin2(R a, R b) { return (b < a) ? b : a; }
 template <class R> __device__ __forceinline__ R fmax2(R a, R b) { return (b > a) ? b : a; }
@@ -310,6 +318,88 @@ __device__ __forceinline__ void flatten(R F, const R *Vc, R vecL[6], R vecR[6])
         vecL[n] = F * Vc[n] + (R(1.0) - F) * vecL[n];
         vecR[n] = F * Vc[n] + (R(1.0) - F) * vecR[n];
     }
+}
+
+// MUSCL-Hancock face states (hy_DataReconstructNormalDir_MH.F90): one TVD
+// slope of the cell (characteristic amplitudes when charLimiting, primitive
+// slopes otherwise), scaled by 1 - F with flattening; eint reconstructed
+// linearly, clamped and traced with the entropy wave when it is carried
+// (aux eint or gravity, hyEndVar >= HY_EINT); D, v1, v2, v3, P traced over
+// the five waves from the cell value, the Roe solver keeping only each
+// wave's upwind side.  Vm, Vc, Vp in sweep order (D, v1, v2, v3, P, EI).
+template <class R>
+__device__ __forceinline__ void mh_trace(const DevParams &prm, const Eig<R> &e, R dtn, R hdtn, const R *Vm,
+                                         const R *Vc, const R *Vp, R F, R Wm[6], R Wp[6])
+{
+    R dL[6], dR[6], A[5], d5;
+#pragma unroll
+    for (int k = 0; k < 6; k++) { dL[k] = Vc[k] - Vm[k]; dR[k] = Vp[k] - Vc[k]; }
+    const R beta = R(prm.limited_beta);
+    if (prm.char_limiting) {
+        Five<R> a = ldot(e, dL[0], dL[1], dL[2], dL[3], dL[4]);
+        Five<R> b = ldot(e, dR[0], dR[1], dR[2], dR[3], dR[4]);
+#pragma unroll
+        for (int w = 0; w < 5; w++) A[w] = limit(prm.limiter, w, -1, a.w[w], b.w[w], beta);
+        d5 = (prm.limiter == LIM_HYBRID) ? lim_mc(dL[5], dR[5]) : limit(prm.limiter, -1, (int)EI, dL[5], dR[5], beta);
+        if (prm.flattening) {
+#pragma unroll
+            for (int w = 0; w < 5; w++) A[w] = A[w] * (R(1.) - F);
+            d5 = d5 * (R(1.) - F);
+        }
+    } else {
+        const int kind[5] = {D, VX, VY, VZ, P};
+        R db[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) db[k] = limit(prm.limiter, -1, kind[k], dL[k], dR[k], beta);
+        d5 = limit(prm.limiter, -1, (int)EI, dL[5], dR[5], beta);
+        if (prm.flattening) {
+#pragma unroll
+            for (int k = 0; k < 5; k++) db[k] = db[k] * (R(1.) - F);
+            d5 = d5 * (R(1.) - F);
+        }
+        Five<R> c = ldot(e, db[0], db[1], db[2], db[3], db[4]);
+#pragma unroll
+        for (int w = 0; w < 5; w++) A[w] = c.w[w];
+    }
+    if (prm.use_aux_eint || prm.use_gravity) {
+        R wp = Vc[5] + R(0.5) * d5, wm = Vc[5] - R(0.5) * d5;
+        wm = fmax2(fmin2(Vc[5], wm), fmin2(fmax2(Vc[5], wm), wm));
+        wp = fmax2(fmin2(Vc[5], wp), fmin2(fmax2(Vc[5], wp), wp));
+        Wp[5] = wp - fmax2(e.un, R(0.)) * hdtn * d5;
+        Wm[5] = wm - fmin2(e.un, R(0.)) * hdtn * d5;
+    } else {
+        Wp[5] = R(0.); Wm[5] = R(0.);
+    }
+    const R lam[5] = {e.lam0, e.un, e.un, e.un, e.lam4};
+    const bool roe = prm.riemann == 1;
+    R cL[5], cR[5];
+    bool useL[5], useR[5];
+#pragma unroll
+    for (int n = 0; n < 5; n++) {
+        cL[n] = R(.5) * (R(-1.) - dtn * lam[n]);
+        cR[n] = R(.5) * (R(1.) - dtn * lam[n]);
+        useL[n] = !roe || lam[n] < R(0.);
+        useR[n] = !roe || !(lam[n] < R(0.));
+    }
+    // nonzero right-eigenvector entries: D (rho, 1, rho on waves 0, 2, 4),
+    // v1 (-c, c on 0, 4), v2 (1 on 1), v3 (1 on 3), P (rho c^2 on 0, 4)
+    R sL[5] = {R(0.), R(0.), R(0.), R(0.), R(0.)}, sR[5] = {R(0.), R(0.), R(0.), R(0.), R(0.)};
+    if (useL[0]) { sL[0] = sL[0] + cL[0] * e.rho * A[0]; sL[1] = sL[1] + cL[0] * (-e.cf) * A[0];
+                   sL[4] = sL[4] + cL[0] * e.rp * A[0]; }
+    if (useR[0]) { sR[0] = sR[0] + cR[0] * e.rho * A[0]; sR[1] = sR[1] + cR[0] * (-e.cf) * A[0];
+                   sR[4] = sR[4] + cR[0] * e.rp * A[0]; }
+    if (useL[1]) sL[2] = sL[2] + cL[1] * A[1];
+    if (useR[1]) sR[2] = sR[2] + cR[1] * A[1];
+    if (useL[2]) sL[0] = sL[0] + cL[2] * A[2];
+    if (useR[2]) sR[0] = sR[0] + cR[2] * A[2];
+    if (useL[3]) sL[3] = sL[3] + cL[3] * A[3];
+    if (useR[3]) sR[3] = sR[3] + cR[3] * A[3];
+    if (useL[4]) { sL[0] = sL[0] + cL[4] * e.rho * A[4]; sL[1] = sL[1] + cL[4] * e.cf * A[4];
+                   sL[4] = sL[4] + cL[4] * e.rp * A[4]; }
+    if (useR[4]) { sR[0] = sR[0] + cR[4] * e.rho * A[4]; sR[1] = sR[1] + cR[4] * e.cf * A[4];
+                   sR[4] = sR[4] + cR[4] * e.rp * A[4]; }
+#pragma unroll
+    for (int v = 0; v < 5; v++) { Wm[v] = Vc[v] + sL[v]; Wp[v] = Vc[v] + sR[v]; }
 }
 
 // contact steepening of the PPM density interface values

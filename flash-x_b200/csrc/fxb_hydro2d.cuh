@@ -162,6 +162,20 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
     } else if (!eigen(Vc[0], Vc[1], Vc[4], s.V[GC][wy][wx], e)) {
         set_err(a.err, ERR_SOUND);
     }
+    if (EXT && a.prm.order == 2) {
+        // MUSCL-Hancock: the cell's own slope, flattening and tracing in one step
+        win6(s, wx - ox, wy - oy, g); rot(dir, g, Vm);
+        win6(s, wx + ox, wy + oy, g); rot(dir, g, Vp);
+        R F = R(0.);
+        if (a.prm.flattening) {
+            const long gx = (long)blockIdx.x * T2 + wx - 3, gy = (long)blockIdx.y * T2 + wy - 3;
+            const long np = (long)(a.nx + 2) * (a.ny + 2);
+            F = ((const R *)a.flat)[dir * np + (gy + 1) * (a.nx + 2) + gx + 1];
+        }
+        R wm[6], wp[6];
+        mh_trace(a.prm, e, dtn, hdtn, Vm, Vc, Vp, F, wm, wp);
+        unrot(dir, wm, Wm); unrot(dir, wp, Wp);
+    } else {
     if (a.prm.order == 5) {
         R S[5][6];
 #pragma unroll
@@ -193,6 +207,7 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
     R wm[6], wp[6];
     ppm_trace(e, dtn, hdtn, Vc, vecL, vecR, wm, wp);
     unrot(dir, wm, Wm); unrot(dir, wp, Wp);
+    }
     // transverse flux of the other direction at this cell (from the analysis stage)
 #pragma unroll
     for (int k = 0; k < 6; k++) {
@@ -286,7 +301,7 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
     const R dtnx = R(dt / a.dx), hdtnx = R(0.5 * (dt / a.dx));
     const R dtny = R(dt / a.dy), hdtny = R(0.5 * (dt / a.dy));
     const R hdtx = R(0.5 * dt / a.dx), hdty = R(0.5 * dt / a.dy);
-    const bool ppm = a.prm.order != 5;
+    const bool ppm = a.prm.order == 3;     // PPM reads the slopes of its neighbours
 
     // ---- B: x slopes and sigma_y
     for (int t = tid; t < NDB; t += NT2) {

@@ -416,20 +416,18 @@ __global__ void __launch_bounds__(256) slope3d_kernel(const Args3D a, int d)
     }
 }
 
-// The face states of one cell from its interface values: flattening,
-// characteristic tracing, transverse terms, negativity fallback, gravity and
-// the 3-D full-CTU terms.  Sc: the cell's rotated primitives, vc its 8-vector.
+// The face states of one cell from its traced states wm, wp (sweep frame):
+// transverse terms, negativity fallback, gravity and the 3-D full-CTU terms.
+// vc: the cell's 8-vector.
 template <class R, bool AMR, int DIR>
-__device__ __forceinline__ void face_states_tail(const Args3D &a, const Ctx3<R, AMR> &X, const double dt, const R dtn,
-                                                 const R hdtn, const R hdtx, const R hdty, const R hdtz, int i, int j,
-                                                 int k, const R Sc[6], const R vc[8], const EigBase<R> &eb,
-                                                 const Eig<R> &e, R vecL[6], R vecR[6], R Wm_out[6], R Wp_out[6])
+__device__ __forceinline__ void face_states_finish(const Args3D &a, const Ctx3<R, AMR> &X, const double dt,
+                                                   const R hdtx, const R hdty, const R hdtz, int i, int j, int k,
+                                                   const R vc[8], const EigBase<R> &eb, const R wm[6], const R wp[6],
+                                                   R Wm_out[6], R Wp_out[6])
 {
     constexpr int d = DIR;
     const Grid3 &G = X.G;
-    if (a.prm.flattening) flatten(X.flat[(long)d * G.npad() + G.pidx(i, j, k)], Sc, vecL, vecR);
-    R wm[6], wp[6], Wm[6], Wp[6];
-    ppm_trace(e, dtn, hdtn, Sc, vecL, vecR, wm, wp);
+    R Wm[6], Wp[6];
     unrot3(d, wm, Wm); unrot3(d, wp, Wp);
     // transverse terms, hy_dataReconstOneStep.F90:931-962
     R s1[6], s2[6];
@@ -495,10 +493,28 @@ __device__ __forceinline__ void face_states_tail(const Args3D &a, const Ctx3<R, 
     for (int q = 0; q < 6; q++) { Wm_out[q] = Wm[q]; Wp_out[q] = Wp[q]; }
 }
 
+// The face states of one cell from its interface values: flattening and
+// characteristic tracing (PPM, WENO), then face_states_finish.  Sc: the
+// cell's rotated primitives, vc its 8-vector.
+template <class R, bool AMR, int DIR>
+__device__ __forceinline__ void face_states_tail(const Args3D &a, const Ctx3<R, AMR> &X, const double dt, const R dtn,
+                                                 const R hdtn, const R hdtx, const R hdty, const R hdtz, int i, int j,
+                                                 int k, const R Sc[6], const R vc[8], const EigBase<R> &eb,
+                                                 const Eig<R> &e, R vecL[6], R vecR[6], R Wm_out[6], R Wp_out[6])
+{
+    constexpr int d = DIR;
+    const Grid3 &G = X.G;
+    if (a.prm.flattening) flatten(X.flat[(long)d * G.npad() + G.pidx(i, j, k)], Sc, vecL, vecR);
+    R wm[6], wp[6];
+    ppm_trace(e, dtn, hdtn, Sc, vecL, vecR, wm, wp);
+    face_states_finish<R, AMR, DIR>(a, X, dt, hdtx, hdty, hdtz, i, j, k, vc, eb, wm, wp, Wm_out, Wp_out);
+}
+
 // ---- face states of one cell in direction d ------------------------------------
 // One instantiation per reconstruction order, so the register allocation of
-// the PPM path (three eigensystems and slopes) and of the WENO path (one
-// eigensystem, five projected cells) do not add up.
+// the PPM path (three eigensystems and slopes), of the WENO path (one
+// eigensystem, five projected cells) and of MUSCL-Hancock (ORDER 2, only in
+// the extended-option kernels) do not add up.
 template <class R, int ORDER, bool AMR, int DIR, bool EXT>
 __device__ __forceinline__ void face_states(const Args3D &a, const Ctx3<R, AMR> &X, const double dt, const R dtn,
                                             const R hdtn, const R hdtx, const R hdty, const R hdtz, int i, int j,
@@ -511,7 +527,7 @@ __device__ __forceinline__ void face_states(const Args3D &a, const Ctx3<R, AMR> 
     R S8[5][8], S[5][6], g[6];
 #pragma unroll
     for (int o = -2; o <= 2; o++) {
-        if (ORDER == 3 && (o == -2 || o == 2)) continue;   // PPM reads its neighbours' slopes instead
+        if (ORDER != 5 && (o == -2 || o == 2)) continue;   // PPM reads its neighbours' slopes; MH needs none
         X.load(a, i + o * di, j + o * dj, k + o * dk, S8[o + 2]);
         six(S8[o + 2], g); rot3(d, g, S[o + 2]);
     }
@@ -521,6 +537,14 @@ __device__ __forceinline__ void face_states(const Args3D &a, const Ctx3<R, AMR> 
     if (!eigen_base(S[2][0], S[2][4], vc[GC], eb)) atomicOr(a.err, ERR_SOUND);
     Eig<R> e;
     eigen_dir(eb, S[2][1], e);
+    if constexpr (ORDER == 2) {
+        const R F = a.prm.flattening ? X.flat[(long)d * G.npad() + G.pidx(i, j, k)] : R(0.);
+        R wm[6], wp[6];
+        mh_trace(a.prm, e, dtn, hdtn, S[1], S[2], S[3], F, wm, wp);
+        face_states_finish<R, AMR, DIR>(a, X, dt, hdtx, hdty, hdtz, i, j, k, vc, eb, wm, wp, Wm_out, Wp_out);
+        gc_out = vc[GC]; ge_out = vc[GE];
+        return;
+    }
     R vecL[6], vecR[6];
     if constexpr (ORDER == 5) {
         weno_interfaces(a.prm, e, S, vecL, vecR);
@@ -878,6 +902,22 @@ inline size_t f3d_bytes(int d, int nx, int ny, int nz, size_t rsz)
 // block for the grid-stride kernels, g.y batch entries
 template <class R, bool AMR, int DIR, bool EXT> void launch_states3d_rs(const Args3D &a, dim3 g, cudaStream_t s)
 {
+    if constexpr (EXT) {
+        if (a.prm.order == 2) {   // MUSCL-Hancock: three cells per face state, no slope pass
+            if constexpr (!FusedFaces<R>::value) {
+                states3d_kernel<R, 2, AMR, DIR, true><<<g, 256, 0, s>>>(a);
+                flux3d_kernel<R, AMR, DIR, true><<<dim3(AMR ? a.cta[2] : g.x, g.y), 256, 0, s>>>(a);
+            } else {
+                const int N = DIR == 0 ? a.nx : DIR == 1 ? a.ny : a.nz;
+                const int N1 = DIR == 0 ? a.ny : a.nx, N2 = DIR == 2 ? a.ny : a.nz;
+                const int Ls = a.sf_len[DIR], T1 = a.sf_lines[DIR];
+                const int nseg = (N + Ls - 1) / (Ls - 1), nt1 = (N1 + T1 - 1) / T1;
+                const dim3 gs((unsigned)(nseg * nt1 * N2), g.y);
+                sflux3d_kernel<R, 2, AMR, DIR, true><<<gs, Ls * T1, 8 * sizeof(R) * (size_t)(Ls * T1), s>>>(a);
+            }
+            return;
+        }
+    }
     if constexpr (!FusedFaces<R>::value) {
         if (a.prm.order == 5) {
             states3d_kernel<R, 5, AMR, DIR, EXT><<<g, 256, 0, s>>>(a);
@@ -900,10 +940,10 @@ template <class R, bool AMR, int DIR, bool EXT> void launch_states3d_rs(const Ar
         }
     }
 }
-// the rarely used options (Roe, contact steepening) have kernel instantiations of their own
+// the rarely used options (Roe, contact steepening, MUSCL-Hancock) have kernel instantiations of their own
 template <class R, bool AMR, int DIR> void launch_states3d(const Args3D &a, dim3 g, cudaStream_t s)
 {
-    if (a.prm.riemann == 1 || a.prm.steepening) launch_states3d_rs<R, AMR, DIR, true>(a, g, s);
+    if (extended_options(a.prm)) launch_states3d_rs<R, AMR, DIR, true>(a, g, s);
     else launch_states3d_rs<R, AMR, DIR, false>(a, g, s);
 }
 

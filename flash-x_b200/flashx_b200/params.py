@@ -21,7 +21,7 @@ BC_NAMES = {"periodic": BC_PERIODIC, "outflow": BC_OUTFLOW, "reflect": BC_REFLEC
 
 @dataclass
 class HydroParams:
-    order: int = 3                      # 3 = PPM, 5 = WENO
+    order: int = 3                      # 2 = MUSCL-Hancock, 3 = PPM, 5 = WENO
     wenoMethod: str = "WENO5"           # WENO5 | WENOZ
     RiemannSolver: str = "HLLC"         # HLLC | HLL | LLF | Roe (entropy fix off)
     slopeLimiter: str = "mc"            # minmod | mc | vanLeer | hybrid | limited
@@ -59,8 +59,8 @@ class HydroParams:
     def validate(self):
         """Reject option combinations this path does not implement, the way
         Hydro_init aborts on unknown choices."""
-        if self.order not in (3, 5):
-            raise ValueError("order must be 3 (PPM) or 5 (WENO)")
+        if self.order not in (2, 3, 5):
+            raise ValueError("order must be 2 (MUSCL-Hancock), 3 (PPM) or 5 (WENO)")
         if self.RiemannSolver.upper() not in ("HLLC", "HLL", "LLF", "ROE"):
             raise ValueError("RiemannSolver must be HLLC, HLL, LLF or Roe")
         if self.slopeLimiter.lower() not in ("minmod", "mc", "vanleer", "hybrid", "limited"):

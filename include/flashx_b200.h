@@ -55,7 +55,7 @@ enum fxb_precision { FXB_FP64 = 0, FXB_MIXED = 1 };   /* MIXED: FP32 reconstruct
 
 /* Resolved runtime parameters (names as in the Flash-X Config files). */
 typedef struct fxb_params {
-    int    order;              /* 3 = PPM, 5 = WENO                                  */
+    int    order;              /* 2 = MUSCL-Hancock, 3 = PPM, 5 = WENO               */
     int    weno_method;        /* 1 = WENO5, 2 = WENOZ                               */
     int    riemann;            /* 1 = Roe, 2 = LLF, 3 = HLL, 4 = HLLC (UHD.h)        */
     int    limiter;            /* 1 minmod, 2 mc, 3 vanLeer, 4 hybrid, 5 limited     */
@@ -205,7 +205,7 @@ int fxb_halo_unpack(const double *recv_lo, const double *recv_hi);
  * max_refine = lrefine_max.  flags[nleaf] (registration order): 1 refine,
  * -1 derefine, 0 neither; error[nleaf] (may be NULL): the error estimate of
  * the last variable.  The tree update itself stays with the caller's PARAMESH
- * (amr_refine_derefine), after which the new leaf list is registered again.
+ * (amr_refine_derefine); fxb_regrid then moves the data to the new leaves.
  * FXB_EUNSUPPORTED on a uniform grid. */
 int fxb_mark_refine_derefine(int nvars, const int *refine_var, const double *refine_cutoff,
                              const double *derefine_cutoff, const double *refine_filter, int max_refine,

@@ -290,6 +290,59 @@ static int recon_ppm(const fxo_params *p, int dir, double dt, double delta,
     return 0;
 }
 
+/* ---- hy_DataReconstructNormalDir_MH.F90 (MUSCL-Hancock, order 2) -------- */
+/* S[1..3] = Vm, Vc, Vp.  One TVD slope of the cell (characteristic amplitudes
+ * for the waves when charLimiting, primitive otherwise), flattened; eint (and
+ * the gravity slot) reconstructed linearly, clamped between the cell value
+ * and the face value and traced with the entropy wave (not gravity); the
+ * primitive variables traced over the five waves (Roe: the upwind side
+ * only); gamc and game constant (FLASH_EOS_GAMMA). */
+static int recon_mh(const fxo_params *p, int dir, double dt, double delta,
+                    const double *S[5], int trans_only, double flat,
+                    double lam0[5], double L0[5][5], double R0[5][5],
+                    double Wp[H_NV], double Wm[H_NV], double sig[H_NV])
+{
+    const int nend = p->use_gravity ? 9 : (p->use_aux_eint ? 8 : 5);   /* hyEndVar + 1 */
+    const double *Vm = S[1], *Vc = S[2], *Vp = S[3];
+    const double dtn = dt / delta, hdtn = 0.5 * dtn;
+    for (int k = 0; k < H_NV; k++) { Wp[k] = 0.; Wm[k] = 0.; }
+    if (eigen(Vc, dir, lam0, L0, R0)) return 1;
+    if (p->ndim > 1) upwind_trans(p, Vm, Vc, Vp, lam0, L0, R0, n_end_vars(p), sig);
+    if (trans_only) return 0;
+    double delbar[H_NV];
+    tvd_slope(p, Vm, Vc, Vp, L0, delbar);
+    if (p->flattening)
+        for (int k = 0; k < H_NV; k++) delbar[k] = delbar[k] * (1. - flat);
+    Wp[H_GC] = Vc[H_GC]; Wp[H_GE] = Vc[H_GE];
+    Wm[H_GC] = Vc[H_GC]; Wm[H_GE] = Vc[H_GE];
+    for (int n = H_EI; n < nend; n++) {
+        Wp[n] = Vc[n] + 0.5 * delbar[n];
+        Wm[n] = Vc[n] - 0.5 * delbar[n];
+        Wm[n] = fmax2(fmin2(Vc[n], Wm[n]), fmin2(fmax2(Vc[n], Wm[n]), Wm[n]));
+        Wp[n] = fmax2(fmin2(Vc[n], Wp[n]), fmin2(fmax2(Vc[n], Wp[n]), Wp[n]));
+        if (n != H_GR) {
+            Wp[n] = Wp[n] - fmax2(lam0[3], 0.) * hdtn * delbar[n];
+            Wm[n] = Wm[n] - fmin2(lam0[3], 0.) * hdtn * delbar[n];
+        }
+    }
+    double sigL[5] = {0., 0., 0., 0., 0.}, sigR[5] = {0., 0., 0., 0., 0.};
+    const int roe = p->riemann == FXO_ROE;
+    for (int n = 0; n < 5; n++) {
+        const double amp = p->char_limiting ? delbar[n] : dot5(L0, n, delbar);
+        const double cL = .5 * (-1. - dtn * lam0[n]), cR = .5 * (1. - dtn * lam0[n]);
+        const int left = !roe || lam0[n] < 0., right = !roe || !(lam0[n] < 0.);
+        for (int v = 0; v < 5; v++) {
+            if (left) sigL[v] = sigL[v] + cL * R0[v][n] * amp;
+            if (right) sigR[v] = sigR[v] + cR * R0[v][n] * amp;
+        }
+    }
+    for (int v = 0; v < 5; v++) {
+        Wm[v] = Vc[v] + sigL[v];
+        Wp[v] = Vc[v] + sigR[v];
+    }
+    return 0;
+}
+
 /* ---- WENO5 / WENO-Z reconstruction: see recon_weno below --------------- */
 static int recon_weno(const fxo_params *p, int dir, double dt, double delta,
                       const double *S[5], int trans_only, double flat,
@@ -718,6 +771,8 @@ static int riemann_states(const blk_t *b, const double *U, double dt, scratch_t 
             double flat = p->flattening ? FC[d * b->ncell + c] : 0.;
             int err = (p->order == 5)
                 ? recon_weno(p, d, dt, del[d], S, tr[d], flat, lam + 5 * d, leig[d], reig[d], Wp[d], Wn[d], sig + 9 * d)
+                : (p->order == 2)
+                ? recon_mh(p, d, dt, del[d], S, tr[d], flat, lam + 5 * d, leig[d], reig[d], Wp[d], Wn[d], sig + 9 * d)
                 : recon_ppm(p, d, dt, del[d], S, tr[d], flat, lam + 5 * d, leig[d], reig[d], Wp[d], Wn[d], sig + 9 * d);
             if (err) return 1;
         }
@@ -1081,7 +1136,7 @@ int fxo_eos_interior(const fxo_params *p, double *unk)
 int fxo_hydro_step(const fxo_params *p, double *unk, double dt, double dt_old, int nthreads)
 {
     (void)dt_old;
-    if (p->ndim < 2 || p->ndim > 3 || p->nguard < 4 || (p->order != 3 && p->order != 5)) return 3;
+    if (p->ndim < 2 || p->ndim > 3 || p->nguard < 4 || (p->order != 2 && p->order != 3 && p->order != 5)) return 3;
     fxo_fill_guardcells(p, unk);
     blk_t b; blk_init(&b, p);
     long nblk = (long)p->nblockx * p->nblocky * p->nblockz;

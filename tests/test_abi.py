@@ -52,7 +52,7 @@ def test_init_validation_codes():
     assert lib.fxb_init(ctypes.byref(p), ctypes.byref(d), H.default_var_map(), 11) == H.FXB_EUNSUPPORTED
     d.ndim = 2; d.nguard = 2
     assert lib.fxb_init(ctypes.byref(p), ctypes.byref(d), H.default_var_map(), 11) == H.FXB_EARG
-    d.nguard = 4; p.order = 2
+    d.nguard = 4; p.order = 4
     assert lib.fxb_init(ctypes.byref(p), ctypes.byref(d), H.default_var_map(), 11) == H.FXB_EUNSUPPORTED
     p.order = 3; p.riemann = 5
     assert lib.fxb_init(ctypes.byref(p), ctypes.byref(d), H.default_var_map(), 11) == H.FXB_EUNSUPPORTED
@@ -109,7 +109,8 @@ def test_parameter_validation_mirrors_hydro_init():
     HydroParams(RiemannSolver="Roe").validate()
     HydroParams(RiemannSolver="Roe", entropy=True, entropyFixMethod="Harten").validate()
     HydroParams(use_steepening=True).validate()
-    for bad in (dict(order=2), dict(RiemannSolver="Marquina"), dict(entropyFixMethod="Einfeldt"),
+    HydroParams(order=2).validate()
+    for bad in (dict(order=4), dict(order=6), dict(RiemannSolver="Marquina"), dict(entropyFixMethod="Einfeldt"),
                 dict(slopeLimiter="superbee"),
                 dict(transOrder=3), dict(use_upwindTVD=True), dict(use_flattening=True, useGravity=True),
                 dict(hydroComputeDtOption=0)):

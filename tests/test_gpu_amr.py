@@ -58,6 +58,7 @@ def _gpu(root, hp, mesh, unk, dts, precision="fp64"):
 
 
 @pytest.mark.parametrize("bc,maxlev,order,flat", [
+    ((BC_PERIODIC,) * 6, 2, 2, False),
     ((BC_PERIODIC,) * 6, 2, 5, False),
     ((BC_OUTFLOW, BC_OUTFLOW, BC_PERIODIC, BC_PERIODIC, BC_REFLECTING, BC_REFLECTING), 2, 3, False),
     ((BC_PERIODIC,) * 6, 3, 5, False),

@@ -96,6 +96,9 @@ def test_100_steps_fp64_l1(oracle, need_gpu, name):
     dict(slopeLimiter="minmod"), dict(slopeLimiter="vanLeer"), dict(slopeLimiter="hybrid"),
     dict(slopeLimiter="limited", LimitedSlopeBeta=1.5), dict(charLimiting=False),
     dict(charLimiting=False, slopeLimiter="hybrid"), dict(use_auxEintEqn=False), dict(hy_fPresInMomFlux=0.5),
+    dict(order=2), dict(order=2, RiemannSolver="Roe"), dict(order=2, charLimiting=False, slopeLimiter="hybrid"),
+    dict(order=2, slopeLimiter="limited", LimitedSlopeBeta=1.5), dict(order=2, RiemannSolver="HLL",
+                                                                      use_auxEintEqn=False),
 ])
 def test_options_one_step_fp64(oracle, need_gpu, opts):
     geom = Geometry(2, 16, 16, 1, 3, 2, 1, bc=(BC_PERIODIC, BC_PERIODIC, BC_REFLECTING, BC_OUTFLOW, 1, 1))
@@ -126,7 +129,7 @@ def test_steepening_2d_fp64(oracle, need_gpu, flattening):
     assert not np.array_equal(ref, ref0)   # the steepening acted
 
 
-@pytest.mark.parametrize("order", [3, 5])
+@pytest.mark.parametrize("order", [2, 3, 5])
 def test_flattening_2d_fp64(oracle, need_gpu, order):
     """use_flattening on the 45-degree Sod problem, where the shock switches it on."""
     geom, _, init = S.config("sod2d", scale=0.25)
@@ -232,7 +235,8 @@ def test_negative_pressure_reports_status(need_gpu):
 # ---------------------------------------------------------------- 3-D
 @pytest.mark.parametrize("case", ["ppm_periodic", "sod_outflow", "rt_weno_gravity", "hll_noctu", "wenoz_reflect",
                                   "sod_flattening", "weno_flattening_reflect", "llf_sod", "roe_sod_reflect",
-                                  "sod_steepening"])
+                                  "sod_steepening", "mh_sod", "mh_rt_gravity", "mh_roe_flattening_reflect",
+                                  "mh_primitive_noctu"])
 def test_3d_fp64_matches_oracle(oracle, need_gpu, case):
     """3-D path (full CTU corner coupling, gravity, WENO) against the oracle,
     three steps, bit for bit."""
@@ -269,6 +273,23 @@ def test_3d_fp64_matches_oracle(oracle, need_gpu, case):
         geom = Geometry(3, 16, 16, 16, 2, 1, 1, bc=(BC_OUTFLOW,) * 6)
         hp = HydroParams(use_flattening=True)
         unk = S.sod(geom, hp, xangle=30.0, yangle=70.0, posn=0.6)
+    elif case == "mh_sod":
+        geom = Geometry(3, 16, 16, 16, 2, 1, 1, bc=(BC_OUTFLOW,) * 6)
+        hp = HydroParams(order=2)
+        unk = S.sod(geom, hp, xangle=30.0, yangle=70.0, posn=0.6)
+    elif case == "mh_rt_gravity":
+        geom = Geometry(3, 16, 16, 16, 1, 1, 2, bbox=((0, 1), (0, 1), (0, 2)),
+                        bc=(BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_REFLECTING, BC_REFLECTING))
+        hp = HydroParams(order=2, useGravity=True, gravity=(0.0, 0.0, -0.1))
+        unk = S.rayleigh_taylor(geom, hp)
+    elif case == "mh_roe_flattening_reflect":
+        geom = Geometry(3, 16, 16, 16, 1, 2, 1, bc=(BC_REFLECTING,) * 6)
+        hp = HydroParams(order=2, RiemannSolver="Roe", use_flattening=True)
+        unk = S.sod(geom, hp, xangle=30.0, yangle=70.0, posn=0.6)
+    elif case == "mh_primitive_noctu":
+        geom = Geometry(3, 16, 16, 16, 1, 2, 1, bc=(BC_PERIODIC,) * 6)
+        hp = HydroParams(order=2, charLimiting=False, use_3dFullCTU=False, slopeLimiter="vanLeer")
+        unk = S.noisy_gas(geom, hp)
     elif case == "weno_flattening_reflect":
         geom = Geometry(3, 16, 16, 16, 1, 1, 1, bc=(BC_REFLECTING,) * 6)
         hp = HydroParams(order=5, use_flattening=True)
@@ -380,3 +401,29 @@ def test_roe_entropy_fix_fp64(oracle, need_gpu, entropy, method):
         hp0 = HydroParams(RiemannSolver="Roe")
         _, ref0 = oracle_dts(oracle, geom, hp0, unk, 5, first=dts[0])
         assert not np.array_equal(ref, ref0)
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_muscl_hancock_mixed_close_to_fp64(need_gpu, ndim):
+    """order = 2 in the FP32-reconstruction path stays within the mixed-precision
+    tolerance of the FP64 path (20 steps)."""
+    if ndim == 2:
+        geom, _, init = S.config("kh2d", scale=1 / 16)
+    else:
+        geom = Geometry(3, 16, 16, 16, 2, 2, 2, bc=(BC_PERIODIC,) * 6)
+        init = S.noisy_gas
+    hp = HydroParams(order=2, gamma=1.4 if ndim == 2 else 5.0 / 3.0)
+    unk = init(geom, hp)
+    outs = []
+    for prec in ("fp64", "mixed"):
+        dev = HydroDevice(geom, hp, prec)
+        dev.attach_unk(unk.copy())
+        dt = 0.5 * dev.Hydro_computeDt()
+        for _ in range(20):
+            dev.Hydro(0.0, dt, dt)
+        o = np.zeros(geom.unk_shape)
+        dev.sync_to_host(o)
+        outs.append(S.gather_global(geom, o)[..., DENS])
+        dev.close()
+    l1 = np.mean(np.abs(outs[1] - outs[0])) / np.mean(np.abs(outs[0]))
+    assert 0 < l1 <= L1_TOL_MIXED

@@ -38,11 +38,13 @@ def run_oracle(O, geom, hp, unk, tmax=None, nsteps=None):
     return t, n
 
 
-def test_sod_2d_matches_exact_solution(oracle):
+@pytest.mark.parametrize("order", [3, 2])
+def test_sod_2d_matches_exact_solution(oracle, order):
     """2-D Sod at 45 degrees, 128^2: density along the diagonal vs the exact
-    solution at t=0.2 (the analytic check of Sod/shocktube.pro, soderror.pro)."""
+    solution at t=0.2 (the analytic check of Sod/shocktube.pro, soderror.pro),
+    with PPM and with MUSCL-Hancock (order 2, same bounds)."""
     geom = Geometry(2, 16, 16, 1, 8, 8, 1, bc=(BC_OUTFLOW,) * 6)
-    hp = HydroParams()
+    hp = HydroParams(order=order)
     unk = S.sod(geom, hp)
     t, n = run_oracle(oracle, geom, hp, unk, tmax=0.2)
     assert abs(t - 0.2) < 1e-12 and n > 50
