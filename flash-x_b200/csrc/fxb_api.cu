@@ -475,6 +475,8 @@ extern "C" int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
     q.flattening = p.flattening ? 1 : 0;
     q.entropy_fix = p.entropy_fix;
     q.steepening = p.steepening ? 1 : 0;
+    q.use_avisc = p.use_avisc ? 1 : 0;
+    q.cvisc = p.cvisc;
     // Gamma/Eos_init.F90:86 and Gamma/Eos.F90:177,240-241
     double gammam1 = 1.0 / (p.gamma - 1.0);
     L.gam1inv = 1. / gammam1;

@@ -31,6 +31,8 @@ struct DevParams {
     int flattening;
     int entropy_fix;           // Roe: 0 off, 1 Harten-Hyman, 2 Harten
     int steepening;            // PPM contact steepening
+    int use_avisc;             // artificial viscosity
+    double cvisc;
 };
 
 // ---- precision helpers ---------------------------------------------------
@@ -49,10 +51,11 @@ template <> __device__ __forceinline__ float divc<float>(float x, double c) { re
 
 // options compiled only into kernel instantiations of their own (template
 // flag EXT), so the default kernels keep their registers: the Roe solver,
-// PPM contact steepening, MUSCL-Hancock reconstruction (order 2)
+// PPM contact steepening, MUSCL-Hancock reconstruction (order 2), artificial
+// viscosity
 __host__ __device__ inline bool extended_options(const DevParams &p)
 {
-    return p.riemann == 1 || p.steepening || p.order == 2;
+    return p.riemann == 1 || p.steepening || p.order == 2 || p.use_avisc;
 }
 
 // Fortran MIN/MAX with gfortran's argument order: mvar = a1; if (a2 < mvar) mvar = a2
@@ -400,6 +403,44 @@ __device__ __forceinline__ void mh_trace(const DevParams &prm, const Eig<R> &e, 
                    sR[4] = sR[4] + cR[4] * e.rp * A[4]; }
 #pragma unroll
     for (int v = 0; v < 5; v++) { Wm[v] = Vc[v] + sL[v]; Wp[v] = Vc[v] + sR[v]; }
+}
+
+// Artificial viscosity of one face (hy_getFaceFlux.F90:397-438 x, 700-745 y,
+// 955-990 z; Colella and Woodward 1984), added to the Godunov flux before the
+// aux-eint fluxes are formed: cvisc times the negative part of the undivided
+// velocity divergence at the face (normal difference nm -> n0 of the cells
+// behind and ahead, plus the transverse terms tr[e] = quarter-weighted
+// central differences of both cells times del[d]/del[e], 0 where absent),
+// times the jump of dens, momenta and total energy.  Ul, Ur: D, VX, VY, VZ,
+// ENER of the cells behind and ahead.
+template <class R>
+__device__ __forceinline__ void avisc_flux(R cvisc, int d, int ndim, R nm, R n0, const R tr[3], const R Ul[5],
+                                           const R Ur[5], R F[])
+{
+    R div;
+    if (d == 0) {
+        div = n0 - nm;
+        if (ndim > 1) div = div + tr[1];
+        if (ndim > 2) div = div + tr[2];
+    } else if (d == 1) {
+        div = tr[0] + n0 - nm;
+        if (ndim > 2) div = div + tr[2];
+    } else {
+        div = tr[0] + tr[1] + n0 - nm;
+    }
+    const R cv = cvisc * fmax2(-(div), R(0.));
+    F[0] = F[0] + cv * (Ul[0] - Ur[0]);
+#pragma unroll
+    for (int q = 1; q < 5; q++) F[q] = F[q] + cv * (Ul[0] * Ul[q] - Ur[0] * Ur[q]);
+}
+// aux-eint and volume fluxes from the final mass flux (hy_getFaceFlux.F90:444-453)
+template <class R>
+__device__ __forceinline__ void eint_fluxes(const DevParams &prm, const R *Vm, const R *Vp, R F[])
+{
+    if (prm.use_aux_eint) {
+        if (F[0] > R(0)) { F[FVOL] = rdiv(F[0], Vm[D]); F[FEI] = F[0] * Vm[5]; }
+        else             { F[FVOL] = rdiv(F[0], Vp[D]); F[FEI] = F[0] * Vp[5]; }
+    } else { F[FVOL] = R(0); F[FEI] = R(0); }
 }
 
 // contact steepening of the PPM density interface values

@@ -224,6 +224,15 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
     for (int k = 0; k < 6; k++) { s.W[k][t] = Wp[k]; s.W[6 + k][t] = Wm[k]; }
 }
 
+// total energy of a window cell, read from the state (the window holds D..EI)
+template <class R> __device__ __forceinline__ R ener2d(const Args2D &a, int wx, int wy)
+{
+    double s_ = 1.0;
+    const int gx = (int)(blockIdx.x * T2) + wx - 3, gy = (int)(blockIdx.y * T2) + wy - 3;
+    const int mx = map_axis(gx, a.nx, a.bc[0], a.bc[1], &s_), my = map_axis(gy, a.ny, a.bc[2], a.bc[3], &s_);
+    return (R)__ldg(a.in + DV_ENER * a.vstride + (long)my * a.nx + mx);
+}
+
 template <class R, bool EXT>
 __device__ __forceinline__ void faces_stage(const Args2D &a, Smem2D<R> &s, int dir, int t, int wl, int wr,
                                             int wxl, int wyl, int wxr, int wyr)
@@ -234,6 +243,17 @@ __device__ __forceinline__ void faces_stage(const Args2D &a, Smem2D<R> &s, int d
     int e = riemann<R, EXT>(a.prm, dir, VL, s.V[GC][wyl][wxl], s.V[GE][wyl][wxl],
                     VR, s.V[GC][wyr][wxr], s.V[GE][wyr][wxr], F);
     if (e) set_err(a.err, e);
+    if (EXT && a.prm.use_avisc) {
+        const int td = 1 - dir, tx = td == 0, ty = td == 1, vt = td == 0 ? VX : VY, vn = dir == 0 ? VX : VY;
+        const R del[2] = {R(a.dx), R(a.dy)};
+        R tr[3] = {R(0.), R(0.), R(0.)};
+        tr[td] = R(0.25) * (s.V[vt][wyr + ty][wxr + tx] - s.V[vt][wyr - ty][wxr - tx] + s.V[vt][wyl + ty][wxl + tx] -
+                            s.V[vt][wyl - ty][wxl - tx]) * del[dir] / del[td];
+        const R Ul[5] = {s.V[D][wyl][wxl], s.V[VX][wyl][wxl], s.V[VY][wyl][wxl], s.V[VZ][wyl][wxl], ener2d<R>(a, wxl, wyl)};
+        const R Ur[5] = {s.V[D][wyr][wxr], s.V[VX][wyr][wxr], s.V[VY][wyr][wxr], s.V[VZ][wyr][wxr], ener2d<R>(a, wxr, wyr)};
+        avisc_flux(R(a.prm.cvisc), dir, 2, s.V[vn][wyl][wxl], s.V[vn][wyr][wxr], tr, Ul, Ur, F);
+        eint_fluxes(a.prm, VL, VR, F);
+    }
 #pragma unroll
     for (int k = 0; k < NF; k++) s.DBF[k * NFC + t] = F[k];
 }

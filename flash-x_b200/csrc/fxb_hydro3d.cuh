@@ -270,6 +270,48 @@ template <class R> __device__ __forceinline__ void unrot3(int dir, const R *r, R
 __device__ __forceinline__ void offs(int d, int o, int &di, int &dj, int &dk)
 { di = d == 0 ? o : 0; dj = d == 1 ? o : 0; dk = d == 2 ? o : 0; }
 
+// one state variable of a possibly virtual cell of the uniform grid
+template <class R>
+__device__ __forceinline__ R state_var(const Args3D &a, int q, int i, int j, int k)
+{
+    double sx = 1.0, sy = 1.0, sz = 1.0;
+    int mi = map_axis(i, a.nx, a.bc[0], a.bc[1], &sx);
+    int mj = map_axis(j, a.ny, a.bc[2], a.bc[3], &sy);
+    int mk = map_axis(k, a.nz, a.bc[4], a.bc[5], &sz);
+    double x = __ldg(a.in + q * a.vstride + ((long)mk * a.ny + mj) * a.nx + mi);
+    if (q == VX) x = x * sx;
+    if (q == VY) x = x * sy;
+    if (q == VZ) x = x * sz;
+    return (R)x;
+}
+
+// artificial viscosity of the direction-d face between cells (i,j,k) - e_d
+// and (i,j,k) of the uniform grid (AMR meshes do not take the option)
+template <class R>
+__device__ __forceinline__ void avisc3d(const Args3D &a, int d, int i, int j, int k, R F[])
+{
+    int di, dj, dk;
+    offs(d, 1, di, dj, dk);
+    const int im = i - di, jm = j - dj, km = k - dk;
+    const R del[3] = {R(a.dx), R(a.dy), R(a.dz)};
+    R tr[3] = {R(0.), R(0.), R(0.)};
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+        if (e == d) continue;
+        int ie, je, ke;
+        offs(e, 1, ie, je, ke);
+        const int v = VX + e;
+        tr[e] = R(0.25) * (state_var<R>(a, v, i + ie, j + je, k + ke) - state_var<R>(a, v, i - ie, j - je, k - ke) +
+                           state_var<R>(a, v, im + ie, jm + je, km + ke) - state_var<R>(a, v, im - ie, jm - je, km - ke)) *
+                del[d] / del[e];
+    }
+    const R Ul[5] = {state_var<R>(a, D, im, jm, km), state_var<R>(a, VX, im, jm, km), state_var<R>(a, VY, im, jm, km),
+                     state_var<R>(a, VZ, im, jm, km), state_var<R>(a, DV_ENER, im, jm, km)};
+    const R Ur[5] = {state_var<R>(a, D, i, j, k), state_var<R>(a, VX, i, j, k), state_var<R>(a, VY, i, j, k),
+                     state_var<R>(a, VZ, i, j, k), state_var<R>(a, DV_ENER, i, j, k)};
+    avisc_flux(R(a.prm.cvisc), d, 3, Ul[1 + d], Ur[1 + d], tr, Ul, Ur, F);
+}
+
 // (i, j, k) of the linear index of an lx * ly * lz box, in 32-bit arithmetic:
 // every box a kernel walks holds fewer than 2^30 cells (checked by fxb_init)
 __device__ __forceinline__ void unflatten(unsigned idx, unsigned lx, unsigned ly, int &i, int &j, int &k)
@@ -643,6 +685,9 @@ __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
         X.load_gammas(a, i, j, k, gcr, ger);
         int e = riemann<R, EXT>(a.prm, d, VL, gcl, gel, VR, gcr, ger, F);
         if (e) atomicOr(a.err, e);
+        if constexpr (EXT && !AMR) {
+            if (a.prm.use_avisc) { avisc3d<R>(a, d, i, j, k, F); eint_fluxes(a.prm, VL, VR, F); }
+        }
 #pragma unroll
         for (int q = 0; q < NF; q++) f[(long)q * nf + idx] = F[q];
     }
@@ -763,6 +808,9 @@ __global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) 
         for (int q = 0; q < 6; q++) VL[q] = sW[q * nt + tl];
         const int e = riemann<R, EXT>(a.prm, d, VL, sW[6 * nt + tl], sW[7 * nt + tl], Wm, gc, ge, F);
         if (e) atomicOr(a.err, e);
+        if constexpr (EXT && !AMR) {
+            if (a.prm.use_avisc) { avisc3d<R>(a, d, i, j, k, F); eint_fluxes(a.prm, VL, Wm, F); }
+        }
         R *f = X.flx[d];
         const long nf = G.nf(d), fi = G.fidx(d, i, j, k);
 #pragma unroll

@@ -45,7 +45,7 @@ class FxbParams(ctypes.Structure):
         ("tiny", ctypes.c_double), ("fpres", ctypes.c_double), ("limited_beta", ctypes.c_double),
         ("gas_constant", ctypes.c_double), ("abar", ctypes.c_double),
         ("precision", ctypes.c_int), ("flattening", ctypes.c_int), ("entropy_fix", ctypes.c_int),
-        ("steepening", ctypes.c_int),
+        ("steepening", ctypes.c_int), ("use_avisc", ctypes.c_int), ("cvisc", ctypes.c_double),
     ]
 
 
@@ -156,6 +156,8 @@ def make_fxb_params(hp: HydroParams, precision="fp64"):
     p.flattening = int(hp.use_flattening)
     p.entropy_fix = 0 if not hp.entropy else (1 if hp.entropyFixMethod.upper() == "HARTENHYMAN" else 2)
     p.steepening = int(hp.use_steepening)
+    p.use_avisc = int(hp.use_avisc)
+    p.cvisc = hp.cvisc
     return p
 
 

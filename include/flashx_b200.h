@@ -73,6 +73,8 @@ typedef struct fxb_params {
     int    entropy_fix;        /* Roe: entropy = .false. (0), entropyFixMethod
                                   HartenHyman (1) or Harten (2)                     */
     int    steepening;         /* use_steepening: PPM contact steepening            */
+    int    use_avisc;          /* use_avisc: artificial viscosity (uniform grids)    */
+    double cvisc;              /* cvisc: its constant (Config default 0.1)           */
 } fxb_params;
 
 /* Domain of a uniform block grid. */

@@ -875,8 +875,54 @@ static int riemann_states(const blk_t *b, const double *U, double dt, scratch_t 
     return 0;
 }
 
+/* Artificial viscosity of one face (hy_getFaceFlux.F90:397-438 x, 700-745 y,
+ * 955-990 z; Colella and Woodward 1984): cvisc times the negative part of the
+ * undivided velocity divergence at the face (the normal difference plus the
+ * quarter-weighted transverse central differences of both cells, scaled by
+ * the cell-width ratios), times the jump of the conserved dens, momenta and
+ * total energy from the cell behind the face to the cell ahead. */
+static void avisc_face(const blk_t *b, const double *U, int d, int i, int j, int k, double fl[8])
+{
+    const fxo_params *p = b->p;
+    const int ndim = p->ndim;
+    const double del[3] = {b->dx, b->dy, b->dz};
+#define UV(var, ii, jj, kk) U[cidx(b, ii, jj, kk) * FXO_NUNK + (var)]
+    const int it = d == 0, jt = d == 1, kt = d == 2;
+    const int im = i - it, jm = j - jt, km = k - kt;
+    /* quarter-weighted central difference of velocity e across axis e, in both cells */
+    double tr[3] = {0., 0., 0.};
+    for (int e = 0; e < ndim; e++) {
+        if (e == d) continue;
+        const int ie = e == 0, je = e == 1, ke = e == 2;
+        const int v = FXO_VELX + e;
+        tr[e] = 0.25 * (UV(v, i + ie, j + je, k + ke) - UV(v, i - ie, j - je, k - ke) +
+                        UV(v, im + ie, jm + je, km + ke) - UV(v, im - ie, jm - je, km - ke)) * del[d] / del[e];
+    }
+    const int vn = FXO_VELX + d;
+    const double nd = UV(vn, i, j, k), ndm = UV(vn, im, jm, km);
+    double div;
+    if (d == 0) {
+        div = nd - ndm;
+        if (ndim > 1) div = div + tr[1];
+        if (ndim > 2) div = div + tr[2];
+    } else if (d == 1) {
+        div = tr[0] + nd - ndm;
+        if (ndim > 2) div = div + tr[2];
+    } else {
+        div = tr[0] + tr[1] + nd - ndm;
+    }
+    const double cv = p->cvisc * fmax2(-(div), 0.);
+    const double dl = UV(FXO_DENS, im, jm, km), dr = UV(FXO_DENS, i, j, k);
+    fl[F_D] = fl[F_D] + cv * (dl - dr);
+    fl[F_MX] = fl[F_MX] + cv * (dl * UV(FXO_VELX, im, jm, km) - dr * UV(FXO_VELX, i, j, k));
+    fl[F_MY] = fl[F_MY] + cv * (dl * UV(FXO_VELY, im, jm, km) - dr * UV(FXO_VELY, i, j, k));
+    fl[F_MZ] = fl[F_MZ] + cv * (dl * UV(FXO_VELZ, im, jm, km) - dr * UV(FXO_VELZ, i, j, k));
+    fl[F_E] = fl[F_E] + cv * (dl * UV(FXO_ENER, im, jm, km) - dr * UV(FXO_ENER, i, j, k));
+#undef UV
+}
+
 /* hy_getFaceFlux.F90:300-572 (+y, z) for one block. */
-static int face_fluxes(const blk_t *b, scratch_t *s)
+static int face_fluxes(const blk_t *b, const double *U, scratch_t *s)
 {
     const fxo_params *p = b->p;
     const int ndim = p->ndim;
@@ -895,6 +941,7 @@ static int face_fluxes(const blk_t *b, scratch_t *s)
             if (err) return 2;
             double *fl = s->flx[d] + c * 8;
             for (int v = 0; v < 6; v++) fl[v] = F[v];
+            if (p->use_avisc) avisc_face(b, U, d, i, j, k, fl);
             if (p->use_aux_eint) {
                 if (fl[F_D] > 0.) { fl[F_VOL] = fl[F_D] / VL[H_D]; fl[F_EI] = fl[F_D] * VL[H_EI]; }
                 else              { fl[F_VOL] = fl[F_D] / VR[H_D]; fl[F_EI] = fl[F_D] * VR[H_EI]; }
@@ -1155,7 +1202,7 @@ int fxo_hydro_step(const fxo_params *p, double *unk, double dt, double dt_old, i
         for (long blk = 0; blk < nblk; blk++) {
             double *U = unk + blk * b.ncell * FXO_NUNK;
             int e = riemann_states(&b, U, dt, &s);
-            if (!e) e = face_fluxes(&b, &s);
+            if (!e) e = face_fluxes(&b, U, &s);
             if (!e) {
                 unsplit_update(&b, U, dt, &s);
                 if (!p->use_gravity) { energy_fix(&b, U); eos_block(&b, U); }

@@ -41,7 +41,7 @@ typedef struct {
     int nguard;                     /* NGUARD (4) */
     double xmin, xmax, ymin, ymax, zmin, zmax;
     int bc[6];                      /* xl xr yl yr zl zr */
-    int order;                      /* 3 = PPM, 5 = WENO */
+    int order;                      /* 2 = MUSCL-Hancock, 3 = PPM, 5 = WENO */
     int weno_method;                /* 1 = WENO5 (Jiang-Shu), 2 = WENO-Z */
     int riemann;                    /* FXO_HLL / FXO_HLLC */
     int limiter;                    /* FXO_MINMOD ... */
@@ -57,6 +57,8 @@ typedef struct {
     int flattening;                 /* use_flattening */
     int entropy_fix;                /* Roe: entropy off (0), HartenHyman (1), Harten (2) */
     int steepening;                 /* use_steepening (PPM contact steepening) */
+    int use_avisc;                  /* artificial viscosity (hy_getFaceFlux.F90:397-438) */
+    double cvisc;                   /* its constant */
 } fxo_params;
 
 /* Number of doubles in one UNK array for the given geometry. */

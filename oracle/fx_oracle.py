@@ -43,6 +43,7 @@ class FxoParams(ctypes.Structure):
         ("limited_beta", ctypes.c_double),
         ("gas_constant", ctypes.c_double), ("abar", ctypes.c_double),
         ("flattening", ctypes.c_int), ("entropy_fix", ctypes.c_int), ("steepening", ctypes.c_int),
+        ("use_avisc", ctypes.c_int), ("cvisc", ctypes.c_double),
     ]
 
 
@@ -116,6 +117,8 @@ def make_params(geom, hp):
     p.flattening = int(hp.use_flattening)
     p.entropy_fix = 0 if not hp.entropy else (1 if hp.entropyFixMethod.upper() == "HARTENHYMAN" else 2)
     p.steepening = int(hp.use_steepening)
+    p.use_avisc = int(hp.use_avisc)
+    p.cvisc = hp.cvisc
     return p
 
 

@@ -112,7 +112,8 @@ def test_parameter_validation_mirrors_hydro_init():
     HydroParams(order=2).validate()
     for bad in (dict(order=4), dict(order=6), dict(RiemannSolver="Marquina"), dict(entropyFixMethod="Einfeldt"),
                 dict(slopeLimiter="superbee"),
-                dict(transOrder=3), dict(use_upwindTVD=True), dict(use_flattening=True, useGravity=True),
+                dict(transOrder=3), dict(use_upwindTVD=True), dict(use_hybridOrder=True),
+                dict(use_flattening=True, useGravity=True),
                 dict(hydroComputeDtOption=0)):
         with pytest.raises(ValueError):
             HydroParams(**bad).validate()

@@ -261,3 +261,11 @@ def test_regrid_rejects_two_levels_and_keeps_the_mesh(oracle, need_gpu):
     dev.sync_to_host(out)
     assert np.array_equal(_interior(root, out), _interior(root, ref))
     dev.close()
+
+
+def test_amr_rejects_artificial_viscosity(need_gpu):
+    root, hp, mesh, unk = _case((BC_PERIODIC,) * 6, 2, order=3)
+    hp.use_avisc = True
+    with pytest.raises(FlashXError) as e:
+        HydroDevice(root, hp, "fp64", mesh=mesh)
+    assert e.value.code == 6

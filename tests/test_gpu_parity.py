@@ -99,6 +99,7 @@ def test_100_steps_fp64_l1(oracle, need_gpu, name):
     dict(order=2), dict(order=2, RiemannSolver="Roe"), dict(order=2, charLimiting=False, slopeLimiter="hybrid"),
     dict(order=2, slopeLimiter="limited", LimitedSlopeBeta=1.5), dict(order=2, RiemannSolver="HLL",
                                                                       use_auxEintEqn=False),
+    dict(use_avisc=True), dict(use_avisc=True, cvisc=0.3, order=2), dict(use_avisc=True, use_auxEintEqn=False),
 ])
 def test_options_one_step_fp64(oracle, need_gpu, opts):
     geom = Geometry(2, 16, 16, 1, 3, 2, 1, bc=(BC_PERIODIC, BC_PERIODIC, BC_REFLECTING, BC_OUTFLOW, 1, 1))
@@ -236,7 +237,7 @@ def test_negative_pressure_reports_status(need_gpu):
 @pytest.mark.parametrize("case", ["ppm_periodic", "sod_outflow", "rt_weno_gravity", "hll_noctu", "wenoz_reflect",
                                   "sod_flattening", "weno_flattening_reflect", "llf_sod", "roe_sod_reflect",
                                   "sod_steepening", "mh_sod", "mh_rt_gravity", "mh_roe_flattening_reflect",
-                                  "mh_primitive_noctu"])
+                                  "mh_primitive_noctu", "avisc_sod", "avisc_weno_periodic"])
 def test_3d_fp64_matches_oracle(oracle, need_gpu, case):
     """3-D path (full CTU corner coupling, gravity, WENO) against the oracle,
     three steps, bit for bit."""
@@ -273,6 +274,15 @@ def test_3d_fp64_matches_oracle(oracle, need_gpu, case):
         geom = Geometry(3, 16, 16, 16, 2, 1, 1, bc=(BC_OUTFLOW,) * 6)
         hp = HydroParams(use_flattening=True)
         unk = S.sod(geom, hp, xangle=30.0, yangle=70.0, posn=0.6)
+    elif case == "avisc_sod":
+        geom = Geometry(3, 16, 16, 16, 2, 1, 1, bc=(BC_OUTFLOW,) * 6)
+        hp = HydroParams(use_avisc=True)
+        unk = S.sod(geom, hp, xangle=30.0, yangle=70.0, posn=0.6)
+    elif case == "avisc_weno_periodic":
+        geom = Geometry(3, 16, 16, 16, 1, 1, 2, bc=(BC_PERIODIC, BC_PERIODIC, BC_REFLECTING, BC_REFLECTING,
+                                                    BC_PERIODIC, BC_PERIODIC))
+        hp = HydroParams(order=5, use_avisc=True, cvisc=0.2, gamma=5.0 / 3.0)
+        unk = S.noisy_gas(geom, hp)
     elif case == "mh_sod":
         geom = Geometry(3, 16, 16, 16, 2, 1, 1, bc=(BC_OUTFLOW,) * 6)
         hp = HydroParams(order=2)

@@ -296,3 +296,27 @@ def test_flattening_acts_only_at_strong_shocks(oracle):
         res.append((g, np.mean(np.abs(g[idx, idx, DENS][keep] - rho_ex[keep]))))
     assert not np.array_equal(res[0][0], res[1][0])
     assert res[1][1] < 5e-3
+
+
+def test_artificial_viscosity_conserves_and_acts(oracle):
+    """use_avisc (hy_getFaceFlux.F90:397-438): the viscous fluxes are
+    conservative (periodic KH keeps mass, momentum and energy to roundoff)
+    and change the solution where the flow converges (Sod)."""
+    geom = Geometry(2, 16, 16, 1, 4, 4, 1, bc=(BC_PERIODIC,) * 6)
+    hp = HydroParams(use_avisc=True, cvisc=0.3)
+    unk = S.kelvin_helmholtz(geom, hp)
+    p = oracle.make_params(geom.as_dict(), hp)
+    I0 = oracle.integrals(p, unk)
+    run_oracle(oracle, geom, hp, unk, nsteps=20)
+    I1 = oracle.integrals(p, unk)
+    assert abs(I1[0] - I0[0]) / I0[0] < 1e-13
+    assert abs(I1[1] - I0[1]) < 1e-13 * I0[0]
+    assert abs(I1[4] - I0[4]) / I0[4] < 1e-13
+    g2 = Geometry(2, 16, 16, 1, 4, 4, 1, bc=(BC_OUTFLOW,) * 6)
+    outs = []
+    for av in (False, True):
+        h = HydroParams(use_avisc=av)
+        u = S.sod(g2, h)
+        run_oracle(oracle, g2, h, u, nsteps=10)
+        outs.append(S.gather_global(g2, u)[..., DENS])
+    assert not np.array_equal(outs[0], outs[1])
