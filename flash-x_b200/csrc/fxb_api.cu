@@ -408,6 +408,9 @@ extern "C" int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
     if (d.ndim == 2 && p.use_gravity) return fail(FXB_EUNSUPPORTED, "fxb_init: gravity is implemented for 3-D only");
     if (p.flattening && p.use_gravity) return fail(FXB_EUNSUPPORTED, "fxb_init: use_flattening with gravity is not implemented");
     if (p.entropy_fix < 0 || p.entropy_fix > 2) return fail(FXB_EARG, "fxb_init: unknown entropyFixMethod");
+    // unsplit/Hydro_init.F90:137: use_upwindTVD only acts with more than four guard cells
+    if (p.upwind_tvd && d.nguard > 4)
+        return fail(FXB_EUNSUPPORTED, "fxb_init: use_upwindTVD with NGUARD > 4 is not implemented");
     for (int i = 0; i < 2 * d.ndim; i++)
         if (d.bc[i] < 0 || d.bc[i] > 2) return fail(FXB_EARG, "fxb_init: unknown boundary condition");
     for (int a = 0; a < d.ndim; a++) {

@@ -46,6 +46,7 @@ class FxbParams(ctypes.Structure):
         ("gas_constant", ctypes.c_double), ("abar", ctypes.c_double),
         ("precision", ctypes.c_int), ("flattening", ctypes.c_int), ("entropy_fix", ctypes.c_int),
         ("steepening", ctypes.c_int), ("use_avisc", ctypes.c_int), ("cvisc", ctypes.c_double),
+        ("upwind_tvd", ctypes.c_int),
     ]
 
 
@@ -158,6 +159,7 @@ def make_fxb_params(hp: HydroParams, precision="fp64"):
     p.steepening = int(hp.use_steepening)
     p.use_avisc = int(hp.use_avisc)
     p.cvisc = hp.cvisc
+    p.upwind_tvd = int(hp.use_upwindTVD)
     return p
 
 

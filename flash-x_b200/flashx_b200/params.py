@@ -34,7 +34,7 @@ class HydroParams:
     entropy: bool = False               # Roe's entropy fix (hy_entropyFix.F90)
     entropyFixMethod: str = "HartenHyman"   # HartenHyman | Harten
     use_steepening: bool = False
-    use_upwindTVD: bool = False
+    use_upwindTVD: bool = False         # off with NGUARD <= 4 (unsplit/Hydro_init.F90:137)
     use_avisc: bool = False             # artificial viscosity (uniform grids)
     cvisc: float = 0.1
     use_hybridOrder: bool = False
@@ -74,7 +74,7 @@ class HydroParams:
             raise ValueError("entropyFixMethod must be HartenHyman or Harten")
         if self.use_flattening and self.useGravity:
             raise ValueError("use_flattening with gravity is not supported by this path")
-        for flag in ("use_upwindTVD", "use_hybridOrder"):
+        for flag in ("use_hybridOrder",):
             if getattr(self, flag):
                 raise ValueError(flag + " is not supported by this path")
         if self.hydroComputeDtOption != -1:

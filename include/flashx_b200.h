@@ -75,6 +75,9 @@ typedef struct fxb_params {
     int    steepening;         /* use_steepening: PPM contact steepening            */
     int    use_avisc;          /* use_avisc: artificial viscosity (uniform grids)    */
     double cvisc;              /* cvisc: its constant (Config default 0.1)           */
+    int    upwind_tvd;         /* use_upwindTVD: off when NGUARD <= 4, as
+                                  unsplit/Hydro_init.F90:137 resets it; rejected
+                                  (FXB_EUNSUPPORTED) with more guard cells        */
 } fxb_params;
 
 /* Domain of a uniform block grid. */

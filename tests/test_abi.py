@@ -86,6 +86,13 @@ def test_slab_validation_codes():
     assert init(0, 2, 0, 40) == H.FXB_EARG         # halo wider than the slab
     assert init(0, 2, 8, 16) == H.FXB_EARG         # halo on an outflow boundary
     assert init(0, 2, 0, 4) == H.FXB_EUNSUPPORTED  # 32 + 4 rows do not fill 16-row tiles
+    # use_upwindTVD: reset with NGUARD = 4 (Hydro_init.F90:137), refused with more guard cells
+    p.upwind_tvd = 1
+    assert init(0, 2, 0, 16) in (H.FXB_OK, H.FXB_ECUDA)
+    d.nguard = 6
+    assert init(0, 2, 0, 16) == H.FXB_EUNSUPPORTED
+    d.nguard = 4
+    p.upwind_tvd = 0
     d.bc[2] = d.bc[3] = BC_PERIODIC
     assert init(0, 4, 8, 8) in (H.FXB_OK, H.FXB_ECUDA)   # one slab exchanging with itself
     sub = H.leaf_blocks(geom, (1, 3))
@@ -110,9 +117,10 @@ def test_parameter_validation_mirrors_hydro_init():
     HydroParams(RiemannSolver="Roe", entropy=True, entropyFixMethod="Harten").validate()
     HydroParams(use_steepening=True).validate()
     HydroParams(order=2).validate()
+    HydroParams(use_upwindTVD=True, use_avisc=True).validate()
     for bad in (dict(order=4), dict(order=6), dict(RiemannSolver="Marquina"), dict(entropyFixMethod="Einfeldt"),
                 dict(slopeLimiter="superbee"),
-                dict(transOrder=3), dict(use_upwindTVD=True), dict(use_hybridOrder=True),
+                dict(transOrder=3), dict(use_hybridOrder=True),
                 dict(use_flattening=True, useGravity=True),
                 dict(hydroComputeDtOption=0)):
         with pytest.raises(ValueError):
