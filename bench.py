@@ -276,6 +276,39 @@ def run_reference(args):
         dist.destroy_process_group()
 
 
+def regrid_cycle(dev, hp, mesh):
+    """One Grid_updateRefinement on the AMR workload after the timed steps
+    (not part of the zone-update rate): refinement marks on the device
+    (density criterion of the workload, Paramesh4 defaults refine_cutoff 0.8,
+    derefine_cutoff 0.2, refine_filter 0.01), the tree update on the host,
+    the data movement on the device (fxb_regrid), then two steps on the new
+    mesh.  Host wall time of each part, with the device synchronised."""
+    import torch
+    maxlev = int(max(mesh.levels))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    flags, _ = dev.Grid_markRefineDerefine([("dens", 0.8, 0.2, 0.01)], maxlev)
+    t1 = time.perf_counter()
+    from flashx_b200.amr import refine_derefine
+    new = refine_derefine(dev.mesh, flags, 1, maxlev)
+    t2 = time.perf_counter()
+    from flashx_b200.hydro import _check, mesh_blocks
+    _check(dev.lib.fxb_regrid(mesh_blocks(new.levels, new.bcoords), new.nleaf))
+    torch.cuda.synchronize()
+    t3 = time.perf_counter()
+    dev.mesh, dev.unk_shape = new, new.unk_shape
+    dt = 0.5 * dev.Hydro_computeDt()
+    for _ in range(2):
+        dev.Hydro(0.0, dt, dt)
+    step_ms = dev.last_timing()[0]
+    return {"leaves_before": int(mesh.nleaf), "leaves_after": int(new.nleaf),
+            "marked_refine": int(np.sum(np.asarray(flags) == 1)), "marked_derefine": int(np.sum(np.asarray(flags) == -1)),
+            "mark_ms": 1e3 * (t1 - t0), "tree_update_ms": 1e3 * (t2 - t1),
+            "regrid_ms": 1e3 * (t3 - t2), "step_ms_after": step_ms,
+            "note": "regrid_ms covers fxb_regrid: restriction, copies, prolongation, Eos and the new mesh's "
+                    "tree, neighbour tables and guard-fill plan (the tuned launch shapes are kept)"}
+
+
 def run_ours(args):
     import torch
     dist, world, rank, local = dist_setup(args, "nccl")
@@ -412,6 +445,7 @@ def run_ours(args):
     if mesh is not None:
         line["config"]["leaves_per_level"] = mesh.level_counts()
         line["config"]["tuning"] = dev.tuning()
+        line["regrid"] = regrid_cycle(dev, hp, mesh)
     dev.close()
 
     # ---- mixed precision

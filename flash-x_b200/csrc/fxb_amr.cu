@@ -1549,9 +1549,9 @@ int amr_step(const double *dtv, double dt, int *launches)
 // keeps its data (a derefined parent its children's average); new children,
 // level by level from coarse to fine, are prolonged from their parent in
 // conserved form (mpi_amr_prolong.F90); Eos on every leaf.  Only the old
-// interior store stays allocated while the new mesh is built.  A rejected
-// list, or a new block whose parent was not an old leaf, restores the old
-// mesh and its data.
+// interior store stays allocated while the new mesh is built, and the launch
+// shapes tuned on the old mesh are kept.  A rejected list, or a new block
+// whose parent was not an old leaf, restores the old mesh and its data.
 int amr_regrid(const fxb_block_desc *leaves, int nleaf)
 {
     if (!S.active) return record_error(FXB_EARG, "fxb_regrid: needs a registered AMR mesh");
@@ -1578,7 +1578,9 @@ int amr_regrid(const fxb_block_desc *leaves, int nleaf)
                             S.C.stream);
         cudaStreamSynchronize(S.C.stream);
         cudaFree(ostore);
-        if (rc == FXB_OK) amr_tune();
+        S.fill_cta = old.fill_cta;
+        for (int q = 0; q < 4; q++) S.cta[q] = old.cta[q];
+        snprintf(S.tune_log, sizeof(S.tune_log), "%s", old.tune_log);
         return code;
     };
     int rc = amr_create(old.C, leaves, nleaf);
@@ -1629,8 +1631,12 @@ int amr_regrid(const fxb_block_desc *leaves, int nleaf)
     cudaFree(d_pairs);
     cudaFree(d_fresh);
     cudaFree(ostore);
-    if (rc) return rc;
-    return amr_tune();
+    // the launch shapes tuned on the old mesh carry over (blocks of the same
+    // size; the shapes change timings, never results)
+    S.fill_cta = old.fill_cta;
+    for (int q = 0; q < 4; q++) S.cta[q] = old.cta[q];
+    snprintf(S.tune_log, sizeof(S.tune_log), "%s", old.tune_log);
+    return rc;
 }
 
 int amr_rate()
