@@ -1166,6 +1166,8 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     if (c.prm.use_gravity) return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: gravity is not implemented on AMR meshes");
     if (c.prm.use_avisc)
         return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: artificial viscosity is implemented for uniform grids");
+    if (c.prm.hybrid_order)
+        return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: hybrid order is implemented for uniform grids");
     S.n = D.nxb;
     S.ng = D.nguard;
     S.nleaf = nleaf;

@@ -52,6 +52,7 @@ struct Lib {
     void *sig3 = nullptr, *w3[3] = {nullptr, nullptr, nullptr}, *f3[3] = {nullptr, nullptr, nullptr};
     void *slp3 = nullptr;          // PPM slopes of one direction (3-D)
     void *flat = nullptr;          // flattening coefficients (2-D and 3-D)
+    void *hyb = nullptr;           // hybrid order (3-D): DivU and the per-cell flags
     fxb_error lasterr{};
 };
 Lib L;
@@ -311,6 +312,7 @@ int launch_hydro(int src, const double *dtv, double dt)
         a.slp_bstride = 0;
         a.flat = L.flat;
         a.flat_bstride = 0;
+        a.hyb = (const unsigned char *)L.hyb;
         for (int d = 0; d < 3; d++) { a.wst[d] = L.w3[d]; a.flx[d] = L.f3[d]; }
         if (L.prm.precision == FXB_MIXED) launch_hydro3d_mixed(a, L.stream);
         else launch_hydro3d_fp64(a, L.stream);
@@ -365,6 +367,7 @@ void free_all()
     if (L.sig3) cudaFree(L.sig3);
     if (L.slp3) cudaFree(L.slp3);
     if (L.flat) cudaFree(L.flat);
+    if (L.hyb) cudaFree(L.hyb);
     for (int d = 0; d < 3; d++) {
         if (L.w3[d]) cudaFree(L.w3[d]);
         if (L.f3[d]) cudaFree(L.f3[d]);
@@ -480,6 +483,8 @@ extern "C" int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
     q.steepening = p.steepening ? 1 : 0;
     q.use_avisc = p.use_avisc ? 1 : 0;
     q.cvisc = p.cvisc;
+    q.use_hybrid = p.hybrid_order ? 1 : 0;
+    q.hybrid_kappa = p.hybrid_kappa;
     // Gamma/Eos_init.F90:86 and Gamma/Eos.F90:177,240-241
     double gammam1 = 1.0 / (p.gamma - 1.0);
     L.gam1inv = 1. / gammam1;
@@ -521,6 +526,7 @@ extern "C" int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
         // intermediates of the unfused 3-D pipeline, in the reconstruction type
         size_t rsz = p.precision == FXB_MIXED ? sizeof(float) : sizeof(double);
         CK(cudaMalloc(&L.sig3, sig3d_bytes(L.nx, L.ny, L.nz, rsz)));
+        if (p.hybrid_order) CK(cudaMalloc(&L.hyb, hyb3d_bytes(L.nx, L.ny, L.nz, rsz)));
         // PPM slopes in memory: FP64 only (the FP32 face-state kernel computes them itself)
         if (p.order == 3 && p.precision == FXB_FP64) CK(cudaMalloc(&L.slp3, slp3d_bytes(L.nx, L.ny, L.nz, rsz)));
         for (int dd = 0; dd < 3; dd++) {

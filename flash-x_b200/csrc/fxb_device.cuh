@@ -33,6 +33,8 @@ struct DevParams {
     int steepening;            // PPM contact steepening
     int use_avisc;             // artificial viscosity
     double cvisc;
+    int use_hybrid;            // hybrid order: first-order states at shocks
+    double hybrid_kappa;
 };
 
 // ---- precision helpers ---------------------------------------------------
@@ -52,10 +54,10 @@ template <> __device__ __forceinline__ float divc<float>(float x, double c) { re
 // options compiled only into kernel instantiations of their own (template
 // flag EXT), so the default kernels keep their registers: the Roe solver,
 // PPM contact steepening, MUSCL-Hancock reconstruction (order 2), artificial
-// viscosity
+// viscosity, hybrid order
 __host__ __device__ inline bool extended_options(const DevParams &p)
 {
-    return p.riemann == 1 || p.steepening || p.order == 2 || p.use_avisc;
+    return p.riemann == 1 || p.steepening || p.order == 2 || p.use_avisc || p.use_hybrid;
 }
 
 // Fortran MIN/MAX with gfortran's argument order: mvar = a1; if (a2 < mvar) mvar = a2
@@ -441,6 +443,40 @@ __device__ __forceinline__ void eint_fluxes(const DevParams &prm, const R *Vm, c
         if (F[0] > R(0)) { F[FVOL] = rdiv(F[0], Vm[D]); F[FEI] = F[0] * Vm[5]; }
         else             { F[FVOL] = rdiv(F[0], Vp[D]); F[FEI] = F[0] * Vp[5]; }
     } else { F[FVOL] = R(0); F[FEI] = R(0); }
+}
+
+// Hybrid order (hy_dataReconstOneStep.F90:864-913, hy_checkRHjumpCond.F90):
+// where the velocity converges (the caller found min DivU over the cell's
+// box below hybridOrderKappa times the sound speed), face states whose
+// density leaves the bounds of a shock jump, (gamc-1)/(gamc+1) to
+// (gamc+1)/(gamc-1) times the cell density, in a flow of Mach^2 > 1e-4,
+// fall back to the cell values.  g: the cell's 6-vector (D, VX, VY, VZ, P,
+// EI) in global order (ndim components in Mach^2); reset: the same values
+// in the frame of Wm/Wp.
+template <class R>
+__device__ __forceinline__ void hybrid_rh(int ndim, const R g[6], const R reset[6], R gamc, R Wm[6], R Wp[6])
+{
+    const R dens = g[0], pres = g[4];
+    const R gr = rdiv(gamc + R(1.), gamc - R(1.));
+    R m2 = R(0.);
+    for (int e = 0; e < ndim; e++) m2 = m2 + g[1 + e] * g[1 + e];
+    m2 = rdiv(m2 * dens, gamc * pres);
+    bool sw = false;
+    if (m2 > R(1.e-4)) {
+        if (Wm[0] > gr * dens || gr * Wm[0] < dens) sw = true;
+        if (Wp[0] > gr * dens || gr * Wp[0] < dens) sw = true;
+    }
+    if (sw) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) { Wm[k] = reset[k]; Wp[k] = reset[k]; }
+    }
+}
+// the hybrid-order threshold hybridOrderKappa * sqrt(gamc p / rho) of a cell
+template <class R> __device__ __forceinline__ R hybrid_eps(const DevParams &prm, R dens, R pres, R gamc)
+{
+    R cs = gamc * pres;
+    cs = rsqrt_(rdiv(cs, dens));
+    return R(prm.hybrid_kappa) * cs;
 }
 
 // contact steepening of the PPM density interface values

@@ -141,6 +141,27 @@ __device__ __forceinline__ void analysis_stage(const Args2D &a, Smem2D<R> &s, in
     for (int k = 0; k < 6; k++) s.SG[k][t] = sg[k];
 }
 
+// velocity component q (VX or VY) of window cell (wx, wy); read from the
+// state through the boundary map when it lies outside the window
+template <class R> __device__ __forceinline__ R vel2d(const Args2D &a, const Smem2D<R> &s, int q, int wx, int wy)
+{
+    if (wx >= 0 && wx < WIN && wy >= 0 && wy < WIN) return s.V[q][wy][wx];
+    double sx = 1.0, sy = 1.0;
+    const int gx = (int)(blockIdx.x * T2) + wx - 3, gy = (int)(blockIdx.y * T2) + wy - 3;
+    const int mx = map_axis(gx, a.nx, a.bc[0], a.bc[1], &sx), my = map_axis(gy, a.ny, a.bc[2], a.bc[3], &sy);
+    double v = __ldg(a.in + q * a.vstride + (long)my * a.nx + mx);
+    if (q == VX) v = v * sx;
+    if (q == VY) v = v * sy;
+    return (R)v;
+}
+// hybrid order's undivided velocity divergence (hy_getRiemannState.F90:341-360)
+template <class R> __device__ __forceinline__ R divu2d(const Args2D &a, const Smem2D<R> &s, int wx, int wy)
+{
+    R dv = vel2d(a, s, VX, wx + 1, wy) - vel2d(a, s, VX, wx - 1, wy);
+    dv = dv + vel2d(a, s, VY, wx, wy + 1) - vel2d(a, s, VY, wx, wy - 1);
+    return R(0.5) * dv;
+}
+
 // face states of one cell along dir, with the transverse correction of the
 // other direction (hy_dataReconstOneStep.F90:931-936) and the negativity
 // fallback (:1131-1165); stores global-order Wp/Wm into s.W[.][t].
@@ -207,6 +228,17 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
     R wm[6], wp[6];
     ppm_trace(e, dtn, hdtn, Vc, vecL, vecR, wm, wp);
     unrot(dir, wm, Wm); unrot(dir, wp, Wp);
+    }
+    if (EXT && a.prm.use_hybrid) {
+        const int k4 = a.prm.order - 1 > 2 ? 2 : a.prm.order - 1;
+        const R eps = hybrid_eps(a.prm, s.V[D][wy][wx], s.V[P][wy][wx], s.V[GC][wy][wx]);
+        R mn = divu2d(a, s, wx - k4, wy - k4);
+        for (int jj = -k4; jj <= k4; jj++)
+            for (int ii = -k4; ii <= k4; ii++) mn = fmin(mn, divu2d(a, s, wx + ii, wy + jj));
+        if (mn < eps) {
+            win6(s, wx, wy, g);
+            hybrid_rh(2, g, g, s.V[GC][wy][wx], Wm, Wp);
+        }
     }
     // transverse flux of the other direction at this cell (from the analysis stage)
 #pragma unroll

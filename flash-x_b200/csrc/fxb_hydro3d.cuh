@@ -79,6 +79,7 @@ struct Args3D {
     int cta[4];                 // CTAs per batch entry: sig3d, slope3d, (unused), update3d
     FastDiv fdx[5], fdy[5];     // divisors nx + e and ny + e (e = 0, 1, 2, 4), set by the launchers
     int sf_len[3], sf_lines[3]; // face-state tiles per direction (cells along d, lines), set by the launchers
+    const unsigned char *hyb;   // hybrid order (uniform grid): 1 where min DivU over the cell's box < eps, padded box
     long rate_c0 = 0, rate_c1 = 0x7fffffffffffffffL;   // cells [c0, c1) enter the CFL rate (a slab's own)
 };
 // Face-state tile of direction d (N cells along d, N1 along the t1 axis):
@@ -535,10 +536,25 @@ __device__ __forceinline__ void face_states_finish(const Args3D &a, const Ctx3<R
     for (int q = 0; q < 6; q++) { Wm_out[q] = Wm[q]; Wp_out[q] = Wp[q]; }
 }
 
+// hybrid order on the traced states wm, wp (sweep frame) of a uniform-grid
+// cell whose flag (hyb3d_kernel) is set
+template <class R, bool AMR>
+__device__ __forceinline__ void hybrid3d(const Args3D &a, const Grid3 &G, int i, int j, int k, const R vc[8],
+                                         const R Sc[6], R wm[6], R wp[6])
+{
+    if constexpr (!AMR) {
+        if (a.prm.use_hybrid && a.hyb[G.pidx(i, j, k)]) {
+            R g[6];
+            six(vc, g);
+            hybrid_rh(3, g, Sc, vc[GC], wm, wp);
+        }
+    }
+}
+
 // The face states of one cell from its interface values: flattening and
 // characteristic tracing (PPM, WENO), then face_states_finish.  Sc: the
 // cell's rotated primitives, vc its 8-vector.
-template <class R, bool AMR, int DIR>
+template <class R, bool AMR, int DIR, bool EXT = false>
 __device__ __forceinline__ void face_states_tail(const Args3D &a, const Ctx3<R, AMR> &X, const double dt, const R dtn,
                                                  const R hdtn, const R hdtx, const R hdty, const R hdtz, int i, int j,
                                                  int k, const R Sc[6], const R vc[8], const EigBase<R> &eb,
@@ -549,6 +565,7 @@ __device__ __forceinline__ void face_states_tail(const Args3D &a, const Ctx3<R, 
     if (a.prm.flattening) flatten(X.flat[(long)d * G.npad() + G.pidx(i, j, k)], Sc, vecL, vecR);
     R wm[6], wp[6];
     ppm_trace(e, dtn, hdtn, Sc, vecL, vecR, wm, wp);
+    if constexpr (EXT) hybrid3d<R, AMR>(a, G, i, j, k, vc, Sc, wm, wp);
     face_states_finish<R, AMR, DIR>(a, X, dt, hdtx, hdty, hdtz, i, j, k, vc, eb, wm, wp, Wm_out, Wp_out);
 }
 
@@ -583,6 +600,7 @@ __device__ __forceinline__ void face_states(const Args3D &a, const Ctx3<R, AMR> 
         const R F = a.prm.flattening ? X.flat[(long)d * G.npad() + G.pidx(i, j, k)] : R(0.);
         R wm[6], wp[6];
         mh_trace(a.prm, e, dtn, hdtn, S[1], S[2], S[3], F, wm, wp);
+        hybrid3d<R, AMR>(a, G, i, j, k, vc, S[2], wm, wp);
         face_states_finish<R, AMR, DIR>(a, X, dt, hdtx, hdty, hdtz, i, j, k, vc, eb, wm, wp, Wm_out, Wp_out);
         gc_out = vc[GC]; ge_out = vc[GE];
         return;
@@ -610,8 +628,8 @@ __device__ __forceinline__ void face_states(const Args3D &a, const Ctx3<R, AMR> 
                     dbN[0], dbP[0], vecL, vecR);
         }
     }
-    face_states_tail<R, AMR, DIR>(a, X, dt, dtn, hdtn, hdtx, hdty, hdtz, i, j, k, S[2], vc, eb, e, vecL, vecR, Wm_out,
-                                  Wp_out);
+    face_states_tail<R, AMR, DIR, EXT>(a, X, dt, dtn, hdtn, hdtx, hdty, hdtz, i, j, k, S[2], vc, eb, e, vecL, vecR,
+                                       Wm_out, Wp_out);
     gc_out = vc[GC]; ge_out = vc[GE];
 }
 
@@ -780,8 +798,8 @@ __global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) 
                 steepen(R(a.prm.tiny), R(d == 0 ? X.dx : d == 1 ? X.dy : X.dz), Smm[D], Sr[0], Sr[1], Sr[2], Spp[D],
                         S8[1][GE], dbN[0], dbP[0], vecL, vecR);
             }
-            face_states_tail<R, AMR, DIR>(a, X, dt, dtn, hdtn, hdtx, hdty, hdtz, i, j, k, Sr[1], S8[1], eb, e, vecL,
-                                          vecR, Wm, Wp);
+            face_states_tail<R, AMR, DIR, EXT>(a, X, dt, dtn, hdtn, hdtx, hdty, hdtz, i, j, k, Sr[1], S8[1], eb, e,
+                                               vecL, vecR, Wm, Wp);
             gc = S8[1][GC];
             ge = S8[1][GE];
         }
@@ -998,10 +1016,66 @@ template <class R, bool AMR, int DIR> void launch_states3d(const Args3D &a, dim3
 // slope cells a face-state tile adds per line: two when the FP32 kernel computes the PPM slopes itself
 template <class R> int sflux_halo(const Args3D &a) { return (FusedFaces<R>::value && a.prm.order == 3) ? 2 : 0; }
 
+// hybrid order, uniform grid: DivU (hy_getRiemannState.F90:341-360) on
+// [-3, n+2]^3, stored with offset 3
+template <class R>
+__global__ void __launch_bounds__(256) divu3d_kernel(const Args3D a, R *divu)
+{
+    const long ex = a.nx + 6, ey = a.ny + 6, n = ex * ey * (a.nz + 6);
+    FXB_GRID_LOOP(idx, n) {
+        const int i = (int)(idx % ex) - 3, j = (int)((idx / ex) % ey) - 3, k = (int)(idx / (ex * ey)) - 3;
+        R dv = state_var<R>(a, VX, i + 1, j, k) - state_var<R>(a, VX, i - 1, j, k);
+        dv = dv + state_var<R>(a, VY, i, j + 1, k) - state_var<R>(a, VY, i, j - 1, k);
+        dv = dv + state_var<R>(a, VZ, i, j, k + 1) - state_var<R>(a, VZ, i, j, k - 1);
+        divu[idx] = R(0.5) * dv;
+    }
+}
+// the flag of every cell of the padded box [-1, n]^3: min DivU over the
+// cell's (2 k4 + 1)^3 box below hybridOrderKappa times its sound speed
+template <class R>
+__global__ void __launch_bounds__(256) hyb3d_kernel(const Args3D a, const R *divu, unsigned char *flag)
+{
+    const Grid3 G{a.nx, a.ny, a.nz};
+    const long ex = a.nx + 6, ey = a.ny + 6, np = G.npad();
+    const int k4 = a.prm.order - 1 > 2 ? 2 : a.prm.order - 1;
+    FXB_GRID_LOOP(idx, np) {
+        const int i = (int)(idx % (a.nx + 2)) - 1, j = (int)((idx / (a.nx + 2)) % (a.ny + 2)) - 1,
+                  k = (int)(idx / ((long)(a.nx + 2) * (a.ny + 2))) - 1;
+        const R eps = hybrid_eps(a.prm, state_var<R>(a, D, i, j, k), state_var<R>(a, P, i, j, k),
+                                 state_var<R>(a, GC, i, j, k));
+        R mn = divu[((long)(k - k4 + 3) * ey + (j - k4 + 3)) * ex + (i - k4 + 3)];
+        for (int kk = -k4; kk <= k4; kk++)
+            for (int jj = -k4; jj <= k4; jj++)
+                for (int ii = -k4; ii <= k4; ii++)
+                    mn = fmin(mn, divu[((long)(k + kk + 3) * ey + (j + jj + 3)) * ex + (i + ii + 3)]);
+        flag[idx] = mn < eps ? 1 : 0;
+    }
+}
+// bytes of the hybrid-order scratch of a uniform grid: DivU in R, then the flags
+inline size_t hyb3d_bytes(int nx, int ny, int nz, size_t rsz)
+{
+    return rsz * (size_t)(nx + 6) * (ny + 6) * (nz + 6) + (size_t)(nx + 2) * (ny + 2) * (nz + 2);
+}
+
 template <class R> void launch_hydro3d_t(const Args3D &a0, cudaStream_t s)
 {
     const Args3D a = with_divisors(a0, sflux_halo<R>(a0));
     const int nb = 148 * 8;
+    if (a.prm.use_hybrid) {
+        R *divu = (R *)a.hyb;
+        unsigned char *flag = (unsigned char *)a.hyb + sizeof(R) * (size_t)(a.nx + 6) * (a.ny + 6) * (a.nz + 6);
+        divu3d_kernel<R><<<nb, 256, 0, s>>>(a, divu);
+        hyb3d_kernel<R><<<nb, 256, 0, s>>>(a, divu, flag);
+        Args3D b = a;
+        b.hyb = flag;
+        if (a.prm.flattening) flat3d_kernel<R, false><<<nb, 256, 0, s>>>(b);
+        sig3d_kernel<R, false><<<nb, 256, 0, s>>>(b);
+        launch_states3d<R, false, 0>(b, dim3(nb), s);
+        launch_states3d<R, false, 1>(b, dim3(nb), s);
+        launch_states3d<R, false, 2>(b, dim3(nb), s);
+        update3d_kernel<R, false><<<nb, 256, 0, s>>>(b);
+        return;
+    }
     if (a.prm.flattening) flat3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
     sig3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
     launch_states3d<R, false, 0>(a, dim3(nb), s);

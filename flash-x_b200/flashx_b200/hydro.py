@@ -46,7 +46,7 @@ class FxbParams(ctypes.Structure):
         ("gas_constant", ctypes.c_double), ("abar", ctypes.c_double),
         ("precision", ctypes.c_int), ("flattening", ctypes.c_int), ("entropy_fix", ctypes.c_int),
         ("steepening", ctypes.c_int), ("use_avisc", ctypes.c_int), ("cvisc", ctypes.c_double),
-        ("upwind_tvd", ctypes.c_int),
+        ("upwind_tvd", ctypes.c_int), ("hybrid_order", ctypes.c_int), ("hybrid_kappa", ctypes.c_double),
     ]
 
 
@@ -160,6 +160,8 @@ def make_fxb_params(hp: HydroParams, precision="fp64"):
     p.use_avisc = int(hp.use_avisc)
     p.cvisc = hp.cvisc
     p.upwind_tvd = int(hp.use_upwindTVD)
+    p.hybrid_order = int(hp.use_hybridOrder)
+    p.hybrid_kappa = hp.hybridOrderKappa
     return p
 
 

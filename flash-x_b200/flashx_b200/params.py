@@ -37,7 +37,8 @@ class HydroParams:
     use_upwindTVD: bool = False         # off with NGUARD <= 4 (unsplit/Hydro_init.F90:137)
     use_avisc: bool = False             # artificial viscosity (uniform grids)
     cvisc: float = 0.1
-    use_hybridOrder: bool = False
+    use_hybridOrder: bool = False       # first-order states at shocks (uniform grids)
+    hybridOrderKappa: float = 0.0
     hydroComputeDtOption: int = -1
     cfl: float = 0.8
     gamma: float = 1.4
@@ -74,9 +75,6 @@ class HydroParams:
             raise ValueError("entropyFixMethod must be HartenHyman or Harten")
         if self.use_flattening and self.useGravity:
             raise ValueError("use_flattening with gravity is not supported by this path")
-        for flag in ("use_hybridOrder",):
-            if getattr(self, flag):
-                raise ValueError(flag + " is not supported by this path")
         if self.hydroComputeDtOption != -1:
             raise ValueError("hydroComputeDtOption must be -1")
         return self

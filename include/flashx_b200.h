@@ -78,6 +78,8 @@ typedef struct fxb_params {
     int    upwind_tvd;         /* use_upwindTVD: off when NGUARD <= 4, as
                                   unsplit/Hydro_init.F90:137 resets it; rejected
                                   (FXB_EUNSUPPORTED) with more guard cells        */
+    int    hybrid_order;       /* use_hybridOrder (uniform grids)                    */
+    double hybrid_kappa;       /* hybridOrderKappa (Config default 0)                */
 } fxb_params;
 
 /* Domain of a uniform block grid. */

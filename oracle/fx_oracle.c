@@ -642,6 +642,7 @@ typedef struct {
     double *reig;       /* [cell][3][5][5] */
     double *pav;        /* VAR1 averaged pressure [cell] */
     double *flat;       /* flattening: FlatTilde [3][cell], then FlatCoeff [3][cell] */
+    double *divu;       /* hybrid order: undivided velocity divergence [cell] */
 } scratch_t;
 
 static void scratch_alloc(scratch_t *s, long ncell)
@@ -656,11 +657,12 @@ static void scratch_alloc(scratch_t *s, long ncell)
     s->reig = (double *)calloc((size_t)ncell * 75, sizeof(double));
     s->pav = (double *)calloc((size_t)ncell, sizeof(double));
     s->flat = (double *)calloc((size_t)ncell * 6, sizeof(double));
+    s->divu = (double *)calloc((size_t)ncell, sizeof(double));
 }
 static void scratch_free(scratch_t *s)
 {
     for (int d = 0; d < 3; d++) { free(s->scr[d]); free(s->flx[d]); }
-    free(s->sig); free(s->lam); free(s->leig); free(s->reig); free(s->pav); free(s->flat);
+    free(s->sig); free(s->lam); free(s->leig); free(s->reig); free(s->pav); free(s->flat); free(s->divu);
 }
 
 static void blk_init(blk_t *b, const fxo_params *p)
@@ -692,6 +694,24 @@ static int riemann_states(const blk_t *b, const double *U, double dt, scratch_t 
     const int klo = b->k3 ? b->k0 - 1 : 0, khi = b->k3 ? b->kmax + 1 : 0;
     const int jlo = b->k2 ? b->j0 - 1 : 0, jhi = b->k2 ? b->jmax + 1 : 0;
     double *FT = s->flat, *FC = s->flat + 3 * b->ncell;
+    /* hybrid order: DivU = (u(i+1) - u(i-1) + v(j+1) - v(j-1) + w(k+1) - w(k-1)) / 2 on
+     * [lo - 1 - k4, hi + 1 + k4] (hy_getRiemannState.F90:322-361, kHydro = 1) */
+    const int k4 = p->order - 1 > 2 ? 2 : p->order - 1;
+    if (p->use_hybrid) {
+        const int hk0 = b->k3 ? b->k0 - 1 - k4 : 0, hk1 = b->k3 ? b->kmax + 1 + k4 : 0;
+        const int hj0 = b->k2 ? b->j0 - 1 - k4 : 0, hj1 = b->k2 ? b->jmax + 1 + k4 : 0;
+        for (int k = hk0; k <= hk1; k++)
+        for (int j = hj0; j <= hj1; j++)
+        for (int i = b->i0 - 1 - k4; i <= b->imax + 1 + k4; i++) {
+            double dv = U[cidx(b, i + 1, j, k) * FXO_NUNK + FXO_VELX] - U[cidx(b, i - 1, j, k) * FXO_NUNK + FXO_VELX];
+            if (ndim > 1) {
+                dv = dv + U[cidx(b, i, j + 1, k) * FXO_NUNK + FXO_VELY] - U[cidx(b, i, j - 1, k) * FXO_NUNK + FXO_VELY];
+                if (ndim > 2)
+                    dv = dv + U[cidx(b, i, j, k + 1) * FXO_NUNK + FXO_VELZ] - U[cidx(b, i, j, k - 1) * FXO_NUNK + FXO_VELZ];
+            }
+            s->divu[cidx(b, i, j, k)] = 0.5 * dv;
+        }
+    }
     if (p->flattening) {
         /* hy_getRiemannState.F90:367-465: FlatTilde on [lo-2, hi+2] (zero
          * elsewhere), then FlatCoeff on the same range (kHydro = 0) */
@@ -775,6 +795,45 @@ static int riemann_states(const blk_t *b, const double *U, double dt, scratch_t 
                 ? recon_mh(p, d, dt, del[d], S, tr[d], flat, lam + 5 * d, leig[d], reig[d], Wp[d], Wn[d], sig + 9 * d)
                 : recon_ppm(p, d, dt, del[d], S, tr[d], flat, lam + 5 * d, leig[d], reig[d], Wp[d], Wn[d], sig + 9 * d);
             if (err) return 1;
+        }
+        /* hybrid order, hy_dataReconstOneStep.F90:864-913: where the velocity
+         * converges (min of DivU over the cell's (2 k4 + 1)^d box below kappa
+         * times the sound speed), a face state that breaks the density bounds
+         * of a shock (hy_checkRHjumpCond) falls back to first order */
+        if (p->use_hybrid) {
+            const double *u = U + c * FXO_NUNK;
+            double cs = u[FXO_GAMC] * u[FXO_PRES];
+            cs = sqrt(cs / u[FXO_DENS]);
+            const double eps = p->hybrid_kappa * cs;
+            double mn = 0.;
+            int first = 1;
+            for (int kk = k - k4 * b->k3; kk <= k + k4 * b->k3; kk++)
+            for (int jj = j - k4 * b->k2; jj <= j + k4 * b->k2; jj++)
+            for (int ii = i - k4; ii <= i + k4; ii++) {
+                double v = s->divu[cidx(b, ii, jj, kk)];
+                if (first || v < mn) mn = v;
+                first = 0;
+            }
+            if (mn < eps) {
+                const double gamc = u[FXO_GAMC], dens = u[FXO_DENS];
+                const double gr = (gamc + 1.) / (gamc - 1.);
+                double m2 = 0.;
+                for (int e = 0; e < ndim; e++) m2 = m2 + u[FXO_VELX + e] * u[FXO_VELX + e];
+                m2 = m2 * dens / (gamc * u[FXO_PRES]);
+                for (int d = 0; d < ndim; d++) {
+                    int sw = 0;
+                    if (m2 > 1.e-4) {
+                        if (Wn[d][H_D] > gr * dens || gr * Wn[d][H_D] < dens) sw = 1;
+                        if (Wp[d][H_D] > gr * dens || gr * Wp[d][H_D] < dens) sw = 1;
+                    }
+                    if (sw) {
+                        Wp[d][H_D] = dens; Wp[d][H_VX] = u[FXO_VELX]; Wp[d][H_VY] = u[FXO_VELY];
+                        Wp[d][H_VZ] = u[FXO_VELZ]; Wp[d][H_P] = u[FXO_PRES]; Wp[d][H_GC] = gamc;
+                        Wp[d][H_GE] = u[FXO_GAME]; Wp[d][H_EI] = u[FXO_EINT];
+                        for (int v = H_D; v <= H_EI; v++) Wn[d][v] = Wp[d][v];
+                    }
+                }
+            }
         }
         /* transverse contributions, hy_dataReconstOneStep.F90:931-962 */
         if (ndim > 1) {

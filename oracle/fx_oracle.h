@@ -59,6 +59,8 @@ typedef struct {
     int steepening;                 /* use_steepening (PPM contact steepening) */
     int use_avisc;                  /* artificial viscosity (hy_getFaceFlux.F90:397-438) */
     double cvisc;                   /* its constant */
+    int use_hybrid;                 /* use_hybridOrder (hy_dataReconstOneStep.F90:864-913) */
+    double hybrid_kappa;            /* hybridOrderKappa */
 } fxo_params;
 
 /* Number of doubles in one UNK array for the given geometry. */

@@ -44,6 +44,7 @@ class FxoParams(ctypes.Structure):
         ("gas_constant", ctypes.c_double), ("abar", ctypes.c_double),
         ("flattening", ctypes.c_int), ("entropy_fix", ctypes.c_int), ("steepening", ctypes.c_int),
         ("use_avisc", ctypes.c_int), ("cvisc", ctypes.c_double),
+        ("use_hybrid", ctypes.c_int), ("hybrid_kappa", ctypes.c_double),
     ]
 
 
@@ -119,6 +120,8 @@ def make_params(geom, hp):
     p.steepening = int(hp.use_steepening)
     p.use_avisc = int(hp.use_avisc)
     p.cvisc = hp.cvisc
+    p.use_hybrid = int(hp.use_hybridOrder)
+    p.hybrid_kappa = hp.hybridOrderKappa
     return p
 
 

@@ -120,7 +120,7 @@ def test_parameter_validation_mirrors_hydro_init():
     HydroParams(use_upwindTVD=True, use_avisc=True).validate()
     for bad in (dict(order=4), dict(order=6), dict(RiemannSolver="Marquina"), dict(entropyFixMethod="Einfeldt"),
                 dict(slopeLimiter="superbee"),
-                dict(transOrder=3), dict(use_hybridOrder=True),
+                dict(transOrder=3),
                 dict(use_flattening=True, useGravity=True),
                 dict(hydroComputeDtOption=0)):
         with pytest.raises(ValueError):

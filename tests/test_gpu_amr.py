@@ -269,3 +269,11 @@ def test_amr_rejects_artificial_viscosity(need_gpu):
     with pytest.raises(FlashXError) as e:
         HydroDevice(root, hp, "fp64", mesh=mesh)
     assert e.value.code == 6
+
+
+def test_amr_rejects_hybrid_order(need_gpu):
+    root, hp, mesh, unk = _case((BC_PERIODIC,) * 6, 2, order=3)
+    hp.use_hybridOrder = True
+    with pytest.raises(FlashXError) as e:
+        HydroDevice(root, hp, "fp64", mesh=mesh)
+    assert e.value.code == 6
