@@ -32,6 +32,7 @@ import numpy as np  # noqa: E402
 METRIC = "zone-updates/s FP64 vs FP32+FP64-update at stated L1 err; % HBM roofline"
 UNIT = "zone-updates/s"
 BYTES_PER_ZONE = 152   # 9 FP64 reads + 10 FP64 writes per zone-update (algorithmic)
+FLOPS_FILES = {"kh2d": os.path.join(ROOT, "profiles", "hydro2d_kh2048_flops.json")}
 TRAFFIC_FILES = {"kh2d": os.path.join(ROOT, "profiles", "hydro2d_kh2048_traffic.json"),
                  "rt3d": os.path.join(ROOT, "profiles", "hydro3d_rt256_traffic.json")}
 WORKLOADS = {
@@ -276,6 +277,27 @@ def run_reference(args):
         dist.destroy_process_group()
 
 
+def fp_roofline(config, precision, zones_per_s):
+    """Floating-point roofline of the hot kernel from the FP operations per
+    zone-update counted by ncu (profiles/*_flops.json: DADD + DMUL + 2 DFMA,
+    FADD + FMUL + 2 FFMA; divisions and square roots count as the FMA
+    sequences they execute) times the measured zone-update rate, against the
+    nominal FP64 / FP32 peaks (no measured figure exists for them)."""
+    try:
+        with open(FLOPS_FILES[config]) as f:
+            fj = json.load(f)
+    except Exception:
+        return None
+    c, pk = fj[precision], fj["peaks_nominal_tflops"]
+    f64 = c["fp64_flops_per_zone"] * zones_per_s / 1e12
+    f32 = c["fp32_flops_per_zone"] * zones_per_s / 1e12
+    return {"bound": "fp64 pipe" if precision == "fp64" else "fp32 + fp64 pipes",
+            "achieved_fp64": f64, "achieved_fp32": f32, "peak_fp64": pk["fp64"], "peak_fp32": pk["fp32"],
+            "unit": "TFLOP/s", "frac_fp64": f64 / pk["fp64"], "frac_fp32": f32 / pk["fp32"],
+            "fp64_flops_per_zone": c["fp64_flops_per_zone"], "fp32_flops_per_zone": c["fp32_flops_per_zone"],
+            "peak_kind": "nominal"}
+
+
 def regrid_cycle(dev, hp, mesh):
     """One Grid_updateRefinement on the AMR workload after the timed steps
     (not part of the zone-update rate): refinement marks on the device
@@ -442,6 +464,9 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24, "d2h_bytes_per_step": 8,
                     "note": "host loop via fxb_hydro_step/fxb_compute_dt: (t, dt, dtOld) in, dt out per step; "
                             "UNK stays resident on the device"}}
+    flops = fp_roofline(args.config, "fp64", ncell / (kernel_ms / 1e3))
+    if flops:
+        line["roofline_fp"] = flops
     if mesh is not None:
         line["config"]["leaves_per_level"] = mesh.level_counts()
         line["config"]["tuning"] = dev.tuning()
@@ -463,9 +488,12 @@ def run_ours(args):
         mdev.close()
         l1 = {v: float(np.mean(np.abs(m_after[..., i] - ref_after[..., i])) / max(np.mean(np.abs(ref_after[..., i])), 1e-300))
               for v, i in (("dens", 0), ("pres", 5), ("velx", 8), ("vely", 9))}
+        mflops = fp_roofline(args.config, "mixed", ncell * K / (mms / 1e3))
         line["mixed"] = {"value": world * ncell * K / (mms / 1e3), "ms_per_step": mms / K,
                          "speedup_vs_fp64": ms / mms, "l1_rel_vs_fp64_after_steps": l1,
                          "dtype": "f32 reconstruction/Riemann + f64 update", "clocks": mclk}
+        if mflops:
+            line["mixed"]["roofline_fp"] = mflops
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_run(args.config, scale=args.scale / 4 if geom.ndim == 2 else args.scale / 4)
