@@ -110,6 +110,7 @@ struct State {
     std::vector<long> rlist_off;                  // per level offset into d_rlist, size maxlev + 1
     int cta[4] = {4, 4, 4, 4};                    // CTAs per block: sig, slopes, (unused), update
     int fill_cta = 8;
+    bool tuned = false;                           // launch shapes chosen (first attach of the mesh)
     char tune_log[256] = "";
     std::unordered_map<uint64_t, int> map;
 };
@@ -1466,6 +1467,8 @@ int amr_attach(const double *unk_host)
         CKA(cudaGetLastError());
     }
     CKA(cudaStreamSynchronize(S.C.stream));
+    if (S.tuned) return FXB_OK;      // new data on the same mesh keeps the launch shapes
+    S.tuned = true;
     return amr_tune();
 }
 
@@ -1583,6 +1586,7 @@ int amr_regrid(const fxb_block_desc *leaves, int nleaf)
         S.fill_cta = old.fill_cta;
         for (int q = 0; q < 4; q++) S.cta[q] = old.cta[q];
         snprintf(S.tune_log, sizeof(S.tune_log), "%s", old.tune_log);
+        S.tuned = old.tuned;
         return code;
     };
     int rc = amr_create(old.C, leaves, nleaf);
@@ -1638,6 +1642,7 @@ int amr_regrid(const fxb_block_desc *leaves, int nleaf)
     S.fill_cta = old.fill_cta;
     for (int q = 0; q < 4; q++) S.cta[q] = old.cta[q];
     snprintf(S.tune_log, sizeof(S.tune_log), "%s", old.tune_log);
+    S.tuned = old.tuned;
     return rc;
 }
 

@@ -257,8 +257,9 @@ int fxb_last_timing(double *ms, int *kernel_launches);
 void *fxb_stream(void);
 /* The kernel launch shape in use, as text (no reference counterpart: the
  * batched-block path picks its CTAs per block for each stage by timing 1, 2,
- * 4, 8 and 16 at fxb_attach_unk; FXB_AMR_TUNE=0 in the environment keeps the
- * defaults).  The choice changes timings, never results. */
+ * 4, 8 and 16 at the first fxb_attach_unk of a registered mesh, and keeps
+ * them for later attaches and regrids; FXB_AMR_TUNE=0 in the environment
+ * keeps the defaults).  The choice changes timings, never results. */
 int fxb_tuning(char *buf, int len);
 int fxb_last_error(fxb_error *err);
 void fxb_finalize(void);
