@@ -330,7 +330,8 @@ def regrid_cycle(dev, hp, mesh):
     """One Grid_updateRefinement on the AMR workload after the timed steps
     (not part of the zone-update rate): refinement marks on the device
     (density criterion of the workload, Paramesh4 defaults refine_cutoff 0.8,
-    derefine_cutoff 0.2, refine_filter 0.01), the tree update on the host,
+    derefine_cutoff 0.2, refine_filter 0.01), the tree update on the host
+    (fxb_refine_derefine),
     the data movement on the device (fxb_regrid), then two steps on the new
     mesh.  Host wall time of each part, with the device synchronised."""
     import torch
@@ -339,7 +340,7 @@ def regrid_cycle(dev, hp, mesh):
     t0 = time.perf_counter()
     flags, _ = dev.Grid_markRefineDerefine([("dens", 0.8, 0.2, 0.01)], maxlev)
     t1 = time.perf_counter()
-    from flashx_b200.amr import refine_derefine
+    from flashx_b200.hydro import refine_derefine
     new = refine_derefine(dev.mesh, flags, 1, maxlev)
     t2 = time.perf_counter()
     from flashx_b200.hydro import _check, mesh_blocks

@@ -11,6 +11,12 @@
 #include <string.h>
 #include <math.h>
 
+#include <algorithm>
+#include <array>
+#include <unordered_map>
+#include <unordered_set>
+#include <vector>
+
 using namespace fxb;
 
 namespace {
@@ -869,6 +875,167 @@ extern "C" int fxb_mark_refine_derefine(int nvars, const int *refine_var, const 
                              error);
     if (rc) return rc;
     return check_err_word();
+}
+
+// ---- PARAMESH's tree update (host only) -----------------------------------------
+namespace {
+uint64_t tree_key(int lev, const int c[3])
+{
+    return ((uint64_t)lev << 60) | ((uint64_t)(uint32_t)c[0] << 40) | ((uint64_t)(uint32_t)c[1] << 20) |
+           (uint64_t)(uint32_t)c[2];
+}
+// Morton key of a block scaled to level maxlev: bits of x, y, z interleaved
+uint64_t morton(int lev, const int c[3], int maxlev)
+{
+    const int sh = maxlev - lev;
+    uint64_t x = (uint64_t)c[0] << sh, y = (uint64_t)c[1] << sh, z = (uint64_t)c[2] << sh, k = 0;
+    for (int b = 0; b < 21; b++)
+        k |= ((x >> b) & 1) << (3 * b) | ((y >> b) & 1) << (3 * b + 1) | ((z >> b) & 1) << (3 * b + 2);
+    return k;
+}
+} // namespace
+
+extern "C" int fxb_refine_derefine(const fxb_domain *dom, const fxb_block_desc *leaves, int n, const int *flags,
+                                   int lrefine_min, int lrefine_max, fxb_block_desc *out, int cap, int *nout)
+{
+    if (!dom || !leaves || n <= 0 || !flags || !nout || (cap > 0 && !out))
+        return fail(FXB_EARG, "fxb_refine_derefine: bad argument");
+    if (dom->ndim != 2 && dom->ndim != 3) return fail(FXB_EARG, "fxb_refine_derefine: ndim must be 2 or 3");
+    if (lrefine_min < 1 || lrefine_max < lrefine_min || lrefine_max > 15)
+        return fail(FXB_EARG, "fxb_refine_derefine: bad lrefine_min / lrefine_max");
+    const int ndim = dom->ndim, nch = ndim == 3 ? 8 : 4;
+    const int nb0[3] = {dom->nblockx, ndim >= 2 ? dom->nblocky : 1, ndim == 3 ? dom->nblockz : 1};
+    auto nb_at = [&](int lev, int d) { return d < ndim ? nb0[d] << (lev - 1) : 1; };
+    std::unordered_map<uint64_t, int> leaf;
+    std::unordered_set<uint64_t> parent;
+    for (int l = 0; l < n; l++) {
+        const fxb_block_desc &B = leaves[l];
+        if (B.level < 1 || B.level > 15) return fail(FXB_EARG, "fxb_refine_derefine: level out of range");
+        for (int d = 0; d < 3; d++)
+            if (B.bcoord[d] < 0 || B.bcoord[d] >= nb_at(B.level, d))
+                return fail(FXB_EARG, "fxb_refine_derefine: block coordinate out of range");
+        if (!leaf.emplace(tree_key(B.level, B.bcoord), l).second) return fail(FXB_EARG, "fxb_refine_derefine: duplicate leaf");
+        int c[3] = {B.bcoord[0], B.bcoord[1], B.bcoord[2]};
+        for (int lev = B.level - 1; lev >= 1; lev--) {
+            for (int d = 0; d < 3; d++) c[d] /= 2;
+            parent.insert(tree_key(lev, c));
+        }
+    }
+    // the leaf covering position p of level lev (itself or a coarser ancestor), or -1
+    auto covering = [&](int lev, const int p[3]) {
+        int c[3] = {p[0], p[1], p[2]};
+        for (int L = lev; L >= 1; L--) {
+            auto it = leaf.find(tree_key(L, c));
+            if (it != leaf.end()) return it->second;
+            for (int d = 0; d < 3; d++) c[d] /= 2;
+        }
+        return -1;
+    };
+    // neighbours across faces, edges and corners, wrapped on periodic axes
+    auto neighbours = [&](int lev, const int c[3], std::vector<std::array<int, 3>> &v) {
+        v.clear();
+        const int K3 = ndim == 3 ? 1 : 0;
+        for (int k = -K3; k <= K3; k++) for (int j = -1; j <= 1; j++) for (int i = -1; i <= 1; i++) {
+            if (!(i | j | k)) continue;
+            std::array<int, 3> p = {c[0] + i, c[1] + j, c[2] + k};
+            bool ok = true;
+            for (int d = 0; d < ndim && ok; d++) {
+                const int nb = nb_at(lev, d);
+                if (p[d] < 0 || p[d] >= nb) {
+                    if (dom->bc[2 * d + (p[d] >= nb)] != FXB_BC_PERIODIC) ok = false;
+                    else p[d] = (p[d] + nb) % nb;
+                }
+            }
+            if (ok) v.push_back(p);
+        }
+    };
+    // level limits, mpi_amr_refine_derefine.F90:157-163
+    std::vector<char> ref(n), deref(n);
+    for (int l = 0; l < n; l++) {
+        ref[l] = flags[l] == 1;
+        deref[l] = flags[l] == -1;
+        if (leaves[l].level >= lrefine_max) ref[l] = 0;
+        if (leaves[l].level == lrefine_min) deref[l] = 0;
+        if (leaves[l].level < lrefine_min) ref[l] = 1;
+    }
+    // amr_check_refine: a leaf one level coarser than a refining neighbour refines too
+    std::vector<std::array<int, 3>> nbrs;
+    for (bool changed = true; changed;) {
+        changed = false;
+        for (int l = 0; l < n; l++) {
+            if (!ref[l]) continue;
+            neighbours(leaves[l].level, leaves[l].bcoord, nbrs);
+            for (auto &p : nbrs) {
+                const int cv = covering(leaves[l].level, p.data());
+                if (cv >= 0 && leaves[cv].level < leaves[l].level && !ref[cv]) {
+                    ref[cv] = 1;
+                    deref[cv] = 0;
+                    changed = true;
+                }
+            }
+        }
+    }
+    // amr_check_derefine: no root blocks, no same-level neighbour that is a
+    // parent or refines, all siblings derefining
+    std::unordered_map<uint64_t, int> group;
+    std::vector<char> grouped(n, 0);
+    for (int l = 0; l < n; l++) {
+        const int lev = leaves[l].level;
+        if (!deref[l] || ref[l] || lev == 1) continue;
+        neighbours(lev, leaves[l].bcoord, nbrs);
+        bool blocked = false;
+        for (auto &p : nbrs) {
+            const uint64_t k = tree_key(lev, p.data());
+            auto it = leaf.find(k);
+            blocked = it != leaf.end() ? (bool)ref[it->second] : parent.count(k) > 0;
+            if (blocked) break;
+        }
+        if (blocked) continue;
+        grouped[l] = 1;
+        const int pc[3] = {leaves[l].bcoord[0] / 2, leaves[l].bcoord[1] / 2, leaves[l].bcoord[2] / 2};
+        group[tree_key(lev - 1, pc)]++;
+    }
+    std::vector<fxb_block_desc> res;
+    std::unordered_set<uint64_t> added;
+    for (int l = 0; l < n; l++) {
+        const fxb_block_desc &B = leaves[l];
+        if (ref[l]) {
+            for (int q = 0; q < nch; q++) {
+                fxb_block_desc C;
+                C.level = B.level + 1;
+                C.bcoord[0] = 2 * B.bcoord[0] + (q & 1);
+                C.bcoord[1] = 2 * B.bcoord[1] + ((q >> 1) & 1);
+                C.bcoord[2] = ndim == 3 ? 2 * B.bcoord[2] + ((q >> 2) & 1) : 0;
+                res.push_back(C);
+            }
+            continue;
+        }
+        if (grouped[l]) {
+            const int pc[3] = {B.bcoord[0] / 2, B.bcoord[1] / 2, B.bcoord[2] / 2};
+            const uint64_t pk = tree_key(B.level - 1, pc);
+            if (group[pk] == nch) {
+                if (added.insert(pk).second) {
+                    fxb_block_desc P;
+                    P.level = B.level - 1;
+                    for (int d = 0; d < 3; d++) P.bcoord[d] = pc[d];
+                    res.push_back(P);
+                }
+                continue;
+            }
+        }
+        res.push_back(B);
+    }
+    // PARAMESH's Morton order (finest-level scaled key, then level)
+    int maxlev = 1;
+    for (auto &B : res) maxlev = std::max(maxlev, B.level);
+    std::sort(res.begin(), res.end(), [&](const fxb_block_desc &a, const fxb_block_desc &b) {
+        const uint64_t ka = morton(a.level, a.bcoord, maxlev), kb = morton(b.level, b.bcoord, maxlev);
+        return ka != kb ? ka < kb : a.level < b.level;
+    });
+    *nout = (int)res.size();
+    if ((int)res.size() > cap) return fail(FXB_EARG, "fxb_refine_derefine: output list too small (see *nout)");
+    std::copy(res.begin(), res.end(), out);
+    return FXB_OK;
 }
 
 extern "C" int fxb_regrid(const fxb_block_desc *blocks, int nblk)

@@ -31,7 +31,8 @@ ABI_SYMBOLS = ("fxb_init", "fxb_register_blocks", "fxb_attach_unk", "fxb_fill_gu
                "fxb_hydro_step", "fxb_compute_dt", "fxb_advance", "fxb_eos", "fxb_sync_to_host",
                "fxb_sync_from_host", "fxb_integrals", "fxb_integrals_noalloc", "fxb_mark_refine_derefine",
                "fxb_last_timing", "fxb_stream", "fxb_tuning", "fxb_last_error", "fxb_finalize",
-               "fxb_init_slab", "fxb_halo_doubles", "fxb_halo_pack", "fxb_halo_unpack", "fxb_regrid")
+               "fxb_init_slab", "fxb_halo_doubles", "fxb_halo_pack", "fxb_halo_unpack", "fxb_regrid",
+               "fxb_refine_derefine")
 
 
 class FxbParams(ctypes.Structure):
@@ -116,6 +117,9 @@ def load_library(path=LIB_PATH):
     L.fxb_halo_pack.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
     L.fxb_halo_unpack.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     L.fxb_regrid.argtypes = [ctypes.POINTER(FxbBlockDesc), ctypes.c_int]
+    L.fxb_refine_derefine.argtypes = [ctypes.POINTER(FxbDomain), ctypes.POINTER(FxbBlockDesc), ctypes.c_int,
+                                      ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
+                                      ctypes.POINTER(FxbBlockDesc), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     for name in ABI_SYMBOLS:
         if name not in ("fxb_stream", "fxb_finalize", "fxb_halo_doubles"):
             getattr(L, name).restype = ctypes.c_int
@@ -216,6 +220,24 @@ def mesh_blocks(levels, bcoords):
         arr[b].level = int(levels[b])
         arr[b].bcoord[0], arr[b].bcoord[1], arr[b].bcoord[2] = (int(v) for v in bcoords[b])
     return arr
+
+
+def refine_derefine(mesh, flags, lrefine_min=1, lrefine_max=None):
+    """PARAMESH's tree update in the library (fxb_refine_derefine, host
+    code): the new AmrMesh of `mesh` for leaf marks `flags` (mesh order)."""
+    from .amr import AmrMesh
+    lib = load_library()
+    lmax = lrefine_max if lrefine_max is not None else mesh.maxlev + 1
+    blocks = mesh_blocks(mesh.levels, mesh.bcoords)
+    fl = (ctypes.c_int * mesh.nleaf)(*[int(f) for f in flags])
+    cap = mesh.nleaf * (8 if mesh.geom.ndim == 3 else 4)
+    out = (FxbBlockDesc * cap)()
+    n = ctypes.c_int()
+    d = make_fxb_domain(mesh.geom)
+    _check(lib.fxb_refine_derefine(ctypes.byref(d), blocks, mesh.nleaf, fl, int(lrefine_min), int(lmax), out, cap,
+                                   ctypes.byref(n)))
+    return AmrMesh(mesh.geom, [(out[i].level, (out[i].bcoord[0], out[i].bcoord[1], out[i].bcoord[2]))
+                               for i in range(n.value)])
 
 
 class HydroDevice:
@@ -365,11 +387,10 @@ class HydroDevice:
 
     def Grid_updateRefinement(self, flags, lrefine_min=1, lrefine_max=None):
         """Grid_updateRefinement after Grid_markRefineDerefine: the tree update
-        (PARAMESH's amr_refine_derefine, restated in flashx_b200.amr) on the
-        host, then the data movement on the device (fxb_regrid).  Returns the
-        new AmrMesh; the host UNK must then have its shape (`unk_shape`) for
+        (PARAMESH's amr_refine_derefine, fxb_refine_derefine on the host),
+        then the data movement on the device (fxb_regrid).  Returns the new
+        AmrMesh; the host UNK must then have its shape (`unk_shape`) for
         sync_to_host."""
-        from .amr import refine_derefine
         if self.mesh is None:
             raise ValueError("Grid_updateRefinement needs an AMR mesh")
         new = refine_derefine(self.mesh, flags, lrefine_min, lrefine_max)

@@ -234,6 +234,20 @@ int fxb_mark_refine_derefine(int nvars, const int *refine_var, const double *ref
  * change); the old mesh and its data are then kept.  FXB_EUNSUPPORTED on a
  * uniform grid. */
 int fxb_regrid(const fxb_block_desc *blocks, int nblk);
+/* PARAMESH's tree update (PM4_package/source/mpi_amr_refine_derefine.F90:157-240,
+ * amr_check_refine.F90, mpi_amr_check_derefine.F90), host only, for callers
+ * without PARAMESH: from the leaves (any order) and their marks flags[n]
+ * (1 refine, -1 derefine, 0 neither, as fxb_mark_refine_derefine returns
+ * them), the new leaf list in PARAMESH's Morton order.  Level limits first
+ * (no refinement at lrefine_max, no derefinement at lrefine_min, refinement
+ * below it); a leaf one level coarser than a refining neighbour, across
+ * faces, edges and corners (periodic axes wrapped), refines too; a leaf
+ * derefines only if it is not a root block, no same-level neighbour is a
+ * parent or refines, and all its siblings derefine, whereupon the siblings
+ * become their parent.  out[cap] receives the list and *nout its length
+ * (FXB_EARG with *nout set when cap is too small). */
+int fxb_refine_derefine(const fxb_domain *domain, const fxb_block_desc *leaves, int n, const int *flags,
+                        int lrefine_min, int lrefine_max, fxb_block_desc *out, int cap, int *nout);
 /* Volume integrals of caller-owned device arrays without allocating any
  * device memory (no counterpart in the reference: an addition of this
  * library).  For callers that cannot call cudaMalloc, e.g. a Fortran code

@@ -159,3 +159,20 @@ def test_oracle_regrid_rejects_two_levels(oracle):
     m2 = A.build_mesh(g, 3, lambda lev, c, gg: c == (1, 1, 1) or (lev == 2 and c == (2, 2, 2)))
     with pytest.raises(RuntimeError):
         oracle.Amr(p, m.levels, m.bcoords).regrid(unk, oracle.Amr(p, m2.levels, m2.bcoords))
+
+
+@pytest.mark.parametrize("ndim,bc", [(3, BC_PERIODIC), (3, BC_OUTFLOW), (2, BC_PERIODIC), (2, BC_OUTFLOW)])
+def test_library_tree_update_matches_the_restatement(ndim, bc):
+    """fxb_refine_derefine (C++, host only) returns the same leaves, in the
+    same Morton order, as amr.refine_derefine for random marks."""
+    from flashx_b200.hydro import refine_derefine as native
+    rng = np.random.default_rng(11 + ndim)
+    g = Geometry(ndim, 8, 8, 8 if ndim == 3 else 1, 3, 2, 2 if ndim == 3 else 1, bc=(bc,) * 6)
+    m = A.build_mesh(g, 3, lambda lev, c, gg: (c[0] + 2 * c[1] + c[2]) % 3 == 0)
+    for _ in range(5):
+        flags = rng.choice([-1, 0, 1], size=m.nleaf, p=[0.45, 0.35, 0.2])
+        for lmin, lmax in ((1, 4), (2, 3)):
+            a = A.refine_derefine(m, flags, lmin, lmax)
+            b = native(m, flags, lmin, lmax)
+            assert np.array_equal(a.levels, b.levels) and np.array_equal(a.bcoords, b.bcoords)
+        m = A.refine_derefine(m, flags, 1, 4)
