@@ -414,7 +414,6 @@ extern "C" int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
         return fail(FXB_EUNSUPPORTED, "fxb_init: RiemannSolver must be Roe, LLF, HLL or HLLC");
     if (p.limiter < 1 || p.limiter > 5) return fail(FXB_EARG, "fxb_init: unknown slope limiter");
     if (p.precision != FXB_FP64 && p.precision != FXB_MIXED) return fail(FXB_EARG, "fxb_init: unknown precision");
-    if (d.ndim == 2 && p.use_gravity) return fail(FXB_EUNSUPPORTED, "fxb_init: gravity is implemented for 3-D only");
     if (p.flattening && p.use_gravity) return fail(FXB_EUNSUPPORTED, "fxb_init: use_flattening with gravity is not implemented");
     if (p.entropy_fix < 0 || p.entropy_fix > 2) return fail(FXB_EARG, "fxb_init: unknown entropyFixMethod");
     // unsplit/Hydro_init.F90:137: use_upwindTVD only acts with more than four guard cells

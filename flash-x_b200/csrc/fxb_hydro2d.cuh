@@ -167,7 +167,7 @@ template <class R> __device__ __forceinline__ R divu2d(const Args2D &a, const Sm
 // fallback (:1131-1165); stores global-order Wp/Wm into s.W[.][t].
 template <class R, bool EXT>
 __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int dir, int t, int wx, int wy,
-                                             int dbi, int dbstep, R dtn, R hdtn, R hdtt)
+                                             int dbi, int dbstep, R dtn, R hdtn, R hdtt, R hdt)
 {
     const int ox = dir == 0, oy = dir == 1;
     R g[6], Vm[6], Vc[6], Vp[6], vecL[6], vecR[6], Wm[6], Wp[6];
@@ -251,6 +251,17 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
         win6(s, wx, wy, g);
 #pragma unroll
         for (int k = 0; k < 6; k++) { Wm[k] = g[k]; Wp[k] = g[k]; }
+    }
+    if (EXT && a.prm.use_gravity) {   // hy_getRiemannState.F90:843-885, global axes after unrot
+        R gl, gr;
+        gravity_faces(a.prm, R(a.prm.grav[dir]), gl, gr);
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            R gp = q == dir ? gr : R(a.prm.grav[q]);
+            R gn = q == dir ? gl : R(a.prm.grav[q]);
+            Wp[1 + q] = Wp[1 + q] + hdt * gp;
+            Wm[1 + q] = Wm[1 + q] + hdt * gn;
+        }
     }
 #pragma unroll
     for (int k = 0; k < 6; k++) { s.W[k][t] = Wp[k]; s.W[6 + k][t] = Wm[k]; }
@@ -364,7 +375,7 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
     // ---- C: x face states
     for (int t = tid; t < NW; t += NT2) {
         int ii = t % (T2 + 2) - 1, jj = t / (T2 + 2);
-        states_stage<R, EXT>(a, s, 0, t, ii + 3, jj + 3, jj * (T2 + 4) + ii + 2, 1, dtnx, hdtnx, hdty);
+        states_stage<R, EXT>(a, s, 0, t, ii + 3, jj + 3, jj * (T2 + 4) + ii + 2, 1, dtnx, hdtnx, hdty, R(0.5 * dt));
     }
     __syncthreads();
     // ---- D: x faces
@@ -410,7 +421,7 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
     // ---- G: y face states
     for (int t = tid; t < NW; t += NT2) {
         int ii = t % T2, jj = t / T2 - 1;
-        states_stage<R, EXT>(a, s, 1, t, ii + 3, jj + 3, (jj + 2) * T2 + ii, T2, dtny, hdtny, hdtx);
+        states_stage<R, EXT>(a, s, 1, t, ii + 3, jj + 3, (jj + 2) * T2 + ii, T2, dtny, hdtny, hdtx, R(0.5 * dt));
     }
     __syncthreads();
     // ---- H: y faces
@@ -441,14 +452,32 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
             inten = inten + dt * 0.0;
         }
         const double Sph[5] = {0., SphX, SphY, 0., 0.};
-        double momOld[3] = {U0[1], U0[2], U0[3]};
-        (void)momOld;
 #pragma unroll
         for (int v = 0; v < 5; v++) U0[v] = U0[v] + dt * (0. + Sph[v]);
+        if (EXT && prm.use_gravity) {   // hy_unsplitUpdate.F90:1234-1245, from the step's old momentum
+            double vold[3];
+#pragma unroll
+            for (int q = 0; q < 3; q++)
+                vold[q] = KeepOwn<R>::value ? s.OWN[KeepOwn<R>::value ? 2 + q : 0][tid]
+                                            : (double)s.V[VX + q][oj + 3][oi + 3];
+            const double momOld[3] = {vold[0] * dens0, vold[1] * dens0, vold[2] * dens0};
+            for (int q = 0; q < 3; q++) U0[1 + q] = U0[1 + q] + 0.5 * dt * dens0 * prm.grav[q];
+            double dp = 0.;
+            for (int q = 0; q < 3; q++) dp = dp + momOld[q] * prm.grav[q];
+            U0[4] = U0[4] + 0.5 * dt * dp;
+        }
         double dens = fmax2(U0[0], prm.small_dens);
         double vx = U0[1] / dens, vy = U0[2] / dens, vz = U0[3] / dens;
         double ener = U0[4] / dens;
         double eint = prm.use_aux_eint ? inten / dens : eint0;
+        if (EXT && prm.use_gravity) {   // hy_gravityStepBlk -> hy_addGravity: the n+1 half step
+            const double hdt = 0.5 * dt;
+            double vn[3] = {vx + hdt * prm.grav[0], vy + hdt * prm.grav[1], vz + hdt * prm.grav[2]};
+            double dp = 0.;
+            for (int q = 0; q < 3; q++) dp = dp + vn[q] * prm.grav[q];
+            ener = ener + hdt * dp;
+            vx = vn[0]; vy = vn[1]; vz = vn[2];
+        }
         // hy_energyFix.F90:240-260
         double ekin = vx * vx; ekin = ekin + vy * vy; ekin = ekin + vz * vz; ekin = 0.5 * ekin;
         double ee = ener - ekin - 0.0;

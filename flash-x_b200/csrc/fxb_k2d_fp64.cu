@@ -12,7 +12,7 @@ cudaError_t setup_hydro2d_fp64()
 void launch_hydro2d_fp64(const Args2D &a, dim3 grid, cudaStream_t s)
 {
     if (a.prm.flattening) flat2d_kernel<double><<<148 * 8, 256, 0, s>>>(a, (double *)a.flat);
-    if (extended_options(a.prm))   // Roe, contact steepening, MUSCL-Hancock: their own instantiation
+    if (extended_options(a.prm) || a.prm.use_gravity)   // Roe, contact steepening, MUSCL-Hancock, 2-D gravity: their own instantiation
         hydro2d_kernel<double, true><<<grid, Threads2D<double>::value, sizeof(Smem2D<double>), s>>>(a);
     else
         hydro2d_kernel<double, false><<<grid, Threads2D<double>::value, sizeof(Smem2D<double>), s>>>(a);

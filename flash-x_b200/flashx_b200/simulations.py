@@ -174,8 +174,23 @@ def kelvin_helmholtz(geom: Geometry, hp: HydroParams, amp=0.01):
 def rayleigh_taylor(geom: Geometry, hp: HydroParams, g=-0.1, p0=2.5, amp=0.01, nmodes=16):
     """Heavy (rho=2) over light (rho=1) fluid at z=0.5 in hydrostatic balance
     under constant gravity g in z; vz = amp * sum of nmodes random-phase
-    Fourier modes times a Gaussian envelope around the interface."""
+    Fourier modes times a Gaussian envelope around the interface.  In 2-D the
+    vertical axis is y (interface at y=0.5, vy perturbed by modes in x)."""
     xc, yc, zc, _, _ = cell_coords(geom)
+    if geom.ndim == 2:
+        Zc, Y, X = np.meshgrid(zc, yc, xc, indexing="ij")
+        heavy = Y > 0.5
+        rho = np.where(heavy, 2.0, 1.0)
+        p = np.where(heavy, p0 + 2.0 * g * (Y - 0.5), p0 + 1.0 * g * (Y - 0.5))
+        a, _ = uniform01(np.arange(nmodes, dtype=np.uint64), stream=1)
+        c, _ = uniform01(np.arange(nmodes, dtype=np.uint64), stream=2)
+        kx = 1.0 + np.floor(4.0 * a)
+        s = np.zeros_like(X)
+        for m in range(nmodes):
+            s += np.sin(2.0 * math.pi * kx[m] * X + 2.0 * math.pi * c[m])
+        vy = amp * s * np.exp(-((Y - 0.5) / 0.1) ** 2)
+        zero = np.zeros_like(rho)
+        return scatter_global(geom, _finish(hp, rho, zero, vy, zero, p))
     Z, Y, X = np.meshgrid(zc, yc, xc, indexing="ij")
     heavy = Z > 0.5
     rho = np.where(heavy, 2.0, 1.0)
@@ -232,6 +247,12 @@ def config(name, scale=1):
         geom = Geometry(3, 16, 16, 16, nb, nb, nb,
                         bc=(BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_PERIODIC, BC_REFLECTING, BC_REFLECTING))
         hp = HydroParams(order=5, useGravity=True, gravity=(0.0, 0.0, -0.1))
+        return geom, hp, rayleigh_taylor
+    if name == "rt2d":
+        nb = max(1, int(16 * scale))
+        geom = Geometry(2, 16, 16, 1, nb, nb, 1,
+                        bc=(BC_PERIODIC, BC_PERIODIC, BC_REFLECTING, BC_REFLECTING, BC_OUTFLOW, BC_OUTFLOW))
+        hp = HydroParams(useGravity=True, gravity=(0.0, -0.1, 0.0))
         return geom, hp, rayleigh_taylor
     if name == "sweep3d":
         nb = max(1, int(4 * scale))

@@ -100,6 +100,22 @@ def test_slab_validation_codes():
     lib.fxb_finalize()
 
 
+def test_gravity_validation_2d_and_3d():
+    """Constant gravity passes the argument checks on 2-D and 3-D grids; only
+    its combination with flattening is refused (FXB_EUNSUPPORTED)."""
+    lib = H.load_library()
+    for geom, g in ((Geometry(2, 16, 16, 1, 2, 2, 1), (0.0, -0.1, 0.0)),
+                    (Geometry(3, 16, 16, 16, 1, 1, 2), (0.0, 0.0, -0.1))):
+        rc, p, d = _init(HydroParams(useGravity=True, gravity=g), geom)
+        assert rc in (H.FXB_OK, H.FXB_ECUDA)
+        p.flattening = 1
+        assert lib.fxb_init(ctypes.byref(p), ctypes.byref(d), H.default_var_map(), 11) == H.FXB_EUNSUPPORTED
+        err = H.FxbError()
+        lib.fxb_last_error(ctypes.byref(err))
+        assert b"gravity" in err.message
+    lib.fxb_finalize()
+
+
 def test_calls_before_init_are_rejected():
     lib = H.load_library()
     lib.fxb_finalize()
