@@ -1164,7 +1164,6 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     if (D.ndim != 3) return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: AMR meshes are implemented for 3-D");
     if (D.nxb != D.nyb || D.nxb != D.nzb || D.nxb % 2 || D.nxb < D.nguard)
         return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: AMR blocks must be cubes of an even size >= NGUARD");
-    if (c.prm.use_gravity) return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: gravity is not implemented on AMR meshes");
     if (c.prm.use_avisc)
         return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: artificial viscosity is implemented for uniform grids");
     if (c.prm.hybrid_order)

@@ -150,7 +150,7 @@ int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
  * (Paramesh4/Grid_fillGuardCells.F90:446-541, levelFlux/Hydro.F90:161-270,
  * levelFlux/Grid_conserveFluxes.F90).  Errors: FXB_EARG for a list that does
  * not tile the domain or is not balanced, FXB_EUNSUPPORTED for 2-D AMR,
- * non-cubic blocks or gravity on AMR meshes. */
+ * non-cubic blocks, artificial viscosity or hybrid order on AMR meshes. */
 int fxb_register_blocks(const fxb_block_desc *blocks, int nblk);
 /* Copy the host UNK (all blocks, guard cells included) into the device mirror. */
 int fxb_attach_unk(const double *unk_host);

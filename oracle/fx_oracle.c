@@ -1082,6 +1082,26 @@ static void unsplit_update(const blk_t *b, double *U, double dt, scratch_t *s)
 }
 
 /* hy_energyFix.F90:240-260 on the block interior. */
+/* hy_gravityStep -> hy_gravityStepBlk.F90:54-78 -> hy_addGravity for constant
+ * gravity: the n+1 half step v += dt/2 g, E += dt/2 v.g on the interior of one
+ * block.  With gravity, energyFix and Eos come after it (hy_updateSolution.F90
+ * defers them under GRAVITY), on uniform grids and AMR meshes alike. */
+static void gravity_step_block(const blk_t *b, double *U, double dt)
+{
+    const fxo_params *p = b->p;
+    for (int k = b->k0; k <= b->kmax; k++)
+    for (int j = b->j0; j <= b->jmax; j++)
+    for (int i = b->i0; i <= b->imax; i++) {
+        double *u = U + cidx(b, i, j, k) * FXO_NUNK;
+        double vold[3] = {u[FXO_VELX], u[FXO_VELY], u[FXO_VELZ]};
+        double hdt = 0.5 * dt;
+        double dp = 0.;
+        for (int d = 0; d < 3; d++) u[FXO_VELX + d] = vold[d] + hdt * p->grav[d];
+        for (int d = 0; d < 3; d++) dp = dp + u[FXO_VELX + d] * p->grav[d];
+        u[FXO_ENER] = u[FXO_ENER] + hdt * dp;
+    }
+}
+
 static void energy_fix(const blk_t *b, double *U)
 {
     const fxo_params *p = b->p;
@@ -1278,17 +1298,7 @@ int fxo_hydro_step(const fxo_params *p, double *unk, double dt, double dt_old, i
         /* hy_gravityStepBlk: the n+1 gravity half step, then energyFix and Eos */
         for (long blk = 0; blk < nblk; blk++) {
             double *U = unk + blk * b.ncell * FXO_NUNK;
-            for (int k = b.k0; k <= b.kmax; k++)
-            for (int j = b.j0; j <= b.jmax; j++)
-            for (int i = b.i0; i <= b.imax; i++) {
-                double *u = U + cidx(&b, i, j, k) * FXO_NUNK;
-                double vold[3] = {u[FXO_VELX], u[FXO_VELY], u[FXO_VELZ]};
-                double hdt = 0.5 * dt;
-                double dp = 0.;
-                for (int d = 0; d < 3; d++) u[FXO_VELX + d] = vold[d] + hdt * p->grav[d];
-                for (int d = 0; d < 3; d++) dp = dp + u[FXO_VELX + d] * p->grav[d];
-                u[FXO_ENER] = u[FXO_ENER] + hdt * dp;
-            }
+            gravity_step_block(&b, U, dt);
             energy_fix(&b, U);
             eos_block(&b, U);
         }

@@ -17,8 +17,8 @@ from flashx_b200.params import (BC_OUTFLOW, BC_PERIODIC, BC_REFLECTING, DENS, EI
                                 Geometry, HydroParams, PRES, TEMP, VELX, VELY, VELZ)
 
 
-def _uniform_level_case(O, ndim, bc, order, steps=2):
-    hp = HydroParams(order=order)
+def _uniform_level_case(O, ndim, bc, order, steps=2, grav=None):
+    hp = HydroParams(order=order) if grav is None else HydroParams(order=order, useGravity=True, gravity=grav)
     nz = 8 if ndim == 3 else 1
     root = Geometry(ndim, 8, 8, nz, 2, 2, 2 if ndim == 3 else 1, bc=bc)
     fine = Geometry(ndim, 8, 8, nz, 4, 4, 4 if ndim == 3 else 1, bc=bc)
@@ -47,6 +47,41 @@ def _uniform_level_case(O, ndim, bc, order, steps=2):
 ])
 def test_uniform_level_mesh_equals_uniform_grid(oracle, ndim, bc, order):
     _uniform_level_case(oracle, ndim, bc, order)
+
+
+@pytest.mark.parametrize("ndim,order", [(2, 3), (3, 5), (3, 2)])
+def test_gravity_on_amr_meshes(oracle, ndim, order):
+    """Constant gravity on AMR meshes: hy_gravityStep's n+1 half step runs on
+    every leaf after the flux-corrected update, before energyFix and Eos
+    (hy_updateSolution.F90 defers them under GRAVITY).  A single-level mesh
+    reproduces the uniform grid bit for bit, and a uniform gas on a mesh of
+    three levels falls freely (v = n dt g, rho and p unchanged)."""
+    refl = (BC_PERIODIC,) * 2 + (BC_REFLECTING,) * 2 + (0, 0) if ndim == 2 else \
+        (BC_PERIODIC,) * 4 + (BC_REFLECTING,) * 2
+    g = (0.02, -0.1, 0.0) if ndim == 2 else (0.02, 0.01, -0.1)
+    _uniform_level_case(oracle, ndim, refl, order, grav=g)
+
+    hp = HydroParams(order=order, useGravity=True, gravity=g)
+    nz = 8 if ndim == 3 else 1
+    root = Geometry(ndim, 8, 8, nz, 4, 4, 4 if ndim == 3 else 1, bc=(BC_PERIODIC,) * 6)
+    mesh = A.build_mesh(root, 3, lambda l, c, gm: (l == 1 and c[0] in (1, 2) and c[1] == 1) or
+                        (l == 2 and c[0] == 3 and c[1] == 3))
+    assert len(set(mesh.levels)) == 3
+
+    def fields(X, Y, Z):
+        one = np.ones_like(X)
+        return 1.3 * one, 0.0 * one, 0.0 * one, 0.0 * one, 0.7 * one
+    unk = A.fill_leaves(mesh, hp, fields)
+    am = oracle.Amr(oracle.make_params(root.as_dict(), hp), mesh.levels, mesh.bcoords)
+    dt = 0.5 * am.compute_dt(unk)
+    for _ in range(3):
+        am.hydro_step(unk, dt)
+    ng = root.nguard
+    inner = unk[:, ng:-ng, ng:-ng, ng:-ng, :] if ndim == 3 else unk[:, :, ng:-ng, ng:-ng, :]
+    for q, v in enumerate((VELX, VELY, VELZ)):
+        assert np.allclose(inner[..., v], 3 * dt * g[q], rtol=1e-12, atol=1e-15)
+    assert np.max(np.abs(inner[..., DENS] - 1.3)) < 1e-13
+    assert np.max(np.abs(inner[..., PRES] - 0.7)) < 1e-12
 
 
 def test_tree_validation(oracle):
