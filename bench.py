@@ -99,6 +99,8 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0, help="block count per axis relative to the config")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=500,
+                    help="steps of the mixed-vs-FP64 L1 and conservation-drift leg (0: skip)")
     ap.add_argument("--sweep", action="store_true",
                     help="throughput sweep of the batched-block path: one JSON line per (block size, count, "
                          "reconstruction, precision)")
@@ -207,8 +209,9 @@ def cpu_baseline_amr(seconds=10.0):
 
 def cpu_baseline_run(name, seconds=10.0, scale=1 / 4):
     """The oracle (OpenMP over blocks, all host cores) on a bounded sample of
-    the workload: the same problem at reduced resolution, as many steps as fit
-    in `seconds`."""
+    the workload: the same problem at `scale` blocks per axis (the stated
+    size for the 2-D workloads, 1/4 per axis for the 3-D ones), as many steps
+    as fit in `seconds`."""
     if name == "amr3d":
         return cpu_baseline_amr(seconds)
     from flashx_b200 import simulations as S
@@ -246,12 +249,18 @@ def run_reference(args):
         steps, warm = max(1, min(args.steps, 3)), min(args.warmup, 1)
         sample = f"amr3d {mesh.nleaf} leaves ({ncell} zones) per step"
     else:
-        geom, hp, unk, mesh, ncell = make_problem(args.config, scale=1 / 4)
+        # 2-D workloads at their stated size; 3-D ones (seconds per oracle
+        # step at 256^3) at 1/4 of the blocks per axis
+        scale = 1.0 if args.config in ("kh2d", "sod2d") else 1 / 4
+        geom, hp, unk, mesh, ncell = make_problem(args.config, scale=scale)
         p = O.make_params(geom.as_dict(), hp)
         step = lambda dt: O.hydro_step(p, unk, dt, dt)
         cfl_dt = lambda: O.compute_dt(p, unk)
         steps, warm = args.steps, args.warmup
-        sample = f"{args.config} {geom.nxb * geom.nblockx}^{geom.ndim} per step"
+        if scale == 1.0 and args.config == "kh2d":
+            steps, warm = min(args.steps, 20), min(args.warmup, 3)
+        sample = f"{args.config} {geom.nxb * geom.nblockx}^{geom.ndim} per step" + (
+            " (the stated configuration)" if scale == 1.0 else " (1/4 of the blocks per axis)")
     dt = 0.5 * cfl_dt()
     for _ in range(warm):
         step(dt)
@@ -303,6 +312,89 @@ def host_unk_round_trip(dev, hp, unk0, steps, barrier, max_over_ranks, global_mi
             "note": "whole UNK (guard cells included) from pinned host memory to the device and back every step, "
                     "for callers whose host units touch UNK every step; the resident-mirror loop above is the "
                     "drop-in's steady state (UNK crosses PCIe only at attach, restart and IO)"}
+
+
+def accuracy_leg(geom, hp, unk0, mesh, steps, global_min):
+    """Mixed precision against plain FP64 on the workload over `steps` steps of
+    one dt sequence (the FP64 run's Driver_computeDt sequence, replayed by the
+    mixed run through Hydro(dt)): relative L1 of density, pressure and speed
+    |v| over all (leaf) interior cells, and for both precisions the mass and
+    total-energy drift |I(t) - I(0)| / |I(0)| from the volume integrals."""
+    from flashx_b200.hydro import HydroDevice, driver_dt
+    res = {"steps": steps}
+    states, drift, dts = {}, {}, []
+    for prec in ("fp64", "mixed"):
+        dev = HydroDevice(geom, hp, prec, mesh=mesh)
+        dev.attach_unk(unk0.copy())
+        I0 = dev.integrals()
+        if prec == "fp64":
+            dt = dt_old = 0.5 * dev.Hydro_computeDt()
+            for _ in range(steps):
+                dts.append(dt)
+                dev.Hydro(0.0, dt, dt_old)
+                dt_old, dt = dt, driver_dt(global_min(dev.Hydro_computeDt()), dt, hp)
+        else:
+            for i, dt in enumerate(dts):
+                dev.Hydro(0.0, dt, dts[i - 1] if i else dt)
+        I1 = dev.integrals()
+        st = np.zeros(unk0.shape)
+        dev.sync_to_host(st)
+        dev.close()
+        states[prec] = interiors(geom, st, mesh)
+        drift[prec] = {"mass": float(abs(I1[0] - I0[0]) / abs(I0[0])),
+                       "total_energy": float(abs(I1[4] - I0[4]) / abs(I0[4]))}
+    a, b = states["mixed"], states["fp64"]
+    rel = lambda x, y: float(np.mean(np.abs(x - y)) / max(np.mean(np.abs(y)), 1e-300))
+    speed = lambda u: np.sqrt(u[:, 8] ** 2 + u[:, 9] ** 2 + u[:, 10] ** 2)
+    res["l1_rel_mixed_vs_fp64"] = {"dens": rel(a[:, 0], b[:, 0]), "pres": rel(a[:, 5], b[:, 5]),
+                                   "speed": rel(speed(a), speed(b))}
+    res["drift"] = drift
+    res["simulated_time"] = float(sum(dts))
+    res["note"] = ("same dt sequence for both precisions (FP64 Driver_computeDt); drift is the relative change "
+                   "of the volume integrals of mass and total energy (conserved on periodic domains; "
+                   "gravity and open boundaries exchange energy)")
+    return res
+
+
+def per_block_driver(dev, geom, mesh, hp, steps, global_min):
+    """The Fortran driver's calling pattern: per step one Hydro() and one
+    Hydro_computeDt per leaf block (Driver_computeDt.F90:306), each returning
+    dtCheck and dtMinLoc, reduced on the host; through the C ABI with host
+    buffers.  The library reduces on the device at the first call of a step
+    and answers the others from its cache (counted by fxb_counters)."""
+    import ctypes
+    from flashx_b200.hydro import COUNT_DT_CACHED, COUNT_DT_DEVICE, _check, driver_dt
+    lib = dev.lib
+    f = lib.fxb_compute_dt
+    nblk = mesh.nleaf if mesh is not None else dev.unk_shape[0]
+    out = ctypes.c_double()
+    loc = (ctypes.c_int32 * 5)()
+    pout = ctypes.byref(out)
+    dt = dt_old = 0.5 * dev.Hydro_computeDt()
+    c0 = dev.counters()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        _check(lib.fxb_hydro_step(0.0, dt, dt_old))
+        dtcheck = 1e300
+        for _b in range(nblk):
+            _check(f(pout, loc))
+            if out.value < dtcheck:
+                dtcheck = out.value
+        dt_old, dt = dt, driver_dt(global_min(dtcheck), dt, hp)
+    el = time.perf_counter() - t0
+    c1 = dev.counters()
+    return {"value": geom_zones(geom, mesh) * steps / el, "unit": UNIT, "steps": steps,
+            "h2d_bytes_per_step": 24, "d2h_bytes_per_step": 8 + 28 * nblk,
+            "hydro_computeDt_calls_per_step": nblk,
+            "device_dt_reductions_per_step": (c1[COUNT_DT_DEVICE] - c0[COUNT_DT_DEVICE]) / steps,
+            "cached_dt_calls_per_step": (c1[COUNT_DT_CACHED] - c0[COUNT_DT_CACHED]) / steps,
+            "note": "per step: fxb_hydro_step, then fxb_compute_dt(dt, dtMinLoc) once per leaf block from a Python "
+                    "loop (ctypes call overhead included); one device reduction per step, the other calls "
+                    "return the cached result"}
+
+
+def geom_zones(geom, mesh):
+    return mesh.ncells() if mesh is not None else geom.ncells
 
 
 def fp_roofline(config, precision, zones_per_s):
@@ -457,6 +549,8 @@ def run_ours(args):
     dev.sync_to_host(fp64_state)
     ref_after = interiors(geom, fp64_state, mesh)
     e2e_host = host_unk_round_trip(dev, hp, unk0, min(K, 20), barrier, max_over_ranks, global_min, world * ncell)
+    dev.attach_unk(unk0.copy())
+    e2e_driver = per_block_driver(dev, geom, mesh, hp, min(K, 5), global_min)
 
     peak, peak_kind = measured_peaks()
     achieved = BYTES_PER_ZONE * ncell / (kernel_ms / 1e3) / 1e9
@@ -494,7 +588,8 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24, "d2h_bytes_per_step": 8,
                     "note": "host loop via fxb_hydro_step/fxb_compute_dt: (t, dt, dtOld) in, dt out per step; "
                             "UNK stays resident on the device"},
-            "e2e_host_unk": e2e_host}
+            "e2e_host_unk": e2e_host,
+            "e2e_driver": e2e_driver}
     flops = fp_roofline(args.config, "fp64", ncell / (kernel_ms / 1e3))
     if flops:
         line["roofline_fp"] = flops
@@ -526,8 +621,11 @@ def run_ours(args):
         if mflops:
             line["mixed"]["roofline_fp"] = mflops
 
+    if not args.no_mixed and world == 1 and args.accuracy_steps > 0:
+        line["accuracy"] = accuracy_leg(geom, hp, unk0, mesh, args.accuracy_steps, global_min)
+
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_run(args.config, scale=args.scale / 4 if geom.ndim == 2 else args.scale / 4)
+        line["cpu_baseline"] = cpu_baseline_run(args.config, scale=args.scale if geom.ndim == 2 else args.scale / 4)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -95,6 +95,7 @@ struct State {
     double *stage = nullptr;                      // UNK staging for attach / sync
     int stage_leaves = 0;
     int *leaf_blk_dev = nullptr, *d_dmap = nullptr;
+    int *d_pmap = nullptr;                        // device variable -> place in a packed guard fill
     int nfiner = 0;
     int *d_glist = nullptr;                       // guard cells the pipeline reads (extended-block offsets)
     int nglist = 0;
@@ -484,7 +485,7 @@ __global__ void __launch_bounds__(256, FXB_FILL_MINB) amr_fill_kernel(MeshArgs m
     const AmrEntry3 e = entries[blockIdx.y];
     const int b = leaf_blk[e.leaf];
     const DevBlk B = m.blk[b];
-    const unsigned mask = eosmask[e.leaf];
+    const unsigned mask = eosmask ? eosmask[e.leaf] : 0u;     // no mask: no Eos on guard cells
     const int n = m.n, g = m.ng, ne = n + 2 * g;
     const long nint = (long)n * n * n;
     const long ncell = glist ? nint + nlist : (long)ne * ne * ne;
@@ -517,7 +518,8 @@ __global__ void __launch_bounds__(256, FXB_FILL_MINB) amr_fill_kernel(MeshArgs m
         }
         if constexpr (TO_UNK) {
 #pragma unroll
-            for (int v = 0; v < NV_DEV; v++) dst[idx * nunk + dmap[v]] = (T)u[v];
+            for (int v = 0; v < NV_DEV; v++)
+                if (dmap[v] >= 0) dst[idx * nunk + dmap[v]] = (T)u[v];   // < 0: not selected by a mask
         } else {
 #pragma unroll
             for (int v = 0; v < NV_GCB; v++) dst[v * gvs + idx] = (T)u[v];
@@ -1144,7 +1146,7 @@ void free_device(State &s)
     dfree(s.d_finer); dfree(s.d_fine); dfree(s.d_dxl); dfree(s.d_entries); dfree(s.leaf_blk_dev);
     dfree(s.gcb); dfree(s.sig); dfree(s.slp); dfree(s.flat);
     for (int d = 0; d < 3; d++) { dfree(s.w[d]); dfree(s.f[d]); }
-    dfree(s.bflux); dfree(s.stage); dfree(s.d_dmap); dfree(s.d_glist);
+    dfree(s.bflux); dfree(s.stage); dfree(s.d_dmap); dfree(s.d_pmap); dfree(s.d_glist);
     dfree(s.d_plan); dfree(s.d_prol); dfree(s.d_poff); dfree(s.d_rlist);
     dfree(s.d_active); dfree(s.d_act_eos); dfree(s.d_act_bnd); dfree(s.d_ext); dfree(s.d_err);
 }
@@ -1490,6 +1492,27 @@ int amr_sync_to_host(double *unk_host)
                             S.C.stream));
     }
     CKA(cudaStreamSynchronize(S.C.stream));
+    return FXB_OK;
+}
+
+int amr_fill_to_host(double *unk_host, const int pos[NV_DEV], int n, const int slot[NV_DEV], bool do_eos)
+{
+    const long per = ne3();
+    restrict_all(S.cur);
+    if (!S.d_pmap) CKA(cudaMalloc(&S.d_pmap, sizeof(int) * NV_DEV));
+    CKA(cudaMemcpyAsync(S.d_pmap, pos, sizeof(int) * NV_DEV, cudaMemcpyHostToDevice, S.C.stream));
+    // the staging buffer holds stage_leaves whole UNK blocks, so at least as
+    // many packed ones
+    const int chunk = S.stage_leaves;
+    for (int l0 = 0; l0 < S.nleaf; l0 += chunk) {
+        const int nl = std::min(chunk, S.nleaf - l0);
+        amr_fill_kernel<double, true><<<dim3(S.fill_cta, nl), 256, 0, S.C.stream>>>(
+            mesh_args(S.cur), S.d_entries + l0, S.leaf_blk_dev, do_eos ? S.d_eosmask : nullptr, S.stage, 0,
+            per * n, n, S.d_pmap, nullptr, 0, S.C.dprm, S.C.gam1inv, S.C.ggprodinv);
+        CKA(cudaGetLastError());
+        int rc = pack_to_host(S.stage, per * nl, n, slot, unk_host + per * S.C.nunk * l0);
+        if (rc) return rc;
+    }
     return FXB_OK;
 }
 

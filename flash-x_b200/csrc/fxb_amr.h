@@ -30,6 +30,11 @@ int amr_cur();      // which interior store holds the current state
 void amr_destroy();
 int amr_attach(const double *unk_host);
 int amr_sync_to_host(double *unk_host);
+// Grid_fillGuardCells into the host UNK for some of the variables: pos[v] is
+// device variable v's place in the packed cell vector (-1: not copied), n the
+// places, slot[q] their UNK slots; Eos on the guard regions next to other
+// levels only with do_eos (Paramesh4/Grid_fillGuardCells.F90:531-548)
+int amr_fill_to_host(double *unk_host, const int pos[NV_DEV], int n, const int slot[NV_DEV], bool do_eos);
 // one Hydro() step enqueued on the stream; dt from dtv when dtv != nullptr
 int amr_step(const double *dtv, double dt, int *launches);
 int amr_rate();
@@ -52,5 +57,9 @@ const char *amr_tuning_log();
 
 // reports through fxb_last_error (defined in fxb_api.cu)
 int record_error(int code, const char *msg);
+// packed cell vectors (ncell x n doubles in device memory) into their UNK
+// slots slot[q] of unk_host (ncell cells of nunk doubles), through a pinned
+// staging copy (defined in fxb_api.cu)
+int pack_to_host(const double *pack_dev, long ncell, int n, const int *slot, double *unk_host);
 
 } // namespace fxb

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <array>
 #include <unordered_map>
+#include <thread>
 #include <unordered_set>
 #include <vector>
 
@@ -48,6 +49,18 @@ struct Lib {
     double *partials = nullptr;
     int npartials = 0;
     bool rate_valid = false;
+    // Hydro_computeDt result of the current state: computed by the first
+    // fxb_compute_dt after the state changed, returned by the later ones
+    bool dt_valid = false, loc_valid = false;
+    double dt_cached = 0.;
+    int32_t loc_cached[5] = {0, 0, 0, 0, 0};
+    long long counts[FXB_NCOUNTERS] = {};
+    double *pack_host = nullptr;   // pinned staging of masked guard fills
+    size_t pack_host_doubles = 0;
+    double *pack_dev = nullptr;    // packed selected variables (uniform grid)
+    size_t pack_dev_doubles = 0;
+    int *pmap_dev = nullptr;       // device variable -> place in a packed cell vector
+    const double *unk_attached = nullptr;
     bool attached = false;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -75,6 +88,14 @@ int cuda_fail(cudaError_t e, const char *where)
     char buf[256];
     snprintf(buf, sizeof(buf), "%s: %s", where, cudaGetErrorString(e));
     return fail(FXB_ECUDA, buf);
+}
+
+// the device state changed: a cached Hydro_computeDt result is stale; the
+// CFL rate is valid only when the change was a fused hydro step
+void state_changed(bool fused_rate)
+{
+    L.rate_valid = fused_rate;
+    L.dt_valid = L.loc_valid = false;
 }
 
 #define CK(call)                                                    \
@@ -135,6 +156,7 @@ __global__ void state_to_unk_kernel(const double *__restrict__ st, double *__res
         long c = ((long)mz * g.ny + my) * g.nx + mx;
         long u = idx * g.nunk;
         for (int v = 0; v < NV_DEV; v++) {
+            if (dmap[v] < 0) continue;          // not selected by a guard-fill mask
             double val = st[v * g.vstride + c];
             if (v == VX) val = val * sx;
             if (v == VY) val = val * sy;
@@ -366,6 +388,9 @@ void free_all()
     if (L.unk_dev) cudaFree(L.unk_dev);
     if (L.bcoord) cudaFree(L.bcoord);
     if (L.dmap_dev) cudaFree(L.dmap_dev);
+    if (L.pmap_dev) cudaFree(L.pmap_dev);
+    if (L.pack_dev) cudaFree(L.pack_dev);
+    if (L.pack_host) cudaFreeHost(L.pack_host);
     if (L.dtv) cudaFree(L.dtv);
     if (L.rate_max) cudaFree(L.rate_max);
     if (L.err) cudaFree(L.err);
@@ -509,6 +534,7 @@ extern "C" int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
     }
     CK(cudaMalloc(&L.unk_dev, sizeof(double) * L.unk_doubles));
     CK(cudaMalloc(&L.dmap_dev, sizeof(int) * NV_DEV));
+    CK(cudaMalloc(&L.pmap_dev, sizeof(int) * NV_DEV));
     CK(cudaMemcpyAsync(L.dmap_dev, L.dmap, sizeof(int) * NV_DEV, cudaMemcpyHostToDevice, L.stream));
     CK(cudaMalloc(&L.dtv, 2 * sizeof(double)));
     CK(cudaMalloc(&L.rate_max, sizeof(unsigned long long)));
@@ -551,7 +577,7 @@ extern "C" int fxb_register_blocks(const fxb_block_desc *blocks, int nblk)
     bool refined = nblk != L.nblk;
     for (int b = 0; b < nblk && !refined; b++) refined = blocks[b].level != 1;
     L.attached = false;
-    L.rate_valid = false;
+    state_changed(false);
     for (int i = 0; i < 2; i++) {
         if (L.graph_exec[i]) cudaGraphExecDestroy(L.graph_exec[i]);
         L.graph_exec[i] = nullptr;
@@ -607,7 +633,8 @@ extern "C" int fxb_attach_unk(const double *unk_host)
         int rc = amr_attach(unk_host);
         if (rc) return rc;
         L.attached = true;
-        L.rate_valid = false;
+        L.unk_attached = unk_host;
+        state_changed(false);
         return FXB_OK;
     }
     if (!L.inited || !L.bcoord) return fail(FXB_EARG, "fxb_attach_unk: call fxb_init and fxb_register_blocks first");
@@ -617,7 +644,8 @@ extern "C" int fxb_attach_unk(const double *unk_host)
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(L.stream));
     L.attached = true;
-    L.rate_valid = false;
+    L.unk_attached = unk_host;
+    state_changed(false);
     return FXB_OK;
 }
 
@@ -636,21 +664,113 @@ extern "C" int fxb_sync_to_host(double *unk_host)
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(unk_host, L.unk_dev, sizeof(double) * L.unk_doubles, cudaMemcpyDeviceToHost, L.stream));
     CK(cudaStreamSynchronize(L.stream));
+    L.counts[FXB_COUNT_GC_FILLS]++;
+    L.counts[FXB_COUNT_GC_DOUBLES] += L.unk_doubles;
     return check_err_word();
 }
 
-extern "C" int fxb_fill_guardcells(double *unk_host) { return fxb_sync_to_host(unk_host); }
+namespace {
+// the device variables a guard-fill mask selects (bit fxb_var; 0 = all),
+// packed per cell in device-variable order: pos[v] is v's place in the
+// packed vector (-1: not selected), slot[q] the UNK slot of place q
+struct VarPack {
+    int pos[NV_DEV];
+    int slot[NV_DEV];
+    int n = 0;
+};
+
+VarPack var_pack(int mask_bits)
+{
+    VarPack vp;
+    for (int v = 0; v < NV_DEV; v++) {
+        const bool sel = mask_bits == 0 || ((mask_bits >> kDevToVar[v]) & 1);
+        vp.pos[v] = sel ? vp.n : -1;
+        if (sel) vp.slot[vp.n++] = L.dmap[v];
+    }
+    return vp;
+}
+} // namespace
+
+namespace fxb {
+// packed cell vectors (ncell x n doubles, device) into their UNK slots of
+// unk_host (ncell x nunk), through a pinned staging copy; variables outside
+// the pack keep their host values
+int pack_to_host(const double *pack_dev, long ncell, int n, const int *slot, double *unk_host)
+{
+    const size_t nd = (size_t)ncell * n;
+    if (nd > L.pack_host_doubles) {
+        if (L.pack_host) cudaFreeHost(L.pack_host);
+        L.pack_host = nullptr;
+        L.pack_host_doubles = 0;
+        CK(cudaMallocHost(&L.pack_host, sizeof(double) * nd));
+        L.pack_host_doubles = nd;
+    }
+    CK(cudaMemcpyAsync(L.pack_host, pack_dev, sizeof(double) * nd, cudaMemcpyDeviceToHost, L.stream));
+    CK(cudaStreamSynchronize(L.stream));
+    const int nunk = L.nunk;
+    const double *src = L.pack_host;
+    auto scatter = [&](long c0, long c1) {
+        for (long c = c0; c < c1; c++)
+            for (int q = 0; q < n; q++) unk_host[c * nunk + slot[q]] = src[c * n + q];
+    };
+    const int nth = ncell >= (1L << 20) ? 8 : 1;
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nth; t++) pool.emplace_back(scatter, ncell * t / nth, ncell * (t + 1) / nth);
+    scatter(0, ncell / nth);
+    for (auto &th : pool) th.join();
+    L.counts[FXB_COUNT_GC_DOUBLES] += (long long)nd;
+    return FXB_OK;
+}
+} // namespace fxb
+
+extern "C" int fxb_fill_guardcells(int mask_bits, int do_eos, double *unk_host)
+{
+    if (!L.attached) return fail(FXB_EARG, "fxb_fill_guardcells: no UNK attached");
+    if (mask_bits < 0 || mask_bits >= (1 << FXB_NVAR))
+        return fail(FXB_EARG, "fxb_fill_guardcells: mask bits outside the fxb_var range");
+    double *dst = unk_host ? unk_host : const_cast<double *>(L.unk_attached);
+    if (!dst) return fail(FXB_EARG, "fxb_fill_guardcells: null UNK");
+    const VarPack vp = var_pack(mask_bits);
+    if (vp.n == 0) return FXB_OK;
+    // all variables: the whole UNK in one copy (Eos on the guard regions next
+    // to other levels is part of the AMR fill, so doEos = .false. takes the
+    // packed path there)
+    if (vp.n == NV_DEV && (do_eos || !amr_active())) return fxb_sync_to_host(dst);
+    L.counts[FXB_COUNT_GC_FILLS]++;
+    if (amr_active()) {
+        int rc = amr_fill_to_host(dst, vp.pos, vp.n, vp.slot, do_eos != 0);
+        return rc ? rc : check_err_word();
+    }
+    // UG (UG/Grid_fillGuardCells.F90 does not act on doEos): the selected
+    // variables of every block, guard cells included, packed per cell
+    const long ncell = L.unk_doubles / L.nunk;
+    const size_t need = (size_t)ncell * vp.n;
+    if (need > L.pack_dev_doubles) {
+        if (L.pack_dev) cudaFree(L.pack_dev);
+        L.pack_dev = nullptr;
+        L.pack_dev_doubles = 0;
+        CK(cudaMalloc(&L.pack_dev, sizeof(double) * need));
+        L.pack_dev_doubles = need;
+    }
+    CK(cudaMemcpyAsync(L.pmap_dev, vp.pos, sizeof(int) * NV_DEV, cudaMemcpyHostToDevice, L.stream));
+    UnkGeom g = unk_geom();
+    g.nunk = vp.n;
+    state_to_unk_kernel<<<1184, 256, 0, L.stream>>>(L.buf[L.cur], L.pack_dev, g, L.bcoord, L.pmap_dev, L.nblk);
+    CK(cudaGetLastError());
+    int rc = pack_to_host(L.pack_dev, ncell, vp.n, vp.slot, dst);
+    return rc ? rc : check_err_word();
+}
 
 extern "C" int fxb_eos(void)
 {
     if (!L.attached) return fail(FXB_EARG, "fxb_eos: no UNK attached");
     if (amr_active()) {
-        L.rate_valid = false;
+        state_changed(false);
         return amr_eos();
     }
     eos_kernel<<<1184, 256, 0, L.stream>>>(L.buf[L.cur], L.vstride, L.ncell, L.dprm, L.gam1inv, L.ggprodinv);
     CK(cudaGetLastError());
-    L.rate_valid = false;
+    state_changed(false);
     return FXB_OK;
 }
 
@@ -672,7 +792,8 @@ extern "C" int fxb_hydro_step(double sim_time, double dt, double dt_old)
         nl = (L.dom.ndim == 2 ? 1 : hydro3d_launches(L.prm)) + (L.prm.flattening ? 1 : 0);
     }
     CK(cudaEventRecord(L.ev1, L.stream));
-    L.rate_valid = true;
+    state_changed(true);
+    L.counts[FXB_COUNT_STEPS]++;
     L.last_launches = nl;
     L.timing_valid = true;
     return FXB_OK;
@@ -682,6 +803,19 @@ extern "C" int fxb_compute_dt(double *dt_out, int32_t loc[5])
 {
     if (!L.attached) return fail(FXB_EARG, "fxb_compute_dt: no UNK attached");
     if (!dt_out) return fail(FXB_EARG, "fxb_compute_dt: null output");
+    // Driver_computeDt.F90:306 calls Hydro_computeDt once per leaf block: the
+    // first call after a state change reduces the whole grid on the device,
+    // the later ones return the cached global result without a launch or a
+    // host synchronisation
+    if (L.dt_valid && (!loc || L.loc_valid)) {
+        L.counts[FXB_COUNT_DT_CACHED]++;
+        if (loc)
+            for (int q = 0; q < 5; q++) loc[q] = L.loc_cached[q];
+        *dt_out = L.dt_cached;
+        if (!(L.dt_cached > 0.)) return fail(FXB_EDT, "[Hydro]: Computed dt is not positive! Aborting!");
+        return FXB_OK;
+    }
+    L.counts[FXB_COUNT_DT_DEVICE]++;
     if (!L.rate_valid && amr_active()) {
         CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
         int rc = amr_rate();
@@ -734,7 +868,11 @@ extern "C" int fxb_compute_dt(double *dt_out, int32_t loc[5])
             loc[3] = amr_active() ? amr_leaf_level((int)b) : 1;
             loc[4] = (int32_t)(b + 1);
         }
+        for (int q = 0; q < 5; q++) L.loc_cached[q] = loc[q];
+        L.loc_valid = true;
     }
+    L.dt_cached = dt;
+    L.dt_valid = true;
     *dt_out = dt;
     if (!(dt > 0.)) return fail(FXB_EDT, "[Hydro]: Computed dt is not positive! Aborting!");
     return FXB_OK;
@@ -786,7 +924,8 @@ extern "C" int fxb_advance(int nsteps, double *dt, double *dt_old, double f, dou
     CK(cudaStreamSynchronize(L.stream));
     *dt = h[0];
     *dt_old = h[1];
-    L.rate_valid = false;
+    state_changed(false);
+    L.counts[FXB_COUNT_STEPS] += nsteps;
     L.last_launches = (step_launches + 1) * nsteps;
     L.timing_valid = true;
     return check_err_word();
@@ -1046,7 +1185,7 @@ extern "C" int fxb_regrid(const fxb_block_desc *blocks, int nblk)
         if (L.graph_exec[i]) cudaGraphExecDestroy(L.graph_exec[i]);
         L.graph_exec[i] = nullptr;
     }
-    L.rate_valid = false;
+    state_changed(false);
     int rc = amr_regrid(blocks, nblk);
     if (rc) return rc;
     return check_err_word();
@@ -1071,6 +1210,13 @@ extern "C" int fxb_tuning(char *buf, int len)
     if (amr_active()) snprintf(buf, len, "%s", amr_tuning_log());
     else if (L.dom.ndim == 2) snprintf(buf, len, "uniform grid 2-D: one CTA of %d threads per 16x16 tile (fixed)", 320);
     else snprintf(buf, len, "uniform grid 3-D: %d CTAs of 256 threads per stage (fixed)", 148 * 8);
+    return FXB_OK;
+}
+
+extern "C" int fxb_counters(long long counts[FXB_NCOUNTERS])
+{
+    if (!counts) return fail(FXB_EARG, "fxb_counters: null output");
+    for (int q = 0; q < FXB_NCOUNTERS; q++) counts[q] = L.counts[q];
     return FXB_OK;
 }
 

@@ -18,15 +18,28 @@
 // the first call on a device does this set-up, make that first call before
 // any stream capture.
 //
+// The cached address belongs to the device's current CUDA context: after a
+// cudaDeviceReset the module is loaded again, possibly elsewhere, and the
+// cached address is stale, so a caller that resets a device must not call
+// this entry point on it again in the same process.  The set-up is guarded
+// by a mutex, so host threads may make their first calls concurrently.
+//
 // Every call on a device shares the one array and leaves its partial sums
 // there; each call writes every slot it later reads, so nothing needs to be
 // cleared first.  Calls that overlap on the GPU (different streams, or
 // different host threads, on the same device) race on the array and must be
 // serialised by the caller.
+//
+// Results are deterministic for a given ncell (fixed chunks per CTA, fixed
+// reduction trees) but are summed in a different order from fxb_integrals,
+// so the two differ by roundoff.
 #include "../../include/flashx_b200.h"
 
 #include <cuda_runtime.h>
 #include <stdio.h>
+
+#include <atomic>
+#include <mutex>
 
 namespace fxb {
 int record_error(int code, const char *msg);   // fxb_api.cu: feeds fxb_last_error
@@ -43,7 +56,8 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) double g_partials[kMaxPartials * 7];
 
 double *g_partials_dev[kMaxDevices];      // device address of g_partials, per device
-bool g_ready[kMaxDevices];
+std::atomic<bool> g_ready[kMaxDevices];   // g_partials_dev[d] is set
+std::mutex g_setup;
 
 __global__ void noalloc_partial_kernel(const double *__restrict__ dens, const double *__restrict__ velx,
                                        const double *__restrict__ vely, const double *__restrict__ velz,
@@ -71,13 +85,21 @@ __global__ void noalloc_partial_kernel(const double *__restrict__ dens, const do
         for (int q = 0; q < 7; q++) partials[blockIdx.x * 7 + q] = sh[q][0];
 }
 
-__global__ void noalloc_final_kernel(const double *partials, int n, double *out)
+// one CTA: each thread sums a fixed stride of the partials, then a tree
+__global__ void __launch_bounds__(kThreads) noalloc_final_kernel(const double *partials, int n, double *out)
 {
-    if (threadIdx.x < 7) {
-        double t = 0.;
-        for (int b = 0; b < n; b++) t += partials[b * 7 + threadIdx.x];
-        out[threadIdx.x] = t;
+    double t[7] = {0., 0., 0., 0., 0., 0., 0.};
+    for (int b = threadIdx.x; b < n; b += kThreads)
+        for (int q = 0; q < 7; q++) t[q] += partials[b * 7 + q];
+    __shared__ double sh[7][kThreads];
+    for (int q = 0; q < 7; q++) sh[q][threadIdx.x] = t[q];
+    __syncthreads();
+    for (int w = kThreads / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            for (int q = 0; q < 7; q++) sh[q][threadIdx.x] += sh[q][threadIdx.x + w];
+        __syncthreads();
     }
+    if (threadIdx.x < 7) out[threadIdx.x] = sh[threadIdx.x][0];
 }
 
 } // namespace
@@ -102,16 +124,19 @@ extern "C" int fxb_integrals_noalloc(const double *dens, const double *velx, con
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fxb::record_error(FXB_ECUDA, cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return fxb::record_error(FXB_EARG, "fxb_integrals_noalloc: device index too large");
-    if (!g_ready[dev]) {
+    if (!g_ready[dev].load(std::memory_order_acquire)) {
         // set-up, once per device, with that device current
-        e = cudaGetSymbolAddress((void **)&g_partials_dev[dev], g_partials);
-        if (e != cudaSuccess) return fxb::record_error(FXB_ECUDA, cudaGetErrorString(e));
-        g_ready[dev] = true;
+        std::lock_guard<std::mutex> lock(g_setup);
+        if (!g_ready[dev].load(std::memory_order_relaxed)) {
+            e = cudaGetSymbolAddress((void **)&g_partials_dev[dev], g_partials);
+            if (e != cudaSuccess) return fxb::record_error(FXB_ECUDA, cudaGetErrorString(e));
+            g_ready[dev].store(true, std::memory_order_release);
+        }
     }
     cudaStream_t s = (cudaStream_t)stream;
     noalloc_partial_kernel<<<(unsigned)nparts, kThreads, 0, s>>>(dens, velx, vely, velz, ener, eint, ncell,
                                                                  cell_volume, g_partials_dev[dev]);
-    noalloc_final_kernel<<<1, 32, 0, s>>>(g_partials_dev[dev], (int)nparts, out_dev);
+    noalloc_final_kernel<<<1, kThreads, 0, s>>>(g_partials_dev[dev], (int)nparts, out_dev);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fxb::record_error(FXB_ECUDA, cudaGetErrorString(e));
     return FXB_OK;

@@ -32,7 +32,9 @@ ABI_SYMBOLS = ("fxb_init", "fxb_register_blocks", "fxb_attach_unk", "fxb_fill_gu
                "fxb_sync_from_host", "fxb_integrals", "fxb_integrals_noalloc", "fxb_mark_refine_derefine",
                "fxb_last_timing", "fxb_stream", "fxb_tuning", "fxb_last_error", "fxb_finalize",
                "fxb_init_slab", "fxb_halo_doubles", "fxb_halo_pack", "fxb_halo_unpack", "fxb_regrid",
-               "fxb_refine_derefine")
+               "fxb_refine_derefine", "fxb_counters")
+# fxb_counters slots
+COUNT_STEPS, COUNT_DT_DEVICE, COUNT_DT_CACHED, COUNT_GC_FILLS, COUNT_GC_DOUBLES = range(5)
 
 
 class FxbParams(ctypes.Structure):
@@ -96,7 +98,8 @@ def load_library(path=LIB_PATH):
     L.fxb_init.argtypes = [ctypes.POINTER(FxbParams), ctypes.POINTER(FxbDomain), I32, ctypes.c_int]
     L.fxb_register_blocks.argtypes = [ctypes.POINTER(FxbBlockDesc), ctypes.c_int]
     L.fxb_attach_unk.argtypes = [D]
-    L.fxb_fill_guardcells.argtypes = [D]
+    L.fxb_fill_guardcells.argtypes = [ctypes.c_int, ctypes.c_int, D]
+    L.fxb_counters.argtypes = [ctypes.POINTER(ctypes.c_longlong)]
     L.fxb_hydro_step.argtypes = [ctypes.c_double] * 3
     L.fxb_compute_dt.argtypes = [D, I32]
     L.fxb_advance.argtypes = [ctypes.c_int, D, D, ctypes.c_double, ctypes.c_double, ctypes.c_double]
@@ -321,11 +324,20 @@ class HydroDevice:
         return unk
 
     # ---- the reference interface
-    def Grid_fillGuardCells(self, unk=None):
-        """Fill the guard cells (and interiors) of the host UNK from the device."""
+    def Grid_fillGuardCells(self, unk=None, mask=None, doEos=True):
+        """Fill the guard cells (and interiors) of the host UNK from the device.
+        mask: names of the variables to fill (Grid_fillGuardCells' mask;
+        None = all); only those cross PCIe and are written.  doEos: Eos on
+        the guard regions next to other refinement levels (AMR meshes; the
+        uniform grid ignores it, as UG's Grid_fillGuardCells does)."""
         unk = self.unk if unk is None else unk
+        if unk is None or unk.shape != self.unk_shape:
+            raise ValueError(f"Grid_fillGuardCells needs a UNK of shape {self.unk_shape}")
+        bits = 0
+        for name in (mask or ()):
+            bits |= 1 << FXB_VARS.index(name)
         self.fill_halos()
-        _check(self.lib.fxb_fill_guardcells(_dp(unk)))
+        _check(self.lib.fxb_fill_guardcells(bits, int(bool(doEos)), _dp(unk)))
         return unk
 
     def Hydro(self, simTime, dt, dtOld):
@@ -405,6 +417,13 @@ class HydroDevice:
         buf = ctypes.create_string_buffer(256)
         _check(self.lib.fxb_tuning(buf, 256))
         return buf.value.decode()
+
+    def counters(self):
+        """fxb_counters: hydro steps, device and cached Hydro_computeDt calls,
+        guard fills to the host and the doubles they moved."""
+        c = (ctypes.c_longlong * 5)()
+        _check(self.lib.fxb_counters(c))
+        return list(c)
 
     def last_timing(self):
         ms = ctypes.c_double()

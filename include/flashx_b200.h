@@ -2,8 +2,8 @@
  * flashx_b200.h -- C ABI of libflashx_b200.so, the B200 (sm_100a) drop-in for
  * the Flash-X unsplit compressible-hydro hot path.
  *
- * Plain C types only: the Fortran driver binds these with ISO_C_BINDING
- * (see INTEGRATION.md), Python with ctypes.  Every function returns an int
+ * Plain C types only: the Fortran driver binds these with ISO_C_BINDING,
+ * Python with ctypes.  Every function returns an int
  * status: FXB_OK (0) or one of the FXB_E* codes; fxb_last_error() gives the
  * message.  The library never calls exit() or abort().
  *
@@ -154,10 +154,19 @@ int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
 int fxb_register_blocks(const fxb_block_desc *blocks, int nblk);
 /* Copy the host UNK (all blocks, guard cells included) into the device mirror. */
 int fxb_attach_unk(const double *unk_host);
-/* Grid_fillGuardCells(CENTER, ALLDIR): the device mirror has no stored guard
- * cells (the hydro kernel resolves neighbour and boundary cells on load), so
- * this writes the filled guard cells, with the interiors, into unk_host. */
-int fxb_fill_guardcells(double *unk_host);
+/* Grid_fillGuardCells(CENTER, ALLDIR, doEos=do_eos, mask=mask_bits): the
+ * device mirror has no stored guard cells (the hydro kernel resolves
+ * neighbour and boundary cells on load), so this writes the filled guard
+ * cells, with the interiors, of the selected variables into unk_host (NULL:
+ * the UNK of the last fxb_attach_unk / fxb_sync_from_host).  mask_bits: bit
+ * (1 << fxb_var) selects a variable, 0 selects all of them (the call without
+ * a mask); only the selected variables cross PCIe and are written, the other
+ * UNK entries keep their host values.  do_eos: on AMR meshes, Eos_guardCells
+ * on the guard regions next to other refinement levels
+ * (Paramesh4/Grid_fillGuardCells.F90:531-548); the uniform grid ignores it,
+ * as UG/Grid_fillGuardCells.F90 does.  FXB_EARG for bits outside the fxb_var
+ * range. */
+int fxb_fill_guardcells(int mask_bits, int do_eos, double *unk_host);
 /* Hydro(simTime, dt, dtOld): one unsplit step of every leaf block on the
  * device (guard resolution, reconstruction, Riemann solve, conserved update,
  * energyFix, Eos), followed on the device by the CFL reduction that
@@ -165,6 +174,11 @@ int fxb_fill_guardcells(double *unk_host);
 int fxb_hydro_step(double sim_time, double dt, double dt_old);
 /* Hydro_computeDt reduced over all blocks (Driver_computeDt's MPI_AllReduce
  * MIN of the per-block dtCheck): the CFL time step of the current state.
+ * Driver_computeDt.F90:306 calls Hydro_computeDt once per leaf block: the
+ * first call after the state changed (a step, an attach, Eos, a regrid)
+ * reduces on the device and synchronises; later calls return the cached
+ * result (and the cached location, once one was computed) with no launch and
+ * no synchronisation (fxb_counters counts both kinds).
  * loc[5] receives, when loc is not NULL, the limiting cell as
  * Hydro_computeDt.F90:231-235 records it: i, j, k in the block's 1-based
  * guard-inclusive index space and the refinement level; the fifth entry is
@@ -248,6 +262,14 @@ int fxb_regrid(const fxb_block_desc *blocks, int nblk);
  * (FXB_EARG with *nout set when cap is too small). */
 int fxb_refine_derefine(const fxb_domain *domain, const fxb_block_desc *leaves, int n, const int *flags,
                         int lrefine_min, int lrefine_max, fxb_block_desc *out, int cap, int *nout);
+/* Call counters, cumulative since fxb_init (no reference counterpart). */
+#define FXB_COUNT_STEPS      0   /* hydro steps: fxb_hydro_step calls and fxb_advance steps  */
+#define FXB_COUNT_DT_DEVICE  1   /* fxb_compute_dt calls that read the device (reduction, sync) */
+#define FXB_COUNT_DT_CACHED  2   /* fxb_compute_dt calls answered from the cached result     */
+#define FXB_COUNT_GC_FILLS   3   /* fxb_fill_guardcells / fxb_sync_to_host copies to the host */
+#define FXB_COUNT_GC_DOUBLES 4   /* doubles those copies moved device -> host                */
+#define FXB_NCOUNTERS        5
+int fxb_counters(long long counts[FXB_NCOUNTERS]);
 /* Volume integrals of caller-owned device arrays without allocating any
  * device memory (no counterpart in the reference: an addition of this
  * library).  For callers that cannot call cudaMalloc, e.g. a Fortran code
@@ -257,8 +279,12 @@ int fxb_refine_derefine(const fxb_domain *domain, const fxb_block_desc *leaves, 
  * default stream) and not synchronised.  Scratch lives in a fixed static
  * device array (8192 partial sums of 4096 cells: at most 33,554,432 cells,
  * larger ncell is rejected with FXB_EARG).  The first call on each device
- * looks up that array's address, so make it before any stream capture;
- * calls that overlap on one GPU race on the shared array. */
+ * looks up that array's address, so make it before any stream capture; the
+ * address stays cached for the process, so do not call it on a device after
+ * a cudaDeviceReset of that device.  Calls that overlap on one GPU race on
+ * the shared array: serialise them.  Results are deterministic for a given
+ * ncell but differ from fxb_integrals' by roundoff (another summation
+ * order). */
 int fxb_integrals_noalloc(const double *dens, const double *velx, const double *vely,
                           const double *velz, const double *ener, const double *eint,
                           long ncell, double cell_volume, double *out_dev, void *stream);

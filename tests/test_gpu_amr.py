@@ -113,6 +113,32 @@ def test_amr_guard_fill_matches_oracle(oracle, need_gpu):
     dev.close()
 
 
+def test_amr_masked_fill_and_doeos(oracle, need_gpu):
+    """Grid_fillGuardCells on an AMR mesh with a mask: the selected variables
+    equal the oracle's fill and nothing else is written; doEos=False skips
+    Eos_guardCells on the guard regions next to other levels
+    (Paramesh4/Grid_fillGuardCells.F90:531-548), which leaves densities and
+    interiors as they are and changes pressures only in guard cells."""
+    from flashx_b200.params import NUNK
+    root, hp, mesh, unk = _case(maxlev=3)
+    am = oracle.Amr(oracle.make_params(root.as_dict(), hp), mesh.levels, mesh.bcoords)
+    ref = unk.copy()
+    am.fill_guardcells(ref)
+    dev = HydroDevice(root, hp, "fp64", mesh=mesh)
+    dev.attach_unk(unk.copy())
+    out = np.full(unk.shape, -7.0)
+    dev.Grid_fillGuardCells(out, mask=["dens", "pres"])
+    sel, rest = [DENS, PRES], [v for v in range(NUNK) if v not in (DENS, PRES)]
+    np.testing.assert_array_equal(out[..., sel], ref[..., sel])
+    assert np.all(out[..., rest] == -7.0)
+    noeos = np.full(unk.shape, -7.0)
+    dev.Grid_fillGuardCells(noeos, mask=["dens", "pres"], doEos=False)
+    np.testing.assert_array_equal(noeos[..., DENS], ref[..., DENS])
+    np.testing.assert_array_equal(_interior(root, noeos)[..., [0, 5]], _interior(root, ref)[..., [0, 5]])
+    assert np.any(noeos[..., PRES] != ref[..., PRES])
+    dev.close()
+
+
 def test_amr_batches_agree(oracle, need_gpu):
     """Leaves processed in several batches (guard fill, fluxes, then a second
     pass for the leaves whose fluxes are corrected) give the one-batch result."""

@@ -159,6 +159,70 @@ def test_fill_guardcells_matches_oracle(oracle, need_gpu, bc):
     assert np.array_equal(out[..., HYDRO_VARS], ref[..., HYDRO_VARS])
 
 
+@pytest.mark.parametrize("bc", [BC_OUTFLOW, BC_REFLECTING, BC_PERIODIC])
+def test_masked_fill_guardcells(oracle, need_gpu, bc):
+    """Grid_fillGuardCells with a mask: only the selected variables cross
+    PCIe and are written (equal to the oracle's fill); every other UNK entry
+    keeps its host value."""
+    from flashx_b200.hydro import COUNT_GC_DOUBLES, COUNT_GC_FILLS
+    geom = Geometry(2, 16, 16, 1, 2, 3, 1, bc=(bc,) * 6)
+    hp = HydroParams()
+    unk = S.kelvin_helmholtz(geom, hp)
+    p = oracle.make_params(geom.as_dict(), hp)
+    ref = unk.copy()
+    oracle.fill_guardcells(p, ref)
+    dev = HydroDevice(geom, hp)
+    dev.attach_unk(unk.copy())
+    c0 = dev.counters()
+    out = np.full(geom.unk_shape, -7.0)
+    dev.Grid_fillGuardCells(out, mask=["dens", "pres", "velx"])
+    c1 = dev.counters()
+    sel = [DENS, PRES, VELX]
+    rest = [v for v in range(NUNK) if v not in sel]
+    assert np.array_equal(out[..., sel], ref[..., sel])
+    assert np.all(out[..., rest] == -7.0)
+    ncell = out.size // NUNK
+    assert c1[COUNT_GC_FILLS] - c0[COUNT_GC_FILLS] == 1
+    assert c1[COUNT_GC_DOUBLES] - c0[COUNT_GC_DOUBLES] == 3 * ncell
+    # no mask: every hydro variable, as before
+    out2 = np.full(geom.unk_shape, -7.0)
+    dev.Grid_fillGuardCells(out2, doEos=False)
+    assert np.array_equal(out2[..., HYDRO_VARS], ref[..., HYDRO_VARS])
+    with pytest.raises(ValueError):
+        dev.Grid_fillGuardCells(out2, mask=["shok"])
+    dev.close()
+
+
+@pytest.mark.parametrize("name", ["kh2d", "sweep3d"])
+def test_compute_dt_once_per_step(oracle, need_gpu, name):
+    """Driver_computeDt calls Hydro_computeDt once per leaf block
+    (Driver_computeDt.F90:306): the first call after a state change reduces
+    on the device, every later call returns the cached global dt (and
+    dtMinLoc) without a launch or a host synchronisation."""
+    from flashx_b200.hydro import COUNT_DT_CACHED, COUNT_DT_DEVICE
+    geom, hp, init = S.config(name, scale=0.25 if name == "kh2d" else 0.5)
+    unk = init(geom, hp)
+    dev = HydroDevice(geom, hp, "fp64")
+    dev.attach_unk(unk.copy())
+    p = oracle.make_params(geom.as_dict(), hp)
+    for step in range(3):
+        c0 = dev.counters()
+        dtcheck, loc = 1e30, None
+        for _ in range(geom.nblocks):                        # Driver_computeDt's block loop
+            dt_b, loc_b = dev.Hydro_computeDt(location=True)
+            if dt_b < dtcheck:
+                dtcheck, loc = dt_b, loc_b
+        c1 = dev.counters()
+        assert c1[COUNT_DT_DEVICE] - c0[COUNT_DT_DEVICE] == 1
+        assert c1[COUNT_DT_CACHED] - c0[COUNT_DT_CACHED] == geom.nblocks - 1
+        host = np.zeros(geom.unk_shape)
+        dev.sync_to_host(host)
+        assert dtcheck == oracle.compute_dt(p, host)
+        assert loc == _expected_loc(geom, host)
+        dev.Hydro(0.0, 0.5 * dtcheck, 0.5 * dtcheck)
+    dev.close()
+
+
 def test_compute_dt_and_device_driver_loop(oracle, need_gpu):
     """Hydro_computeDt equals the oracle's; the graph-captured device driver
     loop (fxb_advance) reproduces the host-driven loop exactly."""

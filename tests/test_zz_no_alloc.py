@@ -52,6 +52,26 @@ def test_integrals_without_allocation_match_fxb_integrals(need_gpu):
         torch.cuda.synchronize()
         got = out.cpu().numpy()
         assert np.allclose(got, ref, rtol=RTOL, atol=1e-14 * abs(ref[0])), (call, got, ref)
+    # a size that is not a whole number of 4096-cell chunks (the last CTA sums
+    # a partial chunk), on a non-default stream, against float64 NumPy sums
+    n = geom.ncells - 1000
+    dv = dx * dy * dz
+    c = {v: np.ascontiguousarray(g[..., v]).ravel()[:n] for v in (DENS, VELX, VELY, VELZ, ENER, EINT)}
+    rho, vx, vy, vz = c[DENS], c[VELX], c[VELY], c[VELZ]
+    expect = np.array([np.sum(rho * dv), np.sum(rho * vx * dv), np.sum(rho * vy * dv), np.sum(rho * vz * dv),
+                       np.sum(rho * c[ENER] * dv), np.sum(rho * c[EINT] * dv),
+                       np.sum(0.5 * rho * (vx * vx + vy * vy + vz * vz) * dv)])
+    side = torch.cuda.Stream()
+    for call in range(2):
+        out.fill_(float("nan"))
+        torch.cuda.synchronize()
+        rc = lib.fxb_integrals_noalloc(ptr(cols[DENS]), ptr(cols[VELX]), ptr(cols[VELY]), ptr(cols[VELZ]),
+                                       ptr(cols[ENER]), ptr(cols[EINT]), n, dv, ptr(out),
+                                       ctypes.c_void_p(side.cuda_stream))
+        assert rc == FXB_OK
+        side.synchronize()
+        got = out.cpu().numpy()
+        assert np.allclose(got, expect, rtol=RTOL, atol=1e-14 * abs(expect[0])), (call, got, expect)
     # sizes beyond the static scratch are rejected with a clear error, before any launch
     rc = lib.fxb_integrals_noalloc(ptr(cols[DENS]), ptr(cols[VELX]), ptr(cols[VELY]), ptr(cols[VELZ]),
                                    ptr(cols[ENER]), ptr(cols[EINT]), 8192 * 4096 + 1, 1.0, ptr(out), None)
