@@ -384,7 +384,7 @@ def per_block_driver(dev, geom, mesh, hp, steps, global_min):
     el = time.perf_counter() - t0
     c1 = dev.counters()
     return {"value": geom_zones(geom, mesh) * steps / el, "unit": UNIT, "steps": steps,
-            "h2d_bytes_per_step": 24, "d2h_bytes_per_step": 8 + 28 * nblk,
+            "h2d_bytes_per_step": 24, "d2h_bytes_per_step": 16,
             "hydro_computeDt_calls_per_step": nblk,
             "device_dt_reductions_per_step": (c1[COUNT_DT_DEVICE] - c0[COUNT_DT_DEVICE]) / steps,
             "cached_dt_calls_per_step": (c1[COUNT_DT_CACHED] - c0[COUNT_DT_CACHED]) / steps,
