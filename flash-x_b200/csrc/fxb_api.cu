@@ -7,7 +7,9 @@
 #include "fxb_amr.h"
 
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 #include <math.h>
 
@@ -72,6 +74,10 @@ struct Lib {
     void *slp3 = nullptr;          // PPM slopes of one direction (3-D)
     void *flat = nullptr;          // flattening coefficients (2-D and 3-D)
     void *hyb = nullptr;           // hybrid order (3-D): DivU and the per-cell flags
+    CUtensorMap tmap2d[2];         // 2-D: the window variables of buf[0] / buf[1] for TMA
+    int use_tma = 1;
+    unsigned tma_extra_tx = 0;     // test hook (FXB_TEST_WAIT_TIMEOUT): a window barrier that never completes
+    long long wait_budget = kTmaWaitBudget;
     fxb_error lasterr{};
 };
 Lib L;
@@ -306,6 +312,32 @@ int int_nz() { return L.dom.ndim == 3 ? L.nint : 1; }
 bool has_halo() { return L.slab.halo_lo > 0 || L.slab.halo_hi > 0; }
 
 
+// tensor map of the 2-D kernel's window: the first 8 device variables of a
+// state buffer as a [var][y][x] FP64 tensor (rows of nx, variables vstride
+// apart), boxes of 8 x 22 x 24 (cuTensorMapEncodeTiled, reached through the
+// runtime's driver entry point so the library needs no link to libcuda)
+int encode_window_map(CUtensorMap *m, const double *base)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+    if (!enc) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+            return fail(FXB_ECUDA, "fxb_init: cuTensorMapEncodeTiled not available from the driver");
+        enc = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    const cuuint64_t dims[3] = {(cuuint64_t)L.nx, (cuuint64_t)L.ny, 8};
+    const cuuint64_t strides[2] = {(cuuint64_t)L.nx * sizeof(double), (cuuint64_t)L.vstride * sizeof(double)};
+    const cuuint32_t box[3] = {(cuuint32_t)WP, (cuuint32_t)WIN, 8};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(FXB_ECUDA, "fxb_init: cuTensorMapEncodeTiled rejected the window map");
+    return FXB_OK;
+}
+
 // launch one fused hydro step reading buffer `src`, writing 1-src
 int launch_hydro(int src, const double *dtv, double dt)
 {
@@ -321,6 +353,10 @@ int launch_hydro(int src, const double *dtv, double dt)
         a.gam1inv = L.gam1inv; a.ggprodinv = L.ggprodinv;
         a.prm = L.dprm; a.rate_max = L.rate_max; a.err = L.err;
         a.flat = L.flat;
+        a.tmap = L.tmap2d[src];
+        a.use_tma = L.use_tma;
+        a.tma_extra_tx = L.tma_extra_tx;
+        a.wait_budget = L.wait_budget;
         dim3 grid(L.nx / T2, L.ny / T2);
         if (L.prm.precision == FXB_MIXED) launch_hydro2d_mixed(a, grid, L.stream);
         else launch_hydro2d_fp64(a, grid, L.stream);
@@ -371,6 +407,7 @@ int check_err_word()
         if (h & ERR_RIEMANN) return fail(FXB_ERIEMANN, "[hy_getFaceFlux]: Riemann solver returned ierr /= 0");
         if (h & 8) return fail(FXB_EDT, "[Hydro]: Computed dt is not positive! Aborting!");
         if (h & 16) return fail(FXB_EARG, "[Grid_fillGuardCells]: AMR guard cell without a covering block");
+        if (h & ERR_TIMEOUT) return fail(FXB_ETIMEOUT, "[Hydro]: a bounded device wait ran out (data never arrived)");
         return fail(FXB_ECUDA, "device error word set");
     }
     return FXB_OK;
@@ -525,6 +562,10 @@ extern "C" int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
         cudaGetLastError();
         return fail(FXB_ECUDA, "fxb_init: no CUDA device visible");
     }
+    // FXB_TEST_WAIT_TIMEOUT=1 (tests only): window barriers expect 8 bytes
+    // more than the box brings, so their bounded waits run out after ~0.5 ms
+    const char *tw = getenv("FXB_TEST_WAIT_TIMEOUT");
+    if (tw && tw[0] == '1') { L.tma_extra_tx = 8; L.wait_budget = 1000000; }
     CK(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&L.ev0));
     CK(cudaEventCreate(&L.ev1));
@@ -551,6 +592,13 @@ extern "C" int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
     if (d.ndim == 2) {
         CK(setup_hydro2d_fp64());
         CK(setup_hydro2d_mixed());
+        for (int i = 0; i < 2; i++) {
+            int rc = encode_window_map(&L.tmap2d[i], L.buf[i]);
+            if (rc) return rc;
+        }
+        // FXB_TMA=0 stages every window with per-thread loads (for comparisons)
+        const char *tv = getenv("FXB_TMA");
+        L.use_tma = !(tv && tv[0] == '0');
     } else {
         CK(setup_hydro3d_fp64());
         CK(setup_hydro3d_mixed());

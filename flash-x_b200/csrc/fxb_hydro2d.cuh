@@ -13,6 +13,10 @@
 //
 // Stages (s = shared memory, R = reconstruction type):
 //   A  load the 22x22 window (tile + 3 halo) of D,VX,VY,VZ,P,GC,GE,EI -> s.V
+//      (tiles whose window lies inside the stored grid: one TMA box
+//      [8][22][24] starting one column left of the window, so that its x
+//      origin is 16-byte aligned; tiles at the grid's edge: per-thread loads
+//      with the boundary conditions resolved by map_axis)
 //   B  x: eigensystem + limited slopes of cells i=-2..17, j=0..15      -> s.DB
 //   C  x: PPM/WENO face states of i=-1..16, j=0..15, minus dt/2dy*sig_y -> s.W
 //   D  x: HLLC/HLL on faces i=0..16                                     -> s.F
@@ -21,10 +25,15 @@
 //   I  owner threads: y update, energyFix, Eos, store, CFL rate max
 #pragma once
 #include "fxb_device.cuh"
+#include "fxb_tma.cuh"
 
 namespace fxb {
 
-struct Args2D {
+struct alignas(64) Args2D {
+    CUtensorMap tmap;        // the 8 window variables of `in` as [var][y][x] (built by the host)
+    int use_tma;             // stage interior windows by TMA (else per-thread loads everywhere)
+    unsigned tma_extra_tx;   // test hook: bytes the barrier expects beyond the box (0)
+    long long wait_budget;   // clock cycles a CTA waits for its window before ERR_TIMEOUT
     const double *in;
     double *out;
     long vstride;            // elements between variables
@@ -43,6 +52,8 @@ struct Args2D {
 
 constexpr int T2 = 16;             // tile edge
 constexpr int WIN = T2 + 6;        // window edge
+constexpr int WP = WIN + 2;        // stored row: one column left of the window (TMA x alignment) and one right
+constexpr int XO = 1;              // stored column of window column 0
 // Threads per CTA.  Two CTAs share an SM's 64K registers, so the count sets
 // the register budget.  320 threads (10 warps, 96 registers) measured fastest
 // for both precisions on B200: 288 threads (112 registers) cannot place 18
@@ -70,7 +81,7 @@ template <class R> struct KeepOwn { static constexpr bool value = sizeof(R) == 4
 constexpr int NOWN = T2 * T2;      // owner cells of a tile
 
 template <class R> struct Smem2D {
-    R V[8][WIN][WIN];
+    R V[8][WIN][WP];
     R DBF[NF * NFC];               // slopes [6][NDB], then fluxes [8][NFC]
     R SG[6][NDB];                  // sigma of the other direction at the slope cells (global order)
     R W[12][NW];                   // Wp (D,VX,VY,VZ,P,EI), then Wm
@@ -99,8 +110,8 @@ template <class R> __device__ __forceinline__ void unrot(int dir, const R *r, R 
 
 template <class R> __device__ __forceinline__ void win6(const Smem2D<R> &s, int wx, int wy, R *g)
 {
-    g[0] = s.V[D][wy][wx]; g[1] = s.V[VX][wy][wx]; g[2] = s.V[VY][wy][wx];
-    g[3] = s.V[VZ][wy][wx]; g[4] = s.V[P][wy][wx]; g[5] = s.V[EI][wy][wx];
+    g[0] = s.V[D][wy][wx + XO]; g[1] = s.V[VX][wy][wx + XO]; g[2] = s.V[VY][wy][wx + XO];
+    g[3] = s.V[VZ][wy][wx + XO]; g[4] = s.V[P][wy][wx + XO]; g[5] = s.V[EI][wy][wx + XO];
 }
 
 __device__ __forceinline__ void set_err(int *err, int code) { atomicOr(err, code); }
@@ -116,7 +127,7 @@ __device__ __forceinline__ void analysis_stage(const Args2D &a, Smem2D<R> &s, in
     win6(s, wx, wy, g);
     // one eigensystem base for the slope direction and the transverse one
     EigBase<R> eb;
-    if (!eigen_base(g[0], g[4], s.V[GC][wy][wx], eb)) set_err(a.err, ERR_SOUND);
+    if (!eigen_base(g[0], g[4], s.V[GC][wy][wx + XO], eb)) set_err(a.err, ERR_SOUND);
     if (KeepOwn<R>::value) { s.EB[0][t] = eb.cf; s.EB[1][t] = eb.ahinv; s.EB[2][t] = eb.lp; s.EB[3][t] = eb.a2inv; }
     if (ppm) {
         const int ox = dir == 0, oy = dir == 1;
@@ -145,7 +156,7 @@ __device__ __forceinline__ void analysis_stage(const Args2D &a, Smem2D<R> &s, in
 // state through the boundary map when it lies outside the window
 template <class R> __device__ __forceinline__ R vel2d(const Args2D &a, const Smem2D<R> &s, int q, int wx, int wy)
 {
-    if (wx >= 0 && wx < WIN && wy >= 0 && wy < WIN) return s.V[q][wy][wx];
+    if (wx >= 0 && wx < WIN && wy >= 0 && wy < WIN) return s.V[q][wy][wx + XO];
     double sx = 1.0, sy = 1.0;
     const int gx = (int)(blockIdx.x * T2) + wx - 3, gy = (int)(blockIdx.y * T2) + wy - 3;
     const int mx = map_axis(gx, a.nx, a.bc[0], a.bc[1], &sx), my = map_axis(gy, a.ny, a.bc[2], a.bc[3], &sy);
@@ -180,7 +191,7 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
         eb.rho = Vc[0];
         eb.rp = eb.rho * (eb.cf * eb.cf);
         eigen_dir(eb, Vc[1], e);
-    } else if (!eigen(Vc[0], Vc[1], Vc[4], s.V[GC][wy][wx], e)) {
+    } else if (!eigen(Vc[0], Vc[1], Vc[4], s.V[GC][wy][wx + XO], e)) {
         set_err(a.err, ERR_SOUND);
     }
     if (EXT && a.prm.order == 2) {
@@ -216,8 +227,8 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
         }
         ppm_interfaces(Vm, Vc, Vp, dbN, db0, dbP, vecL, vecR);
         if (EXT && a.prm.steepening)
-            steepen(R(a.prm.tiny), R(dir == 0 ? a.dx : a.dy), s.V[D][wy - 2 * oy][wx - 2 * ox], Vm, Vc, Vp,
-                    s.V[D][wy + 2 * oy][wx + 2 * ox], s.V[GE][wy][wx], dbN[0], dbP[0], vecL, vecR);
+            steepen(R(a.prm.tiny), R(dir == 0 ? a.dx : a.dy), s.V[D][wy - 2 * oy][wx - 2 * ox + XO], Vm, Vc, Vp,
+                    s.V[D][wy + 2 * oy][wx + 2 * ox + XO], s.V[GE][wy][wx + XO], dbN[0], dbP[0], vecL, vecR);
     }
     if (a.prm.flattening) {
         // the window origin is the tile origin minus three cells
@@ -231,13 +242,13 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
     }
     if (EXT && a.prm.use_hybrid) {
         const int k4 = a.prm.order - 1 > 2 ? 2 : a.prm.order - 1;
-        const R eps = hybrid_eps(a.prm, s.V[D][wy][wx], s.V[P][wy][wx], s.V[GC][wy][wx]);
+        const R eps = hybrid_eps(a.prm, s.V[D][wy][wx + XO], s.V[P][wy][wx + XO], s.V[GC][wy][wx + XO]);
         R mn = divu2d(a, s, wx - k4, wy - k4);
         for (int jj = -k4; jj <= k4; jj++)
             for (int ii = -k4; ii <= k4; ii++) mn = fmin(mn, divu2d(a, s, wx + ii, wy + jj));
         if (mn < eps) {
             win6(s, wx, wy, g);
-            hybrid_rh(2, g, g, s.V[GC][wy][wx], Wm, Wp);
+            hybrid_rh(2, g, g, s.V[GC][wy][wx + XO], Wm, Wp);
         }
     }
     // transverse flux of the other direction at this cell (from the analysis stage)
@@ -283,42 +294,91 @@ __device__ __forceinline__ void faces_stage(const Args2D &a, Smem2D<R> &s, int d
     R VL[6], VR[6], F[8];
 #pragma unroll
     for (int k = 0; k < 6; k++) { VL[k] = s.W[k][wl]; VR[k] = s.W[6 + k][wr]; }
-    int e = riemann<R, EXT>(a.prm, dir, VL, s.V[GC][wyl][wxl], s.V[GE][wyl][wxl],
-                    VR, s.V[GC][wyr][wxr], s.V[GE][wyr][wxr], F);
+    int e = riemann<R, EXT>(a.prm, dir, VL, s.V[GC][wyl][wxl + XO], s.V[GE][wyl][wxl + XO],
+                    VR, s.V[GC][wyr][wxr + XO], s.V[GE][wyr][wxr + XO], F);
     if (e) set_err(a.err, e);
     if (EXT && a.prm.use_avisc) {
         const int td = 1 - dir, tx = td == 0, ty = td == 1, vt = td == 0 ? VX : VY, vn = dir == 0 ? VX : VY;
         const R del[2] = {R(a.dx), R(a.dy)};
         R tr[3] = {R(0.), R(0.), R(0.)};
-        tr[td] = R(0.25) * (s.V[vt][wyr + ty][wxr + tx] - s.V[vt][wyr - ty][wxr - tx] + s.V[vt][wyl + ty][wxl + tx] -
-                            s.V[vt][wyl - ty][wxl - tx]) * del[dir] / del[td];
-        const R Ul[5] = {s.V[D][wyl][wxl], s.V[VX][wyl][wxl], s.V[VY][wyl][wxl], s.V[VZ][wyl][wxl], ener2d<R>(a, wxl, wyl)};
-        const R Ur[5] = {s.V[D][wyr][wxr], s.V[VX][wyr][wxr], s.V[VY][wyr][wxr], s.V[VZ][wyr][wxr], ener2d<R>(a, wxr, wyr)};
-        avisc_flux(R(a.prm.cvisc), dir, 2, s.V[vn][wyl][wxl], s.V[vn][wyr][wxr], tr, Ul, Ur, F);
+        tr[td] = R(0.25) * (s.V[vt][wyr + ty][wxr + tx + XO] - s.V[vt][wyr - ty][wxr - tx + XO] + s.V[vt][wyl + ty][wxl + tx + XO] -
+                            s.V[vt][wyl - ty][wxl - tx + XO]) * del[dir] / del[td];
+        const R Ul[5] = {s.V[D][wyl][wxl + XO], s.V[VX][wyl][wxl + XO], s.V[VY][wyl][wxl + XO], s.V[VZ][wyl][wxl + XO], ener2d<R>(a, wxl, wyl)};
+        const R Ur[5] = {s.V[D][wyr][wxr + XO], s.V[VX][wyr][wxr + XO], s.V[VY][wyr][wxr + XO], s.V[VZ][wyr][wxr + XO], ener2d<R>(a, wxr, wyr)};
+        avisc_flux(R(a.prm.cvisc), dir, 2, s.V[vn][wyl][wxl + XO], s.V[vn][wyr][wxr + XO], tr, Ul, Ur, F);
         eint_fluxes(a.prm, VL, VR, F);
     }
 #pragma unroll
     for (int k = 0; k < NF; k++) s.DBF[k * NFC + t] = F[k];
 }
 
+// dynamic shared memory of one CTA: the stages' arrays plus 128 bytes to
+// align them for TMA
+template <class R> constexpr int smem2d_bytes() { return (int)sizeof(Smem2D<R>) + 128; }
+// bytes of one TMA window box: 8 variables x 22 rows x 24 columns of FP64
+constexpr unsigned kWinBoxBytes = 8u * WIN * WP * 8u;
+// the FP32 kernel stages the FP64 box in the region of its slopes, sigmas,
+// face states and eigensystem bases (unused during stage A), which follows
+// the window at a 128-byte aligned offset
+static_assert(sizeof(float) * 8 * WIN * WP % 128 == 0, "FP32 window size keeps the staging area aligned");
+static_assert(sizeof(float) * (NF * NFC + 6 * NDB + 12 * NW + 4 * NDB) >= kWinBoxBytes,
+              "FP32 staging area holds the FP64 window box");
+
 template <class R, bool EXT>
-__global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::value) hydro2d_kernel(const Args2D a)
+__global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::value)
+hydro2d_kernel(const __grid_constant__ Args2D a)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    Smem2D<R> &s = *reinterpret_cast<Smem2D<R> *>(smem_raw);
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // 128-byte aligned base (the TMA destination); the launch adds 128 bytes
+    unsigned char *base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+    Smem2D<R> &s = *reinterpret_cast<Smem2D<R> *>(base);
+    __shared__ __align__(8) uint64_t wbar;
     constexpr int NT2 = Threads2D<R>::value;
     const int tid = threadIdx.x;
     const int tx0 = blockIdx.x * T2, ty0 = blockIdx.y * T2;
     const double dt = a.dtv ? a.dtv[0] : a.dt_arg;
 
-    // ---- A: window load with guard cells resolved on the fly.  All of a
-    // thread's loads are issued before any is consumed, so they are in flight
-    // together; owner threads also fetch the FP64 update inputs.
-    constexpr int NEL = 8 * WIN * WIN, NLD = (NEL + NT2 - 1) / NT2;
+    // ---- A: window load.  Interior windows: one TMA box (columns tx0-4 ..
+    // tx0+19, rows ty0-3 .. ty0+18, the 8 variables) issued by thread 0 while
+    // the owner threads fetch their FP64 update inputs.  Edge windows: every
+    // cell through map_axis, all of a thread's loads in flight together.
     const bool owner = tid < NOWN;
     const int oi = tid % T2, oj = tid / T2;
     const long gidx = (long)(ty0 + oj) * a.nx + (tx0 + oi);
-    {
+    const bool tma = a.use_tma && tx0 >= 4 && tx0 + T2 + 4 <= a.nx && ty0 >= 3 && ty0 + T2 + 3 <= a.ny;
+    bool ok = true;
+    if (tma) {
+        double *stage = sizeof(R) == 8 ? reinterpret_cast<double *>(&s.V[0][0][0])
+                                       : reinterpret_cast<double *>(&s.DBF[0]);
+        if (tid == 0) mbar_init(&wbar, 1);
+        __syncthreads();
+        if (tid == 0) {
+            mbar_arrive_expect_tx(&wbar, kWinBoxBytes + a.tma_extra_tx);
+            tma_load_3d(stage, &a.tmap, tx0 - 4, ty0 - 3, 0, &wbar);
+        }
+        double own0 = 0.;
+        if (owner) own0 = __ldg(a.in + DV_ENER * a.vstride + gidx);
+        ok = mbar_wait_bounded(&wbar, 0, a.wait_budget, a.err);
+        if (owner) s.OWN[0][tid] = own0;
+        if constexpr (sizeof(R) == 4) {
+            // the FP64 update inputs of the owner cells come from the box exactly
+            if (owner) {
+                const int c = ((oj + 3) * WP) + oi + 3 + XO;
+                s.OWN[KeepOwn<R>::value ? 1 : 0][tid] = stage[D * WIN * WP + c];
+                s.OWN[KeepOwn<R>::value ? 2 : 0][tid] = stage[VX * WIN * WP + c];
+                s.OWN[KeepOwn<R>::value ? 3 : 0][tid] = stage[VY * WIN * WP + c];
+                s.OWN[KeepOwn<R>::value ? 4 : 0][tid] = stage[VZ * WIN * WP + c];
+                s.OWN[KeepOwn<R>::value ? 5 : 0][tid] = stage[EI * WIN * WP + c];
+            }
+            constexpr int NEL = 8 * WIN * WIN;
+            for (int e = tid; e < NEL; e += NT2) {
+                const int v = e / (WIN * WIN), r = e - v * (WIN * WIN);
+                const int wy = r / WIN, wx = r - wy * WIN;
+                s.V[v][wy][wx + XO] = (R)stage[(v * WIN + wy) * WP + wx + XO];
+            }
+        }
+    } else {
+        constexpr int NEL = 8 * WIN * WIN, NLD = (NEL + NT2 - 1) / NT2;
         double buf[NLD];
 #pragma unroll
         for (int q = 0; q < NLD; q++) {
@@ -351,7 +411,7 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
             if (e < NEL) {
                 int v = e / (WIN * WIN), r = e - v * (WIN * WIN);
                 int wy = r / WIN, wx = r - wy * WIN;
-                s.V[v][wy][wx] = (R)buf[q];
+                s.V[v][wy][wx + XO] = (R)buf[q];
             }
         }
         if (owner) {
@@ -359,7 +419,8 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
             for (int q = 0; q < (KeepOwn<R>::value ? 6 : 1); q++) s.OWN[q][tid] = own[q];
         }
     }
-    __syncthreads();
+    // a window that did not arrive in time ends the tile (ERR_TIMEOUT is set)
+    if (__syncthreads_or(!ok)) return;
 
     const R dtnx = R(dt / a.dx), hdtnx = R(0.5 * (dt / a.dx));
     const R dtny = R(dt / a.dy), hdtny = R(0.5 * (dt / a.dy));
@@ -395,9 +456,9 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
             vy = s.OWN[KeepOwn<R>::value ? 3 : 0][tid]; vz = s.OWN[KeepOwn<R>::value ? 4 : 0][tid];
             eint0 = s.OWN[KeepOwn<R>::value ? 5 : 0][tid];
         } else {   // the FP64 window holds these values exactly
-            dens0 = (double)s.V[D][oj + 3][oi + 3]; vx = (double)s.V[VX][oj + 3][oi + 3];
-            vy = (double)s.V[VY][oj + 3][oi + 3]; vz = (double)s.V[VZ][oj + 3][oi + 3];
-            eint0 = (double)s.V[EI][oj + 3][oi + 3];
+            dens0 = (double)s.V[D][oj + 3][oi + 3 + XO]; vx = (double)s.V[VX][oj + 3][oi + 3 + XO];
+            vy = (double)s.V[VY][oj + 3][oi + 3 + XO]; vz = (double)s.V[VZ][oj + 3][oi + 3 + XO];
+            eint0 = (double)s.V[EI][oj + 3][oi + 3 + XO];
         }
         U0[0] = dens0; U0[1] = vx * dens0; U0[2] = vy * dens0; U0[3] = vz * dens0; U0[4] = dens0 * en;
         int fl = oj * (T2 + 1) + oi, fr = fl + 1;
@@ -459,7 +520,7 @@ __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::va
 #pragma unroll
             for (int q = 0; q < 3; q++)
                 vold[q] = KeepOwn<R>::value ? s.OWN[KeepOwn<R>::value ? 2 + q : 0][tid]
-                                            : (double)s.V[VX + q][oj + 3][oi + 3];
+                                            : (double)s.V[VX + q][oj + 3][oi + 3 + XO];
             const double momOld[3] = {vold[0] * dens0, vold[1] * dens0, vold[2] * dens0};
             for (int q = 0; q < 3; q++) U0[1 + q] = U0[1 + q] + 0.5 * dt * dens0 * prm.grav[q];
             double dp = 0.;

@@ -21,7 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.normpath(os.path.join(HERE, "..", "libflashx_b200.so"))
 BUILD_DIR = os.path.normpath(os.path.join(HERE, ".."))
 
-FXB_OK, FXB_EARG, FXB_ECUDA, FXB_ESOUND, FXB_ERIEMANN, FXB_EDT, FXB_EUNSUPPORTED = range(7)
+FXB_OK, FXB_EARG, FXB_ECUDA, FXB_ESOUND, FXB_ERIEMANN, FXB_EDT, FXB_EUNSUPPORTED, FXB_ETIMEOUT = range(8)
 FXB_FP64, FXB_MIXED = 0, 1
 # enum fxb_var order of include/flashx_b200.h
 FXB_VARS = ("dens", "eint", "ener", "gamc", "game", "pres", "temp", "velx", "vely", "velz")

@@ -44,6 +44,7 @@ extern "C" {
 #define FXB_ERIEMANN        4   /* Riemann solver ierr (hy_getFaceFlux.F90:337-378) */
 #define FXB_EDT             5   /* computed dt not positive (Hydro_computeDt.F90:286-288) */
 #define FXB_EUNSUPPORTED    6   /* option combination this path does not implement */
+#define FXB_ETIMEOUT        7   /* a bounded device-side wait ran out (TMA window, device-wide barrier) */
 
 /* variables of the UHD + Gamma solution vector, used to index var_map */
 enum fxb_var { FXB_DENS = 0, FXB_EINT, FXB_ENER, FXB_GAMC, FXB_GAME, FXB_PRES,

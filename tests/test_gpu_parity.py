@@ -223,6 +223,53 @@ def test_compute_dt_once_per_step(oracle, need_gpu, name):
     dev.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_tma_window_equals_thread_loads(need_gpu, monkeypatch, precision):
+    """The 2-D kernel stages interior windows by TMA and edge windows with
+    per-thread loads; staging every window with per-thread loads (FXB_TMA=0)
+    gives the same state bit for bit."""
+    geom, hp, init = S.config("kh2d", scale=1 / 8)          # 256^2: 196 of 256 tiles interior
+    unk = init(geom, hp)
+    outs = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("FXB_TMA", flag)
+        dev = HydroDevice(geom, hp, precision)
+        dev.attach_unk(unk.copy())
+        dt = 0.5 * dev.Hydro_computeDt()
+        dev.advance(6, dt, dt)
+        out = np.zeros(geom.unk_shape)
+        dev.sync_to_host(out)
+        dev.close()
+        outs.append(out)
+    assert np.array_equal(outs[0][..., HYDRO_VARS], outs[1][..., HYDRO_VARS])
+
+
+def test_window_wait_timeout_reports_status(oracle, need_gpu, monkeypatch):
+    """A window barrier that never completes (test hook: it expects 8 bytes
+    more than the TMA box brings) ends each waiting tile after its bounded
+    wait with ERR_TIMEOUT; the host reads FXB_ETIMEOUT, and the context stays
+    usable: the next solver instance steps exactly like the oracle."""
+    from flashx_b200.hydro import FXB_ETIMEOUT
+    geom = Geometry(2, 16, 16, 1, 3, 3, 1, bc=(BC_PERIODIC,) * 6)   # one interior (TMA) tile
+    hp = HydroParams()
+    unk = S.kelvin_helmholtz(geom, hp)
+    monkeypatch.setenv("FXB_TEST_WAIT_TIMEOUT", "1")
+    dev = HydroDevice(geom, hp)
+    dev.attach_unk(unk.copy())
+    dt = 0.5 * dev.Hydro_computeDt()
+    dev.Hydro(0.0, dt, dt)
+    with pytest.raises(FlashXError) as ei:
+        dev.Hydro_computeDt()
+    assert ei.value.code == FXB_ETIMEOUT
+    dev.close()
+    monkeypatch.delenv("FXB_TEST_WAIT_TIMEOUT")
+    p = oracle.make_params(geom.as_dict(), hp)
+    ref = oracle_run(oracle, geom, hp, unk, [dt])
+    _, out = gpu_run(geom, hp, unk, [dt])
+    g, r = compare(geom, out, ref)
+    assert np.array_equal(g, r)
+
+
 def test_compute_dt_and_device_driver_loop(oracle, need_gpu):
     """Hydro_computeDt equals the oracle's; the graph-captured device driver
     loop (fxb_advance) reproduces the host-driven loop exactly."""
