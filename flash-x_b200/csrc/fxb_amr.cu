@@ -24,6 +24,8 @@
 // time, sized to the free device memory.
 #include "fxb_amr.h"
 #include "fxb_launch.h"
+#include "fxb_amr_dev.cuh"
+#include "fxb_amr_persist.cuh"
 
 #include <algorithm>
 #include <stdint.h>
@@ -45,27 +47,6 @@ struct HBlock {
     int leaf;        // leaf slot or -1
     int nodetype;    // 1 leaf, 2 parent with a leaf child, 3 other parent
 };
-
-struct DevBlk {
-    int level, c0, c1, c2, parent;
-};
-
-// device-side description of the mesh for the guard-fill kernels
-struct MeshArgs {
-    const DevBlk *blk;
-    const int *ntab;            // [block][27] same-level neighbour, -1 none, -2 boundary
-    const double *store;        // interior store [block][var][cell]
-    long vstride, bstride;      // cells per block, NV_DEV * cells
-    int n, ng;                  // cells per block side, guard layers
-    int nb1[3];                 // root blocks per axis
-    int bc[6];
-    int *err;
-};
-
-constexpr int ERR_AMR = 16;
-// variables of the guard-filled blocks: D..EI, all the 3-D pipeline reads
-// (ENER feeds the guard cells' Eos, TEMP nothing)
-constexpr int NV_GCB = EI + 1;     // guard cell without a covering block (device error word)
 
 struct State {
     bool active = false;
@@ -114,6 +95,18 @@ struct State {
     bool tuned = false;                           // launch shapes chosen (first attach of the mesh)
     char tune_log[256] = "";
     std::unordered_map<uint64_t, int> map;
+    // the step as one persistent kernel over the leaf list (fxb_amr_persist.cuh)
+    bool persist = false;
+    int pgrid = 0;                                // its CTAs, one scratch slot each
+    int *d_order = nullptr;                       // leaves in queue order, finest level first
+    int *d_ctl = nullptr;                         // queue head, completion counters, abort flag
+    int *d_emitted = nullptr;                     // per leaf: boundary fluxes stored
+    int4 *d_ritems = nullptr;                     // restriction items (level, first, last+1)
+    AmrEntry3 *d_slots = nullptr;                 // the leaf each CTA runs
+    int nritem = 0;
+    int rlev_items[32] = {};
+    long long wait_budget = kTmaWaitBudget;
+    int test_stall = 0;                           // test hook (FXB_TEST_WAIT_TIMEOUT)
 };
 State S;
 
@@ -300,171 +293,6 @@ int build_tree(const fxb_block_desc *leaves, int nleaf, std::vector<int> &finer,
     return FXB_OK;
 }
 
-// ------------------------------------------------------------------ device
-__device__ __forceinline__ int fdiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
-
-// PER_MASS variables of UNK (velx vely velz ener eint) in device order
-__device__ __forceinline__ bool per_mass(int v) { return v == VX || v == VY || v == VZ || v == DV_ENER || v == EI; }
-
-// Eos_wrapped(MODE_DENS_EI) of one cell (Gamma/Eos.F90:238-250)
-__device__ void eos_cell_dev(double u[NV_DEV], const DevParams &prm, double gam1inv, double ggprodinv)
-{
-    double ekin = 0.5 * (u[VX] * u[VX] + u[VY] * u[VY] + u[VZ] * u[VZ]);
-    double eint = u[EI];
-    if (u[DV_ENER] - ekin > fmax2(prm.small_e, prm.eint_switch * ekin)) eint = u[DV_ENER] - ekin;
-    double dens = u[D];
-    double pres = dens * eint * gam1inv;
-    u[P] = pres;
-    u[DV_TEMP] = eint * ggprodinv * prm.abar;
-    u[GC] = prm.gamma;
-    u[EI] = eint;
-    u[DV_ENER] = eint + ekin;
-    u[GE] = pres / (eint * dens) + 1;
-}
-
-// non-periodic boundary map of one level-l cell index along axis a
-__device__ __forceinline__ int bc_map(const MeshArgs &m, int lev, int a, int x, double *sg)
-{
-    const int N = (m.nb1[a] << (lev - 1)) * m.n;
-    if (x < 0) {
-        int bc = m.bc[2 * a];
-        if (bc == FXB_BC_OUTFLOW) return 0;
-        if (bc == FXB_BC_REFLECTING) { *sg = -*sg; return -1 - x; }
-    } else if (x >= N) {
-        int bc = m.bc[2 * a + 1];
-        if (bc == FXB_BC_OUTFLOW) return N - 1;
-        if (bc == FXB_BC_REFLECTING) { *sg = -*sg; return 2 * N - 1 - x; }
-    }
-    return x;   // inside, or periodic (left unwrapped: the neighbour table wraps)
-}
-
-// store offset (variable 0) of the level-lev cell x (unwrapped along periodic
-// axes, inside along the others) in the block holding it among block b's 27
-// neighbours, or -1
-__device__ __forceinline__ long same_level_off(const MeshArgs &m, int b, const DevBlk &B, const int x[3])
-{
-    int r[3], loc[3];
-    const int bc[3] = {B.c0, B.c1, B.c2};
-    for (int a = 0; a < 3; a++) {
-        r[a] = fdiv(x[a] - bc[a] * m.n, m.n);
-        if (r[a] < -1 || r[a] > 1) return -1;
-        loc[a] = x[a] - (bc[a] + r[a]) * m.n;
-    }
-    int nb = m.ntab[(long)b * 27 + (r[2] + 1) * 9 + (r[1] + 1) * 3 + (r[0] + 1)];
-    if (nb < 0) return -1;
-    return (long)nb * m.bstride + ((long)loc[2] * m.n + loc[1]) * m.n + loc[0];
-}
-
-// Where the guard value of one cell of a leaf comes from: a same-level cell
-// (a leaf or a restricted parent), or the eight parent-level cells of the
-// prolongation stencil, as store offsets of variable 0, with the sign flips
-// of reflecting boundaries (bit a: the velocity along axis a changes sign).
-enum { GS_SAME = 0, GS_PROL = 1, GS_NONE = 2 };
-struct GuardSrc {
-    int kind;
-    unsigned own;       // flips of the cell's own boundary map
-    unsigned parity;    // prolongation weights: bit a = x[a] & 1
-    unsigned flips;     // prolongation: three flip bits per stencil cell
-    long off[8];
-};
-
-// the prolongation stencil of the level-lev cell x (mapped into the domain) of
-// block B: amr_1blk_cc_prol_linear from the eight parent-level cells
-// floor((x+1)/2)-1 and +1 per axis, found among the parent's neighbours
-__device__ __forceinline__ void prol_resolve(const MeshArgs &m, const DevBlk &B, const int x[3], GuardSrc &gs)
-{
-    gs.kind = GS_NONE;
-    if (B.parent < 0) return;
-    const int pb = B.parent;
-    const DevBlk PB = m.blk[pb];
-    int p1[3];
-    for (int a = 0; a < 3; a++) {
-        p1[a] = fdiv(x[a] + 1, 2) - 1;
-        gs.parity |= (unsigned)(x[a] & 1) << a;
-    }
-#pragma unroll
-    for (int s8 = 0; s8 < 8; s8++) {
-        const int ii = s8 & 1, jj = (s8 >> 1) & 1, kk = s8 >> 2;
-        int q[3] = {p1[0] + ii, p1[1] + jj, p1[2] + kk};
-        double sq[3] = {1., 1., 1.};
-        for (int a = 0; a < 3; a++) q[a] = bc_map(m, PB.level, a, q[a], &sq[a]);
-        gs.off[s8] = same_level_off(m, pb, PB, q);
-        if (gs.off[s8] < 0) return;
-        gs.flips |= ((sq[0] < 0. ? 1u : 0u) | (sq[1] < 0. ? 2u : 0u) | (sq[2] < 0. ? 4u : 0u)) << (3 * s8);
-    }
-    gs.kind = GS_PROL;
-}
-
-__device__ __forceinline__ void guard_resolve(const MeshArgs &m, int b, const int xin[3], GuardSrc &gs)
-{
-    const DevBlk B = m.blk[b];
-    int x[3];
-    double sg[3] = {1., 1., 1.};
-    for (int a = 0; a < 3; a++) x[a] = bc_map(m, B.level, a, xin[a], &sg[a]);
-    gs.own = (sg[0] < 0. ? 1u : 0u) | (sg[1] < 0. ? 2u : 0u) | (sg[2] < 0. ? 4u : 0u);
-    gs.parity = 0; gs.flips = 0;
-    gs.off[0] = same_level_off(m, b, B, x);
-    if (gs.off[0] >= 0) { gs.kind = GS_SAME; return; }
-    prol_resolve(m, B, x, gs);
-}
-
-// same-level guard value: the cell's first NV variables, velocities flipped at reflecting boundaries
-template <int NV = NV_DEV>
-__device__ __forceinline__ void guard_eval_same(const double *store, long vstride, long off, unsigned own,
-                                                double out[NV_DEV])
-{
-    const double *s = store + off;
-#pragma unroll
-    for (int v = 0; v < NV; v++) out[v] = s[v * vstride];
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-        if ((own >> a) & 1u) out[VX + a] = out[VX + a] * -1.;
-}
-
-// prolonged guard value (amr_1blk_cc_prol_linear, conserved form): weights
-// 0.25 / 0.75 by the cell's parity per axis, per-mass variables times the
-// stencil cells' densities, divided by the interpolated density after
-__device__ __forceinline__ void guard_eval_prol(const double *store, long vstride, const long off[8], unsigned flips,
-                                                unsigned parity, unsigned own, double out[NV_DEV])
-{
-    double dn[8];
-#pragma unroll
-    for (int s8 = 0; s8 < 8; s8++) dn[s8] = store[off[s8] + D * vstride];
-    const double wx = (parity & 1u) ? 0.75 : 0.25, wy = ((parity >> 1) & 1u) ? 0.75 : 0.25,
-                 wz = ((parity >> 2) & 1u) ? 0.75 : 0.25;
-    const double dx = wx, cx = 1. - wx, dy = wy, cy = 1. - wy, dz = wz, cz = 1. - wz;
-#pragma unroll
-    for (int v = 0; v < NV_DEV; v++) {
-        double S[8];
-#pragma unroll
-        for (int s8 = 0; s8 < 8; s8++) {
-            double x8 = store[off[s8] + v * vstride];
-            if (v >= VX && v <= VZ && ((flips >> (3 * s8 + v - VX)) & 1u)) x8 = x8 * -1.;
-            S[s8] = per_mass(v) ? dn[s8] * x8 : x8;
-        }
-        // S[(kk*2 + jj)*2 + ii]
-        out[v] = dz * (dy * (dx * S[0] + cx * S[1]) + cy * (dx * S[2] + cx * S[3])) +
-                 cz * (dy * (dx * S[4] + cx * S[5]) + cy * (dx * S[6] + cx * S[7]));
-    }
-    double dinv = out[D] == 0.0 ? 0.0 : 1. / out[D];
-#pragma unroll
-    for (int v = 0; v < NV_DEV; v++)
-        if (per_mass(v)) out[v] = dinv * out[v];
-#pragma unroll
-    for (int a = 0; a < 3; a++)
-        if ((own >> a) & 1u) out[VX + a] = out[VX + a] * -1.;
-}
-
-// guard value of leaf block b at level-lev cell x
-__device__ __forceinline__ bool guard_value(const MeshArgs &m, int b, const int xin[3], double out[NV_DEV])
-{
-    GuardSrc gs;
-    guard_resolve(m, b, xin, gs);
-    if (gs.kind == GS_SAME) guard_eval_same(m.store, m.vstride, gs.off[0], gs.own, out);
-    else if (gs.kind == GS_PROL) guard_eval_prol(m.store, m.vstride, gs.off, gs.flips, gs.parity, gs.own, out);
-    return gs.kind != GS_NONE;
-}
-
 // guard-filled copies of a batch of leaves, in the reconstruction type T:
 // out[entry][var][nz+2g][ny+2g][nx+2g]; with TO_UNK the FP64 values go into
 // UNK staging instead, out[leaf][k][j][i][nunk] at the variables' UNK slots.
@@ -534,22 +362,6 @@ __global__ void __launch_bounds__(256, FXB_FILL_MINB) amr_fill_kernel(MeshArgs m
 // prolongation records in guard-list order.  The step's fill then copies the
 // same-level cells in one light kernel and interpolates the prolonged ones
 // in another, with the arithmetic of the direct path.
-struct GuardPlan {
-    unsigned off;       // same-level source: store offset of variable 0
-    unsigned flags;     // bits 0-2 own flips, bit 3 Eos, bits 4-5 kind
-};
-struct __align__(16) ProlRec {
-    unsigned idx;       // extended-block offset of the guard cell
-    unsigned flags;     // bits 0-2 parity, 3-5 own flips, 6 Eos, 8-31 stencil flips
-    unsigned off[8];    // stencil cells' store offsets (variable 0)
-    unsigned pad[2];
-};
-
-__device__ __forceinline__ void ext_coords(long idx, int ne, int g, int &i, int &j, int &k)
-{
-    i = (int)(idx % ne) - g; j = (int)((idx / ne) % ne) - g; k = (int)(idx / ((long)ne * ne)) - g;
-}
-
 // one CTA per leaf; pass 0 writes the plan and counts the prolonged cells,
 // pass 1 writes the prolongation records at poff[leaf] in guard-list order
 __global__ void __launch_bounds__(256) amr_plan_kernel(MeshArgs m, const int *leaf_blk, const unsigned *eosmask,
@@ -606,49 +418,13 @@ __global__ void __launch_bounds__(256) amr_plan_kernel(MeshArgs m, const int *le
     if (!pass && threadIdx.x == 0) pcount[leaf] = base;
 }
 
-// interior cells and same-level guard cells of a batch from the plan
 template <class T>
 __global__ void __launch_bounds__(256) amr_copy_kernel(MeshArgs m, const AmrEntry3 *entries, const int *leaf_blk,
                                                        const GuardPlan *plan, const int *glist, int nglist, T *out,
                                                        long gvs, long gbs, DevParams prm, double gam1inv,
                                                        double ggprodinv)
 {
-    const AmrEntry3 e = entries[blockIdx.y];
-    const int b = leaf_blk[e.leaf];
-    const int n = m.n, g = m.ng, ne = n + 2 * g;
-    const long nint = (long)n * n * n;
-    const long ncell = nint + nglist;
-    T *dst = out + (long)blockIdx.y * gbs;
-    const GuardPlan *pl = plan + (long)e.leaf * nglist;
-    for (int t = (int)(blockIdx.x * blockDim.x + threadIdx.x); t < (int)ncell; t += (int)(gridDim.x * blockDim.x)) {
-        double u[NV_DEV];
-        int idx;
-        if (t < nint) {
-            int i, j, k;
-            unflatten(t, n, n, i, j, k);
-            idx = ((k + g) * ne + j + g) * ne + i + g;
-            const double *s = m.store + (long)b * m.bstride + t;
-#pragma unroll
-            for (int v = 0; v < NV_GCB; v++) u[v] = s[v * m.vstride];
-        } else {
-            const GuardPlan gp = pl[t - nint];
-            const unsigned kind = (gp.flags >> 4) & 3u;
-            if (kind == GS_PROL) continue;
-            idx = glist[t - nint];
-            if (kind == GS_NONE) {
-                atomicOr(m.err, ERR_AMR);
-#pragma unroll
-                for (int v = 0; v < NV_DEV; v++) u[v] = 0.;
-            } else if ((gp.flags >> 3) & 1u) {
-                guard_eval_same<NV_DEV>(m.store, m.vstride, gp.off, gp.flags & 7u, u);
-                eos_cell_dev(u, prm, gam1inv, ggprodinv);
-            } else {
-                guard_eval_same<NV_GCB>(m.store, m.vstride, gp.off, gp.flags & 7u, u);
-            }
-        }
-#pragma unroll
-        for (int v = 0; v < NV_GCB; v++) dst[v * gvs + idx] = (T)u[v];
-    }
+    amr_copy_kernel_body<T>(hw_block(), m, entries, leaf_blk, plan, glist, nglist, out, gvs, gbs, prm, gam1inv, ggprodinv);
 }
 
 // prolonged guard cells of a batch from the plan's records
@@ -658,21 +434,7 @@ __global__ void __launch_bounds__(256, FXB_FILL_MINB) amr_prolong_kernel(MeshArg
                                                                          long gvs, long gbs, DevParams prm,
                                                                          double gam1inv, double ggprodinv)
 {
-    const AmrEntry3 e = entries[blockIdx.y];
-    const int r0 = poff[e.leaf], r1 = poff[e.leaf + 1];
-    T *dst = out + (long)blockIdx.y * gbs;
-    for (int r = r0 + blockIdx.x * blockDim.x + threadIdx.x; r < r1; r += gridDim.x * blockDim.x) {
-        const uint4 *q = reinterpret_cast<const uint4 *>(prol + r);
-        const uint4 a = q[0], bq = q[1], c = q[2];
-        const long off[8] = {(long)a.z, (long)a.w, (long)bq.x, (long)bq.y, (long)bq.z, (long)bq.w, (long)c.x, (long)c.y};
-        const unsigned fl = a.y;
-        double u[NV_DEV];
-        guard_eval_prol(m.store, m.vstride, off, fl >> 8, fl & 7u, (fl >> 3) & 7u, u);
-        if ((fl >> 6) & 1u) eos_cell_dev(u, prm, gam1inv, ggprodinv);
-        const long idx = a.x;
-#pragma unroll
-        for (int v = 0; v < NV_GCB; v++) dst[v * gvs + idx] = (T)u[v];
-    }
+    amr_prolong_kernel_body<T>(hw_block(), m, entries, prol, poff, out, gvs, gbs, prm, gam1inv, ggprodinv);
 }
 
 // ---- refinement marking (Grid_markRefineDerefine) -------------------------------
@@ -833,37 +595,6 @@ __global__ void __launch_bounds__(256) amr_error_kernel(const double *ext, const
         if (h) r = fmax2(0x1.fffffffffffffp+1023, r);
         err[sb] = sqrt(r);
     }
-}
-
-// restriction of parent cell c of block p from its eight children cells
-// (amr_restrict_unk_genorder, order 1): conserved form, weights 1/8 in k, j, i order
-__device__ __forceinline__ void restrict_cell(double *store, long vstride, long bstride, int n, int p, int c,
-                                              const int *child)
-{
-    const int h = n / 2;
-    const int pi = c % n, pj = (c / n) % n, pk = c / (n * n);
-    const int q = (pi >= h) | ((pj >= h) << 1) | ((pk >= h) << 2);
-    const int ch = child[(long)p * 8 + q];
-    const int i0 = 2 * (pi - (q & 1) * h), j0 = 2 * (pj - ((q >> 1) & 1) * h), k0 = 2 * (pk - ((q >> 2) & 1) * h);
-    const double *cs = store + (long)ch * bstride;
-    double s[NV_DEV];
-#pragma unroll
-    for (int v = 0; v < NV_DEV; v++) s[v] = 0.;
-    const double w = 0.5 * 0.5 * 0.5;
-    for (int kk = 0; kk < 2; kk++) for (int jj = 0; jj < 2; jj++) for (int ii = 0; ii < 2; ii++) {
-        const long cc = ((long)(k0 + kk) * n + (j0 + jj)) * n + (i0 + ii);
-        const double dens = cs[D * vstride + cc];
-#pragma unroll
-        for (int v = 0; v < NV_DEV; v++) {
-            double x = cs[v * vstride + cc];
-            if (per_mass(v)) x = dens * x;
-            s[v] = s[v] + w * x;
-        }
-    }
-    double dinv = s[D] == 0.0 ? 0.0 : 1. / s[D];
-    double *ps = store + (long)p * bstride + c;
-#pragma unroll
-    for (int v = 0; v < NV_DEV; v++) ps[v * vstride] = per_mass(v) ? dinv * s[v] : s[v];
 }
 
 // every cell of the parents of one level
@@ -1131,6 +862,95 @@ int fill_batch(const AmrEntry3 *entries, int cnt, int which)
     return 1;
 }
 
+// The persistent step: on by default when the mesh has a guard-fill plan and
+// no option that needs the extended-option kernels (FXB_AMR_PERSISTENT=0
+// keeps the batched launches).  Queue order, restriction items (chunks of
+// the needed parent cells, deepest level first) and one scratch slot per
+// resident CTA of the kernel.
+template <class T> cudaError_t upload(T *&dst, const std::vector<T> &v)
+{
+    cudaError_t e = cudaMalloc((void **)&dst, sizeof(T) * std::max<size_t>(1, v.size()));
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpyAsync((void *)dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, S.C.stream);
+}
+
+int persist_setup()
+{
+    const bool mixed = S.C.prm.precision == FXB_MIXED;
+    const char *ev = getenv("FXB_AMR_PERSISTENT");
+    S.persist = !(ev && ev[0] == '0') && S.d_plan && !extended_options(S.C.dprm);
+    if (!S.persist) return FXB_OK;
+    const char *tw = getenv("FXB_TEST_WAIT_TIMEOUT");
+    if (tw && tw[0] == '1') { S.test_stall = 1; S.wait_budget = 1000000; }
+    int grid = mixed ? persist_grid_mixed() : persist_grid_fp64();
+    if (grid <= 0) return record_error(FXB_ECUDA, "fxb_register_blocks: persistent AMR kernel does not fit on an SM");
+    S.pgrid = std::min(grid, S.batch);
+    std::vector<int> order(S.nleaf);
+    for (int l = 0; l < S.nleaf; l++) order[l] = l;
+    std::stable_sort(order.begin(), order.end(), [](int x, int y) {
+        return S.blk[S.leaf_blk[x]].level > S.blk[S.leaf_blk[y]].level;
+    });
+    CKA(upload(S.d_order, order));
+    std::vector<int4> items;
+    const long rch = 2048;
+    for (int i = 0; i < 32; i++) S.rlev_items[i] = 0;
+    if (S.d_rlist)
+        for (int lev = S.maxlev - 1; lev >= 1; lev--) {
+            const long off = S.rlist_off[lev], cnt = S.rlist_off[lev + 1] - off;
+            for (long b = 0; b < cnt; b += rch) {
+                items.push_back(make_int4(lev, (int)(off + b), (int)(off + std::min(b + rch, cnt)), 0));
+                S.rlev_items[lev]++;
+            }
+        }
+    S.nritem = (int)items.size();
+    if (S.nritem) CKA(upload(S.d_ritems, items));
+    CKA(cudaMalloc(&S.d_ctl, sizeof(int) * PQ_WORDS));
+    CKA(cudaMalloc(&S.d_emitted, sizeof(int) * (size_t)S.nleaf));
+    CKA(cudaMalloc(&S.d_slots, sizeof(AmrEntry3) * (size_t)S.pgrid));
+    return FXB_OK;
+}
+
+// one step as the persistent kernel; returns the number of launches
+int persist_step(const double *dtv, double dt)
+{
+    const bool mixed = S.C.prm.precision == FXB_MIXED;
+    CKA(cudaMemsetAsync(S.d_ctl, 0, sizeof(int) * PQ_WORDS, S.C.stream));
+    CKA(cudaMemsetAsync(S.d_emitted, 0, sizeof(int) * (size_t)S.nleaf, S.C.stream));
+    PersistArgs p;
+    memset((void *)&p, 0, sizeof(p));
+    p.a = batch_args(dtv, dt);
+    p.a.batch = S.d_slots;
+    p.m = mesh_args(S.cur);
+    p.slots = S.d_slots;
+    p.leaf_entry = S.d_entries;
+    p.order = S.d_order;
+    p.leaf_blk = S.leaf_blk_dev;
+    p.plan = (const GuardPlan *)S.d_plan;
+    p.glist = S.d_glist;
+    p.nglist = S.nglist;
+    p.prol = (const ProlRec *)S.d_prol;
+    p.poff = S.d_poff;
+    p.has_prol = S.nprol > 0;
+    p.ritems = S.d_ritems;
+    p.rlist = S.d_rlist;
+    p.child = S.d_child;
+    p.nritem = S.nritem;
+    p.nleaf = S.nleaf;
+    for (int i = 0; i < 32; i++) p.rlev_items[i] = S.rlev_items[i];
+    p.bflux = S.bflux;
+    p.nfc = S.nfc;
+    p.fine = S.d_fine;
+    p.finer_mask = S.d_finer;
+    p.ctl = S.d_ctl;
+    p.emitted = S.d_emitted;
+    p.budget = S.wait_budget;
+    p.test_stall = S.test_stall;
+    if (mixed) launch_amr_persist_mixed(p, S.pgrid, S.C.stream);
+    else launch_amr_persist_fp64(p, S.pgrid, S.C.stream);
+    CKA(cudaGetLastError());
+    return FXB_OK;
+}
+
 } // namespace
 
 // ----------------------------------------------------------------- interface
@@ -1148,6 +968,7 @@ void free_device(State &s)
     for (int d = 0; d < 3; d++) { dfree(s.w[d]); dfree(s.f[d]); }
     dfree(s.bflux); dfree(s.stage); dfree(s.d_dmap); dfree(s.d_pmap); dfree(s.d_glist);
     dfree(s.d_plan); dfree(s.d_prol); dfree(s.d_poff); dfree(s.d_rlist);
+    dfree(s.d_order); dfree(s.d_ctl); dfree(s.d_emitted); dfree(s.d_ritems); dfree(s.d_slots);
     dfree(s.d_active); dfree(s.d_act_eos); dfree(s.d_act_bnd); dfree(s.d_ext); dfree(s.d_err);
 }
 } // namespace
@@ -1387,7 +1208,7 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     CKA(cudaStreamSynchronize(st));
     S.cur = 0;
     S.active = true;
-    return FXB_OK;
+    return persist_setup();
 }
 
 // Launch-shape search on the attached state: the guard fill, sigma, the PPM
@@ -1518,6 +1339,13 @@ int amr_fill_to_host(double *unk_host, const int pos[NV_DEV], int n, const int s
 
 int amr_step(const double *dtv, double dt, int *launches)
 {
+    if (S.persist) {
+        int rc = persist_step(dtv, dt);
+        if (rc) return rc;
+        S.cur = 1 - S.cur;
+        if (launches) *launches = 1;
+        return FXB_OK;
+    }
     const bool mixed = S.C.prm.precision == FXB_MIXED;
     int nl = 0;
     nl += restrict_needed(S.cur);

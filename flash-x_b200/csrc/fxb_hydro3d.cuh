@@ -174,8 +174,17 @@ __device__ __forceinline__ void load_cell(const Args3D &a, int i, int j, int k, 
     }
 }
 
+// The block coordinates a stage body works with: CTA x of nx CTAs sharing
+// one batch entry y.  A kernel launch passes (blockIdx.x, blockIdx.y,
+// gridDim.x); the persistent AMR kernel passes (0, its scratch slot, 1), so
+// one CTA runs a whole leaf through every stage.
+struct VB {
+    int x, y, nx;
+};
+__device__ __forceinline__ VB hw_block() { return VB{(int)blockIdx.x, (int)blockIdx.y, (int)gridDim.x}; }
+
 // Geometry, source and intermediates of one kernel invocation: the whole
-// uniform grid, or (AMR) the batch entry blockIdx.y.
+// uniform grid, or (AMR) the batch entry `by`.
 template <class R, bool AMR> struct Ctx3 {
     Grid3 G;
     const double *src;          // uniform grid: the FP64 state
@@ -185,11 +194,11 @@ template <class R, bool AMR> struct Ctx3 {
     R *sig, *wst[3], *flx[3], *slp, *flat;
     double dx, dy, dz;
     AmrEntry3 m;
-    __device__ explicit Ctx3(const Args3D &a)
+    __device__ Ctx3(const Args3D &a, int by)
     {
         G = Grid3{a.nx, a.ny, a.nz};
         if constexpr (AMR) {
-            const int bb = blockIdx.y;
+            const int bb = by;
             m = a.batch[bb];
             src = nullptr;
             srcR = (const R *)a.gcb + (long)bb * a.gcb_bstride;
@@ -329,16 +338,19 @@ __device__ __forceinline__ void unflatten(unsigned idx, const FastDiv &fx, const
 // grid-stride loop bounds of one launch in 32-bit arithmetic
 #define FXB_GRID_LOOP(idx, count) \
     for (int idx = (int)(blockIdx.x * blockDim.x + threadIdx.x); idx < (int)(count); idx += (int)(gridDim.x * blockDim.x))
+// the same loop over the CTAs of a virtual block
+#define FXB_VB_LOOP(idx, count, vb) \
+    for (int idx = (int)((vb).x * blockDim.x + threadIdx.x); idx < (int)(count); idx += (int)((vb).nx * blockDim.x))
 
 // ---- sigma_d of every padded cell --------------------------------------------
 template <class R, bool AMR>
-__global__ void __launch_bounds__(256) sig3d_kernel(const Args3D a)
+__device__ __forceinline__ void sig3d_kernel_body(const Args3D &a, const VB vb)
 {
-    const Ctx3<R, AMR> X(a);
+    const Ctx3<R, AMR> X(a, vb.y);
     const Grid3 &G = X.G;
     R *sig = X.sig;
     const long np = G.npad();
-    FXB_GRID_LOOP(idx, np) {
+    FXB_VB_LOOP(idx, np, vb) {
         int i, j, k;
         unflatten(idx, a.fdx[2], a.fdy[2], i, j, k);
         i -= 1; j -= 1; k -= 1;
@@ -366,17 +378,22 @@ __global__ void __launch_bounds__(256) sig3d_kernel(const Args3D a)
         }
     }
 }
+template <class R, bool AMR>
+__global__ void __launch_bounds__(256) sig3d_kernel(const Args3D a)
+{
+    sig3d_kernel_body<R, AMR>(a, hw_block());
+}
 
 // ---- flattening coefficients of every padded cell, three directions ----------
 // (hy_getRiemannState.F90:367-465; FlatTilde of the cell and its two
 // neighbours along d from pressures three cells either side)
 template <class R, bool AMR>
-__global__ void __launch_bounds__(256) flat3d_kernel(const Args3D a)
+__device__ __forceinline__ void flat3d_kernel_body(const Args3D &a, const VB vb)
 {
-    const Ctx3<R, AMR> X(a);
+    const Ctx3<R, AMR> X(a, vb.y);
     const Grid3 &G = X.G;
     const long np = G.npad();
-    FXB_GRID_LOOP(idx, np) {
+    FXB_VB_LOOP(idx, np, vb) {
         int i, j, k;
         unflatten(idx, a.fdx[2], a.fdy[2], i, j, k);
         i -= 1; j -= 1; k -= 1;
@@ -397,6 +414,11 @@ __global__ void __launch_bounds__(256) flat3d_kernel(const Args3D a)
             X.flat[(long)d * np + idx] = flat_coeff(p[4] - p[2], ftm, ft0, ftp);
         }
     }
+}
+template <class R, bool AMR>
+__global__ void __launch_bounds__(256) flat3d_kernel(const Args3D a)
+{
+    flat3d_kernel_body<R, AMR>(a, hw_block());
 }
 
 template <class R>
@@ -433,14 +455,14 @@ __device__ __forceinline__ void ctu_term(const Args3D &a, const R *sigp, const G
 // of direction d; each face-state cell then reads the slopes of itself and of
 // its two neighbours instead of recomputing them.
 template <class R, bool AMR>
-__global__ void __launch_bounds__(256) slope3d_kernel(const Args3D a, int d)
+__device__ __forceinline__ void slope3d_kernel_body(const Args3D &a, const VB vb, int d)
 {
-    const Ctx3<R, AMR> X(a);
+    const Ctx3<R, AMR> X(a, vb.y);
     const Grid3 &G = X.G;
     const long ns = G.ns(d);
     int di, dj, dk;
     offs(d, 1, di, dj, dk);
-    FXB_GRID_LOOP(idx, ns) {
+    FXB_VB_LOOP(idx, ns, vb) {
         int i, j, k;
         unflatten(idx, a.fdx[d == 0 ? 4 : 0], a.fdy[d == 1 ? 4 : 0], i, j, k);
         if (d == 0) i -= 2; else if (d == 1) j -= 2; else k -= 2;
@@ -457,6 +479,11 @@ __global__ void __launch_bounds__(256) slope3d_kernel(const Args3D a, int d)
 #pragma unroll
         for (int q = 0; q < 6; q++) X.slp[(long)q * ns + idx] = db[q];
     }
+}
+template <class R, bool AMR>
+__global__ void __launch_bounds__(256) slope3d_kernel(const Args3D a, int d)
+{
+    slope3d_kernel_body<R, AMR>(a, hw_block(), d);
 }
 
 // The face states of one cell from its traced states wm, wp (sweep frame):
@@ -656,10 +683,10 @@ template <class R> struct PwSlots {
 #define FXB_S3_MINB_FP64 2
 #endif
 template <class R, int ORDER, bool AMR, int DIR, bool EXT>
-__global__ void __launch_bounds__(256, FXB_S3_MINB_FP64) states3d_kernel(const Args3D a)
+__device__ __forceinline__ void states3d_kernel_body(const Args3D &a, const VB vb)
 {
     constexpr int d = DIR;
-    const Ctx3<R, AMR> X(a);
+    const Ctx3<R, AMR> X(a, vb.y);
     const Grid3 &G = X.G;
     const double dt = a.dtv ? a.dtv[0] : a.dt_arg;
     const double del[3] = {X.dx, X.dy, X.dz};
@@ -667,7 +694,7 @@ __global__ void __launch_bounds__(256, FXB_S3_MINB_FP64) states3d_kernel(const A
     const R hdtx = R(0.5 * dt / X.dx), hdty = R(0.5 * dt / X.dy), hdtz = R(0.5 * dt / X.dz);
     R *w = X.wst[d];
     const long nw = G.nw(d);
-    FXB_GRID_LOOP(idx, nw) {
+    FXB_VB_LOOP(idx, nw, vb) {
         int i, j, k;
         unflatten(idx, a.fdx[d == 0 ? 2 : 0], a.fdy[d == 1 ? 2 : 0], i, j, k);
         if (d == 0) i -= 1; else if (d == 1) j -= 1; else k -= 1;
@@ -677,20 +704,25 @@ __global__ void __launch_bounds__(256, FXB_S3_MINB_FP64) states3d_kernel(const A
         for (int q = 0; q < 6; q++) { w[(long)q * nw + idx] = Wp[q]; w[(long)(6 + q) * nw + idx] = Wm[q]; }
     }
 }
+template <class R, int ORDER, bool AMR, int DIR, bool EXT>
+__global__ void __launch_bounds__(256, FXB_S3_MINB_FP64) states3d_kernel(const Args3D a)
+{
+    states3d_kernel_body<R, ORDER, AMR, DIR, EXT>(a, hw_block());
+}
 
 // ---- Riemann fluxes of direction d ---------------------------------------------
 // the direction is a template parameter so that the solver's per-direction
 // indexing of the state vectors resolves at compile time (no local memory)
 template <class R, bool AMR, int DIR, bool EXT>
-__global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
+__device__ __forceinline__ void flux3d_kernel_body(const Args3D &a, const VB vb)
 {
     constexpr int d = DIR;
-    const Ctx3<R, AMR> X(a);
+    const Ctx3<R, AMR> X(a, vb.y);
     const Grid3 &G = X.G;
     const R *w = X.wst[d];
     R *f = X.flx[d];
     const long nf = G.nf(d), nw = G.nw(d);
-    FXB_GRID_LOOP(idx, nf) {
+    FXB_VB_LOOP(idx, nf, vb) {
         int i, j, k;
         unflatten(idx, a.fdx[d == 0 ? 1 : 0], a.fdy[d == 1 ? 1 : 0], i, j, k);
         int di, dj, dk;
@@ -710,6 +742,11 @@ __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
         for (int q = 0; q < NF; q++) f[(long)q * nf + idx] = F[q];
     }
 }
+template <class R, bool AMR, int DIR, bool EXT>
+__global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
+{
+    flux3d_kernel_body<R, AMR, DIR, EXT>(a, hw_block());
+}
 
 // ---- face states and Riemann fluxes of direction d --------------------------------
 // A CTA takes Ls consecutive cells (a segment seg: cells seg*S - 1 ..
@@ -726,14 +763,13 @@ template <class R> struct SfluxRegs {
     static constexpr int value = (65536 / ((sizeof(R) == 8 ? 2 : 3) * FXB_SF_MAXT)) / 8 * 8;
 };
 template <class R, int ORDER, bool AMR, int DIR, bool EXT>
-__global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) sflux3d_kernel(const Args3D a)
+__device__ __forceinline__ void sflux3d_kernel_body(const Args3D &a, const VB vb, unsigned char *sflux_smem, int nt)
 {
     constexpr int d = DIR;
     constexpr int H = ORDER == 3 ? 1 : 0;          // PPM: one slope cell either side of the face-state cells
-    extern __shared__ __align__(16) unsigned char sflux_smem[];
     R *sW = reinterpret_cast<R *>(sflux_smem);     // [8][threads]: right-face state, then gamc, game
-    R *sD = sW + 8 * blockDim.x;                   // PPM: [6][threads] limited slopes
-    const Ctx3<R, AMR> X(a);
+    R *sD = sW + 8 * nt;                           // PPM: [6][threads] limited slopes
+    const Ctx3<R, AMR> X(a, vb.y);
     const Grid3 &G = X.G;
     const double dt = a.dtv ? a.dtv[0] : a.dt_arg;
     const double del[3] = {X.dx, X.dy, X.dz};
@@ -743,16 +779,16 @@ __global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) 
     const int N1 = d == 0 ? a.ny : a.nx, N2 = d == 2 ? a.ny : a.nz;
     const int Ls = a.sf_len[d], T1 = a.sf_lines[d], S = Ls - 1, Lt = Ls + 2 * H;
     const int nseg = (N + S) / S, nt1 = (N1 + T1 - 1) / T1;
-    const int t = threadIdx.x, nt = blockDim.x;
+    const int t = threadIdx.x;
     const int ld = d == 0 ? t % Lt : t / T1;
     const int l1 = d == 0 ? t / Lt : t % T1;
     const int step = d == 0 ? 1 : T1;              // the neighbour along d, in threads
-    int b = blockIdx.x;
+    int b = vb.x;
     const int seg = b % nseg;
     b /= nseg;
     const int t1 = (b % nt1) * T1 + l1, t2 = b / nt1;
     const int c = seg * S - 1 - H + ld;
-    const bool line = t1 < N1 && t2 < N2;
+    const bool line = t < nt && t1 < N1 && t2 < N2;   // threads beyond the tile only meet the barriers
     const bool st = line && ld >= H && ld < Lt - H && c <= N;   // a face-state cell
     const int i = d == 0 ? c : t1, j = d == 0 ? t1 : d == 1 ? c : t2, k = d == 2 ? c : t2;
     R Wm[6], Wp[6], gc = R(0), ge = R(0);
@@ -835,6 +871,12 @@ __global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) 
         for (int q = 0; q < NF; q++) f[q * nf + fi] = F[q];
     }
 }
+template <class R, int ORDER, bool AMR, int DIR, bool EXT>
+__global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) sflux3d_kernel(const Args3D a)
+{
+    extern __shared__ __align__(16) unsigned char sflux_smem[];
+    sflux3d_kernel_body<R, ORDER, AMR, DIR, EXT>(a, hw_block(), sflux_smem, (int)blockDim.x);
+}
 
 // ---- update, energyFix, Eos, CFL rate -------------------------------------------
 // four resident CTAs per SM (64 registers, ~200 bytes of spills) measured
@@ -843,9 +885,9 @@ __global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) 
 #define FXB_UPD_MINB 4
 #endif
 template <class R, bool AMR>
-__global__ void __launch_bounds__(256, FXB_UPD_MINB) update3d_kernel(const Args3D a)
+__device__ __forceinline__ void update3d_kernel_body(const Args3D &a, const VB vb)
 {
-    const Ctx3<R, AMR> X(a);
+    const Ctx3<R, AMR> X(a, vb.y);
     const Grid3 &G = X.G;
     if (AMR && (X.m.flags & AMR_SKIP_UPDATE)) return;
     const double dt = a.dtv ? a.dtv[0] : a.dt_arg;
@@ -855,7 +897,7 @@ __global__ void __launch_bounds__(256, FXB_UPD_MINB) update3d_kernel(const Args3
     double *out = AMR ? a.odata + (long)X.m.out_blk * a.o_bstride : a.out;
     const long ovs = AMR ? a.o_vstride : a.vstride;
     double rate = 0.;
-    FXB_GRID_LOOP(c, n) {
+    FXB_VB_LOOP(c, n, vb) {
         int i, j, k;
         unflatten(c, a.fdx[0], a.fdy[0], i, j, k);
         // the update starts from the FP64 state: the grid, or the leaf's interior store
@@ -938,6 +980,11 @@ __global__ void __launch_bounds__(256, FXB_UPD_MINB) update3d_kernel(const Args3
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) rate = fmax(rate, __shfl_xor_sync(0xffffffffu, rate, off));
     if ((threadIdx.x & 31) == 0) atomicMax(a.rate_max, (unsigned long long)__double_as_longlong(rate));
+}
+template <class R, bool AMR>
+__global__ void __launch_bounds__(256, FXB_UPD_MINB) update3d_kernel(const Args3D a)
+{
+    update3d_kernel_body<R, AMR>(a, hw_block());
 }
 
 // bytes of the 3-D intermediates for R of the given size
@@ -1089,9 +1136,9 @@ template <class R> void launch_hydro3d_t(const Args3D &a0, cudaStream_t s)
 // [leaf][face][slot][t2 * n1 + t1] with (t1, t2) the face's transverse cell
 // (x faces: (y, z); y faces: (x, z); z faces: (x, y)).
 template <class R>
-__global__ void __launch_bounds__(256) amr_emit_flux_kernel(const Args3D a, R *bflux, long nfc)
+__device__ __forceinline__ void amr_emit_flux_kernel_body(const Args3D &a, const VB vb, R *bflux, long nfc)
 {
-    const Ctx3<R, true> X(a);
+    const Ctx3<R, true> X(a, vb.y);
     const Grid3 &G = X.G;
     const int n[3] = {a.nx, a.ny, a.nz};
     R *dst = bflux + (long)X.m.leaf * 6 * NF * nfc;
@@ -1100,7 +1147,7 @@ __global__ void __launch_bounds__(256) amr_emit_flux_kernel(const Args3D a, R *b
         const int a1 = d == 0 ? 1 : 0, a2 = d == 2 ? 1 : 2;
         const long nface = (long)n[a1] * n[a2];
         const long nfd = G.nf(d);
-        for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nface * NF; t += (long)gridDim.x * blockDim.x) {
+        for (long t = vb.x * (long)blockDim.x + threadIdx.x; t < nface * NF; t += (long)vb.nx * blockDim.x) {
             const int v = (int)(t / nface);
             const long tt = t - v * nface;
             const int t1 = (int)(tt % n[a1]), t2 = (int)(tt / n[a1]);
@@ -1110,16 +1157,20 @@ __global__ void __launch_bounds__(256) amr_emit_flux_kernel(const Args3D a, R *b
         }
     }
 }
+template <class R>
+__global__ void __launch_bounds__(256) amr_emit_flux_kernel(const Args3D a, R *bflux, long nfc)
+{
+    amr_emit_flux_kernel_body<R>(a, hw_block(), bflux, nfc);
+}
 
 // Grid_conserveFluxes: on a face whose same-level neighbour is refined, the
 // fluxes become the fine fluxes restricted as amr_restrict_red does:
 // (((f(a) + f(a+e1)) + f(a+e2)) + f(a+e1+e2)) * 0.25.  fine[leaf*24 + face*4 + q]
 // is the fine leaf across the face at transverse child position q = o1 + 2*o2.
 template <class R>
-__global__ void __launch_bounds__(256) amr_correct_flux_kernel(const Args3D a, const R *bflux, long nfc,
-                                                               const int *fine, const int *finer_mask)
+__device__ __forceinline__ void amr_correct_flux_kernel_body(const Args3D &a, const VB vb, const R *bflux, long nfc, const int *fine, const int *finer_mask)
 {
-    const Ctx3<R, true> X(a);
+    const Ctx3<R, true> X(a, vb.y);
     const Grid3 &G = X.G;
     const int mask = finer_mask[X.m.leaf];
     if (!mask) return;
@@ -1131,7 +1182,7 @@ __global__ void __launch_bounds__(256) amr_correct_flux_kernel(const Args3D a, c
         const long nface = (long)n[a1] * n[a2];
         const long nfd = G.nf(d);
         const int ff = f ^ 1;      // the fine leaves' face toward this block
-        for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nface * NF; t += (long)gridDim.x * blockDim.x) {
+        for (long t = vb.x * (long)blockDim.x + threadIdx.x; t < nface * NF; t += (long)vb.nx * blockDim.x) {
             const int v = (int)(t / nface);
             const long tt = t - v * nface;
             const int t1 = (int)(tt % n[a1]), t2 = (int)(tt / n[a1]);
@@ -1139,13 +1190,20 @@ __global__ void __launch_bounds__(256) amr_correct_flux_kernel(const Args3D a, c
             const int f1 = 2 * t1 - o1 * n[a1], f2 = 2 * t2 - o2 * n[a2];
             const int fl = fine[(long)X.m.leaf * 24 + f * 4 + o1 + 2 * o2];
             const R *src = bflux + (((long)fl * 6 + ff) * NF + v) * nfc;
-            const R fa = src[(long)f2 * n[a1] + f1], fb = src[(long)f2 * n[a1] + f1 + 1];
-            const R fc = src[(long)(f2 + 1) * n[a1] + f1], fd = src[(long)(f2 + 1) * n[a1] + f1 + 1];
+            // L2 loads: in the persistent AMR kernel another SM stored these this step
+            const R fa = __ldcg(src + (long)f2 * n[a1] + f1), fb = __ldcg(src + (long)f2 * n[a1] + f1 + 1);
+            const R fc = __ldcg(src + (long)(f2 + 1) * n[a1] + f1), fd = __ldcg(src + (long)(f2 + 1) * n[a1] + f1 + 1);
             int c[3];
             c[d] = side ? n[d] : 0; c[a1] = t1; c[a2] = t2;
             X.flx[d][(long)v * nfd + G.fidx(d, c[0], c[1], c[2])] = (((fa + fb) + fc) + fd) * R(0.25);
         }
     }
+}
+template <class R>
+__global__ void __launch_bounds__(256) amr_correct_flux_kernel(const Args3D a, const R *bflux, long nfc,
+                                                               const int *fine, const int *finer_mask)
+{
+    amr_correct_flux_kernel_body<R>(a, hw_block(), bflux, nfc, fine, finer_mask);
 }
 
 // The 3-D pipeline over one AMR batch of `entries` guard-filled blocks; `which`

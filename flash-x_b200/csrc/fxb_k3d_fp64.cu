@@ -1,5 +1,6 @@
 // FP64 instantiation of the 3-D kernels (built with -fmad=false).
 #include "fxb_launch.h"
+#include "fxb_amr_persist.cuh"
 namespace fxb {
 cudaError_t setup_hydro3d_fp64() { return cudaSuccess; }
 void launch_hydro3d_fp64(const Args3D &a, cudaStream_t s) { launch_hydro3d_t<double>(a, s); }
@@ -11,4 +12,6 @@ void launch_amr3d_correct_fp64(const Args3D &a, int entries, const void *bflux, 
                                const int *finer_mask, cudaStream_t s)
 { launch_amr3d_correct_t<double>(a, entries, bflux, nfc, fine, finer_mask, s); }
 void launch_amr3d_update_fp64(const Args3D &a, int entries, cudaStream_t s) { launch_amr3d_update_t<double>(a, entries, s); }
+void launch_amr_persist_fp64(const PersistArgs &p, int grid, cudaStream_t s) { launch_amr_persist_t<double>(p, grid, s); }
+int persist_grid_fp64() { return persist_grid<double>(); }
 } // namespace fxb

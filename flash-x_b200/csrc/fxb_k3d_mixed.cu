@@ -1,6 +1,7 @@
 // Mixed-precision instantiation of the 3-D kernels: FP32 reconstruction, CTU
 // terms and Riemann solve with FP32 intermediates; FP64 update, Eos and CFL rate.
 #include "fxb_launch.h"
+#include "fxb_amr_persist.cuh"
 namespace fxb {
 cudaError_t setup_hydro3d_mixed() { return cudaSuccess; }
 void launch_hydro3d_mixed(const Args3D &a, cudaStream_t s) { launch_hydro3d_t<float>(a, s); }
@@ -12,4 +13,6 @@ void launch_amr3d_correct_mixed(const Args3D &a, int entries, const void *bflux,
                                const int *finer_mask, cudaStream_t s)
 { launch_amr3d_correct_t<float>(a, entries, bflux, nfc, fine, finer_mask, s); }
 void launch_amr3d_update_mixed(const Args3D &a, int entries, cudaStream_t s) { launch_amr3d_update_t<float>(a, entries, s); }
+void launch_amr_persist_mixed(const PersistArgs &p, int grid, cudaStream_t s) { launch_amr_persist_t<float>(p, grid, s); }
+int persist_grid_mixed() { return persist_grid<float>(); }
 } // namespace fxb

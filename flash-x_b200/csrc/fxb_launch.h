@@ -26,4 +26,10 @@ void launch_amr3d_emit_mixed(const Args3D &a, int entries, void *bflux, long nfc
 void launch_amr3d_correct_mixed(const Args3D &a, int entries, const void *bflux, long nfc, const int *fine,
                                const int *finer_mask, cudaStream_t s);
 void launch_amr3d_update_mixed(const Args3D &a, int entries, cudaStream_t s);
+// the persistent AMR step (fxb_amr_persist.cuh): launch and resident CTAs
+struct PersistArgs;
+void launch_amr_persist_fp64(const PersistArgs &p, int grid, cudaStream_t s);
+void launch_amr_persist_mixed(const PersistArgs &p, int grid, cudaStream_t s);
+int persist_grid_fp64();
+int persist_grid_mixed();
 } // namespace fxb

@@ -139,18 +139,74 @@ def test_amr_masked_fill_and_doeos(oracle, need_gpu):
     dev.close()
 
 
-def test_amr_batches_agree(oracle, need_gpu):
-    """Leaves processed in several batches (guard fill, fluxes, then a second
-    pass for the leaves whose fluxes are corrected) give the one-batch result."""
+@pytest.mark.parametrize("persistent", ["0", "1"])
+def test_amr_batches_agree(oracle, need_gpu, monkeypatch, persistent):
+    """Batched launches: leaves processed in several batches (guard fill,
+    fluxes, then a second pass for the leaves whose fluxes are corrected)
+    give the one-batch result.  Persistent kernel: 37 scratch slots (CTAs)
+    for all leaves give the same result."""
     root, hp, mesh, unk = _case(maxlev=2)
     am = oracle.Amr(oracle.make_params(root.as_dict(), hp), mesh.levels, mesh.bcoords)
     dt = 0.5 * am.compute_dt(unk)
     _, ref = _oracle(oracle, root, hp, mesh, unk, [dt])
-    os.environ["FXB_AMR_MAX_BATCH"] = "37"
-    try:
-        dev, out = _gpu(root, hp, mesh, unk, [dt])
-    finally:
-        del os.environ["FXB_AMR_MAX_BATCH"]
+    monkeypatch.setenv("FXB_AMR_MAX_BATCH", "37")
+    monkeypatch.setenv("FXB_AMR_PERSISTENT", persistent)
+    dev, out = _gpu(root, hp, mesh, unk, [dt])
+    np.testing.assert_array_equal(_interior(root, out), _interior(root, ref))
+    dev.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_amr_persistent_kernel_equals_batched_launches(oracle, need_gpu, monkeypatch, precision):
+    """One persistent kernel per step (device work queue: restriction by level,
+    then the leaves finest first, each leaf's whole pipeline in one CTA, bounded
+    waits for finer neighbours' boundary fluxes) against the batched launches:
+    bit for bit in FP64 (both equal the oracle), within round-off of the FP64
+    guard-fill arithmetic (compiled with FMA in the mixed kernels) in mixed
+    precision; one kernel launch per step."""
+    root, hp, mesh, unk = _case(maxlev=3, order=3)
+    am = oracle.Amr(oracle.make_params(root.as_dict(), hp), mesh.levels, mesh.bcoords)
+    dt = 0.5 * am.compute_dt(unk)
+    outs = {}
+    for flag in ("0", "1"):
+        monkeypatch.setenv("FXB_AMR_PERSISTENT", flag)
+        dev, out = _gpu(root, hp, mesh, unk, [dt, dt, dt], precision)
+        outs[flag] = _interior(root, out)
+        if flag == "1":
+            assert dev.last_timing()[1] == 1
+            dtn, dto = dev.advance(4, dt, dt)              # graph-captured persistent steps
+            assert dtn > 0 and dto > 0
+        dev.close()
+    if precision == "fp64":
+        _, ref = _oracle(oracle, root, hp, mesh, unk, [dt, dt, dt])
+        np.testing.assert_array_equal(outs["1"], _interior(root, ref))
+        np.testing.assert_array_equal(outs["1"], outs["0"])
+    else:
+        a, b = outs["1"][..., 0], outs["0"][..., 0]
+        assert np.mean(np.abs(a - b)) / np.mean(b) <= 1e-7
+
+
+def test_amr_persistent_wait_timeout_reports_status(oracle, need_gpu, monkeypatch):
+    """The persistent kernel's waits are bounded: with a test hook that makes
+    every leaf next to finer leaves wait on a flag that nothing sets, the wait
+    runs out (~0.5 ms), the kernel raises its abort flag, every CTA leaves, and
+    the host reads FXB_ETIMEOUT; the next solver instance on the same context
+    steps exactly like the oracle."""
+    from flashx_b200.hydro import FXB_ETIMEOUT
+    root, hp, mesh, unk = _case(maxlev=2)
+    am = oracle.Amr(oracle.make_params(root.as_dict(), hp), mesh.levels, mesh.bcoords)
+    dt = 0.5 * am.compute_dt(unk)
+    monkeypatch.setenv("FXB_TEST_WAIT_TIMEOUT", "1")
+    dev = HydroDevice(root, hp, "fp64", mesh=mesh)
+    dev.attach_unk(unk.copy())
+    dev.Hydro(0.0, dt, dt)
+    with pytest.raises(FlashXError) as ei:
+        dev.Hydro_computeDt()
+    assert ei.value.code == FXB_ETIMEOUT
+    dev.close()
+    monkeypatch.delenv("FXB_TEST_WAIT_TIMEOUT")
+    _, ref = _oracle(oracle, root, hp, mesh, unk, [dt])
+    dev, out = _gpu(root, hp, mesh, unk, [dt])
     np.testing.assert_array_equal(_interior(root, out), _interior(root, ref))
     dev.close()
 
