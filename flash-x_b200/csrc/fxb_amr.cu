@@ -93,11 +93,14 @@ struct State {
     int cta[4] = {4, 4, 4, 4};                    // CTAs per block: sig, slopes, (unused), update
     int fill_cta = 8;
     bool tuned = false;                           // launch shapes chosen (first attach of the mesh)
-    char tune_log[256] = "";
+    char tune_log[512] = "";
     std::unordered_map<uint64_t, int> map;
     // the step as one persistent kernel over the leaf list (fxb_amr_persist.cuh)
     bool persist = false;
-    int pgrid = 0;                                // its CTAs, one scratch slot each
+    bool persist_ok = false;                      // the mesh and options allow the persistent kernel
+    int pK = 4;                                   // CTAs per cluster (one leaf per cluster)
+    int pclusters = 0;                            // resident clusters, one scratch slot each
+    int pslots = 0;                               // slots allocated (the most clusters of any K)
     int *d_order = nullptr;                       // leaves in queue order, finest level first
     int *d_ctl = nullptr;                         // queue head, completion counters, abort flag
     int *d_emitted = nullptr;                     // per leaf: boundary fluxes stored
@@ -862,11 +865,21 @@ int fill_batch(const AmrEntry3 *entries, int cnt, int which)
     return 1;
 }
 
+int persist_upload();
+
 // The persistent step: on by default when the mesh has a guard-fill plan and
 // no option that needs the extended-option kernels (FXB_AMR_PERSISTENT=0
 // keeps the batched launches).  Queue order, restriction items (chunks of
 // the needed parent cells, deepest level first) and one scratch slot per
 // resident CTA of the kernel.
+// clusters of K CTAs of the persistent kernel to launch: those that fit at
+// once, at most one per scratch slot of the batch arrays
+int persist_clusters(int K)
+{
+    const int n = S.C.prm.precision == FXB_MIXED ? persist_grid_mixed(K) : persist_grid_fp64(K);
+    return std::min(n, S.batch);
+}
+
 template <class T> cudaError_t upload(T *&dst, const std::vector<T> &v)
 {
     cudaError_t e = cudaMalloc((void **)&dst, sizeof(T) * std::max<size_t>(1, v.size()));
@@ -876,15 +889,19 @@ template <class T> cudaError_t upload(T *&dst, const std::vector<T> &v)
 
 int persist_setup()
 {
-    const bool mixed = S.C.prm.precision == FXB_MIXED;
     const char *ev = getenv("FXB_AMR_PERSISTENT");
-    S.persist = !(ev && ev[0] == '0') && S.d_plan && !extended_options(S.C.dprm);
+    S.persist_ok = !(ev && ev[0] == '0') && S.d_plan && !extended_options(S.C.dprm);
+    S.persist = S.persist_ok;
     if (!S.persist) return FXB_OK;
     const char *tw = getenv("FXB_TEST_WAIT_TIMEOUT");
     if (tw && tw[0] == '1') { S.test_stall = 1; S.wait_budget = 1000000; }
-    int grid = mixed ? persist_grid_mixed() : persist_grid_fp64();
-    if (grid <= 0) return record_error(FXB_ECUDA, "fxb_register_blocks: persistent AMR kernel does not fit on an SM");
-    S.pgrid = std::min(grid, S.batch);
+    const char *ek = getenv("FXB_AMR_CLUSTER");
+    if (ek) S.pK = atoi(ek);
+    if (S.pK != 1 && S.pK != 2 && S.pK != 4 && S.pK != 8) S.pK = 4;
+    const int most = persist_clusters(1);
+    if (most <= 0) return record_error(FXB_ECUDA, "fxb_register_blocks: persistent AMR kernel does not fit on an SM");
+    S.pslots = most;
+    S.pclusters = persist_clusters(S.pK);
     std::vector<int> order(S.nleaf);
     for (int l = 0; l < S.nleaf; l++) order[l] = l;
     std::stable_sort(order.begin(), order.end(), [](int x, int y) {
@@ -906,47 +923,64 @@ int persist_setup()
     if (S.nritem) CKA(upload(S.d_ritems, items));
     CKA(cudaMalloc(&S.d_ctl, sizeof(int) * PQ_WORDS));
     CKA(cudaMalloc(&S.d_emitted, sizeof(int) * (size_t)S.nleaf));
-    CKA(cudaMalloc(&S.d_slots, sizeof(AmrEntry3) * (size_t)S.pgrid));
+    CKA(cudaMalloc(&S.d_slots, sizeof(AmrEntry3) * (size_t)S.pslots));
+    return persist_upload();
+}
+
+// the kernel's argument sets for current store 0 and 1 (dt read from the
+// library's device dt, AmrCommon::dtv)
+int persist_upload()
+{
+    PersistArgs p[2];
+    for (int w = 0; w < 2; w++) {
+        memset((void *)&p[w], 0, sizeof(PersistArgs));
+        const int keep = S.cur;
+        S.cur = w;
+        p[w].a = batch_args(S.C.dtv, 0.0);
+        p[w].m = mesh_args(w);
+        S.cur = keep;
+        p[w].a.batch = S.d_slots;
+        p[w].slots = S.d_slots;
+        p[w].leaf_entry = S.d_entries;
+        p[w].order = S.d_order;
+        p[w].leaf_blk = S.leaf_blk_dev;
+        p[w].plan = (const GuardPlan *)S.d_plan;
+        p[w].glist = S.d_glist;
+        p[w].nglist = S.nglist;
+        p[w].prol = (const ProlRec *)S.d_prol;
+        p[w].poff = S.d_poff;
+        p[w].has_prol = S.nprol > 0;
+        p[w].ritems = S.d_ritems;
+        p[w].rlist = S.d_rlist;
+        p[w].child = S.d_child;
+        p[w].nritem = S.nritem;
+        p[w].nleaf = S.nleaf;
+        for (int i = 0; i < 32; i++) p[w].rlev_items[i] = S.rlev_items[i];
+        p[w].bflux = S.bflux;
+        p[w].nfc = S.nfc;
+        p[w].fine = S.d_fine;
+        p[w].finer_mask = S.d_finer;
+        p[w].ctl = S.d_ctl;
+        p[w].emitted = S.d_emitted;
+        p[w].budget = S.wait_budget;
+        p[w].test_stall = S.test_stall;
+    }
+    CKA(S.C.prm.precision == FXB_MIXED ? persist_upload_mixed(p) : persist_upload_fp64(p));
     return FXB_OK;
 }
 
-// one step as the persistent kernel; returns the number of launches
+// one step as the persistent kernel; dt from dtv (a device pointer, the
+// library's dt in graph-captured loops) or from the argument
 int persist_step(const double *dtv, double dt)
 {
     const bool mixed = S.C.prm.precision == FXB_MIXED;
+    if (!dtv) CKA(cudaMemcpyAsync(S.C.dtv, &dt, sizeof(double), cudaMemcpyHostToDevice, S.C.stream));
+    else if (dtv != S.C.dtv) return record_error(FXB_EARG, "persistent AMR step: dt must be the library's device dt");
     CKA(cudaMemsetAsync(S.d_ctl, 0, sizeof(int) * PQ_WORDS, S.C.stream));
     CKA(cudaMemsetAsync(S.d_emitted, 0, sizeof(int) * (size_t)S.nleaf, S.C.stream));
-    PersistArgs p;
-    memset((void *)&p, 0, sizeof(p));
-    p.a = batch_args(dtv, dt);
-    p.a.batch = S.d_slots;
-    p.m = mesh_args(S.cur);
-    p.slots = S.d_slots;
-    p.leaf_entry = S.d_entries;
-    p.order = S.d_order;
-    p.leaf_blk = S.leaf_blk_dev;
-    p.plan = (const GuardPlan *)S.d_plan;
-    p.glist = S.d_glist;
-    p.nglist = S.nglist;
-    p.prol = (const ProlRec *)S.d_prol;
-    p.poff = S.d_poff;
-    p.has_prol = S.nprol > 0;
-    p.ritems = S.d_ritems;
-    p.rlist = S.d_rlist;
-    p.child = S.d_child;
-    p.nritem = S.nritem;
-    p.nleaf = S.nleaf;
-    for (int i = 0; i < 32; i++) p.rlev_items[i] = S.rlev_items[i];
-    p.bflux = S.bflux;
-    p.nfc = S.nfc;
-    p.fine = S.d_fine;
-    p.finer_mask = S.d_finer;
-    p.ctl = S.d_ctl;
-    p.emitted = S.d_emitted;
-    p.budget = S.wait_budget;
-    p.test_stall = S.test_stall;
-    if (mixed) launch_amr_persist_mixed(p, S.pgrid, S.C.stream);
-    else launch_amr_persist_fp64(p, S.pgrid, S.C.stream);
+    if (S.pclusters <= 0) return record_error(FXB_ECUDA, "persistent AMR kernel: no cluster fits");
+    CKA(mixed ? launch_amr_persist_mixed(S.cur, S.pclusters, S.pK, S.C.stream)
+              : launch_amr_persist_fp64(S.cur, S.pclusters, S.pK, S.C.stream));
     CKA(cudaGetLastError());
     return FXB_OK;
 }
@@ -1211,6 +1245,59 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     return persist_setup();
 }
 
+// one step as batched launches of the stage kernels (the current state is
+// not switched); nl: the launches
+int batched_step(const double *dtv, double dt, int &nl)
+{
+    const bool mixed = S.C.prm.precision == FXB_MIXED;
+    nl = 0;
+    nl += restrict_needed(S.cur);
+    Args3D a = batch_args(dtv, dt);
+    auto fluxes = [&](int cnt) {
+        const int all = AMR_SIG | AMR_STATES;
+        if (mixed) launch_amr3d_fluxes_mixed(a, cnt, all, S.C.stream);
+        else launch_amr3d_fluxes_fp64(a, cnt, all, S.C.stream);
+    };
+    auto emit = [&](int cnt) {
+        if (mixed) launch_amr3d_emit_mixed(a, cnt, S.bflux, S.nfc, S.C.stream);
+        else launch_amr3d_emit_fp64(a, cnt, S.bflux, S.nfc, S.C.stream);
+    };
+    auto correct = [&](int cnt) {
+        if (mixed) launch_amr3d_correct_mixed(a, cnt, S.bflux, S.nfc, S.d_fine, S.d_finer, S.C.stream);
+        else launch_amr3d_correct_fp64(a, cnt, S.bflux, S.nfc, S.d_fine, S.d_finer, S.C.stream);
+    };
+    auto update = [&](int cnt) {
+        if (mixed) launch_amr3d_update_mixed(a, cnt, S.C.stream); else launch_amr3d_update_fp64(a, cnt, S.C.stream);
+    };
+    // sigma (+ flattening), then per direction the slopes, face states and
+    // fluxes (one fused kernel in FP32; slopes (PPM), face states and fluxes
+    // as separate kernels in FP64)
+    const int pipe = 1 + (S.C.prm.flattening ? 1 : 0) + 3 * (mixed ? 1 : (S.C.prm.order == 3 ? 3 : 2));
+    if (S.nleaf <= S.batch) {
+        a.batch = S.d_entries;
+        nl += fill_batch(a.batch, S.nleaf, S.cur);
+        fluxes(S.nleaf); emit(S.nleaf); correct(S.nleaf); update(S.nleaf);
+        nl += pipe + 3;
+    } else {
+        for (int l0 = 0; l0 < S.nleaf; l0 += S.batch) {
+            int cnt = std::min(S.batch, S.nleaf - l0);
+            a.batch = S.d_entries + S.nleaf + l0;
+            nl += fill_batch(a.batch, cnt, S.cur);
+            fluxes(cnt); emit(cnt); update(cnt);
+            nl += pipe + 2;
+        }
+        for (int l0 = 0; l0 < S.nfiner; l0 += S.batch) {
+            int cnt = std::min(S.batch, S.nfiner - l0);
+            a.batch = S.d_entries + 2 * S.nleaf + l0;
+            nl += fill_batch(a.batch, cnt, S.cur);
+            fluxes(cnt); correct(cnt); update(cnt);
+            nl += pipe + 2;
+        }
+    }
+    CKA(cudaGetLastError());
+    return FXB_OK;
+}
+
 // Launch-shape search on the attached state: the guard fill, sigma, the PPM
 // slopes and the update are timed with 1, 2, 4, 8 and 16 CTAs per block (one
 // warm-up pass, one timed pass each) and the fastest count per stage is kept
@@ -1258,18 +1345,60 @@ int amr_tune()
         for (int k = 0; k < 4; k++)
             if (t[k] < best[k]) { best[k] = t[k]; pick[k] = c; }
     }
-    for (int i = 0; i < 5; i++) cudaEventDestroy(e[i]);
     S.fill_cta = pick[0];
     S.cta[0] = pick[1];
     S.cta[1] = pick[2];
     S.cta[2] = pick[2];
     S.cta[3] = pick[3];
+    // the step's form: one persistent kernel with clusters of K CTAs per
+    // leaf, or the batched launches; each timed over a whole step (one
+    // warm-up run, one timed run), the fastest kept.  FXB_AMR_PERSISTENT=1
+    // keeps the persistent kernel, FXB_AMR_CLUSTER=K its cluster size.
+    char form[160] = "";
+    if (S.persist_ok && !S.test_stall) {
+        auto time_step = [&](bool pers, float &ms) -> int {
+            for (int rep = 0; rep < 2; rep++) {
+                CKA(cudaEventRecord(e[0], S.C.stream));
+                int nl = 0;
+                int rc = pers ? persist_step(nullptr, 0.0) : batched_step(nullptr, 0.0, nl);
+                if (rc) return rc;
+                CKA(cudaEventRecord(e[1], S.C.stream));
+                CKA(cudaEventSynchronize(e[1]));
+                CKA(cudaEventElapsedTime(&ms, e[0], e[1]));
+            }
+            return FXB_OK;
+        };
+        float tb = 0.f;
+        int rc = time_step(false, tb);
+        if (rc) return rc;
+        const char *ek = getenv("FXB_AMR_CLUSTER"), *ep = getenv("FXB_AMR_PERSISTENT");
+        const int kc[4] = {1, 2, 4, 8};
+        float tk[4] = {-1.f, -1.f, -1.f, -1.f}, tbest = 1e30f;
+        int kbest = S.pK;
+        for (int q = 0; q < 4; q++) {
+            if (ek && kc[q] != S.pK) continue;
+            const int nc = persist_clusters(kc[q]);
+            if (nc < 1) continue;
+            S.pK = kc[q];
+            S.pclusters = nc;
+            rc = time_step(true, tk[q]);
+            if (rc) return rc;
+            if (tk[q] < tbest) { tbest = tk[q]; kbest = kc[q]; }
+        }
+        S.pK = kbest;
+        S.pclusters = persist_clusters(kbest);
+        S.persist = (ep && ep[0] == '1') || tbest < tb;
+        snprintf(form, sizeof(form), "; step form: %s (ms per step: batched %.2f, persistent K=1 %.2f K=2 %.2f K=4 %.2f "
+                 "K=8 %.2f)", S.persist ? (kbest == 1 ? "persistent, 1 CTA per leaf" : "persistent, cluster per leaf")
+                 : "batched launches", tb, tk[0], tk[1], tk[2], tk[3]);
+    }
+    for (int i = 0; i < 5; i++) cudaEventDestroy(e[i]);
     CKA(cudaMemsetAsync(S.C.rate_max, 0, sizeof(unsigned long long), S.C.stream));
     CKA(cudaStreamSynchronize(S.C.stream));
     snprintf(S.tune_log, sizeof(S.tune_log),
              "AMR launch shape (CTAs of 256 per block, %d blocks of %d^3): fill=%d sig=%d slopes=%d update=%d "
-             "(ms fill %.3f, sigma %.3f, slopes + face states + fluxes %.3f, update %.3f)", cnt, S.n, pick[0], pick[1],
-             pick[2], pick[3], best[0], best[1], best[2], best[3]);
+             "(ms fill %.3f, sigma %.3f, slopes + face states + fluxes %.3f, update %.3f)%s", cnt, S.n, pick[0],
+             pick[1], pick[2], pick[3], best[0], best[1], best[2], best[3], form);
     return FXB_OK;
 }
 
@@ -1339,59 +1468,9 @@ int amr_fill_to_host(double *unk_host, const int pos[NV_DEV], int n, const int s
 
 int amr_step(const double *dtv, double dt, int *launches)
 {
-    if (S.persist) {
-        int rc = persist_step(dtv, dt);
-        if (rc) return rc;
-        S.cur = 1 - S.cur;
-        if (launches) *launches = 1;
-        return FXB_OK;
-    }
-    const bool mixed = S.C.prm.precision == FXB_MIXED;
-    int nl = 0;
-    nl += restrict_needed(S.cur);
-    Args3D a = batch_args(dtv, dt);
-    auto fluxes = [&](int cnt) {
-        const int all = AMR_SIG | AMR_STATES;
-        if (mixed) launch_amr3d_fluxes_mixed(a, cnt, all, S.C.stream);
-        else launch_amr3d_fluxes_fp64(a, cnt, all, S.C.stream);
-    };
-    auto emit = [&](int cnt) {
-        if (mixed) launch_amr3d_emit_mixed(a, cnt, S.bflux, S.nfc, S.C.stream);
-        else launch_amr3d_emit_fp64(a, cnt, S.bflux, S.nfc, S.C.stream);
-    };
-    auto correct = [&](int cnt) {
-        if (mixed) launch_amr3d_correct_mixed(a, cnt, S.bflux, S.nfc, S.d_fine, S.d_finer, S.C.stream);
-        else launch_amr3d_correct_fp64(a, cnt, S.bflux, S.nfc, S.d_fine, S.d_finer, S.C.stream);
-    };
-    auto update = [&](int cnt) {
-        if (mixed) launch_amr3d_update_mixed(a, cnt, S.C.stream); else launch_amr3d_update_fp64(a, cnt, S.C.stream);
-    };
-    // sigma (+ flattening), then per direction the slopes, face states and
-    // fluxes (one fused kernel in FP32; slopes (PPM), face states and fluxes
-    // as separate kernels in FP64)
-    const int pipe = 1 + (S.C.prm.flattening ? 1 : 0) + 3 * (mixed ? 1 : (S.C.prm.order == 3 ? 3 : 2));
-    if (S.nleaf <= S.batch) {
-        a.batch = S.d_entries;
-        nl += fill_batch(a.batch, S.nleaf, S.cur);
-        fluxes(S.nleaf); emit(S.nleaf); correct(S.nleaf); update(S.nleaf);
-        nl += pipe + 3;
-    } else {
-        for (int l0 = 0; l0 < S.nleaf; l0 += S.batch) {
-            int cnt = std::min(S.batch, S.nleaf - l0);
-            a.batch = S.d_entries + S.nleaf + l0;
-            nl += fill_batch(a.batch, cnt, S.cur);
-            fluxes(cnt); emit(cnt); update(cnt);
-            nl += pipe + 2;
-        }
-        for (int l0 = 0; l0 < S.nfiner; l0 += S.batch) {
-            int cnt = std::min(S.batch, S.nfiner - l0);
-            a.batch = S.d_entries + 2 * S.nleaf + l0;
-            nl += fill_batch(a.batch, cnt, S.cur);
-            fluxes(cnt); correct(cnt); update(cnt);
-            nl += pipe + 2;
-        }
-    }
-    CKA(cudaGetLastError());
+    int nl = 1;
+    int rc = S.persist ? persist_step(dtv, dt) : batched_step(dtv, dt, nl);
+    if (rc) return rc;
     S.cur = 1 - S.cur;
     if (launches) *launches = nl;
     return FXB_OK;

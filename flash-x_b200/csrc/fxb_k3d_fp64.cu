@@ -12,6 +12,8 @@ void launch_amr3d_correct_fp64(const Args3D &a, int entries, const void *bflux, 
                                const int *finer_mask, cudaStream_t s)
 { launch_amr3d_correct_t<double>(a, entries, bflux, nfc, fine, finer_mask, s); }
 void launch_amr3d_update_fp64(const Args3D &a, int entries, cudaStream_t s) { launch_amr3d_update_t<double>(a, entries, s); }
-void launch_amr_persist_fp64(const PersistArgs &p, int grid, cudaStream_t s) { launch_amr_persist_t<double>(p, grid, s); }
-int persist_grid_fp64() { return persist_grid<double>(); }
+cudaError_t launch_amr_persist_fp64(int which, int clusters, int K, cudaStream_t s)
+{ return launch_amr_persist_t<double>(which, clusters, K, s); }
+cudaError_t persist_upload_fp64(const PersistArgs p[2]) { return persist_upload_t<double>(p); }
+int persist_grid_fp64(int K) { return persist_grid<double>(K); }
 } // namespace fxb

@@ -13,6 +13,8 @@ void launch_amr3d_correct_mixed(const Args3D &a, int entries, const void *bflux,
                                const int *finer_mask, cudaStream_t s)
 { launch_amr3d_correct_t<float>(a, entries, bflux, nfc, fine, finer_mask, s); }
 void launch_amr3d_update_mixed(const Args3D &a, int entries, cudaStream_t s) { launch_amr3d_update_t<float>(a, entries, s); }
-void launch_amr_persist_mixed(const PersistArgs &p, int grid, cudaStream_t s) { launch_amr_persist_t<float>(p, grid, s); }
-int persist_grid_mixed() { return persist_grid<float>(); }
+cudaError_t launch_amr_persist_mixed(int which, int clusters, int K, cudaStream_t s)
+{ return launch_amr_persist_t<float>(which, clusters, K, s); }
+cudaError_t persist_upload_mixed(const PersistArgs p[2]) { return persist_upload_t<float>(p); }
+int persist_grid_mixed(int K) { return persist_grid<float>(K); }
 } // namespace fxb

@@ -28,8 +28,10 @@ void launch_amr3d_correct_mixed(const Args3D &a, int entries, const void *bflux,
 void launch_amr3d_update_mixed(const Args3D &a, int entries, cudaStream_t s);
 // the persistent AMR step (fxb_amr_persist.cuh): launch and resident CTAs
 struct PersistArgs;
-void launch_amr_persist_fp64(const PersistArgs &p, int grid, cudaStream_t s);
-void launch_amr_persist_mixed(const PersistArgs &p, int grid, cudaStream_t s);
-int persist_grid_fp64();
-int persist_grid_mixed();
+cudaError_t launch_amr_persist_fp64(int which, int clusters, int K, cudaStream_t s);
+cudaError_t launch_amr_persist_mixed(int which, int clusters, int K, cudaStream_t s);
+cudaError_t persist_upload_fp64(const PersistArgs p[2]);   // argument sets for current store 0 and 1
+cudaError_t persist_upload_mixed(const PersistArgs p[2]);
+int persist_grid_fp64(int K);    // clusters of K CTAs that fit at once
+int persist_grid_mixed(int K);
 } // namespace fxb

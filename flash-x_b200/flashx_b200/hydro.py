@@ -414,8 +414,8 @@ class HydroDevice:
 
     def tuning(self):
         """The launch shape in use (the batched-block path tunes it at attach)."""
-        buf = ctypes.create_string_buffer(256)
-        _check(self.lib.fxb_tuning(buf, 256))
+        buf = ctypes.create_string_buffer(1024)
+        _check(self.lib.fxb_tuning(buf, 1024))
         return buf.value.decode()
 
     def counters(self):

@@ -156,8 +156,8 @@ def test_amr_batches_agree(oracle, need_gpu, monkeypatch, persistent):
     dev.close()
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_amr_persistent_kernel_equals_batched_launches(oracle, need_gpu, monkeypatch, precision):
+@pytest.mark.parametrize("precision,cluster", [("fp64", "1"), ("fp64", "4"), ("fp64", "8"), ("mixed", "2")])
+def test_amr_persistent_kernel_equals_batched_launches(oracle, need_gpu, monkeypatch, precision, cluster):
     """One persistent kernel per step (device work queue: restriction by level,
     then the leaves finest first, each leaf's whole pipeline in one CTA, bounded
     waits for finer neighbours' boundary fluxes) against the batched launches:
@@ -168,6 +168,7 @@ def test_amr_persistent_kernel_equals_batched_launches(oracle, need_gpu, monkeyp
     am = oracle.Amr(oracle.make_params(root.as_dict(), hp), mesh.levels, mesh.bcoords)
     dt = 0.5 * am.compute_dt(unk)
     outs = {}
+    monkeypatch.setenv("FXB_AMR_CLUSTER", cluster)          # CTAs per leaf (a thread-block cluster)
     for flag in ("0", "1"):
         monkeypatch.setenv("FXB_AMR_PERSISTENT", flag)
         dev, out = _gpu(root, hp, mesh, unk, [dt, dt, dt], precision)
