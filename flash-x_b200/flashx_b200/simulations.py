@@ -70,14 +70,16 @@ def cell_coords(geom: Geometry):
 
 
 def scatter_global(geom: Geometry, field_zyx):
-    """Global (nz, ny, nx, nvar) interior -> UNK with zeroed guard cells."""
-    unk = np.zeros(geom.unk_shape)
+    """Global (nz, ny, nx, nvar) interior -> UNK with zeroed guard cells
+    (nvar values per cell: UNK's, or the mass fractions of a species array)."""
+    nv = field_zyx.shape[-1]
+    unk = np.zeros(geom.unk_shape[:-1] + (nv,))
     g = geom.nguard
     nk, nj, ni = (geom.nzb if geom.ndim == 3 else 1), (geom.nyb if geom.ndim >= 2 else 1), geom.nxb
     gk, gj = (g if geom.ndim == 3 else 0), (g if geom.ndim >= 2 else 0)
     f = field_zyx.reshape(geom.nblockz if geom.ndim == 3 else 1, nk,
-                          geom.nblocky if geom.ndim >= 2 else 1, nj, geom.nblockx, ni, NUNK)
-    blocks = f.transpose(0, 2, 4, 1, 3, 5, 6).reshape(-1, nk, nj, ni, NUNK)
+                          geom.nblocky if geom.ndim >= 2 else 1, nj, geom.nblockx, ni, nv)
+    blocks = f.transpose(0, 2, 4, 1, 3, 5, 6).reshape(-1, nk, nj, ni, nv)
     unk[:, gk:gk + nk, gj:gj + nj, g:g + ni, :] = blocks
     return unk
 
@@ -89,8 +91,9 @@ def gather_global(geom: Geometry, unk):
     gk, gj = (g if geom.ndim == 3 else 0), (g if geom.ndim >= 2 else 0)
     bz = geom.nblockz if geom.ndim == 3 else 1
     by = geom.nblocky if geom.ndim >= 2 else 1
-    inner = unk[:, gk:gk + nk, gj:gj + nj, g:g + ni, :].reshape(bz, by, geom.nblockx, nk, nj, ni, NUNK)
-    return inner.transpose(0, 3, 1, 4, 2, 5, 6).reshape(bz * nk, by * nj, geom.nblockx * ni, NUNK)
+    nv = unk.shape[-1]
+    inner = unk[:, gk:gk + nk, gj:gj + nj, g:g + ni, :].reshape(bz, by, geom.nblockx, nk, nj, ni, nv)
+    return inner.transpose(0, 3, 1, 4, 2, 5, 6).reshape(bz * nk, by * nj, geom.nblockx * ni, nv)
 
 
 def eos_dens_ei(hp: HydroParams, u):
@@ -231,6 +234,26 @@ def noisy_gas(geom: Geometry, hp: HydroParams, vmag=0.1, noise=0.05):
 
 
 # ---------------------------------------------------------------- configurations
+def species_blob(geom: Geometry, ns=3, nspecies=2, center=(0.5, 0.5, 0.5), radius=0.2, width=0.03):
+    """Advected mass fractions, (blk, k, j, i, ns) like UNK: species 0 is a
+    smoothed disc (sphere in 3-D) of `radius` around `center`, species 1 its
+    complement (the species add up to one), further values mass scalars
+    0.3 + 0.2 sin(2 pi x) sin(2 pi y) (not renormalised)."""
+    xc, yc, zc, _, _ = cell_coords(geom)
+    Z, Y, X = np.meshgrid(zc, yc, xc, indexing="ij")
+    r2 = (X - center[0]) ** 2 + (Y - center[1]) ** 2
+    if geom.ndim == 3:
+        r2 = r2 + (Z - center[2]) ** 2
+    blob = 0.5 * (1.0 - np.tanh((np.sqrt(r2) - radius) / width))
+    f = np.zeros(X.shape + (ns,))
+    f[..., 0] = blob
+    if nspecies > 1:
+        f[..., 1] = 1.0 - blob
+    for q in range(nspecies, ns):
+        f[..., q] = 0.3 + 0.2 * np.sin(2 * math.pi * X) * np.sin(2 * math.pi * Y) + 0.01 * q
+    return scatter_global(geom, f)
+
+
 def config(name, scale=1):
     """(Geometry, HydroParams, init function) for a named benchmark problem.
     scale < 1 shrinks the block count per axis for quick parity cases."""

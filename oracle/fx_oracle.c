@@ -643,6 +643,7 @@ typedef struct {
     double *pav;        /* VAR1 averaged pressure [cell] */
     double *flat;       /* flattening: FlatTilde [3][cell], then FlatCoeff [3][cell] */
     double *divu;       /* hybrid order: undivided velocity divergence [cell] */
+    unsigned char *ctufb;   /* 3-D CTU: 1 where the face states of (cell, dir) fell back to first order */
 } scratch_t;
 
 static void scratch_alloc(scratch_t *s, long ncell)
@@ -658,11 +659,12 @@ static void scratch_alloc(scratch_t *s, long ncell)
     s->pav = (double *)calloc((size_t)ncell, sizeof(double));
     s->flat = (double *)calloc((size_t)ncell * 6, sizeof(double));
     s->divu = (double *)calloc((size_t)ncell, sizeof(double));
+    s->ctufb = (unsigned char *)calloc((size_t)ncell * 3, 1);
 }
 static void scratch_free(scratch_t *s)
 {
     for (int d = 0; d < 3; d++) { free(s->scr[d]); free(s->flx[d]); }
-    free(s->sig); free(s->lam); free(s->leig); free(s->reig); free(s->pav); free(s->flat); free(s->divu);
+    free(s->sig); free(s->lam); free(s->leig); free(s->reig); free(s->pav); free(s->flat); free(s->divu); free(s->ctufb);
 }
 
 static void blk_init(blk_t *b, const fxo_params *p)
@@ -925,8 +927,10 @@ static int riemann_states(const blk_t *b, const double *U, double dt, scratch_t 
                     scr[v] = scr[v] + (T1[v] + T2[v]) * fac;
                     scr[8 + v] = scr[8 + v] + (T1[v] + T2[v]) * fac;
                 }
+                s->ctufb[c * 3 + fd] = 0;
                 if (scr[0] <= 0. || scr[8] <= 0. || scr[4] <= 0. || scr[12] <= 0.) {
                     for (int v = 0; v < 8; v++) { scr[v] = Vc[v]; scr[8 + v] = Vc[v]; }
+                    s->ctufb[c * 3 + fd] = 1;
                 }
             }
         }
@@ -1170,7 +1174,21 @@ long fxo_index(const fxo_params *p, int var, int i, int j, int k, int blk)
  * full guard extent of the other axes, followed by the physical boundary
  * conditions applied in the order Z, Y, X over whole guard vectors
  * (gr_bcApplyToAllBlks with WHOLE_VECTOR), as Grid_fillGuardCells.F90:300. */
-int fxo_fill_guardcells(const fxo_params *p, double *unk)
+#include "fx_oracle_spec.inc"
+
+/* UG guard fill of nv values per cell (UNK: nv = FXO_NUNK with the normal
+ * velocity flipped at reflecting faces; mass fractions: nv = ns, no flip) */
+static int fill_guard_nv(const fxo_params *p, double *unk, int nv, int flip);
+
+int fxo_fill_guardcells(const fxo_params *p, double *unk) { return fill_guard_nv(p, unk, FXO_NUNK, 1); }
+
+int fxo_fill_guardcells_spec(const fxo_params *p, double *spec, int ns)
+{
+    if (ns <= 0) return 0;
+    return fill_guard_nv(p, spec, ns, 0);
+}
+
+static int fill_guard_nv(const fxo_params *p, double *unk, int nv, int flip)
 {
     blk_t b; blk_init(&b, p);
     const int ng = b.ng, ndim = p->ndim;
@@ -1180,19 +1198,19 @@ int fxo_fill_guardcells(const fxo_params *p, double *unk)
     long N[3], G[3];
     for (int d = 0; d < 3; d++) { N[d] = (long)nb[d] * nn[d]; G[d] = N[d] + 2 * gx[d]; }
     /* global grid with a guard ring */
-    double *g = (double *)malloc(sizeof(double) * G[0] * G[1] * G[2] * FXO_NUNK);
-#define GI(i, j, k) ((((long)(k) * G[1] + (j)) * G[0] + (i)) * FXO_NUNK)
+    double *g = (double *)malloc(sizeof(double) * G[0] * G[1] * G[2] * nv);
+#define GI(i, j, k) ((((long)(k) * G[1] + (j)) * G[0] + (i)) * nv)
     long nblk = (long)nb[0] * nb[1] * nb[2];
     for (long blk = 0; blk < nblk; blk++) {
         int bx = blk % nb[0], by = (blk / nb[0]) % nb[1], bz = blk / ((long)nb[0] * nb[1]);
-        const double *U = unk + blk * b.ncell * FXO_NUNK;
+        const double *U = unk + blk * b.ncell * nv;
         for (int k = b.k0; k <= b.kmax; k++)
         for (int j = b.j0; j <= b.jmax; j++)
         for (int i = b.i0; i <= b.imax; i++) {
             long gi = (long)bx * nn[0] + (i - b.i0) + gx[0];
             long gj = (long)by * nn[1] + (j - b.j0) + gx[1];
             long gk = (long)bz * nn[2] + (k - b.k0) + gx[2];
-            memcpy(g + GI(gi, gj, gk), U + cidx(&b, i, j, k) * FXO_NUNK, sizeof(double) * FXO_NUNK);
+            memcpy(g + GI(gi, gj, gk), U + cidx(&b, i, j, k) * nv, sizeof(double) * nv);
         }
     }
     /* periodic exchanges, axis order X, Y, Z, full extent of the other axes */
@@ -1204,7 +1222,7 @@ int fxo_fill_guardcells(const fxo_params *p, double *unk)
             if (x >= gx[a] && x < gx[a] + N[a]) continue;
             long src = (x < gx[a]) ? x + N[a] : x - N[a];
             long sidx[3] = {i, j, k}; sidx[a] = src;
-            memcpy(g + GI(i, j, k), g + GI(sidx[0], sidx[1], sidx[2]), sizeof(double) * FXO_NUNK);
+            memcpy(g + GI(i, j, k), g + GI(sidx[0], sidx[1], sidx[2]), sizeof(double) * nv);
         }
     }
     /* physical boundaries, order Z, Y, X */
@@ -1226,8 +1244,8 @@ int fxo_fill_guardcells(const fxo_params *p, double *unk)
                 }
                 double *dst = g + GI(i, j, k);
                 const double *src = g + GI(sidx[0], sidx[1], sidx[2]);
-                for (int v = 0; v < FXO_NUNK; v++) {
-                    double sgn = (bc == FXO_BC_REFLECTING && v == FXO_VELX + a) ? -1. : 1.;
+                for (int v = 0; v < nv; v++) {
+                    double sgn = (flip && bc == FXO_BC_REFLECTING && v == FXO_VELX + a) ? -1. : 1.;
                     dst[v] = src[v] * sgn;
                 }
             }
@@ -1236,14 +1254,14 @@ int fxo_fill_guardcells(const fxo_params *p, double *unk)
     /* scatter windows back into each block's guard cells */
     for (long blk = 0; blk < nblk; blk++) {
         int bx = blk % nb[0], by = (blk / nb[0]) % nb[1], bz = blk / ((long)nb[0] * nb[1]);
-        double *U = unk + blk * b.ncell * FXO_NUNK;
+        double *U = unk + blk * b.ncell * nv;
         for (int k = 0; k < b.nkg; k++)
         for (int j = 0; j < b.njg; j++)
         for (int i = 0; i < b.nig; i++) {
             long gi = (long)bx * nn[0] + i;
             long gj = (long)by * nn[1] + j;
             long gk = (long)bz * nn[2] + k;
-            memcpy(U + cidx(&b, i, j, k) * FXO_NUNK, g + GI(gi, gj, gk), sizeof(double) * FXO_NUNK);
+            memcpy(U + cidx(&b, i, j, k) * nv, g + GI(gi, gj, gk), sizeof(double) * nv);
         }
     }
 #undef GI
@@ -1261,9 +1279,17 @@ int fxo_eos_interior(const fxo_params *p, double *unk)
 
 int fxo_hydro_step(const fxo_params *p, double *unk, double dt, double dt_old, int nthreads)
 {
+    return fxo_hydro_step_spec(p, unk, NULL, 0, 0, dt, dt_old, nthreads);
+}
+
+int fxo_hydro_step_spec(const fxo_params *p, double *unk, double *spec, int ns, int nsp, double dt, double dt_old,
+                        int nthreads)
+{
     (void)dt_old;
     if (p->ndim < 2 || p->ndim > 3 || p->nguard < 4 || (p->order != 2 && p->order != 3 && p->order != 5)) return 3;
+    if (ns < 0 || nsp < 0 || nsp > ns || (ns > 0 && !spec)) return 3;
     fxo_fill_guardcells(p, unk);
+    if (ns) fxo_fill_guardcells_spec(p, spec, ns);
     blk_t b; blk_init(&b, p);
     long nblk = (long)p->nblockx * p->nblocky * p->nblockz;
     int status = 0;
@@ -1274,20 +1300,31 @@ int fxo_hydro_step(const fxo_params *p, double *unk, double dt, double dt_old, i
     {
         scratch_t s;
         scratch_alloc(&s, b.ncell);
+        spec_t q;
+        memset(&q, 0, sizeof(q));
+        if (ns) spec_alloc(&q, b.ncell, ns);
         int lerr = 0;
 #ifdef _OPENMP
 #pragma omp for schedule(dynamic, 1)
 #endif
         for (long blk = 0; blk < nblk; blk++) {
             double *U = unk + blk * b.ncell * FXO_NUNK;
+            double *SP = ns ? spec + blk * b.ncell * ns : NULL;
             int e = riemann_states(&b, U, dt, &s);
             if (!e) e = face_fluxes(&b, U, &s);
             if (!e) {
+                if (ns) {
+                    spec_states(&b, U, SP, dt, &s, &q);
+                    spec_fluxes(&b, &s, &q);
+                    for (long c = 0; c < b.ncell; c++) q.dold[c] = U[c * FXO_NUNK + FXO_DENS];
+                }
                 unsplit_update(&b, U, dt, &s);
+                if (ns) spec_update(&b, U, SP, dt, &q, nsp);
                 if (!p->use_gravity) { energy_fix(&b, U); eos_block(&b, U); }
             }
             if (e) lerr = e;
         }
+        if (ns) spec_free(&q);
         scratch_free(&s);
 #ifdef _OPENMP
 #pragma omp critical

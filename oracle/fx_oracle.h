@@ -77,6 +77,12 @@ int fxo_eos_interior(const fxo_params *p, double *unk);
  * (1 imaginary sound speed, 2 Riemann solver failure). */
 int fxo_hydro_step(const fxo_params *p, double *unk, double dt, double dt_old,
                    int nthreads);
+/* fxo_hydro_step with ns advected mass fractions per cell, spec[blk][k][j][i][ns]
+ * (guard cells included, like UNK), the first nsp of them species that are
+ * renormalised to add up to one, the rest mass scalars (fx_oracle_spec.inc) */
+int fxo_hydro_step_spec(const fxo_params *p, double *unk, double *spec, int ns, int nsp, double dt,
+                        double dt_old, int nthreads);
+int fxo_fill_guardcells_spec(const fxo_params *p, double *spec, int ns);
 /* Hydro_computeDt over all blocks: returns the global CFL time step. */
 int fxo_compute_dt(const fxo_params *p, const double *unk, double *dt_out);
 /* Driver_computeDt growth limit and clamp (Driver_computeDt.F90:452,460). */

@@ -68,6 +68,9 @@ def lib():
         L.fxo_fill_guardcells.argtypes = [P, D]
         L.fxo_eos_interior.argtypes = [P, D]
         L.fxo_hydro_step.argtypes = [P, D, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        L.fxo_hydro_step_spec.argtypes = [P, D, D, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_int]
+        L.fxo_fill_guardcells_spec.argtypes = [P, D, ctypes.c_int]
         L.fxo_compute_dt.argtypes = [P, D, D]
         L.fxo_driver_dt.argtypes = [ctypes.c_double] * 5
         L.fxo_driver_dt.restype = ctypes.c_double
@@ -138,10 +141,21 @@ def eos_interior(p, unk):
     lib().fxo_eos_interior(ctypes.byref(p), _dp(unk))
 
 
-def hydro_step(p, unk, dt, dt_old, nthreads=0):
-    rc = lib().fxo_hydro_step(ctypes.byref(p), _dp(unk), dt, dt_old, nthreads)
+def hydro_step(p, unk, dt, dt_old, nthreads=0, spec=None, nspecies=None):
+    """One unsplit step; `spec` (blk, k, j, i, ns) advects ns mass fractions
+    with it, the first `nspecies` (default all) renormalised as species."""
+    if spec is None:
+        rc = lib().fxo_hydro_step(ctypes.byref(p), _dp(unk), dt, dt_old, nthreads)
+    else:
+        ns = spec.shape[-1]
+        nsp = ns if nspecies is None else nspecies
+        rc = lib().fxo_hydro_step_spec(ctypes.byref(p), _dp(unk), _dp(spec), ns, nsp, dt, dt_old, nthreads)
     if rc:
         raise RuntimeError(f"oracle hydro step failed with code {rc}")
+
+
+def fill_guardcells_spec(p, spec):
+    lib().fxo_fill_guardcells_spec(ctypes.byref(p), _dp(spec), spec.shape[-1])
 
 
 def compute_dt(p, unk):
