@@ -5,6 +5,7 @@
 #include "../../include/flashx_b200.h"
 #include "fxb_launch.h"
 #include "fxb_amr.h"
+#include "fxb_species.cuh"
 
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
@@ -74,6 +75,16 @@ struct Lib {
     void *slp3 = nullptr;          // PPM slopes of one direction (3-D)
     void *flat = nullptr;          // flattening coefficients (2-D and 3-D)
     void *hyb = nullptr;           // hybrid order (3-D): DivU and the per-cell flags
+    // species and mass scalars (fxb_init_species): mass fractions [ns][vstride]
+    // per state buffer, their scratch, the hydro's exports
+    int ns = 0, nsp = 0;
+    int sslot[FXB_MAX_SPECIES];
+    int *sslot_dev = nullptr;
+    double *spb[2] = {nullptr, nullptr};
+    void *ssg = nullptr, *ssl = nullptr, *ssr = nullptr;
+    void *sfd[2] = {nullptr, nullptr};             // 2-D mass fluxes
+    unsigned char *ctufb[3] = {nullptr, nullptr, nullptr};   // 3-D CTU fallback flags
+    long snpad = 0, snw = 0;
     CUtensorMap tmap2d[2];         // 2-D: the window variables of buf[0] / buf[1] for TMA
     int use_tma = 1;
     unsigned tma_extra_tx = 0;     // test hook (FXB_TEST_WAIT_TIMEOUT): a window barrier that never completes
@@ -169,6 +180,49 @@ __global__ void state_to_unk_kernel(const double *__restrict__ st, double *__res
             if (v == VZ) val = val * sz;
             unk[u + dmap[v]] = val;
         }
+    }
+}
+
+// UNK species slots <-> device mass fractions (interior on the way in; with
+// the guard cells, filled by the boundary conditions without sign flips, on
+// the way out)
+__global__ void unk_to_spec_kernel(const double *__restrict__ unk, double *__restrict__ sp, UnkGeom g,
+                                   const int *__restrict__ bcoord, const int *__restrict__ slot, int ns, int nblk)
+{
+    long n = (long)nblk * g.nxb * g.nyb * g.nzb;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
+        long per = (long)g.nxb * g.nyb * g.nzb;
+        int blk = (int)(idx / per);
+        long r = idx - blk * per;
+        int k = (int)(r / ((long)g.nxb * g.nyb)); r -= (long)k * g.nxb * g.nyb;
+        int j = (int)(r / g.nxb), i = (int)(r - (long)j * g.nxb);
+        int gj = g.ndim >= 2 ? g.ng : 0, gk = g.ndim == 3 ? g.ng : 0;
+        long u = ((((long)blk * g.nkg + k + gk) * g.njg + j + gj) * g.nig + i + g.ng) * g.nunk;
+        long gx = (long)bcoord[3 * blk] * g.nxb + i;
+        long gy = (long)bcoord[3 * blk + 1] * g.nyb + j;
+        long gz = (long)bcoord[3 * blk + 2] * g.nzb + k;
+        long c = (gz * g.ny + gy) * g.nx + gx;
+        for (int q = 0; q < ns; q++) sp[q * g.vstride + c] = unk[u + slot[q]];
+    }
+}
+
+__global__ void spec_to_unk_kernel(const double *__restrict__ sp, double *__restrict__ unk, UnkGeom g,
+                                   const int *__restrict__ bcoord, const int *__restrict__ slot, int ns, int nblk)
+{
+    long per = (long)g.nig * g.njg * g.nkg;
+    long n = (long)nblk * per;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
+        int blk = (int)(idx / per);
+        long r = idx - blk * per;
+        int k = (int)(r / ((long)g.nig * g.njg)); r -= (long)k * g.nig * g.njg;
+        int j = (int)(r / g.nig), i = (int)(r - (long)j * g.nig);
+        int gj = g.ndim >= 2 ? g.ng : 0, gk = g.ndim == 3 ? g.ng : 0;
+        double s_ = 1.0;
+        int mx = map_axis(bcoord[3 * blk] * g.nxb + i - g.ng, g.nx, g.bc[0], g.bc[1], &s_);
+        int my = g.ndim >= 2 ? map_axis(bcoord[3 * blk + 1] * g.nyb + j - gj, g.ny, g.bc[2], g.bc[3], &s_) : 0;
+        int mz = g.ndim == 3 ? map_axis(bcoord[3 * blk + 2] * g.nzb + k - gk, g.nz, g.bc[4], g.bc[5], &s_) : 0;
+        long c = ((long)mz * g.ny + my) * g.nx + mx;
+        for (int q = 0; q < ns; q++) unk[idx * g.nunk + slot[q]] = sp[q * g.vstride + c];
     }
 }
 
@@ -338,6 +392,8 @@ int encode_window_map(CUtensorMap *m, const double *base)
     return FXB_OK;
 }
 
+int launch_species(int src, const double *dtv, double dt);
+
 // launch one fused hydro step reading buffer `src`, writing 1-src
 int launch_hydro(int src, const double *dtv, double dt)
 {
@@ -354,6 +410,7 @@ int launch_hydro(int src, const double *dtv, double dt)
         a.prm = L.dprm; a.rate_max = L.rate_max; a.err = L.err;
         a.flat = L.flat;
         a.tmap = L.tmap2d[src];
+        a.fd[0] = L.sfd[0]; a.fd[1] = L.sfd[1];
         a.use_tma = L.use_tma;
         a.tma_extra_tx = L.tma_extra_tx;
         a.wait_budget = L.wait_budget;
@@ -377,12 +434,43 @@ int launch_hydro(int src, const double *dtv, double dt)
         a.flat = L.flat;
         a.flat_bstride = 0;
         a.hyb = (const unsigned char *)L.hyb;
-        for (int d = 0; d < 3; d++) { a.wst[d] = L.w3[d]; a.flx[d] = L.f3[d]; }
+        for (int d = 0; d < 3; d++) { a.wst[d] = L.w3[d]; a.flx[d] = L.f3[d]; a.ctufb[d] = L.ctufb[d]; }
+        for (int d = 0; d < 3 && L.ns; d++)
+            if (cudaMemsetAsync(L.ctufb[d], 0, L.snw, L.stream) != cudaSuccess) return cuda_fail(cudaGetLastError(), "memset");
         if (L.prm.precision == FXB_MIXED) launch_hydro3d_mixed(a, L.stream);
         else launch_hydro3d_fp64(a, L.stream);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "hydro kernel launch");
+    if (L.ns) return launch_species(src, dtv, dt);
+    return FXB_OK;
+}
+
+// species after the hydro step that read buffer `src` and wrote 1-src
+int launch_species(int src, const double *dtv, double dt)
+{
+    SpecArgs s;
+    memset((void *)&s, 0, sizeof(s));
+    s.st_old = L.buf[src]; s.st_new = L.buf[1 - src]; s.vstride = L.vstride;
+    s.sp_in = L.spb[src]; s.sp_out = L.spb[1 - src];
+    s.ns = L.ns; s.nsp = L.nsp;
+    s.ndim = L.dom.ndim; s.nx = L.nx; s.ny = L.ny; s.nz = L.nz;
+    for (int i = 0; i < 6; i++) s.bc[i] = L.kbc[i];
+    s.dx = cell_dx(0); s.dy = cell_dx(1); s.dz = cell_dx(2);
+    s.dt_arg = dt; s.dtv = dtv;
+    s.prm = L.dprm;
+    if (L.dom.ndim == 2) {
+        s.fd[0] = L.sfd[0]; s.fd[1] = L.sfd[1];
+    } else {
+        for (int d = 0; d < 3; d++) { s.fd[d] = L.f3[d]; s.ctufb[d] = L.ctufb[d]; }
+    }
+    s.flat = L.flat;
+    s.sg = L.ssg; s.sl = L.ssl; s.sr = L.ssr;
+    s.npad = L.snpad; s.nwmax = L.snw;
+    if (L.prm.precision == FXB_MIXED) launch_species_mixed(s, L.stream);
+    else launch_species_fp64(s, L.stream);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "species kernel launch");
     return FXB_OK;
 }
 
@@ -393,6 +481,11 @@ int hydro3d_launches(const fxb_params &p)
 {
     const int per_dir = p.precision == FXB_MIXED ? 1 : (p.order == 3 ? 3 : 2);
     return 1 + 3 * per_dir + 1;
+}
+// launches of one uniform-grid step (flattening and species add kernels)
+int ug_step_launches()
+{
+    return (L.dom.ndim == 2 ? 1 : hydro3d_launches(L.prm)) + (L.prm.flattening ? 1 : 0) + (L.ns ? 3 : 0);
 }
 
 int check_err_word()
@@ -425,6 +518,16 @@ void free_all()
     if (L.unk_dev) cudaFree(L.unk_dev);
     if (L.bcoord) cudaFree(L.bcoord);
     if (L.dmap_dev) cudaFree(L.dmap_dev);
+    if (L.sslot_dev) cudaFree(L.sslot_dev);
+    for (int i = 0; i < 2; i++) {
+        if (L.spb[i]) cudaFree(L.spb[i]);
+        if (L.sfd[i]) cudaFree(L.sfd[i]);
+    }
+    if (L.ssg) cudaFree(L.ssg);
+    if (L.ssl) cudaFree(L.ssl);
+    if (L.ssr) cudaFree(L.ssr);
+    for (int d = 0; d < 3; d++)
+        if (L.ctufb[d]) cudaFree(L.ctufb[d]);
     if (L.pmap_dev) cudaFree(L.pmap_dev);
     if (L.pack_dev) cudaFree(L.pack_dev);
     if (L.pack_host) cudaFreeHost(L.pack_host);
@@ -618,6 +721,55 @@ extern "C" int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
     return FXB_OK;
 }
 
+extern "C" int fxb_init_species(int nspec, int nspecies, const int32_t *unk_slots)
+{
+    if (!L.inited) return fail(FXB_EARG, "fxb_init_species: call fxb_init first");
+    if (nspec < 1 || nspec > FXB_MAX_SPECIES || nspecies < 0 || nspecies > nspec || !unk_slots)
+        return fail(FXB_EARG, "fxb_init_species: need 1..FXB_MAX_SPECIES values, at most nspec species, and their slots");
+    if (L.ns) return fail(FXB_EARG, "fxb_init_species: species are already set");
+    if (amr_active()) return fail(FXB_EUNSUPPORTED, "fxb_init_species: species on AMR meshes are not implemented");
+    if (has_halo()) return fail(FXB_EUNSUPPORTED, "fxb_init_species: species on a slab with halos are not implemented");
+    for (int q = 0; q < nspec; q++) {
+        if (unk_slots[q] < 0 || unk_slots[q] >= L.nunk) return fail(FXB_EARG, "fxb_init_species: slot out of range");
+        for (int v = 0; v < NV_DEV; v++)
+            if (unk_slots[q] == L.dmap[v]) return fail(FXB_EARG, "fxb_init_species: slot of a hydro variable");
+        for (int r = 0; r < q; r++)
+            if (unk_slots[r] == unk_slots[q]) return fail(FXB_EARG, "fxb_init_species: duplicate slot");
+    }
+    const bool mixed = L.prm.precision == FXB_MIXED;
+    const size_t rsz = mixed ? sizeof(float) : sizeof(double);
+    const int nd = L.dom.ndim;
+    L.snpad = (long)(L.nx + 2) * (L.ny + 2) * (nd == 3 ? L.nz + 2 : 1);
+    const long nz = nd == 3 ? L.nz : 1;
+    L.snw = std::max((long)(L.nx + 2) * L.ny * nz, (long)L.nx * (L.ny + 2) * nz);
+    if (nd == 3) L.snw = std::max(L.snw, (long)L.nx * L.ny * (L.nz + 2));
+    for (int i = 0; i < 2; i++) {
+        CK(cudaMalloc(&L.spb[i], sizeof(double) * L.vstride * nspec));
+        CK(cudaMemsetAsync(L.spb[i], 0, sizeof(double) * L.vstride * nspec, L.stream));
+    }
+    CK(cudaMalloc(&L.ssg, rsz * 3 * nspec * L.snpad));
+    CK(cudaMalloc(&L.ssl, rsz * 3 * nspec * L.snw));
+    CK(cudaMalloc(&L.ssr, rsz * 3 * nspec * L.snw));
+    if (nd == 2) {
+        CK(cudaMalloc(&L.sfd[0], rsz * (size_t)(L.nx + 1) * L.ny));
+        CK(cudaMalloc(&L.sfd[1], rsz * (size_t)L.nx * (L.ny + 1)));
+    } else {
+        for (int d = 0; d < 3; d++) CK(cudaMalloc(&L.ctufb[d], (size_t)L.snw));
+    }
+    CK(cudaMalloc(&L.sslot_dev, sizeof(int) * nspec));
+    for (int q = 0; q < nspec; q++) L.sslot[q] = unk_slots[q];
+    CK(cudaMemcpyAsync(L.sslot_dev, L.sslot, sizeof(int) * nspec, cudaMemcpyHostToDevice, L.stream));
+    CK(cudaStreamSynchronize(L.stream));
+    L.ns = nspec;
+    L.nsp = nspecies;
+    L.dprm.nspec = nspec;          // the step runs the extended-option kernels, which export what species read
+    for (int i = 0; i < 2; i++) {
+        if (L.graph_exec[i]) cudaGraphExecDestroy(L.graph_exec[i]);
+        L.graph_exec[i] = nullptr;
+    }
+    return FXB_OK;
+}
+
 extern "C" int fxb_register_blocks(const fxb_block_desc *blocks, int nblk)
 {
     if (!L.inited) return fail(FXB_EARG, "fxb_register_blocks: call fxb_init first");
@@ -631,6 +783,7 @@ extern "C" int fxb_register_blocks(const fxb_block_desc *blocks, int nblk)
         L.graph_exec[i] = nullptr;
     }
     if (refined) {
+        if (L.ns) return fail(FXB_EUNSUPPORTED, "fxb_register_blocks: species on AMR meshes are not implemented");
         const int nlay = L.dom.ndim == 3 ? L.dom.nblockz : L.dom.nblocky;
         if (has_halo() || L.slab.layer_lo != 0 || L.slab.layer_hi != nlay)
             return fail(FXB_EUNSUPPORTED, "fxb_register_blocks: a slab of a grid takes its level-1 blocks only");
@@ -689,6 +842,8 @@ extern "C" int fxb_attach_unk(const double *unk_host)
     CK(cudaMemcpyAsync(L.unk_dev, unk_host, sizeof(double) * L.unk_doubles, cudaMemcpyHostToDevice, L.stream));
     UnkGeom g = unk_geom();
     unk_to_state_kernel<<<1184, 256, 0, L.stream>>>(L.unk_dev, L.buf[L.cur], g, L.bcoord, L.dmap_dev, L.nblk);
+    if (L.ns)
+        unk_to_spec_kernel<<<1184, 256, 0, L.stream>>>(L.unk_dev, L.spb[L.cur], g, L.bcoord, L.sslot_dev, L.ns, L.nblk);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(L.stream));
     L.attached = true;
@@ -709,6 +864,8 @@ extern "C" int fxb_sync_to_host(double *unk_host)
     }
     UnkGeom g = unk_geom();
     state_to_unk_kernel<<<1184, 256, 0, L.stream>>>(L.buf[L.cur], L.unk_dev, g, L.bcoord, L.dmap_dev, L.nblk);
+    if (L.ns)
+        spec_to_unk_kernel<<<1184, 256, 0, L.stream>>>(L.spb[L.cur], L.unk_dev, g, L.bcoord, L.sslot_dev, L.ns, L.nblk);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(unk_host, L.unk_dev, sizeof(double) * L.unk_doubles, cudaMemcpyDeviceToHost, L.stream));
     CK(cudaStreamSynchronize(L.stream));
@@ -837,7 +994,7 @@ extern "C" int fxb_hydro_step(double sim_time, double dt, double dt_old)
         int rc = launch_hydro(L.cur, nullptr, dt);
         if (rc) return rc;
         L.cur = 1 - L.cur;
-        nl = (L.dom.ndim == 2 ? 1 : hydro3d_launches(L.prm)) + (L.prm.flattening ? 1 : 0);
+        nl = ug_step_launches();
     }
     CK(cudaEventRecord(L.ev1, L.stream));
     state_changed(true);
@@ -936,7 +1093,7 @@ extern "C" int fxb_advance(int nsteps, double *dt, double *dt_old, double f, dou
     CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
     // graphs of two steps (buffer c -> 1-c -> c), built once per starting buffer
     const bool amr = amr_active();
-    int step_launches = (L.dom.ndim == 2 ? 1 : hydro3d_launches(L.prm)) + (L.prm.flattening ? 1 : 0);
+    int step_launches = amr ? 0 : ug_step_launches();
     auto one_step = [&](int src) -> int {
         int rc = amr ? amr_step(L.dtv, 0., &step_launches) : launch_hydro(src, L.dtv, 0.);
         if (rc) return rc;

@@ -35,6 +35,7 @@ struct DevParams {
     double cvisc;
     int use_hybrid;            // hybrid order: first-order states at shocks
     double hybrid_kappa;
+    int nspec;                 // advected mass fractions (species and mass scalars; uniform grids)
 };
 
 // ---- precision helpers ---------------------------------------------------
@@ -54,10 +55,11 @@ template <> __device__ __forceinline__ float divc<float>(float x, double c) { re
 // options compiled only into kernel instantiations of their own (template
 // flag EXT), so the default kernels keep their registers: the Roe solver,
 // PPM contact steepening, MUSCL-Hancock reconstruction (order 2), artificial
-// viscosity, hybrid order
+// viscosity, hybrid order, and the exports species advection reads (2-D mass
+// fluxes)
 __host__ __device__ inline bool extended_options(const DevParams &p)
 {
-    return p.riemann == 1 || p.steepening || p.order == 2 || p.use_avisc || p.use_hybrid;
+    return p.riemann == 1 || p.steepening || p.order == 2 || p.use_avisc || p.use_hybrid || p.nspec > 0;
 }
 
 // Fortran MIN/MAX with gfortran's argument order: mvar = a1; if (a2 < mvar) mvar = a2

@@ -47,6 +47,7 @@ struct alignas(64) Args2D {
     unsigned long long *rate_max;
     int *err;
     const void *flat;        // flattening coefficients [2][(nx+2)(ny+2)] of R, padded by one cell
+    void *fd[2] = {nullptr, nullptr};   // species on: the mass flux of every x / y face, R ((nx+1) ny, nx (ny+1))
     long rate_c0 = 0, rate_c1 = 0x7fffffffffffffffL;   // cells [c0, c1) enter the CFL rate (a slab's own)
 };
 
@@ -443,6 +444,8 @@ hydro2d_kernel(const __grid_constant__ Args2D a)
     for (int t = tid; t < NFC; t += NT2) {
         int fi = t % (T2 + 1), jj = t / (T2 + 1);
         faces_stage<R, EXT>(a, s, 0, t, jj * (T2 + 2) + fi, jj * (T2 + 2) + fi + 1, fi + 2, jj + 3, fi + 3, jj + 3);
+        if (EXT && a.fd[0] && (fi < T2 || tx0 + T2 == a.nx))   // the species' mass fluxes
+            ((R *)a.fd[0])[(long)(ty0 + jj) * (a.nx + 1) + tx0 + fi] = s.DBF[FD * NFC + t];
     }
     __syncthreads();
 
@@ -489,6 +492,8 @@ hydro2d_kernel(const __grid_constant__ Args2D a)
     for (int t = tid; t < NFC; t += NT2) {
         int ii = t % T2, fj = t / T2;
         faces_stage<R, EXT>(a, s, 1, t, fj * T2 + ii, (fj + 1) * T2 + ii, ii + 3, fj + 2, ii + 3, fj + 3);
+        if (EXT && a.fd[1] && (fj < T2 || ty0 + T2 == a.ny))
+            ((R *)a.fd[1])[(long)(ty0 + fj) * a.nx + tx0 + ii] = s.DBF[FD * NFC + t];
     }
     __syncthreads();
 

@@ -81,6 +81,7 @@ struct Args3D {
     int sf_len[3], sf_lines[3]; // face-state tiles per direction (cells along d, lines), set by the launchers
     const unsigned char *hyb;   // hybrid order (uniform grid): 1 where min DivU over the cell's box < eps, padded box
     long rate_c0 = 0, rate_c1 = 0x7fffffffffffffffL;   // cells [c0, c1) enter the CFL rate (a slab's own)
+    unsigned char *ctufb[3] = {nullptr, nullptr, nullptr};   // species on: 1 where the CTU fallback fired (Grid3::widx)
 };
 // Face-state tile of direction d (N cells along d, N1 along the t1 axis):
 // the fewest warp lanes in total (the N + 1 faces split into segments of
@@ -489,7 +490,7 @@ __global__ void __launch_bounds__(256) slope3d_kernel(const Args3D a, int d)
 // The face states of one cell from its traced states wm, wp (sweep frame):
 // transverse terms, negativity fallback, gravity and the 3-D full-CTU terms.
 // vc: the cell's 8-vector.
-template <class R, bool AMR, int DIR>
+template <class R, bool AMR, int DIR, bool EXT>
 __device__ __forceinline__ void face_states_finish(const Args3D &a, const Ctx3<R, AMR> &X, const double dt,
                                                    const R hdtx, const R hdty, const R hdtz, int i, int j, int k,
                                                    const R vc[8], const EigBase<R> &eb, const R wm[6], const R wp[6],
@@ -557,6 +558,9 @@ __device__ __forceinline__ void face_states_finish(const Args3D &a, const Ctx3<R
         if (Wp[0] <= R(0) || Wm[0] <= R(0) || Wp[4] <= R(0) || Wm[4] <= R(0)) {
 #pragma unroll
             for (int q = 0; q < 6; q++) { Wm[q] = gvc[q]; Wp[q] = gvc[q]; }
+            if constexpr (EXT && !AMR) {   // species (extended-option kernels) fall back too
+                if (a.ctufb[d]) a.ctufb[d][G.widx(d, i, j, k)] = 1;
+            }
         }
     }
 #pragma unroll
@@ -593,7 +597,7 @@ __device__ __forceinline__ void face_states_tail(const Args3D &a, const Ctx3<R, 
     R wm[6], wp[6];
     ppm_trace(e, dtn, hdtn, Sc, vecL, vecR, wm, wp);
     if constexpr (EXT) hybrid3d<R, AMR>(a, G, i, j, k, vc, Sc, wm, wp);
-    face_states_finish<R, AMR, DIR>(a, X, dt, hdtx, hdty, hdtz, i, j, k, vc, eb, wm, wp, Wm_out, Wp_out);
+    face_states_finish<R, AMR, DIR, EXT>(a, X, dt, hdtx, hdty, hdtz, i, j, k, vc, eb, wm, wp, Wm_out, Wp_out);
 }
 
 // ---- face states of one cell in direction d ------------------------------------
@@ -628,7 +632,7 @@ __device__ __forceinline__ void face_states(const Args3D &a, const Ctx3<R, AMR> 
         R wm[6], wp[6];
         mh_trace(a.prm, e, dtn, hdtn, S[1], S[2], S[3], F, wm, wp);
         hybrid3d<R, AMR>(a, G, i, j, k, vc, S[2], wm, wp);
-        face_states_finish<R, AMR, DIR>(a, X, dt, hdtx, hdty, hdtz, i, j, k, vc, eb, wm, wp, Wm_out, Wp_out);
+        face_states_finish<R, AMR, DIR, EXT>(a, X, dt, hdtx, hdty, hdtz, i, j, k, vc, eb, wm, wp, Wm_out, Wp_out);
         gc_out = vc[GC]; ge_out = vc[GE];
         return;
     }

@@ -1,6 +1,7 @@
 // FP64 instantiation of the 3-D kernels (built with -fmad=false).
 #include "fxb_launch.h"
 #include "fxb_amr_persist.cuh"
+#include "fxb_species.cuh"
 namespace fxb {
 cudaError_t setup_hydro3d_fp64() { return cudaSuccess; }
 void launch_hydro3d_fp64(const Args3D &a, cudaStream_t s) { launch_hydro3d_t<double>(a, s); }
@@ -16,4 +17,5 @@ cudaError_t launch_amr_persist_fp64(int which, int clusters, int K, cudaStream_t
 { return launch_amr_persist_t<double>(which, clusters, K, s); }
 cudaError_t persist_upload_fp64(const PersistArgs p[2]) { return persist_upload_t<double>(p); }
 int persist_grid_fp64(int K) { return persist_grid<double>(K); }
+void launch_species_fp64(const SpecArgs &a, cudaStream_t s) { launch_species_t<double>(a, s); }
 } // namespace fxb

@@ -2,6 +2,7 @@
 // terms and Riemann solve with FP32 intermediates; FP64 update, Eos and CFL rate.
 #include "fxb_launch.h"
 #include "fxb_amr_persist.cuh"
+#include "fxb_species.cuh"
 namespace fxb {
 cudaError_t setup_hydro3d_mixed() { return cudaSuccess; }
 void launch_hydro3d_mixed(const Args3D &a, cudaStream_t s) { launch_hydro3d_t<float>(a, s); }
@@ -17,4 +18,5 @@ cudaError_t launch_amr_persist_mixed(int which, int clusters, int K, cudaStream_
 { return launch_amr_persist_t<float>(which, clusters, K, s); }
 cudaError_t persist_upload_mixed(const PersistArgs p[2]) { return persist_upload_t<float>(p); }
 int persist_grid_mixed(int K) { return persist_grid<float>(K); }
+void launch_species_mixed(const SpecArgs &a, cudaStream_t s) { launch_species_t<float>(a, s); }
 } // namespace fxb

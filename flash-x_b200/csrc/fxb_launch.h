@@ -26,6 +26,10 @@ void launch_amr3d_emit_mixed(const Args3D &a, int entries, void *bflux, long nfc
 void launch_amr3d_correct_mixed(const Args3D &a, int entries, const void *bflux, long nfc, const int *fine,
                                const int *finer_mask, cudaStream_t s);
 void launch_amr3d_update_mixed(const Args3D &a, int entries, cudaStream_t s);
+// species and mass scalars after a uniform-grid step (fxb_species.cuh)
+struct SpecArgs;
+void launch_species_fp64(const SpecArgs &a, cudaStream_t s);
+void launch_species_mixed(const SpecArgs &a, cudaStream_t s);
 // the persistent AMR step (fxb_amr_persist.cuh): launch and resident CTAs
 struct PersistArgs;
 cudaError_t launch_amr_persist_fp64(int which, int clusters, int K, cudaStream_t s);

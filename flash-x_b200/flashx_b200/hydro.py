@@ -32,7 +32,7 @@ ABI_SYMBOLS = ("fxb_init", "fxb_register_blocks", "fxb_attach_unk", "fxb_fill_gu
                "fxb_sync_from_host", "fxb_integrals", "fxb_integrals_noalloc", "fxb_mark_refine_derefine",
                "fxb_last_timing", "fxb_stream", "fxb_tuning", "fxb_last_error", "fxb_finalize",
                "fxb_init_slab", "fxb_halo_doubles", "fxb_halo_pack", "fxb_halo_unpack", "fxb_regrid",
-               "fxb_refine_derefine", "fxb_counters")
+               "fxb_refine_derefine", "fxb_counters", "fxb_init_species")
 # fxb_counters slots
 COUNT_STEPS, COUNT_DT_DEVICE, COUNT_DT_CACHED, COUNT_GC_FILLS, COUNT_GC_DOUBLES = range(5)
 
@@ -100,6 +100,7 @@ def load_library(path=LIB_PATH):
     L.fxb_attach_unk.argtypes = [D]
     L.fxb_fill_guardcells.argtypes = [ctypes.c_int, ctypes.c_int, D]
     L.fxb_counters.argtypes = [ctypes.POINTER(ctypes.c_longlong)]
+    L.fxb_init_species.argtypes = [ctypes.c_int, ctypes.c_int, I32]
     L.fxb_hydro_step.argtypes = [ctypes.c_double] * 3
     L.fxb_compute_dt.argtypes = [D, I32]
     L.fxb_advance.argtypes = [ctypes.c_int, D, D, ctypes.c_double, ctypes.c_double, ctypes.c_double]
@@ -255,9 +256,14 @@ class HydroDevice:
     host; Hydro_computeDt and integrals cover the rank's own cells, for the
     caller to reduce over ranks."""
 
-    def __init__(self, geom: Geometry, hp: HydroParams, precision="fp64", mesh=None, slab=None):
+    def __init__(self, geom: Geometry, hp: HydroParams, precision="fp64", mesh=None, slab=None, species=None):
+        """species = (nspec, nspecies): that many advected mass fractions in
+        UNK slots NUNK .. NUNK + nspec - 1 after the hydro variables (the
+        first nspecies renormalised as species, the rest mass scalars)."""
         self.lib = load_library()
         self.geom, self.hp, self.precision, self.mesh, self.slab = geom, hp, precision, mesh, slab
+        nspec = species[0] if species else 0
+        self.nunk = NUNK + nspec
         self._p = make_fxb_params(hp, precision)
         self._d = make_fxb_domain(geom)
         self._vm = default_var_map()
@@ -266,19 +272,22 @@ class HydroDevice:
             if mesh is not None:
                 raise ValueError("a slab splits a uniform grid, not an AMR mesh")
             self._s = FxbSlab(slab.layer_lo, slab.layer_hi, slab.halo_lo, slab.halo_hi)
-            _check(self.lib.fxb_init_slab(ctypes.byref(self._p), ctypes.byref(self._d), self._vm, NUNK,
+            _check(self.lib.fxb_init_slab(ctypes.byref(self._p), ctypes.byref(self._d), self._vm, self.nunk,
                                           ctypes.byref(self._s)))
         else:
-            _check(self.lib.fxb_init(ctypes.byref(self._p), ctypes.byref(self._d), self._vm, NUNK))
+            _check(self.lib.fxb_init(ctypes.byref(self._p), ctypes.byref(self._d), self._vm, self.nunk))
+        if nspec:
+            slots = (ctypes.c_int32 * nspec)(*range(NUNK, NUNK + nspec))
+            _check(self.lib.fxb_init_species(nspec, int(species[1]), slots))
         if slab is not None:
             b0, b1 = slab.block_range()
             blocks, n = leaf_blocks(geom, (slab.layer_lo, slab.layer_hi)), b1 - b0
-            self.unk_shape = (n,) + geom.block_shape
+            self.unk_shape = (n,) + geom.block_shape[:-1] + (self.nunk,)
             if slab.halo_lo or slab.halo_hi:
                 self.exchange = self._make_exchange(slab)
         elif mesh is None:
             blocks, n = leaf_blocks(geom), geom.nblocks
-            self.unk_shape = geom.unk_shape
+            self.unk_shape = geom.unk_shape[:-1] + (self.nunk,)
         else:
             blocks, n = mesh_blocks(mesh.levels, mesh.bcoords), mesh.nleaf
             self.unk_shape = mesh.unk_shape

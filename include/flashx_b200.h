@@ -139,6 +139,20 @@ int fxb_init(const fxb_params *params, const fxb_domain *domain,
  * not split (FXB_EUNSUPPORTED at fxb_register_blocks). */
 int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
                   const int32_t *var_map, int nunk, const fxb_slab *slab);
+/* Species and mass scalars (NSPECIES + NMASS_SCALARS of Simulation.h),
+ * advected with every step as hy_fullSpecMsFluxHandling does (unsplit/
+ * Config:165): mass fractions reconstructed along each direction and traced
+ * with the entropy wave (hy_DataReconstructNormalDir_{PPM,WENO,MH}.F90),
+ * upwind transverse and 3-D CTU terms (hy_upwindTransverseFlux.F90,
+ * hy_getRiemannState.F90:1063-1100), fluxes = mass flux x upwind value
+ * (hy_getFaceFlux.F90:464-477), the conservative update and the species'
+ * renormalisation (hy_unsplitUpdate.F90:846-881).  Call after fxb_init and
+ * before fxb_attach_unk: unk_slots[nspec] are the 0-based UNK slots of the
+ * values (SPECIES_BEGIN - 1 ...), the first nspecies of them species that are
+ * renormalised to add up to one, the rest mass scalars.  Uniform grids
+ * without halos only (FXB_EUNSUPPORTED on AMR meshes and slabs). */
+#define FXB_MAX_SPECIES 32
+int fxb_init_species(int nspec, int nspecies, const int32_t *unk_slots);
 /* The leaf-block list (Grid_getTileIterator(LEAF)); block b is UNK slot b.
  * All leaves at level 1 covering the root grid: the uniform-grid path.
  * Otherwise (3-D only) a block-structured AMR mesh: the leaves must tile the
