@@ -17,6 +17,7 @@ MPI_SendRecv along each process axis (Grid/GridMain/UG/Grid_fillGuardCells.F90:
 import datetime
 import os
 
+import numpy as np
 import torch
 import torch.distributed as dist
 
@@ -248,3 +249,160 @@ class HaloExchange:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
         self.unpack(self.recv_lo, self.recv_hi)
+
+
+class AmrDecomposition:
+    """A block-structured AMR mesh split over ranks along PARAMESH's Morton
+    order (PM4_package/source/amr_morton_order.F90, amr_sort_morton.F90): the
+    leaf list of an AmrMesh is Morton-ordered, and rank r owns the contiguous
+    range [n r / world, n (r + 1) / world) of it.
+
+    Every rank keeps the whole mesh and a full UNK; per step it exchanges
+    the interiors of the leaves another rank's step reads, then steps:
+      * role 1, its own leaves: guard fill, fluxes, boundary fluxes, flux
+        correction, update (levelFlux/Hydro.F90:161-270);
+      * role 2, "flux ghosts": the other ranks' leaves one level finer that
+        share a face with an own leaf -- their fluxes are computed here too
+        (from exchanged data, bit for bit what their owner computes), so that
+        Grid_conserveFluxes on the own leaf needs no second exchange in the
+        step (the reference's mpi_amr_flux_conserve.F90:87-132 sends them).
+    A leaf's guard fill reads leaves within two steps of the "touching"
+    relation (sharing a face, edge or corner, across levels and periodic
+    boundaries): same-level neighbours, coarser neighbours and their
+    neighbours for the prolongation stencil, finer neighbours through the
+    restricted parent cells.  With flux ghosts one step away, every rank
+    therefore receives the leaves within `hops` = 3 steps of its own."""
+
+    def __init__(self, mesh, world, rank, hops=3):
+        self.mesh, self.world, self.rank = mesh, world, rank
+        n = mesh.nleaf
+        if world < 1 or not 0 <= rank < world or n < world:
+            raise ValueError("AmrDecomposition: need 1 <= world <= leaves and 0 <= rank < world")
+        self.bounds = [n * r // world for r in range(world + 1)]
+        self.owner = np.zeros(n, dtype=np.int64)
+        for r in range(world):
+            self.owner[self.bounds[r]:self.bounds[r + 1]] = r
+        self._touch, self._face = self._adjacency(mesh)
+        self.ghosts = [self._ghosts_of(r, hops) for r in range(world)]
+        self.roles = self.roles_of(rank)
+
+    @staticmethod
+    def _adjacency(mesh):
+        """Per leaf: the leaves it touches (face, edge or corner) and those it
+        shares a face with; boxes in units of the finest cells, periodic axes
+        wrapped."""
+        g = mesh.geom
+        nd = g.ndim
+        L = int(mesh.maxlev)
+        lev = np.asarray(mesh.levels, dtype=np.int64)
+        scale = 1 << (L - lev)
+        lo = np.asarray(mesh.bcoords, dtype=np.int64)[:, :nd] * scale[:, None]
+        hi = lo + scale[:, None]
+        nb = [g.nblockx, g.nblocky, g.nblockz][:nd]
+        ext = np.array([b << (L - 1) for b in nb], dtype=np.int64)
+        per = [g.bc[2 * a] == BC_PERIODIC for a in range(nd)]
+        touch, face = [], []
+        for i in range(mesh.nleaf):
+            contact = np.ones(mesh.nleaf, dtype=bool)   # closed boxes meet on every axis
+            overlap = np.zeros((nd, mesh.nleaf), dtype=bool)   # open intervals overlap (positive length)
+            for a in range(nd):
+                shifts = (-ext[a], 0, ext[a]) if per[a] else (0,)
+                c = np.zeros(mesh.nleaf, dtype=bool)
+                o = np.zeros(mesh.nleaf, dtype=bool)
+                for sh in shifts:
+                    l2, h2 = lo[:, a] + sh, hi[:, a] + sh
+                    c |= (lo[i, a] <= h2) & (l2 <= hi[i, a])
+                    o |= (lo[i, a] < h2) & (l2 < hi[i, a])
+                contact &= c
+                overlap[a] = o
+            contact[i] = False
+            nover = overlap.sum(axis=0)
+            touch.append(np.nonzero(contact)[0])
+            face.append(np.nonzero(contact & (nover == nd - 1))[0])
+        return touch, face
+
+    def _ghosts_of(self, r, hops):
+        own = set(range(self.bounds[r], self.bounds[r + 1]))
+        seen, front = set(own), set(own)
+        for _ in range(hops):
+            nxt = set()
+            for l in front:
+                nxt.update(int(x) for x in self._touch[l] if int(x) not in seen)
+            seen |= nxt
+            front = nxt
+        return np.array(sorted(seen - own), dtype=np.int64)
+
+    def flux_ghosts_of(self, r):
+        """Other ranks' leaves one level finer sharing a face with a leaf of r."""
+        lev = np.asarray(self.mesh.levels)
+        out = set()
+        for l in range(self.bounds[r], self.bounds[r + 1]):
+            for x in self._face[l]:
+                x = int(x)
+                if self.owner[x] != r and lev[x] == lev[l] + 1:
+                    out.add(x)
+        return np.array(sorted(out), dtype=np.int64)
+
+    def roles_of(self, r):
+        roles = np.zeros(self.mesh.nleaf, dtype=np.uint8)
+        roles[self.bounds[r]:self.bounds[r + 1]] = 1
+        roles[self.flux_ghosts_of(r)] = 2
+        return roles
+
+    def owned(self, r=None):
+        r = self.rank if r is None else r
+        return np.arange(self.bounds[r], self.bounds[r + 1])
+
+    def sends(self):
+        """{peer: own leaves the peer reads}"""
+        own = self.owned()
+        return {s: np.intersect1d(own, self.ghosts[s]) for s in range(self.world)
+                if s != self.rank and len(np.intersect1d(own, self.ghosts[s]))}
+
+    def recvs(self):
+        """{peer: leaves of the peer this rank reads}"""
+        mine = self.ghosts[self.rank]
+        return {s: mine[self.owner[mine] == s] for s in range(self.world)
+                if s != self.rank and np.any(self.owner[mine] == s)}
+
+
+class AmrExchange:
+    """The step's one exchange of leaf data between the ranks of an
+    AmrDecomposition (PARAMESH's mpi_amr_comm_setup + mpi_xchange_blocks for
+    the guard fill, mpi_amr_comm_setup.F90:531): per peer one message with
+    the leaves it reads, `leaf_doubles` values each, over
+    torch.distributed.batch_isend_irecv (NCCL between GPUs, gloo on CPU).
+    pack(leaves, buf) fills a message, unpack(leaves, buf) stores one."""
+
+    def __init__(self, dec, leaf_doubles, pack, unpack, device=None, stream=None):
+        self.dec, self.n, self.pack, self.unpack = dec, int(leaf_doubles), pack, unpack
+        self.device = device if device is not None else _device()
+        self.stream = stream
+        self.sends, self.recvs = dec.sends(), dec.recvs()
+        self.sbuf = {s: torch.empty(len(v) * self.n, dtype=torch.float64, device=self.device)
+                     for s, v in self.sends.items()}
+        self.rbuf = {s: torch.empty(len(v) * self.n, dtype=torch.float64, device=self.device)
+                     for s, v in self.recvs.items()}
+
+    def __call__(self):
+        if self.dec.world == 1:
+            return
+        ctx = torch.cuda.stream(self.stream) if self.stream is not None else _nullctx()
+        with ctx:
+            for s, leaves in self.sends.items():
+                self.pack(leaves, self.sbuf[s])
+            ops = [dist.P2POp(dist.isend, self.sbuf[s], s) for s in sorted(self.sends)]
+            ops += [dist.P2POp(dist.irecv, self.rbuf[s], s) for s in sorted(self.recvs)]
+            if ops:
+                for w in dist.batch_isend_irecv(ops):
+                    w.wait()
+            for s, leaves in self.recvs.items():
+                self.unpack(leaves, self.rbuf[s])
+
+
+class _nullctx:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False

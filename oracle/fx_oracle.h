@@ -118,6 +118,12 @@ int fxo_amr_fill_guardcells(fxo_amr *a, double *unk);
 /* levelFlux Hydro(): guard fill, fluxes of every leaf, flux correction at
  * fine/coarse faces, update, energyFix, Eos. */
 int fxo_amr_hydro_step(fxo_amr *a, double *unk, double dt, int nthreads);
+/* one rank's share of the step of a mesh split over ranks: role[leaf] 1 owned,
+ * 2 finer leaf of another rank across an owned leaf's refined face (fluxes
+ * only), 0 not stepped; and dt and integrals over the owned leaves */
+int fxo_amr_hydro_step_roles(fxo_amr *a, double *unk, double dt, const unsigned char *role, int nthreads);
+int fxo_amr_compute_dt_roles(const fxo_amr *a, const double *unk, const unsigned char *role, double *dt_out);
+int fxo_amr_integrals_roles(const fxo_amr *a, const double *unk, const unsigned char *role, double out[7]);
 int fxo_amr_compute_dt(const fxo_amr *a, const double *unk, double *dt_out);
 int fxo_amr_integrals(const fxo_amr *a, const double *unk, double out[7]);
 /* Grid_markRefineDerefine on the leaves: flags[leaf] = 1 refine, -1 derefine,

@@ -86,6 +86,10 @@ def lib():
         L.fxo_amr_hydro_step.argtypes = [ctypes.c_void_p, D, ctypes.c_double, ctypes.c_int]
         L.fxo_amr_compute_dt.argtypes = [ctypes.c_void_p, D, D]
         L.fxo_amr_integrals.argtypes = [ctypes.c_void_p, D, D]
+        U8 = ctypes.POINTER(ctypes.c_ubyte)
+        L.fxo_amr_hydro_step_roles.argtypes = [ctypes.c_void_p, D, ctypes.c_double, U8, ctypes.c_int]
+        L.fxo_amr_compute_dt_roles.argtypes = [ctypes.c_void_p, D, U8, D]
+        L.fxo_amr_integrals_roles.argtypes = [ctypes.c_void_p, D, U8, D]
         L.fxo_amr_mark_refine.argtypes = [ctypes.c_void_p, D, ctypes.c_int, I, D, D, D, ctypes.c_int, I, D]
         L.fxo_amr_regrid.argtypes = [ctypes.c_void_p, D, ctypes.c_void_p, D]
         _lib = L
@@ -234,14 +238,31 @@ class Amr:
         if rc:
             raise RuntimeError(f"oracle AMR guard fill failed with code {rc}")
 
-    def hydro_step(self, unk, dt, nthreads=0):
-        rc = lib().fxo_amr_hydro_step(self.h, _dp(unk), dt, nthreads)
+    @staticmethod
+    def _roles(roles):
+        if roles is None:
+            return None
+        r = np.ascontiguousarray(roles, dtype=np.uint8)
+        return r, r.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte))
+
+    def hydro_step(self, unk, dt, nthreads=0, roles=None):
+        """The AMR step; with `roles` (per leaf: 1 owned, 2 flux ghost, 0
+        not stepped) one rank's share of a mesh split over ranks."""
+        if roles is None:
+            rc = lib().fxo_amr_hydro_step(self.h, _dp(unk), dt, nthreads)
+        else:
+            keep, rp = self._roles(roles)
+            rc = lib().fxo_amr_hydro_step_roles(self.h, _dp(unk), dt, rp, nthreads)
         if rc:
             raise RuntimeError(f"oracle AMR hydro step failed with code {rc}")
 
-    def compute_dt(self, unk):
+    def compute_dt(self, unk, roles=None):
         out = ctypes.c_double()
-        rc = lib().fxo_amr_compute_dt(self.h, _dp(unk), ctypes.byref(out))
+        if roles is None:
+            rc = lib().fxo_amr_compute_dt(self.h, _dp(unk), ctypes.byref(out))
+        else:
+            keep, rp = self._roles(roles)
+            rc = lib().fxo_amr_compute_dt_roles(self.h, _dp(unk), rp, ctypes.byref(out))
         if rc:
             raise RuntimeError("oracle: computed dt is not positive")
         return out.value
@@ -265,9 +286,13 @@ class Amr:
             raise RuntimeError(f"oracle AMR refinement marking failed with code {rc}")
         return flags, err
 
-    def integrals(self, unk):
+    def integrals(self, unk, roles=None):
         out = np.zeros(7)
-        lib().fxo_amr_integrals(self.h, _dp(unk), _dp(out))
+        if roles is None:
+            lib().fxo_amr_integrals(self.h, _dp(unk), _dp(out))
+        else:
+            keep, rp = self._roles(roles)
+            lib().fxo_amr_integrals_roles(self.h, _dp(unk), rp, _dp(out))
         return out
 
     def regrid(self, unk, new):
