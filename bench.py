@@ -366,7 +366,7 @@ def per_block_driver(dev, geom, mesh, hp, steps, global_min):
     from flashx_b200.hydro import COUNT_DT_CACHED, COUNT_DT_DEVICE, _check, driver_dt
     lib = dev.lib
     f = lib.fxb_compute_dt
-    nblk = mesh.nleaf if mesh is not None else dev.unk_shape[0]
+    nblk = dev.unk_shape[0]       # this rank's blocks
     out = ctypes.c_double()
     loc = (ctypes.c_int32 * 5)()
     pout = ctypes.byref(out)
@@ -374,6 +374,7 @@ def per_block_driver(dev, geom, mesh, hp, steps, global_min):
     c0 = dev.counters()
     t0 = time.perf_counter()
     for _ in range(steps):
+        dev.fill_halos()          # halos or leaves from the other ranks (no-op on one GPU)
         _check(lib.fxb_hydro_step(0.0, dt, dt_old))
         dtcheck = 1e300
         for _b in range(nblk):
@@ -476,14 +477,23 @@ def run_ours(args):
 
     from flashx_b200.parallel import allreduce_min as global_min   # Driver_computeDt's AllReduce(MIN)
 
-    # uniform grids split into slabs over the ranks; AMR meshes run as replicas
-    slab = None
+    # uniform grids split into slabs over the ranks, AMR meshes into Morton
+    # ranges of `world` stacked copies (each rank owns one copy's leaves)
+    slab = split = None
     if world > 1 and mesh is None:
         whole, slab = slab_split(geom, world, rank)
+    elif world > 1:
+        from flashx_b200 import amr as A
+        from flashx_b200.parallel import AmrDecomposition
+        whole, wmesh = A.stack_copies(mesh, world)
+        split = AmrDecomposition(wmesh, world, rank)
+        assert split.bounds[rank] == rank * mesh.nleaf and len(split.owned()) == mesh.nleaf
 
     def timed_run(precision):
         if slab is not None:
             dev = HydroDevice(whole, hp, precision, slab=slab)   # this rank's slab: the per-GPU grid's blocks
+        elif split is not None:
+            dev = HydroDevice(whole, hp, precision, mesh=wmesh, amr_split=split)   # host UNK: the own copy
         else:
             dev = HydroDevice(geom, hp, precision, mesh=mesh)
         dev.attach_unk(unk0.copy())
@@ -569,7 +579,12 @@ def run_ours(args):
             "config": {"workload": WORKLOADS[args.config] + ("" if args.scale == 1.0 else f" at scale {args.scale}"),
                        "zones_per_gpu": ncell,
                        "parallelism": ("single" if world == 1 else
-                                       "replicas (one AMR mesh per GPU, common dt)" if slab is None else
+                                       f"AMR mesh of {world} copies of the per-GPU mesh stacked along z, split in "
+                                       f"Morton ranges (one copy per GPU); per step each rank receives the "
+                                       f"{len(split.ghosts[rank]) if split else 0} leaves its guard fills read "
+                                       f"(NCCL send/recv) and computes the fluxes of "
+                                       f"{int((split.roles == 2).sum()) if split else 0} finer face neighbours; "
+                                       f"common dt (all-reduce)" if slab is None else
                                        f"slabs: {world} copies of the grid stacked along its slowest axis, one "
                                        f"slab per GPU, halos of {slab.halos[0]} planes exchanged every step "
                                        f"(NCCL send/recv), common dt (all-reduce)"),
@@ -596,7 +611,8 @@ def run_ours(args):
     if mesh is not None:
         line["config"]["leaves_per_level"] = mesh.level_counts()
         line["config"]["tuning"] = dev.tuning()
-        line["regrid"] = regrid_cycle(dev, hp, mesh)
+        if world == 1:
+            line["regrid"] = regrid_cycle(dev, hp, mesh)
     dev.close()
 
     # ---- mixed precision

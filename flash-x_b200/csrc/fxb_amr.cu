@@ -95,6 +95,21 @@ struct State {
     bool tuned = false;                           // launch shapes chosen (first attach of the mesh)
     char tune_log[512] = "";
     std::unordered_map<uint64_t, int> map;
+    // one rank's share of a mesh split over ranks (fxb_amr_set_roles): per leaf
+    // 1 owned, 2 flux ghost, 0 not stepped; the step's entry lists over the
+    // active leaves (same three parts as d_entries)
+    std::vector<unsigned char> roles;
+    std::vector<int> finer_h;                     // per leaf: faces toward finer leaves (d_finer)
+    unsigned char *d_roles = nullptr;
+    AmrEntry3 *d_step_entries = nullptr;
+    AmrEntry3 *d_leaf_entry = nullptr;            // entry of every leaf with its role's flags
+    int nstep = 0, nstep_finer = 0;
+    int *d_xlist = nullptr;                       // leaf list of the last exchange message
+    int xcap = 0;
+    // a split mesh's host UNK holds the own leaves only (in leaf order)
+    int nown = 0;
+    int *d_own_blk = nullptr;                     // their blocks in the interior store
+    AmrEntry3 *d_own_entries = nullptr;           // their fill entries
     // the step as one persistent kernel over the leaf list (fxb_amr_persist.cuh)
     bool persist = false;
     bool persist_ok = false;                      // the mesh and options allow the persistent kernel
@@ -620,20 +635,34 @@ __global__ void __launch_bounds__(256) amr_restrict_list_kernel(double *store, l
 }
 
 // parent-block cells the guard-fill plan reads (same-level copies and prolongation stencils)
-__global__ void __launch_bounds__(256) amr_need_kernel(const GuardPlan *plan, long nplan, const ProlRec *prol, long nprol,
-                                                       long vstride, long bstride, unsigned char *need)
+// roles (nullptr: every leaf): only the plans of leaves with a nonzero role
+__global__ void __launch_bounds__(256) amr_need_kernel(const GuardPlan *plan, long nplan, int nglist,
+                                                       const ProlRec *prol, long nprol, const int *poff, int nleaf,
+                                                       const unsigned char *roles, long vstride, long bstride,
+                                                       unsigned char *need)
 {
     const long stride = (long)gridDim.x * blockDim.x;
     for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nplan; t += stride) {
+        if (roles && !roles[t / nglist]) continue;
         const GuardPlan gp = plan[t];
         if (((gp.flags >> 4) & 3u) == GS_SAME) need[(gp.off / bstride) * vstride + gp.off % bstride] = 1;
     }
-    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nprol; t += stride)
+    for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < nprol; t += stride) {
+        if (roles) {
+            // the leaf whose records hold t: poff[l] <= t < poff[l + 1]
+            int lo = 0, hi = nleaf;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (poff[mid] <= t) lo = mid; else hi = mid;
+            }
+            if (!roles[lo]) continue;
+        }
 #pragma unroll
         for (int s8 = 0; s8 < 8; s8++) {
             const unsigned off = prol[t].off[s8];
             need[(off / bstride) * vstride + off % bstride] = 1;
         }
+    }
 }
 
 // UNK staging (leaf, k, j, i, var with guard cells) <-> interior store / guard-filled blocks
@@ -667,11 +696,13 @@ __global__ void amr_eos_kernel(double *store, long vstride, long bstride, int n,
 }
 
 __global__ void amr_rate_kernel(const double *store, long vstride, long bstride, int n, const int *leaf_blk,
-                                const DevBlk *blk, const double *dxl, int nleaf, unsigned long long *rate_max)
+                                const DevBlk *blk, const double *dxl, int nleaf, unsigned long long *rate_max,
+                                const unsigned char *role)
 {
     const long per = (long)n * n * n;
     double r = 0.;
     for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)nleaf * per; idx += (long)gridDim.x * blockDim.x) {
+        if (role && role[idx / per] != 1) continue;     // a split mesh: the rank's own leaves
         const int b = leaf_blk[idx / per];
         const double *s = store + (long)b * bstride + idx % per;
         const double *dl = dxl + 3 * (blk[b].level - 1);
@@ -688,11 +719,12 @@ __global__ void amr_rate_kernel(const double *store, long vstride, long bstride,
 // limiting cell of the leaves: first (leaf, k, j, i) whose rate equals the maximum
 __global__ void amr_locate_kernel(const double *store, long vstride, long bstride, int n, const int *leaf_blk,
                                   const DevBlk *blk, const double *dxl, int nleaf, const unsigned long long *rate_max,
-                                  unsigned long long *key)
+                                  unsigned long long *key, const unsigned char *role)
 {
     const long per = (long)n * n * n;
     const unsigned long long rm = *rate_max;
     for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)nleaf * per; idx += (long)gridDim.x * blockDim.x) {
+        if (role && role[idx / per] != 1) continue;
         const int b = leaf_blk[idx / per];
         const double *s = store + (long)b * bstride + idx % per;
         const double *dl = dxl + 3 * (blk[b].level - 1);
@@ -704,12 +736,30 @@ __global__ void amr_locate_kernel(const double *store, long vstride, long bstrid
     }
 }
 
+// one exchange message: y = listed leaf, x = chunk of its interior; the
+// message holds one interior per leaf (mstride = bstride), or one for all
+// (mstride = 0, unpack only)
+__global__ void __launch_bounds__(256) amr_leaf_copy_kernel(double *store, long bstride, const int *leaf_blk,
+                                                            const int *list, double *msg, long mstride, int pack)
+{
+    const int q = blockIdx.y;
+    double2 *blk = reinterpret_cast<double2 *>(store + (long)leaf_blk[list[q]] * bstride);
+    double2 *m = reinterpret_cast<double2 *>(msg + (long)q * mstride);
+    const long n2 = bstride / 2;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n2; i += (long)gridDim.x * blockDim.x) {
+        if (pack) m[i] = __ldcg(blk + i);
+        else blk[i] = __ldcg(m + i);
+    }
+}
+
 __global__ void amr_integrals_kernel(const double *store, long vstride, long bstride, int n, const int *leaf_blk,
-                                     const DevBlk *blk, const double *dxl, int nleaf, double *partials)
+                                     const DevBlk *blk, const double *dxl, int nleaf, double *partials,
+                                     const unsigned char *role)
 {
     const long per = (long)n * n * n;
     double s[7] = {0., 0., 0., 0., 0., 0., 0.};
     for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < (long)nleaf * per; idx += (long)gridDim.x * blockDim.x) {
+        if (role && role[idx / per] != 1) continue;
         const int b = leaf_blk[idx / per];
         const double *c = store + (long)b * bstride + idx % per;
         const double *dl = dxl + 3 * (blk[b].level - 1);
@@ -865,7 +915,104 @@ int fill_batch(const AmrEntry3 *entries, int cnt, int which)
     return 1;
 }
 
+template <class T> cudaError_t upload(T *&dst, const std::vector<T> &v)
+{
+    cudaError_t e = cudaMalloc((void **)&dst, sizeof(T) * std::max<size_t>(1, v.size()));
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpyAsync((void *)dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, S.C.stream);
+}
+
 int persist_upload();
+
+// parent cells the guard-fill plans of the stepped leaves read (every leaf,
+// or with roles set the active ones), and below them the parent cells their
+// restriction reads (coarse to fine); listed per level for the step
+static cudaError_t build_rlist()
+{
+#define CKR(call) do { cudaError_t _e = (call); if (_e != cudaSuccess) return _e; } while (0)
+    cudaStream_t st = S.C.stream;
+    const size_t ncb = (size_t)S.nblk * S.vstride;
+    unsigned char *d_need = nullptr;
+    CKR(cudaMalloc(&d_need, ncb));
+    CKR(cudaMemsetAsync(d_need, 0, ncb, st));
+    const long nplan = (long)S.nleaf * S.nglist;
+    const int grid = (int)std::min<long>((std::max(nplan, S.nprol) + 255) / 256, 148L * 16);
+    amr_need_kernel<<<grid, 256, 0, st>>>((const GuardPlan *)S.d_plan, nplan, S.nglist, (const ProlRec *)S.d_prol,
+                                           S.nprol, S.d_poff, S.nleaf, S.roles.empty() ? nullptr : S.d_roles,
+                                           S.vstride, S.bstride, d_need);
+    CKR(cudaGetLastError());
+    std::vector<unsigned char> need(ncb);
+    CKR(cudaMemcpyAsync(need.data(), d_need, ncb, cudaMemcpyDeviceToHost, st));
+    CKR(cudaStreamSynchronize(st));
+    cudaFree(d_need);
+    const int n = S.n, h = n / 2;
+    for (int lev = 1; lev < S.maxlev; lev++)
+        for (int p : S.parents_at[lev])
+            for (int cidx = 0; cidx < S.vstride; cidx++) {
+                if (!need[(size_t)p * S.vstride + cidx]) continue;
+                const int pi = cidx % n, pj = (cidx / n) % n, pk = cidx / (n * n);
+                const int q = (pi >= h) | ((pj >= h) << 1) | ((pk >= h) << 2);
+                const int ch = S.blk[p].child[q];
+                if (S.blk[ch].leaf >= 0) continue;
+                const int i0 = 2 * (pi - (q & 1) * h), j0 = 2 * (pj - ((q >> 1) & 1) * h),
+                          k0 = 2 * (pk - ((q >> 2) & 1) * h);
+                for (int kk = 0; kk < 2; kk++) for (int jj = 0; jj < 2; jj++) for (int ii = 0; ii < 2; ii++)
+                    need[(size_t)ch * S.vstride + ((k0 + kk) * n + (j0 + jj)) * n + (i0 + ii)] = 1;
+            }
+    std::vector<int2> rl;
+    S.rlist_off.assign(S.maxlev + 1, 0);
+    for (int lev = 1; lev <= S.maxlev; lev++) {
+        S.rlist_off[lev] = (long)rl.size();
+        if (lev == S.maxlev) break;
+        for (int p : S.parents_at[lev])
+            for (int cidx = 0; cidx < S.vstride; cidx++)
+                if (need[(size_t)p * S.vstride + cidx]) rl.push_back(make_int2(p, cidx));
+    }
+    dfree(S.d_rlist);
+    return upload(S.d_rlist, rl);
+#undef CKR
+}
+
+// the step's entry lists and queue over the active leaves (all leaves, or a
+// rank's roles): [one batch][first pass of several batches][corrected leaves],
+// the flags of d_entries, and role 2 never updated
+int set_step_entries()
+{
+    const bool split = !S.roles.empty();
+    auto role = [&](int l) { return split ? (int)S.roles[l] : 1; };
+    std::vector<AmrEntry3> ent, per(S.nleaf);
+    std::vector<int> act;
+    for (int l = 0; l < S.nleaf; l++)
+        if (role(l)) act.push_back(l);
+    for (int pass = 0; pass < 2; pass++)
+        for (int l : act) {
+            const bool fin = S.finer_h[l] != 0;
+            const bool skip = role(l) == 2 || (pass == 1 && fin);
+            ent.push_back(AmrEntry3{S.leaf_blk[l], S.blk[S.leaf_blk[l]].level, l, skip ? (int)AMR_SKIP_UPDATE : 0});
+        }
+    int nfin = 0;
+    for (int l : act)
+        if (role(l) == 1 && S.finer_h[l]) { ent.push_back(AmrEntry3{S.leaf_blk[l], S.blk[S.leaf_blk[l]].level, l, 0}); nfin++; }
+    for (int l = 0; l < S.nleaf; l++)
+        per[l] = AmrEntry3{S.leaf_blk[l], S.blk[S.leaf_blk[l]].level, l, role(l) == 2 ? (int)AMR_SKIP_UPDATE : 0};
+    dfree(S.d_step_entries);
+    dfree(S.d_leaf_entry);
+    CKA(upload(S.d_step_entries, ent));
+    CKA(upload(S.d_leaf_entry, per));
+    S.nstep = (int)act.size();
+    S.nstep_finer = nfin;
+    if (S.persist_ok) {
+        // the persistent queue: the active leaves, finest level first
+        std::vector<int> order(act);
+        std::stable_sort(order.begin(), order.end(), [](int x, int y) {
+            return S.blk[S.leaf_blk[x]].level > S.blk[S.leaf_blk[y]].level;
+        });
+        dfree(S.d_order);
+        CKA(upload(S.d_order, order));
+        return persist_upload();
+    }
+    return FXB_OK;
+}
 
 // The persistent step: on by default when the mesh has a guard-fill plan and
 // no option that needs the extended-option kernels (FXB_AMR_PERSISTENT=0
@@ -880,12 +1027,6 @@ int persist_clusters(int K)
     return std::min(n, S.batch);
 }
 
-template <class T> cudaError_t upload(T *&dst, const std::vector<T> &v)
-{
-    cudaError_t e = cudaMalloc((void **)&dst, sizeof(T) * std::max<size_t>(1, v.size()));
-    if (e != cudaSuccess || v.empty()) return e;
-    return cudaMemcpyAsync((void *)dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, S.C.stream);
-}
 
 int persist_setup()
 {
@@ -924,7 +1065,7 @@ int persist_setup()
     CKA(cudaMalloc(&S.d_ctl, sizeof(int) * PQ_WORDS));
     CKA(cudaMalloc(&S.d_emitted, sizeof(int) * (size_t)S.nleaf));
     CKA(cudaMalloc(&S.d_slots, sizeof(AmrEntry3) * (size_t)S.pslots));
-    return persist_upload();
+    return FXB_OK;    // the argument sets are uploaded with the step's entry lists
 }
 
 // the kernel's argument sets for current store 0 and 1 (dt read from the
@@ -941,7 +1082,7 @@ int persist_upload()
         S.cur = keep;
         p[w].a.batch = S.d_slots;
         p[w].slots = S.d_slots;
-        p[w].leaf_entry = S.d_entries;
+        p[w].leaf_entry = S.d_leaf_entry;
         p[w].order = S.d_order;
         p[w].leaf_blk = S.leaf_blk_dev;
         p[w].plan = (const GuardPlan *)S.d_plan;
@@ -954,7 +1095,7 @@ int persist_upload()
         p[w].rlist = S.d_rlist;
         p[w].child = S.d_child;
         p[w].nritem = S.nritem;
-        p[w].nleaf = S.nleaf;
+        p[w].nleaf = S.nstep;
         for (int i = 0; i < 32; i++) p[w].rlev_items[i] = S.rlev_items[i];
         p[w].bflux = S.bflux;
         p[w].nfc = S.nfc;
@@ -1003,6 +1144,8 @@ void free_device(State &s)
     dfree(s.bflux); dfree(s.stage); dfree(s.d_dmap); dfree(s.d_pmap); dfree(s.d_glist);
     dfree(s.d_plan); dfree(s.d_prol); dfree(s.d_poff); dfree(s.d_rlist);
     dfree(s.d_order); dfree(s.d_ctl); dfree(s.d_emitted); dfree(s.d_ritems); dfree(s.d_slots);
+    dfree(s.d_roles); dfree(s.d_step_entries); dfree(s.d_leaf_entry); dfree(s.d_xlist);
+    dfree(s.d_own_blk); dfree(s.d_own_entries);
     dfree(s.d_active); dfree(s.d_act_eos); dfree(s.d_act_bnd); dfree(s.d_ext); dfree(s.d_err);
 }
 } // namespace
@@ -1093,6 +1236,7 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     CKA(up(S.d_plist, plist));
     CKA(up(S.d_eosmask, eos));
     CKA(up(S.d_finer, finer));
+    S.finer_h = finer;
     CKA(up(S.d_fine, fine));
     CKA(up(S.d_dxl, dxl));
     CKA(up(S.d_entries, ent));
@@ -1147,45 +1291,7 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
             amr_plan_kernel<<<nleaf, 256, 0, st>>>(mesh_args(0), S.leaf_blk_dev, S.d_eosmask, S.d_glist, S.nglist,
                                                    nullptr, nullptr, (ProlRec *)S.d_prol, S.d_poff, 1);
         CKA(cudaGetLastError());
-        // parent cells the plan reads, and below them the parent cells their
-        // restriction reads (coarse to fine); listed per level for the step
-        const size_t ncb = (size_t)S.nblk * S.vstride;
-        unsigned char *d_need = nullptr;
-        CKA(cudaMalloc(&d_need, ncb));
-        CKA(cudaMemsetAsync(d_need, 0, ncb, st));
-        const long nplan = (long)nleaf * S.nglist;
-        const int grid = (int)std::min<long>((std::max(nplan, S.nprol) + 255) / 256, 148L * 16);
-        amr_need_kernel<<<grid, 256, 0, st>>>((const GuardPlan *)S.d_plan, nplan, (const ProlRec *)S.d_prol, S.nprol,
-                                               S.vstride, S.bstride, d_need);
-        CKA(cudaGetLastError());
-        std::vector<unsigned char> need(ncb);
-        CKA(cudaMemcpyAsync(need.data(), d_need, ncb, cudaMemcpyDeviceToHost, st));
-        CKA(cudaStreamSynchronize(st));
-        cudaFree(d_need);
-        const int n = S.n, h = n / 2;
-        for (int lev = 1; lev < S.maxlev; lev++)
-            for (int p : S.parents_at[lev])
-                for (int cidx = 0; cidx < S.vstride; cidx++) {
-                    if (!need[(size_t)p * S.vstride + cidx]) continue;
-                    const int pi = cidx % n, pj = (cidx / n) % n, pk = cidx / (n * n);
-                    const int q = (pi >= h) | ((pj >= h) << 1) | ((pk >= h) << 2);
-                    const int ch = S.blk[p].child[q];
-                    if (S.blk[ch].leaf >= 0) continue;
-                    const int i0 = 2 * (pi - (q & 1) * h), j0 = 2 * (pj - ((q >> 1) & 1) * h),
-                              k0 = 2 * (pk - ((q >> 2) & 1) * h);
-                    for (int kk = 0; kk < 2; kk++) for (int jj = 0; jj < 2; jj++) for (int ii = 0; ii < 2; ii++)
-                        need[(size_t)ch * S.vstride + ((k0 + kk) * n + (j0 + jj)) * n + (i0 + ii)] = 1;
-                }
-        std::vector<int2> rl;
-        S.rlist_off.assign(S.maxlev + 1, 0);
-        for (int lev = 1; lev <= S.maxlev; lev++) {
-            S.rlist_off[lev] = (long)rl.size();
-            if (lev == S.maxlev) break;
-            for (int p : S.parents_at[lev])
-                for (int cidx = 0; cidx < S.vstride; cidx++)
-                    if (need[(size_t)p * S.vstride + cidx]) rl.push_back(make_int2(p, cidx));
-        }
-        CKA(up(S.d_rlist, rl));
+        CKA(build_rlist());
     }
     // active blocks for refinement marking: Eos masks and non-periodic domain faces
     {
@@ -1242,7 +1348,9 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     CKA(cudaStreamSynchronize(st));
     S.cur = 0;
     S.active = true;
-    return persist_setup();
+    int prc = persist_setup();
+    if (prc) return prc;
+    return set_step_entries();
 }
 
 // one step as batched launches of the stage kernels (the current state is
@@ -1273,22 +1381,22 @@ int batched_step(const double *dtv, double dt, int &nl)
     // fluxes (one fused kernel in FP32; slopes (PPM), face states and fluxes
     // as separate kernels in FP64)
     const int pipe = 1 + (S.C.prm.flattening ? 1 : 0) + 3 * (mixed ? 1 : (S.C.prm.order == 3 ? 3 : 2));
-    if (S.nleaf <= S.batch) {
-        a.batch = S.d_entries;
-        nl += fill_batch(a.batch, S.nleaf, S.cur);
-        fluxes(S.nleaf); emit(S.nleaf); correct(S.nleaf); update(S.nleaf);
+    if (S.nstep <= S.batch) {
+        a.batch = S.d_step_entries;
+        nl += fill_batch(a.batch, S.nstep, S.cur);
+        fluxes(S.nstep); emit(S.nstep); correct(S.nstep); update(S.nstep);
         nl += pipe + 3;
     } else {
-        for (int l0 = 0; l0 < S.nleaf; l0 += S.batch) {
-            int cnt = std::min(S.batch, S.nleaf - l0);
-            a.batch = S.d_entries + S.nleaf + l0;
+        for (int l0 = 0; l0 < S.nstep; l0 += S.batch) {
+            int cnt = std::min(S.batch, S.nstep - l0);
+            a.batch = S.d_step_entries + S.nstep + l0;
             nl += fill_batch(a.batch, cnt, S.cur);
             fluxes(cnt); emit(cnt); update(cnt);
             nl += pipe + 2;
         }
-        for (int l0 = 0; l0 < S.nfiner; l0 += S.batch) {
-            int cnt = std::min(S.batch, S.nfiner - l0);
-            a.batch = S.d_entries + 2 * S.nleaf + l0;
+        for (int l0 = 0; l0 < S.nstep_finer; l0 += S.batch) {
+            int cnt = std::min(S.batch, S.nstep_finer - l0);
+            a.batch = S.d_step_entries + 2 * S.nstep + l0;
             nl += fill_batch(a.batch, cnt, S.cur);
             fluxes(cnt); correct(cnt); update(cnt);
             nl += pipe + 2;
@@ -1404,18 +1512,46 @@ int amr_tune()
 
 const char *amr_tuning_log() { return S.tune_log; }
 
+static int copy_leaves(const int *leaves, int n, double *buf, long mstride, bool pack);
+
+// the leaves a host UNK holds: every leaf, or a split mesh's own leaves
+static bool split_unk() { return !S.roles.empty(); }
+static int host_nleaf() { return split_unk() ? S.nown : S.nleaf; }
+static const int *host_leaf_blk() { return split_unk() ? S.d_own_blk : S.leaf_blk_dev; }
+static const AmrEntry3 *host_entries() { return split_unk() ? S.d_own_entries : S.d_entries; }
+
+int amr_host_leaves() { return host_nleaf(); }
+
 int amr_attach(const double *unk_host)
 {
     const size_t per_unk = (size_t)ne3() * S.C.nunk;
-    for (int l0 = 0; l0 < S.nleaf; l0 += S.stage_leaves) {
-        int nl = std::min(S.stage_leaves, S.nleaf - l0);
+    const int nh = host_nleaf();
+    for (int l0 = 0; l0 < nh; l0 += S.stage_leaves) {
+        int nl = std::min(S.stage_leaves, nh - l0);
         CKA(cudaMemcpyAsync(S.stage, unk_host + per_unk * l0, sizeof(double) * per_unk * nl, cudaMemcpyHostToDevice,
                             S.C.stream));
         long work = (long)nl * S.vstride;
         int grid = (int)std::min<long>((work + 255) / 256, 148L * 16);
-        amr_unk_to_store_kernel<<<grid, 256, 0, S.C.stream>>>(S.stage, l0, nl, S.leaf_blk_dev, S.store[S.cur],
+        amr_unk_to_store_kernel<<<grid, 256, 0, S.C.stream>>>(S.stage, l0, nl, host_leaf_blk(), S.store[S.cur],
                                                              S.vstride, S.bstride, S.n, S.ng, S.C.nunk, S.d_dmap);
         CKA(cudaGetLastError());
+    }
+    if (split_unk() && nh > 0 && nh < S.nleaf) {
+        // the other ranks' leaves start as copies of the first own leaf (a
+        // valid state for the launch-shape timing; the exchange before each
+        // step replaces the ones the step reads)
+        std::vector<int> rest;
+        rest.reserve(S.nleaf - nh);
+        for (int l = 0; l < S.nleaf; l++)
+            if (S.roles[l] != 1) rest.push_back(l);
+        int first = 0;
+        while (S.roles[first] != 1) first++;
+        const double *src = S.store[S.cur] + (long)S.leaf_blk[first] * S.bstride;
+        for (size_t q0 = 0; q0 < rest.size(); q0 += 65535) {
+            const int cnt = (int)std::min<size_t>(65535, rest.size() - q0);
+            int rc = copy_leaves(rest.data() + q0, cnt, const_cast<double *>(src), 0, false);
+            if (rc) return rc;
+        }
     }
     CKA(cudaStreamSynchronize(S.C.stream));
     if (S.tuned) return FXB_OK;      // new data on the same mesh keeps the launch shapes
@@ -1427,15 +1563,15 @@ int amr_sync_to_host(double *unk_host)
 {
     const size_t per_unk = (size_t)ne3() * S.C.nunk;
     restrict_all(S.cur);
-    const int chunk = S.stage_leaves;
-    for (int l0 = 0; l0 < S.nleaf; l0 += chunk) {
-        int nl = std::min(chunk, S.nleaf - l0);
+    const int chunk = S.stage_leaves, nh = host_nleaf();
+    for (int l0 = 0; l0 < nh; l0 += chunk) {
+        int nl = std::min(chunk, nh - l0);
         // variables the device does not hold keep their host values
         CKA(cudaMemcpyAsync(S.stage, unk_host + per_unk * l0, sizeof(double) * per_unk * nl, cudaMemcpyHostToDevice,
                             S.C.stream));
         // guard fill straight into the FP64 staging copy
         amr_fill_kernel<double, true><<<dim3(S.fill_cta, nl), 256, 0, S.C.stream>>>(
-            mesh_args(S.cur), S.d_entries + l0, S.leaf_blk_dev, S.d_eosmask, S.stage, 0, (long)per_unk, S.C.nunk,
+            mesh_args(S.cur), host_entries() + l0, S.leaf_blk_dev, S.d_eosmask, S.stage, 0, (long)per_unk, S.C.nunk,
             S.d_dmap, nullptr, 0, S.C.dprm, S.C.gam1inv, S.C.ggprodinv);
         CKA(cudaGetLastError());
         CKA(cudaMemcpyAsync(unk_host + per_unk * l0, S.stage, sizeof(double) * per_unk * nl, cudaMemcpyDeviceToHost,
@@ -1453,11 +1589,11 @@ int amr_fill_to_host(double *unk_host, const int pos[NV_DEV], int n, const int s
     CKA(cudaMemcpyAsync(S.d_pmap, pos, sizeof(int) * NV_DEV, cudaMemcpyHostToDevice, S.C.stream));
     // the staging buffer holds stage_leaves whole UNK blocks, so at least as
     // many packed ones
-    const int chunk = S.stage_leaves;
-    for (int l0 = 0; l0 < S.nleaf; l0 += chunk) {
-        const int nl = std::min(chunk, S.nleaf - l0);
+    const int chunk = S.stage_leaves, nh = host_nleaf();
+    for (int l0 = 0; l0 < nh; l0 += chunk) {
+        const int nl = std::min(chunk, nh - l0);
         amr_fill_kernel<double, true><<<dim3(S.fill_cta, nl), 256, 0, S.C.stream>>>(
-            mesh_args(S.cur), S.d_entries + l0, S.leaf_blk_dev, do_eos ? S.d_eosmask : nullptr, S.stage, 0,
+            mesh_args(S.cur), host_entries() + l0, S.leaf_blk_dev, do_eos ? S.d_eosmask : nullptr, S.stage, 0,
             per * n, n, S.d_pmap, nullptr, 0, S.C.dprm, S.C.gam1inv, S.C.ggprodinv);
         CKA(cudaGetLastError());
         int rc = pack_to_host(S.stage, per * nl, n, slot, unk_host + per * S.C.nunk * l0);
@@ -1580,7 +1716,7 @@ int amr_rate()
     long work = amr_leaf_cells();
     int grid = (int)std::min<long>((work + 255) / 256, 148L * 16);
     amr_rate_kernel<<<grid, 256, 0, S.C.stream>>>(S.store[S.cur], S.vstride, S.bstride, S.n, S.leaf_blk_dev, S.d_blk,
-                                                  S.d_dxl, S.nleaf, S.C.rate_max);
+                                                  S.d_dxl, S.nleaf, S.C.rate_max, S.d_roles);
     CKA(cudaGetLastError());
     return FXB_OK;
 }
@@ -1600,7 +1736,7 @@ int amr_locate(unsigned long long *key)
     long work = amr_leaf_cells();
     int grid = (int)std::min<long>((work + 255) / 256, 148L * 16);
     amr_locate_kernel<<<grid, 256, 0, S.C.stream>>>(S.store[S.cur], S.vstride, S.bstride, S.n, S.leaf_blk_dev, S.d_blk,
-                                                    S.d_dxl, S.nleaf, S.C.rate_max, key);
+                                                    S.d_dxl, S.nleaf, S.C.rate_max, key, S.d_roles);
     CKA(cudaGetLastError());
     return FXB_OK;
 }
@@ -1654,10 +1790,74 @@ int amr_mark_refine(int nvars, const int *dvar, const int *need_eos, const doubl
 
 int amr_leaf_level(int leaf) { return (leaf >= 0 && leaf < S.nleaf) ? S.blk[S.leaf_blk[leaf]].level : 0; }
 
+int amr_set_roles(const unsigned char *roles, int nleaf)
+{
+    if (nleaf != S.nleaf) return record_error(FXB_EARG, "fxb_amr_set_roles: one role per leaf");
+    dfree(S.d_own_blk);
+    dfree(S.d_own_entries);
+    S.nown = 0;
+    if (!roles) {
+        S.roles.clear();
+        dfree(S.d_roles);
+    } else {
+        for (int l = 0; l < nleaf; l++)
+            if (roles[l] > 2) return record_error(FXB_EARG, "fxb_amr_set_roles: roles are 0, 1 or 2");
+        std::vector<int> own_blk;
+        std::vector<AmrEntry3> own_ent;
+        for (int l = 0; l < nleaf; l++)
+            if (roles[l] == 1) {
+                own_blk.push_back(S.leaf_blk[l]);
+                own_ent.push_back(AmrEntry3{S.leaf_blk[l], S.blk[S.leaf_blk[l]].level, l, 0});
+            }
+        if (own_blk.empty()) return record_error(FXB_EARG, "fxb_amr_set_roles: a rank owns at least one leaf");
+        S.roles.assign(roles, roles + nleaf);
+        if (!S.d_roles) CKA(cudaMalloc(&S.d_roles, (size_t)nleaf));
+        CKA(cudaMemcpyAsync(S.d_roles, roles, (size_t)nleaf, cudaMemcpyHostToDevice, S.C.stream));
+        CKA(upload(S.d_own_blk, own_blk));
+        CKA(upload(S.d_own_entries, own_ent));
+        S.nown = (int)own_blk.size();
+    }
+    if (S.d_plan) CKA(build_rlist());     // restriction of the parent cells the active leaves read
+    int rc = set_step_entries();
+    if (rc) return rc;
+    CKA(cudaStreamSynchronize(S.C.stream));
+    return FXB_OK;
+}
+
+long amr_leaf_doubles() { return S.bstride; }
+
+// leaf interiors of the current state <-> a device message [q][var][cell]:
+// one CTA row per listed leaf, 16-byte copies (a block's interior is
+// NV_DEV * n^3 doubles, an even count at every supported n)
+static int copy_leaves(const int *leaves, int n, double *buf, long mstride, bool pack)
+{
+    if (n > S.xcap) {
+        dfree(S.d_xlist);
+        CKA(cudaMalloc(&S.d_xlist, sizeof(int) * (size_t)n));
+        S.xcap = n;
+    }
+    CKA(cudaMemcpyAsync(S.d_xlist, leaves, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, S.C.stream));
+    const int chunks = (int)std::min<long>(8, (S.bstride / 2 + 255) / 256);
+    amr_leaf_copy_kernel<<<dim3(chunks, n), 256, 0, S.C.stream>>>(S.store[S.cur], S.bstride, S.leaf_blk_dev,
+                                                                   S.d_xlist, buf, mstride, pack ? 1 : 0);
+    CKA(cudaGetLastError());
+    return FXB_OK;
+}
+
+int amr_copy_leaves(const int *leaves, int n, double *buf, bool pack)
+{
+    if (n == 0) return FXB_OK;
+    if (n > 65535) return record_error(FXB_EARG, "fxb_amr_pack_leaves: at most 65535 leaves per message");
+    if (((uintptr_t)buf & 15) != 0) return record_error(FXB_EARG, "fxb_amr_pack_leaves: buffer not 16-byte aligned");
+    for (int q = 0; q < n; q++)
+        if (leaves[q] < 0 || leaves[q] >= S.nleaf) return record_error(FXB_EARG, "fxb_amr_pack_leaves: leaf out of range");
+    return copy_leaves(leaves, n, buf, S.bstride, pack);
+}
+
 int amr_integrals(double *out7, double *partials, int npartials)
 {
     amr_integrals_kernel<<<npartials, 256, 0, S.C.stream>>>(S.store[S.cur], S.vstride, S.bstride, S.n, S.leaf_blk_dev,
-                                                            S.d_blk, S.d_dxl, S.nleaf, partials);
+                                                            S.d_blk, S.d_dxl, S.nleaf, partials, S.d_roles);
     amr_integrals_final_kernel<<<1, 32, 0, S.C.stream>>>(partials, npartials, partials + (long)npartials * 7);
     CKA(cudaGetLastError());
     CKA(cudaMemcpyAsync(out7, partials + (long)npartials * 7, 7 * sizeof(double), cudaMemcpyDeviceToHost, S.C.stream));

@@ -47,6 +47,12 @@ long amr_leaf_cells();
 // first leaf cell (leaf, k, j, i linear index) whose CFL rate equals the reduced maximum
 int amr_locate(unsigned long long *key);
 int amr_leaf_level(int leaf);
+// a rank's share of a split mesh: per leaf 1 owned, 2 flux ghost, 0 not stepped (NULL: all owned)
+int amr_set_roles(const unsigned char *roles, int nleaf);
+long amr_leaf_doubles();
+// leaves of the host UNK: every leaf, or with roles set the own leaves in leaf order
+int amr_host_leaves();
+int amr_copy_leaves(const int *leaves, int n, double *buf, bool pack);
 // Grid_markRefineDerefine on the leaves; dvar: device variables, need_eos:
 // the variable is an Eos output (the guard regions get the Eos)
 int amr_mark_refine(int nvars, const int *dvar, const int *need_eos, const double *refine_cutoff,

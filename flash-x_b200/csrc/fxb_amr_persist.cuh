@@ -265,7 +265,8 @@ amr_persist_kernel(const int which)
         }
         persist_emit<R>(which, vb);
         persist_signal(p.emitted + leaf);
-        const int mask = p.finer_mask[leaf];
+        // flux ghosts of a split mesh (never updated) skip the correction
+        const int mask = (p.leaf_entry[leaf].flags & AMR_SKIP_UPDATE) ? 0 : p.finer_mask[leaf];
         if (mask) {
             // Grid_conserveFluxes: the finer leaves across each refined face
             // must have stored their boundary fluxes

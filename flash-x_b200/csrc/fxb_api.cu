@@ -1196,6 +1196,35 @@ extern "C" int fxb_halo_unpack(const double *recv_lo, const double *recv_hi)
     return FXB_OK;
 }
 
+extern "C" int fxb_amr_set_roles(const unsigned char *roles, int nleaf)
+{
+    if (!amr_active()) return fail(FXB_EUNSUPPORTED, "fxb_amr_set_roles: needs a registered AMR mesh");
+    int rc = amr_set_roles(roles, nleaf);
+    if (rc) return rc;
+    state_changed(false);
+    for (int i = 0; i < 2; i++) {
+        if (L.graph_exec[i]) cudaGraphExecDestroy(L.graph_exec[i]);
+        L.graph_exec[i] = nullptr;
+    }
+    return FXB_OK;
+}
+
+extern "C" long fxb_amr_leaf_doubles(void) { return amr_active() ? amr_leaf_doubles() : 0; }
+
+extern "C" int fxb_amr_pack_leaves(const int32_t *leaves, int n, double *buf)
+{
+    if (!L.attached || !amr_active()) return fail(FXB_EARG, "fxb_amr_pack_leaves: needs an attached AMR mesh");
+    if (n < 0 || (n && (!leaves || !buf))) return fail(FXB_EARG, "fxb_amr_pack_leaves: bad list or buffer");
+    return amr_copy_leaves(leaves, n, buf, true);
+}
+
+extern "C" int fxb_amr_unpack_leaves(const int32_t *leaves, int n, const double *buf)
+{
+    if (!L.attached || !amr_active()) return fail(FXB_EARG, "fxb_amr_unpack_leaves: needs an attached AMR mesh");
+    if (n < 0 || (n && (!leaves || !buf))) return fail(FXB_EARG, "fxb_amr_unpack_leaves: bad list or buffer");
+    return amr_copy_leaves(leaves, n, const_cast<double *>(buf), false);
+}
+
 extern "C" int fxb_mark_refine_derefine(int nvars, const int *refine_var, const double *refine_cutoff,
                                         const double *derefine_cutoff, const double *refine_filter, int max_refine,
                                         int *flags, double *error)

@@ -1176,7 +1176,8 @@ __device__ __forceinline__ void amr_correct_flux_kernel_body(const Args3D &a, co
 {
     const Ctx3<R, true> X(a, vb.y);
     const Grid3 &G = X.G;
-    const int mask = finer_mask[X.m.leaf];
+    // leaves whose update waits, or that are never updated (flux ghosts of a split mesh), skip it
+    const int mask = (X.m.flags & AMR_SKIP_UPDATE) ? 0 : finer_mask[X.m.leaf];
     if (!mask) return;
     const int n[3] = {a.nx, a.ny, a.nz};
     for (int f = 0; f < 6; f++) {

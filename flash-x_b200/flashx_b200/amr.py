@@ -343,3 +343,36 @@ def levelset_problem(geom: Geometry, hp: HydroParams, maxlev, threshold=0.1):
         p = np.full_like(rho, 2.5)
         return rho, vx, vy, vz, p
     return mesh, fill_leaves(mesh, hp, fields)
+
+
+def stack_copies(mesh: AmrMesh, copies):
+    """`copies` copies of a mesh stacked along the slowest axis (z in 3-D, y
+    in 2-D), that axis' extent and root blocks multiplied: the mesh of a
+    weak-scaling run split over `copies` ranks.  The copies are whole
+    root-block layers, which the Morton order visits one after the other, so
+    copy c is the leaf range [c n, (c + 1) n) of the result, its leaves in
+    the order of `mesh` (a rank owning that range holds `mesh`'s leaf UNK).
+    Returns (geometry, mesh)."""
+    import dataclasses
+    g = mesh.geom
+    ax = g.ndim - 1
+    key = ("nblockx", "nblocky", "nblockz")[ax]
+    bbox = list(g.bbox)
+    lo, hi = bbox[ax]
+    bbox[ax] = (lo, lo + copies * (hi - lo))
+    whole = dataclasses.replace(g, bbox=tuple(bbox), **{key: getattr(g, key) * copies})
+    nroot = getattr(g, key)
+    lev = mesh.levels.astype(np.int64)
+    leaves = []
+    for c in range(copies):
+        b = mesh.bcoords.astype(np.int64).copy()
+        b[:, ax] += c * (nroot << (lev - 1))
+        leaves += [(int(l), tuple(int(v) for v in bc)) for l, bc in zip(lev, b)]
+    out = AmrMesh(whole, leaves)
+    n = mesh.nleaf
+    for c in range(copies):
+        b = out.bcoords[c * n:(c + 1) * n].astype(np.int64)
+        b[:, ax] -= c * (nroot << (out.levels[c * n:(c + 1) * n].astype(np.int64) - 1))
+        if not (np.array_equal(b, mesh.bcoords) and np.array_equal(out.levels[c * n:(c + 1) * n], mesh.levels)):
+            raise ValueError("stack_copies: the copies are not contiguous in Morton order")
+    return whole, out

@@ -26,13 +26,17 @@ FXB_FP64, FXB_MIXED = 0, 1
 # enum fxb_var order of include/flashx_b200.h
 FXB_VARS = ("dens", "eint", "ener", "gamc", "game", "pres", "temp", "velx", "vely", "velz")
 
+# variable order of an AMR leaf message (fxb_amr_pack_leaves / fxb_amr_unpack_leaves)
+LEAF_MSG_VARS = ("dens", "velx", "vely", "velz", "pres", "gamc", "game", "eint", "ener", "temp")
+
 # entry points declared in include/flashx_b200.h
 ABI_SYMBOLS = ("fxb_init", "fxb_register_blocks", "fxb_attach_unk", "fxb_fill_guardcells",
                "fxb_hydro_step", "fxb_compute_dt", "fxb_advance", "fxb_eos", "fxb_sync_to_host",
                "fxb_sync_from_host", "fxb_integrals", "fxb_integrals_noalloc", "fxb_mark_refine_derefine",
                "fxb_last_timing", "fxb_stream", "fxb_tuning", "fxb_last_error", "fxb_finalize",
                "fxb_init_slab", "fxb_halo_doubles", "fxb_halo_pack", "fxb_halo_unpack", "fxb_regrid",
-               "fxb_refine_derefine", "fxb_counters", "fxb_init_species")
+               "fxb_refine_derefine", "fxb_counters", "fxb_init_species", "fxb_amr_set_roles",
+               "fxb_amr_leaf_doubles", "fxb_amr_pack_leaves", "fxb_amr_unpack_leaves")
 # fxb_counters slots
 COUNT_STEPS, COUNT_DT_DEVICE, COUNT_DT_CACHED, COUNT_GC_FILLS, COUNT_GC_DOUBLES = range(5)
 
@@ -101,6 +105,11 @@ def load_library(path=LIB_PATH):
     L.fxb_fill_guardcells.argtypes = [ctypes.c_int, ctypes.c_int, D]
     L.fxb_counters.argtypes = [ctypes.POINTER(ctypes.c_longlong)]
     L.fxb_init_species.argtypes = [ctypes.c_int, ctypes.c_int, I32]
+    L.fxb_amr_set_roles.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.fxb_amr_leaf_doubles.argtypes = []
+    L.fxb_amr_leaf_doubles.restype = ctypes.c_long
+    L.fxb_amr_pack_leaves.argtypes = [I32, ctypes.c_int, ctypes.c_void_p]
+    L.fxb_amr_unpack_leaves.argtypes = [I32, ctypes.c_int, ctypes.c_void_p]
     L.fxb_hydro_step.argtypes = [ctypes.c_double] * 3
     L.fxb_compute_dt.argtypes = [D, I32]
     L.fxb_advance.argtypes = [ctypes.c_int, D, D, ctypes.c_double, ctypes.c_double, ctypes.c_double]
@@ -125,7 +134,7 @@ def load_library(path=LIB_PATH):
                                       ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
                                       ctypes.POINTER(FxbBlockDesc), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     for name in ABI_SYMBOLS:
-        if name not in ("fxb_stream", "fxb_finalize", "fxb_halo_doubles"):
+        if name not in ("fxb_stream", "fxb_finalize", "fxb_halo_doubles", "fxb_amr_leaf_doubles"):
             getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -215,6 +224,17 @@ def leaf_blocks(geom: Geometry, layers=None):
     return arr
 
 
+def amr_leaf_message(geom: Geometry, unk, leaves):
+    """The message fxb_amr_pack_leaves makes of `leaves` of a host UNK (an
+    AmrMesh UNK, default variable map): per leaf the interior cells of the
+    variables LEAF_MSG_VARS, [leaf][var][k][j][i]."""
+    g = geom.nguard
+    sl = [slice(g, g + n) if n > 1 else slice(0, 1) for n in (geom.nzb, geom.nyb, geom.nxb)]
+    slots = [UNK_VARS.index(v) for v in LEAF_MSG_VARS]
+    sub = unk[np.asarray(leaves, dtype=np.int64)][:, sl[0], sl[1], sl[2]][..., slots]
+    return np.ascontiguousarray(np.moveaxis(sub, -1, 1)).reshape(-1)
+
+
 def mesh_blocks(levels, bcoords):
     """Leaf-block list of an AMR mesh (levels from 1, block coordinates at
     each leaf's level), in UNK slot order."""
@@ -254,9 +274,16 @@ class HydroDevice:
     (UNK slots in the grid's block order) and exchanges halos with the
     neighbouring ranks before each step and before guard cells go to the
     host; Hydro_computeDt and integrals cover the rank's own cells, for the
-    caller to reduce over ranks."""
+    caller to reduce over ranks.
+    `amr_split` (a flashx_b200.parallel.AmrDecomposition of `mesh`) makes it
+    one rank's share of an AMR mesh: the device holds the whole mesh, the
+    host UNK the rank's own leaves (unk_shape); it steps its own leaves (and
+    computes the fluxes of its flux ghosts) and receives the other ranks'
+    leaves its guard fills read before each step and before guard cells go
+    to the host; Hydro_computeDt and integrals cover its own leaves."""
 
-    def __init__(self, geom: Geometry, hp: HydroParams, precision="fp64", mesh=None, slab=None, species=None):
+    def __init__(self, geom: Geometry, hp: HydroParams, precision="fp64", mesh=None, slab=None, species=None,
+                 amr_split=None):
         """species = (nspec, nspecies): that many advected mass fractions in
         UNK slots NUNK .. NUNK + nspec - 1 after the hydro variables (the
         first nspecies renormalised as species, the rest mass scalars)."""
@@ -293,6 +320,56 @@ class HydroDevice:
             self.unk_shape = mesh.unk_shape
         _check(self.lib.fxb_register_blocks(blocks, n))
         self.unk = None
+        self.split = None
+        if amr_split is not None:
+            if mesh is None or amr_split.mesh is not mesh:
+                raise ValueError("amr_split must decompose the mesh given")
+            self._set_split(amr_split)
+
+    def _set_split(self, dec):
+        roles = np.ascontiguousarray(dec.roles, dtype=np.uint8)
+        _check(self.lib.fxb_amr_set_roles(roles.ctypes.data, len(roles)))
+        self.split = dec
+        self.unk_shape = (len(dec.owned()),) + dec.mesh.unk_shape[1:]
+        self.exchange = self._make_amr_exchange(dec) if dec.world > 1 else None
+
+    def _make_amr_exchange(self, dec):
+        import torch
+        from .parallel import AmrExchange
+        lib = self.lib
+        lists = {}
+
+        def i32(leaves):
+            key = id(leaves)
+            if key not in lists:
+                lists[key] = (leaves, np.ascontiguousarray(leaves, dtype=np.int32))
+            a = lists[key][1]
+            return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(a)
+
+        def pack(leaves, buf):
+            p, n = i32(leaves)
+            _check(lib.fxb_amr_pack_leaves(p, n, ctypes.c_void_p(buf.data_ptr())))
+
+        def unpack(leaves, buf):
+            p, n = i32(leaves)
+            _check(lib.fxb_amr_unpack_leaves(p, n, ctypes.c_void_p(buf.data_ptr())))
+
+        dev = torch.device("cuda", torch.cuda.current_device())
+        stream = torch.cuda.ExternalStream(lib.fxb_stream(), device=dev)
+        return AmrExchange(dec, lib.fxb_amr_leaf_doubles(), pack, unpack, device=dev, stream=stream)
+
+    def unpack_leaves(self, leaves, buf):
+        """fxb_amr_unpack_leaves: store the interiors in the message `buf` (a
+        float64 CUDA tensor laid out as amr_leaf_message) into `leaves`."""
+        a = np.ascontiguousarray(leaves, dtype=np.int32)
+        _check(self.lib.fxb_amr_unpack_leaves(a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(a),
+                                              ctypes.c_void_p(buf.data_ptr())))
+
+    def pack_leaves(self, leaves, buf):
+        """fxb_amr_pack_leaves: the interiors of `leaves` into the message `buf`."""
+        a = np.ascontiguousarray(leaves, dtype=np.int32)
+        _check(self.lib.fxb_amr_pack_leaves(a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(a),
+                                            ctypes.c_void_p(buf.data_ptr())))
 
     def _make_exchange(self, slab):
         import torch
@@ -311,8 +388,9 @@ class HydroDevice:
         return HaloExchange(slab, lib.fxb_halo_doubles(1), pack, unpack, device=dev, stream=stream)
 
     def fill_halos(self):
-        """Grid_fillGuardCells between slabs: the halo planes from the
-        neighbouring ranks (every rank calls it at the same point)."""
+        """Grid_fillGuardCells between ranks: the halo planes from the
+        neighbouring slabs, or the other ranks' leaves this rank's guard
+        fills read (every rank calls it at the same point)."""
         if self.exchange is not None:
             self.exchange()
 
@@ -368,8 +446,8 @@ class HydroDevice:
     # ---- driver helpers
     def advance(self, nsteps, dt, dt_old):
         """nsteps of Hydro + Driver_computeDt on the device (CUDA graph); a
-        slab with halos steps from the host instead, exchanging halos and
-        reducing dt over the ranks every step."""
+        slab with halos or a split AMR mesh steps from the host instead,
+        exchanging halos or leaves and reducing dt over the ranks every step."""
         hp = self.hp
         if self.exchange is not None:
             from .parallel import allreduce_min
@@ -392,7 +470,10 @@ class HydroDevice:
         (variable name, refine_cutoff, derefine_cutoff, refine_filter) per
         refinement variable, names as in UNK ("dens", "pres", ...).
         Returns (flags, errors) per leaf: 1 refine, -1 derefine, 0 neither;
-        the error estimate of the last variable."""
+        the error estimate of the last variable.  On a split mesh every rank
+        first receives every leaf, so that all ranks mark the same leaves."""
+        if self.split is not None and self.exchange is not None:
+            self._full_exchange()
         nv = len(refine_vars)
         ids = [FXB_VARS.index(r[0]) for r in refine_vars]
         iv = (ctypes.c_int * nv)(*ids)
@@ -415,11 +496,37 @@ class HydroDevice:
         if self.mesh is None:
             raise ValueError("Grid_updateRefinement needs an AMR mesh")
         new = refine_derefine(self.mesh, flags, lrefine_min, lrefine_max)
+        if self.split is not None:
+            # every leaf's data on every rank for the data movement, then the
+            # new mesh's Morton split
+            from .parallel import AmrDecomposition
+            if self.exchange is not None:
+                self._full_exchange()
         _check(self.lib.fxb_regrid(mesh_blocks(new.levels, new.bcoords), new.nleaf))
         self.mesh = new
         self.unk_shape = new.unk_shape
         self.unk = None
+        if self.split is not None:
+            self._set_split(AmrDecomposition(new, self.split.world, self.split.rank, self.split.hops))
         return new
+
+    def _full_exchange(self):
+        """Every rank's own leaves to every other rank (before a regrid, whose
+        prolongation and restriction read leaves anywhere in the mesh)."""
+        import torch
+        import torch.distributed as dist
+        dec, n = self.split, self.lib.fxb_amr_leaf_doubles()
+        dev = torch.device("cuda", torch.cuda.current_device())
+        stream = torch.cuda.ExternalStream(self.lib.fxb_stream(), device=dev)
+        most = max(dec.bounds[r + 1] - dec.bounds[r] for r in range(dec.world))
+        with torch.cuda.stream(stream):
+            mine = torch.empty(most * n, dtype=torch.float64, device=dev)
+            self.pack_leaves(dec.owned(), mine)
+            parts = [torch.empty(most * n, dtype=torch.float64, device=dev) for _ in range(dec.world)]
+            dist.all_gather(parts, mine)
+            for r in range(dec.world):
+                if r != dec.rank:
+                    self.unpack_leaves(dec.owned(r), parts[r])
 
     def tuning(self):
         """The launch shape in use (the batched-block path tunes it at attach)."""

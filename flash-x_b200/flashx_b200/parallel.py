@@ -274,7 +274,7 @@ class AmrDecomposition:
     therefore receives the leaves within `hops` = 3 steps of its own."""
 
     def __init__(self, mesh, world, rank, hops=3):
-        self.mesh, self.world, self.rank = mesh, world, rank
+        self.mesh, self.world, self.rank, self.hops = mesh, world, rank, hops
         n = mesh.nleaf
         if world < 1 or not 0 <= rank < world or n < world:
             raise ValueError("AmrDecomposition: need 1 <= world <= leaves and 0 <= rank < world")
@@ -290,7 +290,10 @@ class AmrDecomposition:
     def _adjacency(mesh):
         """Per leaf: the leaves it touches (face, edge or corner) and those it
         shares a face with; boxes in units of the finest cells, periodic axes
-        wrapped."""
+        wrapped.  A leaf lies inside its root block, so the leaves it touches
+        lie in its own root block or in one touching it: each root block's
+        leaves are tested against those of its (up to 3^ndim) neighbours."""
+        import itertools
         g = mesh.geom
         nd = g.ndim
         L = int(mesh.maxlev)
@@ -301,24 +304,44 @@ class AmrDecomposition:
         nb = [g.nblockx, g.nblocky, g.nblockz][:nd]
         ext = np.array([b << (L - 1) for b in nb], dtype=np.int64)
         per = [g.bc[2 * a] == BC_PERIODIC for a in range(nd)]
-        touch, face = [], []
-        for i in range(mesh.nleaf):
-            contact = np.ones(mesh.nleaf, dtype=bool)   # closed boxes meet on every axis
-            overlap = np.zeros((nd, mesh.nleaf), dtype=bool)   # open intervals overlap (positive length)
+        root = lo >> (L - 1)
+        buckets = {}
+        for i, rc in enumerate(map(tuple, root)):
+            buckets.setdefault(rc, []).append(i)
+        touch, face = [None] * mesh.nleaf, [None] * mesh.nleaf
+        for rc, members in buckets.items():
+            near = set()
+            for off in itertools.product((-1, 0, 1), repeat=nd):
+                c = []
+                for a in range(nd):
+                    v = rc[a] + off[a]
+                    if per[a]:
+                        v %= nb[a]
+                    elif not 0 <= v < nb[a]:
+                        break
+                    c.append(v)
+                else:
+                    near.update(buckets.get(tuple(c), ()))
+            A = np.asarray(members, dtype=np.int64)
+            C = np.asarray(sorted(near), dtype=np.int64)
+            contact = np.ones((len(A), len(C)), dtype=bool)     # closed boxes meet on every axis
+            nover = np.zeros((len(A), len(C)), dtype=np.int64)   # axes where open intervals overlap
             for a in range(nd):
                 shifts = (-ext[a], 0, ext[a]) if per[a] else (0,)
-                c = np.zeros(mesh.nleaf, dtype=bool)
-                o = np.zeros(mesh.nleaf, dtype=bool)
+                cm = np.zeros_like(contact)
+                om = np.zeros_like(contact)
+                la, ha = lo[A, a][:, None], hi[A, a][:, None]
                 for sh in shifts:
-                    l2, h2 = lo[:, a] + sh, hi[:, a] + sh
-                    c |= (lo[i, a] <= h2) & (l2 <= hi[i, a])
-                    o |= (lo[i, a] < h2) & (l2 < hi[i, a])
-                contact &= c
-                overlap[a] = o
-            contact[i] = False
-            nover = overlap.sum(axis=0)
-            touch.append(np.nonzero(contact)[0])
-            face.append(np.nonzero(contact & (nover == nd - 1))[0])
+                    l2, h2 = lo[C, a][None, :] + sh, hi[C, a][None, :] + sh
+                    cm |= (la <= h2) & (l2 <= ha)
+                    om |= (la < h2) & (l2 < ha)
+                contact &= cm
+                nover += om
+            contact &= A[:, None] != C[None, :]
+            fmask = contact & (nover == nd - 1)
+            for q, i in enumerate(A):
+                touch[i] = C[contact[q]]
+                face[i] = C[fmask[q]]
         return touch, face
 
     def _ghosts_of(self, r, hops):

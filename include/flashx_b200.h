@@ -246,6 +246,29 @@ int fxb_halo_unpack(const double *recv_lo, const double *recv_hi);
 int fxb_mark_refine_derefine(int nvars, const int *refine_var, const double *refine_cutoff,
                              const double *derefine_cutoff, const double *refine_filter, int max_refine,
                              int *flags, double *error);
+/* A block-structured AMR mesh split over ranks (one GPU each), PARAMESH's
+ * Morton distribution (PM4_package/source/amr_morton_order.F90): every rank
+ * registers the whole leaf list (the device keeps every leaf's interior);
+ * roles[nleaf] (registration order, set before fxb_attach_unk) give this
+ * rank's share of each step, and from then on the host UNK of
+ * fxb_attach_unk, fxb_sync_to_host and fxb_fill_guardcells holds the own
+ * leaves only, in leaf order (Flash-X's local blocks): 1 = own leaf
+ * (stepped and updated; the only leaves fxb_compute_dt and fxb_integrals
+ * cover), 2 = another rank's leaf one level finer across a face of an own
+ * leaf (its fluxes are computed here, for the own leaf's Grid_conserveFluxes,
+ * mpi_amr_flux_conserve.F90:87-132, but it is not updated), 0 = not stepped.
+ * Before every step the rank receives, with fxb_amr_unpack_leaves, the
+ * current interiors of the other ranks' leaves its active leaves' guard fills
+ * read (mpi_amr_comm_setup.F90:531 -> mpi_xchange_blocks), packed by their
+ * owners with fxb_amr_pack_leaves; a message holds fxb_amr_leaf_doubles()
+ * values per leaf, [leaf][var][k][j][i] over the leaf's interior cells with
+ * var in the order DENS VELX VELY VELZ PRES GAMC GAME EINT ENER TEMP, in
+ * 16-byte aligned device memory, queued on the library stream.  roles NULL:
+ * every leaf own. */
+int fxb_amr_set_roles(const unsigned char *roles, int nleaf);
+long fxb_amr_leaf_doubles(void);
+int fxb_amr_pack_leaves(const int32_t *leaves, int n, double *buf);
+int fxb_amr_unpack_leaves(const int32_t *leaves, int n, const double *buf);
 /* Grid_updateRefinement's data movement on the device, after the caller's
  * tree update (Paramesh4/Grid_updateRefinement.F90:109,
  * gr_updateRefinement.F90:130-265): `blocks` is the new leaf list of the

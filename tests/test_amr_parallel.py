@@ -152,3 +152,94 @@ def test_amr_ranks_reproduce_the_whole_mesh_gloo(name, world, oracle):
         sums = z["sums"]
     assert covered == mesh.nleaf
     np.testing.assert_allclose(sums, am.integrals(u), rtol=1e-12, atol=1e-12)
+
+
+def _touch_brute_force(mesh):
+    """Every pair of leaves tested: closed boxes (finest-cell units) that meet
+    on every axis, periodic axes wrapped; face neighbours overlap with positive
+    length on all axes but one."""
+    g = mesh.geom
+    nd = g.ndim
+    L = int(mesh.maxlev)
+    lev = np.asarray(mesh.levels, dtype=np.int64)
+    sc = 1 << (L - lev)
+    lo = np.asarray(mesh.bcoords, dtype=np.int64)[:, :nd] * sc[:, None]
+    hi = lo + sc[:, None]
+    ext = [b << (L - 1) for b in (g.nblockx, g.nblocky, g.nblockz)[:nd]]
+    touch, face = [], []
+    for i in range(mesh.nleaf):
+        t, f = [], []
+        for j in range(mesh.nleaf):
+            if i == j:
+                continue
+            meet, nover = True, 0
+            for a in range(nd):
+                sh = (-ext[a], 0, ext[a]) if g.bc[2 * a] == BC_PERIODIC else (0,)
+                meet &= any(lo[i, a] <= hi[j, a] + s and lo[j, a] + s <= hi[i, a] for s in sh)
+                nover += any(lo[i, a] < hi[j, a] + s and lo[j, a] + s < hi[i, a] for s in sh)
+            if meet:
+                t.append(j)
+                if nover == nd - 1:
+                    f.append(j)
+        touch.append(t)
+        face.append(f)
+    return touch, face
+
+
+@pytest.mark.parametrize("ndim,nroot,maxlev,bc", [
+    (2, 4, 3, (BC_PERIODIC,) * 4 + (BC_OUTFLOW,) * 2),
+    (2, 2, 3, (BC_OUTFLOW, BC_OUTFLOW, BC_PERIODIC, BC_PERIODIC, BC_OUTFLOW, BC_OUTFLOW)),
+    (2, 1, 3, (BC_PERIODIC,) * 4 + (BC_OUTFLOW,) * 2),
+    (3, 2, 2, (BC_PERIODIC, BC_PERIODIC, BC_OUTFLOW, BC_OUTFLOW, BC_REFLECTING, BC_REFLECTING)),
+    (3, 3, 2, (BC_PERIODIC,) * 6),
+])
+def test_adjacency_matches_all_pairs(ndim, nroot, maxlev, bc):
+    """The root-block buckets of AmrDecomposition._adjacency find the same
+    neighbours as testing every pair (one and two root blocks per periodic
+    axis included, where a neighbour is reached across both sides)."""
+    from flashx_b200.parallel import AmrDecomposition
+    if ndim == 2:
+        root = Geometry(2, 8, 8, 1, nroot, nroot, 1, bc=bc)
+    else:
+        root = Geometry(3, 8, 8, 8, nroot, nroot, nroot, bc=bc)
+    mesh, _ = A.levelset_problem(root, HydroParams(), maxlev)
+    touch, face = AmrDecomposition._adjacency(mesh)
+    bt, bf = _touch_brute_force(mesh)
+    for i in range(mesh.nleaf):
+        assert list(touch[i]) == bt[i] and list(face[i]) == bf[i], f"leaf {i}"
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_stacked_copies_step_like_the_single_mesh(ndim, oracle):
+    """The weak-scaling mesh: `world` copies of a periodic mesh stacked along
+    the slowest axis.  Copy r is rank r's Morton range, and the oracle's
+    whole-mesh step of the stacked mesh leaves every copy equal, bit for bit,
+    to the step of the single mesh (the copies join like the periodic
+    boundary they replace)."""
+    from flashx_b200.parallel import AmrDecomposition
+    if ndim == 2:
+        root = Geometry(2, 8, 8, 1, 4, 4, 1, bc=(BC_PERIODIC,) * 4 + (BC_OUTFLOW,) * 2)
+        mesh, unk = A.levelset_problem(root, HydroParams(order=3), 3)
+    else:
+        root = Geometry(3, 8, 8, 8, 2, 2, 2, bc=(BC_PERIODIC,) * 6)
+        mesh, unk = A.levelset_problem(root, HydroParams(order=3), 2)
+    hp = HydroParams(order=3)
+    world = 3
+    whole, wmesh = A.stack_copies(mesh, world)
+    n = mesh.nleaf
+    assert wmesh.nleaf == world * n
+    for r in range(world):
+        d = AmrDecomposition(wmesh, world, r)
+        assert np.array_equal(d.owned(), np.arange(r * n, (r + 1) * n))
+    one = oracle.Amr(oracle.make_params(root.as_dict(), hp), mesh.levels, mesh.bcoords)
+    many = oracle.Amr(oracle.make_params(whole.as_dict(), hp), wmesh.levels, wmesh.bcoords)
+    u1, uw = unk.copy(), np.concatenate([unk] * world, axis=0)
+    dt = 0.5 * one.compute_dt(u1)
+    assert many.compute_dt(uw) == one.compute_dt(u1)
+    for _ in range(2):
+        one.hydro_step(u1, dt)
+        many.hydro_step(uw, dt)
+    g = root.nguard
+    sl = (slice(None), slice(g, -g) if ndim == 3 else slice(None), slice(g, -g), slice(g, -g))
+    for r in range(world):
+        assert np.array_equal(uw[r * n:(r + 1) * n][sl], u1[sl]), f"copy {r}"
