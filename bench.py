@@ -34,7 +34,8 @@ UNIT = "zone-updates/s"
 BYTES_PER_ZONE = 152   # 9 FP64 reads + 10 FP64 writes per zone-update (algorithmic)
 FLOPS_FILES = {"kh2d": os.path.join(ROOT, "profiles", "hydro2d_kh2048_flops.json")}
 TRAFFIC_FILES = {"kh2d": os.path.join(ROOT, "profiles", "hydro2d_kh2048_traffic.json"),
-                 "rt3d": os.path.join(ROOT, "profiles", "hydro3d_rt256_traffic.json")}
+                 "rt3d": os.path.join(ROOT, "profiles", "hydro3d_rt256_traffic.json"),
+                 "amr3d": os.path.join(ROOT, "profiles", "amr_step_amr3d5230_traffic.json")}
 WORKLOADS = {
     "kh2d": "kh2d: 2-D Kelvin-Helmholtz 2048^2 (128x128 blocks of 16^2), periodic, PPM+HLLC, "
             "mc/char limiting, CFL 0.8, gamma 1.4",
@@ -608,9 +609,9 @@ def run_ours(args):
     flops = fp_roofline(args.config, "fp64", ncell / (kernel_ms / 1e3))
     if flops:
         line["roofline_fp"] = flops
+    line["config"]["tuning"] = dev.tuning()
     if mesh is not None:
         line["config"]["leaves_per_level"] = mesh.level_counts()
-        line["config"]["tuning"] = dev.tuning()
         if world == 1:
             line["regrid"] = regrid_cycle(dev, hp, mesh)
     dev.close()

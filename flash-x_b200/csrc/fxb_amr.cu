@@ -1032,8 +1032,9 @@ int persist_setup()
 {
     const char *ev = getenv("FXB_AMR_PERSISTENT");
     S.persist_ok = !(ev && ev[0] == '0') && S.d_plan && !extended_options(S.C.dprm);
-    S.persist = S.persist_ok;
-    if (!S.persist) return FXB_OK;
+    // the batched launches until the tuner times both forms (FXB_AMR_PERSISTENT=1 forces this one)
+    S.persist = S.persist_ok && ev && ev[0] == '1';
+    if (!S.persist_ok) return FXB_OK;
     const char *tw = getenv("FXB_TEST_WAIT_TIMEOUT");
     if (tw && tw[0] == '1') { S.test_stall = 1; S.wait_budget = 1000000; }
     const char *ek = getenv("FXB_AMR_CLUSTER");
@@ -1418,7 +1419,8 @@ int amr_tune()
     const char *ev = getenv("FXB_AMR_TUNE");
     if (ev && atoi(ev) == 0) {
         snprintf(S.tune_log, sizeof(S.tune_log), "AMR launch shape (CTAs per block): fill=%d sig=%d slopes=%d "
-                 "update=%d, defaults (tuning off)", S.fill_cta, S.cta[0], S.cta[1], S.cta[3]);
+                 "update=%d, defaults (tuning off); step form: %s", S.fill_cta, S.cta[0], S.cta[1], S.cta[3],
+                 S.persist ? "persistent" : "batched launches");
         return FXB_OK;
     }
     const bool mixed = S.C.prm.precision == FXB_MIXED;
@@ -1499,6 +1501,8 @@ int amr_tune()
         snprintf(form, sizeof(form), "; step form: %s (ms per step: batched %.2f, persistent K=1 %.2f K=2 %.2f K=4 %.2f "
                  "K=8 %.2f)", S.persist ? (kbest == 1 ? "persistent, 1 CTA per leaf" : "persistent, cluster per leaf")
                  : "batched launches", tb, tk[0], tk[1], tk[2], tk[3]);
+    } else {
+        snprintf(form, sizeof(form), "; step form: %s (not timed)", S.persist ? "persistent" : "batched launches");
     }
     for (int i = 0; i < 5; i++) cudaEventDestroy(e[i]);
     CKA(cudaMemsetAsync(S.C.rate_max, 0, sizeof(unsigned long long), S.C.stream));

@@ -87,6 +87,11 @@ struct Lib {
     long snpad = 0, snw = 0;
     CUtensorMap tmap2d[2];         // 2-D: the window variables of buf[0] / buf[1] for TMA
     int use_tma = 1;
+    // launch shapes of the uniform grid, chosen by ug_tune at the first attach
+    bool ug_tuned = false;
+    int ug_cta[4] = {8, 8, 8, 8};  // 3-D: CTAs per SM of sigma, face states, fluxes, update
+    int sf_t1[3] = {0, 0, 0};      // 3-D FP32: lines per fused face-state tile (0: by lane count)
+    char ug_log[512] = "";
     unsigned tma_extra_tx = 0;     // test hook (FXB_TEST_WAIT_TIMEOUT): a window barrier that never completes
     long long wait_budget = kTmaWaitBudget;
     fxb_error lasterr{};
@@ -435,6 +440,8 @@ int launch_hydro(int src, const double *dtv, double dt)
         a.flat_bstride = 0;
         a.hyb = (const unsigned char *)L.hyb;
         for (int d = 0; d < 3; d++) { a.wst[d] = L.w3[d]; a.flx[d] = L.f3[d]; a.ctufb[d] = L.ctufb[d]; }
+        for (int q = 0; q < 4; q++) a.cta[q] = 148 * L.ug_cta[q];
+        for (int d = 0; d < 3; d++) a.sf_t1[d] = L.sf_t1[d];
         for (int d = 0; d < 3 && L.ns; d++)
             if (cudaMemsetAsync(L.ctufb[d], 0, L.snw, L.stream) != cudaSuccess) return cuda_fail(cudaGetLastError(), "memset");
         if (L.prm.precision == FXB_MIXED) launch_hydro3d_mixed(a, L.stream);
@@ -827,6 +834,118 @@ extern "C" int fxb_register_blocks(const fxb_block_desc *blocks, int nblk)
     return FXB_OK;
 }
 
+// one step from the current state with dt = 0 (the state is not switched):
+// the fastest of `reps` runs, in ms
+static int time_ug_step(float &best, int reps)
+{
+    best = 1e30f;
+    for (int r = 0; r < reps; r++) {
+        CK(cudaEventRecord(L.ev0, L.stream));
+        int rc = launch_hydro(L.cur, nullptr, 0.0);
+        if (rc) return rc;
+        CK(cudaEventRecord(L.ev1, L.stream));
+        CK(cudaEventSynchronize(L.ev1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, L.ev0, L.ev1));
+        best = ms < best ? ms : best;
+    }
+    return FXB_OK;
+}
+
+// The uniform grid's launch shapes, timed over whole steps on the attached
+// state at the first attach: 2-D window staging by TMA or by per-thread
+// loads; 3-D CTAs per SM of each stage (2, 4, 8, 16), one stage at a time,
+// and in FP32 the lines per fused face-state tile of each direction.  A
+// candidate replaces the current choice when it is more than 1 % faster.
+// FXB_UG_TUNE=0 keeps the defaults; FXB_TMA=0/1 fixes the 2-D staging.  The
+// timed steps leave no trace: the CFL rate and the error word are cleared.
+static int ug_tune()
+{
+    const char *ev = getenv("FXB_UG_TUNE");
+    const bool off = ev && ev[0] == '0';
+    float base = 0.f;
+    int rc = FXB_OK;
+    if (!off) {
+        // warm-up: about 50 ms of steps (clocks up from idle), then the defaults
+        float spent = 0.f;
+        for (int w = 0; w < 64 && spent < 50.f && !rc; w++) {
+            rc = time_ug_step(base, 1);
+            spent += base;
+        }
+        if (!rc) rc = time_ug_step(base, 3);
+        if (rc) return rc;
+    }
+    if (L.dom.ndim == 2) {
+        float t[2] = {-1.f, -1.f};
+        if (!off && !getenv("FXB_TMA") && !L.tma_extra_tx) {
+            const int keep = L.use_tma;
+            t[keep] = base;
+            L.use_tma = 1 - keep;
+            rc = time_ug_step(t[1 - keep], 3);
+            if (rc) return rc;
+            L.use_tma = t[1 - keep] < 0.99f * t[keep] ? 1 - keep : keep;
+        }
+        snprintf(L.ug_log, sizeof(L.ug_log), "uniform grid 2-D: one CTA of 320 threads per 16x16 tile; window "
+                 "staging: %s (ms per step: TMA %.3f, per-thread loads %.3f%s)", L.use_tma ? "TMA" : "per-thread loads",
+                 t[1], t[0], off ? ", tuning off" : "");
+    } else {
+        const bool fused = L.prm.precision == FXB_MIXED;
+        float cur = base;
+        // FXB_UG_CTA="s,f,x,u" and FXB_UG_T1="x,y,z" fix the shapes instead
+        const char *ec = getenv("FXB_UG_CTA"), *et = getenv("FXB_UG_T1");
+        if (ec) {
+            int v[4];
+            if (sscanf(ec, "%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3]) != 4)
+                return fail(FXB_EARG, "FXB_UG_CTA: four CTA counts per SM expected");
+            for (int q = 0; q < 4; q++) L.ug_cta[q] = v[q] < 1 ? 1 : v[q] > 32 ? 32 : v[q];
+        }
+        if (et) {
+            int v[3];
+            if (sscanf(et, "%d,%d,%d", &v[0], &v[1], &v[2]) != 3)
+                return fail(FXB_EARG, "FXB_UG_T1: three line counts expected");
+            for (int d = 0; d < 3; d++) L.sf_t1[d] = v[d] < 0 ? 0 : v[d];
+        }
+        if (!off && !ec && !et) {
+            const int cand[4] = {2, 4, 8, 16};
+            for (int q = 0; q < 4; q++) {
+                if (fused && (q == 1 || q == 2)) continue;     // the fused kernel's grid follows its tiles
+                int keep = L.ug_cta[q];
+                for (int c : cand) {
+                    if (c == keep) continue;
+                    L.ug_cta[q] = c;
+                    float t = 0.f;
+                    rc = time_ug_step(t, 3);
+                    if (rc) return rc;
+                    if (t < 0.99f * cur) { cur = t; keep = c; }
+                    L.ug_cta[q] = keep;
+                }
+            }
+            if (fused)
+                for (int d = 0; d < 3; d++) {
+                    int keep = L.sf_t1[d];
+                    for (int t1 : {1, 2, 4, 8, 16}) {
+                        L.sf_t1[d] = t1;
+                        float t = 0.f;
+                        rc = time_ug_step(t, 3);
+                        if (rc) return rc;
+                        if (t < 0.99f * cur) { cur = t; keep = t1; }
+                        L.sf_t1[d] = keep;
+                    }
+                }
+        }
+        char tiles[96] = "";
+        if (fused) snprintf(tiles, sizeof(tiles), "; face-state tile lines x/y/z: %d/%d/%d (0: by lane count)",
+                            L.sf_t1[0], L.sf_t1[1], L.sf_t1[2]);
+        snprintf(L.ug_log, sizeof(L.ug_log), "uniform grid 3-D: CTAs of 256 threads per SM: sigma %d, face states %d, "
+                 "fluxes %d, update %d%s (ms per step: defaults %.3f, tuned %.3f%s)", L.ug_cta[0], L.ug_cta[1],
+                 L.ug_cta[2], L.ug_cta[3], tiles, base, cur, off ? ", tuning off" : "");
+    }
+    CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
+    CK(cudaMemsetAsync(L.err, 0, sizeof(int), L.stream));
+    CK(cudaStreamSynchronize(L.stream));
+    return FXB_OK;
+}
+
 extern "C" int fxb_attach_unk(const double *unk_host)
 {
     if (!unk_host) return fail(FXB_EARG, "fxb_attach_unk: null UNK");
@@ -849,6 +968,12 @@ extern "C" int fxb_attach_unk(const double *unk_host)
     L.attached = true;
     L.unk_attached = unk_host;
     state_changed(false);
+    if (!L.ug_tuned) {
+        L.ug_tuned = true;        // new data on the same grid keeps the launch shapes
+        int rc = ug_tune();
+        if (rc) return rc;
+        state_changed(false);
+    }
     return FXB_OK;
 }
 
@@ -1442,8 +1567,7 @@ extern "C" int fxb_tuning(char *buf, int len)
 {
     if (!buf || len <= 0) return fail(FXB_EARG, "fxb_tuning: null or empty buffer");
     if (amr_active()) snprintf(buf, len, "%s", amr_tuning_log());
-    else if (L.dom.ndim == 2) snprintf(buf, len, "uniform grid 2-D: one CTA of %d threads per 16x16 tile (fixed)", 320);
-    else snprintf(buf, len, "uniform grid 3-D: %d CTAs of 256 threads per stage (fixed)", 148 * 8);
+    else snprintf(buf, len, "%s", L.ug_tuned ? L.ug_log : "uniform grid: launch shapes are chosen at the first attach");
     return FXB_OK;
 }
 

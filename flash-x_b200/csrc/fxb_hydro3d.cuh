@@ -76,9 +76,11 @@ struct Args3D {
     double *odata;              // interior store [block][var][cell]
     long o_vstride, o_bstride;
     long sig_bstride, w_bstride[3], f_bstride[3];   // elements of R per batch entry
-    int cta[4];                 // CTAs per batch entry: sig3d, slope3d, (unused), update3d
+    int cta[4];                 // AMR: CTAs per batch entry (sig3d, slope3d, flux3d, update3d); uniform
+                                // grid: CTAs of sig3d (+ flattening, hybrid), states3d (+ slopes), flux3d, update3d
     FastDiv fdx[5], fdy[5];     // divisors nx + e and ny + e (e = 0, 1, 2, 4), set by the launchers
     int sf_len[3], sf_lines[3]; // face-state tiles per direction (cells along d, lines), set by the launchers
+    int sf_t1[3] = {0, 0, 0};   // lines per face-state tile chosen by the tuner (0: the launchers' choice)
     const unsigned char *hyb;   // hybrid order (uniform grid): 1 where min DivU over the cell's box < eps, padded box
     long rate_c0 = 0, rate_c1 = 0x7fffffffffffffffL;   // cells [c0, c1) enter the CFL rate (a slab's own)
     unsigned char *ctufb[3] = {nullptr, nullptr, nullptr};   // species on: 1 where the CTU fallback fired (Grid3::widx)
@@ -91,14 +93,16 @@ struct Args3D {
 #ifndef FXB_SF_MAXT
 #define FXB_SF_MAXT 288
 #endif
-inline void sflux_tile(int d, int N, int N1, int halo, int &Ls, int &T1)
+// force_t1 > 0 takes that line count (when it fits) and only picks Ls.
+inline void sflux_tile(int d, int N, int N1, int halo, int &Ls, int &T1, int force_t1 = 0)
 {
     long best = -1;
     Ls = 3; T1 = 1;
     const int cand[5] = {16, 8, 4, 2, 1};
+    const bool forced = force_t1 > 0 && force_t1 <= N1;
     for (int t1 : cand) {
         if (t1 > N1) continue;
-        if (d != 0 && t1 < (N1 < 8 ? N1 : 8)) continue;
+        if (forced ? t1 != force_t1 : (d != 0 && t1 < (N1 < 8 ? N1 : 8))) continue;
         for (int ls = 3; (ls + halo) * t1 <= FXB_SF_MAXT; ls++) {
             const long nseg = (N + ls - 1) / (ls - 1);
             const long work = nseg * (long)((N1 + t1 - 1) / t1) * (((ls + halo) * t1 + 31) / 32 * 32);
@@ -116,7 +120,7 @@ inline Args3D with_divisors(const Args3D &a, int halo = 0)
     Args3D b = a;
     for (int e = 0; e <= 4; e++) { b.fdx[e] = make_fastdiv((unsigned)a.nx + e); b.fdy[e] = make_fastdiv((unsigned)a.ny + e); }
     const int n[3] = {a.nx, a.ny, a.nz};
-    for (int d = 0; d < 3; d++) sflux_tile(d, n[d], d == 0 ? a.ny : a.nx, halo, b.sf_len[d], b.sf_lines[d]);
+    for (int d = 0; d < 3; d++) sflux_tile(d, n[d], d == 0 ? a.ny : a.nx, halo, b.sf_len[d], b.sf_lines[d], a.sf_t1[d]);
     return b;
 }
 enum { AMR_SIG = 1, AMR_STATES = 2 };   // sigma (+ flattening); slopes, face states and fluxes
@@ -1023,7 +1027,7 @@ template <class R, bool AMR, int DIR, bool EXT> void launch_states3d_rs(const Ar
         if (a.prm.order == 2) {   // MUSCL-Hancock: three cells per face state, no slope pass
             if constexpr (!FusedFaces<R>::value) {
                 states3d_kernel<R, 2, AMR, DIR, true><<<g, 256, 0, s>>>(a);
-                flux3d_kernel<R, AMR, DIR, true><<<dim3(AMR ? a.cta[2] : g.x, g.y), 256, 0, s>>>(a);
+                flux3d_kernel<R, AMR, DIR, true><<<dim3(a.cta[2], g.y), 256, 0, s>>>(a);
             } else {
                 const int N = DIR == 0 ? a.nx : DIR == 1 ? a.ny : a.nz;
                 const int N1 = DIR == 0 ? a.ny : a.nx, N2 = DIR == 2 ? a.ny : a.nz;
@@ -1042,7 +1046,7 @@ template <class R, bool AMR, int DIR, bool EXT> void launch_states3d_rs(const Ar
             slope3d_kernel<R, AMR><<<g, 256, 0, s>>>(a, DIR);
             states3d_kernel<R, 3, AMR, DIR, EXT><<<g, 256, 0, s>>>(a);
         }
-        flux3d_kernel<R, AMR, DIR, EXT><<<dim3(AMR ? a.cta[2] : g.x, g.y), 256, 0, s>>>(a);
+        flux3d_kernel<R, AMR, DIR, EXT><<<dim3(a.cta[2], g.y), 256, 0, s>>>(a);
     } else {
         const int N = DIR == 0 ? a.nx : DIR == 1 ? a.ny : a.nz;
         const int N1 = DIR == 0 ? a.ny : a.nx, N2 = DIR == 2 ? a.ny : a.nz;
@@ -1108,31 +1112,32 @@ inline size_t hyb3d_bytes(int nx, int ny, int nz, size_t rsz)
     return rsz * (size_t)(nx + 6) * (ny + 6) * (nz + 6) + (size_t)(nx + 2) * (ny + 2) * (nz + 2);
 }
 
+// a.cta: the CTAs of each stage (grid-stride kernels of 256 threads)
 template <class R> void launch_hydro3d_t(const Args3D &a0, cudaStream_t s)
 {
     const Args3D a = with_divisors(a0, sflux_halo<R>(a0));
-    const int nb = 148 * 8;
+    const int nsig = a.cta[0], nst = a.cta[1], nupd = a.cta[3];
     if (a.prm.use_hybrid) {
         R *divu = (R *)a.hyb;
         unsigned char *flag = (unsigned char *)a.hyb + sizeof(R) * (size_t)(a.nx + 6) * (a.ny + 6) * (a.nz + 6);
-        divu3d_kernel<R><<<nb, 256, 0, s>>>(a, divu);
-        hyb3d_kernel<R><<<nb, 256, 0, s>>>(a, divu, flag);
+        divu3d_kernel<R><<<nsig, 256, 0, s>>>(a, divu);
+        hyb3d_kernel<R><<<nsig, 256, 0, s>>>(a, divu, flag);
         Args3D b = a;
         b.hyb = flag;
-        if (a.prm.flattening) flat3d_kernel<R, false><<<nb, 256, 0, s>>>(b);
-        sig3d_kernel<R, false><<<nb, 256, 0, s>>>(b);
-        launch_states3d<R, false, 0>(b, dim3(nb), s);
-        launch_states3d<R, false, 1>(b, dim3(nb), s);
-        launch_states3d<R, false, 2>(b, dim3(nb), s);
-        update3d_kernel<R, false><<<nb, 256, 0, s>>>(b);
+        if (a.prm.flattening) flat3d_kernel<R, false><<<nsig, 256, 0, s>>>(b);
+        sig3d_kernel<R, false><<<nsig, 256, 0, s>>>(b);
+        launch_states3d<R, false, 0>(b, dim3(nst), s);
+        launch_states3d<R, false, 1>(b, dim3(nst), s);
+        launch_states3d<R, false, 2>(b, dim3(nst), s);
+        update3d_kernel<R, false><<<nupd, 256, 0, s>>>(b);
         return;
     }
-    if (a.prm.flattening) flat3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
-    sig3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
-    launch_states3d<R, false, 0>(a, dim3(nb), s);
-    launch_states3d<R, false, 1>(a, dim3(nb), s);
-    launch_states3d<R, false, 2>(a, dim3(nb), s);
-    update3d_kernel<R, false><<<nb, 256, 0, s>>>(a);
+    if (a.prm.flattening) flat3d_kernel<R, false><<<nsig, 256, 0, s>>>(a);
+    sig3d_kernel<R, false><<<nsig, 256, 0, s>>>(a);
+    launch_states3d<R, false, 0>(a, dim3(nst), s);
+    launch_states3d<R, false, 1>(a, dim3(nst), s);
+    launch_states3d<R, false, 2>(a, dim3(nst), s);
+    update3d_kernel<R, false><<<nupd, 256, 0, s>>>(a);
 }
 
 // ---- AMR batch: boundary fluxes for flux correction ------------------------------

@@ -198,14 +198,17 @@ def test_amr_persistent_wait_timeout_reports_status(oracle, need_gpu, monkeypatc
     am = oracle.Amr(oracle.make_params(root.as_dict(), hp), mesh.levels, mesh.bcoords)
     dt = 0.5 * am.compute_dt(unk)
     monkeypatch.setenv("FXB_TEST_WAIT_TIMEOUT", "1")
+    monkeypatch.setenv("FXB_AMR_PERSISTENT", "1")
     dev = HydroDevice(root, hp, "fp64", mesh=mesh)
     dev.attach_unk(unk.copy())
+    assert "step form: persistent" in dev.tuning()
     dev.Hydro(0.0, dt, dt)
     with pytest.raises(FlashXError) as ei:
         dev.Hydro_computeDt()
     assert ei.value.code == FXB_ETIMEOUT
     dev.close()
     monkeypatch.delenv("FXB_TEST_WAIT_TIMEOUT")
+    monkeypatch.delenv("FXB_AMR_PERSISTENT")
     _, ref = _oracle(oracle, root, hp, mesh, unk, [dt])
     dev, out = _gpu(root, hp, mesh, unk, [dt])
     np.testing.assert_array_equal(_interior(root, out), _interior(root, ref))

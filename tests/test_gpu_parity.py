@@ -244,6 +244,39 @@ def test_tma_window_equals_thread_loads(need_gpu, monkeypatch, precision):
     assert np.array_equal(outs[0][..., HYDRO_VARS], outs[1][..., HYDRO_VARS])
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("config", ["rt3d", "sweep3d"])
+def test_ug_launch_shapes_give_identical_states(need_gpu, monkeypatch, precision, config):
+    """The uniform-grid tuner only changes launch shapes: the defaults
+    (FXB_UG_TUNE=0), the tuned shapes and forced odd ones (CTAs per SM per
+    stage, lines per fused face-state tile) step to the same state bit for
+    bit, and fxb_tuning reports the shapes in use."""
+    geom, hp, init = S.config(config, scale=0.25 if config == "rt3d" else 0.5)
+    unk = init(geom, hp)
+    outs = []
+    for env in ({"FXB_UG_TUNE": "0"}, {}, {"FXB_UG_CTA": "2,16,4,1", "FXB_UG_T1": "1,16,2"}):
+        for k in ("FXB_UG_TUNE", "FXB_UG_CTA", "FXB_UG_T1"):
+            monkeypatch.delenv(k, raising=False)
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+        dev = HydroDevice(geom, hp, precision)
+        dev.attach_unk(unk.copy())
+        log = dev.tuning()
+        assert log.startswith("uniform grid 3-D")
+        if "FXB_UG_CTA" in env:
+            assert "sigma 2, face states 16, fluxes 4, update 1" in log
+            if precision == "mixed":
+                assert "x/y/z: 1/16/2" in log
+        dt = 0.5 * dev.Hydro_computeDt()
+        dev.advance(4, dt, dt)
+        out = np.zeros(geom.unk_shape)
+        dev.sync_to_host(out)
+        dev.close()
+        outs.append(out)
+    assert np.array_equal(outs[0][..., HYDRO_VARS], outs[1][..., HYDRO_VARS])
+    assert np.array_equal(outs[0][..., HYDRO_VARS], outs[2][..., HYDRO_VARS])
+
+
 def test_window_wait_timeout_reports_status(oracle, need_gpu, monkeypatch):
     """A window barrier that never completes (test hook: it expects 8 bytes
     more than the TMA box brings) ends each waiting tile after its bounded
