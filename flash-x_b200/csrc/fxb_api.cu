@@ -582,8 +582,8 @@ extern "C" int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
     if (d.nguard < 4) return fail(FXB_EARG, "fxb_init: NGUARD must be at least 4");
     if (p.order != 2 && p.order != 3 && p.order != 5)
         return fail(FXB_EUNSUPPORTED, "fxb_init: order must be 2 (MUSCL-Hancock), 3 (PPM) or 5 (WENO)");
-    if (p.riemann < 1 || p.riemann > 4)
-        return fail(FXB_EUNSUPPORTED, "fxb_init: RiemannSolver must be Roe, LLF, HLL or HLLC");
+    if (p.riemann < 1 || p.riemann > 7 || p.riemann == 6)
+        return fail(FXB_EUNSUPPORTED, "fxb_init: RiemannSolver must be Roe, LLF, HLL, HLLC, Marquina or MarquinaModified");
     if (p.limiter < 1 || p.limiter > 5) return fail(FXB_EARG, "fxb_init: unknown slope limiter");
     if (p.precision != FXB_FP64 && p.precision != FXB_MIXED) return fail(FXB_EARG, "fxb_init: unknown precision");
     if (p.flattening && p.use_gravity) return fail(FXB_EUNSUPPORTED, "fxb_init: use_flattening with gravity is not implemented");

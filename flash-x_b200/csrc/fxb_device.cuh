@@ -57,9 +57,15 @@ template <> __device__ __forceinline__ float divc<float>(float x, double c) { re
 // PPM contact steepening, MUSCL-Hancock reconstruction (order 2), artificial
 // viscosity, hybrid order, and the exports species advection reads (2-D mass
 // fluxes)
+// The kernels come in three instantiations (template flag EXT): 0 the
+// default options, 1 the rarely used ones (Roe, contact steepening,
+// MUSCL-Hancock, artificial viscosity, hybrid order, species), 2 those with a
+// Marquina solver, so that each keeps the register allocation of its own code.
+__host__ __device__ inline bool marquina_solver(const DevParams &p) { return p.riemann == 5 || p.riemann == 7; }
 __host__ __device__ inline bool extended_options(const DevParams &p)
 {
-    return p.riemann == 1 || p.steepening || p.order == 2 || p.use_avisc || p.use_hybrid || p.nspec > 0;
+    return p.riemann == 1 || p.riemann == 5 || p.riemann == 7 || p.steepening || p.order == 2 || p.use_avisc ||
+           p.use_hybrid || p.nspec > 0;
 }
 
 // Fortran MIN/MAX with gfortran's argument order: mvar = a1; if (a2 < mvar) mvar = a2
@@ -621,6 +627,41 @@ __device__ __forceinline__ void gravity_faces(const DevParams &prm, R g, R &gl, 
 // ---- Riemann solvers (hy_HLLC.F90:64-335, hy_HLL.F90:64-182) ---------------
 // Vm/Vp: 6-vectors D, VX, VY, VZ, P (global axes), EI; gamc/game passed separately.
 // F[8] receives the HY_*_FLUX slots including the aux-eint pair.
+// OnlyHydro/hy_eigenVector.F90:195-260 (cons = .true.): conservative left and
+// right eigenvectors of the state Va = D, VX, VY, VZ, P with gamma_e ge and
+// sound speed cf along dir; L[variable][wave], Rv[variable][wave], the waves
+// u - c, shear, entropy, shear, u + c
+template <class R>
+__device__ __forceinline__ void cons_eigvec(int dir, const R Va[5], R ge, R cf, R L[5][5], R Rv[5][5])
+{
+    const int v1 = 1 + dir, v2 = 1 + (dir + 1) % 3, v3 = 1 + (dir + 2) % 3;
+    const R V1 = Va[v1], V2 = Va[v2], V3 = Va[v3];
+    const R k = R(1.) - ge;
+    const R a2e = cf * cf, a2inv = rdiv(R(1.), a2e), Na = R(0.5) * a2inv;
+    R u2 = R(0.);
+    u2 = u2 + Va[1] * Va[1]; u2 = u2 + Va[2] * Va[2]; u2 = u2 + Va[3] * Va[3];
+    u2 = R(0.5) * u2;
+    const R H = rdiv(Va[0] * u2 - rdiv(Va[4], k) + Va[4], Va[0]);
+#pragma unroll
+    for (int a = 0; a < 5; a++)
+#pragma unroll
+        for (int w = 0; w < 5; w++) { L[a][w] = R(0); Rv[a][w] = R(0); }
+    L[0][0] = Na * (-(k * u2) + V1 * cf); L[v1][0] = -(Na * (-(k * V1) + cf));
+    L[v2][0] = Na * k * V2; L[v3][0] = Na * k * V3; L[4][0] = -(Na * k);
+    L[0][1] = -V2; L[v2][1] = R(1.);
+    L[0][2] = R(1.) + Na * k * u2 * R(2.);
+    L[v1][2] = -(k * V1 * a2inv); L[v2][2] = -(k * V2 * a2inv); L[v3][2] = -(k * V3 * a2inv);
+    L[4][2] = k * a2inv;
+    L[0][3] = -V3; L[v3][3] = R(1.);
+    L[0][4] = Na * (-(k * u2) - V1 * cf); L[v1][4] = -(Na * (-(k * V1) - cf));
+    L[v2][4] = Na * k * V2; L[v3][4] = Na * k * V3; L[4][4] = -(Na * k);
+    Rv[0][0] = R(1.); Rv[v1][0] = V1 - cf; Rv[v2][0] = V2; Rv[v3][0] = V3; Rv[4][0] = H - V1 * cf;
+    Rv[v2][1] = R(1.); Rv[4][1] = V2;
+    Rv[0][2] = R(1.); Rv[v1][2] = V1; Rv[v2][2] = V2; Rv[v3][2] = V3; Rv[4][2] = u2;
+    Rv[v3][3] = R(1.); Rv[4][3] = V3;
+    Rv[0][4] = R(1.); Rv[v1][4] = V1 + cf; Rv[v2][4] = V2; Rv[v3][4] = V3; Rv[4][4] = H + V1 * cf;
+}
+
 // hy_Roe.F90:62-205 (acoustic eigenvalues entropy-fixed by hy_entropyFix.F90
 // when entropy = .true.): the mean state of hy_avgState, its
 // conservative eigenvectors (OnlyHydro/hy_eigenVector.F90:128-166) and
@@ -665,33 +706,8 @@ __device__ __forceinline__ int riemann_roe(int dir, int entropy_fix, const R *Vm
             }
         }
     }
-    const int v1 = 1 + dir, v2 = 1 + (dir + 1) % 3, v3 = 1 + (dir + 2) % 3;
-    const R V1 = Va[v1], V2 = Va[v2], V3 = Va[v3];
-    const R k = R(1.) - geA;
-    const R a2e = cf * cf, a2inv = rdiv(R(1.), a2e), Na = R(0.5) * a2inv;
-    R u2 = R(0.);
-    u2 = u2 + Va[1] * Va[1]; u2 = u2 + Va[2] * Va[2]; u2 = u2 + Va[3] * Va[3];
-    u2 = R(0.5) * u2;
-    const R H = rdiv(Va[0] * u2 - rdiv(Va[4], k) + Va[4], Va[0]);
     R L[5][5], Rv[5][5];
-#pragma unroll
-    for (int a = 0; a < 5; a++)
-#pragma unroll
-        for (int w = 0; w < 5; w++) { L[a][w] = R(0); Rv[a][w] = R(0); }
-    L[0][0] = Na * (-(k * u2) + V1 * cf); L[v1][0] = -(Na * (-(k * V1) + cf));
-    L[v2][0] = Na * k * V2; L[v3][0] = Na * k * V3; L[4][0] = -(Na * k);
-    L[0][1] = -V2; L[v2][1] = R(1.);
-    L[0][2] = R(1.) + Na * k * u2 * R(2.);
-    L[v1][2] = -(k * V1 * a2inv); L[v2][2] = -(k * V2 * a2inv); L[v3][2] = -(k * V3 * a2inv);
-    L[4][2] = k * a2inv;
-    L[0][3] = -V3; L[v3][3] = R(1.);
-    L[0][4] = Na * (-(k * u2) - V1 * cf); L[v1][4] = -(Na * (-(k * V1) - cf));
-    L[v2][4] = Na * k * V2; L[v3][4] = Na * k * V3; L[4][4] = -(Na * k);
-    Rv[0][0] = R(1.); Rv[v1][0] = V1 - cf; Rv[v2][0] = V2; Rv[v3][0] = V3; Rv[4][0] = H - V1 * cf;
-    Rv[v2][1] = R(1.); Rv[4][1] = V2;
-    Rv[0][2] = R(1.); Rv[v1][2] = V1; Rv[v2][2] = V2; Rv[v3][2] = V3; Rv[4][2] = u2;
-    Rv[v3][3] = R(1.); Rv[4][3] = V3;
-    Rv[0][4] = R(1.); Rv[v1][4] = V1 + cf; Rv[v2][4] = V2; Rv[v3][4] = V3; Rv[4][4] = H + V1 * cf;
+    cons_eigvec(dir, Va, geA, cf, L, Rv);
     R dU[5], sigF[5] = {R(0), R(0), R(0), R(0), R(0)};
 #pragma unroll
     for (int a = 0; a < 5; a++) dU[a] = UR[a] - UL[a];
@@ -709,15 +725,181 @@ __device__ __forceinline__ int riemann_roe(int dir, int entropy_fix, const R *Vm
     return 0;
 }
 
-template <class R, bool EXT>
+// Columns of the conservative eigenvectors of cons_eigvec, one at a time
+// (same expressions): the per-state constants, then column w of L or R in
+// variable order D, MX, MY, MZ, E.
+template <class R> struct EigC {
+    R k, a2inv, Na, u2, H, V1, V2, V3, cf;
+    int v1, v2, v3;
+};
+template <class R>
+__device__ __forceinline__ EigC<R> eig_consts(int dir, const R Va[5], R ge, R cf)
+{
+    EigC<R> e;
+    e.v1 = 1 + dir; e.v2 = 1 + (dir + 1) % 3; e.v3 = 1 + (dir + 2) % 3;
+    e.V1 = Va[e.v1]; e.V2 = Va[e.v2]; e.V3 = Va[e.v3];
+    e.k = R(1.) - ge;
+    e.cf = cf;
+    const R a2e = cf * cf;
+    e.a2inv = rdiv(R(1.), a2e);
+    e.Na = R(0.5) * e.a2inv;
+    R u2 = R(0.);
+    u2 = u2 + Va[1] * Va[1]; u2 = u2 + Va[2] * Va[2]; u2 = u2 + Va[3] * Va[3];
+    e.u2 = R(0.5) * u2;
+    e.H = rdiv(Va[0] * e.u2 - rdiv(Va[4], e.k) + Va[4], Va[0]);
+    return e;
+}
+// d: density row, n / t1 / t2: momentum along v1 / v2 / v3, en: energy row
+template <class R>
+__device__ __forceinline__ void eig_place(const EigC<R> &e, R d, R n, R t1, R t2, R en, R c[5])
+{
+    c[0] = d; c[4] = en;
+#pragma unroll
+    for (int a = 1; a < 4; a++) c[a] = a == e.v1 ? n : (a == e.v2 ? t1 : t2);
+}
+template <class R>
+__device__ __forceinline__ void eig_lcol(const EigC<R> &e, int w, R c[5])
+{
+    const R z = R(0);
+    if (w == 0)
+        eig_place(e, e.Na * (-(e.k * e.u2) + e.V1 * e.cf), -(e.Na * (-(e.k * e.V1) + e.cf)), e.Na * e.k * e.V2,
+                  e.Na * e.k * e.V3, -(e.Na * e.k), c);
+    else if (w == 1)
+        eig_place(e, -e.V2, z, R(1.), z, z, c);
+    else if (w == 2)
+        eig_place(e, R(1.) + e.Na * e.k * e.u2 * R(2.), -(e.k * e.V1 * e.a2inv), -(e.k * e.V2 * e.a2inv),
+                  -(e.k * e.V3 * e.a2inv), e.k * e.a2inv, c);
+    else if (w == 3)
+        eig_place(e, -e.V3, z, z, R(1.), z, c);
+    else
+        eig_place(e, e.Na * (-(e.k * e.u2) - e.V1 * e.cf), -(e.Na * (-(e.k * e.V1) - e.cf)), e.Na * e.k * e.V2,
+                  e.Na * e.k * e.V3, -(e.Na * e.k), c);
+}
+template <class R>
+__device__ __forceinline__ void eig_rcol(const EigC<R> &e, int w, R c[5])
+{
+    const R z = R(0);
+    if (w == 0) eig_place(e, R(1.), e.V1 - e.cf, e.V2, e.V3, e.H - e.V1 * e.cf, c);
+    else if (w == 1) eig_place(e, z, z, R(1.), z, e.V2, c);
+    else if (w == 2) eig_place(e, R(1.), e.V1, e.V2, e.V3, e.u2, c);
+    else if (w == 3) eig_place(e, z, z, z, R(1.), e.V3, c);
+    else eig_place(e, R(1.), e.V1 + e.cf, e.V2, e.V3, e.H + e.V1 * e.cf, c);
+}
+
+// hy_Marquina.F90:52-227 and hy_MarquinaModified.F90:52-195 (hydro), with the
+// arithmetic of the oracle: eigenvalues and conservative eigenvectors of the
+// left and of the right state.  Marquina (modified = false) is restated as
+// the reference writes it: per wave k, leig is read as leig(k, 1:5) (the
+// stored layout is leig(variable, wave)), each projection adds leig(k, XMOM
+// + dir - 1) times the face pressure, the upwind side's part where both
+// states' eigenvalues share a sign, else half of each side's flux plus or
+// minus the largest |eigenvalue| times its conserved state; the sum along
+// the right eigenvectors, face-pressure slot zero.  MarquinaModified: the
+// mean flux less half the sum over waves of 0.5 (|lam_L| + |lam_R|)
+// (r_R (l_R . U_R) - r_L (l_L . U_L)).  The eigenvectors are built a column
+// at a time; only the EXT = 2 kernel instantiations contain this.
+template <class R>
+__device__ __forceinline__ int riemann_marquina(int dir, bool modified, const R *Vm, R gcL, R geL, const R *Vp, R gcR,
+                                                R geR, const R UL[5], const R UR[5], const R FL[6], const R FR[6],
+                                                R F[8])
+{
+    const R aL2 = rdiv(gcL * Vm[P], Vm[D]), aR2 = rdiv(gcR * Vp[P], Vp[D]);
+    if (aL2 <= R(0) || aR2 <= R(0)) return ERR_SOUND;   // hy_eigenParameters aborts
+    const R cL = rsqrt_(aL2), cR = rsqrt_(aR2);
+    const R uL = Vm[1 + dir], uR = Vp[1 + dir];
+    // hy_eigenValue: u - c, u, u, u, u + c
+    auto lam = [](R u, R c, int k) { return k == 0 ? u - c : (k == 4 ? u + c : u); };
+    if (!modified) {
+        R mL = fabs(lam(uL, cL, 0)), mR = fabs(lam(uR, cR, 0));
+#pragma unroll
+        for (int k = 1; k < 5; k++) {
+            if (fabs(lam(uL, cL, k)) > mL) mL = fabs(lam(uL, cL, k));
+            if (fabs(lam(uR, cR, k)) > mR) mR = fabs(lam(uR, cR, k));
+        }
+        const R amax = fmax2(mL, mR);
+        const int mom = 1 + dir;
+        R part0[5];
+#pragma unroll
+        for (int side = 0; side < 2; side++) {
+            const R *Vs = side ? Vp : Vm;
+            const R Va[5] = {Vs[D], Vs[VX], Vs[VY], Vs[VZ], Vs[P]};
+            const EigC<R> e = eig_consts(dir, Va, side ? geR : geL, side ? cR : cL);
+            const R *Fs = side ? FR : FL;
+            const R *Us = side ? UR : UL;
+            // dot_product(leig(k, 1:5), .): row k across the wave columns
+            R lf[5], lu[5], lm[5];
+#pragma unroll
+            for (int j = 0; j < 5; j++) {
+                R c[5];
+                eig_lcol(e, j, c);
+#pragma unroll
+                for (int k = 0; k < 5; k++) {
+                    lf[k] = (j == 0 ? R(0.) : lf[k]) + c[k] * Fs[j];
+                    lu[k] = (j == 0 ? R(0.) : lu[k]) + c[k] * Us[j];
+                    if (j == 0 || j == mom) lm[k] = c[k];
+                }
+            }
+            R vec[5];
+#pragma unroll
+            for (int k = 0; k < 5; k++) {
+                const R lk = lam(uL, cL, k), rk = lam(uR, cR, k);
+                if (lk * rk > R(0.))
+                    vec[k] = ((lk > R(0.)) == (side == 0)) ? lf[k] + lm[k] * Fs[5] : R(0.);
+                else if (side == 0)
+                    vec[k] = R(0.5) * (lf[k] + amax * lu[k] + lm[k] * Fs[5]);
+                else
+                    vec[k] = R(0.5) * (lf[k] - amax * lu[k] + lm[k] * Fs[5]);
+            }
+            R acc[5];
+#pragma unroll
+            for (int w = 0; w < 5; w++) {
+                R c[5];
+                eig_rcol(e, w, c);
+#pragma unroll
+                for (int v = 0; v < 5; v++) acc[v] = (w == 0 ? vec[0] * c[v] : acc[v] + vec[w] * c[v]);
+            }
+#pragma unroll
+            for (int v = 0; v < 5; v++) {
+                if (side == 0) part0[v] = acc[v];
+                else F[v] = part0[v] + acc[v];
+            }
+        }
+        F[5] = R(0.0);
+    } else {
+        const R VaL[5] = {Vm[D], Vm[VX], Vm[VY], Vm[VZ], Vm[P]}, VaR[5] = {Vp[D], Vp[VX], Vp[VY], Vp[VZ], Vp[P]};
+        const EigC<R> eL = eig_consts(dir, VaL, geL, cL), eR = eig_consts(dir, VaR, geR, cR);
+        R sigF[5] = {R(0), R(0), R(0), R(0), R(0)};
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            R cr[5], cl[5];
+            eig_lcol(eR, k, cr);
+            eig_lcol(eL, k, cl);
+            R dR = R(0.), dL = R(0.);
+#pragma unroll
+            for (int v = 0; v < 5; v++) { dR = dR + cr[v] * UR[v]; dL = dL + cl[v] * UL[v]; }
+            const R c = R(0.5) * (fabs(lam(uL, cL, k)) + fabs(lam(uR, cR, k)));
+            eig_rcol(eR, k, cr);
+            eig_rcol(eL, k, cl);
+#pragma unroll
+            for (int v = 0; v < 5; v++) sigF[v] = sigF[v] + c * (cr[v] * dR - cl[v] * dL);
+        }
+#pragma unroll
+        for (int v = 0; v < 5; v++) F[v] = (FR[v] + FL[v] - sigF[v]) * R(0.5);
+        F[5] = (FR[5] + FL[5] - R(0.)) * R(0.5);
+    }
+    return 0;
+}
+
+template <class R, int EXT>
 __device__ __forceinline__ int riemann(const DevParams &prm, int dir, const R *Vm, R gcL, R geL,
                                        const R *Vp, R gcR, R geR, R F[8])
 {
     const R velNL = Vm[1 + dir], velNR = Vp[1 + dir];
     const R aL2 = rdiv(gcL * Vm[P], Vm[D]);
     const R aR2 = rdiv(gcR * Vp[P], Vp[D]);
-    const bool roe = EXT && prm.riemann == 1;
-    const bool hllc = !roe && prm.riemann == 4, llf = !roe && prm.riemann == 2;
+    const bool roe = EXT == 1 && prm.riemann == 1;
+    const bool marq = EXT == 2 && (prm.riemann == 5 || prm.riemann == 7);
+    const bool hllc = !roe && !marq && prm.riemann == 4, llf = !roe && !marq && prm.riemann == 2;
     const R tiny = hllc ? R(prm.tiny) : R(1.e-32);
     if ((Vm[D] < tiny && Vm[D] > R(0)) || (Vp[D] < tiny && Vp[D] > R(0)) ||
         (Vm[P] < tiny && Vm[P] > R(0)) || (Vp[P] < tiny && Vp[P] > R(0))) {
@@ -770,6 +952,9 @@ __device__ __forceinline__ int riemann(const DevParams &prm, int dir, const R *V
             F[5] = (FR[5] + FL[5] - smax * (R(0.0) - R(0.0))) * R(0.5);
         } else if (roe) {
             const int e = riemann_roe(dir, prm.entropy_fix, Vm, gcL, geL, Vp, gcR, geR, UL, UR, FL, FR, F);
+            if (e) return e;
+        } else if (marq) {
+            const int e = riemann_marquina(dir, prm.riemann == 7, Vm, gcL, geL, Vp, gcR, geR, UL, UR, FL, FR, F);
             if (e) return e;
         } else if (hllc) {
             R qStar = Vp[D] * velNR * (SR - velNR) - Vm[D] * velNL * (SL - velNL) + Vm[P] - Vp[P];

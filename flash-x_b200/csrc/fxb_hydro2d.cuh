@@ -177,7 +177,7 @@ template <class R> __device__ __forceinline__ R divu2d(const Args2D &a, const Sm
 // face states of one cell along dir, with the transverse correction of the
 // other direction (hy_dataReconstOneStep.F90:931-936) and the negativity
 // fallback (:1131-1165); stores global-order Wp/Wm into s.W[.][t].
-template <class R, bool EXT>
+template <class R, int EXT>
 __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int dir, int t, int wx, int wy,
                                              int dbi, int dbstep, R dtn, R hdtn, R hdtt, R hdt)
 {
@@ -288,7 +288,7 @@ template <class R> __device__ __forceinline__ R ener2d(const Args2D &a, int wx, 
     return (R)__ldg(a.in + DV_ENER * a.vstride + (long)my * a.nx + mx);
 }
 
-template <class R, bool EXT>
+template <class R, int EXT>
 __device__ __forceinline__ void faces_stage(const Args2D &a, Smem2D<R> &s, int dir, int t, int wl, int wr,
                                             int wxl, int wyl, int wxr, int wyr)
 {
@@ -325,7 +325,7 @@ static_assert(sizeof(float) * 8 * WIN * WP % 128 == 0, "FP32 window size keeps t
 static_assert(sizeof(float) * (NF * NFC + 6 * NDB + 12 * NW + 4 * NDB) >= kWinBoxBytes,
               "FP32 staging area holds the FP64 window box");
 
-template <class R, bool EXT>
+template <class R, int EXT>
 __global__ void __launch_bounds__(Threads2D<R>::value) __maxnreg__(Regs2D<R>::value)
 hydro2d_kernel(const __grid_constant__ Args2D a)
 {

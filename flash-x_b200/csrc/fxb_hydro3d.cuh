@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(256) slope3d_kernel(const Args3D a, int d)
 // The face states of one cell from its traced states wm, wp (sweep frame):
 // transverse terms, negativity fallback, gravity and the 3-D full-CTU terms.
 // vc: the cell's 8-vector.
-template <class R, bool AMR, int DIR, bool EXT>
+template <class R, bool AMR, int DIR, int EXT>
 __device__ __forceinline__ void face_states_finish(const Args3D &a, const Ctx3<R, AMR> &X, const double dt,
                                                    const R hdtx, const R hdty, const R hdtz, int i, int j, int k,
                                                    const R vc[8], const EigBase<R> &eb, const R wm[6], const R wp[6],
@@ -589,7 +589,7 @@ __device__ __forceinline__ void hybrid3d(const Args3D &a, const Grid3 &G, int i,
 // The face states of one cell from its interface values: flattening and
 // characteristic tracing (PPM, WENO), then face_states_finish.  Sc: the
 // cell's rotated primitives, vc its 8-vector.
-template <class R, bool AMR, int DIR, bool EXT = false>
+template <class R, bool AMR, int DIR, int EXT = 0>
 __device__ __forceinline__ void face_states_tail(const Args3D &a, const Ctx3<R, AMR> &X, const double dt, const R dtn,
                                                  const R hdtn, const R hdtx, const R hdty, const R hdtz, int i, int j,
                                                  int k, const R Sc[6], const R vc[8], const EigBase<R> &eb,
@@ -609,7 +609,7 @@ __device__ __forceinline__ void face_states_tail(const Args3D &a, const Ctx3<R, 
 // the PPM path (three eigensystems and slopes), of the WENO path (one
 // eigensystem, five projected cells) and of MUSCL-Hancock (ORDER 2, only in
 // the extended-option kernels) do not add up.
-template <class R, int ORDER, bool AMR, int DIR, bool EXT>
+template <class R, int ORDER, bool AMR, int DIR, int EXT>
 __device__ __forceinline__ void face_states(const Args3D &a, const Ctx3<R, AMR> &X, const double dt, const R dtn,
                                             const R hdtn, const R hdtx, const R hdty, const R hdtz, int i, int j,
                                             int k, R Wm_out[6], R Wp_out[6], R &gc_out, R &ge_out)
@@ -690,7 +690,7 @@ template <class R> struct PwSlots {
 #ifndef FXB_S3_MINB_FP64
 #define FXB_S3_MINB_FP64 2
 #endif
-template <class R, int ORDER, bool AMR, int DIR, bool EXT>
+template <class R, int ORDER, bool AMR, int DIR, int EXT>
 __device__ __forceinline__ void states3d_kernel_body(const Args3D &a, const VB vb)
 {
     constexpr int d = DIR;
@@ -712,7 +712,7 @@ __device__ __forceinline__ void states3d_kernel_body(const Args3D &a, const VB v
         for (int q = 0; q < 6; q++) { w[(long)q * nw + idx] = Wp[q]; w[(long)(6 + q) * nw + idx] = Wm[q]; }
     }
 }
-template <class R, int ORDER, bool AMR, int DIR, bool EXT>
+template <class R, int ORDER, bool AMR, int DIR, int EXT>
 __global__ void __launch_bounds__(256, FXB_S3_MINB_FP64) states3d_kernel(const Args3D a)
 {
     states3d_kernel_body<R, ORDER, AMR, DIR, EXT>(a, hw_block());
@@ -721,7 +721,7 @@ __global__ void __launch_bounds__(256, FXB_S3_MINB_FP64) states3d_kernel(const A
 // ---- Riemann fluxes of direction d ---------------------------------------------
 // the direction is a template parameter so that the solver's per-direction
 // indexing of the state vectors resolves at compile time (no local memory)
-template <class R, bool AMR, int DIR, bool EXT>
+template <class R, bool AMR, int DIR, int EXT>
 __device__ __forceinline__ void flux3d_kernel_body(const Args3D &a, const VB vb)
 {
     constexpr int d = DIR;
@@ -750,7 +750,7 @@ __device__ __forceinline__ void flux3d_kernel_body(const Args3D &a, const VB vb)
         for (int q = 0; q < NF; q++) f[(long)q * nf + idx] = F[q];
     }
 }
-template <class R, bool AMR, int DIR, bool EXT>
+template <class R, bool AMR, int DIR, int EXT>
 __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
 {
     flux3d_kernel_body<R, AMR, DIR, EXT>(a, hw_block());
@@ -770,7 +770,7 @@ __global__ void __launch_bounds__(256) flux3d_kernel(const Args3D a)
 template <class R> struct SfluxRegs {
     static constexpr int value = (65536 / ((sizeof(R) == 8 ? 2 : 3) * FXB_SF_MAXT)) / 8 * 8;
 };
-template <class R, int ORDER, bool AMR, int DIR, bool EXT>
+template <class R, int ORDER, bool AMR, int DIR, int EXT>
 __device__ __forceinline__ void sflux3d_kernel_body(const Args3D &a, const VB vb, unsigned char *sflux_smem, int nt)
 {
     constexpr int d = DIR;
@@ -879,7 +879,7 @@ __device__ __forceinline__ void sflux3d_kernel_body(const Args3D &a, const VB vb
         for (int q = 0; q < NF; q++) f[q * nf + fi] = F[q];
     }
 }
-template <class R, int ORDER, bool AMR, int DIR, bool EXT>
+template <class R, int ORDER, bool AMR, int DIR, int EXT>
 __global__ void __launch_bounds__(FXB_SF_MAXT) __maxnreg__(SfluxRegs<R>::value) sflux3d_kernel(const Args3D a)
 {
     extern __shared__ __align__(16) unsigned char sflux_smem[];
@@ -1021,30 +1021,32 @@ inline size_t f3d_bytes(int d, int nx, int ny, int nz, size_t rsz)
 
 // face states and fluxes of one direction (PPM: slopes first); g.x CTAs per
 // block for the grid-stride kernels, g.y batch entries
-template <class R, bool AMR, int DIR, bool EXT> void launch_states3d_rs(const Args3D &a, dim3 g, cudaStream_t s)
+template <class R, bool AMR, int DIR, int EXT> void launch_states3d_rs(const Args3D &a, dim3 g, cudaStream_t s)
 {
     if constexpr (EXT) {
         if (a.prm.order == 2) {   // MUSCL-Hancock: three cells per face state, no slope pass
             if constexpr (!FusedFaces<R>::value) {
-                states3d_kernel<R, 2, AMR, DIR, true><<<g, 256, 0, s>>>(a);
-                flux3d_kernel<R, AMR, DIR, true><<<dim3(a.cta[2], g.y), 256, 0, s>>>(a);
+                states3d_kernel<R, 2, AMR, DIR, 1><<<g, 256, 0, s>>>(a);
+                flux3d_kernel<R, AMR, DIR, EXT><<<dim3(a.cta[2], g.y), 256, 0, s>>>(a);
             } else {
                 const int N = DIR == 0 ? a.nx : DIR == 1 ? a.ny : a.nz;
                 const int N1 = DIR == 0 ? a.ny : a.nx, N2 = DIR == 2 ? a.ny : a.nz;
                 const int Ls = a.sf_len[DIR], T1 = a.sf_lines[DIR];
                 const int nseg = (N + Ls - 1) / (Ls - 1), nt1 = (N1 + T1 - 1) / T1;
                 const dim3 gs((unsigned)(nseg * nt1 * N2), g.y);
-                sflux3d_kernel<R, 2, AMR, DIR, true><<<gs, Ls * T1, 8 * sizeof(R) * (size_t)(Ls * T1), s>>>(a);
+                sflux3d_kernel<R, 2, AMR, DIR, EXT><<<gs, Ls * T1, 8 * sizeof(R) * (size_t)(Ls * T1), s>>>(a);
             }
             return;
         }
     }
     if constexpr (!FusedFaces<R>::value) {
+        // the face states hold no Riemann solve: EXT = 2 runs the EXT = 1 ones
+        constexpr int SX = EXT ? 1 : 0;
         if (a.prm.order == 5) {
-            states3d_kernel<R, 5, AMR, DIR, EXT><<<g, 256, 0, s>>>(a);
+            states3d_kernel<R, 5, AMR, DIR, SX><<<g, 256, 0, s>>>(a);
         } else {
             slope3d_kernel<R, AMR><<<g, 256, 0, s>>>(a, DIR);
-            states3d_kernel<R, 3, AMR, DIR, EXT><<<g, 256, 0, s>>>(a);
+            states3d_kernel<R, 3, AMR, DIR, SX><<<g, 256, 0, s>>>(a);
         }
         flux3d_kernel<R, AMR, DIR, EXT><<<dim3(a.cta[2], g.y), 256, 0, s>>>(a);
     } else {
@@ -1064,8 +1066,9 @@ template <class R, bool AMR, int DIR, bool EXT> void launch_states3d_rs(const Ar
 // the rarely used options (Roe, contact steepening, MUSCL-Hancock) have kernel instantiations of their own
 template <class R, bool AMR, int DIR> void launch_states3d(const Args3D &a, dim3 g, cudaStream_t s)
 {
-    if (extended_options(a.prm)) launch_states3d_rs<R, AMR, DIR, true>(a, g, s);
-    else launch_states3d_rs<R, AMR, DIR, false>(a, g, s);
+    if (marquina_solver(a.prm)) launch_states3d_rs<R, AMR, DIR, 2>(a, g, s);
+    else if (extended_options(a.prm)) launch_states3d_rs<R, AMR, DIR, 1>(a, g, s);
+    else launch_states3d_rs<R, AMR, DIR, 0>(a, g, s);
 }
 
 // slope cells a face-state tile adds per line: two when the FP32 kernel computes the PPM slopes itself

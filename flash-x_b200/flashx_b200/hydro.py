@@ -158,7 +158,8 @@ def make_fxb_params(hp: HydroParams, precision="fp64"):
     p = FxbParams()
     p.order = hp.order
     p.weno_method = 2 if hp.wenoMethod.upper() == "WENOZ" else 1
-    p.riemann = {"HLLC": 4, "HLL": 3, "LLF": 2, "ROE": 1}[hp.RiemannSolver.upper()]
+    p.riemann = {"HLLC": 4, "HLL": 3, "LLF": 2, "ROE": 1, "MARQUINA": 5,
+                 "MARQUINAMODIFIED": 7}[hp.RiemannSolver.upper()]
     p.limiter = {"minmod": 1, "mc": 2, "vanleer": 3, "hybrid": 4, "limited": 5}[hp.slopeLimiter.lower()]
     p.char_limiting = int(hp.charLimiting)
     p.use_3d_full_ctu = int(hp.use_3dFullCTU)

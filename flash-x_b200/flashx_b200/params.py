@@ -23,7 +23,7 @@ BC_NAMES = {"periodic": BC_PERIODIC, "outflow": BC_OUTFLOW, "reflect": BC_REFLEC
 class HydroParams:
     order: int = 3                      # 2 = MUSCL-Hancock, 3 = PPM, 5 = WENO
     wenoMethod: str = "WENO5"           # WENO5 | WENOZ
-    RiemannSolver: str = "HLLC"         # HLLC | HLL | LLF | Roe (entropy fix off)
+    RiemannSolver: str = "HLLC"         # HLLC | HLL | LLF | Roe | Marquina | MarquinaModified
     slopeLimiter: str = "mc"            # minmod | mc | vanLeer | hybrid | limited
     LimitedSlopeBeta: float = 1.0
     charLimiting: bool = True
@@ -63,8 +63,8 @@ class HydroParams:
         Hydro_init aborts on unknown choices."""
         if self.order not in (2, 3, 5):
             raise ValueError("order must be 2 (MUSCL-Hancock), 3 (PPM) or 5 (WENO)")
-        if self.RiemannSolver.upper() not in ("HLLC", "HLL", "LLF", "ROE"):
-            raise ValueError("RiemannSolver must be HLLC, HLL, LLF or Roe")
+        if self.RiemannSolver.upper() not in ("HLLC", "HLL", "LLF", "ROE", "MARQUINA", "MARQUINAMODIFIED"):
+            raise ValueError("RiemannSolver must be HLLC, HLL, LLF, Roe, Marquina or MarquinaModified")
         if self.slopeLimiter.lower() not in ("minmod", "mc", "vanleer", "hybrid", "limited"):
             raise ValueError("unknown slopeLimiter " + self.slopeLimiter)
         if self.wenoMethod.upper() not in ("WENO5", "WENOZ"):

@@ -58,7 +58,8 @@ enum fxb_precision { FXB_FP64 = 0, FXB_MIXED = 1 };   /* MIXED: FP32 reconstruct
 typedef struct fxb_params {
     int    order;              /* 2 = MUSCL-Hancock, 3 = PPM, 5 = WENO               */
     int    weno_method;        /* 1 = WENO5, 2 = WENOZ                               */
-    int    riemann;            /* 1 = Roe, 2 = LLF, 3 = HLL, 4 = HLLC (UHD.h)        */
+    int    riemann;            /* 1 = Roe, 2 = LLF, 3 = HLL, 4 = HLLC, 5 = Marquina,
+                                  7 = MarquinaModified (UHD.h)                      */
     int    limiter;            /* 1 minmod, 2 mc, 3 vanLeer, 4 hybrid, 5 limited     */
     int    char_limiting;      /* charLimiting                                       */
     int    use_3d_full_ctu;    /* use_3dFullCTU                                      */

@@ -621,12 +621,137 @@ static int riemann_roe(const fxo_params *p, int dir, const double *Vm, const dou
     return 0;
 }
 
+/* hy_eigenValue.F90 (hydro): u - c, u, u, u, u + c */
+static void eigen_values(double un, double cf, double lam[5])
+{
+    lam[0] = un - cf; lam[1] = un; lam[2] = un; lam[3] = un; lam[4] = un + cf;
+}
+
+/* hy_Marquina.F90:52-227 (hydro), restated as written: the eigenvalues and
+ * conservative eigenvectors (OnlyHydro/hy_eigenVector.F90, cons = .true.)
+ * of the left and of the right state; per wave k, where both states move
+ * the same way, the upwind state's characteristic flux, else half of each
+ * state's flux plus or minus the largest |eigenvalue| times its conserved
+ * state; the flux is the sum of both sides' parts along their right
+ * eigenvectors.  Two details of the reference are kept: the left
+ * eigenvectors, stored as leig(variable, wave), are read as leig(k, 1:5)
+ * (:165-183), and each projection adds leig(k, XMOM + dir - 1) times the
+ * face pressure to a momentum flux that already carries hy_fPresInMomFlux
+ * times the pressure (hy_prim2flx.F90).  The face-pressure slot is zero
+ * (:186). */
+static int riemann_marquina(const fxo_params *p, int dir, const double *Vm, const double *Vp, double Fs[6],
+                            double *speed)
+{
+    const double tiny = 1.e-32;
+    const double aL2 = Vm[H_GC] * Vm[H_P] / Vm[H_D];
+    const double aR2 = Vp[H_GC] * Vp[H_P] / Vp[H_D];
+    if ((Vm[H_D] < tiny && Vm[H_D] > 0.) || (Vp[H_D] < tiny && Vp[H_D] > 0.) ||
+        (Vm[H_P] < tiny && Vm[H_P] > 0.) || (Vp[H_P] < tiny && Vp[H_P] > 0.)) {
+        for (int k = 0; k < 6; k++) Fs[k] = 0.;
+        *speed = 0.;
+        return 0;
+    } else if (aL2 < 0. || aR2 < 0.) {
+        return 1;
+    }
+    if (aL2 <= 0. || aR2 <= 0.) return 1;      /* hy_eigenParameters aborts */
+    const double cL = sqrt(aL2), cR = sqrt(aR2);
+    double lamL[5], lamR[5], LL[5][5], RL[5][5], LR[5][5], RR[5][5];
+    eigen_values(Vm[H_VX + dir], cL, lamL);
+    cons_eigen(Vm, dir, cL, LL, RL);
+    eigen_values(Vp[H_VX + dir], cR, lamR);
+    cons_eigen(Vp, dir, cR, LR, RR);
+    double UL[5], UR[5], FL[6], FR[6];
+    prim2con(Vm, UL); prim2con(Vp, UR);
+    prim2flx(p, dir, Vm, FL); prim2flx(p, dir, Vp, FR);
+    *speed = fmax2(fabs(lamL[4]), fabs(lamR[4]));
+    double mL = fabs(lamL[0]), mR = fabs(lamR[0]);
+    for (int k = 1; k < 5; k++) {
+        if (fabs(lamL[k]) > mL) mL = fabs(lamL[k]);
+        if (fabs(lamR[k]) > mR) mR = fabs(lamR[k]);
+    }
+    const double amax = fmax2(mL, mR);
+    const int mom = 1 + dir;
+    double vecL[5], vecR[5];
+    for (int k = 0; k < 5; k++) {
+        double lf = 0., lu = 0., rf = 0., ru = 0.;   /* dot_product(leig(k, 1:5), .) */
+        for (int j = 0; j < 5; j++) {
+            lf = lf + LL[k][j] * FL[j]; lu = lu + LL[k][j] * UL[j];
+            rf = rf + LR[k][j] * FR[j]; ru = ru + LR[k][j] * UR[j];
+        }
+        if (lamL[k] * lamR[k] > 0.) {
+            if (lamL[k] > 0.) {
+                vecL[k] = lf + LL[k][mom] * FL[F_P];
+                vecR[k] = 0.;
+            } else {
+                vecL[k] = 0.;
+                vecR[k] = rf + LR[k][mom] * FR[F_P];
+            }
+        } else {
+            vecL[k] = 0.5 * (lf + amax * lu + LL[k][mom] * FL[F_P]);
+            vecR[k] = 0.5 * (rf - amax * ru + LR[k][mom] * FR[F_P]);
+        }
+    }
+    for (int v = 0; v < 5; v++) {
+        double fl = vecL[0] * RL[v][0], fr = vecR[0] * RR[v][0];
+        for (int w = 1; w < 5; w++) {
+            fl = fl + vecL[w] * RL[v][w];
+            fr = fr + vecR[w] * RR[v][w];
+        }
+        Fs[v] = fl + fr;
+    }
+    Fs[F_P] = 0.0;
+    return 0;
+}
+
+/* hy_MarquinaModified.F90:52-195 (hydro): per wave k the mean of the two
+ * states' |eigenvalues| times the jump of the wave's conserved part,
+ * r_R (l_R . U_R) - r_L (l_L . U_L), subtracted from the sum of the two
+ * fluxes and halved; the wave speed reported is |u| + c of the right state
+ * (the last hy_eigenParameters call). */
+static int riemann_marquina_mod(const fxo_params *p, int dir, const double *Vm, const double *Vp, double Fs[6],
+                                double *speed)
+{
+    const double tiny = 1.e-32;
+    const double aL2 = Vm[H_GC] * Vm[H_P] / Vm[H_D];
+    const double aR2 = Vp[H_GC] * Vp[H_P] / Vp[H_D];
+    if ((Vm[H_D] < tiny && Vm[H_D] > 0.) || (Vp[H_D] < tiny && Vp[H_D] > 0.) ||
+        (Vm[H_P] < tiny && Vm[H_P] > 0.) || (Vp[H_P] < tiny && Vp[H_P] > 0.)) {
+        for (int k = 0; k < 6; k++) Fs[k] = 0.;
+        *speed = 0.;
+        return 0;
+    } else if (aL2 < 0. || aR2 < 0.) {
+        return 1;
+    }
+    if (aL2 <= 0. || aR2 <= 0.) return 1;      /* hy_eigenParameters aborts */
+    const double cL = sqrt(aL2), cR = sqrt(aR2);
+    double lamL[5], lamR[5], LL[5][5], RL[5][5], LR[5][5], RR[5][5];
+    eigen_values(Vm[H_VX + dir], cL, lamL);
+    cons_eigen(Vm, dir, cL, LL, RL);
+    eigen_values(Vp[H_VX + dir], cR, lamR);
+    cons_eigen(Vp, dir, cR, LR, RR);
+    double UL[5], UR[5], FL[6], FR[6];
+    prim2con(Vm, UL); prim2con(Vp, UR);
+    prim2flx(p, dir, Vm, FL); prim2flx(p, dir, Vp, FR);
+    *speed = fabs(Vp[H_VX + dir]) + fabs(cR);
+    double sigF[6] = {0., 0., 0., 0., 0., 0.};
+    for (int k = 0; k < 5; k++) {
+        double dR = 0., dL = 0.;
+        for (int v = 0; v < 5; v++) { dR = dR + LR[v][k] * UR[v]; dL = dL + LL[v][k] * UL[v]; }
+        const double c = 0.5 * (fabs(lamL[k]) + fabs(lamR[k]));
+        for (int v = 0; v < 5; v++) sigF[v] = sigF[v] + c * (RR[v][k] * dR - RL[v][k] * dL);
+    }
+    for (int v = 0; v < 6; v++) Fs[v] = (FR[v] + FL[v] - sigF[v]) * 0.5;
+    return 0;
+}
+
 /* the Riemann solver of the runtime parameter RiemannSolver */
 static int riemann_solve(const fxo_params *p, int dir, const double *Vm, const double *Vp, double Fs[6], double *speed)
 {
     if (p->riemann == FXO_HLL) return riemann_hll(p, dir, Vm, Vp, Fs, speed);
     if (p->riemann == FXO_LLF) return riemann_llf(p, dir, Vm, Vp, Fs, speed);
     if (p->riemann == FXO_ROE) return riemann_roe(p, dir, Vm, Vp, Fs, speed);
+    if (p->riemann == FXO_MARQ) return riemann_marquina(p, dir, Vm, Vp, Fs, speed);
+    if (p->riemann == FXO_MARM) return riemann_marquina_mod(p, dir, Vm, Vp, Fs, speed);
     return riemann_hllc(p, dir, Vm, Vp, Fs, speed);
 }
 

@@ -30,7 +30,7 @@ enum { FXO_DENS = 0, FXO_EINT, FXO_ENER, FXO_GAMC, FXO_GAME, FXO_PRES,
        FXO_SHOK, FXO_TEMP, FXO_VELX, FXO_VELY, FXO_VELZ, FXO_NUNK };
 
 enum { FXO_BC_PERIODIC = 0, FXO_BC_OUTFLOW = 1, FXO_BC_REFLECTING = 2 };
-enum { FXO_ROE = 1, FXO_LLF = 2, FXO_HLL = 3, FXO_HLLC = 4 };   /* UHD.h:59-62 */
+enum { FXO_ROE = 1, FXO_LLF = 2, FXO_HLL = 3, FXO_HLLC = 4, FXO_MARQ = 5, FXO_MARM = 7 };   /* UHD.h:365-370 */
 enum { FXO_MINMOD = 1, FXO_MC = 2, FXO_VANLEER = 3, FXO_HYBRID = 4,
        FXO_LIMITED = 5 };
 
@@ -43,7 +43,7 @@ typedef struct {
     int bc[6];                      /* xl xr yl yr zl zr */
     int order;                      /* 2 = MUSCL-Hancock, 3 = PPM, 5 = WENO */
     int weno_method;                /* 1 = WENO5 (Jiang-Shu), 2 = WENO-Z */
-    int riemann;                    /* FXO_HLL / FXO_HLLC */
+    int riemann;                    /* FXO_ROE .. FXO_MARM */
     int limiter;                    /* FXO_MINMOD ... */
     int char_limiting;
     int use_3d_full_ctu;

@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(HERE, "libfx_oracle.so")
 NUNK = 11
 DENS, EINT, ENER, GAMC, GAME, PRES, SHOK, TEMP, VELX, VELY, VELZ = range(11)
 BC_PERIODIC, BC_OUTFLOW, BC_REFLECTING = 0, 1, 2
-ROE, LLF, HLL, HLLC = 1, 2, 3, 4
+ROE, LLF, HLL, HLLC, MARQ, MARM = 1, 2, 3, 4, 5, 7
 LIMITERS = {"minmod": 1, "mc": 2, "vanleer": 3, "hybrid": 4, "limited": 5}
 
 
@@ -110,7 +110,8 @@ def make_params(geom, hp):
         p.bc[i] = b
     p.order = hp.order
     p.weno_method = 2 if hp.wenoMethod.upper() == "WENOZ" else 1
-    p.riemann = {"HLLC": HLLC, "HLL": HLL, "LLF": LLF, "ROE": ROE}[hp.RiemannSolver.upper()]
+    p.riemann = {"HLLC": HLLC, "HLL": HLL, "LLF": LLF, "ROE": ROE, "MARQUINA": MARQ,
+                 "MARQUINAMODIFIED": MARM}[hp.RiemannSolver.upper()]
     p.limiter = LIMITERS[hp.slopeLimiter.lower()]
     p.char_limiting = int(hp.charLimiting)
     p.use_3d_full_ctu = int(hp.use_3dFullCTU)

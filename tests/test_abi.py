@@ -54,8 +54,10 @@ def test_init_validation_codes():
     assert lib.fxb_init(ctypes.byref(p), ctypes.byref(d), H.default_var_map(), 11) == H.FXB_EARG
     d.nguard = 4; p.order = 4
     assert lib.fxb_init(ctypes.byref(p), ctypes.byref(d), H.default_var_map(), 11) == H.FXB_EUNSUPPORTED
-    p.order = 3; p.riemann = 5
-    assert lib.fxb_init(ctypes.byref(p), ctypes.byref(d), H.default_var_map(), 11) == H.FXB_EUNSUPPORTED
+    p.order = 3
+    for bad in (6, 8):      # HLLD is MHD-only, the hybrid solver needs shock detection
+        p.riemann = bad
+        assert lib.fxb_init(ctypes.byref(p), ctypes.byref(d), H.default_var_map(), 11) == H.FXB_EUNSUPPORTED
     p.riemann = 4
     vm = H.default_var_map(); vm[0] = 11
     assert lib.fxb_init(ctypes.byref(p), ctypes.byref(d), vm, 11) == H.FXB_EARG
@@ -134,7 +136,9 @@ def test_parameter_validation_mirrors_hydro_init():
     HydroParams(use_steepening=True).validate()
     HydroParams(order=2).validate()
     HydroParams(use_upwindTVD=True, use_avisc=True).validate()
-    for bad in (dict(order=4), dict(order=6), dict(RiemannSolver="Marquina"), dict(entropyFixMethod="Einfeldt"),
+    HydroParams(RiemannSolver="Marquina").validate()
+    HydroParams(RiemannSolver="MarquinaModified").validate()
+    for bad in (dict(order=4), dict(order=6), dict(RiemannSolver="HLLD"), dict(entropyFixMethod="Einfeldt"),
                 dict(slopeLimiter="superbee"),
                 dict(transOrder=3),
                 dict(use_flattening=True, useGravity=True),

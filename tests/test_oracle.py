@@ -461,3 +461,114 @@ def test_species_oracle_transpose_symmetry(oracle):
     a = S.gather_global(geom, spec)
     b = S.gather_global(geom, st).transpose(0, 2, 1, 3)
     assert np.max(np.abs(a - b)) < 1e-13
+
+
+def _cons_eigenvectors(V, d):
+    """hy_eigenVector.F90 (OnlyHydro, cons = .true.) in numpy, stored as the
+    reference stores them: L[variable, wave], R[variable, wave]."""
+    rho, vel, p, ge = V[0], np.array(V[1:4]), V[4], V[6]
+    c = math.sqrt(V[5] * p / rho)
+    v1, v2, v3 = 1 + d, 1 + (d + 1) % 3, 1 + (d + 2) % 3
+    V1, V2, V3 = vel[d], vel[(d + 1) % 3], vel[(d + 2) % 3]
+    k = 1 - ge
+    na = 0.5 / c ** 2
+    u2 = 0.5 * np.dot(vel, vel)
+    H = (rho * u2 - p / k + p) / rho
+    L = np.zeros((5, 5))
+    Rm = np.zeros((5, 5))
+    L[[0, v1, v2, v3, 4], 0] = [na * (-k * u2 + V1 * c), -na * (-k * V1 + c), na * k * V2, na * k * V3, -na * k]
+    L[[0, v2], 1] = [-V2, 1]
+    L[[0, v1, v2, v3, 4], 2] = [1 + 2 * na * k * u2, -k * V1 / c ** 2, -k * V2 / c ** 2, -k * V3 / c ** 2, k / c ** 2]
+    L[[0, v3], 3] = [-V3, 1]
+    L[[0, v1, v2, v3, 4], 4] = [na * (-k * u2 - V1 * c), -na * (-k * V1 - c), na * k * V2, na * k * V3, -na * k]
+    Rm[[0, v1, v2, v3, 4], 0] = [1, V1 - c, V2, V3, H - V1 * c]
+    Rm[[v2, 4], 1] = [1, V2]
+    Rm[[0, v1, v2, v3, 4], 2] = [1, V1, V2, V3, u2]
+    Rm[[v3, 4], 3] = [1, V3]
+    Rm[[0, v1, v2, v3, 4], 4] = [1, V1 + c, V2, V3, H + V1 * c]
+    lam = np.array([vel[d] - c, vel[d], vel[d], vel[d], vel[d] + c])
+    return lam, L, Rm
+
+
+def _marquina_numpy(VL, VR, d, modified):
+    """hy_Marquina.F90:120-227 / hy_MarquinaModified.F90:120-195 line by line
+    in numpy, Fortran indices kept: leigL(k, 1:5) is L[k, :] (the row of
+    variable k across the waves, as the reference writes it)."""
+    lamL, LL, RL = _cons_eigenvectors(VL, d)
+    lamR, LR, RR = _cons_eigenvectors(VR, d)
+    UL, UR = _cons(VL)[:5], _cons(VR)[:5]
+    FL, FR = _phys_flux(VL, d), _phys_flux(VR, d)
+    F = np.zeros(6)
+    if modified:
+        sig = np.zeros(5)
+        for k in range(5):
+            sig += 0.5 * (abs(lamL[k]) + abs(lamR[k])) * (RR[:, k] * (LR[:, k] @ UR) - RL[:, k] * (LL[:, k] @ UL))
+        F[:5] = 0.5 * (FR[:5] + FL[:5] - sig)
+        F[5] = 0.5 * (FR[5] + FL[5])
+        return F
+    amax = max(np.max(np.abs(lamL)), np.max(np.abs(lamR)))
+    vL, vR = np.zeros(5), np.zeros(5)
+    for k in range(5):
+        if lamL[k] * lamR[k] > 0:
+            if lamL[k] > 0:
+                vL[k] = LL[k, :] @ FL[:5] + LL[k, 1 + d] * FL[5]
+            else:
+                vR[k] = LR[k, :] @ FR[:5] + LR[k, 1 + d] * FR[5]
+        else:
+            vL[k] = 0.5 * (LL[k, :] @ FL[:5] + amax * (LL[k, :] @ UL) + LL[k, 1 + d] * FL[5])
+            vR[k] = 0.5 * (LR[k, :] @ FR[:5] - amax * (LR[k, :] @ UR) + LR[k, 1 + d] * FR[5])
+    F[:5] = RL @ vL + RR @ vR
+    return F
+
+
+@pytest.mark.parametrize("solver", ["Marquina", "MarquinaModified"])
+def test_marquina_fluxes_follow_the_reference_lines(oracle, solver):
+    """The oracle's Marquina fluxes equal an independent numpy restatement of
+    the reference routines (both directions, subsonic and supersonic pairs,
+    waves of both signs) to rounding; MarquinaModified gives the physical
+    flux of identical states, Marquina as written does not (its transposed
+    left-eigenvector read and doubled face pressure make it inconsistent)."""
+    geom = Geometry(2, 16, 16, 1, 1, 1, 1)
+    p = oracle.make_params(geom.as_dict(), HydroParams(RiemannSolver=solver))
+    rng = np.random.default_rng(7)
+    for _ in range(40):
+        VL = _state(rng.uniform(0.2, 2), *rng.uniform(-3, 3, 3), rng.uniform(0.1, 3))
+        VR = _state(rng.uniform(0.2, 2), *rng.uniform(-3, 3, 3), rng.uniform(0.1, 3))
+        for d in range(3):
+            F = oracle.riemann(p, d, VL, VR)
+            want = _marquina_numpy(VL, VR, d, solver == "MarquinaModified")
+            assert np.allclose(F[:6], want, rtol=1e-11, atol=1e-11 * np.max(np.abs(want)))
+    V = _state(1.3, 0.2, -0.1, 0.05, 0.9)
+    F = oracle.riemann(p, 0, V, V)
+    if solver == "MarquinaModified":
+        assert np.array_equal(F[:6], _phys_flux(V, 0))
+    else:
+        assert not np.allclose(F[:5], _phys_flux(V, 0)[:5])
+        assert F[5] == 0.0
+    # vacuum guard and imaginary sound speed as the other solvers
+    assert np.all(oracle.riemann(p, 0, _state(1e-40, 0, 0, 0, 1.0), V)[:6] == 0.0)
+    bad = _state(1.0, 0, 0, 0, 1.0)
+    bad[5] = -1.4
+    with pytest.raises(RuntimeError):
+        oracle.riemann(p, 0, bad, V)
+
+
+def test_sod_2d_marquina_modified_matches_exact_solution(oracle):
+    """MarquinaModified with PPM on the 45-degree Sod problem, 128^2, t = 0.2:
+    the bounds of the HLLC test against the exact solution."""
+    geom = Geometry(2, 16, 16, 1, 8, 8, 1, bc=(BC_OUTFLOW,) * 6)
+    hp = HydroParams(RiemannSolver="MarquinaModified")
+    unk = S.sod(geom, hp)
+    t, n = run_oracle(oracle, geom, hp, unk, tmax=0.2)
+    assert abs(t - 0.2) < 1e-12 and n > 50
+    g = S.gather_global(geom, unk)[0]
+    N = g.shape[0]
+    idx = np.arange(N)
+    x = (idx + 0.5) / N
+    xi = (2 * x - 1.0) / math.sqrt(2.0) + 0.5
+    rho_ex, u_ex, p_ex = sod_exact(xi, 0.2)
+    keep = (xi > 0.05) & (xi < 0.95)
+    l1 = lambda a, b: np.mean(np.abs(a[keep] - b[keep]))
+    assert l1(g[idx, idx, DENS], rho_ex) < 0.01
+    assert l1(g[idx, idx, PRES], p_ex) < 0.01
+    assert l1((g[idx, idx, VELX] + g[idx, idx, VELY]) / math.sqrt(2.0), u_ex) < 0.02
