@@ -68,6 +68,8 @@ struct State {
     AmrEntry3 *d_entries = nullptr;               // [all][all, finer ones skipped][finer ones]
     int batch = 0;
     void *gcb = nullptr;                          // guard-filled blocks in the reconstruction type
+    int ngcb = NV_GCB;                            // their variables (NV_GCB, + total energy with avisc)
+    void *hyb = nullptr;                          // hybrid order: DivU [batch][(n+6)^3] of R, then flags [batch][(n+2)^3]
     void *sig = nullptr, *w[3] = {nullptr, nullptr, nullptr}, *f[3] = {nullptr, nullptr, nullptr};
     void *slp = nullptr;                          // PPM slopes of one direction per batch entry
     void *flat = nullptr;                         // flattening coefficients per batch entry
@@ -369,6 +371,7 @@ __global__ void __launch_bounds__(256, FXB_FILL_MINB) amr_fill_kernel(MeshArgs m
         } else {
 #pragma unroll
             for (int v = 0; v < NV_GCB; v++) dst[v * gvs + idx] = (T)u[v];
+            if (gbs > NV_GCB * gvs) dst[DV_ENER * gvs + idx] = (T)u[DV_ENER];   // blocks with total energy
         }
     }
 }
@@ -836,7 +839,7 @@ Args3D batch_args(const double *dtv, double dt)
     a.slp = S.slp;
     a.flat = S.flat;
     for (int d = 0; d < 3; d++) { a.wst[d] = S.w[d]; a.flx[d] = S.f[d]; }
-    a.gcb = S.gcb; a.gcb_vstride = ne3(); a.gcb_bstride = ne3() * NV_GCB; a.ng = S.ng;
+    a.gcb = S.gcb; a.gcb_vstride = ne3(); a.gcb_bstride = ne3() * S.ngcb; a.ng = S.ng;
     a.istore = S.store[S.cur];
     a.dxl = S.d_dxl;
     for (int q = 0; q < 4; q++) a.cta[q] = S.cta[q];
@@ -848,6 +851,13 @@ Args3D batch_args(const double *dtv, double dt)
     for (int d = 0; d < 3; d++) {
         a.w_bstride[d] = (long)(w3d_bytes(d, S.n, S.n, S.n, r) / r);
         a.f_bstride[d] = (long)(f3d_bytes(d, S.n, S.n, S.n, r) / r);
+    }
+    if (S.hyb) {
+        const long nd = (long)(S.n + 6) * (S.n + 6) * (S.n + 6);
+        a.divu = S.hyb;
+        a.divu_bstride = nd;
+        a.hyb = (const unsigned char *)S.hyb + r * nd * S.batch;
+        a.hyb_bstride = (long)(S.n + 2) * (S.n + 2) * (S.n + 2);
     }
     return a;
 }
@@ -868,11 +878,11 @@ template <class T> void fill_planned(const AmrEntry3 *entries, int cnt, int whic
 {
     const dim3 g(S.fill_cta, cnt);
     amr_copy_kernel<T><<<g, 256, 0, S.C.stream>>>(mesh_args(which), entries, S.leaf_blk_dev, (const GuardPlan *)S.d_plan,
-                                                  S.d_glist, S.nglist, (T *)S.gcb, ne3(), ne3() * NV_GCB, S.C.dprm,
+                                                  S.d_glist, S.nglist, (T *)S.gcb, ne3(), ne3() * S.ngcb, S.C.dprm,
                                                   S.C.gam1inv, S.C.ggprodinv);
     if (S.nprol)
         amr_prolong_kernel<T><<<g, 256, 0, S.C.stream>>>(mesh_args(which), entries, (const ProlRec *)S.d_prol, S.d_poff,
-                                                         (T *)S.gcb, ne3(), ne3() * NV_GCB, S.C.dprm, S.C.gam1inv,
+                                                         (T *)S.gcb, ne3(), ne3() * S.ngcb, S.C.dprm, S.C.gam1inv,
                                                          S.C.ggprodinv);
 }
 
@@ -904,12 +914,12 @@ int fill_batch(const AmrEntry3 *entries, int cnt, int which)
     }
     if (S.C.prm.precision == FXB_MIXED)
         amr_fill_kernel<float, false><<<g, 256, 0, S.C.stream>>>(mesh_args(which), entries, S.leaf_blk_dev, S.d_eosmask,
-                                                                (float *)S.gcb, ne3(), ne3() * NV_GCB, 0, nullptr,
+                                                                (float *)S.gcb, ne3(), ne3() * S.ngcb, 0, nullptr,
                                                                 S.d_glist, S.nglist, S.C.dprm, S.C.gam1inv,
                                                                 S.C.ggprodinv);
     else
         amr_fill_kernel<double, false><<<g, 256, 0, S.C.stream>>>(mesh_args(which), entries, S.leaf_blk_dev, S.d_eosmask,
-                                                                 (double *)S.gcb, ne3(), ne3() * NV_GCB, 0, nullptr,
+                                                                 (double *)S.gcb, ne3(), ne3() * S.ngcb, 0, nullptr,
                                                                  S.d_glist, S.nglist, S.C.dprm, S.C.gam1inv,
                                                                  S.C.ggprodinv);
     return 1;
@@ -1140,7 +1150,7 @@ void free_device(State &s)
     dfree(s.store[0]); dfree(s.store[1]);
     dfree(s.d_blk); dfree(s.d_ntab); dfree(s.d_child); dfree(s.d_plist); dfree(s.d_eosmask);
     dfree(s.d_finer); dfree(s.d_fine); dfree(s.d_dxl); dfree(s.d_entries); dfree(s.leaf_blk_dev);
-    dfree(s.gcb); dfree(s.sig); dfree(s.slp); dfree(s.flat);
+    dfree(s.gcb); dfree(s.sig); dfree(s.slp); dfree(s.flat); dfree(s.hyb);
     for (int d = 0; d < 3; d++) { dfree(s.w[d]); dfree(s.f[d]); }
     dfree(s.bflux); dfree(s.stage); dfree(s.d_dmap); dfree(s.d_pmap); dfree(s.d_glist);
     dfree(s.d_plan); dfree(s.d_prol); dfree(s.d_poff); dfree(s.d_rlist);
@@ -1165,13 +1175,12 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     if (D.ndim != 3) return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: AMR meshes are implemented for 3-D");
     if (D.nxb != D.nyb || D.nxb != D.nzb || D.nxb % 2 || D.nxb < D.nguard)
         return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: AMR blocks must be cubes of an even size >= NGUARD");
-    if (c.prm.use_avisc)
-        return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: artificial viscosity is implemented for uniform grids");
-    if (c.prm.hybrid_order)
-        return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: hybrid order is implemented for uniform grids");
     S.n = D.nxb;
     S.ng = D.nguard;
     S.nleaf = nleaf;
+    // artificial viscosity reads the total energy of the guard-filled blocks
+    // (the variable after EINT in the device order)
+    S.ngcb = c.prm.use_avisc ? DV_ENER + 1 : NV_GCB;
     std::vector<int> finer, fine;
     int rc = build_tree(leaves, nleaf, finer, fine);
     if (rc) { S = State(); return rc; }
@@ -1267,6 +1276,7 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
                 if (c.prm.flattening || depth1) need = in_box(o1) && in_box(o2);
                 else if (depth2) need = in_int(o1) && in_int(o2);
             }
+            if (c.prm.hybrid_order) need = true;     // DivU reads four cells out, edges and corners too
             if (need) gl.push_back(((k + g) * ne + (j + g)) * ne + (i + g));
         }
         S.nglist = (int)gl.size();
@@ -1321,11 +1331,13 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     S.stage_leaves = (int)std::max<size_t>(1, std::min<size_t>(nleaf, (1ull << 30) / per_unk));
     CKA(cudaMalloc(&S.stage, per_unk * S.stage_leaves));
     // batch of guard-filled blocks + pipeline intermediates: up to 60 % of what is free
-    const size_t per_entry = r * NV_GCB * ne3() + sig3d_bytes(S.n, S.n, S.n, r) +
+    const size_t per_entry = r * S.ngcb * ne3() + sig3d_bytes(S.n, S.n, S.n, r) +
                              w3d_bytes(0, S.n, S.n, S.n, r) + w3d_bytes(1, S.n, S.n, S.n, r) + w3d_bytes(2, S.n, S.n, S.n, r) +
                              f3d_bytes(0, S.n, S.n, S.n, r) + f3d_bytes(1, S.n, S.n, S.n, r) + f3d_bytes(2, S.n, S.n, S.n, r) +
                              (c.prm.order == 3 && r == 8 ? slp3d_bytes(S.n, S.n, S.n, r) : 0) +
-                             (c.prm.flattening ? r * 3 * (size_t)(S.n + 2) * (S.n + 2) * (S.n + 2) : 0);
+                             (c.prm.flattening ? r * 3 * (size_t)(S.n + 2) * (S.n + 2) * (S.n + 2) : 0) +
+                             (c.prm.hybrid_order ? r * (size_t)(S.n + 6) * (S.n + 6) * (S.n + 6) +
+                                                       (size_t)(S.n + 2) * (S.n + 2) * (S.n + 2) : 0);
     size_t fr = 0, tot = 0;
     CKA(cudaMemGetInfo(&fr, &tot));
     long cap = (long)((fr * 6 / 10) / per_entry);
@@ -1337,11 +1349,14 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
         long mb = atol(ev);
         if (mb >= 1) S.batch = (int)std::min<long>(S.batch, mb);
     }
-    CKA(cudaMalloc(&S.gcb, r * NV_GCB * ne3() * S.batch));
+    CKA(cudaMalloc(&S.gcb, r * S.ngcb * ne3() * S.batch));
     CKA(cudaMalloc(&S.sig, sig3d_bytes(S.n, S.n, S.n, r) * S.batch));
     // PPM slopes in memory: FP64 only (the FP32 face-state kernel computes them itself)
     if (c.prm.order == 3 && r == 8) CKA(cudaMalloc(&S.slp, slp3d_bytes(S.n, S.n, S.n, r) * S.batch));
     if (c.prm.flattening) CKA(cudaMalloc(&S.flat, r * 3 * (size_t)(S.n + 2) * (S.n + 2) * (S.n + 2) * S.batch));
+    if (c.prm.hybrid_order)
+        CKA(cudaMalloc(&S.hyb, (r * (size_t)(S.n + 6) * (S.n + 6) * (S.n + 6) + (size_t)(S.n + 2) * (S.n + 2) * (S.n + 2)) *
+                                   S.batch));
     for (int d = 0; d < 3; d++) {
         CKA(cudaMalloc(&S.w[d], w3d_bytes(d, S.n, S.n, S.n, r) * S.batch));
         CKA(cudaMalloc(&S.f[d], f3d_bytes(d, S.n, S.n, S.n, r) * S.batch));

@@ -30,8 +30,10 @@ struct MeshArgs {
 
 constexpr int ERR_AMR = 16;
 // variables of the guard-filled blocks: D..EI, all the 3-D pipeline reads
-// (ENER feeds the guard cells' Eos, TEMP nothing)
-constexpr int NV_GCB = EI + 1;     // guard cell without a covering block (device error word)
+// (ENER feeds the guard cells' Eos, TEMP nothing); artificial viscosity adds
+// ENER, the next variable
+constexpr int NV_GCB = EI + 1;
+static_assert(DV_ENER == NV_GCB, "total energy follows the guard-filled variables");     // guard cell without a covering block (device error word)
 
 
 // ------------------------------------------------------------------ device
@@ -228,6 +230,7 @@ __device__ __forceinline__ void amr_copy_kernel_body(const VB vb, MeshArgs m, co
     const long ncell = nint + nglist;
     T *dst = out + (long)vb.y * gbs;
     const GuardPlan *pl = plan + (long)e.leaf * nglist;
+    const bool wide = gbs > NV_GCB * gvs;   // blocks with total energy (artificial viscosity)
     for (int t = (int)(vb.x * blockDim.x + threadIdx.x); t < (int)ncell; t += (int)(vb.nx * blockDim.x)) {
         double u[NV_DEV];
         int idx;
@@ -238,6 +241,7 @@ __device__ __forceinline__ void amr_copy_kernel_body(const VB vb, MeshArgs m, co
             const double *s = m.store + (long)b * m.bstride + t;
 #pragma unroll
             for (int v = 0; v < NV_GCB; v++) u[v] = s[v * m.vstride];
+            if (wide) u[DV_ENER] = s[DV_ENER * m.vstride];
         } else {
             const GuardPlan gp = pl[t - nint];
             const unsigned kind = (gp.flags >> 4) & 3u;
@@ -252,10 +256,12 @@ __device__ __forceinline__ void amr_copy_kernel_body(const VB vb, MeshArgs m, co
                 eos_cell_dev(u, prm, gam1inv, ggprodinv);
             } else {
                 guard_eval_same<NV_GCB>(m.store, m.vstride, gp.off, gp.flags & 7u, u);
+                if (wide) u[DV_ENER] = m.store[gp.off + DV_ENER * m.vstride];
             }
         }
 #pragma unroll
         for (int v = 0; v < NV_GCB; v++) dst[v * gvs + idx] = (T)u[v];
+        if (wide) dst[DV_ENER * gvs + idx] = (T)u[DV_ENER];
     }
 }
 template <class T>
@@ -275,6 +281,7 @@ __device__ __forceinline__ void amr_prolong_kernel_body(const VB vb, MeshArgs m,
         const long idx = a.x;
 #pragma unroll
         for (int v = 0; v < NV_GCB; v++) dst[v * gvs + idx] = (T)u[v];
+        if (gbs > NV_GCB * gvs) dst[DV_ENER * gvs + idx] = (T)u[DV_ENER];
     }
 }
 

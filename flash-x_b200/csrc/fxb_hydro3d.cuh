@@ -81,7 +81,10 @@ struct Args3D {
     FastDiv fdx[5], fdy[5];     // divisors nx + e and ny + e (e = 0, 1, 2, 4), set by the launchers
     int sf_len[3], sf_lines[3]; // face-state tiles per direction (cells along d, lines), set by the launchers
     int sf_t1[3] = {0, 0, 0};   // lines per face-state tile chosen by the tuner (0: the launchers' choice)
-    const unsigned char *hyb;   // hybrid order (uniform grid): 1 where min DivU over the cell's box < eps, padded box
+    const unsigned char *hyb;   // hybrid order: 1 where min DivU over the cell's box < eps, padded box (AMR: per entry)
+    long hyb_bstride = 0;       // AMR: flags per batch entry
+    void *divu = nullptr;       // AMR: DivU scratch per batch entry, box [-3, n+2]^3 of R
+    long divu_bstride = 0;
     long rate_c0 = 0, rate_c1 = 0x7fffffffffffffffL;   // cells [c0, c1) enter the CFL rate (a slab's own)
     unsigned char *ctufb[3] = {nullptr, nullptr, nullptr};   // species on: 1 where the CTU fallback fired (Grid3::widx)
 };
@@ -199,12 +202,14 @@ template <class R, bool AMR> struct Ctx3 {
     R *sig, *wst[3], *flx[3], *slp, *flat;
     double dx, dy, dz;
     AmrEntry3 m;
+    const unsigned char *hyb;   // hybrid-order flags of the padded box
     __device__ Ctx3(const Args3D &a, int by)
     {
         G = Grid3{a.nx, a.ny, a.nz};
         if constexpr (AMR) {
             const int bb = by;
             m = a.batch[bb];
+            hyb = a.hyb ? a.hyb + (long)bb * a.hyb_bstride : nullptr;
             src = nullptr;
             srcR = (const R *)a.gcb + (long)bb * a.gcb_bstride;
             svs = a.gcb_vstride;
@@ -219,6 +224,7 @@ template <class R, bool AMR> struct Ctx3 {
             dx = a.dxl[3 * (m.level - 1)]; dy = a.dxl[3 * (m.level - 1) + 1]; dz = a.dxl[3 * (m.level - 1) + 2];
         } else {
             m = AmrEntry3{0, 1, 0, 0};
+            hyb = a.hyb;
             src = a.in; srcR = nullptr; svs = a.vstride; so = 0; sx = a.nx; sy = a.ny;
             sig = (R *)a.sig;
             slp = (R *)a.slp;
@@ -262,6 +268,9 @@ template <class R, bool AMR> struct Ctx3 {
     // offset of interior cell (i,j,k) in the source arrays
     __device__ __forceinline__ long cell(int i, int j, int k) const
     { return ((long)(k + so) * sy + (j + so)) * sx + (i + so); }
+    // variable q of cell (i,j,k): the uniform grid's state (boundaries
+    // mapped, rounded to R), or the AMR leaf's guard-filled block
+    __device__ __forceinline__ R var(const Args3D &a, int q, int i, int j, int k) const;
 };
 
 template <class R> __device__ __forceinline__ void six(const R v[8], R g[6])
@@ -300,15 +309,23 @@ __device__ __forceinline__ R state_var(const Args3D &a, int q, int i, int j, int
     return (R)x;
 }
 
+template <class R, bool AMR>
+__device__ __forceinline__ R Ctx3<R, AMR>::var(const Args3D &a, int q, int i, int j, int k) const
+{
+    if constexpr (AMR) return __ldg(srcR + q * svs + cell(i, j, k));
+    else return state_var<R>(a, q, i, j, k);
+}
+
 // artificial viscosity of the direction-d face between cells (i,j,k) - e_d
-// and (i,j,k) of the uniform grid (AMR meshes do not take the option)
-template <class R>
-__device__ __forceinline__ void avisc3d(const Args3D &a, int d, int i, int j, int k, R F[])
+// and (i,j,k), on the uniform grid or an AMR leaf (whose guard-filled block
+// then carries the total energy)
+template <class R, bool AMR>
+__device__ __forceinline__ void avisc3d(const Args3D &a, const Ctx3<R, AMR> &X, int d, int i, int j, int k, R F[])
 {
     int di, dj, dk;
     offs(d, 1, di, dj, dk);
     const int im = i - di, jm = j - dj, km = k - dk;
-    const R del[3] = {R(a.dx), R(a.dy), R(a.dz)};
+    const R del[3] = {R(X.dx), R(X.dy), R(X.dz)};
     R tr[3] = {R(0.), R(0.), R(0.)};
 #pragma unroll
     for (int e = 0; e < 3; e++) {
@@ -316,14 +333,14 @@ __device__ __forceinline__ void avisc3d(const Args3D &a, int d, int i, int j, in
         int ie, je, ke;
         offs(e, 1, ie, je, ke);
         const int v = VX + e;
-        tr[e] = R(0.25) * (state_var<R>(a, v, i + ie, j + je, k + ke) - state_var<R>(a, v, i - ie, j - je, k - ke) +
-                           state_var<R>(a, v, im + ie, jm + je, km + ke) - state_var<R>(a, v, im - ie, jm - je, km - ke)) *
+        tr[e] = R(0.25) * (X.var(a, v, i + ie, j + je, k + ke) - X.var(a, v, i - ie, j - je, k - ke) +
+                           X.var(a, v, im + ie, jm + je, km + ke) - X.var(a, v, im - ie, jm - je, km - ke)) *
                 del[d] / del[e];
     }
-    const R Ul[5] = {state_var<R>(a, D, im, jm, km), state_var<R>(a, VX, im, jm, km), state_var<R>(a, VY, im, jm, km),
-                     state_var<R>(a, VZ, im, jm, km), state_var<R>(a, DV_ENER, im, jm, km)};
-    const R Ur[5] = {state_var<R>(a, D, i, j, k), state_var<R>(a, VX, i, j, k), state_var<R>(a, VY, i, j, k),
-                     state_var<R>(a, VZ, i, j, k), state_var<R>(a, DV_ENER, i, j, k)};
+    const R Ul[5] = {X.var(a, D, im, jm, km), X.var(a, VX, im, jm, km), X.var(a, VY, im, jm, km),
+                     X.var(a, VZ, im, jm, km), X.var(a, DV_ENER, im, jm, km)};
+    const R Ur[5] = {X.var(a, D, i, j, k), X.var(a, VX, i, j, k), X.var(a, VY, i, j, k), X.var(a, VZ, i, j, k),
+                     X.var(a, DV_ENER, i, j, k)};
     avisc_flux(R(a.prm.cvisc), d, 3, Ul[1 + d], Ur[1 + d], tr, Ul, Ur, F);
 }
 
@@ -574,15 +591,13 @@ __device__ __forceinline__ void face_states_finish(const Args3D &a, const Ctx3<R
 // hybrid order on the traced states wm, wp (sweep frame) of a uniform-grid
 // cell whose flag (hyb3d_kernel) is set
 template <class R, bool AMR>
-__device__ __forceinline__ void hybrid3d(const Args3D &a, const Grid3 &G, int i, int j, int k, const R vc[8],
+__device__ __forceinline__ void hybrid3d(const Args3D &a, const Ctx3<R, AMR> &X, int i, int j, int k, const R vc[8],
                                          const R Sc[6], R wm[6], R wp[6])
 {
-    if constexpr (!AMR) {
-        if (a.prm.use_hybrid && a.hyb[G.pidx(i, j, k)]) {
-            R g[6];
-            six(vc, g);
-            hybrid_rh(3, g, Sc, vc[GC], wm, wp);
-        }
+    if (a.prm.use_hybrid && X.hyb[X.G.pidx(i, j, k)]) {
+        R g[6];
+        six(vc, g);
+        hybrid_rh(3, g, Sc, vc[GC], wm, wp);
     }
 }
 
@@ -600,7 +615,7 @@ __device__ __forceinline__ void face_states_tail(const Args3D &a, const Ctx3<R, 
     if (a.prm.flattening) flatten(X.flat[(long)d * G.npad() + G.pidx(i, j, k)], Sc, vecL, vecR);
     R wm[6], wp[6];
     ppm_trace(e, dtn, hdtn, Sc, vecL, vecR, wm, wp);
-    if constexpr (EXT) hybrid3d<R, AMR>(a, G, i, j, k, vc, Sc, wm, wp);
+    if constexpr (EXT) hybrid3d<R, AMR>(a, X, i, j, k, vc, Sc, wm, wp);
     face_states_finish<R, AMR, DIR, EXT>(a, X, dt, hdtx, hdty, hdtz, i, j, k, vc, eb, wm, wp, Wm_out, Wp_out);
 }
 
@@ -635,7 +650,7 @@ __device__ __forceinline__ void face_states(const Args3D &a, const Ctx3<R, AMR> 
         const R F = a.prm.flattening ? X.flat[(long)d * G.npad() + G.pidx(i, j, k)] : R(0.);
         R wm[6], wp[6];
         mh_trace(a.prm, e, dtn, hdtn, S[1], S[2], S[3], F, wm, wp);
-        hybrid3d<R, AMR>(a, G, i, j, k, vc, S[2], wm, wp);
+        hybrid3d<R, AMR>(a, X, i, j, k, vc, S[2], wm, wp);
         face_states_finish<R, AMR, DIR, EXT>(a, X, dt, hdtx, hdty, hdtz, i, j, k, vc, eb, wm, wp, Wm_out, Wp_out);
         gc_out = vc[GC]; ge_out = vc[GE];
         return;
@@ -743,8 +758,8 @@ __device__ __forceinline__ void flux3d_kernel_body(const Args3D &a, const VB vb)
         X.load_gammas(a, i, j, k, gcr, ger);
         int e = riemann<R, EXT>(a.prm, d, VL, gcl, gel, VR, gcr, ger, F);
         if (e) atomicOr(a.err, e);
-        if constexpr (EXT && !AMR) {
-            if (a.prm.use_avisc) { avisc3d<R>(a, d, i, j, k, F); eint_fluxes(a.prm, VL, VR, F); }
+        if constexpr (EXT) {
+            if (a.prm.use_avisc) { avisc3d<R, AMR>(a, X, d, i, j, k, F); eint_fluxes(a.prm, VL, VR, F); }
         }
 #pragma unroll
         for (int q = 0; q < NF; q++) f[(long)q * nf + idx] = F[q];
@@ -870,8 +885,8 @@ __device__ __forceinline__ void sflux3d_kernel_body(const Args3D &a, const VB vb
         for (int q = 0; q < 6; q++) VL[q] = sW[q * nt + tl];
         const int e = riemann<R, EXT>(a.prm, d, VL, sW[6 * nt + tl], sW[7 * nt + tl], Wm, gc, ge, F);
         if (e) atomicOr(a.err, e);
-        if constexpr (EXT && !AMR) {
-            if (a.prm.use_avisc) { avisc3d<R>(a, d, i, j, k, F); eint_fluxes(a.prm, VL, Wm, F); }
+        if constexpr (EXT) {
+            if (a.prm.use_avisc) { avisc3d<R, AMR>(a, X, d, i, j, k, F); eint_fluxes(a.prm, VL, Wm, F); }
         }
         R *f = X.flx[d];
         const long nf = G.nf(d), fi = G.fidx(d, i, j, k);
@@ -1074,33 +1089,39 @@ template <class R, bool AMR, int DIR> void launch_states3d(const Args3D &a, dim3
 // slope cells a face-state tile adds per line: two when the FP32 kernel computes the PPM slopes itself
 template <class R> int sflux_halo(const Args3D &a) { return (FusedFaces<R>::value && a.prm.order == 3) ? 2 : 0; }
 
-// hybrid order, uniform grid: DivU (hy_getRiemannState.F90:341-360) on
-// [-3, n+2]^3, stored with offset 3
-template <class R>
-__global__ void __launch_bounds__(256) divu3d_kernel(const Args3D a, R *divu)
+// hybrid order: DivU (hy_getRiemannState.F90:341-360) on [-3, n+2]^3,
+// stored with offset 3 (AMR: per batch entry y, from the guard-filled block)
+template <class R, bool AMR>
+__global__ void __launch_bounds__(256) divu3d_kernel(const Args3D a, R *divu_base)
 {
+    const VB vb = hw_block();
+    const Ctx3<R, AMR> X(a, vb.y);
+    R *divu = divu_base + (AMR ? (long)vb.y * a.divu_bstride : 0L);
     const long ex = a.nx + 6, ey = a.ny + 6, n = ex * ey * (a.nz + 6);
-    FXB_GRID_LOOP(idx, n) {
+    for (long idx = (long)vb.x * blockDim.x + threadIdx.x; idx < n; idx += (long)vb.nx * blockDim.x) {
         const int i = (int)(idx % ex) - 3, j = (int)((idx / ex) % ey) - 3, k = (int)(idx / (ex * ey)) - 3;
-        R dv = state_var<R>(a, VX, i + 1, j, k) - state_var<R>(a, VX, i - 1, j, k);
-        dv = dv + state_var<R>(a, VY, i, j + 1, k) - state_var<R>(a, VY, i, j - 1, k);
-        dv = dv + state_var<R>(a, VZ, i, j, k + 1) - state_var<R>(a, VZ, i, j, k - 1);
+        R dv = X.var(a, VX, i + 1, j, k) - X.var(a, VX, i - 1, j, k);
+        dv = dv + X.var(a, VY, i, j + 1, k) - X.var(a, VY, i, j - 1, k);
+        dv = dv + X.var(a, VZ, i, j, k + 1) - X.var(a, VZ, i, j, k - 1);
         divu[idx] = R(0.5) * dv;
     }
 }
 // the flag of every cell of the padded box [-1, n]^3: min DivU over the
 // cell's (2 k4 + 1)^3 box below hybridOrderKappa times its sound speed
-template <class R>
-__global__ void __launch_bounds__(256) hyb3d_kernel(const Args3D a, const R *divu, unsigned char *flag)
+template <class R, bool AMR>
+__global__ void __launch_bounds__(256) hyb3d_kernel(const Args3D a, const R *divu_base, unsigned char *flag_base)
 {
+    const VB vb = hw_block();
+    const Ctx3<R, AMR> X(a, vb.y);
+    const R *divu = divu_base + (AMR ? (long)vb.y * a.divu_bstride : 0L);
+    unsigned char *flag = flag_base + (AMR ? (long)vb.y * a.hyb_bstride : 0L);
     const Grid3 G{a.nx, a.ny, a.nz};
     const long ex = a.nx + 6, ey = a.ny + 6, np = G.npad();
     const int k4 = a.prm.order - 1 > 2 ? 2 : a.prm.order - 1;
-    FXB_GRID_LOOP(idx, np) {
+    for (long idx = (long)vb.x * blockDim.x + threadIdx.x; idx < np; idx += (long)vb.nx * blockDim.x) {
         const int i = (int)(idx % (a.nx + 2)) - 1, j = (int)((idx / (a.nx + 2)) % (a.ny + 2)) - 1,
                   k = (int)(idx / ((long)(a.nx + 2) * (a.ny + 2))) - 1;
-        const R eps = hybrid_eps(a.prm, state_var<R>(a, D, i, j, k), state_var<R>(a, P, i, j, k),
-                                 state_var<R>(a, GC, i, j, k));
+        const R eps = hybrid_eps(a.prm, X.var(a, D, i, j, k), X.var(a, P, i, j, k), X.var(a, GC, i, j, k));
         R mn = divu[((long)(k - k4 + 3) * ey + (j - k4 + 3)) * ex + (i - k4 + 3)];
         for (int kk = -k4; kk <= k4; kk++)
             for (int jj = -k4; jj <= k4; jj++)
@@ -1123,8 +1144,8 @@ template <class R> void launch_hydro3d_t(const Args3D &a0, cudaStream_t s)
     if (a.prm.use_hybrid) {
         R *divu = (R *)a.hyb;
         unsigned char *flag = (unsigned char *)a.hyb + sizeof(R) * (size_t)(a.nx + 6) * (a.ny + 6) * (a.nz + 6);
-        divu3d_kernel<R><<<nsig, 256, 0, s>>>(a, divu);
-        hyb3d_kernel<R><<<nsig, 256, 0, s>>>(a, divu, flag);
+        divu3d_kernel<R, false><<<nsig, 256, 0, s>>>(a, divu);
+        hyb3d_kernel<R, false><<<nsig, 256, 0, s>>>(a, divu, flag);
         Args3D b = a;
         b.hyb = flag;
         if (a.prm.flattening) flat3d_kernel<R, false><<<nsig, 256, 0, s>>>(b);
@@ -1225,6 +1246,11 @@ __global__ void __launch_bounds__(256) amr_correct_flux_kernel(const Args3D a, c
 template <class R> void launch_amr3d_fluxes_t(const Args3D &a0, int entries, int which, cudaStream_t s)
 {
     const Args3D a = with_divisors(a0, sflux_halo<R>(a0));
+    if ((which & AMR_SIG) && a.prm.use_hybrid) {
+        divu3d_kernel<R, true><<<dim3(a.cta[0], entries), 256, 0, s>>>(a, (R *)a.divu);
+        hyb3d_kernel<R, true><<<dim3(a.cta[0], entries), 256, 0, s>>>(a, (const R *)a.divu,
+                                                                       const_cast<unsigned char *>(a.hyb));
+    }
     if ((which & AMR_SIG) && a.prm.flattening) flat3d_kernel<R, true><<<dim3(a.cta[0], entries), 256, 0, s>>>(a);
     if (which & AMR_SIG) sig3d_kernel<R, true><<<dim3(a.cta[0], entries), 256, 0, s>>>(a);
     if (which & AMR_STATES) {

@@ -35,9 +35,9 @@ class HydroParams:
     entropyFixMethod: str = "HartenHyman"   # HartenHyman | Harten
     use_steepening: bool = False
     use_upwindTVD: bool = False         # off with NGUARD <= 4 (unsplit/Hydro_init.F90:137)
-    use_avisc: bool = False             # artificial viscosity (uniform grids)
+    use_avisc: bool = False             # artificial viscosity
     cvisc: float = 0.1
-    use_hybridOrder: bool = False       # first-order states at shocks (uniform grids)
+    use_hybridOrder: bool = False       # first-order states at shocks
     hybridOrderKappa: float = 0.0
     hydroComputeDtOption: int = -1
     cfl: float = 0.8

@@ -75,12 +75,12 @@ typedef struct fxb_params {
     int    entropy_fix;        /* Roe: entropy = .false. (0), entropyFixMethod
                                   HartenHyman (1) or Harten (2)                     */
     int    steepening;         /* use_steepening: PPM contact steepening            */
-    int    use_avisc;          /* use_avisc: artificial viscosity (uniform grids)    */
+    int    use_avisc;          /* use_avisc: artificial viscosity                    */
     double cvisc;              /* cvisc: its constant (Config default 0.1)           */
     int    upwind_tvd;         /* use_upwindTVD: off when NGUARD <= 4, as
                                   unsplit/Hydro_init.F90:137 resets it; rejected
                                   (FXB_EUNSUPPORTED) with more guard cells        */
-    int    hybrid_order;       /* use_hybridOrder (uniform grids)                    */
+    int    hybrid_order;       /* use_hybridOrder                                    */
     double hybrid_kappa;       /* hybridOrderKappa (Config default 0)                */
 } fxb_params;
 
@@ -165,8 +165,8 @@ int fxb_init_species(int nspec, int nspecies, const int32_t *unk_slots);
  * other levels and corrects the fluxes on fine/coarse faces
  * (Paramesh4/Grid_fillGuardCells.F90:446-541, levelFlux/Hydro.F90:161-270,
  * levelFlux/Grid_conserveFluxes.F90).  Errors: FXB_EARG for a list that does
- * not tile the domain or is not balanced, FXB_EUNSUPPORTED for 2-D AMR,
- * non-cubic blocks, artificial viscosity or hybrid order on AMR meshes. */
+ * not tile the domain or is not balanced, FXB_EUNSUPPORTED for 2-D AMR and
+ * non-cubic blocks. */
 int fxb_register_blocks(const fxb_block_desc *blocks, int nblk);
 /* Copy the host UNK (all blocks, guard cells included) into the device mirror. */
 int fxb_attach_unk(const double *unk_host);

@@ -372,17 +372,52 @@ def test_regrid_rejects_two_levels_and_keeps_the_mesh(oracle, need_gpu):
     dev.close()
 
 
-def test_amr_rejects_artificial_viscosity(need_gpu):
-    root, hp, mesh, unk = _case((BC_PERIODIC,) * 6, 2, order=3)
-    hp.use_avisc = True
-    with pytest.raises(FlashXError) as e:
-        HydroDevice(root, hp, "fp64", mesh=mesh)
-    assert e.value.code == 6
+def _rough_gas(X, Y, Z):
+    """Density varying by e^1.2 from cell to cell, velocities of order one, p = 1."""
+    rho = np.exp(1.2 * np.sin(311.0 * X + 17.0 * Y) * np.cos(173.0 * Y - 29.0 * Z + 3.0 * X))
+    vx, vy, vz = np.sin(251.0 * Y + 7.0 * Z), np.cos(199.0 * Z - 11.0 * X), np.sin(277.0 * X + 5.0 * Y)
+    return rho, vx, vy, vz, np.ones_like(rho)
 
 
-def test_amr_rejects_hybrid_order(need_gpu):
-    root, hp, mesh, unk = _case((BC_PERIODIC,) * 6, 2, order=3)
-    hp.use_hybridOrder = True
-    with pytest.raises(FlashXError) as e:
-        HydroDevice(root, hp, "fp64", mesh=mesh)
-    assert e.value.code == 6
+@pytest.mark.parametrize("opts,order,bc", [
+    (dict(use_avisc=True), 3, (BC_PERIODIC,) * 6),
+    (dict(use_avisc=True, cvisc=0.3), 5, (BC_OUTFLOW, BC_OUTFLOW, BC_PERIODIC, BC_PERIODIC, BC_REFLECTING,
+                                          BC_REFLECTING)),
+    (dict(use_hybridOrder=True), 3, (BC_PERIODIC,) * 6),
+    (dict(use_hybridOrder=True, hybridOrderKappa=0.05), 5, (BC_REFLECTING,) * 6),
+    (dict(use_hybridOrder=True, use_avisc=True), 2, (BC_PERIODIC,) * 6),
+])
+def test_amr_avisc_and_hybrid_order_match_oracle(oracle, need_gpu, opts, order, bc):
+    """Artificial viscosity (the guard-filled blocks then carry the total
+    energy) and hybrid order (DivU and flags per leaf from a guard fill of
+    every guard cell) on a two-level mesh, FP64 bit for bit, two steps; the
+    options change the solution."""
+    hyb = opts.get("use_hybridOrder", False)
+    hp = HydroParams(order=order, gamma=3.0 if hyb else 1.4, **opts)
+    root = Geometry(3, 8, 8, 8, 4, 4, 4, bc=bc)
+    mesh, unk = A.levelset_problem(root, hp, 2)
+    if hyb:     # steep converging cells, where face states break the shock density bounds
+        unk = A.fill_leaves(mesh, hp, _rough_gas)
+    am = oracle.Amr(oracle.make_params(root.as_dict(), hp), mesh.levels, mesh.bcoords)
+    dt = 0.5 * am.compute_dt(unk)
+    _, ref = _oracle(oracle, root, hp, mesh, unk, [dt, dt])
+    dev, out = _gpu(root, hp, mesh, unk, [dt, dt])
+    g, r = _interior(root, out), _interior(root, ref)
+    assert np.max(np.abs(g - r) / np.maximum(np.abs(r), 1e-300)) <= REL_TOL_ONE_STEP
+    assert np.array_equal(g, r)
+    dev.close()
+    _, plain = _oracle(oracle, root, HydroParams(order=order, gamma=hp.gamma), mesh, unk, [dt, dt])
+    assert not np.array_equal(r, _interior(root, plain))
+
+
+def test_amr_avisc_mixed_close_to_fp64(need_gpu):
+    root, hp, mesh, unk = _case(maxlev=2)
+    hp = HydroParams(order=5, use_avisc=True, use_hybridOrder=True)
+    dev = HydroDevice(root, hp, "fp64", mesh=mesh)
+    dev.attach_unk(unk.copy())
+    dt = 0.5 * dev.Hydro_computeDt()
+    dev.close()
+    _, a = _gpu(root, hp, mesh, unk, [dt] * 5, "mixed")
+    _, b = _gpu(root, hp, mesh, unk, [dt] * 5)
+    x, y = _interior(root, a)[..., 0], _interior(root, b)[..., 0]
+    assert np.mean(np.abs(x - y)) / np.mean(np.abs(y)) <= L1_TOL_MIXED
