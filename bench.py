@@ -105,6 +105,10 @@ def parse():
     ap.add_argument("--sweep", action="store_true",
                     help="throughput sweep of the batched-block path: one JSON line per (block size, count, "
                          "reconstruction, precision)")
+    ap.add_argument("--sweep-blocks", type=int, nargs="+", default=[8, 16, 32],
+                    help="block sizes (cells per side) the sweep covers")
+    ap.add_argument("--sweep-min-blocks", type=int, default=0,
+                    help="skip sweep points with fewer blocks")
     return ap.parse_args()
 
 
@@ -650,11 +654,25 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def sweep_points(hbm_bytes, host_limit=12e9):
+def host_available():
+    """Bytes of host memory available now (MemAvailable), 12 GB if unknown."""
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 12e9
+
+
+def sweep_points(hbm_bytes, host_limit=None, blocks=(8, 16, 32)):
     """(n, nb) pairs: blocks of n^3 interior cells, (2 nb)^3 leaves at level 2,
-    capped by the host UNK copy (guard cells included) and by device memory."""
+    capped by the host UNK (guard cells included; at most 45 % of the host
+    memory available) and by device memory."""
+    host_limit = 0.45 * host_available() if host_limit is None else host_limit
     pts = []
-    for n in (8, 16, 32):
+    for n in blocks:
         for nb in (2, 4, 8, 16, 29):
             count = (2 * nb) ** 3
             unk_bytes = count * (n + 8) ** 3 * 11 * 8
@@ -677,15 +695,17 @@ def run_sweep(args):
     torch.cuda.set_device(0)
     peak, peak_kind = measured_peaks()
     hbm = torch.cuda.get_device_properties(0).total_memory
-    for n, nb in sweep_points(hbm):
+    for n, nb in sweep_points(hbm, blocks=args.sweep_blocks):
+        if (2 * nb) ** 3 < args.sweep_min_blocks:
+            continue
         root = Geometry(3, n, n, n, nb, nb, nb, bc=(BC_PERIODIC,) * 6)
         fine = Geometry(3, n, n, n, 2 * nb, 2 * nb, 2 * nb, bc=(BC_PERIODIC,) * 6)
-        mesh = A.build_mesh(root, 2, lambda l, c, g: True)
+        # every block a leaf at level 2, Morton order; the state filled in place
+        # (the values of the uniform grid's noisy gas at the same cells)
+        mesh = A.AmrMesh(root, [(2, (i, j, k)) for k in range(2 * nb) for j in range(2 * nb) for i in range(2 * nb)])
         hp0 = HydroParams(gamma=5.0 / 3.0)
-        ug = S.noisy_gas(fine, hp0)
-        slot = [(c[2] * fine.nblocky + c[1]) * fine.nblockx + c[0] for c in mesh.bcoords]
-        unk = np.ascontiguousarray(ug[slot])
-        del ug
+        unk = np.zeros(mesh.unk_shape)
+        S.noisy_gas_blocks(fine, hp0, mesh.bcoords, unk, chunk=256, threads=os.cpu_count() or 1)
         zones = mesh.ncells()
         K = max(3, min(50, int(4e8 / zones)))
         for order in (3, 5):

@@ -233,6 +233,49 @@ def noisy_gas(geom: Geometry, hp: HydroParams, vmag=0.1, noise=0.05):
     return scatter_global(geom, _finish(hp, rho, vm * dirx, vm * diry, vm * dirz, p))
 
 
+def noisy_gas_blocks(geom: Geometry, hp: HydroParams, bcoords, out, vmag=0.1, noise=0.05, chunk=2048, threads=1):
+    """noisy_gas's values for the listed blocks of a 3-D `geom`, written
+    block chunk by block chunk into the UNK `out` (len(bcoords), k, j, i, var)
+    (guard cells untouched): the same global cell indices, so the same values,
+    without a copy of the whole grid.  threads > 1 fills disjoint chunks
+    concurrently."""
+    nbx, nby, nbz = geom.nxb, geom.nyb, geom.nzb
+    nx, ny = nbx * geom.nblockx, nby * geom.nblocky
+    dx, dy, dz = geom.deltas()
+    g = geom.nguard
+    kk, jj, ii = np.meshgrid(np.arange(nbz), np.arange(nby), np.arange(nbx), indexing="ij")
+    bc = np.asarray(bcoords, dtype=np.int64)
+
+    def fill(c0):
+        b = bc[c0:c0 + chunk]
+        gi = b[:, 0, None, None, None] * nbx + ii
+        gj = b[:, 1, None, None, None] * nby + jj
+        gk = b[:, 2, None, None, None] * nbz + kk
+        idx = ((gk * ny + gj) * nx + gi).astype(np.uint64)
+
+        def normal(stream):
+            u1, u2 = uniform01(idx, stream=stream)
+            return np.sqrt(-2.0 * np.log(1.0 - u1)) * np.cos(2.0 * math.pi * u2)
+        u1, u2 = uniform01(idx, stream=10)
+        cost = 2.0 * u1 - 1.0
+        sint = np.sqrt(np.maximum(0.0, 1.0 - cost * cost))
+        ph = 2.0 * math.pi * u2
+        dirx, diry, dirz = sint * np.cos(ph), sint * np.sin(ph), cost
+        rho = 1.0 * (1.0 + noise * normal(11))
+        p = 1.0 * (1.0 + noise * normal(12))
+        vm = vmag * (1.0 + noise * normal(13))
+        out[c0:c0 + len(b), g:g + nbz, g:g + nby, g:g + nbx, :] = _finish(hp, rho, vm * dirx, vm * diry, vm * dirz, p)
+    starts = range(0, len(bc), chunk)
+    if threads > 1:
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(threads) as ex:
+            list(ex.map(fill, starts))
+    else:
+        for c0 in starts:
+            fill(c0)
+    return out
+
+
 # ---------------------------------------------------------------- configurations
 def species_blob(geom: Geometry, ns=3, nspecies=2, center=(0.5, 0.5, 0.5), radius=0.2, width=0.03):
     """Advected mass fractions, (blk, k, j, i, ns) like UNK: species 0 is a
