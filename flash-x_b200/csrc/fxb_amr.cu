@@ -1175,6 +1175,8 @@ int amr_create(const AmrCommon &c, const fxb_block_desc *leaves, int nleaf)
     if (D.ndim != 3) return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: AMR meshes are implemented for 3-D");
     if (D.nxb != D.nyb || D.nxb != D.nzb || D.nxb % 2 || D.nxb < D.nguard)
         return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: AMR blocks must be cubes of an even size >= NGUARD");
+    if (c.dprm.shock_detect)
+        return record_error(FXB_EUNSUPPORTED, "fxb_register_blocks: the shock detector is implemented for uniform grids");
     S.n = D.nxb;
     S.ng = D.nguard;
     S.nleaf = nleaf;

@@ -36,6 +36,9 @@ struct Lib {
     long ncell = 0, vstride = 0;
     int gext[3] = {1, 1, 1};       // cells per axis of the whole grid (cell widths)
     int kbc[6];                    // boundary handling of the stored grid (outflow beside a halo)
+    unsigned char *shok = nullptr; // shock detector on: the SHOK flag of every stored cell
+    int shock_slot = -1;           // UNK slot of SHOK_VAR (< 0: not written to the host)
+    bool shok_valid = false;       // the flags belong to a step taken since the last attach
     fxb_slab slab{};               // this rank's layers of the slowest axis and its halos
     long plane = 1;                // cells in one plane of the slowest axis
     int nint = 1;                  // interior planes of the slowest axis
@@ -138,6 +141,74 @@ struct UnkGeom {
     long vstride;
     int soff;      // stored plane of a global index of the slowest axis: global + soff
 };
+
+// hy_shockDetectBlk.F90 on the stored grid: 1 where the summed |central
+// pressure differences| / 2 reach 0.5 min p over the cell's 3^d box and the
+// velocity divergence is at most -0.1 min c_s over the box, cells outside the
+// domain mapped as the guard fill maps them (the oracle's arithmetic)
+__global__ void __launch_bounds__(256) shock_kernel(const double *__restrict__ st, long vs, int ndim, int nx, int ny,
+                                                    int nz, UnkGeom g, unsigned char *__restrict__ shok)
+{
+    const long n = (long)nx * ny * nz;
+    auto var = [&](int q, int i, int j, int k) {
+        double sx = 1.0, sy = 1.0, sz = 1.0;
+        const int mi = map_axis(i, nx, g.bc[0], g.bc[1], &sx);
+        const int mj = ndim > 1 ? map_axis(j, ny, g.bc[2], g.bc[3], &sy) : 0;
+        const int mk = ndim > 2 ? map_axis(k, nz, g.bc[4], g.bc[5], &sz) : 0;
+        double x = st[q * vs + ((long)mk * ny + mj) * nx + mi];
+        if (q == VX) x = x * sx;
+        if (q == VY) x = x * sy;
+        if (q == VZ) x = x * sz;
+        return x;
+    };
+    const int k2 = ndim > 1, k3 = ndim > 2;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % nx), j = (int)((idx / nx) % ny), k = (int)(idx / ((long)nx * ny));
+        double minP = 0., minC = 0.;
+        bool first = true;
+        for (int kk = k - k3; kk <= k + k3; kk++)
+            for (int jj = j - k2; jj <= j + k2; jj++)
+                for (int ii = i - 1; ii <= i + 1; ii++) {
+                    const double pr = var(P, ii, jj, kk);
+                    const double cs = sqrt(var(GC, ii, jj, kk) * var(P, ii, jj, kk) / var(D, ii, jj, kk));
+                    if (first || pr < minP) minP = pr;
+                    if (first || cs < minC) minC = cs;
+                    first = false;
+                }
+        double divv = var(VX, i + 1, j, k) - var(VX, i - 1, j, k);
+        if (ndim > 1) divv = divv + var(VY, i, j + 1, k) - var(VY, i, j - 1, k);
+        if (ndim > 2) divv = divv + var(VZ, i, j, k + 1) - var(VZ, i, j, k - 1);
+        divv = 0.5 * divv;
+        const double gx = 0.5 * (var(P, i + 1, j, k) - var(P, i - 1, j, k));
+        double gy = 0., gz = 0.;
+        if (ndim > 1) gy = 0.5 * (var(P, i, j + 1, k) - var(P, i, j - 1, k));
+        if (ndim > 2) gz = 0.5 * (var(P, i, j, k + 1) - var(P, i, j, k - 1));
+        const bool sw1 = fabs(gx) + fabs(gy) + fabs(gz) >= 0.5 * minP;
+        const bool sw2 = -0.1 * minC >= divv;
+        shok[idx] = (sw1 && sw2) ? 1 : 0;
+    }
+}
+
+// the flags into UNK slot `slot` of every block cell, guard cells mapped
+__global__ void shok_to_unk_kernel(const unsigned char *__restrict__ shok, double *__restrict__ unk, UnkGeom g,
+                                   const int *__restrict__ bcoord, int nblk, int slot)
+{
+    long per = (long)g.nig * g.njg * g.nkg;
+    long n = (long)nblk * per;
+    for (long idx = blockIdx.x * (long)blockDim.x + threadIdx.x; idx < n; idx += (long)gridDim.x * blockDim.x) {
+        int blk = (int)(idx / per);
+        long r = idx - blk * per;
+        int k = (int)(r / ((long)g.nig * g.njg)); r -= (long)k * g.nig * g.njg;
+        int j = (int)(r / g.nig), i = (int)(r - (long)j * g.nig);
+        int gj = g.ndim >= 2 ? g.ng : 0, gk = g.ndim == 3 ? g.ng : 0;
+        double s_;
+        int mx = map_axis(bcoord[3 * blk] * g.nxb + i - g.ng, g.nx, g.bc[0], g.bc[1], &s_);
+        int my = g.ndim >= 2 ? map_axis(bcoord[3 * blk + 1] * g.nyb + j - gj + (g.ndim == 2 ? g.soff : 0), g.ny,
+                                        g.bc[2], g.bc[3], &s_) : 0;
+        int mz = g.ndim == 3 ? map_axis(bcoord[3 * blk + 2] * g.nzb + k - gk + g.soff, g.nz, g.bc[4], g.bc[5], &s_) : 0;
+        unk[idx * g.nunk + slot] = (double)shok[((long)mz * g.ny + my) * g.nx + mx];
+    }
+}
 
 __global__ void unk_to_state_kernel(const double *__restrict__ unk, double *__restrict__ st, UnkGeom g,
                                     const int *__restrict__ bcoord, const int *__restrict__ dmap, int nblk)
@@ -402,6 +473,11 @@ int launch_species(int src, const double *dtv, double dt);
 // launch one fused hydro step reading buffer `src`, writing 1-src
 int launch_hydro(int src, const double *dtv, double dt)
 {
+    if (L.shok) {   // levelFlux/Hydro.F90:133-149: the flags of the step's initial state
+        UnkGeom g = unk_geom();
+        shock_kernel<<<148 * 8, 256, 0, L.stream>>>(L.buf[src], L.vstride, L.dom.ndim, L.nx, L.ny, L.nz, g, L.shok);
+        L.shok_valid = true;
+    }
     if (L.dom.ndim == 2) {
         Args2D a;
         a.in = L.buf[src]; a.out = L.buf[1 - src]; a.vstride = L.vstride;
@@ -416,6 +492,7 @@ int launch_hydro(int src, const double *dtv, double dt)
         a.flat = L.flat;
         a.tmap = L.tmap2d[src];
         a.fd[0] = L.sfd[0]; a.fd[1] = L.sfd[1];
+        a.shok = L.shok;
         a.use_tma = L.use_tma;
         a.tma_extra_tx = L.tma_extra_tx;
         a.wait_budget = L.wait_budget;
@@ -441,6 +518,7 @@ int launch_hydro(int src, const double *dtv, double dt)
         a.hyb = (const unsigned char *)L.hyb;
         for (int d = 0; d < 3; d++) { a.wst[d] = L.w3[d]; a.flx[d] = L.f3[d]; a.ctufb[d] = L.ctufb[d]; }
         for (int q = 0; q < 4; q++) a.cta[q] = 148 * L.ug_cta[q];
+        a.shok = L.shok;
         for (int d = 0; d < 3; d++) a.sf_t1[d] = L.sf_t1[d];
         for (int d = 0; d < 3 && L.ns; d++)
             if (cudaMemsetAsync(L.ctufb[d], 0, L.snw, L.stream) != cudaSuccess) return cuda_fail(cudaGetLastError(), "memset");
@@ -539,6 +617,7 @@ void free_all()
     if (L.pack_dev) cudaFree(L.pack_dev);
     if (L.pack_host) cudaFreeHost(L.pack_host);
     if (L.dtv) cudaFree(L.dtv);
+    if (L.shok) cudaFree(L.shok);
     if (L.rate_max) cudaFree(L.rate_max);
     if (L.err) cudaFree(L.err);
     if (L.partials) cudaFree(L.partials);
@@ -582,8 +661,10 @@ extern "C" int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
     if (d.nguard < 4) return fail(FXB_EARG, "fxb_init: NGUARD must be at least 4");
     if (p.order != 2 && p.order != 3 && p.order != 5)
         return fail(FXB_EUNSUPPORTED, "fxb_init: order must be 2 (MUSCL-Hancock), 3 (PPM) or 5 (WENO)");
-    if (p.riemann < 1 || p.riemann > 7 || p.riemann == 6)
-        return fail(FXB_EUNSUPPORTED, "fxb_init: RiemannSolver must be Roe, LLF, HLL, HLLC, Marquina or MarquinaModified");
+    if (p.riemann < 1 || p.riemann > 8 || p.riemann == 6)
+        return fail(FXB_EUNSUPPORTED,
+                    "fxb_init: RiemannSolver must be Roe, LLF, HLL, HLLC, Marquina, MarquinaModified or hybrid");
+    if (p.shock_slot >= nunk) return fail(FXB_EARG, "fxb_init: shock_slot outside UNK");
     if (p.limiter < 1 || p.limiter > 5) return fail(FXB_EARG, "fxb_init: unknown slope limiter");
     if (p.precision != FXB_FP64 && p.precision != FXB_MIXED) return fail(FXB_EARG, "fxb_init: unknown precision");
     if (p.flattening && p.use_gravity) return fail(FXB_EUNSUPPORTED, "fxb_init: use_flattening with gravity is not implemented");
@@ -662,6 +743,9 @@ extern "C" int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
     q.cvisc = p.cvisc;
     q.use_hybrid = p.hybrid_order ? 1 : 0;
     q.hybrid_kappa = p.hybrid_kappa;
+    // Hydro_init.F90:391-394: the hybrid solver turns the shock detector on
+    q.shock_detect = (p.shock_detect || p.riemann == 8) ? 1 : 0;
+    L.shock_slot = p.shock_slot;
     // Gamma/Eos_init.F90:86 and Gamma/Eos.F90:177,240-241
     double gammam1 = 1.0 / (p.gamma - 1.0);
     L.gam1inv = 1. / gammam1;
@@ -688,6 +772,10 @@ extern "C" int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
     CK(cudaMalloc(&L.pmap_dev, sizeof(int) * NV_DEV));
     CK(cudaMemcpyAsync(L.dmap_dev, L.dmap, sizeof(int) * NV_DEV, cudaMemcpyHostToDevice, L.stream));
     CK(cudaMalloc(&L.dtv, 2 * sizeof(double)));
+    if (L.dprm.shock_detect) {
+        CK(cudaMalloc(&L.shok, (size_t)L.vstride));
+        CK(cudaMemsetAsync(L.shok, 0, (size_t)L.vstride, L.stream));
+    }
     CK(cudaMalloc(&L.rate_max, sizeof(unsigned long long)));
     CK(cudaMalloc(&L.err, sizeof(int)));
     CK(cudaMemsetAsync(L.err, 0, sizeof(int), L.stream));
@@ -974,6 +1062,7 @@ extern "C" int fxb_attach_unk(const double *unk_host)
         if (rc) return rc;
         state_changed(false);
     }
+    L.shok_valid = false;         // the attached UNK's SHOK stands until the next step
     return FXB_OK;
 }
 
@@ -991,6 +1080,9 @@ extern "C" int fxb_sync_to_host(double *unk_host)
     state_to_unk_kernel<<<1184, 256, 0, L.stream>>>(L.buf[L.cur], L.unk_dev, g, L.bcoord, L.dmap_dev, L.nblk);
     if (L.ns)
         spec_to_unk_kernel<<<1184, 256, 0, L.stream>>>(L.spb[L.cur], L.unk_dev, g, L.bcoord, L.sslot_dev, L.ns, L.nblk);
+    CK(cudaGetLastError());
+    if (L.shok && L.shok_valid && L.shock_slot >= 0)   // SHOK_VAR, guard cells filled like the other variables
+        shok_to_unk_kernel<<<1184, 256, 0, L.stream>>>(L.shok, L.unk_dev, g, L.bcoord, L.nblk, L.shock_slot);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(unk_host, L.unk_dev, sizeof(double) * L.unk_doubles, cudaMemcpyDeviceToHost, L.stream));
     CK(cudaStreamSynchronize(L.stream));

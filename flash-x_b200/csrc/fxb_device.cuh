@@ -36,6 +36,7 @@ struct DevParams {
     int use_hybrid;            // hybrid order: first-order states at shocks
     double hybrid_kappa;
     int nspec;                 // advected mass fractions (species and mass scalars; uniform grids)
+    int shock_detect;          // the SHOK flag before each step (uniform grids)
 };
 
 // ---- precision helpers ---------------------------------------------------
@@ -64,8 +65,8 @@ template <> __device__ __forceinline__ float divc<float>(float x, double c) { re
 __host__ __device__ inline bool marquina_solver(const DevParams &p) { return p.riemann == 5 || p.riemann == 7; }
 __host__ __device__ inline bool extended_options(const DevParams &p)
 {
-    return p.riemann == 1 || p.riemann == 5 || p.riemann == 7 || p.steepening || p.order == 2 || p.use_avisc ||
-           p.use_hybrid || p.nspec > 0;
+    return p.riemann == 1 || p.riemann == 5 || p.riemann == 7 || p.riemann == 8 || p.steepening || p.order == 2 ||
+           p.use_avisc || p.use_hybrid || p.nspec > 0;
 }
 
 // Fortran MIN/MAX with gfortran's argument order: mvar = a1; if (a2 < mvar) mvar = a2
@@ -890,16 +891,19 @@ __device__ __forceinline__ int riemann_marquina(int dir, bool modified, const R 
     return 0;
 }
 
+// shock: the hybrid solver's face is next to a cell the shock detector marked
 template <class R, int EXT>
 __device__ __forceinline__ int riemann(const DevParams &prm, int dir, const R *Vm, R gcL, R geL,
-                                       const R *Vp, R gcR, R geR, R F[8])
+                                       const R *Vp, R gcR, R geR, R F[8], bool shock = false)
 {
     const R velNL = Vm[1 + dir], velNR = Vp[1 + dir];
     const R aL2 = rdiv(gcL * Vm[P], Vm[D]);
     const R aR2 = rdiv(gcR * Vp[P], Vp[D]);
     const bool roe = EXT == 1 && prm.riemann == 1;
     const bool marq = EXT == 2 && (prm.riemann == 5 || prm.riemann == 7);
-    const bool hllc = !roe && !marq && prm.riemann == 4, llf = !roe && !marq && prm.riemann == 2;
+    // hy_getFaceFlux.F90:364-383: the hybrid solver is HLL next to a marked cell, HLLC elsewhere
+    const bool hybr = EXT == 1 && prm.riemann == 8;
+    const bool hllc = !roe && !marq && (prm.riemann == 4 || (hybr && !shock)), llf = !roe && !marq && prm.riemann == 2;
     const R tiny = hllc ? R(prm.tiny) : R(1.e-32);
     if ((Vm[D] < tiny && Vm[D] > R(0)) || (Vp[D] < tiny && Vp[D] > R(0)) ||
         (Vm[P] < tiny && Vm[P] > R(0)) || (Vp[P] < tiny && Vp[P] > R(0))) {
@@ -1032,6 +1036,19 @@ __device__ __forceinline__ int map_axis(int g, int n, int bclo, int bchi, double
         *s = -1.0; return 2 * n - 1 - g;
     }
     return g;
+}
+
+// the shock flag of cell (i, j, k) of the uniform grid, outside the domain
+// mapped as the guard fill maps a scalar (SHOK_VAR after Grid_fillGuardCells);
+// ny = 1 in 2-D, nz = 1 in 2-D
+__device__ __forceinline__ int shock_flag(const unsigned char *shok, int i, int j, int k, int nx, int ny, int nz,
+                                          const int *bc)
+{
+    double s;
+    const int mi = map_axis(i, nx, bc[0], bc[1], &s);
+    const int mj = ny > 1 ? map_axis(j, ny, bc[2], bc[3], &s) : 0;
+    const int mk = nz > 1 ? map_axis(k, nz, bc[4], bc[5], &s) : 0;
+    return shok[((long)mk * ny + mj) * nx + mi];
 }
 
 } // namespace fxb

@@ -49,6 +49,7 @@ struct alignas(64) Args2D {
     const void *flat;        // flattening coefficients [2][(nx+2)(ny+2)] of R, padded by one cell
     void *fd[2] = {nullptr, nullptr};   // species on: the mass flux of every x / y face, R ((nx+1) ny, nx (ny+1))
     long rate_c0 = 0, rate_c1 = 0x7fffffffffffffffL;   // cells [c0, c1) enter the CFL rate (a slab's own)
+    const unsigned char *shok = nullptr;   // shock detector on: the flag of every cell [y][x]
 };
 
 constexpr int T2 = 16;             // tile edge
@@ -295,8 +296,14 @@ __device__ __forceinline__ void faces_stage(const Args2D &a, Smem2D<R> &s, int d
     R VL[6], VR[6], F[8];
 #pragma unroll
     for (int k = 0; k < 6; k++) { VL[k] = s.W[k][wl]; VR[k] = s.W[6 + k][wr]; }
+    bool shock = false;
+    if (EXT && a.shok) {       // window column/row w is grid cell tile origin + w - 3
+        const int x0 = blockIdx.x * T2 - 3, y0 = blockIdx.y * T2 - 3;
+        shock = shock_flag(a.shok, x0 + wxl, y0 + wyl, 0, a.nx, a.ny, 1, a.bc) +
+                shock_flag(a.shok, x0 + wxr, y0 + wyr, 0, a.nx, a.ny, 1, a.bc) > 0;
+    }
     int e = riemann<R, EXT>(a.prm, dir, VL, s.V[GC][wyl][wxl + XO], s.V[GE][wyl][wxl + XO],
-                    VR, s.V[GC][wyr][wxr + XO], s.V[GE][wyr][wxr + XO], F);
+                    VR, s.V[GC][wyr][wxr + XO], s.V[GE][wyr][wxr + XO], F, shock);
     if (e) set_err(a.err, e);
     if (EXT && a.prm.use_avisc) {
         const int td = 1 - dir, tx = td == 0, ty = td == 1, vt = td == 0 ? VX : VY, vn = dir == 0 ? VX : VY;

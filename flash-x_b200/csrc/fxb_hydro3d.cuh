@@ -87,6 +87,7 @@ struct Args3D {
     long divu_bstride = 0;
     long rate_c0 = 0, rate_c1 = 0x7fffffffffffffffL;   // cells [c0, c1) enter the CFL rate (a slab's own)
     unsigned char *ctufb[3] = {nullptr, nullptr, nullptr};   // species on: 1 where the CTU fallback fired (Grid3::widx)
+    const unsigned char *shok = nullptr;   // shock detector on (uniform grid): the flag of every cell
 };
 // Face-state tile of direction d (N cells along d, N1 along the t1 axis):
 // the fewest warp lanes in total (the N + 1 faces split into segments of
@@ -756,7 +757,11 @@ __device__ __forceinline__ void flux3d_kernel_body(const Args3D &a, const VB vb)
         for (int q = 0; q < 6; q++) { VL[q] = w[(long)q * nw + wl]; VR[q] = w[(long)(6 + q) * nw + wr]; }
         X.load_gammas(a, i - di, j - dj, k - dk, gcl, gel);
         X.load_gammas(a, i, j, k, gcr, ger);
-        int e = riemann<R, EXT>(a.prm, d, VL, gcl, gel, VR, gcr, ger, F);
+        bool shock = false;
+        if (EXT && !AMR && a.shok)
+            shock = shock_flag(a.shok, i - di, j - dj, k - dk, a.nx, a.ny, a.nz, a.bc) +
+                    shock_flag(a.shok, i, j, k, a.nx, a.ny, a.nz, a.bc) > 0;
+        int e = riemann<R, EXT>(a.prm, d, VL, gcl, gel, VR, gcr, ger, F, shock);
         if (e) atomicOr(a.err, e);
         if constexpr (EXT) {
             if (a.prm.use_avisc) { avisc3d<R, AMR>(a, X, d, i, j, k, F); eint_fluxes(a.prm, VL, VR, F); }
@@ -883,7 +888,14 @@ __device__ __forceinline__ void sflux3d_kernel_body(const Args3D &a, const VB vb
         R VL[6], F[NF];
 #pragma unroll
         for (int q = 0; q < 6; q++) VL[q] = sW[q * nt + tl];
-        const int e = riemann<R, EXT>(a.prm, d, VL, sW[6 * nt + tl], sW[7 * nt + tl], Wm, gc, ge, F);
+        bool shock = false;      // the face between cell (i, j, k) - e_d and (i, j, k)
+        if (EXT && !AMR && a.shok) {
+            int di, dj, dk;
+            offs(d, 1, di, dj, dk);
+            shock = shock_flag(a.shok, i - di, j - dj, k - dk, a.nx, a.ny, a.nz, a.bc) +
+                    shock_flag(a.shok, i, j, k, a.nx, a.ny, a.nz, a.bc) > 0;
+        }
+        const int e = riemann<R, EXT>(a.prm, d, VL, sW[6 * nt + tl], sW[7 * nt + tl], Wm, gc, ge, F, shock);
         if (e) atomicOr(a.err, e);
         if constexpr (EXT) {
             if (a.prm.use_avisc) { avisc3d<R, AMR>(a, X, d, i, j, k, F); eint_fluxes(a.prm, VL, Wm, F); }

@@ -54,6 +54,7 @@ class FxbParams(ctypes.Structure):
         ("precision", ctypes.c_int), ("flattening", ctypes.c_int), ("entropy_fix", ctypes.c_int),
         ("steepening", ctypes.c_int), ("use_avisc", ctypes.c_int), ("cvisc", ctypes.c_double),
         ("upwind_tvd", ctypes.c_int), ("hybrid_order", ctypes.c_int), ("hybrid_kappa", ctypes.c_double),
+        ("shock_detect", ctypes.c_int), ("shock_slot", ctypes.c_int),
     ]
 
 
@@ -159,7 +160,7 @@ def make_fxb_params(hp: HydroParams, precision="fp64"):
     p.order = hp.order
     p.weno_method = 2 if hp.wenoMethod.upper() == "WENOZ" else 1
     p.riemann = {"HLLC": 4, "HLL": 3, "LLF": 2, "ROE": 1, "MARQUINA": 5,
-                 "MARQUINAMODIFIED": 7}[hp.RiemannSolver.upper()]
+                 "MARQUINAMODIFIED": 7, "HYBRID": 8}[hp.RiemannSolver.upper()]
     p.limiter = {"minmod": 1, "mc": 2, "vanleer": 3, "hybrid": 4, "limited": 5}[hp.slopeLimiter.lower()]
     p.char_limiting = int(hp.charLimiting)
     p.use_3d_full_ctu = int(hp.use_3dFullCTU)
@@ -180,6 +181,8 @@ def make_fxb_params(hp: HydroParams, precision="fp64"):
     p.upwind_tvd = int(hp.use_upwindTVD)
     p.hybrid_order = int(hp.use_hybridOrder)
     p.hybrid_kappa = hp.hybridOrderKappa
+    p.shock_detect = int(hp.shock_detect)
+    p.shock_slot = UNK_VARS.index("shok") if hp.shock_detect else -1
     return p
 
 

@@ -23,7 +23,7 @@ BC_NAMES = {"periodic": BC_PERIODIC, "outflow": BC_OUTFLOW, "reflect": BC_REFLEC
 class HydroParams:
     order: int = 3                      # 2 = MUSCL-Hancock, 3 = PPM, 5 = WENO
     wenoMethod: str = "WENO5"           # WENO5 | WENOZ
-    RiemannSolver: str = "HLLC"         # HLLC | HLL | LLF | Roe | Marquina | MarquinaModified
+    RiemannSolver: str = "HLLC"         # HLLC | HLL | LLF | Roe | Marquina | MarquinaModified | hybrid
     slopeLimiter: str = "mc"            # minmod | mc | vanLeer | hybrid | limited
     LimitedSlopeBeta: float = 1.0
     charLimiting: bool = True
@@ -39,6 +39,8 @@ class HydroParams:
     cvisc: float = 0.1
     use_hybridOrder: bool = False       # first-order states at shocks
     hybridOrderKappa: float = 0.0
+    shockDetect: bool = False           # the strong-shock flag SHOK (hy_shockDetectBlk); on with RiemannSolver hybrid
+    shockLowerCFL: bool = False
     hydroComputeDtOption: int = -1
     cfl: float = 0.8
     gamma: float = 1.4
@@ -58,13 +60,21 @@ class HydroParams:
     dtmax: float = 1.0e5
     tstep_change_factor: float = 2.0
 
+    @property
+    def shock_detect(self):
+        """Hydro_init.F90:117-122, 391-394: the shock detector runs when asked
+        for, and always with the hybrid Riemann solver."""
+        return bool(self.shockDetect) or self.RiemannSolver.upper() == "HYBRID"
+
     def validate(self):
         """Reject option combinations this path does not implement, the way
         Hydro_init aborts on unknown choices."""
         if self.order not in (2, 3, 5):
             raise ValueError("order must be 2 (MUSCL-Hancock), 3 (PPM) or 5 (WENO)")
-        if self.RiemannSolver.upper() not in ("HLLC", "HLL", "LLF", "ROE", "MARQUINA", "MARQUINAMODIFIED"):
-            raise ValueError("RiemannSolver must be HLLC, HLL, LLF, Roe, Marquina or MarquinaModified")
+        if self.RiemannSolver.upper() not in ("HLLC", "HLL", "LLF", "ROE", "MARQUINA", "MARQUINAMODIFIED", "HYBRID"):
+            raise ValueError("RiemannSolver must be HLLC, HLL, LLF, Roe, Marquina, MarquinaModified or hybrid")
+        if self.shockLowerCFL:
+            raise ValueError("shockLowerCFL is not implemented")
         if self.slopeLimiter.lower() not in ("minmod", "mc", "vanleer", "hybrid", "limited"):
             raise ValueError("unknown slopeLimiter " + self.slopeLimiter)
         if self.wenoMethod.upper() not in ("WENO5", "WENOZ"):

@@ -59,7 +59,9 @@ typedef struct fxb_params {
     int    order;              /* 2 = MUSCL-Hancock, 3 = PPM, 5 = WENO               */
     int    weno_method;        /* 1 = WENO5, 2 = WENOZ                               */
     int    riemann;            /* 1 = Roe, 2 = LLF, 3 = HLL, 4 = HLLC, 5 = Marquina,
-                                  7 = MarquinaModified (UHD.h)                      */
+                                  7 = MarquinaModified, 8 = hybrid (HLL next to a
+                                  cell the shock detector marks, HLLC elsewhere;
+                                  turns shock_detect on) (UHD.h)                    */
     int    limiter;            /* 1 minmod, 2 mc, 3 vanLeer, 4 hybrid, 5 limited     */
     int    char_limiting;      /* charLimiting                                       */
     int    use_3d_full_ctu;    /* use_3dFullCTU                                      */
@@ -82,6 +84,10 @@ typedef struct fxb_params {
                                   (FXB_EUNSUPPORTED) with more guard cells        */
     int    hybrid_order;       /* use_hybridOrder                                    */
     double hybrid_kappa;       /* hybridOrderKappa (Config default 0)                */
+    int    shock_detect;       /* shockDetect: the SHOK flag of every cell before each
+                                  step (hy_shockDetectBlk.F90; uniform grids)       */
+    int    shock_slot;         /* 0-based UNK slot of SHOK_VAR that fxb_sync_to_host
+                                  and unmasked guard fills write (< 0: none)        */
 } fxb_params;
 
 /* Domain of a uniform block grid. */

@@ -744,6 +744,47 @@ static int riemann_marquina_mod(const fxo_params *p, int dir, const double *Vm, 
     return 0;
 }
 
+/* hy_shockDetectBlk.F90 on one block: SHOK = 0 over the whole block, then
+ * 1 in every interior cell where the pressure jump |grad p| (central
+ * differences, summed over the axes) reaches half the smallest pressure of
+ * the cell's 3^d box and the velocity divergence is below -0.1 times the
+ * smallest sound speed of that box (beta = 0.5, delta = 0.1). */
+static void shock_detect_block(const blk_t *b, double *U)
+{
+    const fxo_params *p = b->p;
+    const int k2 = p->ndim > 1, k3 = p->ndim > 2;
+#define UV(var, ii, jj, kk) U[cidx(b, ii, jj, kk) * FXO_NUNK + (var)]
+    for (long c = 0; c < b->ncell; c++) U[c * FXO_NUNK + FXO_SHOK] = 0.;
+    const double beta = 0.5, delta = 0.1;
+    for (int k = b->k0; k <= b->kmax; k++)
+    for (int j = b->j0; j <= b->jmax; j++)
+    for (int i = b->i0; i <= b->imax; i++) {
+        double minP = 0., minC = 0.;
+        int first = 1;
+        for (int kk = k - k3; kk <= k + k3; kk++)
+        for (int jj = j - k2; jj <= j + k2; jj++)
+        for (int ii = i - 1; ii <= i + 1; ii++) {
+            const double pr = UV(FXO_PRES, ii, jj, kk);
+            const double cs = sqrt(UV(FXO_GAMC, ii, jj, kk) * UV(FXO_PRES, ii, jj, kk) / UV(FXO_DENS, ii, jj, kk));
+            if (first || pr < minP) minP = pr;
+            if (first || cs < minC) minC = cs;
+            first = 0;
+        }
+        double divv = UV(FXO_VELX, i + 1, j, k) - UV(FXO_VELX, i - 1, j, k);
+        if (p->ndim > 1) divv = divv + UV(FXO_VELY, i, j + 1, k) - UV(FXO_VELY, i, j - 1, k);
+        if (p->ndim > 2) divv = divv + UV(FXO_VELZ, i, j, k + 1) - UV(FXO_VELZ, i, j, k - 1);
+        divv = 0.5 * divv;
+        const double gx = 0.5 * (UV(FXO_PRES, i + 1, j, k) - UV(FXO_PRES, i - 1, j, k));
+        double gy = 0., gz = 0.;
+        if (p->ndim > 1) gy = 0.5 * (UV(FXO_PRES, i, j + 1, k) - UV(FXO_PRES, i, j - 1, k));
+        if (p->ndim > 2) gz = 0.5 * (UV(FXO_PRES, i, j, k + 1) - UV(FXO_PRES, i, j, k - 1));
+        const int sw1 = fabs(gx) + fabs(gy) + fabs(gz) >= beta * minP;
+        const int sw2 = -delta * minC >= divv;
+        if (sw1 && sw2) UV(FXO_SHOK, i, j, k) = 1.;
+    }
+#undef UV
+}
+
 /* the Riemann solver of the runtime parameter RiemannSolver */
 static int riemann_solve(const fxo_params *p, int dir, const double *Vm, const double *Vp, double Fs[6], double *speed)
 {
@@ -1125,7 +1166,12 @@ static int face_fluxes(const blk_t *b, const double *U, scratch_t *s)
             for (int v = 0; v < 8; v++) { VL[v] = s->scr[d][cm * 16 + v]; VR[v] = s->scr[d][c * 16 + 8 + v]; }
             VL[H_GR] = 0.; VR[H_GR] = 0.;
             double F[6], speed;
-            int err = riemann_solve(p, d, VL, VR, F, &speed);
+            int err;
+            if (p->riemann == FXO_HYBR)     /* hy_getFaceFlux.F90:364-383: HLL next to a shocked cell */
+                err = U[cm * FXO_NUNK + FXO_SHOK] + U[c * FXO_NUNK + FXO_SHOK] > 0.
+                    ? riemann_hll(p, d, VL, VR, F, &speed) : riemann_hllc(p, d, VL, VR, F, &speed);
+            else
+                err = riemann_solve(p, d, VL, VR, F, &speed);
             if (err) return 2;
             double *fl = s->flx[d] + c * 8;
             for (int v = 0; v < 6; v++) fl[v] = F[v];
@@ -1417,6 +1463,12 @@ int fxo_hydro_step_spec(const fxo_params *p, double *unk, double *spec, int ns, 
     if (ns) fxo_fill_guardcells_spec(p, spec, ns);
     blk_t b; blk_init(&b, p);
     long nblk = (long)p->nblockx * p->nblocky * p->nblockz;
+    if (p->shock_detect) {
+        /* levelFlux/Hydro.F90:133-149: the flag of every interior cell from the
+         * filled state, then the guard fill again, which carries SHOK too */
+        for (long blk = 0; blk < nblk; blk++) shock_detect_block(&b, unk + blk * b.ncell * FXO_NUNK);
+        fxo_fill_guardcells(p, unk);
+    }
     int status = 0;
 #ifdef _OPENMP
     if (nthreads <= 0) nthreads = omp_get_max_threads();

@@ -30,7 +30,7 @@ enum { FXO_DENS = 0, FXO_EINT, FXO_ENER, FXO_GAMC, FXO_GAME, FXO_PRES,
        FXO_SHOK, FXO_TEMP, FXO_VELX, FXO_VELY, FXO_VELZ, FXO_NUNK };
 
 enum { FXO_BC_PERIODIC = 0, FXO_BC_OUTFLOW = 1, FXO_BC_REFLECTING = 2 };
-enum { FXO_ROE = 1, FXO_LLF = 2, FXO_HLL = 3, FXO_HLLC = 4, FXO_MARQ = 5, FXO_MARM = 7 };   /* UHD.h:365-370 */
+enum { FXO_ROE = 1, FXO_LLF = 2, FXO_HLL = 3, FXO_HLLC = 4, FXO_MARQ = 5, FXO_MARM = 7, FXO_HYBR = 8 };   /* UHD.h:365-371 */
 enum { FXO_MINMOD = 1, FXO_MC = 2, FXO_VANLEER = 3, FXO_HYBRID = 4,
        FXO_LIMITED = 5 };
 
@@ -61,6 +61,7 @@ typedef struct {
     double cvisc;                   /* its constant */
     int use_hybrid;                 /* use_hybridOrder (hy_dataReconstOneStep.F90:864-913) */
     double hybrid_kappa;            /* hybridOrderKappa */
+    int shock_detect;               /* shockDetect: the SHOK flag before each step (hy_shockDetectBlk.F90) */
 } fxo_params;
 
 /* Number of doubles in one UNK array for the given geometry. */

@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(HERE, "libfx_oracle.so")
 NUNK = 11
 DENS, EINT, ENER, GAMC, GAME, PRES, SHOK, TEMP, VELX, VELY, VELZ = range(11)
 BC_PERIODIC, BC_OUTFLOW, BC_REFLECTING = 0, 1, 2
-ROE, LLF, HLL, HLLC, MARQ, MARM = 1, 2, 3, 4, 5, 7
+ROE, LLF, HLL, HLLC, MARQ, MARM, HYBR = 1, 2, 3, 4, 5, 7, 8
 LIMITERS = {"minmod": 1, "mc": 2, "vanleer": 3, "hybrid": 4, "limited": 5}
 
 
@@ -45,6 +45,7 @@ class FxoParams(ctypes.Structure):
         ("flattening", ctypes.c_int), ("entropy_fix", ctypes.c_int), ("steepening", ctypes.c_int),
         ("use_avisc", ctypes.c_int), ("cvisc", ctypes.c_double),
         ("use_hybrid", ctypes.c_int), ("hybrid_kappa", ctypes.c_double),
+        ("shock_detect", ctypes.c_int),
     ]
 
 
@@ -111,7 +112,7 @@ def make_params(geom, hp):
     p.order = hp.order
     p.weno_method = 2 if hp.wenoMethod.upper() == "WENOZ" else 1
     p.riemann = {"HLLC": HLLC, "HLL": HLL, "LLF": LLF, "ROE": ROE, "MARQUINA": MARQ,
-                 "MARQUINAMODIFIED": MARM}[hp.RiemannSolver.upper()]
+                 "MARQUINAMODIFIED": MARM, "HYBRID": HYBR}[hp.RiemannSolver.upper()]
     p.limiter = LIMITERS[hp.slopeLimiter.lower()]
     p.char_limiting = int(hp.charLimiting)
     p.use_3d_full_ctu = int(hp.use_3dFullCTU)
@@ -130,6 +131,7 @@ def make_params(geom, hp):
     p.cvisc = hp.cvisc
     p.use_hybrid = int(hp.use_hybridOrder)
     p.hybrid_kappa = hp.hybridOrderKappa
+    p.shock_detect = int(getattr(hp, "shock_detect", False))
     return p
 
 

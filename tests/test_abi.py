@@ -55,7 +55,7 @@ def test_init_validation_codes():
     d.nguard = 4; p.order = 4
     assert lib.fxb_init(ctypes.byref(p), ctypes.byref(d), H.default_var_map(), 11) == H.FXB_EUNSUPPORTED
     p.order = 3
-    for bad in (6, 8):      # HLLD is MHD-only, the hybrid solver needs shock detection
+    for bad in (6, 9):      # HLLD is MHD-only; no solver 9
         p.riemann = bad
         assert lib.fxb_init(ctypes.byref(p), ctypes.byref(d), H.default_var_map(), 11) == H.FXB_EUNSUPPORTED
     p.riemann = 4
@@ -138,7 +138,9 @@ def test_parameter_validation_mirrors_hydro_init():
     HydroParams(use_upwindTVD=True, use_avisc=True).validate()
     HydroParams(RiemannSolver="Marquina").validate()
     HydroParams(RiemannSolver="MarquinaModified").validate()
-    for bad in (dict(order=4), dict(order=6), dict(RiemannSolver="HLLD"), dict(entropyFixMethod="Einfeldt"),
+    HydroParams(RiemannSolver="hybrid").validate()
+    HydroParams(shockDetect=True).validate()
+    for bad in (dict(order=4), dict(order=6), dict(RiemannSolver="HLLD"), dict(shockLowerCFL=True), dict(entropyFixMethod="Einfeldt"),
                 dict(slopeLimiter="superbee"),
                 dict(transOrder=3),
                 dict(use_flattening=True, useGravity=True),

@@ -13,7 +13,9 @@
   periodic x/y, reflecting z): one step, bit for bit.
 * Configuration 4, the AMR benchmark mesh (5,230 leaves of 16^3 on levels
   1-4): one step with guard fill, prolongation, restriction and flux
-  correction, bit for bit.
+  correction, bit for bit; and three steps in batches of at most 700
+  leaves (eight batches, leaves next to refined faces updated in a second
+  pass) equal to the one-batch steps bit for bit.
 
 The host needs about 14 GB for the two largest cases (two UNK copies each).
 """
@@ -160,3 +162,35 @@ def test_amr_benchmark_mesh_one_step(oracle, need_gpu):
     b = unk[:, g:-g, g:-g, g:-g, :][..., HYDRO_VARS]
     assert np.max(_rel(a, b)) <= REL_TOL_ONE_STEP
     assert np.array_equal(a, b)
+
+
+def test_amr_benchmark_mesh_in_batches(need_gpu, monkeypatch):
+    """The multi-batch step (FXB_AMR_MAX_BATCH caps the leaves per batch) on
+    the benchmark mesh gives the one-batch state bit for bit, in both
+    precisions; the tuning log shows the batch size in use."""
+    from flashx_b200 import amr as A
+    from flashx_b200.params import BC_PERIODIC, Geometry, HydroParams
+    geom = Geometry(3, 16, 16, 16, 4, 4, 4, bc=(BC_PERIODIC,) * 6)
+    hp = HydroParams()
+    mesh, unk = A.levelset_problem(geom, hp, maxlev=4)
+    for prec in ("fp64", "mixed"):
+        outs = []
+        for cap in (None, "700"):
+            if cap:
+                monkeypatch.setenv("FXB_AMR_MAX_BATCH", cap)
+            else:
+                monkeypatch.delenv("FXB_AMR_MAX_BATCH", raising=False)
+            monkeypatch.setenv("FXB_AMR_PERSISTENT", "0")
+            dev = HydroDevice(geom, hp, prec, mesh=mesh)
+            dev.attach_unk(unk.copy())
+            if cap:
+                assert "700 blocks" in dev.tuning()
+            dt = 0.5 * dev.Hydro_computeDt()
+            for _ in range(3):
+                dev.Hydro(0.0, dt, dt)
+            out = np.zeros(unk.shape)
+            dev.sync_to_host(out)
+            dev.close()
+            outs.append(out)
+        g = geom.nguard
+        assert np.array_equal(outs[0][:, g:-g, g:-g, g:-g], outs[1][:, g:-g, g:-g, g:-g])

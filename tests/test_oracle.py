@@ -15,7 +15,7 @@ import pytest
 
 from flashx_b200 import simulations as S
 from flashx_b200.params import (BC_OUTFLOW, BC_PERIODIC, BC_REFLECTING, DENS, EINT, ENER, GAMC, GAME,
-                                Geometry, HydroParams, PRES, TEMP, VELX, VELY)
+                                Geometry, HydroParams, PRES, SHOK, TEMP, VELX, VELY)
 from exact_sod import sod_exact
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
@@ -572,3 +572,56 @@ def test_sod_2d_marquina_modified_matches_exact_solution(oracle):
     assert l1(g[idx, idx, DENS], rho_ex) < 0.01
     assert l1(g[idx, idx, PRES], p_ex) < 0.01
     assert l1((g[idx, idx, VELX] + g[idx, idx, VELY]) / math.sqrt(2.0), u_ex) < 0.02
+
+
+def _shock_flags_numpy(unk, g):
+    """hy_shockDetectBlk.F90 in numpy on a filled 2-D UNK: 1 where the sum of
+    |central pressure difference| / 2 reaches 0.5 min p over the cell's 3x3
+    box and the velocity divergence is at most -0.1 min c_s over the box."""
+    out = np.zeros(unk.shape[:1] + (unk.shape[2] - 2 * g, unk.shape[3] - 2 * g))
+    for b in range(unk.shape[0]):
+        B = unk[b, 0]
+        P = B[..., PRES]
+        cs = np.sqrt(B[..., GAMC] * P / B[..., DENS])
+        for j in range(g, B.shape[0] - g):
+            for i in range(g, B.shape[1] - g):
+                minP, minC = P[j - 1:j + 2, i - 1:i + 2].min(), cs[j - 1:j + 2, i - 1:i + 2].min()
+                divv = 0.5 * ((B[j, i + 1, VELX] - B[j, i - 1, VELX]) + B[j + 1, i, VELY] - B[j - 1, i, VELY])
+                gp = abs(0.5 * (P[j, i + 1] - P[j, i - 1])) + abs(0.5 * (P[j + 1, i] - P[j - 1, i]))
+                out[b, j - g, i - g] = 1.0 if (gp >= 0.5 * minP and -0.1 * minC >= divv) else 0.0
+    return out
+
+
+def test_shock_detector_and_hybrid_solver(oracle):
+    """shockDetect marks the cells the two switches of hy_shockDetectBlk pick
+    (against numpy on the filled state before the step) and leaves them in
+    UNK's SHOK slot; the hybrid Riemann solver (HLL next to a marked cell,
+    HLLC elsewhere) stays within the exact Sod bounds at t = 0.2 and differs
+    from plain HLLC."""
+    geom = Geometry(2, 16, 16, 1, 8, 8, 1, bc=(BC_OUTFLOW,) * 6)
+    hp = HydroParams(RiemannSolver="hybrid")
+    assert hp.shock_detect
+    p = oracle.make_params(geom.as_dict(), hp)
+    u = S.sod(geom, hp)
+    run_oracle(oracle, geom, hp, u, tmax=0.05)          # the shock has formed
+    pre = u.copy()
+    oracle.fill_guardcells(p, pre)
+    dt = 0.5 * oracle.compute_dt(p, u)
+    oracle.hydro_step(p, u, dt, dt)
+    g = geom.nguard
+    shok = u[:, 0, g:-g, g:-g, SHOK]
+    assert np.array_equal(shok, _shock_flags_numpy(pre, g))
+    assert 20 < shok.sum() < 0.2 * shok.size
+    unk = S.sod(geom, hp)
+    run_oracle(oracle, geom, hp, unk, tmax=0.2)
+    gl = S.gather_global(geom, unk)[0]
+    N = gl.shape[0]
+    idx = np.arange(N)
+    xi = (2 * (idx + 0.5) / N - 1.0) / math.sqrt(2.0) + 0.5
+    rho_ex, u_ex, p_ex = sod_exact(xi, 0.2)
+    keep = (xi > 0.05) & (xi < 0.95)
+    assert np.mean(np.abs(gl[idx, idx, DENS][keep] - rho_ex[keep])) < 0.01
+    assert np.mean(np.abs(gl[idx, idx, PRES][keep] - p_ex[keep])) < 0.01
+    ref = S.sod(geom, HydroParams())
+    run_oracle(oracle, geom, HydroParams(), ref, tmax=0.2)
+    assert not np.array_equal(S.gather_global(geom, ref)[..., DENS], S.gather_global(geom, unk)[..., DENS])
