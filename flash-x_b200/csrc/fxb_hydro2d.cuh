@@ -79,13 +79,18 @@ constexpr int NFC = (T2 + 1) * T2; // 272 faces
 // eigensystem: its 10 KB more shared memory leaves too little L1 for its
 // register spills (29 % slower measured on B200).
 template <class R> struct KeepOwn { static constexpr bool value = sizeof(R) == 4; };
+// FP32 keeps the slope stage's sigma of the other direction in shared memory;
+// FP64 recomputes it in the face-state stage from the window (the same
+// operations on the same cells): the 15 KB it frees per CTA stay L1, which
+// holds the FP64 kernel's register spills
+template <class R> struct KeepSig { static constexpr bool value = sizeof(R) == 4; };
 
 constexpr int NOWN = T2 * T2;      // owner cells of a tile
 
 template <class R> struct Smem2D {
     R V[8][WIN][WP];
     R DBF[NF * NFC];               // slopes [6][NDB], then fluxes [8][NFC]
-    R SG[6][NDB];                  // sigma of the other direction at the slope cells (global order)
+    R SG[6][KeepSig<R>::value ? NDB : 1];   // sigma of the other direction at the slope cells (global order)
     R W[12][NW];                   // Wp (D,VX,VY,VZ,P,EI), then Wm
     R EB[4][KeepOwn<R>::value ? NDB : 1];   // eigensystem base of the slope cells: cf, ahinv, lp, a2inv
     // FP64 update inputs of the owner cells that the window does not hold
@@ -118,6 +123,23 @@ template <class R> __device__ __forceinline__ void win6(const Smem2D<R> &s, int 
 
 __device__ __forceinline__ void set_err(int *err, int code) { atomicOr(err, code); }
 
+// the upwind transverse flux sigma of the direction other than dir at window
+// cell (wx, wy) (hy_upwindTransverseFlux), g its global-order 6-vector, eb its
+// eigensystem base; global order
+template <class R>
+__device__ __forceinline__ void sigma_other(const Args2D &a, const Smem2D<R> &s, int dir, int wx, int wy, const R g[6],
+                                            const EigBase<R> &eb, R sg[6])
+{
+    const int td = 1 - dir, tx = td == 0, ty = td == 1;
+    R gm[6], gp[6], m[6], c[6], p[6], sr[6];
+    win6(s, wx - tx, wy - ty, gm); win6(s, wx + tx, wy + ty, gp);
+    rot(td, gm, m); rot(td, g, c); rot(td, gp, p);
+    Eig<R> et;
+    eigen_dir(eb, c[1], et);
+    trans_flux(et, m, c, p, a.prm.use_aux_eint != 0, sr);
+    unrot(td, sr, sg);
+}
+
 // Per-cell analysis along dir at a slope cell: the eigensystem and limited
 // slopes (PPM), and the upwind transverse flux sigma of the other direction
 // (hy_upwindTransverseFlux), which the state stage of dir subtracts.
@@ -142,16 +164,12 @@ __device__ __forceinline__ void analysis_stage(const Args2D &a, Smem2D<R> &s, in
 #pragma unroll
         for (int k = 0; k < 6; k++) s.DBF[k * NDB + t] = db[k];
     }
-    const int td = 1 - dir, tx = td == 0, ty = td == 1;
-    R gm[6], gp[6], m[6], p[6], sr[6], sg[6];
-    win6(s, wx - tx, wy - ty, gm); win6(s, wx + tx, wy + ty, gp);
-    rot(td, gm, m); rot(td, g, c); rot(td, gp, p);
-    Eig<R> et;
-    eigen_dir(eb, c[1], et);
-    trans_flux(et, m, c, p, a.prm.use_aux_eint != 0, sr);
-    unrot(td, sr, sg);
+    if (KeepSig<R>::value) {
+        R sg[6];
+        sigma_other(a, s, dir, wx, wy, g, eb, sg);
 #pragma unroll
-    for (int k = 0; k < 6; k++) s.SG[k][t] = sg[k];
+        for (int k = 0; k < 6; k++) s.SG[k][t] = sg[k];
+    }
 }
 
 // velocity component q (VX or VY) of window cell (wx, wy); read from the
@@ -184,6 +202,7 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
 {
     const int ox = dir == 0, oy = dir == 1;
     R g[6], Vm[6], Vc[6], Vp[6], vecL[6], vecR[6], Wm[6], Wp[6];
+    R sgo[6];   // FP64: sigma of the other direction at this cell, recomputed here
     win6(s, wx, wy, g); rot(dir, g, Vc);
     // the cell's eigensystem along dir (FP32: from the base the slope stage kept)
     Eig<R> e;
@@ -193,8 +212,11 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
         eb.rho = Vc[0];
         eb.rp = eb.rho * (eb.cf * eb.cf);
         eigen_dir(eb, Vc[1], e);
-    } else if (!eigen(Vc[0], Vc[1], Vc[4], s.V[GC][wy][wx + XO], e)) {
-        set_err(a.err, ERR_SOUND);
+    } else {
+        EigBase<R> eb;
+        if (!eigen_base(Vc[0], Vc[4], s.V[GC][wy][wx + XO], eb)) set_err(a.err, ERR_SOUND);
+        eigen_dir(eb, Vc[1], e);
+        if (!KeepSig<R>::value) sigma_other(a, s, dir, wx, wy, g, eb, sgo);
     }
     if (EXT && a.prm.order == 2) {
         // MUSCL-Hancock: the cell's own slope, flattening and tracing in one step
@@ -256,7 +278,7 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
     // transverse flux of the other direction at this cell (from the analysis stage)
 #pragma unroll
     for (int k = 0; k < 6; k++) {
-        R sg = s.SG[k][dbi];
+        R sg = KeepSig<R>::value ? s.SG[k][dbi] : sgo[k];
         Wm[k] = Wm[k] - hdtt * sg;
         Wp[k] = Wp[k] - hdtt * sg;
     }
