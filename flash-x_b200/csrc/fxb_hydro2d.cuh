@@ -202,7 +202,6 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
 {
     const int ox = dir == 0, oy = dir == 1;
     R g[6], Vm[6], Vc[6], Vp[6], vecL[6], vecR[6], Wm[6], Wp[6];
-    R sgo[6];   // FP64: sigma of the other direction at this cell, recomputed here
     win6(s, wx, wy, g); rot(dir, g, Vc);
     // the cell's eigensystem along dir (FP32: from the base the slope stage kept)
     Eig<R> e;
@@ -216,7 +215,14 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
         EigBase<R> eb;
         if (!eigen_base(Vc[0], Vc[4], s.V[GC][wy][wx + XO], eb)) set_err(a.err, ERR_SOUND);
         eigen_dir(eb, Vc[1], e);
-        if (!KeepSig<R>::value) sigma_other(a, s, dir, wx, wy, g, eb, sgo);
+        if (!KeepSig<R>::value) {
+            // sigma of the other direction at this cell, times dt/2 dx_t, parked
+            // in this thread's face-state slots until the transverse correction
+            R sgo[6];
+            sigma_other(a, s, dir, wx, wy, g, eb, sgo);
+#pragma unroll
+            for (int k = 0; k < 6; k++) s.W[k][t] = hdtt * sgo[k];
+        }
     }
     if (EXT && a.prm.order == 2) {
         // MUSCL-Hancock: the cell's own slope, flattening and tracing in one step
@@ -278,9 +284,9 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
     // transverse flux of the other direction at this cell (from the analysis stage)
 #pragma unroll
     for (int k = 0; k < 6; k++) {
-        R sg = KeepSig<R>::value ? s.SG[k][dbi] : sgo[k];
-        Wm[k] = Wm[k] - hdtt * sg;
-        Wp[k] = Wp[k] - hdtt * sg;
+        const R corr = KeepSig<R>::value ? hdtt * s.SG[k][dbi] : s.W[k][t];
+        Wm[k] = Wm[k] - corr;
+        Wp[k] = Wp[k] - corr;
     }
     if (Wm[0] < R(0) || Wp[0] < R(0) || Wm[4] < R(0) || Wp[4] < R(0)) {
         win6(s, wx, wy, g);
