@@ -358,9 +358,11 @@ class HydroDevice:
             p, n = i32(leaves)
             _check(lib.fxb_amr_unpack_leaves(p, n, ctypes.c_void_p(buf.data_ptr())))
 
+        import torch.distributed as dist
         dev = torch.device("cuda", torch.cuda.current_device())
         stream = torch.cuda.ExternalStream(lib.fxb_stream(), device=dev)
-        return AmrExchange(dec, lib.fxb_amr_leaf_doubles(), pack, unpack, device=dev, stream=stream)
+        host = dist.is_initialized() and dist.get_backend() != "nccl"     # e.g. gloo: messages via pinned host copies
+        return AmrExchange(dec, lib.fxb_amr_leaf_doubles(), pack, unpack, device=dev, stream=stream, host_stage=host)
 
     def unpack_leaves(self, leaves, buf):
         """fxb_amr_unpack_leaves: store the interiors in the message `buf` (a
@@ -484,7 +486,7 @@ class HydroDevice:
         rc_ = (ctypes.c_double * nv)(*[float(r[1]) for r in refine_vars])
         dc = (ctypes.c_double * nv)(*[float(r[2]) for r in refine_vars])
         fl = (ctypes.c_double * nv)(*[float(r[3]) for r in refine_vars])
-        n = self.unk_shape[0]
+        n = self.mesh.nleaf if self.mesh is not None else self.unk_shape[0]   # every leaf, split mesh or not
         flags = np.zeros(n, dtype=np.int32)
         err = np.zeros(n)
         _check(self.lib.fxb_mark_refine_derefine(nv, iv, rc_, dc, fl, int(max_refine),
@@ -523,11 +525,20 @@ class HydroDevice:
         dev = torch.device("cuda", torch.cuda.current_device())
         stream = torch.cuda.ExternalStream(self.lib.fxb_stream(), device=dev)
         most = max(dec.bounds[r + 1] - dec.bounds[r] for r in range(dec.world))
+        host = dist.get_backend() != "nccl"      # e.g. gloo: through pinned host copies
         with torch.cuda.stream(stream):
             mine = torch.empty(most * n, dtype=torch.float64, device=dev)
             self.pack_leaves(dec.owned(), mine)
-            parts = [torch.empty(most * n, dtype=torch.float64, device=dev) for _ in range(dec.world)]
-            dist.all_gather(parts, mine)
+            if host:
+                mine_h = torch.empty(most * n, dtype=torch.float64, pin_memory=True)
+                mine_h.copy_(mine, non_blocking=True)
+                stream.synchronize()
+                parts_h = [torch.empty(most * n, dtype=torch.float64) for _ in range(dec.world)]
+                dist.all_gather(parts_h, mine_h)
+                parts = [p.to(dev, non_blocking=False) for p in parts_h]
+            else:
+                parts = [torch.empty(most * n, dtype=torch.float64, device=dev) for _ in range(dec.world)]
+                dist.all_gather(parts, mine)
             for r in range(dec.world):
                 if r != dec.rank:
                     self.unpack_leaves(dec.owned(r), parts[r])

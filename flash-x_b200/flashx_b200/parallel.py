@@ -395,17 +395,24 @@ class AmrExchange:
     the guard fill, mpi_amr_comm_setup.F90:531): per peer one message with
     the leaves it reads, `leaf_doubles` values each, over
     torch.distributed.batch_isend_irecv (NCCL between GPUs, gloo on CPU).
-    pack(leaves, buf) fills a message, unpack(leaves, buf) stores one."""
+    pack(leaves, buf) fills a message, unpack(leaves, buf) stores one.
+    host_stage: the messages are packed in device memory but cross between
+    the ranks through pinned host copies (a process group whose backend
+    moves host memory, e.g. gloo between processes that share a GPU)."""
 
-    def __init__(self, dec, leaf_doubles, pack, unpack, device=None, stream=None):
+    def __init__(self, dec, leaf_doubles, pack, unpack, device=None, stream=None, host_stage=False):
         self.dec, self.n, self.pack, self.unpack = dec, int(leaf_doubles), pack, unpack
         self.device = device if device is not None else _device()
         self.stream = stream
+        self.host_stage = host_stage
         self.sends, self.recvs = dec.sends(), dec.recvs()
         self.sbuf = {s: torch.empty(len(v) * self.n, dtype=torch.float64, device=self.device)
                      for s, v in self.sends.items()}
         self.rbuf = {s: torch.empty(len(v) * self.n, dtype=torch.float64, device=self.device)
                      for s, v in self.recvs.items()}
+        if host_stage:
+            self.shost = {s: torch.empty(b.numel(), dtype=torch.float64, pin_memory=True) for s, b in self.sbuf.items()}
+            self.rhost = {s: torch.empty(b.numel(), dtype=torch.float64, pin_memory=True) for s, b in self.rbuf.items()}
 
     def __call__(self):
         if self.dec.world == 1:
@@ -414,11 +421,20 @@ class AmrExchange:
         with ctx:
             for s, leaves in self.sends.items():
                 self.pack(leaves, self.sbuf[s])
-            ops = [dist.P2POp(dist.isend, self.sbuf[s], s) for s in sorted(self.sends)]
-            ops += [dist.P2POp(dist.irecv, self.rbuf[s], s) for s in sorted(self.recvs)]
+            tx, rx = self.sbuf, self.rbuf
+            if self.host_stage:
+                for s in self.sends:
+                    self.shost[s].copy_(self.sbuf[s], non_blocking=True)
+                torch.cuda.current_stream().synchronize()
+                tx, rx = self.shost, self.rhost
+            ops = [dist.P2POp(dist.isend, tx[s], s) for s in sorted(self.sends)]
+            ops += [dist.P2POp(dist.irecv, rx[s], s) for s in sorted(self.recvs)]
             if ops:
                 for w in dist.batch_isend_irecv(ops):
                     w.wait()
+            if self.host_stage:
+                for s in self.recvs:
+                    self.rbuf[s].copy_(self.rhost[s], non_blocking=True)
             for s, leaves in self.recvs.items():
                 self.unpack(leaves, self.rbuf[s])
 

@@ -124,3 +124,109 @@ def test_leaf_messages_round_trip(need_gpu):
     with pytest.raises(FlashXError):
         dev.pack_leaves([mesh.nleaf], buf)
     dev.close()
+
+
+def _split_worker(rank, world, port, outdir):
+    import os
+    import sys
+    import traceback
+    root_dir = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path[:0] = [root_dir, os.path.join(root_dir, "flash-x_b200"), os.path.join(root_dir, "tests")]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK="0", FXB_AMR_PERSISTENT="0", FXB_AMR_TUNE="0")
+    result = "ok"
+    try:
+        import torch
+        from flashx_b200 import parallel as P
+        torch.cuda.set_device(0)
+        P.init_from_env("gloo", timeout_s=120)
+        root, hp, mesh, unk = _split_case()
+        dec = AmrDecomposition(mesh, world, rank)
+        dev = HydroDevice(root, hp, mesh=mesh, amr_split=dec)
+        dev.attach_unk(unk[dec.owned()].copy())
+        dt = 0.5 * P.allreduce_min(dev.Hydro_computeDt())
+        for _ in range(3):
+            dev.Hydro(0.0, dt, dt)
+        dtn = P.allreduce_min(dev.Hydro_computeDt())
+        out = np.zeros(dev.unk_shape)
+        dev.sync_to_host(out)
+        integ = P.allreduce_sum(dev.integrals())
+        flags, _ = dev.Grid_markRefineDerefine([("dens", 0.3, 0.05, 0.01)], 3)
+        m1 = dev.Grid_updateRefinement(flags, lrefine_max=3)
+        dev.Hydro(0.0, dt, dt)
+        out2 = np.zeros(dev.unk_shape)
+        dev.sync_to_host(out2)
+        np.savez(os.path.join(outdir, f"rank{rank}.npz"), own=dec.owned(), out=out, dt=dt, dtn=dtn,
+                 integ=np.array(integ), flags=flags, own2=dev.split.owned(), out2=out2,
+                 levels=m1.levels, bcoords=m1.bcoords)
+        dev.close()
+    except Exception as e:  # noqa: BLE001
+        result = f"error: {type(e).__name__}: {e}\n{traceback.format_exc()}"
+    with open(os.path.join(outdir, f"result{rank}.txt"), "w") as f:
+        f.write(result)
+    try:
+        import torch.distributed as dist
+        if dist.is_initialized() and result == "ok":
+            dist.destroy_process_group()
+    except Exception:
+        pass
+
+
+def _split_case():
+    hp = HydroParams(order=3)
+    root = Geometry(3, 8, 8, 8, 6, 6, 6, bc=(BC_PERIODIC,) * 6)
+    mesh, unk = A.levelset_problem(root, hp, 2)
+    return root, hp, mesh, unk
+
+
+def test_two_ranks_on_one_gpu_reproduce_the_whole_mesh(oracle, need_gpu):
+    """Two ranks, as two processes sharing the GPU and a gloo group (their
+    leaf messages cross through pinned host copies; no kernel of one waits for
+    the other): each steps its Morton half with the real per-step exchange,
+    then both mark and regrid together and step again.  Every rank's own
+    leaves, the reduced dt and integrals and the marks equal the whole-mesh
+    oracle's, bit for bit (integrals to summation order)."""
+    import multiprocessing as mp
+    import socket
+    import tempfile
+    from flashx_b200.params import DENS as _D
+    world = 2
+    out = tempfile.mkdtemp()
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_split_worker, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=600)
+        assert not p.is_alive(), "a rank did not finish"
+    import os
+    for r in range(world):
+        with open(os.path.join(out, f"result{r}.txt")) as f:
+            assert f.read() == "ok"
+    ranks = [np.load(os.path.join(out, f"rank{r}.npz")) for r in range(world)]
+    root, hp, mesh, unk = _split_case()
+    p = oracle.make_params(root.as_dict(), hp)
+    am = oracle.Amr(p, mesh.levels, mesh.bcoords)
+    dt = 0.5 * am.compute_dt(unk)
+    assert all(float(d["dt"]) == dt for d in ranks)
+    u = unk.copy()
+    for _ in range(3):
+        am.hydro_step(u, dt)
+    assert all(float(d["dtn"]) == am.compute_dt(u) for d in ranks)
+    for d in ranks:
+        g, r = _interior(root, d["out"]), _interior(root, u)[d["own"]]
+        assert np.array_equal(g, r)
+        assert np.allclose(d["integ"], am.integrals(u), rtol=1e-12, atol=0)
+    flags, _ = am.mark_refine_derefine(u, [(_D, 0.3, 0.05, 0.01)], 3)
+    assert all(np.array_equal(d["flags"], flags) for d in ranks)
+    m1 = A.refine_derefine(mesh, flags, 1, 3)
+    assert all(np.array_equal(d["levels"], m1.levels) and np.array_equal(d["bcoords"], m1.bcoords) for d in ranks)
+    am1 = oracle.Amr(p, m1.levels, m1.bcoords)
+    u1 = am.regrid(u, am1)
+    am1.hydro_step(u1, dt)
+    for d in ranks:
+        assert np.array_equal(_interior(root, d["out2"]), _interior(root, u1)[d["own2"]])
