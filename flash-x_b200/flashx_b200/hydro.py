@@ -389,9 +389,11 @@ class HydroDevice:
         def unpack(recv_lo, recv_hi):
             _check(lib.fxb_halo_unpack(ptr(recv_lo), ptr(recv_hi)))
 
+        import torch.distributed as dist
         dev = torch.device("cuda", torch.cuda.current_device())
         stream = torch.cuda.ExternalStream(lib.fxb_stream(), device=dev)
-        return HaloExchange(slab, lib.fxb_halo_doubles(1), pack, unpack, device=dev, stream=stream)
+        host = dist.is_initialized() and dist.get_backend() != "nccl"     # e.g. gloo: planes via pinned host copies
+        return HaloExchange(slab, lib.fxb_halo_doubles(1), pack, unpack, device=dev, stream=stream, host_stage=host)
 
     def fill_halos(self):
         """Grid_fillGuardCells between ranks: the halo planes from the

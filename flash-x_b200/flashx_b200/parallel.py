@@ -213,14 +213,21 @@ class HaloExchange:
     are matched per neighbour pair in issue order, downward planes (tag 0)
     before upward planes (tag 1), so two ranks that are each other's lower
     and upper neighbour (a periodic pair) pair them correctly.  A rank that
-    is its own neighbour packs straight into its receive buffers."""
+    is its own neighbour packs straight into its receive buffers.
+    host_stage: the planes are packed in device memory but cross between the
+    ranks through pinned host copies (a process group whose backend moves
+    host memory, e.g. gloo between processes that share a GPU)."""
 
-    def __init__(self, dec, doubles_per_plane, pack, unpack, device="cpu", stream=None):
+    def __init__(self, dec, doubles_per_plane, pack, unpack, device="cpu", stream=None, host_stage=False):
         self.dec, self.pack, self.unpack, self.stream = dec, pack, unpack, stream
         buf = lambda n: torch.empty(n * doubles_per_plane, dtype=torch.float64, device=device) if n else None
         self.send_lo, self.send_hi = buf(dec.send_lo), buf(dec.send_hi)
         self.recv_lo, self.recv_hi = buf(dec.halo_lo), buf(dec.halo_hi)
         self.own_neighbour = dec.nranks == 1
+        self.host_stage = host_stage and not self.own_neighbour
+        if self.host_stage:
+            pin = lambda b: torch.empty(b.numel(), dtype=torch.float64, pin_memory=True) if b is not None else None
+            self.h = {k: pin(getattr(self, k)) for k in ("send_lo", "send_hi", "recv_lo", "recv_hi")}
 
     def __call__(self):
         d = self.dec
@@ -237,17 +244,28 @@ class HaloExchange:
             self.pack(self.recv_hi, d.send_lo, self.recv_lo, d.send_hi)
         else:
             self.pack(self.send_lo, d.send_lo, self.send_hi, d.send_hi)
+            b = {k: getattr(self, k) for k in ("send_lo", "send_hi", "recv_lo", "recv_hi")}
+            if self.host_stage:
+                for k in ("send_lo", "send_hi"):
+                    if b[k] is not None:
+                        self.h[k].copy_(b[k], non_blocking=True)
+                torch.cuda.current_stream().synchronize()
+                b = self.h
             ops = []
             if d.halo_lo:
-                ops.append(dist.P2POp(dist.isend, self.send_lo, d.lo_rank, tag=0))
+                ops.append(dist.P2POp(dist.isend, b["send_lo"], d.lo_rank, tag=0))
             if d.halo_hi:
-                ops.append(dist.P2POp(dist.irecv, self.recv_hi, d.hi_rank, tag=0))
+                ops.append(dist.P2POp(dist.irecv, b["recv_hi"], d.hi_rank, tag=0))
             if d.halo_hi:
-                ops.append(dist.P2POp(dist.isend, self.send_hi, d.hi_rank, tag=1))
+                ops.append(dist.P2POp(dist.isend, b["send_hi"], d.hi_rank, tag=1))
             if d.halo_lo:
-                ops.append(dist.P2POp(dist.irecv, self.recv_lo, d.lo_rank, tag=1))
+                ops.append(dist.P2POp(dist.irecv, b["recv_lo"], d.lo_rank, tag=1))
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
+            if self.host_stage:
+                for k in ("recv_lo", "recv_hi"):
+                    if b[k] is not None:
+                        getattr(self, k).copy_(b[k], non_blocking=True)
         self.unpack(self.recv_lo, self.recv_hi)
 
 

@@ -127,3 +127,86 @@ def test_slab_with_oracle_neighbour_fp64(name, rank, oracle, need_gpu):
     np.testing.assert_array_equal(_inner(geom, out), _inner(geom, whole[b0:b1]))
     assert nbr.checked >= NSTEPS
     dev.close()
+
+
+def _slab_worker(name, rank, world, port, outdir):
+    import os
+    import sys
+    import traceback
+    root_dir = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path[:0] = [root_dir, os.path.join(root_dir, "flash-x_b200"), os.path.join(root_dir, "tests"),
+                    os.path.join(root_dir, "oracle")]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK="0")
+    result = "ok"
+    try:
+        import torch
+        from flashx_b200 import parallel as P
+        from flashx_b200.hydro import driver_dt
+        torch.cuda.set_device(0)
+        P.init_from_env("gloo", timeout_s=120)
+        geom, hp, unk = C.case(name)
+        dec = SlabDecomposition(geom, world, rank)
+        b0, b1 = dec.block_range()
+        dev = HydroDevice(geom, hp, "fp64", slab=dec)
+        dev.attach_unk(np.ascontiguousarray(unk[b0:b1]))
+        dt = dt_old = 0.5 * P.allreduce_min(dev.Hydro_computeDt())
+        dts = [dt]
+        for _ in range(NSTEPS):
+            dev.Hydro(0.0, dt, dt_old)
+            dt_old, dt = dt, driver_dt(P.allreduce_min(dev.Hydro_computeDt()), dt, hp)
+            dts.append(dt)
+        out = np.zeros(dev.unk_shape)
+        dev.sync_to_host(out)
+        integ = P.allreduce_sum(dev.integrals())
+        np.savez(os.path.join(outdir, f"{name}{rank}.npz"), out=out, b0=b0, b1=b1, dts=np.array(dts),
+                 integ=np.array(integ))
+        dev.close()
+    except Exception as e:  # noqa: BLE001
+        result = f"error: {type(e).__name__}: {e}\n{traceback.format_exc()}"
+    with open(os.path.join(outdir, f"{name}{rank}.txt"), "w") as f:
+        f.write(result)
+    try:
+        import torch.distributed as dist
+        if dist.is_initialized() and result == "ok":
+            dist.destroy_process_group()
+    except Exception:
+        pass
+
+
+@pytest.mark.parametrize("name", ["kh2d", "sod2d", "rt3d"])
+def test_two_slabs_on_one_gpu_match_whole_grid(name, oracle, need_gpu):
+    """Two ranks, as two processes sharing the GPU and a gloo group (their
+    halo planes cross through pinned host copies; no kernel of one waits for
+    the other), each stepping its slab with the real exchange (KH: each rank
+    is both neighbours of the other across the periodic axis): the slabs, the
+    reduced dt sequence and integrals equal the oracle on the whole grid."""
+    import multiprocessing as mp
+    import os
+    import socket
+    import tempfile
+    world = 2
+    out = tempfile.mkdtemp()
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_slab_worker, args=(name, r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=600)
+        assert not p.is_alive(), "a rank did not finish"
+    for r in range(world):
+        with open(os.path.join(out, f"{name}{r}.txt")) as f:
+            assert f.read() == "ok"
+    geom, hp, unk = C.case(name)
+    whole, dts = C.whole_run(oracle, geom, hp, unk, NSTEPS)
+    ref = oracle.integrals(oracle.make_params(geom.as_dict(), hp), whole)
+    for r in range(world):
+        d = np.load(os.path.join(out, f"{name}{r}.npz"))
+        assert list(d["dts"]) == dts
+        b0, b1 = int(d["b0"]), int(d["b1"])
+        np.testing.assert_array_equal(_inner(geom, d["out"])[..., C.DEV_VARS], _inner(geom, whole[b0:b1])[..., C.DEV_VARS])
+        np.testing.assert_allclose(d["integ"], ref, rtol=1e-12, atol=1e-12)
