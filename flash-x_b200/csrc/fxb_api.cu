@@ -782,6 +782,14 @@ extern "C" int fxb_init_slab(const fxb_params *params, const fxb_domain *domain,
     CK(cudaMemsetAsync(L.rate_max, 0, sizeof(unsigned long long), L.stream));
     L.npartials = 1024;
     CK(cudaMalloc(&L.partials, sizeof(double) * (L.npartials * 7 + 8)));
+    if (q.use_gravity) {   // gravity's face values, once, in each precision's kernels' arithmetic
+        launch_gravity_faces_fp64(q, L.partials, L.stream);
+        launch_gravity_faces_mixed(q, L.partials + 6, L.stream);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(&q.gface[0][0], L.partials, sizeof(q.gface), cudaMemcpyDeviceToHost, L.stream));
+        CK(cudaMemcpyAsync(&q.gfacef[0][0], L.partials + 6, sizeof(q.gfacef), cudaMemcpyDeviceToHost, L.stream));
+        CK(cudaStreamSynchronize(L.stream));
+    }
     if (p.flattening) {
         size_t rsz0 = p.precision == FXB_MIXED ? sizeof(float) : sizeof(double);
         size_t npad = (size_t)(L.nx + 2) * (L.ny + 2) * (d.ndim == 3 ? L.nz + 2 : 1);

@@ -37,6 +37,12 @@ struct DevParams {
     double hybrid_kappa;
     int nspec;                 // advected mass fractions (species and mass scalars; uniform grids)
     int shock_detect;          // the SHOK flag before each step (uniform grids)
+    // Face values (left, right) of the constant gravity component along each
+    // sweep direction after the reconstruction (gravity_faces), in FP64 and
+    // in FP32: the same for every cell, so fxb_init computes them once with
+    // the arithmetic of the kernels that use them, instead of every cell.
+    double gface[3][2];
+    float gfacef[3][2];
 };
 
 // ---- precision helpers ---------------------------------------------------
@@ -623,6 +629,18 @@ __device__ __forceinline__ void gravity_faces(const DevParams &prm, R g, R &gl, 
     if (R(6) * (Rr - L) * (C - R(.5) * (L + Rr)) > (Rr - L) * (Rr - L)) L = R(3) * C - R(2) * Rr;
     if (R(6) * (Rr - L) * (C - R(.5) * (L + Rr)) < -((Rr - L) * (Rr - L))) Rr = R(3) * C - R(2) * L;
     gl = L; gr = Rr;
+}
+// gravity_faces of direction d as computed at initialisation
+template <class R> __device__ __forceinline__ void gravity_face_values(const DevParams &prm, int d, R &gl, R &gr);
+template <> __device__ __forceinline__ void gravity_face_values<double>(const DevParams &prm, int d, double &gl,
+                                                                        double &gr)
+{ gl = prm.gface[d][0]; gr = prm.gface[d][1]; }
+template <> __device__ __forceinline__ void gravity_face_values<float>(const DevParams &prm, int d, float &gl,
+                                                                      float &gr)
+{ gl = prm.gfacef[d][0]; gr = prm.gfacef[d][1]; }
+template <class R> __global__ void gravity_faces_kernel(DevParams prm, R *out)
+{
+    for (int d = 0; d < 3; d++) gravity_faces(prm, R(prm.grav[d]), out[2 * d], out[2 * d + 1]);
 }
 
 // ---- Riemann solvers (hy_HLLC.F90:64-335, hy_HLL.F90:64-182) ---------------

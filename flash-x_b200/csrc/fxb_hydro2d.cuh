@@ -295,7 +295,7 @@ __device__ __forceinline__ void states_stage(const Args2D &a, Smem2D<R> &s, int 
     }
     if (EXT && a.prm.use_gravity) {   // hy_getRiemannState.F90:843-885, global axes after unrot
         R gl, gr;
-        gravity_faces(a.prm, R(a.prm.grav[dir]), gl, gr);
+        gravity_face_values(a.prm, dir, gl, gr);
 #pragma unroll
         for (int q = 0; q < 3; q++) {
             R gp = q == dir ? gr : R(a.prm.grav[q]);

@@ -554,7 +554,7 @@ __device__ __forceinline__ void face_states_finish(const Args3D &a, const Ctx3<R
     if (a.prm.use_gravity) {   // hy_getRiemannState.F90:843-885
         const R hdt = R(0.5 * dt);
         R gl, gr;
-        gravity_faces(a.prm, R(a.prm.grav[d]), gl, gr);
+        gravity_face_values(a.prm, d, gl, gr);
 #pragma unroll
         for (int q = 0; q < 3; q++) {
             R gp = q == d ? gr : R(a.prm.grav[q]);

@@ -3,6 +3,8 @@
 #include "fxb_amr_persist.cuh"
 #include "fxb_species.cuh"
 namespace fxb {
+void launch_gravity_faces_fp64(const DevParams &p, void *out, cudaStream_t s)
+{ gravity_faces_kernel<double><<<1, 1, 0, s>>>(p, (double *)out); }
 cudaError_t setup_hydro3d_fp64() { return cudaSuccess; }
 void launch_hydro3d_fp64(const Args3D &a, cudaStream_t s) { launch_hydro3d_t<double>(a, s); }
 void launch_amr3d_fluxes_fp64(const Args3D &a, int entries, int which, cudaStream_t s)

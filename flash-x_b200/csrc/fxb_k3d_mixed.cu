@@ -4,6 +4,8 @@
 #include "fxb_amr_persist.cuh"
 #include "fxb_species.cuh"
 namespace fxb {
+void launch_gravity_faces_mixed(const DevParams &p, void *out, cudaStream_t s)
+{ gravity_faces_kernel<float><<<1, 1, 0, s>>>(p, (float *)out); }
 cudaError_t setup_hydro3d_mixed() { return cudaSuccess; }
 void launch_hydro3d_mixed(const Args3D &a, cudaStream_t s) { launch_hydro3d_t<float>(a, s); }
 void launch_amr3d_fluxes_mixed(const Args3D &a, int entries, int which, cudaStream_t s)

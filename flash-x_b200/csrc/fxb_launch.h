@@ -13,6 +13,9 @@ cudaError_t setup_hydro2d_mixed();
 void launch_hydro2d_fp64(const Args2D &a, dim3 grid, cudaStream_t s);
 void launch_hydro2d_mixed(const Args2D &a, dim3 grid, cudaStream_t s);
 cudaError_t setup_hydro3d_fp64();
+// gravity_faces of the three directions into out[6] (double, float)
+void launch_gravity_faces_fp64(const DevParams &p, void *out, cudaStream_t s);
+void launch_gravity_faces_mixed(const DevParams &p, void *out, cudaStream_t s);
 cudaError_t setup_hydro3d_mixed();
 void launch_hydro3d_fp64(const Args3D &a, cudaStream_t s);
 void launch_hydro3d_mixed(const Args3D &a, cudaStream_t s);
