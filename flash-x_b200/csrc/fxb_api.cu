@@ -65,6 +65,9 @@ struct Lib {
     size_t pack_host_doubles = 0;
     double *pack_dev = nullptr;    // packed selected variables (uniform grid)
     size_t pack_dev_doubles = 0;
+    const void *mapped_host = nullptr;   // caller's UNK page-locked for the interior transfers
+    size_t mapped_bytes = 0;
+    bool mapped_registered = false;      // locked by the library (released at finalize)
     int *pmap_dev = nullptr;       // device variable -> place in a packed cell vector
     const double *unk_attached = nullptr;
     bool attached = false;
@@ -629,6 +632,7 @@ void free_all()
         if (L.w3[d]) cudaFree(L.w3[d]);
         if (L.f3[d]) cudaFree(L.f3[d]);
     }
+    if (L.mapped_registered) cudaHostUnregister(const_cast<void *>(L.mapped_host));
     if (L.ev0) cudaEventDestroy(L.ev0);
     if (L.ev1) cudaEventDestroy(L.ev1);
     if (L.stream) cudaStreamDestroy(L.stream);
@@ -1096,6 +1100,101 @@ extern "C" int fxb_sync_to_host(double *unk_host)
     CK(cudaStreamSynchronize(L.stream));
     L.counts[FXB_COUNT_GC_FILLS]++;
     L.counts[FXB_COUNT_GC_DOUBLES] += L.unk_doubles;
+    return check_err_word();
+}
+
+// ---- interior transfers --------------------------------------------------
+// The step reads and writes the device variables (and species) of block
+// interiors only.  fxb_put_interior / fxb_get_interior move the interior
+// rows of every block (nxb cells x nunk slots, contiguous in UNK) between
+// the caller's UNK, page-locked at the first call, and the device UNK mirror
+// with strided copies on the copy engine; the mirror's rows are then
+// unpacked into the state, or packed from it, by the attach and sync kernels.
+namespace {
+// page-lock unk_host (bytes long) unless it already is; a different UNK
+// releases the previous one
+int lock_host_unk(const void *unk_host, size_t bytes)
+{
+    if (L.mapped_host == unk_host && L.mapped_bytes == bytes) return FXB_OK;
+    if (L.mapped_registered) cudaHostUnregister(const_cast<void *>(L.mapped_host));
+    L.mapped_host = nullptr;
+    L.mapped_bytes = 0;
+    L.mapped_registered = false;
+    cudaPointerAttributes at{};
+    const bool locked = cudaPointerGetAttributes(&at, unk_host) == cudaSuccess && at.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    if (!locked) {
+        CK(cudaHostRegister(const_cast<void *>(unk_host), bytes, cudaHostRegisterDefault));
+        L.mapped_registered = true;
+    }
+    L.mapped_host = unk_host;
+    L.mapped_bytes = bytes;
+    return FXB_OK;
+}
+
+// the interior rows of every block, between the caller's UNK and the device
+// mirror: one 3-D copy over all blocks in 2-D (their rows are evenly
+// spaced), one per block in 3-D (the k guard planes separate the blocks)
+int copy_interior_rows(double *dst, const double *src, cudaMemcpyKind kind)
+{
+    const UnkGeom g = unk_geom();
+    const size_t pitch = sizeof(double) * g.nunk * g.nig;
+    cudaMemcpy3DParms p{};
+    p.srcPtr = make_cudaPitchedPtr(const_cast<double *>(src), pitch, pitch, g.njg);
+    p.dstPtr = make_cudaPitchedPtr(dst, pitch, pitch, g.njg);
+    p.kind = kind;
+    const size_t x0 = sizeof(double) * g.nunk * g.ng, w = sizeof(double) * g.nunk * g.nxb;
+    if (g.ndim == 2) {
+        p.srcPos = p.dstPos = make_cudaPos(x0, g.ng, 0);
+        p.extent = make_cudaExtent(w, g.nyb, L.nblk);
+        CK(cudaMemcpy3DAsync(&p, L.stream));
+        return FXB_OK;
+    }
+    p.extent = make_cudaExtent(w, g.nyb, g.nzb);
+    for (int b = 0; b < L.nblk; b++) {
+        p.srcPos = p.dstPos = make_cudaPos(x0, g.ng, (size_t)b * g.nkg + g.ng);
+        CK(cudaMemcpy3DAsync(&p, L.stream));
+    }
+    return FXB_OK;
+}
+} // namespace
+
+extern "C" int fxb_put_interior(const double *unk_host)
+{
+    if (!unk_host) return fail(FXB_EARG, "fxb_put_interior: null UNK");
+    if (!L.attached) return fail(FXB_EARG, "fxb_put_interior: call fxb_attach_unk first");
+    if (amr_active()) return fxb_attach_unk(unk_host);
+    int rc = lock_host_unk(unk_host, sizeof(double) * L.unk_doubles);
+    if (!rc) rc = copy_interior_rows(L.unk_dev, unk_host, cudaMemcpyHostToDevice);
+    if (rc) return rc;
+    UnkGeom g = unk_geom();
+    unk_to_state_kernel<<<1184, 256, 0, L.stream>>>(L.unk_dev, L.buf[L.cur], g, L.bcoord, L.dmap_dev, L.nblk);
+    if (L.ns)
+        unk_to_spec_kernel<<<1184, 256, 0, L.stream>>>(L.unk_dev, L.spb[L.cur], g, L.bcoord, L.sslot_dev, L.ns, L.nblk);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(L.stream));
+    state_changed(false);
+    L.shok_valid = false;         // the host's SHOK stands until the next step
+    return check_err_word();
+}
+
+extern "C" int fxb_get_interior(double *unk_host)
+{
+    if (!unk_host) return fail(FXB_EARG, "fxb_get_interior: null UNK");
+    if (!L.attached) return fail(FXB_EARG, "fxb_get_interior: no UNK attached");
+    if (amr_active()) return fxb_sync_to_host(unk_host);
+    int rc = lock_host_unk(unk_host, sizeof(double) * L.unk_doubles);
+    if (rc) return rc;
+    UnkGeom g = unk_geom();
+    state_to_unk_kernel<<<1184, 256, 0, L.stream>>>(L.buf[L.cur], L.unk_dev, g, L.bcoord, L.dmap_dev, L.nblk);
+    if (L.ns)
+        spec_to_unk_kernel<<<1184, 256, 0, L.stream>>>(L.spb[L.cur], L.unk_dev, g, L.bcoord, L.sslot_dev, L.ns, L.nblk);
+    if (L.shok && L.shok_valid && L.shock_slot >= 0)
+        shok_to_unk_kernel<<<1184, 256, 0, L.stream>>>(L.shok, L.unk_dev, g, L.bcoord, L.nblk, L.shock_slot);
+    CK(cudaGetLastError());
+    rc = copy_interior_rows(unk_host, L.unk_dev, cudaMemcpyDeviceToHost);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(L.stream));
     return check_err_word();
 }
 

@@ -32,7 +32,7 @@ LEAF_MSG_VARS = ("dens", "velx", "vely", "velz", "pres", "gamc", "game", "eint",
 # entry points declared in include/flashx_b200.h
 ABI_SYMBOLS = ("fxb_init", "fxb_register_blocks", "fxb_attach_unk", "fxb_fill_guardcells",
                "fxb_hydro_step", "fxb_compute_dt", "fxb_advance", "fxb_eos", "fxb_sync_to_host",
-               "fxb_sync_from_host", "fxb_integrals", "fxb_integrals_noalloc", "fxb_mark_refine_derefine",
+               "fxb_sync_from_host", "fxb_put_interior", "fxb_get_interior", "fxb_integrals", "fxb_integrals_noalloc", "fxb_mark_refine_derefine",
                "fxb_last_timing", "fxb_stream", "fxb_tuning", "fxb_last_error", "fxb_finalize",
                "fxb_init_slab", "fxb_halo_doubles", "fxb_halo_pack", "fxb_halo_unpack", "fxb_regrid",
                "fxb_refine_derefine", "fxb_counters", "fxb_init_species", "fxb_amr_set_roles",
@@ -117,6 +117,8 @@ def load_library(path=LIB_PATH):
     L.fxb_eos.argtypes = []
     L.fxb_sync_to_host.argtypes = [D]
     L.fxb_sync_from_host.argtypes = [D]
+    L.fxb_put_interior.argtypes = [D]
+    L.fxb_get_interior.argtypes = [D]
     L.fxb_integrals.argtypes = [D]
     L.fxb_integrals_noalloc.argtypes = [ctypes.c_void_p] * 6 + [ctypes.c_long, ctypes.c_double,
                                                                  ctypes.c_void_p, ctypes.c_void_p]
@@ -418,6 +420,29 @@ class HydroDevice:
         _check(self.lib.fxb_sync_to_host(_dp(unk)))
         return unk
 
+    def put_interior(self, unk=None):
+        """Replace the device state's block interiors with the host UNK's
+        (fxb_put_interior: the hydro variables and mass fractions only)."""
+        unk = self.unk if unk is None else unk
+        if unk is None or unk.shape != self.unk_shape:
+            raise ValueError(f"put_interior needs a UNK of shape {self.unk_shape}")
+        self._mapped = unk          # the library maps this array's pages: keep it alive
+        _check(self.lib.fxb_put_interior(_dp(unk)))
+
+    def get_interior(self, unk=None):
+        """Write the device state's block interiors into the host UNK
+        (fxb_get_interior); its guard cells keep their values, the other
+        slots of interior cells get the values last read from the host.
+        AMR meshes copy whole blocks (sync_to_host)."""
+        unk = self.unk if unk is None else unk
+        if unk is None or unk.shape != self.unk_shape:
+            raise ValueError(f"get_interior needs a UNK of shape {self.unk_shape}")
+        if self.mesh is not None:
+            return self.sync_to_host(unk)
+        self._mapped = unk
+        _check(self.lib.fxb_get_interior(_dp(unk)))
+        return unk
+
     # ---- the reference interface
     def Grid_fillGuardCells(self, unk=None, mask=None, doEos=True):
         """Fill the guard cells (and interiors) of the host UNK from the device.
@@ -566,6 +591,7 @@ class HydroDevice:
 
     def close(self):
         self.lib.fxb_finalize()
+        self._mapped = None
 
 
 def driver_dt(dt_cfl, dt_old, hp: HydroParams):

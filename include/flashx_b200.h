@@ -219,6 +219,28 @@ int fxb_eos(void);
 int fxb_sync_to_host(double *unk_host);
 /* Re-read unk_host after a host-side write (init, restart, regrid). */
 int fxb_sync_from_host(const double *unk_host);
+/* Interior transfers, for drivers whose host units read or write UNK
+ * between hydro steps.  Hydro fills the guard cells from the interiors
+ * before it reconstructs (levelFlux/Hydro.F90:161) and hy_unsplitUpdate
+ * writes only the cells inside blkLimits (hy_unsplitUpdate.F90:84-131), so a
+ * step depends on, and changes, block interiors only.  fxb_put_interior
+ * replaces the interiors of the device state with unk_host's (the ten hydro
+ * variables dens, velx, vely, velz, pres, gamc, game, eint, ener, temp and
+ * the advected mass fractions of fxb_init_species); fxb_get_interior writes
+ * the current interiors of the same variables, and SHOK when the shock
+ * detector ran, into unk_host and leaves its guard cells as they are.  Both
+ * move whole interior rows (nxb cells x nunk slots, contiguous in UNK) with
+ * strided copies on the copy engine, so the other slots of interior cells
+ * receive the values last read from the host (fxb_attach_unk,
+ * fxb_sync_from_host or fxb_put_interior): the caller changes them after
+ * fxb_get_interior, not between a put and the next get.  The first call
+ * page-locks unk_host (unless it already is); there is no host-side copy.
+ * unk_host stays locked until fxb_finalize or a call with another UNK and
+ * must stay allocated until then.  fxb_put_interior needs a prior
+ * fxb_attach_unk (FXB_EARG otherwise).  AMR meshes move whole blocks, as
+ * fxb_sync_from_host and fxb_sync_to_host do. */
+int fxb_put_interior(const double *unk_host);
+int fxb_get_interior(double *unk_host);
 /* Volume integrals: mass, x/y/z momentum, total, internal, kinetic energy. */
 int fxb_integrals(double out[7]);
 /* Guard-cell exchange between slabs (UG/Grid_fillGuardCells.F90:261-306 and

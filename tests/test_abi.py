@@ -125,6 +125,10 @@ def test_calls_before_init_are_rejected():
     assert lib.fxb_compute_dt(ctypes.byref(out), None) == H.FXB_EARG
     assert lib.fxb_hydro_step(0.0, 1e-3, 1e-3) == H.FXB_EARG
     assert lib.fxb_eos() == H.FXB_EARG
+    buf = (ctypes.c_double * 16)()
+    for f in (lib.fxb_put_interior, lib.fxb_get_interior):
+        assert f(None) == H.FXB_EARG
+        assert f(buf) == H.FXB_EARG                  # nothing attached
 
 
 def test_parameter_validation_mirrors_hydro_init():
