@@ -11,6 +11,7 @@ CUDA library (ctypes, plain C ABI).  There is no CPU fallback: if the library
 or a GPU is missing every call raises.
 """
 import ctypes
+import functools
 import os
 
 import numpy as np
@@ -293,7 +294,10 @@ class HydroDevice:
         """species = (nspec, nspecies): that many advected mass fractions in
         UNK slots NUNK .. NUNK + nspec - 1 after the hydro variables (the
         first nspecies renormalised as species, the rest mass scalars)."""
+        global _active
         self.lib = load_library()
+        # the library holds one grid: this device replaces any earlier one
+        self._token = _active = object()
         self.geom, self.hp, self.precision, self.mesh, self.slab = geom, hp, precision, mesh, slab
         nspec = species[0] if species else 0
         self.nunk = NUNK + nspec
@@ -590,8 +594,33 @@ class HydroDevice:
         return ms.value, n.value
 
     def close(self):
-        self.lib.fxb_finalize()
+        """Release the library's grid (fxb_finalize), unless a newer device
+        has replaced this one already."""
+        global _active
+        if _active is self._token:
+            self.lib.fxb_finalize()
+            _active = None
         self._mapped = None
+
+
+_active = None   # token of the HydroDevice whose grid the library holds
+
+
+def _guarded(fn):
+    @functools.wraps(fn)
+    def call(self, *args, **kwargs):
+        if _active is not self._token:
+            raise FlashXError(FXB_EARG, "this HydroDevice was replaced by a newer one or closed "
+                                        "(the library holds one grid at a time)")
+        return fn(self, *args, **kwargs)
+    return call
+
+
+for _name in ("attach_unk", "sync_to_host", "put_interior", "get_interior", "Grid_fillGuardCells", "Hydro",
+              "Hydro_computeDt", "Eos_wrapped", "advance", "integrals", "Grid_markRefineDerefine",
+              "Grid_updateRefinement", "unpack_leaves", "pack_leaves", "fill_halos", "tuning", "counters",
+              "last_timing"):
+    setattr(HydroDevice, _name, _guarded(getattr(HydroDevice, _name)))
 
 
 def driver_dt(dt_cfl, dt_old, hp: HydroParams):

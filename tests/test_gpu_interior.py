@@ -170,3 +170,23 @@ def test_put_interior_needs_an_attached_unk(need_gpu):
     with pytest.raises(FlashXError):
         dev.put_interior(init(geom, hp))
     dev.close()
+
+
+def test_a_replaced_device_refuses_calls(need_gpu):
+    """The library holds one grid: a second HydroDevice replaces the first,
+    whose calls then raise instead of acting on the newer grid, and whose
+    close leaves the newer grid alone."""
+    geom, hp, init = _cases()["kh2d"]
+    unk = init(geom, hp)
+    a = HydroDevice(geom, hp, "fp64")
+    a.attach_unk(unk.copy())
+    b = HydroDevice(geom, hp, "fp64")
+    b.attach_unk(unk.copy())
+    with pytest.raises(FlashXError):
+        a.Hydro_computeDt()
+    a.close()
+    dt = 0.5 * b.Hydro_computeDt()
+    b.Hydro(0.0, dt, dt)
+    b.close()
+    with pytest.raises(FlashXError):
+        b.Hydro_computeDt()
