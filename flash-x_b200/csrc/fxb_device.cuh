@@ -53,11 +53,29 @@ template <class R> __device__ __forceinline__ R rsqrt_(R a);
 template <> __device__ __forceinline__ double rsqrt_<double>(double a) { return sqrt(a); }
 template <> __device__ __forceinline__ float rsqrt_<float>(float a) { return __fsqrt_rn(a); }
 
-// division by a literal constant: exact IEEE division in FP64 (the oracle's
-// operation), multiplication by the rounded reciprocal in the FP32 path
-template <class R> __device__ __forceinline__ R divc(R x, double c);
-template <> __device__ __forceinline__ double divc<double>(double x, double c) { return x / c; }
-template <> __device__ __forceinline__ float divc<float>(float x, double c) { return x * (float)(1.0 / c); }
+// Division by the literal constants 3, 6 and 12 of the PPM formulas.
+// FP64: the correctly rounded quotient x / C (the oracle's operation) without
+// a division, by Markstein's correction step (P. Markstein, "Computation of
+// elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Dev. 34(1), 1990): with y = RN(1/C) within half an ulp of 1/C and q0 within
+// one ulp of x/C, the remainder r = x - C q0 is exact in one FMA and
+// RN(q0 + r y) = RN(x/C).  For C = 3 * 2^k the reciprocal RN(1/C) has a
+// relative error of exactly 2^-54, so q0 = RN(x y) is within one ulp of x/C
+// for every x.  Three dependent FP64 operations replace the division's
+// iteration and its slow-path branch; copysign keeps the sign of a zero
+// quotient (x = -0).  Valid for finite x whose quotient is a normal number
+// (|x| >= 2^-1018): the values that reach it here are differences of
+// primitive slopes and states.  FP32: multiplication by the rounded
+// reciprocal.
+template <int C> __device__ __forceinline__ double divk(double x)
+{
+    static_assert(C == 3 || C == 6 || C == 12, "divk: the correction is shown for 3 * 2^k only");
+    constexpr double y = 1.0 / C;
+    const double q0 = x * y;
+    const double r = fma(-double(C), q0, x);
+    return copysign(fma(r, y, q0), x);
+}
+template <int C> __device__ __forceinline__ float divk(float x) { return x * (float)(1.0 / C); }
 
 // options compiled only into kernel instantiations of their own (template
 // flag EXT), so the default kernels keep their registers: the Roe solver,
@@ -252,9 +270,9 @@ __device__ __forceinline__ void ppm_trace(const Eig<R> &e, R dtn, R hdtn, const 
     // secondary variable EI: initial guess survives (gamc/game are reset to Vc)
     {
         R lmax = fmax2(e.un, R(0));
-        Wp[5] = vecR[5] - lmax * hdtn * (delW[5] - (R(1.0) - divc(lmax * hdtn * R(4.), 3.)) * W6[5]);
+        Wp[5] = vecR[5] - lmax * hdtn * (delW[5] - (R(1.0) - divk<3>(lmax * hdtn * R(4.))) * W6[5]);
         R lmin = -fmin2(e.un, R(0));
-        Wm[5] = vecL[5] + lmin * hdtn * (delW[5] + (R(1.0) - divc(lmin * hdtn * R(4.), 3.)) * W6[5]);
+        Wm[5] = vecL[5] + lmin * hdtn * (delW[5] + (R(1.0) - divk<3>(lmin * hdtn * R(4.))) * W6[5]);
     }
     // tracing over the five waves, HLL-type branch
     Five<R> cA = ldot(e, delW[0], delW[1], delW[2], delW[3], delW[4]);
@@ -300,7 +318,7 @@ __device__ __forceinline__ void ppm_trace(const Eig<R> &e, R dtn, R hdtn, const 
     const R sl[5] = {sLD, sL1, sL2, sL3, sLP}, sr[5] = {sRD, sR1, sR2, sR3, sRP};
 #pragma unroll
     for (int v = 0; v < 5; v++) {
-        R base = Vc[v] + divc(W6[v], 12.);
+        R base = Vc[v] + divk<12>(W6[v]);
         Wm[v] = base + sl[v];
         Wp[v] = base + sr[v];
     }
@@ -317,7 +335,7 @@ __device__ __forceinline__ R flat_tilde(R pm2, R pm1, R pp1, R pp2, R vm1, R vp1
     R dv1 = vp1 - vm1;
     R Sp = (fabs(dp2) > R(1.e-15)) ? rdiv(dp1, dp2) - R(0.75) : R(0.);
     R ft = fmax2(R(0.), fmin2(R(1.), R(10.) * Sp));
-    if ((rdiv(fabs(dp1), fmin2(pm1, pp1)) < divc(R(1.), 3.)) || dv1 > R(0.)) ft = R(0.);
+    if ((rdiv(fabs(dp1), fmin2(pm1, pp1)) < R(1. / 3.)) || dv1 > R(0.)) ft = R(0.);
     return ft;
 }
 // FlatCoeff: the larger FlatTilde of the cell and its upstream neighbour in pressure
@@ -526,8 +544,8 @@ __device__ __forceinline__ void ppm_interfaces(const R *Vm, const R *Vc, const R
 {
 #pragma unroll
     for (int n = 0; n < 6; n++) {
-        vecL[n] = R(.5) * (Vc[n] + Vm[n]) - divc(db0[n] - dbN[n], 6.);
-        vecR[n] = R(.5) * (Vc[n] + Vp[n]) - divc(dbP[n] - db0[n], 6.);
+        vecL[n] = R(.5) * (Vc[n] + Vm[n]) - divk<6>(db0[n] - dbN[n]);
+        vecR[n] = R(.5) * (Vc[n] + Vp[n]) - divk<6>(dbP[n] - db0[n]);
     }
 }
 

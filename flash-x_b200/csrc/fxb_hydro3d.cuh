@@ -962,7 +962,7 @@ __device__ __forceinline__ void update3d_kernel_body(const Args3D &a, const VB v
             double sum = (double)w[(long)PwSlots<R>::wm * nw + wc] + (double)w[(long)PwSlots<R>::wp * nw + wc];
             if (d == 0) pav = 0.5 * sum;
             else if (d == 1) pav = pav * 0.5 + sum * 0.25;
-            else pav = (pav * 4.0 + sum) / 6.0;
+            else pav = divk<6>(pav * 4.0 + sum);
         }
         double inten = 0.;
         if (prm.use_aux_eint) {

@@ -122,8 +122,8 @@ __device__ __forceinline__ void spec_recon(const DevParams &prm, const R s[5], R
         const R dP = lim_minmod(s[3] - s[2], s[4] - s[3]);
         const R d0 = lim_minmod(s[2] - s[1], s[3] - s[2]);
         const R dN = lim_minmod(s[1] - s[0], s[2] - s[1]);
-        Sl = R(0.5) * (Sc + Sm) - divc(d0 - dN, 6.);
-        Sr = R(0.5) * (Sc + Sp) - divc(dP - d0, 6.);
+        Sl = R(0.5) * (Sc + Sm) - divk<6>(d0 - dN);
+        Sr = R(0.5) * (Sc + Sp) - divk<6>(dP - d0);
         Sl = fmax2(fmin2(Sc, Sm), fmin2(fmax2(Sc, Sm), Sl));
         Sr = fmax2(fmin2(Sc, Sp), fmin2(fmax2(Sc, Sp), Sr));
         if ((Sr - Sc) * (Sc - Sl) <= R(0)) { Sr = Sc; Sl = Sc; }
@@ -133,8 +133,8 @@ __device__ __forceinline__ void spec_recon(const DevParams &prm, const R s[5], R
     const R del0 = Sr - Sl;
     const R S6 = R(6.) * (Sc - R(0.5) * (Sr + Sl));
     const R lmn = fmin2(lam, R(0)), lmx = fmax2(lam, R(0));
-    Sl = Sl - lmn * hdtn * (del0 + (R(1.) + divc(lmn * R(4.), 3.) * hdtn) * S6);
-    Sr = Sr - lmx * hdtn * (del0 - (R(1.) - divc(lmx * R(4.), 3.) * hdtn) * S6);
+    Sl = Sl - lmn * hdtn * (del0 + (R(1.) + divk<3>(lmn * R(4.)) * hdtn) * S6);
+    Sr = Sr - lmx * hdtn * (del0 - (R(1.) - divk<3>(lmx * R(4.)) * hdtn) * S6);
     if (prm.flattening) {
         Sl = flat * Sc + (R(1.0) - flat) * Sl;
         Sr = flat * Sc + (R(1.0) - flat) * Sr;
