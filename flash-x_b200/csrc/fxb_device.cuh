@@ -51,7 +51,15 @@ template <> __device__ __forceinline__ double rdiv<double>(double a, double b) {
 template <> __device__ __forceinline__ float rdiv<float>(float a, float b) { return __fdividef(a, b); }
 template <class R> __device__ __forceinline__ R rsqrt_(R a);
 template <> __device__ __forceinline__ double rsqrt_<double>(double a) { return sqrt(a); }
-template <> __device__ __forceinline__ float rsqrt_<float>(float a) { return __fsqrt_rn(a); }
+// FP32 (mixed precision): the hardware approximation (PTX sqrt.approx.f32,
+// relative error about 2^-23), one instruction instead of the correctly
+// rounded sequence
+template <> __device__ __forceinline__ float rsqrt_<float>(float a)
+{
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(a));
+    return r;
+}
 
 // Division by the literal constants 3, 6 and 12 of the PPM formulas.
 // FP64: the correctly rounded quotient x / C (the oracle's operation) without
@@ -96,6 +104,11 @@ __host__ __device__ inline bool extended_options(const DevParams &p)
 // Fortran MIN/MAX with gfortran's argument order: mvar = a1; if (a2 < mvar) mvar = a2
 template <class R> __device__ __forceinline__ R fmin2(R a, R b) { return (b < a) ? b : a; }
 template <class R> __device__ __forceinline__ R fmax2(R a, R b) { return (b > a) ? b : a; }
+// FP32 (mixed precision, compared within a tolerance): one min/max
+// instruction instead of a compare and a select; the two forms differ only
+// for NaN and for the sign of equal zeros
+template <> __device__ __forceinline__ float fmin2<float>(float a, float b) { return fminf(a, b); }
+template <> __device__ __forceinline__ float fmax2<float>(float a, float b) { return fmaxf(a, b); }
 template <class R> __device__ __forceinline__ R sgn1(R b) { return copysign(R(1), b); }
 
 // ---- limiters (hy_slopeLimiters.F90) ----------------------------------------

@@ -406,11 +406,15 @@ hydro2d_kernel(const __grid_constant__ Args2D a)
                 s.OWN[KeepOwn<R>::value ? 4 : 0][tid] = stage[VZ * WIN * WP + c];
                 s.OWN[KeepOwn<R>::value ? 5 : 0][tid] = stage[EI * WIN * WP + c];
             }
-            constexpr int NEL = 8 * WIN * WIN;
-            for (int e = tid; e < NEL; e += NT2) {
-                const int v = e / (WIN * WIN), r = e - v * (WIN * WIN);
-                const int wy = r / WIN, wx = r - wy * WIN;
-                s.V[v][wy][wx + XO] = (R)stage[(v * WIN + wy) * WP + wx + XO];
+            // whole stored rows (the box's 24 columns, pads included) two
+            // values at a time: 16-byte shared loads, 8-byte stores
+            constexpr int NPR = WP / 2, NPAIR = 8 * WIN * NPR;
+            static_assert(WP % 2 == 0, "stored rows hold whole pairs");
+            float *vw = reinterpret_cast<float *>(&s.V[0][0][0]);
+            for (int e = tid; e < NPAIR; e += NT2) {
+                const int row = e / NPR, q = e - row * NPR;
+                const double2 d2 = reinterpret_cast<const double2 *>(stage + row * WP)[q];
+                reinterpret_cast<float2 *>(vw + row * WP)[q] = make_float2((float)d2.x, (float)d2.y);
             }
         }
     } else {
@@ -455,12 +459,20 @@ hydro2d_kernel(const __grid_constant__ Args2D a)
             for (int q = 0; q < (KeepOwn<R>::value ? 6 : 1); q++) s.OWN[q][tid] = own[q];
         }
     }
+    // the step's quotients of dt and the cell sizes, one FP64 division per
+    // thread of the first six instead of all six in every thread
+    __shared__ double uq[6];
+    if (tid < 6) {
+        const double num = tid < 2 ? dt : (tid < 4 ? 0.5 * dt : 1.0);
+        uq[tid] = num / ((tid & 1) ? a.dy : a.dx);
+    }
     // a window that did not arrive in time ends the tile (ERR_TIMEOUT is set)
     if (__syncthreads_or(!ok)) return;
 
-    const R dtnx = R(dt / a.dx), hdtnx = R(0.5 * (dt / a.dx));
-    const R dtny = R(dt / a.dy), hdtny = R(0.5 * (dt / a.dy));
-    const R hdtx = R(0.5 * dt / a.dx), hdty = R(0.5 * dt / a.dy);
+    const double dt_dx = uq[0], dt_dy = uq[1];
+    const R dtnx = R(dt_dx), hdtnx = R(0.5 * dt_dx);
+    const R dtny = R(dt_dy), hdtny = R(0.5 * dt_dy);
+    const R hdtx = R(uq[2]), hdty = R(uq[3]);
     const bool ppm = a.prm.order == 3;     // PPM reads the slopes of its neighbours
 
     // ---- B: x slopes and sigma_y
@@ -486,7 +498,7 @@ hydro2d_kernel(const __grid_constant__ Args2D a)
 
     // ---- E: owner threads, x part of the update
     double U0[5], dens0 = 0., Ax = 0., Bx = 0., pav = 0., SphX = 0., eint0 = 0.;
-    const double dtdx = dt / a.dx, dtdy = dt / a.dy;
+    const double dtdx = dt_dx, dtdy = dt_dy;
     if (owner) {
         double vx, vy, vz, en = s.OWN[0][tid];
         if (KeepOwn<R>::value) {
@@ -600,8 +612,8 @@ hydro2d_kernel(const __grid_constant__ Args2D a)
         o[EI * vs + gidx] = eg; o[DV_ENER * vs + gidx] = eg + ek2; o[DV_TEMP * vs + gidx] = temp;
         // Hydro_computeDt.F90:215-222 rate, in FP64
         double cs = sqrt(prm.gamma * pres / dens);
-        rate = (fabs(vx - 0.) + cs) * (1.0 / a.dx);
-        rate = fmax2(rate, (fabs(vy - 0.) + cs) * (1.0 / a.dy));
+        rate = (fabs(vx - 0.) + cs) * uq[4];
+        rate = fmax2(rate, (fabs(vy - 0.) + cs) * uq[5]);
         if (gidx < a.rate_c0 || gidx >= a.rate_c1) rate = 0.;
     }
     // CTA max, then one atomic per CTA (positive doubles order like their bits)
