@@ -49,6 +49,25 @@ struct DevParams {
 template <class R> __device__ __forceinline__ R rdiv(R a, R b);
 template <> __device__ __forceinline__ double rdiv<double>(double a, double b) { return a / b; }
 template <> __device__ __forceinline__ float rdiv<float>(float a, float b) { return __fdividef(a, b); }
+// a / b for several numerators over one denominator, given y = rdiv(1, b).
+// FP64: the correctly rounded quotient from the correctly rounded
+// reciprocal y by two correction steps q + (a - b q) y: q = a y is within
+// 1.5 ulp of a/b, the first step leaves it within one ulp, and the second is
+// Markstein's (P. Markstein, IBM J. Res. Dev. 34(1), 1990): with y within
+// half an ulp of 1/b and q within one ulp, the remainder is exact in one FMA
+// and RN(q + r y) = RN(a/b).  copysign gives a zero quotient the sign of
+// a / b.  Five FP64 operations per quotient after one division for y.
+// Valid for finite nonzero b and quotients and remainders in the normal
+// range (|a| >= 2^-960 or a = 0).  FP32: the fast division.
+template <class R> __device__ __forceinline__ R rdiv_y(R a, R b, R y);
+template <> __device__ __forceinline__ double rdiv_y<double>(double a, double b, double y)
+{
+    double q = a * y;
+    q = fma(fma(-b, q, a), y, q);
+    q = fma(fma(-b, q, a), y, q);
+    return copysign(q, a * y);
+}
+template <> __device__ __forceinline__ float rdiv_y<float>(float a, float b, float y) { return __fdividef(a, b); }
 template <class R> __device__ __forceinline__ R rsqrt_(R a);
 template <> __device__ __forceinline__ double rsqrt_<double>(double a) { return sqrt(a); }
 // FP32 (mixed precision): the hardware approximation (PTX sqrt.approx.f32,
@@ -155,10 +174,10 @@ template <class R> struct EigBase {
 };
 template <class R> __device__ __forceinline__ bool eigen_base(R rho, R p, R gamc, EigBase<R> &b)
 {
-    R a2 = rdiv(gamc * p, rho);
+    const R dinv = rdiv(R(1), rho);
+    R a2 = rdiv_y(gamc * p, rho, dinv);
     if (a2 <= R(0)) return false;
     R cf = rsqrt_(a2);
-    R dinv = rdiv(R(1), rho);
     R aa2 = cf * cf;
     b.a2inv = rdiv(R(1), aa2);
     b.ahinv = rdiv(R(.5), cf);
@@ -1033,12 +1052,13 @@ __device__ __forceinline__ int riemann(const DevParams &prm, int dir, const R *V
             } else if (SL < R(0) && qStar >= R(0)) {
                 const R numerL = SL - velNL, denomL = SL - qStar;
                 const R pStar = Vm[D] * numerL * (qStar - velNL) + Vm[P];
-                const R dStar = rdiv(UL[0] * numerL, denomL);
+                const R yd = rdiv(R(1), denomL);
+                const R dStar = rdiv_y(UL[0] * numerL, denomL, yd);
                 R UC[5];
                 UC[0] = dStar;
-                UC[4] = rdiv(UL[4] * numerL, denomL) + rdiv(pStar * qStar - Vm[P] * velNL, denomL);
+                UC[4] = rdiv_y(UL[4] * numerL, denomL, yd) + rdiv_y(pStar * qStar - Vm[P] * velNL, denomL, yd);
 #pragma unroll
-                for (int d = 0; d < 3; d++) UC[1 + d] = (d == dir) ? dStar * qStar : rdiv(UL[1 + d] * numerL, denomL);
+                for (int d = 0; d < 3; d++) UC[1 + d] = (d == dir) ? dStar * qStar : rdiv_y(UL[1 + d] * numerL, denomL, yd);
 #pragma unroll
                 for (int k = 0; k < 5; k++) F[k] = FL[k] + SL * (UC[k] - UL[k]);
                 F[5] = FL[5];
@@ -1046,12 +1066,13 @@ __device__ __forceinline__ int riemann(const DevParams &prm, int dir, const R *V
                 const R numerR = SR - velNR, denomR = SR - qStar;
                 const R numerL = SL - velNL;
                 const R pStar = Vm[D] * numerL * (qStar - velNL) + Vm[P];
-                const R dStar = rdiv(UR[0] * numerR, denomR);
+                const R yd = rdiv(R(1), denomR);
+                const R dStar = rdiv_y(UR[0] * numerR, denomR, yd);
                 R UC[5];
                 UC[0] = dStar;
-                UC[4] = rdiv(UR[4] * numerR, denomR) + rdiv(pStar * qStar - Vp[P] * velNR, denomR);
+                UC[4] = rdiv_y(UR[4] * numerR, denomR, yd) + rdiv_y(pStar * qStar - Vp[P] * velNR, denomR, yd);
 #pragma unroll
-                for (int d = 0; d < 3; d++) UC[1 + d] = (d == dir) ? dStar * qStar : rdiv(UR[1 + d] * numerR, denomR);
+                for (int d = 0; d < 3; d++) UC[1 + d] = (d == dir) ? dStar * qStar : rdiv_y(UR[1 + d] * numerR, denomR, yd);
 #pragma unroll
                 for (int k = 0; k < 5; k++) F[k] = FR[k] + SR * (UC[k] - UR[k]);
                 F[5] = FR[5];

@@ -580,9 +580,10 @@ hydro2d_kernel(const __grid_constant__ Args2D a)
             U0[4] = U0[4] + 0.5 * dt * dp;
         }
         double dens = fmax2(U0[0], prm.small_dens);
-        double vx = U0[1] / dens, vy = U0[2] / dens, vz = U0[3] / dens;
-        double ener = U0[4] / dens;
-        double eint = prm.use_aux_eint ? inten / dens : eint0;
+        const double rdens = 1.0 / dens;   // one division for the five quotients by dens
+        double vx = rdiv_y(U0[1], dens, rdens), vy = rdiv_y(U0[2], dens, rdens), vz = rdiv_y(U0[3], dens, rdens);
+        double ener = rdiv_y(U0[4], dens, rdens);
+        double eint = prm.use_aux_eint ? rdiv_y(inten, dens, rdens) : eint0;
         if (EXT && prm.use_gravity) {   // hy_gravityStepBlk -> hy_addGravity: the n+1 half step
             const double hdt = 0.5 * dt;
             double vn[3] = {vx + hdt * prm.grav[0], vy + hdt * prm.grav[1], vz + hdt * prm.grav[2]};
@@ -611,7 +612,7 @@ hydro2d_kernel(const __grid_constant__ Args2D a)
         o[P * vs + gidx] = pres; o[GC * vs + gidx] = prm.gamma; o[GE * vs + gidx] = game;
         o[EI * vs + gidx] = eg; o[DV_ENER * vs + gidx] = eg + ek2; o[DV_TEMP * vs + gidx] = temp;
         // Hydro_computeDt.F90:215-222 rate, in FP64
-        double cs = sqrt(prm.gamma * pres / dens);
+        double cs = sqrt(rdiv_y(prm.gamma * pres, dens, rdens));
         rate = (fabs(vx - 0.) + cs) * uq[4];
         rate = fmax2(rate, (fabs(vy - 0.) + cs) * uq[5]);
         if (gidx < a.rate_c0 || gidx >= a.rate_c1) rate = 0.;

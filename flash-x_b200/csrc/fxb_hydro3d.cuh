@@ -979,9 +979,10 @@ __device__ __forceinline__ void update3d_kernel_body(const Args3D &a, const VB v
             U0[4] = U0[4] + 0.5 * dt * dp;
         }
         double dens = fmax2(U0[0], prm.small_dens);
-        double vx = U0[1] / dens, vy = U0[2] / dens, vz = U0[3] / dens;
-        double ener = U0[4] / dens;
-        double eint = prm.use_aux_eint ? inten / dens : eint0;
+        const double rdens = 1.0 / dens;   // one division for the five quotients by dens
+        double vx = rdiv_y(U0[1], dens, rdens), vy = rdiv_y(U0[2], dens, rdens), vz = rdiv_y(U0[3], dens, rdens);
+        double ener = rdiv_y(U0[4], dens, rdens);
+        double eint = prm.use_aux_eint ? rdiv_y(inten, dens, rdens) : eint0;
         if (prm.use_gravity) {   // hy_gravityStepBlk -> hy_addGravity: n+1 half step
             const double hdt = 0.5 * dt;
             double vn[3] = {vx + hdt * prm.grav[0], vy + hdt * prm.grav[1], vz + hdt * prm.grav[2]};
@@ -1006,7 +1007,7 @@ __device__ __forceinline__ void update3d_kernel_body(const Args3D &a, const VB v
         o[D * ovs] = dens; o[VX * ovs] = vx; o[VY * ovs] = vy; o[VZ * ovs] = vz;
         o[P * ovs] = pres; o[GC * ovs] = prm.gamma; o[GE * ovs] = game;
         o[EI * ovs] = eg; o[DV_ENER * ovs] = eg + ek2; o[DV_TEMP * ovs] = temp;
-        double cs = sqrt(prm.gamma * pres / dens);
+        double cs = sqrt(rdiv_y(prm.gamma * pres, dens, rdens));
         double r = (fabs(vx - 0.) + cs) * (1.0 / X.dx);
         r = fmax2(r, (fabs(vy - 0.) + cs) * (1.0 / X.dy));
         r = fmax2(r, (fabs(vz - 0.) + cs) * (1.0 / X.dz));
