@@ -622,29 +622,35 @@ __device__ __noinline__ WenoPair<R> weno_scalar_body(int method, R I0, R I1, R I
     t1 = I2 - R(2.) * I3 + I4; t2 = R(3.) * I2 - R(4.) * I3 + I4;
     R b2 = c1312 * (t1 * t1) + R(0.25) * (t2 * t2);
     const R tiny = R(1.e-36);
-    R a0, a1, a2, s;
+    // every quotient below shares its denominator with another: the
+    // indicators' with the other side's, the sums' with the other weights
+    const R d0 = tiny + b0, d1 = tiny + b1, d2 = tiny + b2;
+    const R y0 = rdiv(R(1), d0), y1 = rdiv(R(1), d1), y2 = rdiv(R(1), d2);
+    R a0, a1, a2, s, ys;
     // i+1/2, gammas (0.1, 0.6, 0.3)
     if (method == 2) {
         R tau = fabs(b0 - b2);
-        a0 = R(0.1) * (R(1.) + rdiv(tau, tiny + b0));
-        a1 = R(0.6) * (R(1.) + rdiv(tau, tiny + b1));
-        a2 = R(0.3) * (R(1.) + rdiv(tau, tiny + b2));
+        a0 = R(0.1) * (R(1.) + rdiv_y(tau, d0, y0));
+        a1 = R(0.6) * (R(1.) + rdiv_y(tau, d1, y1));
+        a2 = R(0.3) * (R(1.) + rdiv_y(tau, d2, y2));
     } else {
-        a0 = rdiv(R(0.1), tiny + b0); a1 = rdiv(R(0.6), tiny + b1); a2 = rdiv(R(0.3), tiny + b2);
+        a0 = rdiv_y(R(0.1), d0, y0); a1 = rdiv_y(R(0.6), d1, y1); a2 = rdiv_y(R(0.3), d2, y2);
     }
     s = a0 + a1 + a2;
-    vr = rdiv(a0, s) * w5p0 + rdiv(a1, s) * w5p1 + rdiv(a2, s) * w5p2;
+    ys = rdiv(R(1), s);
+    vr = rdiv_y(a0, s, ys) * w5p0 + rdiv_y(a1, s, ys) * w5p1 + rdiv_y(a2, s, ys) * w5p2;
     // i-1/2, gammas (0.3, 0.6, 0.1)
     if (method == 2) {
         R tau = fabs(b0 - b2);
-        a0 = R(0.3) * (R(1.) + rdiv(tau, tiny + b0));
-        a1 = R(0.6) * (R(1.) + rdiv(tau, tiny + b1));
-        a2 = R(0.1) * (R(1.) + rdiv(tau, tiny + b2));
+        a0 = R(0.3) * (R(1.) + rdiv_y(tau, d0, y0));
+        a1 = R(0.6) * (R(1.) + rdiv_y(tau, d1, y1));
+        a2 = R(0.1) * (R(1.) + rdiv_y(tau, d2, y2));
     } else {
-        a0 = rdiv(R(0.3), tiny + b0); a1 = rdiv(R(0.6), tiny + b1); a2 = rdiv(R(0.1), tiny + b2);
+        a0 = rdiv_y(R(0.3), d0, y0); a1 = rdiv_y(R(0.6), d1, y1); a2 = rdiv_y(R(0.1), d2, y2);
     }
     s = a0 + a1 + a2;
-    vl = rdiv(a0, s) * w5m0 + rdiv(a1, s) * w5m1 + rdiv(a2, s) * w5m2;
+    ys = rdiv(R(1), s);
+    vl = rdiv_y(a0, s, ys) * w5m0 + rdiv_y(a1, s, ys) * w5m1 + rdiv_y(a2, s, ys) * w5m2;
     return WenoPair<R>{vr, vl};
 }
 
